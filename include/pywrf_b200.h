@@ -1,0 +1,144 @@
+/*
+ * pywrf_b200 C ABI: the ARW integration step of PyWRF on sm_100a.
+ *
+ * Everything here is plain C: device pointers, sizes and a cudaStream_t
+ * (passed as void*).  The caller owns all memory (no allocation inside any
+ * entry point) and launches run asynchronously on the given stream.  Return
+ * value: 0 on success, negative WRF_E* codes on bad arguments or CUDA launch
+ * errors.  Device-side failures (NaN in the diagnosed pressure, exhausted
+ * bounded waits) are recorded in the WF_STATUS int array and read with
+ * wrf_status_read after the stream is synchronised.
+ *
+ * Layout: 3-D fields are [nz][ny][nx] float32 (x fastest) with the
+ * reference's 5-cell frame: ids = jds = 5, ide = nx - 5, jde = ny - 5
+ * (pywrf/config_params.py:67-99); 2-D fields [ny][nx]; vertical profiles
+ * [nz]; the 7 moisture slots [7][nz][ny][nx] (slot 0 unused, 1..6 =
+ * qv qc qr qi qs qg, config_params.py:102-108); lateral-boundary arrays in
+ * the reference's permuted layout: x sides [nzb][ny][5], y sides [nzb][5][nx]
+ * with nzb = nz (nzb = 1 for mu) (pywrf/solver.py:468-482).
+ */
+#ifndef PYWRF_B200_H
+#define PYWRF_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WRF_OK 0
+#define WRF_EINVAL (-1)   /* bad grid / null pointer / unsupported option */
+#define WRF_ECUDA (-2)    /* a kernel launch failed (see wrf_last_error) */
+
+/* kinds of the fields in the state table */
+#define WRF_K3 3      /* [nz][ny][nx] */
+#define WRF_K2 2      /* [ny][nx] */
+#define WRF_K1 1      /* [nz] */
+#define WRF_K4 4      /* [7][nz][ny][nx] */
+#define WRF_KBX 10    /* [nz][ny][5] */
+#define WRF_KBY 11    /* [nz][5][nx] */
+#define WRF_KBX2 12   /* [1][ny][5] */
+#define WRF_KBY2 13   /* [1][5][nx] */
+#define WRF_KSF 20    /* float[16] device scalars */
+#define WRF_KSI 21    /* int32[16] device status words */
+
+/* status words (WF_STATUS) */
+#define WRF_ST_NAN_P 0        /* NaN points met in the diagnosed p (summed over RK stages) */
+#define WRF_ST_STEP 1         /* completed steps (device step counter) */
+
+/* the persistent state of one integration, in table order */
+#define WRF_FIELD_TABLE(X) \
+  X(U, WRF_K3) X(V, WRF_K3) X(W, WRF_K3) X(T, WRF_K3) X(PH, WRF_K3) X(P, WRF_K3) X(AL, WRF_K3) \
+  X(PB, WRF_K3) X(PHB, WRF_K3) X(T_INIT, WRF_K3) X(ALB, WRF_K3) X(RU, WRF_K3) X(RV, WRF_K3) \
+  X(RW, WRF_K3) X(WW, WRF_K3) X(WW1, WRF_K3) X(CQU, WRF_K3) X(CQV, WRF_K3) X(CQW, WRF_K3) \
+  X(ALT, WRF_K3) X(PHP, WRF_K3) X(RU_TENDF, WRF_K3) X(RV_TENDF, WRF_K3) X(RW_TENDF, WRF_K3) \
+  X(PH_TENDF, WRF_K3) X(T_TENDF, WRF_K3) X(RU_TEND, WRF_K3) X(RV_TEND, WRF_K3) X(RW_TEND, WRF_K3) \
+  X(PH_TEND, WRF_K3) X(T_TEND, WRF_K3) X(U_SAVE, WRF_K3) X(V_SAVE, WRF_K3) X(W_SAVE, WRF_K3) \
+  X(PH_SAVE, WRF_K3) X(T_SAVE, WRF_K3) X(RDZW, WRF_K3) X(ZX, WRF_K3) X(ZY, WRF_K3) \
+  X(DEFOR11, WRF_K3) X(DEFOR22, WRF_K3) X(DEFOR12, WRF_K3) X(XKMH, WRF_K3) X(XKHH, WRF_K3) \
+  X(U_1, WRF_K3) X(V_1, WRF_K3) X(W_1, WRF_K3) X(T_1, WRF_K3) X(PH_1, WRF_K3) X(C2A, WRF_K3) \
+  X(PM1, WRF_K3) X(A, WRF_K3) X(ALPHA, WRF_K3) X(GAMMA, WRF_K3) X(RU_M, WRF_K3) X(RV_M, WRF_K3) \
+  X(WW_M, WRF_K3) X(T_2SAVE, WRF_K3) X(H_DIABATIC, WRF_K3) X(QV_DIABATIC, WRF_K3) \
+  X(QC_DIABATIC, WRF_K3) \
+  X(MU, WRF_K2) X(MUB, WRF_K2) X(MSFU, WRF_K2) X(MSFV, WRF_K2) X(MSFVX_INV, WRF_K2) \
+  X(MSFT, WRF_K2) X(MSFTX, WRF_K2) X(MSFTY, WRF_K2) X(MSFUX, WRF_K2) X(MSFUY, WRF_K2) \
+  X(MSFVX, WRF_K2) X(MSFVY, WRF_K2) X(F, WRF_K2) X(E, WRF_K2) X(SINA, WRF_K2) X(COSA, WRF_K2) \
+  X(HT, WRF_K2) X(RAINNC, WRF_K2) X(RAINNCV, WRF_K2) X(SNOWNC, WRF_K2) X(SNOWNCV, WRF_K2) \
+  X(GRAUPELNC, WRF_K2) X(GRAUPELNCV, WRF_K2) X(SR, WRF_K2) X(MUT, WRF_K2) X(MUU, WRF_K2) \
+  X(MUV, WRF_K2) X(MU_TENDF, WRF_K2) X(MU_TEND, WRF_K2) X(MU_SAVE, WRF_K2) X(MU_1, WRF_K2) \
+  X(MUUS, WRF_K2) X(MUVS, WRF_K2) X(MUTS, WRF_K2) X(MUDF, WRF_K2) X(MUAVE, WRF_K2) \
+  X(RDNW, WRF_K1) X(RDN, WRF_K1) X(C1H, WRF_K1) X(FNM, WRF_K1) X(FNP, WRF_K1) X(DN, WRF_K1) \
+  X(DNW, WRF_K1) \
+  X(MOIST, WRF_K4) X(MOIST_TEND, WRF_K4) X(ADVECT_TEND, WRF_K4) X(MOIST_OLD, WRF_K4) \
+  X(U_BXS, WRF_KBX) X(U_BXE, WRF_KBX) X(U_BYS, WRF_KBY) X(U_BYE, WRF_KBY) \
+  X(U_BTXS, WRF_KBX) X(U_BTXE, WRF_KBX) X(U_BTYS, WRF_KBY) X(U_BTYE, WRF_KBY) \
+  X(V_BXS, WRF_KBX) X(V_BXE, WRF_KBX) X(V_BYS, WRF_KBY) X(V_BYE, WRF_KBY) \
+  X(V_BTXS, WRF_KBX) X(V_BTXE, WRF_KBX) X(V_BTYS, WRF_KBY) X(V_BTYE, WRF_KBY) \
+  X(PH_BXS, WRF_KBX) X(PH_BXE, WRF_KBX) X(PH_BYS, WRF_KBY) X(PH_BYE, WRF_KBY) \
+  X(PH_BTXS, WRF_KBX) X(PH_BTXE, WRF_KBX) X(PH_BTYS, WRF_KBY) X(PH_BTYE, WRF_KBY) \
+  X(T_BXS, WRF_KBX) X(T_BXE, WRF_KBX) X(T_BYS, WRF_KBY) X(T_BYE, WRF_KBY) \
+  X(T_BTXS, WRF_KBX) X(T_BTXE, WRF_KBX) X(T_BTYS, WRF_KBY) X(T_BTYE, WRF_KBY) \
+  X(MU_BXS, WRF_KBX2) X(MU_BXE, WRF_KBX2) X(MU_BYS, WRF_KBY2) X(MU_BYE, WRF_KBY2) \
+  X(MU_BTXS, WRF_KBX2) X(MU_BTXE, WRF_KBX2) X(MU_BTYS, WRF_KBY2) X(MU_BTYE, WRF_KBY2) \
+  X(QV_BXS, WRF_KBX) X(QV_BXE, WRF_KBX) X(QV_BYS, WRF_KBY) X(QV_BYE, WRF_KBY) \
+  X(QV_BTXS, WRF_KBX) X(QV_BTXE, WRF_KBX) X(QV_BTYS, WRF_KBY) X(QV_BTYE, WRF_KBY) \
+  X(DSCAL, WRF_KSF) X(STATUS, WRF_KSI)
+
+#define WRF_ENUM_ENTRY(name, kind) WF_##name,
+enum WrfFieldId { WRF_FIELD_TABLE(WRF_ENUM_ENTRY) WF_COUNT };
+#undef WRF_ENUM_ENTRY
+
+/* Grid, time step and the scalar coefficients read from the input file
+ * (CF1..CFN1, pywrf/solver.py:267-271).  Index bounds follow the reference's
+ * python-style WRF index sets. */
+typedef struct WrfGrid {
+  int nx, ny, nz;
+  int ids, ide, jds, jde;
+  int soundsteps;
+  int spec_zone;
+  int bdy_interval;
+  int top_lid;
+  float dx, dy, dt;
+  float smdiv, emdiv, epssm, khdif, kvdif;
+  float cf1, cf2, cf3, cfn, cfn1;
+} WrfGrid;
+
+/* device pointers of every state field, indexed by WrfFieldId */
+typedef struct WrfState {
+  void* f[WF_COUNT];
+} WrfState;
+
+/* optional host callback invoked after each phase of wrf_rk3_step (the
+ * stream is not synchronised by the library; the callback may do so) */
+typedef void (*wrf_probe_fn)(const char* phase, void* user);
+
+/* table introspection (names are the lower-case reference variable names) */
+int wrf_field_count(void);
+const char* wrf_field_name(int id);
+int wrf_field_kind(int id);
+const char* wrf_last_error(void);
+
+/* Replaces one time step of WrfSolver.solve (pywrf/solver.py:709-1910): the
+ * three RK stages with their acoustic substeps, moisture transport, WSM6 and
+ * the end-of-step lateral-boundary updates.  The step number used for the
+ * boundary time (solver.py:713) is the device counter STATUS[WRF_ST_STEP]+1,
+ * so the call can be captured once in a CUDA graph and replayed. */
+int wrf_rk3_step(const WrfGrid* g, const WrfState* s, void* stream, wrf_probe_fn probe, void* user);
+
+/* Reference function-level entry points (same arguments as the step
+ * driver; each runs exactly the reference function named). */
+/* wrf_dynamics.py:1841-2028 advect_scalar: tend += flux-form advection of field */
+int wrf_advect_scalar(const WrfGrid* g, const float* field, float* tend, const float* ru,
+                      const float* rv, const float* rom, const float* msftx, const float* fzm,
+                      const float* fzp, const float* rdzw, void* stream);
+/* wrf_physics.py:94-136 microphysics_driver -> wsm6 on the solver's column block */
+int wrf_wsm6(const WrfGrid* g, float* th, float* qv, float* qc, float* qr, float* qi, float* qs,
+             float* qg, const float* rho, const float* pii, const float* p, const float* dz8w,
+             float delt, float* rainnc, float* rainncv, float* snownc, float* snowncv,
+             float* graupelnc, float* graupelncv, float* sr, void* stream);
+
+/* copies the 16 device status words to host memory (synchronises the stream) */
+int wrf_status_read(const WrfState* s, void* stream, int* out16);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYWRF_B200_H */

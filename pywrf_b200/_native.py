@@ -1,0 +1,96 @@
+"""ctypes binding of the C ABI in ``include/pywrf_b200.h``.
+
+The library is ``pywrf_b200/lib/libpywrf_b200.so`` (built in-tree by
+:mod:`pywrf_b200.build`).  There is no fallback: if the library is missing or
+cannot be loaded, :func:`lib` raises and nothing runs.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .build import LIB
+
+WRF_OK = 0
+WRF_EINVAL = -1
+WRF_ECUDA = -2
+
+WRF_K3, WRF_K2, WRF_K1, WRF_K4 = 3, 2, 1, 4
+WRF_KBX, WRF_KBY, WRF_KBX2, WRF_KBY2 = 10, 11, 12, 13
+WRF_KSF, WRF_KSI = 20, 21
+
+WRF_ST_NAN_P = 0
+WRF_ST_STEP = 1
+
+
+class WrfGridC(ctypes.Structure):
+    """``WrfGrid`` of include/pywrf_b200.h"""
+    _fields_ = [(n, ctypes.c_int) for n in ("nx", "ny", "nz", "ids", "ide", "jds", "jde", "soundsteps",
+                                             "spec_zone", "bdy_interval", "top_lid")] + \
+               [(n, ctypes.c_float) for n in ("dx", "dy", "dt", "smdiv", "emdiv", "epssm", "khdif", "kvdif",
+                                               "cf1", "cf2", "cf3", "cfn", "cfn1")]
+
+
+PROBE_FN = ctypes.CFUNCTYPE(None, ctypes.c_char_p, ctypes.c_void_p)
+
+_lib = None
+_names: list[str] | None = None
+_kinds: list[int] | None = None
+
+
+class NativeLibraryError(RuntimeError):
+    pass
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded kernel library (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        raise NativeLibraryError(f"{LIB} is not built; run `python -m pywrf_b200.build` (needs nvcc)")
+    try:
+        L = ctypes.CDLL(LIB)
+    except OSError as e:  # pragma: no cover - depends on the machine
+        raise NativeLibraryError(f"cannot load {LIB}: {e}") from e
+    vp, fp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int
+    L.wrf_field_count.restype = ip
+    L.wrf_field_name.restype = ctypes.c_char_p
+    L.wrf_field_name.argtypes = [ip]
+    L.wrf_field_kind.restype = ip
+    L.wrf_field_kind.argtypes = [ip]
+    L.wrf_last_error.restype = ctypes.c_char_p
+    L.wrf_rk3_step.restype = ip
+    L.wrf_rk3_step.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, PROBE_FN, vp]
+    L.wrf_advect_scalar.restype = ip
+    L.wrf_advect_scalar.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 9 + [vp]
+    L.wrf_wsm6.restype = ip
+    L.wrf_wsm6.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 11 + [ctypes.c_float] + [vp] * 7 + [vp]
+    L.wrf_status_read.restype = ip
+    L.wrf_status_read.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int)]
+    _lib = L
+    return L
+
+
+def field_names() -> list[str]:
+    global _names
+    if _names is None:
+        L = lib()
+        _names = [L.wrf_field_name(i).decode() for i in range(L.wrf_field_count())]
+    return _names
+
+
+def field_kinds() -> list[int]:
+    global _kinds
+    if _kinds is None:
+        L = lib()
+        _kinds = [L.wrf_field_kind(i) for i in range(L.wrf_field_count())]
+    return _kinds
+
+
+def check(rc: int, what: str) -> None:
+    if rc != WRF_OK:
+        msg = lib().wrf_last_error().decode(errors="replace")
+        if rc == WRF_EINVAL:
+            raise ValueError(f"{what}: {msg}")
+        raise RuntimeError(f"{what} failed ({rc}): {msg}")

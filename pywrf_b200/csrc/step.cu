@@ -1,0 +1,306 @@
+// C ABI and the host-side step driver: the launch sequence of one ARW time
+// step in the order of WrfSolver.solve (pywrf/solver.py:709-1910).
+//
+// The driver only enqueues kernels and memsets on the caller's stream; it
+// allocates nothing and never synchronises (a probe callback may).  The
+// boundary time of the step is derived on the device from the step counter
+// STATUS[WRF_ST_STEP], so one captured CUDA graph replays every step.
+#include <cstdio>
+#include <cstring>
+#include <cctype>
+#include <string>
+#include "kernels.cuh"
+
+namespace wrf {
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int check_launch(const char* where) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(WRF_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+  return WRF_OK;
+}
+
+#define WRF_NAME_ENTRY(name, kind) #name,
+const char* const kUpperNames[WF_COUNT] = {WRF_FIELD_TABLE(WRF_NAME_ENTRY)};
+#undef WRF_NAME_ENTRY
+#define WRF_KIND_ENTRY(name, kind) kind,
+const int kKinds[WF_COUNT] = {WRF_FIELD_TABLE(WRF_KIND_ENTRY)};
+#undef WRF_KIND_ENTRY
+
+struct LowerNames {
+  char buf[WF_COUNT][24];
+  LowerNames() {
+    for (int i = 0; i < WF_COUNT; ++i) {
+      size_t n = strlen(kUpperNames[i]);
+      if (n > 23) n = 23;
+      for (size_t c = 0; c < n; ++c) buf[i][c] = (char)tolower((unsigned char)kUpperNames[i][c]);
+      buf[i][n] = 0;
+    }
+  }
+};
+const LowerNames kLower;
+
+int make_grid(const WrfGrid* in, Grid& g) {
+  if (!in) return fail(WRF_EINVAL, "null grid");
+  g.nx = in->nx; g.ny = in->ny; g.nz = in->nz;
+  g.ids = in->ids; g.ide = in->ide; g.jds = in->jds; g.jde = in->jde;
+  g.soundsteps = in->soundsteps; g.spec_zone = in->spec_zone; g.top_lid = in->top_lid;
+  if (g.nz < 12 || g.nz > kMaxNz) return fail(WRF_EINVAL, "nz must lie in [12, 64]");
+  if (g.ids != 5 || g.jds != 5 || g.ide != g.nx - 5 || g.jde != g.ny - 5)
+    return fail(WRF_EINVAL, "the 5-cell frame needs ids = jds = 5, ide = nx - 5, jde = ny - 5");
+  if (g.nx < 24 || g.ny < 24) return fail(WRF_EINVAL, "nx and ny must be at least 24");
+  if (g.spec_zone != 1) return fail(WRF_EINVAL, "spec_zone must be 1 (relax zone 4, bdy width 5)");
+  if (g.soundsteps < 2 || (g.soundsteps % 2) != 0) return fail(WRF_EINVAL, "soundsteps must be even and >= 2");
+  if (in->kvdif != 0.0f) return fail(WRF_EINVAL, "kvdif != 0 (vertical diffusion) is not supported");
+  if (in->bdy_interval < 1) return fail(WRF_EINVAL, "bdy_interval must be >= 1");
+  if (!(in->dx > 0.f) || !(in->dy > 0.f) || !(in->dt > 0.f)) return fail(WRF_EINVAL, "dx, dy, dt must be > 0");
+  g.dx = in->dx; g.dy = in->dy; g.dt = in->dt;
+  g.dxd = in->dx; g.dyd = in->dy; g.dtd = in->dt;
+  g.rdxd = 1.0 / g.dxd; g.rdyd = 1.0 / g.dyd;
+  g.rdx = (float)g.rdxd; g.rdy = (float)g.rdyd;
+  g.smdiv = in->smdiv; g.emdiv = in->emdiv; g.epssm = in->epssm;
+  g.cf1 = in->cf1; g.cf2 = in->cf2; g.cf3 = in->cf3; g.cfn = in->cfn; g.cfn1 = in->cfn1;
+  return WRF_OK;
+}
+
+int make_state(const WrfState* in, S& s) {
+  if (!in) return fail(WRF_EINVAL, "null state");
+  for (int i = 0; i < WF_COUNT; ++i) {
+    s.f[i] = static_cast<float*>(in->f[i]);
+    if (!s.f[i]) return fail(WRF_EINVAL, std::string("null field ") + kLower.buf[i]);
+  }
+  return WRF_OK;
+}
+
+// boundary time of this step from the device step counter (solver.py:713-718)
+__global__ void k_step_begin(float* dscal, const int* status, int bdy_interval, double dt) {
+  const int step = status[WRF_ST_STEP] + 1;
+  const int it_bdy = bdy_interval > 1 ? (step - 1) / bdy_interval : 0;
+  dscal[DS_DTBC] = (float)(dt * (double)(step - it_bdy * bdy_interval));
+  dscal[DS_STEP] = (float)step;
+}
+
+__global__ void k_step_end(int* status) { status[WRF_ST_STEP] += 1; }
+
+struct Driver {
+  Grid g;
+  S s;
+  cudaStream_t st;
+  wrf_probe_fn probe;
+  void* user;
+  int rc = WRF_OK;
+
+  size_t b3() const { return g.n3() * sizeof(float); }
+  size_t b2() const { return g.n2() * sizeof(float); }
+
+  bool ok(const char* where) {
+    if (rc != WRF_OK) return false;
+    rc = check_launch(where);
+    return rc == WRF_OK;
+  }
+  void zero3(int id) { if (rc == WRF_OK && cudaMemsetAsync(s[id], 0, b3(), st) != cudaSuccess) rc = check_launch("memset"); }
+  void zero2(int id) { if (rc == WRF_OK && cudaMemsetAsync(s[id], 0, b2(), st) != cudaSuccess) rc = check_launch("memset"); }
+  void zero4(int id) { if (rc == WRF_OK && cudaMemsetAsync(s[id], 0, 7 * b3(), st) != cudaSuccess) rc = check_launch("memset"); }
+  void phase(const char* name) {
+    if (!ok(name)) return;
+    if (probe) probe(name, user);
+  }
+  void bc(std::initializer_list<std::pair<int, char>> f3, std::initializer_list<std::pair<int, char>> f2 = {}) {
+    BcBatch b;
+    for (auto& e : f3) {
+      if (b.n == kBcMax) { launch_bc(g, b, st); b.n = 0; }
+      b.add(bc_item(g, s[e.first], e.second, false));
+    }
+    for (auto& e : f2) {
+      if (b.n == kBcMax) { launch_bc(g, b, st); b.n = 0; }
+      b.add(bc_item(g, s[e.first], e.second, true));
+    }
+    launch_bc(g, b, st);
+  }
+  void bc_moist() {
+    BcBatch b;
+    for (int m = 1; m < 7; ++m) b.add(bc_item(g, s[WF_MOIST] + m * g.n3(), 'p', false));
+    launch_bc(g, b, st);
+  }
+
+  void run() {
+    const float dt = g.dt;
+    const float dts = (float)(g.dtd / g.soundsteps);
+    k_step_begin<<<1, 1, 0, st>>>(s[WF_DSCAL], reinterpret_cast<const int*>(s[WF_STATUS]), bdy_interval, g.dtd);
+    if (!ok("step_begin")) return;
+    char tag[32];
+    for (int rk = 1; rk <= 3; ++rk) {
+      float dt_rk, dts_rk;
+      int nsub;
+      if (rk == 1) { dt_rk = (float)(g.dtd / 3.0); dts_rk = dt_rk; nsub = 1; }
+      else if (rk == 2) { dt_rk = (float)(0.5 * g.dtd); dts_rk = dts; nsub = g.soundsteps / 2; }
+      else { dt_rk = dt; dts_rk = dts; nsub = g.soundsteps; }
+      // rk_step_prep (solver.py:736-778)
+      launch_prep(g, s, st);
+      bc({{WF_RU, 'u'}, {WF_RV, 'v'}, {WF_RW, 'w'}, {WF_WW, 'w'}, {WF_PHP, 'w'}, {WF_ALT, 't'}, {WF_P, 'p'},
+          {WF_AL, 'p'}, {WF_PH, 'w'}},
+         {{WF_MUU, 'u'}, {WF_MUV, 'v'}, {WF_MUT, 't'}});
+      snprintf(tag, sizeof tag, "s%d.prep", rk);
+      phase(tag);
+      if (rk == 1) {
+        // physics tendencies start from zero; diffusion metrics and eddy viscosities
+        zero3(WF_RU_TENDF); zero3(WF_RV_TENDF); zero3(WF_RW_TENDF); zero3(WF_PH_TENDF); zero3(WF_T_TENDF);
+        zero2(WF_MU_TENDF);
+        zero4(WF_MOIST_TEND);
+        launch_diff_metrics(g, s, st);
+        bc({{WF_RDZW, 'w'}, {WF_ZX, 'e'}, {WF_ZY, 'f'}});
+        launch_km(g, s, st);
+        bc({{WF_XKMH, 't'}, {WF_XKHH, 't'}});
+        snprintf(tag, sizeof tag, "s%d.km", rk);
+        phase(tag);
+      }
+      zero3(WF_RU_TEND); zero3(WF_RV_TEND); zero3(WF_RW_TEND); zero3(WF_T_TEND); zero3(WF_PH_TEND);
+      zero3(WF_U_SAVE); zero3(WF_V_SAVE); zero3(WF_W_SAVE); zero3(WF_PH_SAVE); zero3(WF_T_SAVE);
+      zero2(WF_MU_TEND); zero2(WF_MU_SAVE);
+      launch_advect_forces(g, s, st);
+      snprintf(tag, sizeof tag, "s%d.forces", rk);
+      phase(tag);
+      if (rk == 1) {
+        launch_hdiff_relax(g, s, st);
+        snprintf(tag, sizeof tag, "s%d.diff", rk);
+        phase(tag);
+      }
+      launch_addtend(g, s, rk, st);
+      snprintf(tag, sizeof tag, "s%d.tend", rk);
+      phase(tag);
+      // acoustic set-up (solver.py:1258-1345)
+      launch_small_step_prep(g, s, rk, dts_rk, st);
+      bc({{WF_RU_TEND, 'u'}, {WF_RV_TEND, 'v'}, {WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}, {WF_T_1, 't'},
+          {WF_T_SAVE, 't'}},
+         {{WF_MU_1, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
+      snprintf(tag, sizeof tag, "s%d.acprep", rk);
+      phase(tag);
+      for (int it = 1; it <= nsub; ++it) {
+        launch_substep(g, s, dts_rk, it, nsub, st);
+        bc({{WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}}, {{WF_MUTS, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
+        snprintf(tag, sizeof tag, "s%d.sub%d", rk, it);
+        phase(tag);
+      }
+      launch_small_step_finish(g, s, dts_rk, nsub, rk, st);
+      if (rk == 3)
+        bc({{WF_RU_M, 'u'}, {WF_RV_M, 'v'}, {WF_WW_M, 'w'}}, {{WF_MUT, 't'}, {WF_MUTS, 't'}});
+      snprintf(tag, sizeof tag, "s%d.acfinish", rk);
+      phase(tag);
+      // moisture transport (solver.py:1548-1604)
+      launch_advect_moist(g, s, st);
+      if (rk == 1) {
+        launch_hdiff_moist(g, s, st);
+        launch_relax_qv(g, s, st);
+      }
+      launch_moist(g, s, rk, dt_rk, st);
+      if (rk < 3) {
+        bc({{WF_U, 'U'}, {WF_V, 'V'}, {WF_W, 'w'}, {WF_T, 'p'}, {WF_PH, 'w'}}, {{WF_MU, 't'}});
+        bc_moist();
+      }
+      snprintf(tag, sizeof tag, "s%d.moist", rk);
+      phase(tag);
+    }
+    // microphysics (solver.py:1714-1766)
+    launch_physics(g, s, st);
+    phase("mp");
+    // end-of-step boundaries (solver.py:1776-1910)
+    bc({{WF_U_1, 'U'}, {WF_U, 'U'}, {WF_V_1, 'V'}, {WF_V, 'V'}, {WF_W_1, 'w'}, {WF_W, 'w'}, {WF_T_1, 'p'},
+        {WF_T, 'p'}, {WF_PH_1, 'w'}, {WF_PH, 'w'}},
+       {{WF_MU_1, 't'}, {WF_MU, 't'}});
+    bc_moist();
+    launch_bdy_final(g, s, st);
+    k_step_end<<<1, 1, 0, st>>>(reinterpret_cast<int*>(s[WF_STATUS]));
+    phase("end");
+  }
+  int bdy_interval = 360;
+};
+
+}  // namespace
+}  // namespace wrf
+
+using namespace wrf;
+
+extern "C" {
+
+int wrf_field_count(void) { return WF_COUNT; }
+
+const char* wrf_field_name(int id) {
+  if (id < 0 || id >= WF_COUNT) return nullptr;
+  return kLower.buf[id];
+}
+
+int wrf_field_kind(int id) {
+  if (id < 0 || id >= WF_COUNT) return WRF_EINVAL;
+  return kKinds[id];
+}
+
+const char* wrf_last_error(void) { return g_err.c_str(); }
+
+int wrf_rk3_step(const WrfGrid* gin, const WrfState* sin, void* stream, wrf_probe_fn probe, void* user) {
+  Driver d;
+  int rc = make_grid(gin, d.g);
+  if (rc) return rc;
+  rc = make_state(sin, d.s);
+  if (rc) return rc;
+  d.st = static_cast<cudaStream_t>(stream);
+  d.probe = probe;
+  d.user = user;
+  d.bdy_interval = gin->bdy_interval;
+  cudaGetLastError();  // clear a stale error from an unrelated earlier call
+  d.run();
+  return d.rc;
+}
+
+int wrf_advect_scalar(const WrfGrid* gin, const float* field, float* tend, const float* ru, const float* rv,
+                      const float* rom, const float* msftx, const float* fzm, const float* fzp, const float* rdzw,
+                      void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!field || !tend || !ru || !rv || !rom || !msftx || !fzm || !fzp || !rdzw)
+    return fail(WRF_EINVAL, "null argument");
+  S s{};
+  s.f[WF_MSFTX] = const_cast<float*>(msftx);
+  s.f[WF_FNM] = const_cast<float*>(fzm);
+  s.f[WF_FNP] = const_cast<float*>(fzp);
+  s.f[WF_RDNW] = const_cast<float*>(rdzw);
+  cudaGetLastError();
+  launch_advect_scalar(g, s, field, tend, ru, rv, rom, static_cast<cudaStream_t>(stream));
+  return check_launch("advect_scalar");
+}
+
+int wrf_wsm6(const WrfGrid* gin, float* th, float* qv, float* qc, float* qr, float* qi, float* qs, float* qg,
+             const float* rho, const float* pii, const float* p, const float* dz8w, float delt, float* rainnc,
+             float* rainncv, float* snownc, float* snowncv, float* graupelnc, float* graupelncv, float* sr,
+             void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  float* f[18] = {th, qv, qc, qr, qi, qs, qg, const_cast<float*>(rho), const_cast<float*>(pii),
+                  const_cast<float*>(p), const_cast<float*>(dz8w), rainnc, rainncv, snownc, snowncv,
+                  graupelnc, graupelncv, sr};
+  for (float* x : f)
+    if (!x) return fail(WRF_EINVAL, "null argument");
+  if (!(delt > 0.f)) return fail(WRF_EINVAL, "delt must be > 0");
+  cudaGetLastError();
+  launch_wsm6(g, f, delt, static_cast<cudaStream_t>(stream));
+  return check_launch("wsm6");
+}
+
+int wrf_status_read(const WrfState* sin, void* stream, int* out16) {
+  if (!sin || !sin->f[WF_STATUS] || !out16) return fail(WRF_EINVAL, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemcpyAsync(out16, sin->f[WF_STATUS], 16 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return check_launch("status_read");
+  if (cudaStreamSynchronize(st) != cudaSuccess) return check_launch("status_read");
+  return WRF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+"""Drop-in ``WrfSolver``: the reference's time loop on the sm_100a kernels.
+
+``WrfSolver.solve`` keeps the reference's contract (pywrf/solver.py:32-1921):
+it obtains the input / boundary / reference datasets from
+``self._load_datasets()`` (override it to feed other data, exactly as with
+the reference), runs ``nsteps`` ARW time steps and returns the final
+``{"u", "v", "w", "t", "ph", "mu", "moist"}`` tensors in the reference's
+halo-frame layout.  The step itself is :class:`Integrator.step`, one call of
+``wrf_rk3_step`` (include/pywrf_b200.h), optionally replayed from a CUDA
+graph; nothing of it runs on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Callable, Mapping
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .config import Grid
+from .state import DeviceState, grid_from_inputs
+
+# run parameters of the reference configuration (pywrf/config_params.py:41-72)
+DEFAULTS = dict(dx=9000.0, dy=9000.0, dt=60.0, p_top=1000.0, soundsteps=4, bdy_interval=360, nsteps=720)
+
+
+def _stream_handle(stream: torch.cuda.Stream | None) -> ctypes.c_void_p:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+class Integrator:
+    """Advances one :class:`DeviceState` by whole ARW time steps."""
+
+    def __init__(self, state: DeviceState):
+        if state.device.type != "cuda":
+            raise ValueError("the ARW step runs on a CUDA device only")
+        self.state = state
+        self.lib = N.lib()
+        self._graph: torch.cuda.CUDAGraph | None = None
+        self._graph_stream: torch.cuda.Stream | None = None
+
+    def step(self, probe: Callable[[str], None] | None = None, stream: torch.cuda.Stream | None = None) -> None:
+        """Enqueue one time step on ``stream`` (default: the current stream).
+        ``probe(phase)`` is called after each phase, with the stream not yet
+        synchronised."""
+        cb = N.PROBE_FN(lambda name, user: probe(name.decode())) if probe else N.PROBE_FN()
+        with torch.cuda.device(self.state.device):
+            rc = self.lib.wrf_rk3_step(ctypes.byref(self.state.cgrid), self.state.ptr, _stream_handle(stream), cb, None)
+        N.check(rc, "wrf_rk3_step")
+
+    def capture(self) -> None:
+        """Record one step into a CUDA graph (the step number lives on the
+        device, so the same graph serves every step)."""
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.device(self.state.device):
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(g, stream=s):
+                    rc = self.lib.wrf_rk3_step(ctypes.byref(self.state.cgrid), self.state.ptr,
+                                               _stream_handle(s), N.PROBE_FN(), None)
+            torch.cuda.current_stream().wait_stream(s)
+        N.check(rc, "wrf_rk3_step (capture)")
+        self._graph, self._graph_stream = g, s
+
+    def replay(self) -> None:
+        if self._graph is None:
+            self.capture()
+        self._graph.replay()
+
+    def run(self, nsteps: int, graph: bool = True) -> None:
+        for _ in range(nsteps):
+            if graph:
+                self.replay()
+            else:
+                self.step()
+
+    def status(self) -> dict[str, int]:
+        out = (ctypes.c_int * 16)()
+        with torch.cuda.device(self.state.device):
+            torch.cuda.current_stream().synchronize()
+            rc = self.lib.wrf_status_read(self.state.ptr, _stream_handle(None), out)
+        N.check(rc, "wrf_status_read")
+        return {"nan_p": out[N.WRF_ST_NAN_P], "step": out[N.WRF_ST_STEP]}
+
+
+class WrfSolver:
+    """Orchestrate one WRF run on the GPU (same call pattern as the reference:
+    construct, then :meth:`solve`)."""
+
+    def __init__(self, nsteps: int | None = None, device: str | torch.device | None = None, graph: bool = True,
+                 **params):
+        p = dict(DEFAULTS)
+        unknown = set(params) - set(p)
+        if unknown:
+            raise TypeError(f"unknown parameters {sorted(unknown)}")
+        p.update(params)
+        if nsteps is not None:
+            p["nsteps"] = int(nsteps)
+        self.params = p
+        self.nsteps = p["nsteps"]
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.graph = graph
+        self.integrator: Integrator | None = None
+
+    def _load_datasets(self):
+        """Open the input / boundary / reference WRF NetCDF files named by
+        PYWRF_DATA_DIR and PYWRF_RUN_NAME (pywrf/solver.py:22-46)."""
+        import xarray as xr   # I/O only; absent here unless installed
+        data_dir = os.environ.get("PYWRF_DATA_DIR", "data")
+        run = os.environ.get("PYWRF_RUN_NAME", "2024020106")
+        return (xr.open_dataset(os.path.join(data_dir, f"wrf_inout_step3_{run}")),
+                xr.open_dataset(os.path.join(data_dir, f"wrfbdy_d01_{run}")),
+                xr.open_dataset(os.path.join(data_dir, f"wrfout_d01_{run}")))
+
+    @staticmethod
+    def _arrays(ds) -> Mapping[str, np.ndarray]:
+        class _View(dict):
+            def __missing__(self, key):
+                v = ds[key]
+                v = np.asarray(getattr(v, "data", v))
+                self[key] = v
+                return v
+        return _View()
+
+    def prepare(self) -> Integrator:
+        wrfinput, wrfbdy, _ = self._load_datasets()
+        inputs, bdy = self._arrays(wrfinput), self._arrays(wrfbdy)
+        p = self.params
+        g = grid_from_inputs(inputs, p["dx"], p["dy"], p["dt"], p["p_top"], p["soundsteps"], p["bdy_interval"])
+        state = DeviceState.from_inputs(g, inputs, bdy, device=self.device)
+        self.integrator = Integrator(state)
+        return self.integrator
+
+    def solve(self):
+        """Integrate ``nsteps`` steps; returns the final key fields."""
+        it = self.prepare()
+        it.run(self.nsteps, graph=self.graph)
+        st = it.status()
+        if st["nan_p"]:
+            raise FloatingPointError(f"NaN in the diagnosed pressure ({st['nan_p']} stage(s)) by step {st['step']}")
+        s = it.state
+        return {k: s[k] for k in ("u", "v", "w", "t", "ph", "mu", "moist")}

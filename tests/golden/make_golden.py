@@ -1,0 +1,97 @@
+"""Generate the golden fixtures by running the reference PyWRF step on CPU.
+
+Usage:  python tests/golden/make_golden.py [--reference /path/to/PyWRF]
+
+Writes, next to this script:
+
+* ``small_ref64.npz`` / ``small_ref32.npz``: full fields after 2 RK3 steps of
+  a 28x28x16 synthetic state with seeded lateral-boundary tendencies, from the
+  reference in float64 and float32.
+* ``c0_ref64_summary.json``: per-field checksums (sum, L2 norm) and 64 sampled
+  values per field after 3 steps of configuration 0 (64x64x41) in float64.
+* ``c1_ref64_summary.json``: the same after 1 step of the 240x240x41
+  configuration with boundary tendencies.
+
+The reference is read from its source tree (default /root/reference); this
+script is the only producer of the fixtures and is never run by the tests.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+sys.path.insert(0, HERE)
+
+from pywrf_b200 import synthetic  # noqa: E402
+
+FIELDS = ["u", "v", "w", "t", "ph", "mu", "p", "al", "h_diabatic", "rainnc", "muts", "ww"]
+SPECIES = ["qv", "qc", "qr", "qi", "qs", "qg"]
+SMALL = dict(n=28, nz=16, nsteps=2, bdy_tend_amp=1.0e-4, seed=3)
+
+
+def pick(res):
+    out = {k: res[k] for k in FIELDS}
+    for i, nm in enumerate(SPECIES, start=1):
+        out[nm] = res["moist"][i]
+    return out
+
+
+def summary(res, nsample=64, seed=0):
+    rng = np.random.default_rng(seed)
+    out = {}
+    for k, a in pick(res).items():
+        a = np.asarray(a, np.float64)
+        idx = rng.integers(0, a.size, nsample)
+        out[k] = {"sum": float(a.sum()), "l2": float(np.sqrt((a * a).sum())), "idx": idx.tolist(),
+                  "val": a.reshape(-1)[idx].tolist(), "shape": list(a.shape)}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("PYWRF_REFERENCE_ROOT", "/root/reference"))
+    ap.add_argument("--skip-c1", action="store_true")
+    args = ap.parse_args()
+    os.environ["PYWRF_REFERENCE_ROOT"] = args.reference
+    import refharness
+    refharness.REF_ROOT = args.reference
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = synthetic.grid_for(spec)
+    inp, bdy = synthetic.build(spec)
+    meta = {"case": SMALL, "solver_sha256": None}
+    for dt in ("float64", "float32"):
+        res = refharness.run_reference(g, inp, bdy, spec.nsteps, dtype=dt)
+        meta["solver_sha256"] = refharness.SOLVER_SHA256
+        np.savez_compressed(os.path.join(HERE, f"small_ref{dt[-2:]}.npz"),
+                            meta=json.dumps(meta), **{k: np.asarray(v, dt) for k, v in pick(res).items()})
+        print("wrote small", dt)
+
+    spec0 = synthetic.spec_for_config(0)
+    g0 = synthetic.grid_for(spec0)
+    inp0, bdy0 = synthetic.build(spec0)
+    res0 = refharness.run_reference(g0, inp0, bdy0, 3, dtype="float64")
+    with open(os.path.join(HERE, "c0_ref64_summary.json"), "w") as f:
+        json.dump({"config": 0, "nsteps": 3, "solver_sha256": refharness.SOLVER_SHA256,
+                   "fields": summary(res0)}, f)
+    print("wrote c0 summary")
+    if not args.skip_c1:
+        spec1 = synthetic.spec_for_config(1)
+        g1 = synthetic.grid_for(spec1)
+        inp1, bdy1 = synthetic.build(spec1)
+        res1 = refharness.run_reference(g1, inp1, bdy1, 1, dtype="float64")
+        with open(os.path.join(HERE, "c1_ref64_summary.json"), "w") as f:
+            json.dump({"config": 1, "nsteps": 1, "solver_sha256": refharness.SOLVER_SHA256,
+                       "fields": summary(res1)}, f)
+        print("wrote c1 summary")
+
+
+if __name__ == "__main__":
+    main()
