@@ -138,6 +138,10 @@ int wrf_wsm6(const WrfGrid* g, float* th, float* qv, float* qc, float* qr, float
 /* copies the 16 device status words to host memory (synchronises the stream) */
 int wrf_status_read(const WrfState* s, void* stream, int* out16);
 
+/* number of kernels the calling thread's last wrf_rk3_step enqueued (the
+ * reference has no counterpart; used to report launch counts) */
+int wrf_last_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

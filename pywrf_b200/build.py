@@ -26,7 +26,11 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libpywrf_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+# -fmad=false: the reference rounds every multiply and add separately; letting
+# nvcc contract them into FMAs changes the rounding of the many
+# cancellation-prone differences of the step (bdy - ph*mu, muts*t_1 - mut*t_2,
+# p0*pp - pb ...) for no measurable gain in these memory-bound kernels.
+NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                      "-I" + INCLUDE, "-I" + CSRC]
 
 

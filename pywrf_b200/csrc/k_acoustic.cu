@@ -506,26 +506,29 @@ __global__ void k_ssfinish(Grid g, S s, float dts, int nsub, int rk_step) {
   }
 }
 
-void launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cudaStream_t st) {
+int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);
   k_ssp2d<<<col_grid(g, b2), b2, 0, st>>>(g, s, rk_step);
   k_ssp3d<<<point_grid(g, b3), b3, 0, st>>>(g, s, rk_step);
   k_p_rho<<<point_grid(g, b3), b3, 0, st>>>(g, s, 0);
   k_coef_w<<<col_grid(g, b2), b2, 0, st>>>(g, s, dts);
+  return 4;
 }
 
-void launch_substep(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st) {
+int launch_substep(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);
   k_advance_uv<<<point_grid(g, b3), b3, 0, st>>>(g, s, dts);
   k_advance_mu_t<<<col_grid(g, b2), b2, 0, st>>>(g, s, dts);
   k_advance_w<<<col_grid(g, b2), b2, 0, st>>>(g, s, dts, iteration, nsub);
   k_p_rho<<<point_grid(g, b3), b3, 0, st>>>(g, s, iteration);
+  return 4;
 }
 
-void launch_small_step_finish(const Grid& g, const S& s, float dts, int nsub, int rk_step, cudaStream_t st) {
+int launch_small_step_finish(const Grid& g, const S& s, float dts, int nsub, int rk_step, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);
   k_mu_uv_1<<<col_grid(g, b2), b2, 0, st>>>(g, s);
   k_ssfinish<<<point_grid(g, b3), b3, 0, st>>>(g, s, dts, nsub, rk_step);
+  return 2;
 }
 
 }  // namespace wrf

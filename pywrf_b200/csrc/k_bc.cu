@@ -104,7 +104,7 @@ int launch_bc(const Grid& g, const BcBatch& b, cudaStream_t st) {
   dim3 blk(128, 1, 1);
   k_bc_x<<<dim3((g.ny + 127) / 128, kmax, b.n), blk, 0, st>>>(g, b);
   k_bc_y<<<dim3((g.nx + 127) / 128, kmax, b.n), blk, 0, st>>>(g, b);
-  return 0;
+  return 2;
 }
 
 }  // namespace wrf

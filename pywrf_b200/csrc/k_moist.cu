@@ -177,21 +177,24 @@ __global__ void k_w_surface(Grid g, S s) {
   s[WF_W][c] = msfty[c] * 0.5f * g.rdy * yterm + mx * 0.5f * g.rdx * xterm;
 }
 
-void launch_moist(const Grid& g, const S& s, int rk_step, float dt_rk, cudaStream_t st) {
+int launch_moist(const Grid& g, const S& s, int rk_step, float dt_rk, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_moist_update<<<point_grid(g, b3), b3, 0, st>>>(g, s, rk_step, dt_rk);
   k_eos_flowdep<<<point_grid(g, b3), b3, 0, st>>>(g, s, 1);
+  return 2;
 }
 
-void launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st) {
+int launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_hdiff_moist<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  return 1;
 }
 
-void launch_bdy_final(const Grid& g, const S& s, cudaStream_t st) {
+int launch_bdy_final(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);
   k_bdy_final<<<point_grid(g, b3), b3, 0, st>>>(g, s);
   k_w_surface<<<col_grid(g, b2), b2, 0, st>>>(g, s);
+  return 2;
 }
 
 }  // namespace wrf

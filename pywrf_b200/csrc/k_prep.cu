@@ -484,34 +484,39 @@ __global__ void k_relax_qv(Grid g, S s) {
   if (hit) tend[p] = val;
 }
 
-void launch_prep(const Grid& g, const S& s, cudaStream_t st) {
+int launch_prep(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);
   k_rk_prep2d<<<col_grid(g, b2), b2, 0, st>>>(g, s);
   k_rk_prep3d<<<point_grid(g, b3), b3, 0, st>>>(g, s);
   k_ww_cp<<<col_grid(g, b2), b2, 0, st>>>(g, s);
+  return 3;
 }
 
-void launch_km(const Grid& g, const S& s, cudaStream_t st) {
+int launch_km(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_deform<<<point_grid(g, b3), b3, 0, st>>>(g, s);
   k_defor12_bc<<<point_grid(g, b3), b3, 0, st>>>(g, s);
   k_km<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  return 3;
 }
 
-void launch_diff_metrics(const Grid& g, const S& s, cudaStream_t st) {
+int launch_diff_metrics(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_diff_metrics<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  return 1;
 }
 
-void launch_hdiff_relax(const Grid& g, const S& s, cudaStream_t st) {
+int launch_hdiff_relax(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_hdiff<<<point_grid(g, b3), b3, 0, st>>>(g, s);
   k_relax<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  return 2;
 }
 
-void launch_relax_qv(const Grid& g, const S& s, cudaStream_t st) {
+int launch_relax_qv(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_relax_qv<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  return 1;
 }
 
 }  // namespace wrf

@@ -539,26 +539,30 @@ __global__ void k_advect_scalar(Grid g, S s, const float* q, float* tend, const 
   advect_scalar_point(g, s, q, tend, ru, rv, rom, k, j, i);
 }
 
-void launch_advect_forces(const Grid& g, const S& s, cudaStream_t st) {
+int launch_advect_forces(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_advect<<<point_grid(g, b3), b3, 0, st>>>(g, s);
   k_forces<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  return 2;
 }
 
-void launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st) {
+int launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_addtend<<<point_grid(g, b3), b3, 0, st>>>(g, s, rk_step);
+  return 1;
 }
 
-void launch_advect_scalar(const Grid& g, const S& s, const float* field, float* tend, const float* ru,
+int launch_advect_scalar(const Grid& g, const S& s, const float* field, float* tend, const float* ru,
                           const float* rv, const float* rom, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_advect_scalar<<<point_grid(g, b3), b3, 0, st>>>(g, s, field, tend, ru, rv, rom);
+  return 1;
 }
 
-void launch_advect_moist(const Grid& g, const S& s, cudaStream_t st) {
+int launch_advect_moist(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_advect_moist<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  return 1;
 }
 
 }  // namespace wrf

@@ -766,17 +766,19 @@ __global__ void __launch_bounds__(128) k_wsm6(Grid g, Wsm6Args a, float delt) {
 
 #undef F
 
-void launch_physics(const Grid& g, const S& s, cudaStream_t st) {
+int launch_physics(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b(32, 4);
   k_physics<<<col_grid(g, b), b, 0, st>>>(g, s, g.dt);
+  return 1;
 }
 
 // f: th qv qc qr qi qs qg rho pii p dz8w rainnc rainncv snownc snowncv graupelnc graupelncv sr
-void launch_wsm6(const Grid& g, float* const* f, float delt, cudaStream_t st) {
+int launch_wsm6(const Grid& g, float* const* f, float delt, cudaStream_t st) {
   Wsm6Args a{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], f[10],
              f[11], f[12], f[13], f[14], f[15], f[16], f[17]};
   const dim3 b(32, 4);
   k_wsm6<<<col_grid(g, b), b, 0, st>>>(g, a, delt);
+  return 1;
 }
 
 }  // namespace wrf

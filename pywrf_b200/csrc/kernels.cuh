@@ -1,4 +1,5 @@
-// Launchers of the step kernels (one group per reference phase).
+// Launchers of the step kernels (one group per reference phase).  Each
+// returns the number of kernels it enqueued.
 #pragma once
 #include "wrf_common.cuh"
 #include "bc.cuh"
@@ -10,39 +11,39 @@ constexpr int kMaxNz = 64;
 
 // rk_step_prep: calculate_full, calc_mu_uv, couple_momentum, calc_ww_cp,
 // calc_cq, calc_alt, calc_php (k_prep.cu)
-void launch_prep(const Grid& g, const S& s, cudaStream_t st);
+int launch_prep(const Grid& g, const S& s, cudaStream_t st);
 // compute_diff_metrics (k_prep.cu)
-void launch_diff_metrics(const Grid& g, const S& s, cudaStream_t st);
+int launch_diff_metrics(const Grid& g, const S& s, cudaStream_t st);
 // cal_deform_and_div + calculate_km_kh (k_prep.cu)
-void launch_km(const Grid& g, const S& s, cudaStream_t st);
+int launch_km(const Grid& g, const S& s, cudaStream_t st);
 // horizontal_diffusion u/v/w/theta + relax_bdytend u/v/ph/t/mu (k_prep.cu)
-void launch_hdiff_relax(const Grid& g, const S& s, cudaStream_t st);
+int launch_hdiff_relax(const Grid& g, const S& s, cudaStream_t st);
 // relax_bdytend + spec_bdytend of qv into moist_tend (k_prep.cu)
-void launch_relax_qv(const Grid& g, const S& s, cudaStream_t st);
+int launch_relax_qv(const Grid& g, const S& s, cudaStream_t st);
 
 // advection of u, v, w, theta and the pressure-gradient / buoyancy /
 // Coriolis / curvature forces (k_tend.cu)
-void launch_advect_forces(const Grid& g, const S& s, cudaStream_t st);
+int launch_advect_forces(const Grid& g, const S& s, cudaStream_t st);
 // rk_addtend_dry + spec_bdytend (k_tend.cu)
-void launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st);
+int launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st);
 // moisture advection with the time-averaged fluxes (k_tend.cu)
-void launch_advect_moist(const Grid& g, const S& s, cudaStream_t st);
+int launch_advect_moist(const Grid& g, const S& s, cudaStream_t st);
 // stand-alone advect_scalar (k_tend.cu)
-void launch_advect_scalar(const Grid& g, const S& s, const float* field, float* tend, const float* ru,
+int launch_advect_scalar(const Grid& g, const S& s, const float* field, float* tend, const float* ru,
                           const float* rv, const float* rom, cudaStream_t st);
 
 // acoustic steps (k_acoustic.cu)
-void launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cudaStream_t st);
-void launch_substep(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st);
-void launch_small_step_finish(const Grid& g, const S& s, float dts, int nsub, int rk_step, cudaStream_t st);
+int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cudaStream_t st);
+int launch_substep(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st);
+int launch_small_step_finish(const Grid& g, const S& s, float dts, int nsub, int rk_step, cudaStream_t st);
 
 // moisture (k_moist.cu)
-void launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st);
-void launch_moist(const Grid& g, const S& s, int rk_step, float dt_rk, cudaStream_t st);
-void launch_bdy_final(const Grid& g, const S& s, cudaStream_t st);
+int launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st);
+int launch_moist(const Grid& g, const S& s, int rk_step, float dt_rk, cudaStream_t st);
+int launch_bdy_final(const Grid& g, const S& s, cudaStream_t st);
 
 // microphysics (k_wsm6.cu)
-void launch_physics(const Grid& g, const S& s, cudaStream_t st);
-void launch_wsm6(const Grid& g, float* const* f, float delt, cudaStream_t st);
+int launch_physics(const Grid& g, const S& s, cudaStream_t st);
+int launch_wsm6(const Grid& g, float* const* f, float delt, cudaStream_t st);
 
 }  // namespace wrf

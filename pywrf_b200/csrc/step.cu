@@ -15,6 +15,7 @@ namespace wrf {
 namespace {
 
 thread_local std::string g_err;
+thread_local int g_last_launches = 0;
 
 int fail(int code, const std::string& msg) {
   g_err = msg;
@@ -96,6 +97,7 @@ struct Driver {
   wrf_probe_fn probe;
   void* user;
   int rc = WRF_OK;
+  int n = 0;  // kernels enqueued
 
   size_t b3() const { return g.n3() * sizeof(float); }
   size_t b2() const { return g.n2() * sizeof(float); }
@@ -115,25 +117,26 @@ struct Driver {
   void bc(std::initializer_list<std::pair<int, char>> f3, std::initializer_list<std::pair<int, char>> f2 = {}) {
     BcBatch b;
     for (auto& e : f3) {
-      if (b.n == kBcMax) { launch_bc(g, b, st); b.n = 0; }
+      if (b.n == kBcMax) { n += launch_bc(g, b, st); b.n = 0; }
       b.add(bc_item(g, s[e.first], e.second, false));
     }
     for (auto& e : f2) {
-      if (b.n == kBcMax) { launch_bc(g, b, st); b.n = 0; }
+      if (b.n == kBcMax) { n += launch_bc(g, b, st); b.n = 0; }
       b.add(bc_item(g, s[e.first], e.second, true));
     }
-    launch_bc(g, b, st);
+    n += launch_bc(g, b, st);
   }
   void bc_moist() {
     BcBatch b;
     for (int m = 1; m < 7; ++m) b.add(bc_item(g, s[WF_MOIST] + m * g.n3(), 'p', false));
-    launch_bc(g, b, st);
+    n += launch_bc(g, b, st);
   }
 
   void run() {
     const float dt = g.dt;
     const float dts = (float)(g.dtd / g.soundsteps);
     k_step_begin<<<1, 1, 0, st>>>(s[WF_DSCAL], reinterpret_cast<const int*>(s[WF_STATUS]), bdy_interval, g.dtd);
+    ++n;
     if (!ok("step_begin")) return;
     char tag[32];
     for (int rk = 1; rk <= 3; ++rk) {
@@ -143,7 +146,7 @@ struct Driver {
       else if (rk == 2) { dt_rk = (float)(0.5 * g.dtd); dts_rk = dts; nsub = g.soundsteps / 2; }
       else { dt_rk = dt; dts_rk = dts; nsub = g.soundsteps; }
       // rk_step_prep (solver.py:736-778)
-      launch_prep(g, s, st);
+      n += launch_prep(g, s, st);
       bc({{WF_RU, 'u'}, {WF_RV, 'v'}, {WF_RW, 'w'}, {WF_WW, 'w'}, {WF_PHP, 'w'}, {WF_ALT, 't'}, {WF_P, 'p'},
           {WF_AL, 'p'}, {WF_PH, 'w'}},
          {{WF_MUU, 'u'}, {WF_MUV, 'v'}, {WF_MUT, 't'}});
@@ -154,9 +157,9 @@ struct Driver {
         zero3(WF_RU_TENDF); zero3(WF_RV_TENDF); zero3(WF_RW_TENDF); zero3(WF_PH_TENDF); zero3(WF_T_TENDF);
         zero2(WF_MU_TENDF);
         zero4(WF_MOIST_TEND);
-        launch_diff_metrics(g, s, st);
+        n += launch_diff_metrics(g, s, st);
         bc({{WF_RDZW, 'w'}, {WF_ZX, 'e'}, {WF_ZY, 'f'}});
-        launch_km(g, s, st);
+        n += launch_km(g, s, st);
         bc({{WF_XKMH, 't'}, {WF_XKHH, 't'}});
         snprintf(tag, sizeof tag, "s%d.km", rk);
         phase(tag);
@@ -164,42 +167,42 @@ struct Driver {
       zero3(WF_RU_TEND); zero3(WF_RV_TEND); zero3(WF_RW_TEND); zero3(WF_T_TEND); zero3(WF_PH_TEND);
       zero3(WF_U_SAVE); zero3(WF_V_SAVE); zero3(WF_W_SAVE); zero3(WF_PH_SAVE); zero3(WF_T_SAVE);
       zero2(WF_MU_TEND); zero2(WF_MU_SAVE);
-      launch_advect_forces(g, s, st);
+      n += launch_advect_forces(g, s, st);
       snprintf(tag, sizeof tag, "s%d.forces", rk);
       phase(tag);
       if (rk == 1) {
-        launch_hdiff_relax(g, s, st);
+        n += launch_hdiff_relax(g, s, st);
         snprintf(tag, sizeof tag, "s%d.diff", rk);
         phase(tag);
       }
-      launch_addtend(g, s, rk, st);
+      n += launch_addtend(g, s, rk, st);
       snprintf(tag, sizeof tag, "s%d.tend", rk);
       phase(tag);
       // acoustic set-up (solver.py:1258-1345)
-      launch_small_step_prep(g, s, rk, dts_rk, st);
+      n += launch_small_step_prep(g, s, rk, dts_rk, st);
       bc({{WF_RU_TEND, 'u'}, {WF_RV_TEND, 'v'}, {WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}, {WF_T_1, 't'},
           {WF_T_SAVE, 't'}},
          {{WF_MU_1, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
       snprintf(tag, sizeof tag, "s%d.acprep", rk);
       phase(tag);
       for (int it = 1; it <= nsub; ++it) {
-        launch_substep(g, s, dts_rk, it, nsub, st);
+        n += launch_substep(g, s, dts_rk, it, nsub, st);
         bc({{WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}}, {{WF_MUTS, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
         snprintf(tag, sizeof tag, "s%d.sub%d", rk, it);
         phase(tag);
       }
-      launch_small_step_finish(g, s, dts_rk, nsub, rk, st);
+      n += launch_small_step_finish(g, s, dts_rk, nsub, rk, st);
       if (rk == 3)
         bc({{WF_RU_M, 'u'}, {WF_RV_M, 'v'}, {WF_WW_M, 'w'}}, {{WF_MUT, 't'}, {WF_MUTS, 't'}});
       snprintf(tag, sizeof tag, "s%d.acfinish", rk);
       phase(tag);
       // moisture transport (solver.py:1548-1604)
-      launch_advect_moist(g, s, st);
+      n += launch_advect_moist(g, s, st);
       if (rk == 1) {
-        launch_hdiff_moist(g, s, st);
-        launch_relax_qv(g, s, st);
+        n += launch_hdiff_moist(g, s, st);
+        n += launch_relax_qv(g, s, st);
       }
-      launch_moist(g, s, rk, dt_rk, st);
+      n += launch_moist(g, s, rk, dt_rk, st);
       if (rk < 3) {
         bc({{WF_U, 'U'}, {WF_V, 'V'}, {WF_W, 'w'}, {WF_T, 'p'}, {WF_PH, 'w'}}, {{WF_MU, 't'}});
         bc_moist();
@@ -208,15 +211,16 @@ struct Driver {
       phase(tag);
     }
     // microphysics (solver.py:1714-1766)
-    launch_physics(g, s, st);
+    n += launch_physics(g, s, st);
     phase("mp");
     // end-of-step boundaries (solver.py:1776-1910)
     bc({{WF_U_1, 'U'}, {WF_U, 'U'}, {WF_V_1, 'V'}, {WF_V, 'V'}, {WF_W_1, 'w'}, {WF_W, 'w'}, {WF_T_1, 'p'},
         {WF_T, 'p'}, {WF_PH_1, 'w'}, {WF_PH, 'w'}},
        {{WF_MU_1, 't'}, {WF_MU, 't'}});
     bc_moist();
-    launch_bdy_final(g, s, st);
+    n += launch_bdy_final(g, s, st);
     k_step_end<<<1, 1, 0, st>>>(reinterpret_cast<int*>(s[WF_STATUS]));
+    ++n;
     phase("end");
   }
   int bdy_interval = 360;
@@ -243,6 +247,8 @@ int wrf_field_kind(int id) {
 
 const char* wrf_last_error(void) { return g_err.c_str(); }
 
+int wrf_last_launch_count(void) { return g_last_launches; }
+
 int wrf_rk3_step(const WrfGrid* gin, const WrfState* sin, void* stream, wrf_probe_fn probe, void* user) {
   Driver d;
   int rc = make_grid(gin, d.g);
@@ -255,6 +261,7 @@ int wrf_rk3_step(const WrfGrid* gin, const WrfState* sin, void* stream, wrf_prob
   d.bdy_interval = gin->bdy_interval;
   cudaGetLastError();  // clear a stale error from an unrelated earlier call
   d.run();
+  g_last_launches = d.n;
   return d.rc;
 }
 
