@@ -108,7 +108,7 @@ __global__ void k_eos_flowdep(Grid g, S s, int do_flowdep) {
     s[WF_AL][p] = al;
     const float qvf = 1.0f + (float)RVOVRD * s[WF_MOIST][n3 + p];
     const float temp = ((float)R_D * ((float)T0 + s[WF_T][p]) * qvf) / ((float)P0 * (al + alb));
-    const float pv = powf(temp, (float)CPOVCV) * (float)P0 - s[WF_PB][p];
+    const float pv = wpow_eos(temp, (float)CPOVCV) * (float)P0 - s[WF_PB][p];
     s[WF_P][p] = pv;
     if (isnan(pv)) atomicAdd(reinterpret_cast<int*>(s[WF_STATUS]) + WRF_ST_NAN_P, 1);
   }

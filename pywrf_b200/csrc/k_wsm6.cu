@@ -40,14 +40,14 @@ constexpr double RSLOPER3MAX = 1.9531248e-15;
 struct Slope { float rs[3], rb[3], r2[3], r3[3], vt[3]; };
 
 __device__ __forceinline__ float n0sfac_of(float t) {
-  return fmaxf(fminf(expf(F(mp::ALPHA) * (F(mp::T0C) - t)), F(mp::N0SMAX / mp::N0S)), 1.0f);
+  return fmaxf(fminf(wexp(F(mp::ALPHA) * (F(mp::T0C) - t)), F(mp::N0SMAX / mp::N0S)), 1.0f);
 }
 
 // slope_wsm6 (wrf_physics.py:2048-2104); the rain caps serve all species
 __device__ __forceinline__ void slope_point(float q0, float q1, float q2, float den, float denfac, float t, Slope& o) {
   const float n0 = n0sfac_of(t);
-  const float lam[3] = {powf(F(mp::PIDN0R) / (q0 * den), 0.25f), powf(F(mp::PIDN0S) * n0 / (q1 * den), 0.25f),
-                        powf(F(mp::PIDN0G) / (q2 * den), 0.25f)};
+  const float lam[3] = {wpow(F(mp::PIDN0R) / (q0 * den), 0.25f), wpow(F(mp::PIDN0S) * n0 / (q1 * den), 0.25f),
+                        wpow(F(mp::PIDN0G) / (q2 * den), 0.25f)};
   const float be[3] = {F(mp::BVTR), F(mp::BVTS), F(mp::BVTG)};
   const float pv[3] = {F(mp::PVTR), F(mp::PVTS), F(mp::PVTG)};
   const float qq[3] = {q0, q1, q2};
@@ -56,7 +56,7 @@ __device__ __forceinline__ void slope_point(float q0, float q1, float q2, float 
     const bool small = qq[m] <= F(mp::QCRMIN);
     const float a = small ? F(mp::RSLOPERMAX) : 1.0f / lam[m];
     o.rs[m] = a;
-    o.rb[m] = small ? F(mp::RSLOPERBMAX) : powf(a, be[m]);
+    o.rb[m] = small ? F(mp::RSLOPERBMAX) : wpow(a, be[m]);
     o.r2[m] = small ? F(mp::RSLOPER2MAX) : a * a;
     o.r3[m] = small ? F(mp::RSLOPER3MAX) : a * a * a;
     const float v = pv[m] * o.rb[m] * denfac;
@@ -66,23 +66,23 @@ __device__ __forceinline__ void slope_point(float q0, float q1, float q2, float 
 
 // terminal velocities alone (wrf_physics.py:1988-2046)
 __device__ __forceinline__ float vt_rain(float qr, float den, float denfac) {
-  const float lam = powf(F(mp::PIDN0R) / (qr * den), 0.25f);
+  const float lam = wpow(F(mp::PIDN0R) / (qr * den), 0.25f);
   const float rs = qr <= F(mp::QCRMIN) ? F(mp::RSLOPERMAX) : 1.0f / lam;
-  const float rb = qr <= F(mp::QCRMIN) ? F(mp::RSLOPERBMAX) : powf(rs, F(mp::BVTR));
+  const float rb = qr <= F(mp::QCRMIN) ? F(mp::RSLOPERBMAX) : wpow(rs, F(mp::BVTR));
   const float v = F(mp::PVTR) * rb * denfac;
   return qr <= 0.f ? 0.f : v;
 }
 __device__ __forceinline__ float vt_snow(float qs, float den, float denfac, float t) {
-  const float lam = powf(F(mp::PIDN0S) * n0sfac_of(t) / (qs * den), 0.25f);
+  const float lam = wpow(F(mp::PIDN0S) * n0sfac_of(t) / (qs * den), 0.25f);
   const float rs = qs <= F(mp::QCRMIN) ? F(mp::RSLOPERMAX) : 1.0f / lam;
-  const float rb = qs <= F(mp::QCRMIN) ? F(mp::RSLOPERBMAX) : powf(rs, F(mp::BVTS));
+  const float rb = qs <= F(mp::QCRMIN) ? F(mp::RSLOPERBMAX) : wpow(rs, F(mp::BVTS));
   const float v = F(mp::PVTS) * rb * denfac;
   return qs <= 0.f ? 0.f : v;
 }
 __device__ __forceinline__ float vt_graup(float qg, float den, float denfac) {
-  const float lam = powf(F(mp::PIDN0G) / (qg * den), 0.25f);
+  const float lam = wpow(F(mp::PIDN0G) / (qg * den), 0.25f);
   const float rs = qg <= F(mp::QCRMIN) ? F(mp::RSLOPERMAX) : 1.0f / lam;
-  const float rb = qg <= F(mp::QCRMIN) ? F(mp::RSLOPERBMAX) : powf(rs, F(mp::BVTG));
+  const float rb = qg <= F(mp::QCRMIN) ? F(mp::RSLOPERBMAX) : wpow(rs, F(mp::BVTG));
   const float v = F(mp::PVTG) * rb * denfac;
   return qg <= 0.f ? 0.f : v;
 }
@@ -226,11 +226,11 @@ __device__ __forceinline__ void fpvs(float t, float p, float& qs0, float& qs1) {
   const double dldt = mp::CPV - mp::CLIQ, xa = -dldt / mp::RV, xb = xa + mp::XLV0 / (mp::RV * ttp);
   const double dldti = mp::CPV - mp::CICE, xai = -dldti / mp::RV, xbi = xai + mp::XLS / (mp::RV * ttp);
   const float tr = F(ttp) / t;
-  const float w1 = F(mp::PSAT) * expf(logf(tr) * F(xa)) * expf(F(xb) * (1.0f - tr));
+  const float w1 = F(mp::PSAT) * wexp(wlog(tr) * F(xa)) * wexp(F(xb) * (1.0f - tr));
   float a = fminf(w1, 0.99f * p);
   a = F(mp::EP2) * a / (p - a);
   qs0 = fmaxf(a, F(mp::QMIN));
-  const float w0 = F(mp::PSAT) * expf(logf(tr) * F(xai)) * expf(F(xbi) * (1.0f - tr));
+  const float w0 = F(mp::PSAT) * wexp(wlog(tr) * F(xai)) * wexp(F(xbi) * (1.0f - tr));
   float b = t < F(ttp) ? w0 : w1;
   b = fminf(b, 0.99f * p);
   b = F(mp::EP2) * b / (p - b);
@@ -238,13 +238,13 @@ __device__ __forceinline__ void fpvs(float t, float p, float& qs0, float& qs1) {
 }
 
 __device__ __forceinline__ float viscos(float t, float den) { return 1.496e-6f * (t * sqrtf(t)) / (t + 120.0f) / den; }
-__device__ __forceinline__ float diffus(float t, float p) { return 8.794e-5f * expf(logf(t) * 1.81f) / p; }
+__device__ __forceinline__ float diffus(float t, float p) { return 8.794e-5f * wexp(wlog(t) * 1.81f) / p; }
 __device__ __forceinline__ float xka(float t, float den) { return 1.414e3f * viscos(t, den) * den; }
 __device__ __forceinline__ float diffac(float a, float p, float t, float den, float qs) {
   return den * a * a / (xka(t, den) * F(mp::RV) * t * t) + 1.0f / (qs * diffus(t, p));
 }
 __device__ __forceinline__ float venfac(float p, float t, float den) {
-  return expf(logf(viscos(t, den) / diffus(t, p)) * 0.3333333f) / sqrtf(viscos(t, den)) *
+  return wexp(wlog(viscos(t, den) / diffus(t, p)) * 0.3333333f) / sqrtf(viscos(t, den)) *
          sqrtf(sqrtf(F(mp::DEN0) / den));
 }
 
@@ -272,7 +272,7 @@ __device__ void wsm6_point(float& t, float& q, float& qc0, float& qc1, float& qr
       t = t + xlf3 / cpm * qc0;
       qc0 = 0.f;
     }
-    const float pfrzdtc = fminf(F(mp::PFRZ1) * (expf(F(mp::PFRZ2) * fminf(supcol, 50.0f)) - 1.0f) * den / F(mp::DENR) /
+    const float pfrzdtc = fminf(F(mp::PFRZ1) * (wexp(F(mp::PFRZ2) * fminf(supcol, 50.0f)) - 1.0f) * den / F(mp::DENR) /
                                     F(mp::XNCR) * qc0 * qc0 * dtcld, qc0);
     if (supcol > 0.f && qc0 > F(mp::QMIN)) {
       qc1 = qc1 + pfrzdtc;
@@ -280,7 +280,7 @@ __device__ void wsm6_point(float& t, float& q, float& qc0, float& qc1, float& qr
       qc0 = qc0 - pfrzdtc;
     }
     const float pfrzdtr = fminf(F(20.0 * mp::PI * mp::PI * mp::PFRZ1 * mp::N0R * mp::DENR) / den *
-                                    (expf(F(mp::PFRZ2) * fminf(supcol, 50.0f)) - 1.0f) * r30pre * r30pre * rs0pre * dtcld, qr0);
+                                    (wexp(F(mp::PFRZ2) * fminf(supcol, 50.0f)) - 1.0f) * r30pre * r30pre * rs0pre * dtcld, qr0);
     if (supcol > 0.f && qr0 > 0.f) {
       qr2 = qr2 + pfrzdtr;
       t = t + xlf3 / cpm * pfrzdtr;
@@ -293,7 +293,7 @@ __device__ void wsm6_point(float& t, float& q, float& qc0, float& qc1, float& qr
   const float work1_1 = diffac(F(mp::XLS), p, t, den, qs1);
   float work2 = venfac(p, t, den);
   float supsat = fmaxf(q, F(mp::QMIN)) - qs0;
-  float praut = F(mp::QCK1) * powf(qc0, F(7.0 / 3.0));
+  float praut = F(mp::QCK1) * wpow(qc0, F(7.0 / 3.0));
   praut = qc0 > F(mp::QC0) ? fminf(praut, qc0 / dtcld) : 0.f;
   float pracw = (qr0 > F(mp::QCRMIN) && qc0 > F(mp::QMIN))
                     ? fminf(F(mp::PACRR) * sl.r3[0] * sl.rb[0] * qc0 * denfac, qc0 / dtcld) : 0.f;
@@ -310,15 +310,15 @@ __device__ void wsm6_point(float& t, float& q, float& qc0, float& qc1, float& qr
     if (c3) prevp = fminf(prevp, supsat / dtcld / 2.0f);
   }
   supcol = t0c - t;
-  const float n0sfac = fmaxf(fminf(expf(F(mp::ALPHA) * supcol), F(mp::N0SMAX / mp::N0S)), 1.0f);
+  const float n0sfac = fmaxf(fminf(wexp(F(mp::ALPHA) * supcol), F(mp::N0SMAX / mp::N0S)), 1.0f);
   supsat = fmaxf(q, F(mp::QMIN)) - qs1;
   const float satdt = supsat / dtcld;
   bool ifsat = false;
-  const float xni = fminf(fmaxf(5.38e7f * powf(den * fmaxf(qc1, F(mp::QMIN)), 0.75f), 1.0e3f), 1.0e6f);
-  const float eacrs = expf(0.07f * (-supcol));
+  const float xni = fminf(fmaxf(5.38e7f * wpow(den * fmaxf(qc1, F(mp::QMIN)), 0.75f), 1.0e3f), 1.0e6f);
+  const float eacrs = wexp(0.07f * (-supcol));
   const float xmi = den * qc1 / xni;
   const float diameter = fminf(F(mp::DICON) * sqrtf(xmi), F(mp::DIMAX));
-  const float vt2i = 1.49e4f * powf(diameter, 1.31f);
+  const float vt2i = 1.49e4f * wpow(diameter, 1.31f);
   const float vt2r = F(mp::PVTR) * sl.rb[0] * denfac;
   const float vt2s = F(mp::PVTS) * sl.rb[1] * denfac;
   const float vt2g = F(mp::PVTG) * sl.rb[2] * denfac;
@@ -339,7 +339,7 @@ __device__ void wsm6_point(float& t, float& q, float& qc0, float& qc1, float& qr
     psaci = fminf(pi_ * qc1 * eacrs * F(mp::N0S) * n0sfac * fabsf(vt2ave - vt2i) * acrfac / 4.0f, qc1 / dtcld);
   }
   if (qr2 > F(mp::QCRMIN) && cnd) {
-    const float egi = expf(-0.07f * supcol);
+    const float egi = wexp(-0.07f * supcol);
     const float acrfac = 2.0f * sl.r3[2] + 2.0f * diameter * sl.r2[2] + diameter * diameter * sl.rs[2];
     pgaci = fminf(pi_ * egi * qc1 * F(mp::N0G) * fabsf(vt2ave - vt2i) * acrfac / 4.0f, qc1 / dtcld);
   }
@@ -414,12 +414,12 @@ __device__ void wsm6_point(float& t, float& q, float& qc0, float& qc1, float& qr
   }
   if (supsat > 0.f && !ifsat && cold) {
     const float supice = satdt - prevp - pidep - psdep - pgdep;
-    const float roqi0 = 4.92e-11f * powf(1.0e3f * expf(0.1f * supcol), 1.33f);
+    const float roqi0 = 4.92e-11f * wpow(1.0e3f * wexp(0.1f * supcol), 1.33f);
     pigen = fmaxf(0.0f, (roqi0 / den - fmaxf(qc1, 0.0f)) / dtcld);
     pigen = fminf(fminf(pigen, satdt), supice);
   }
   if (qc1 > 0.f && cold) psaut = fmaxf(0.0f, (qc1 - F(mp::ROQIMAX) / den) / dtcld);
-  if (qr1 > 0.f && cold) pgaut = fminf(fmaxf(0.0f, 1.0e-3f * expf(-0.09f * supcol) * (qr1 - F(mp::QS0))), qr1 / dtcld);
+  if (qr1 > 0.f && cold) pgaut = fminf(fmaxf(0.0f, 1.0e-3f * wexp(-0.09f * supcol) * (qr1 - F(mp::QS0))), qr1 / dtcld);
   float psevp = 0.f, pgevp = 0.f;
   if (supcol < 0.f && rh0 < 1.0f) {
     if (qr1 > 0.f) {
@@ -600,9 +600,9 @@ __device__ void wsm6_column(Column& c, int km, float delt, Precip& pr) {
       c.t[k] = t;
       // cloud-ice fall speed (ice number from the loop-start ice)
       const float qi = c.qc1[k];
-      const float xni = fminf(fmaxf(5.387e7f * powf(den * fmaxf(qi, F(mp::QMIN)), 0.75f), 1.0e3f), 1.0e6f);
+      const float xni = fminf(fmaxf(5.387e7f * wpow(den * fmaxf(qi, F(mp::QMIN)), 0.75f), 1.0e3f), 1.0e6f);
       float wt = fmaxf(fminf(F(mp::DICON) * sqrtf(den * qi / xni), F(mp::DIMAX)), 1.0e-25f);
-      wt = 1.49e4f * expf(logf(wt) * 1.31f);
+      wt = 1.49e4f * wexp(wlog(wt) * 1.31f);
       c.ww[k] = qi <= 0.f ? 0.f : wt;
       c.rq[k] = den * qi;
     }
@@ -642,7 +642,7 @@ __device__ __forceinline__ void eos_point(const Grid& g, const S& s, int k, size
   s[WF_AL][p] = al;
   const float qvf = 1.0f + (float)RVOVRD * s[WF_MOIST][n3 + p];
   const float temp = ((float)R_D * ((float)T0 + s[WF_T][p]) * qvf) / ((float)P0 * (al + alb));
-  s[WF_P][p] = powf(temp, (float)CPOVCV) * (float)P0 - s[WF_PB][p];
+  s[WF_P][p] = wpow_eos(temp, (float)CPOVCV) * (float)P0 - s[WF_PB][p];
 }
 
 // moist_physics_prep_em + wsm6 + moist_physics_finish_em + calc_p_rho_phi
@@ -664,7 +664,7 @@ __global__ void __launch_bounds__(128) k_physics(Grid g, S s, float dt) {
       const size_t p = k * lev + c2;
       const float th = T[p] + (float)T0;
       const float pfull = s[WF_P][p] + s[WF_PB][p];
-      const float pii = powf(pfull / (float)P0, F(mp::RCP));
+      const float pii = wpow(pfull / (float)P0, F(mp::RCP));
       c.t[k] = th * pii;
       c.den[k] = 1.0f / (s[WF_AL][p] + s[WF_ALB][p]);
       c.p[k] = pfull;
@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(128) k_physics(Grid g, S s, float dt) {
     for (int k = 0; k < km; ++k) {
       const size_t p = k * lev + c2;
       const float thold = T[p] + (float)T0;
-      const float pii = powf((s[WF_P][p] + s[WF_PB][p]) / (float)P0, F(mp::RCP));
+      const float pii = wpow((s[WF_P][p] + s[WF_PB][p]) / (float)P0, F(mp::RCP));
       const float mpten = c.t[k] / pii - thold;
       T[p] = T[p] + mpten;
       s[WF_H_DIABATIC][p] = mpten / dt;

@@ -53,6 +53,24 @@ struct S {
 
 __device__ __forceinline__ float ldg(const float* p) { return __ldg(p); }
 
+// Transcendentals of the equation of state (wpow_eos) and of the
+// microphysics (wpow, wexp, wlog).  With WRF_EOS_DOUBLE / WRF_MP_DOUBLE they
+// are evaluated in double precision and rounded once to float.
+#ifdef WRF_EOS_DOUBLE
+__device__ __forceinline__ float wpow_eos(float a, float b) { return (float)pow((double)a, (double)b); }
+#else
+__device__ __forceinline__ float wpow_eos(float a, float b) { return powf(a, b); }
+#endif
+#ifdef WRF_MP_DOUBLE
+__device__ __forceinline__ float wpow(float a, float b) { return (float)pow((double)a, (double)b); }
+__device__ __forceinline__ float wexp(float a) { return (float)exp((double)a); }
+__device__ __forceinline__ float wlog(float a) { return (float)log((double)a); }
+#else
+__device__ __forceinline__ float wpow(float a, float b) { return powf(a, b); }
+__device__ __forceinline__ float wexp(float a) { return expf(a); }
+__device__ __forceinline__ float wlog(float a) { return logf(a); }
+#endif
+
 // 1.0 if ua >= 0 else -1.0 (fortran_sign(1., ua), wrf_dynamics.py:1309-1311)
 __device__ __forceinline__ float sgnf(float ua) { return ua >= 0.f ? 1.f : -1.f; }
 
