@@ -57,7 +57,7 @@ extern "C" {
   X(U_1, WRF_K3) X(V_1, WRF_K3) X(W_1, WRF_K3) X(T_1, WRF_K3) X(PH_1, WRF_K3) X(C2A, WRF_K3) \
   X(PM1, WRF_K3) X(A, WRF_K3) X(ALPHA, WRF_K3) X(GAMMA, WRF_K3) X(RU_M, WRF_K3) X(RV_M, WRF_K3) \
   X(WW_M, WRF_K3) X(T_2SAVE, WRF_K3) X(H_DIABATIC, WRF_K3) X(QV_DIABATIC, WRF_K3) \
-  X(QC_DIABATIC, WRF_K3) \
+  X(QC_DIABATIC, WRF_K3) X(WSM_T, WRF_K3) X(WSM_QR0S, WRF_K3) \
   X(MU, WRF_K2) X(MUB, WRF_K2) X(MSFU, WRF_K2) X(MSFV, WRF_K2) X(MSFVX_INV, WRF_K2) \
   X(MSFT, WRF_K2) X(MSFTX, WRF_K2) X(MSFTY, WRF_K2) X(MSFUX, WRF_K2) X(MSFUY, WRF_K2) \
   X(MSFVX, WRF_K2) X(MSFVY, WRF_K2) X(F, WRF_K2) X(E, WRF_K2) X(SINA, WRF_K2) X(COSA, WRF_K2) \

@@ -1,12 +1,12 @@
 // WSM6 single-moment 6-class microphysics and the moist-physics wrappers.
 //
-// k_physics runs one thread per (j, i) column of [jds, jde-1) x [ids, ide-1)
-// and fuses, column by column:
+// k_physics gives each (j, i) column of [jds, jde-1) x [ids, ide-1) to a
+// segment of lanes (one level per lane and slot) and fuses, column by column:
 //   moist_physics_prep_em   (wrf_physics.py:27-91, columns [ids+1, ide-1))
 //   wsm6                    (wrf_physics.py:137-1214, columns [ids+1, ide-2))
 //   moist_physics_finish_em (wrf_physics.py:2106-2137)
 //   calc_p_rho_phi          (wrf_dynamics.py:4124-4164, every column)
-// so theta, density, Exner function and layer depths never leave the SM.
+// so theta, density, Exner function and layer depths stay in registers.
 // Sedimentation follows nislfv_rain_plm / _plm6 (wrf_physics.py:1216-1583):
 // 3rd-order interface fall speeds with the CFL limiter, departure cells,
 // piecewise-constant overlap remap (the top cell 3800 m deep, the top
@@ -85,138 +85,6 @@ __device__ __forceinline__ float vt_graup(float qg, float den, float denfac) {
   const float rb = qg <= F(mp::QCRMIN) ? F(mp::RSLOPERBMAX) : wpow(rs, F(mp::BVTG));
   const float v = F(mp::PVTG) * rb * denfac;
   return qg <= 0.f ? 0.f : v;
-}
-
-// per-column working storage (thread-local; km <= kMaxNz levels)
-struct Column {
-  float t[kMaxNz], q[kMaxNz], qc0[kMaxNz], qc1[kMaxNz], qr0[kMaxNz], qr1[kMaxNz], qr2[kMaxNz];
-  float den[kMaxNz], p[kMaxNz], delz[kMaxNz];
-  float denfac[kMaxNz], cpm[kMaxNz], xl[kMaxNz], qs0[kMaxNz], qs1[kMaxNz];
-  float rs0[kMaxNz], r30[kMaxNz];          // rain slope after sedimentation (rain freezing)
-  float ww[kMaxNz], ww2[kMaxNz], rq[kMaxNz], rq2[kMaxNz], rq3[kMaxNz];
-  // sedimentation scratch
-  float zi[kMaxNz + 1], wi[kMaxNz + 1], za[kMaxNz + 1], dza[kMaxNz + 1];
-  float qa[kMaxNz + 1], qa2[kMaxNz + 1], www[kMaxNz], qn[kMaxNz];
-};
-
-// interface fall speeds (wrf_physics.py:1269-1293)
-__device__ void fall_interfaces(const float* ww, const float* dz, int km, float dt, float* wi) {
-  const float fa1 = 9.0f / 16.0f, fa2 = 1.0f / 16.0f;
-  wi[0] = ww[0];
-  wi[1] = 0.5f * (ww[1] + ww[0]);
-  for (int k = 2; k < km - 1; ++k) wi[k] = fa1 * (ww[k] + ww[k - 1]) - fa2 * (ww[k + 1] + ww[k - 2]);
-  wi[km - 1] = 0.5f * (ww[km - 1] + ww[km - 2]);
-  wi[km] = ww[km - 1];
-  for (int k = 1; k < km; ++k)
-    if (ww[k] == 0.0f) wi[k] = ww[k - 1];
-  for (int k = km - 1; k >= 0; --k) {
-    const float decfl = (wi[k + 1] - wi[k]) * dt / dz[k];
-    if (decfl > 0.05f) wi[k] = wi[k + 1] - 0.05f * dz[k] / dt;
-  }
-}
-
-// overlap remap (wrf_physics.py:1339-1357): qn[k] = sum_ka qa[ka] * overlap / dz[k],
-// summed in ka order
-__device__ void remap(const float* qa, const float* zi, const float* za, const float* dz, int km, float* qn) {
-  for (int k = 0; k < km; ++k) {
-    const float lo = zi[k];
-    const float hi = (k < km - 1) ? zi[k + 1] : zi[km - 1] + 3800.0f;
-    float acc = 0.f;
-    for (int ka = 0; ka < km; ++ka) {
-      const float alo = za[ka];
-      const float ahi = (ka < km - 1) ? za[ka + 1] : za[km - 1] + 3800.0f;
-      const float ov = fmaxf(0.0f, fminf(hi, ahi) - fmaxf(lo, alo));
-      acc = acc + qa[ka] * ov;
-    }
-    qn[k] = acc / dz[k];
-  }
-}
-
-// mass that left through the ground (wrf_physics.py:1361-1374)
-__device__ float surface_flux(const float* qa, const float* za, const float* dza, int km) {
-  float precip = 0.f;
-  for (int k = 0; k < km; ++k) {
-    if (za[k] < 0.f && za[k + 1] < 0.f) precip = precip + qa[k] * dza[k];
-    if (za[k] < 0.f && za[k + 1] > 0.f) precip = precip + qa[k] * (0.0f - za[k]);
-  }
-  return precip;
-}
-
-__device__ void departure(Column& c, int km, float dt) {
-  fall_interfaces(c.www, c.delz, km, dt, c.wi);
-  for (int k = 0; k <= km; ++k) c.za[k] = c.zi[k] - c.wi[k] * dt;
-  for (int k = 0; k < km; ++k) c.dza[k] = c.za[k + 1] - c.za[k];
-  c.dza[km] = c.zi[km] - c.za[km];
-}
-
-// nislfv_rain_plm (wrf_physics.py:1216-1381) on rq with fall speed ww;
-// iter 1 re-estimates the fall speed once from the departure cells
-__device__ float nislfv_plm(Column& c, const float* ww, float* rq, int km, float dt, int iter) {
-  float allold = 0.f;
-  for (int k = 0; k < km; ++k) allold = allold + rq[k];
-  c.zi[0] = 0.f;
-  for (int k = 0; k < km; ++k) c.zi[k + 1] = c.zi[k] + c.delz[k];
-  for (int k = 0; k < km; ++k) c.www[k] = ww[k];
-  const int npass = iter >= 1 ? 2 : 1;
-  for (int n = 1; n <= npass; ++n) {
-    departure(c, km, dt);
-    for (int k = 0; k < km; ++k) c.qa[k] = rq[k] * c.delz[k] / c.dza[k];
-    c.qa[km] = 0.f;
-    if (n <= iter) {
-      for (int k = 0; k < km; ++k) {
-        const float qr = c.qa[k] / c.den[k];
-        c.www[k] = 0.5f * (ww[k] + vt_rain(qr, c.den[k], c.denfac[k]));
-      }
-    }
-  }
-  c.qa[km - 1] = 0.f;
-  remap(c.qa, c.zi, c.za, c.delz, km, c.qn);
-  const float precip = surface_flux(c.qa, c.za, c.dza, km);
-  const bool ok = allold > 0.f;
-  for (int k = 0; k < km; ++k) rq[k] = ok ? c.qn[k] : 0.f;
-  return ok ? precip : 0.f;
-}
-
-// nislfv_rain_plm6 (wrf_physics.py:1383-1583): snow and graupel move with the
-// shared mass-weighted fall speed, then each is remapped separately
-__device__ void nislfv_plm6(Column& c, const float* ww, float* rq, float* rq2, int km, float dt, int iter,
-                            float* p1, float* p2) {
-  float allold = 0.f, a2 = 0.f;
-  for (int k = 0; k < km; ++k) allold = allold + rq[k];
-  for (int k = 0; k < km; ++k) a2 = a2 + rq2[k];
-  allold = allold + a2;
-  c.zi[0] = 0.f;
-  for (int k = 0; k < km; ++k) c.zi[k + 1] = c.zi[k] + c.delz[k];
-  for (int k = 0; k < km; ++k) c.www[k] = ww[k];
-  const int npass = iter >= 1 ? 2 : 1;
-  for (int n = 1; n <= npass; ++n) {
-    departure(c, km, dt);
-    for (int k = 0; k < km; ++k) {
-      c.qa[k] = rq[k] * c.delz[k] / c.dza[k];
-      c.qa2[k] = rq2[k] * c.delz[k] / c.dza[k];
-    }
-    c.qa[km] = 0.f;
-    c.qa2[km] = 0.f;
-    if (n <= iter) {
-      for (int k = 0; k < km; ++k) {
-        const float qr = c.qa[k] / c.den[k], qr2 = c.qa2[k] / c.den[k];
-        float wa = vt_snow(qr, c.den[k], c.denfac[k], c.t[k]);
-        const float wa2 = vt_graup(qr2, c.den[k], c.denfac[k]);
-        const float tmp = fmaxf(qr + qr2, 1.0e-15f);
-        wa = tmp > 1.0e-15f ? (wa * qr + wa2 * qr2) / tmp : 0.f;
-        c.www[k] = 0.5f * (ww[k] + wa);
-      }
-    }
-  }
-  const bool ok = allold > 0.f;
-  c.qa[km - 1] = 0.f;
-  remap(c.qa, c.zi, c.za, c.delz, km, c.qn);
-  *p1 = ok ? surface_flux(c.qa, c.za, c.dza, km) : 0.f;
-  for (int k = 0; k < km; ++k) rq[k] = ok ? c.qn[k] : 0.f;
-  c.qa2[km - 1] = 0.f;
-  remap(c.qa2, c.zi, c.za, c.delz, km, c.qn);
-  *p2 = ok ? surface_flux(c.qa2, c.za, c.dza, km) : 0.f;
-  for (int k = 0; k < km; ++k) rq2[k] = ok ? c.qn[k] : 0.f;
 }
 
 // saturation mixing ratios over water and (below the triple point) ice
@@ -524,21 +392,320 @@ __device__ void wsm6_point(float& t, float& q, float& qc0, float& qc1, float& qr
 
 // precipitation accumulators of one column
 struct Precip { float rain, rainncv, snow, snowncv, graupel, graupelncv, sr; };
+// ------------------------------------------------------- warp-segment columns
+//
+// A segment of SEG lanes owns one column; lane l holds levels k = s*SEG + l
+// (s < NS) in registers.  Point processes run on all levels at once; the
+// column-coupled steps of the sedimentation (interface fall speeds, the CFL
+// limiter, the overlap remap, the surface flux) use shuffles inside the
+// segment and a small per-segment shared-memory scratch.  Results equal the
+// reference's sequential sweeps: sums keep their order (terms that are exactly
+// zero are skipped), and the backward CFL recursion is replayed exactly on the
+// levels where it can act.
+//
+// Every function below that shuffles, ballots or syncs (shift, the *_w
+// sedimentation steps, surface_flux_w, wsm6_column_w) must be reached by all
+// 32 lanes of the warp: segments of one warp belong to different columns, so
+// no call may sit under a per-segment condition.
 
-// WSM6 on a loaded column (c.t temperature, c.q .. c.qr2, c.den, c.p, c.delz)
-// (wrf_physics.py:137-1214)
-__device__ void wsm6_column(Column& c, int km, float delt, Precip& pr) {
-  const float t0c = F(mp::T0C);
-  for (int k = 0; k < km; ++k) {
-    c.qc0[k] = fmaxf(c.qc0[k], 0.0f);
-    c.qc1[k] = fmaxf(c.qc1[k], 0.0f);
-    c.qr0[k] = fmaxf(c.qr0[k], 0.0f);
-    c.qr1[k] = fmaxf(c.qr1[k], 0.0f);
-    c.qr2[k] = fmaxf(c.qr2[k], 0.0f);
-    c.cpm[k] = c.q[k] >= F(mp::QMIN) ? F(mp::CPV) * c.q[k] + (1.0f - c.q[k]) * F(mp::CPD)
-                                     : F(mp::CPD * (1.0 - mp::QMIN) + mp::CPV * mp::QMIN);
-    c.xl[k] = F(mp::XLV0) - F(mp::XLV1) * (c.t[k] - t0c);
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int SEG, int NS>
+struct Seg {
+  int l;     // lane within the segment
+  int base;  // first lane of the segment within the warp
+  int km;    // mass levels
+  __device__ __forceinline__ int k(int s) const { return s * SEG + l; }
+  __device__ __forceinline__ unsigned bits(unsigned ballot) const {
+    return SEG == 32 ? ballot : ((ballot >> base) & ((1u << (SEG & 31)) - 1u));
   }
+};
+
+template <int SEG, int NS>
+struct SegScratch {
+  float dz[NS * SEG + 1], zi[NS * SEG + 1], wi[NS * SEG + 1], za[NS * SEG + 1], qa[NS * SEG + 1],
+      qa2[NS * SEG + 1];
+};
+
+template <int NS>
+__device__ __forceinline__ float pick(const float (&v)[NS], int s) {
+  float r = v[0];
+#pragma unroll
+  for (int i = 1; i < NS; ++i)
+    if (s == i) r = v[i];
+  return r;
+}
+
+// out[s] = value at level k(s) + d (unspecified outside [0, NS*SEG))
+template <int SEG, int NS>
+__device__ __forceinline__ void shift(const float (&v)[NS], int d, int l, float (&out)[NS]) {
+  const int src = l + d;
+  const int sl = src & (SEG - 1);
+  float a[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) a[s] = __shfl_sync(kFull, v[s], sl, SEG);
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    float r = a[s];
+    if (src < 0 && s > 0) r = a[s > 0 ? s - 1 : 0];
+    if (src >= SEG && s < NS - 1) r = a[s < NS - 1 ? s + 1 : s];
+    out[s] = r;
+  }
+}
+
+// interface fall speeds into sc.wi[0..km] (wrf_physics.py:1269-1293)
+template <int SEG, int NS>
+__device__ void fall_interfaces_w(const Seg<SEG, NS>& g, const float (&ww)[NS], const float (&dz)[NS], float dt,
+                                  SegScratch<SEG, NS>& sc) {
+  const int km = g.km;
+  const float fa1 = 9.0f / 16.0f, fa2 = 1.0f / 16.0f;
+  float wm1[NS], wp1[NS], wm2[NS];
+  shift<SEG, NS>(ww, -1, g.l, wm1);
+  shift<SEG, NS>(ww, 1, g.l, wp1);
+  shift<SEG, NS>(ww, -2, g.l, wm2);
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int k = g.k(s);
+    if (k > km) continue;
+    float w;
+    if (k == 0) w = ww[s];
+    else if (k == 1) w = 0.5f * (ww[s] + wm1[s]);
+    else if (k == km) w = wm1[s];
+    else if (k == km - 1) w = 0.5f * (ww[s] + wm1[s]);
+    else w = fa1 * (ww[s] + wm1[s]) - fa2 * (wp1[s] + wm2[s]);
+    if (k >= 1 && k < km && ww[s] == 0.0f) w = wm1[s];
+    sc.wi[k] = w;
+  }
+  __syncwarp();
+  // backward CFL limiter: flags computed with the unmodified upper neighbour;
+  // the sequential replay visits flagged levels and every level below a
+  // modified one, which is where the sequential sweep can act
+  unsigned long long mask = 0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int k = g.k(s);
+    bool f = false;
+    if (k < km) f = (sc.wi[k + 1] - sc.wi[k]) * dt / dz[s] > 0.05f;
+    mask |= (unsigned long long)g.bits(__ballot_sync(kFull, f)) << (s * SEG);
+  }
+  __syncwarp();
+  if (g.l == 0 && mask) {
+    int k = 63 - __clzll((long long)mask);
+    while (true) {
+      const float a = sc.wi[k + 1], b = sc.wi[k], dzk = sc.dz[k];
+      bool modified = false;
+      if ((a - b) * dt / dzk > 0.05f) {
+        sc.wi[k] = a - 0.05f * dzk / dt;
+        modified = true;
+      }
+      if (k == 0) break;
+      if (modified) {
+        --k;
+        continue;
+      }
+      const unsigned long long below = mask & ((1ull << k) - 1ull);
+      if (!below) break;
+      k = 63 - __clzll((long long)below);
+    }
+  }
+  __syncwarp();
+}
+
+// departure points sc.za[0..km] and the departure-cell depths of my levels
+template <int SEG, int NS>
+__device__ __forceinline__ void departure_w(const Seg<SEG, NS>& g, float dt, SegScratch<SEG, NS>& sc, float (&dza)[NS]) {
+  const int km = g.km;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int k = g.k(s);
+    if (k <= km) sc.za[k] = sc.zi[k] - sc.wi[k] * dt;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int k = g.k(s);
+    dza[s] = k < km ? sc.za[k + 1] - sc.za[k] : 1.0f;
+  }
+}
+
+// overlap remap of qa (scratch) onto my levels (wrf_physics.py:1339-1357)
+template <int SEG, int NS>
+__device__ __forceinline__ void remap_w(const Seg<SEG, NS>& g, const float* qa, const SegScratch<SEG, NS>& sc,
+                                        const float (&dz)[NS], float (&qn)[NS]) {
+  const int km = g.km;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int k = g.k(s);
+    qn[s] = 0.f;
+    if (k >= km) continue;
+    const float lo = sc.zi[k];
+    const float hi = (k < km - 1) ? sc.zi[k + 1] : sc.zi[km - 1] + 3800.0f;
+    // first departure cell reaching above lo: mass falls, so it is normally
+    // cell k itself; walk down while the cell below still overlaps (the tops
+    // za_hi are ordered, so every cell below the start has zero overlap)
+    int ka0 = k;
+    while (ka0 > 0 && sc.za[ka0] > lo) --ka0;
+    float acc = 0.f;
+    for (int ka = ka0; ka < km; ++ka) {
+      const float alo = sc.za[ka];
+      if (alo >= hi) break;  // departure cells are ordered: no later overlap
+      const float ahi = (ka < km - 1) ? sc.za[ka + 1] : sc.za[km - 1] + 3800.0f;
+      const float ov = fmaxf(0.0f, fminf(hi, ahi) - fmaxf(lo, alo));
+      acc = acc + qa[ka] * ov;
+    }
+    qn[s] = acc / dz[s];
+  }
+}
+
+// mass through the ground (wrf_physics.py:1361-1374), summed in level order
+template <int SEG, int NS>
+__device__ __forceinline__ float surface_flux_w(const Seg<SEG, NS>& g, const float* qa, const SegScratch<SEG, NS>& sc) {
+  float precip = 0.f;
+  if (g.l == 0) {
+    for (int k = 0; k < g.km; ++k) {
+      const float a = sc.za[k], b = sc.za[k + 1];
+      if (!(a < 0.f)) break;  // ordered departure points: no later crossing
+      if (b < 0.f) precip = precip + qa[k] * (b - a);
+      if (b > 0.f) precip = precip + qa[k] * (0.0f - a);
+    }
+  }
+  return __shfl_sync(kFull, precip, 0, SEG);
+}
+
+// nislfv_rain_plm (wrf_physics.py:1216-1381): rq in place, returns precip
+template <int SEG, int NS>
+__device__ float nislfv_w(const Seg<SEG, NS>& g, const float (&den)[NS], const float (&denfac)[NS],
+                          const float (&dz)[NS], const float (&ww0)[NS], float (&rq)[NS], float dt, int iter,
+                          SegScratch<SEG, NS>& sc) {
+  const int km = g.km;
+  bool any = false;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) any |= (g.k(s) < km && rq[s] > 0.f);
+  const bool ok = g.bits(__ballot_sync(kFull, any)) != 0u;
+  float www[NS], dza[NS], qa[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) www[s] = ww0[s];
+  const int npass = iter >= 1 ? 2 : 1;
+  for (int n = 1; n <= npass; ++n) {
+    fall_interfaces_w<SEG, NS>(g, www, dz, dt, sc);
+    departure_w<SEG, NS>(g, dt, sc, dza);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      qa[s] = rq[s] * dz[s] / dza[s];
+      if (n <= iter && g.k(s) < km) www[s] = 0.5f * (ww0[s] + vt_rain(qa[s] / den[s], den[s], denfac[s]));
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int k = g.k(s);
+    if (k < km) sc.qa[k] = (k == km - 1) ? 0.f : qa[s];
+  }
+  __syncwarp();
+  float qn[NS];
+  remap_w<SEG, NS>(g, sc.qa, sc, dz, qn);
+  const float precip = surface_flux_w<SEG, NS>(g, sc.qa, sc);
+#pragma unroll
+  for (int s = 0; s < NS; ++s) rq[s] = ok ? qn[s] : 0.f;
+  __syncwarp();
+  return ok ? precip : 0.f;
+}
+
+// nislfv_rain_plm6 (wrf_physics.py:1383-1583): snow (rq) and graupel (rq2)
+template <int SEG, int NS>
+__device__ void nislfv6_w(const Seg<SEG, NS>& g, const float (&den)[NS], const float (&denfac)[NS],
+                          const float (&tk)[NS], const float (&dz)[NS], const float (&ww0)[NS], float (&rq)[NS],
+                          float (&rq2)[NS], float dt, int iter, SegScratch<SEG, NS>& sc, float* p1, float* p2) {
+  const int km = g.km;
+  bool any = false;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) any |= (g.k(s) < km && (rq[s] > 0.f || rq2[s] > 0.f));
+  const bool ok = g.bits(__ballot_sync(kFull, any)) != 0u;
+  float www[NS], dza[NS], qa[NS], qa2[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) www[s] = ww0[s];
+  const int npass = iter >= 1 ? 2 : 1;
+  for (int n = 1; n <= npass; ++n) {
+    fall_interfaces_w<SEG, NS>(g, www, dz, dt, sc);
+    departure_w<SEG, NS>(g, dt, sc, dza);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      qa[s] = rq[s] * dz[s] / dza[s];
+      qa2[s] = rq2[s] * dz[s] / dza[s];
+      if (n <= iter && g.k(s) < km) {
+        const float qr = qa[s] / den[s], qr2 = qa2[s] / den[s];
+        float wa = vt_snow(qr, den[s], denfac[s], tk[s]);
+        const float wa2 = vt_graup(qr2, den[s], denfac[s]);
+        const float tmp = fmaxf(qr + qr2, 1.0e-15f);
+        wa = tmp > 1.0e-15f ? (wa * qr + wa2 * qr2) / tmp : 0.f;
+        www[s] = 0.5f * (ww0[s] + wa);
+      }
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int k = g.k(s);
+    if (k < km) {
+      sc.qa[k] = (k == km - 1) ? 0.f : qa[s];
+      sc.qa2[k] = (k == km - 1) ? 0.f : qa2[s];
+    }
+  }
+  __syncwarp();
+  float qn[NS];
+  remap_w<SEG, NS>(g, sc.qa, sc, dz, qn);
+  const float f1 = surface_flux_w<SEG, NS>(g, sc.qa, sc);  // all lanes: it shuffles
+  *p1 = ok ? f1 : 0.f;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) rq[s] = ok ? qn[s] : 0.f;
+  remap_w<SEG, NS>(g, sc.qa2, sc, dz, qn);
+  const float f2 = surface_flux_w<SEG, NS>(g, sc.qa2, sc);  // all lanes: it shuffles
+  *p2 = ok ? f2 : 0.f;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) rq2[s] = ok ? qn[s] : 0.f;
+  __syncwarp();
+}
+
+// the column state a segment carries through the scheme
+template <int NS>
+struct WCol {
+  float t[NS], q[NS], qc0[NS], qc1[NS], qr0[NS], qr1[NS], qr2[NS], den[NS], p[NS], delz[NS];
+};
+
+// WSM6 on one loaded column (wrf_physics.py:137-1214).  With kPoint false
+// the column stops after the sedimentation, melting and ice fall of a single
+// time-split loop and hands back the rain left by the sedimentation (qr0s),
+// from which k_wsm6_finish recomputes the rain slope for the point processes.
+template <int SEG, int NS, bool kPoint>
+__device__ void wsm6_column_w(const Seg<SEG, NS>& g, WCol<NS>& c, float delt, Precip& pr, SegScratch<SEG, NS>& sc,
+                              float (&qr0s)[NS]) {
+  const int km = g.km;
+  const float t0c = F(mp::T0C);
+  float cpm[NS], xl[NS], denfac[NS], qs0[NS], qs1[NS], rs0[NS], r30[NS], ww[NS], ww2[NS], rq[NS], rq2[NS], rq3[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    c.qc0[s] = fmaxf(c.qc0[s], 0.0f);
+    c.qc1[s] = fmaxf(c.qc1[s], 0.0f);
+    c.qr0[s] = fmaxf(c.qr0[s], 0.0f);
+    c.qr1[s] = fmaxf(c.qr1[s], 0.0f);
+    c.qr2[s] = fmaxf(c.qr2[s], 0.0f);
+    cpm[s] = c.q[s] >= F(mp::QMIN) ? F(mp::CPV) * c.q[s] + (1.0f - c.q[s]) * F(mp::CPD)
+                                   : F(mp::CPD * (1.0 - mp::QMIN) + mp::CPV * mp::QMIN);
+    xl[s] = F(mp::XLV0) - F(mp::XLV1) * (c.t[s] - t0c);
+    const int k = g.k(s);
+    if (k < km) sc.dz[k] = c.delz[s];
+  }
+  __syncwarp();
+  if (g.l == 0) {
+    float z = 0.f;
+    sc.zi[0] = z;
+    for (int k = 0; k < km; ++k) {
+      z = z + sc.dz[k];
+      sc.zi[k + 1] = z;
+    }
+  }
+  __syncwarp();
+  const float dz0 = __shfl_sync(kFull, c.delz[0], 0, SEG);
   pr.rainncv = 0.f;
   pr.snowncv = 0.f;
   pr.graupelncv = 0.f;
@@ -547,72 +714,74 @@ __device__ void wsm6_column(Column& c, int km, float delt, Precip& pr) {
   const float dtcld = ((double)delt <= mp::DTCLDCR) ? delt : F(1.0 * (double)delt / loops);
   const int nloop = (int)loops;
   for (int loop = 0; loop < nloop; ++loop) {
-    for (int k = 0; k < km; ++k) {
-      c.denfac[k] = sqrtf(1.0f / c.den[k] * F(mp::DEN0));
-      fpvs(c.t[k], c.p[k], c.qs0[k], c.qs1[k]);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      denfac[s] = sqrtf(1.0f / c.den[s] * F(mp::DEN0));
+      fpvs(c.t[s], c.p[s], qs0[s], qs1[s]);
       Slope sl;
-      slope_point(c.qr0[k], c.qr1[k], c.qr2[k], c.den[k], c.denfac[k], c.t[k], sl);
-      const float qsum = fmaxf(c.qr1[k] + c.qr2[k], 1.0e-15f);
-      c.ww2[k] = qsum > 1.0e-15f ? (sl.vt[1] * c.qr1[k] + sl.vt[2] * c.qr2[k]) / qsum : 0.f;
-      c.ww[k] = c.qr0[k] <= 0.f ? 0.f : sl.vt[0];
-      c.rq[k] = c.den[k] * c.qr0[k];
-      c.rq2[k] = c.den[k] * c.qr1[k];
-      c.rq3[k] = c.den[k] * c.qr2[k];
+      slope_point(c.qr0[s], c.qr1[s], c.qr2[s], c.den[s], denfac[s], c.t[s], sl);
+      const float qsum = fmaxf(c.qr1[s] + c.qr2[s], 1.0e-15f);
+      ww2[s] = qsum > 1.0e-15f ? (sl.vt[1] * c.qr1[s] + sl.vt[2] * c.qr2[s]) / qsum : 0.f;
+      ww[s] = c.qr0[s] <= 0.f ? 0.f : sl.vt[0];
+      rq[s] = c.den[s] * c.qr0[s];
+      rq2[s] = c.den[s] * c.qr1[s];
+      rq3[s] = c.den[s] * c.qr2[s];
     }
     // sedimentation of rain, then of snow + graupel
-    const float delq1 = nislfv_plm(c, c.ww, c.rq, km, dtcld, 1);
+    const float delq1 = nislfv_w<SEG, NS>(g, c.den, denfac, c.delz, ww, rq, dtcld, 1, sc);
     float delq2, delq3;
-    nislfv_plm6(c, c.ww2, c.rq2, c.rq3, km, dtcld, 1, &delq2, &delq3);
-    const float fall0 = delq1 / c.delz[0] / dtcld, fall1 = delq2 / c.delz[0] / dtcld;
-    const float fall2 = delq3 / c.delz[0] / dtcld;
-    for (int k = 0; k < km; ++k) {
-      const float den = c.den[k];
-      c.qr0[k] = fmaxf(c.rq[k] / den, 0.0f);
-      c.qr1[k] = fmaxf(c.rq2[k] / den, 0.0f);
-      c.qr2[k] = fmaxf(c.rq3[k] / den, 0.0f);
+    nislfv6_w<SEG, NS>(g, c.den, denfac, c.t, c.delz, ww2, rq2, rq3, dtcld, 1, sc, &delq2, &delq3);
+    const float fall0 = delq1 / dz0 / dtcld, fall1 = delq2 / dz0 / dtcld, fall2 = delq3 / dz0 / dtcld;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const float den = c.den[s];
+      c.qr0[s] = fmaxf(rq[s] / den, 0.0f);
+      c.qr1[s] = fmaxf(rq2[s] / den, 0.0f);
+      c.qr2[s] = fmaxf(rq3[s] / den, 0.0f);
+      qr0s[s] = c.qr0[s];
       Slope sl;
-      slope_point(c.qr0[k], c.qr1[k], c.qr2[k], den, c.denfac[k], c.t[k], sl);
-      c.rs0[k] = sl.rs[0];
-      c.r30[k] = sl.r3[0];
+      slope_point(c.qr0[s], c.qr1[s], c.qr2[s], den, denfac[s], c.t[s], sl);
+      rs0[s] = sl.rs[0];
+      r30[s] = sl.r3[0];
       // melting of snow, then graupel
-      float t = c.t[k];
+      float t = c.t[s];
       const float n0sfac = n0sfac_of(t);
       const bool cond = t > t0c;
-      const float work2 = cond ? venfac(c.p[k], t, den) : 0.f;
+      const float work2 = cond ? venfac(c.p[s], t, den) : 0.f;
       const float xlf = F(mp::XLF0);
-      if (c.qr1[k] > 0.f && cond) {
+      if (c.qr1[s] > 0.f && cond) {
         const float coeres = sl.r2[1] * sqrtf(sl.rs[1] * sl.rb[1]);
         float psmlt = xka(t, den) / xlf * (t0c - t) * F(mp::PI) / 2.0f * n0sfac *
                       (F(mp::PRECS1) * sl.r2[1] + F(mp::PRECS2) * work2 * coeres) / den;
-        psmlt = fminf(fmaxf(psmlt * dtcld / 1.0f, -c.qr1[k] / 1.0f), 0.0f);
-        c.qr1[k] = c.qr1[k] + psmlt;
-        c.qr0[k] = c.qr0[k] - psmlt;
-        t = t + xlf / c.cpm[k] * psmlt;
+        psmlt = fminf(fmaxf(psmlt * dtcld / 1.0f, -c.qr1[s] / 1.0f), 0.0f);
+        c.qr1[s] = c.qr1[s] + psmlt;
+        c.qr0[s] = c.qr0[s] - psmlt;
+        t = t + xlf / cpm[s] * psmlt;
       }
-      if (c.qr2[k] > 0.f && cond) {
+      if (c.qr2[s] > 0.f && cond) {
         const float coeres = sl.r2[2] * sqrtf(sl.rs[2] * sl.rb[2]);
         float pgmlt = xka(t, den) / xlf * (t0c - t) * (F(mp::PRECG1) * sl.r2[2] + F(mp::PRECG2) * work2 * coeres) / den;
-        pgmlt = fminf(fmaxf(pgmlt * dtcld / 1.0f, -c.qr2[k] / 1.0f), 0.0f);
-        c.qr2[k] = c.qr2[k] + pgmlt;
-        c.qr0[k] = c.qr0[k] - pgmlt;
-        t = t + xlf / c.cpm[k] * pgmlt;
+        pgmlt = fminf(fmaxf(pgmlt * dtcld / 1.0f, -c.qr2[s] / 1.0f), 0.0f);
+        c.qr2[s] = c.qr2[s] + pgmlt;
+        c.qr0[s] = c.qr0[s] - pgmlt;
+        t = t + xlf / cpm[s] * pgmlt;
       }
-      c.t[k] = t;
+      c.t[s] = t;
       // cloud-ice fall speed (ice number from the loop-start ice)
-      const float qi = c.qc1[k];
+      const float qi = c.qc1[s];
       const float xni = fminf(fmaxf(5.387e7f * wpow(den * fmaxf(qi, F(mp::QMIN)), 0.75f), 1.0e3f), 1.0e6f);
       float wt = fmaxf(fminf(F(mp::DICON) * sqrtf(den * qi / xni), F(mp::DIMAX)), 1.0e-25f);
       wt = 1.49e4f * wexp(wlog(wt) * 1.31f);
-      c.ww[k] = qi <= 0.f ? 0.f : wt;
-      c.rq[k] = den * qi;
+      ww[s] = qi <= 0.f ? 0.f : wt;
+      rq[s] = den * qi;
     }
-    const float delqi = nislfv_plm(c, c.ww, c.rq, km, dtcld, 0);
-    for (int k = 0; k < km; ++k) c.qc1[k] = fmaxf(c.rq[k] / c.den[k], 0.0f);
-    const float fallc = delqi / c.delz[0] / dtcld;
+    const float delqi = nislfv_w<SEG, NS>(g, c.den, denfac, c.delz, ww, rq, dtcld, 0, sc);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) c.qc1[s] = fmaxf(rq[s] / c.den[s], 0.0f);
+    const float fallc = delqi / dz0 / dtcld;
     const float fallsum = fall0 + fall1 + fall2 + fallc;
     const float fallsum_qsi = fall1 + fallc;
     const float fallsum_qg = fall2;
-    const float dz0 = c.delz[0];
     auto acc = [&](float fs) { return fs * dz0 / F(mp::DENR) * dtcld * 1000.0f; };
     if (fallsum > 0.f) {
       pr.rainncv = acc(fallsum) + pr.rainncv;
@@ -627,75 +796,140 @@ __device__ void wsm6_column(Column& c, int km, float delt, Precip& pr) {
       pr.graupel = acc(fallsum_qg) + pr.graupel;
     }
     if (fallsum > 0.f) pr.sr = (pr.snowncv + pr.graupelncv) / (pr.rainncv + 1.0e-12f);
-    for (int k = 0; k < km; ++k)
-      wsm6_point(c.t[k], c.q[k], c.qc0[k], c.qc1[k], c.qr0[k], c.qr1[k], c.qr2[k], c.den[k], c.p[k], c.denfac[k],
-                 c.cpm[k], c.xl[k], c.qs0[k], c.qs1[k], c.rs0[k], c.r30[k], dtcld);
+    if constexpr (kPoint) {
+#pragma unroll
+      for (int s = 0; s < NS; ++s)
+        if (g.k(s) < km)
+          wsm6_point(c.t[s], c.q[s], c.qc0[s], c.qc1[s], c.qr0[s], c.qr1[s], c.qr2[s], c.den[s], c.p[s], denfac[s],
+                     cpm[s], xl[s], qs0[s], qs1[s], rs0[s], r30[s], dtcld);
+    } else {
+      (void)qs0; (void)qs1; (void)rs0; (void)r30;
+      break;  // one time-split loop (the host checks nloop == 1)
+    }
   }
 }
 
-// calc_p_rho_phi at one mass point (wrf_dynamics.py:4124-4164)
-__device__ __forceinline__ void eos_point(const Grid& g, const S& s, int k, size_t p, int c) {
-  const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
+// calc_p_rho_phi at one mass point (wrf_dynamics.py:4124-4164) given t, qv
+__device__ __forceinline__ void eos_point(const Grid& g, const S& s, int k, size_t p, int c, float t, float qv) {
+  const size_t lev = (size_t)g.ny * g.nx;
   const float* ph = s[WF_PH];
   const float alb = s[WF_ALB][p];
   const float al = -1.0f / s[WF_MUTS][c] * (alb * s[WF_MU][c] + s[WF_RDNW][k] * (ph[p + lev] - ph[p]));
   s[WF_AL][p] = al;
-  const float qvf = 1.0f + (float)RVOVRD * s[WF_MOIST][n3 + p];
-  const float temp = ((float)R_D * ((float)T0 + s[WF_T][p]) * qvf) / ((float)P0 * (al + alb));
+  const float qvf = 1.0f + (float)RVOVRD * qv;
+  const float temp = ((float)R_D * ((float)T0 + t) * qvf) / ((float)P0 * (al + alb));
   s[WF_P][p] = wpow_eos(temp, (float)CPOVCV) * (float)P0 - s[WF_PB][p];
 }
 
-// moist_physics_prep_em + wsm6 + moist_physics_finish_em + calc_p_rho_phi
-__global__ void __launch_bounds__(128) k_physics(Grid g, S s, float dt) {
-  WRF_COLUMN_INDEX(g, j, i);
-  const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde;
-  if (j < jds || j >= jde - 1 || i < ids || i >= ide - 1) return;
-  const int km = g.nz - 1;
+constexpr int kWarpsPerBlock = 8;
+
+// dummy column for segments without a column of their own (they take part in
+// the segment shuffles; nothing they compute is stored)
+template <int NS>
+__device__ __forceinline__ void dummy_column(WCol<NS>& c) {
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    c.t[s] = 280.f; c.q[s] = 0.f; c.qc0[s] = 0.f; c.qc1[s] = 0.f; c.qr0[s] = 0.f; c.qr1[s] = 0.f; c.qr2[s] = 0.f;
+    c.den[s] = 1.f; c.p[s] = 8.0e4f; c.delz[s] = 100.f;
+  }
+}
+
+// moist_physics_prep_em + wsm6 + moist_physics_finish_em + calc_p_rho_phi;
+// block (x, y): SPB consecutive mass columns of row jds + y
+template <int SEG, int NS>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_physics(Grid g, S s, float dt) {
+  constexpr int SPW = 32 / SEG, SPB = kWarpsPerBlock * SPW;
+  __shared__ SegScratch<SEG, NS> scratch[SPB];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int segw = lane / SEG;
+  Seg<SEG, NS> sg;
+  sg.l = lane % SEG;
+  sg.base = segw * SEG;
+  sg.km = g.nz - 1;
+  const int km = sg.km;
+  const int col = warp * SPW + segw;
+  const int j = g.jds + blockIdx.y;
+  const int i = g.ids + blockIdx.x * SPB + col;
+  const bool mass = i < g.ide - 1 && j < g.jde - 1;
+  const bool run = mass && j >= g.jds + 1 && j < g.jde - 2 && i >= g.ids + 1 && i < g.ide - 2;
+  const bool prep = mass && j >= g.jds + 1 && i >= g.ids + 1;
   const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
-  const int c2 = g.i2(j, i);
-  const bool prep = j >= jds + 1 && j < jde - 1 && i >= ids + 1 && i < ide - 1;
-  const bool run = j >= jds + 1 && j < jde - 2 && i >= ids + 1 && i < ide - 2;
+  const int c2 = mass ? g.i2(j, i) : 0;
+  float* T = s[WF_T];
+  float* qv = s[WF_MOIST] + 1 * n3;
+  float* qc = s[WF_MOIST] + 2 * n3;
+  WCol<NS> c;
+  float th[NS], pii[NS];
   if (run) {
-    float* T = s[WF_T];
-    float* qv = s[WF_MOIST] + 1 * n3;
-    float* qc = s[WF_MOIST] + 2 * n3;
-    Column c;
-    for (int k = 0; k < km; ++k) {
-      const size_t p = k * lev + c2;
-      const float th = T[p] + (float)T0;
-      const float pfull = s[WF_P][p] + s[WF_PB][p];
-      const float pii = wpow(pfull / (float)P0, F(mp::RCP));
-      c.t[k] = th * pii;
-      c.den[k] = 1.0f / (s[WF_AL][p] + s[WF_ALB][p]);
-      c.p[k] = pfull;
-      const float zlo = (s[WF_PH][p] + s[WF_PHB][p]) / (float)G;
-      const float zhi = (s[WF_PH][p + lev] + s[WF_PHB][p + lev]) / (float)G;
-      c.delz[k] = zhi - zlo;
-      c.q[k] = qv[p];
-      c.qc0[k] = qc[p];
-      c.qr0[k] = s[WF_MOIST][3 * n3 + p];
-      c.qc1[k] = s[WF_MOIST][4 * n3 + p];
-      c.qr1[k] = s[WF_MOIST][5 * n3 + p];
-      c.qr2[k] = s[WF_MOIST][6 * n3 + p];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      const int k = sg.k(q);
+      if (k < km) {
+        const size_t p = k * lev + c2;
+        th[q] = T[p] + (float)T0;
+        const float pfull = s[WF_P][p] + s[WF_PB][p];
+        pii[q] = wpow(pfull / (float)P0, F(mp::RCP));
+        c.t[q] = th[q] * pii[q];
+        c.den[q] = 1.0f / (s[WF_AL][p] + s[WF_ALB][p]);
+        c.p[q] = pfull;
+        const float zlo = (s[WF_PH][p] + s[WF_PHB][p]) / (float)G;
+        const float zhi = (s[WF_PH][p + lev] + s[WF_PHB][p + lev]) / (float)G;
+        c.delz[q] = zhi - zlo;
+        c.q[q] = qv[p];
+        c.qc0[q] = qc[p];
+        c.qr0[q] = s[WF_MOIST][3 * n3 + p];
+        c.qc1[q] = s[WF_MOIST][4 * n3 + p];
+        c.qr1[q] = s[WF_MOIST][5 * n3 + p];
+        c.qr2[q] = s[WF_MOIST][6 * n3 + p];
+      } else {
+        th[q] = 300.f; pii[q] = 1.f;
+        c.t[q] = 280.f; c.q[q] = 0.f; c.qc0[q] = 0.f; c.qc1[q] = 0.f; c.qr0[q] = 0.f; c.qr1[q] = 0.f; c.qr2[q] = 0.f;
+        c.den[q] = 1.f; c.p[q] = 8.0e4f; c.delz[q] = 100.f;
+      }
     }
-    Precip pr{s[WF_RAINNC][c2], 0.f, s[WF_SNOWNC][c2], 0.f, s[WF_GRAUPELNC][c2], 0.f, 0.f};
-    wsm6_column(c, km, dt, pr);
-    for (int k = 0; k < km; ++k) {
-      const size_t p = k * lev + c2;
-      const float thold = T[p] + (float)T0;
-      const float pii = wpow((s[WF_P][p] + s[WF_PB][p]) / (float)P0, F(mp::RCP));
-      const float mpten = c.t[k] / pii - thold;
-      T[p] = T[p] + mpten;
+  } else {
+    dummy_column<NS>(c);
+#pragma unroll
+    for (int q = 0; q < NS; ++q) { th[q] = 300.f; pii[q] = 1.f; }
+  }
+  Precip pr{run ? s[WF_RAINNC][c2] : 0.f, 0.f, run ? s[WF_SNOWNC][c2] : 0.f, 0.f,
+            run ? s[WF_GRAUPELNC][c2] : 0.f, 0.f, 0.f};
+  // every segment of the warp takes part (shuffles); only run columns store
+  float qr0s[NS];
+  wsm6_column_w<SEG, NS, true>(sg, c, dt, pr, scratch[col], qr0s);
+  if (!mass) return;
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    const int k = sg.k(q);
+    if (k >= km) continue;
+    const size_t p = k * lev + c2;
+    float tnew, qvnew;
+    if (run) {
+      const float mpten = c.t[q] / pii[q] - th[q];
+      tnew = T[p] + mpten;
+      T[p] = tnew;
       s[WF_H_DIABATIC][p] = mpten / dt;
-      s[WF_QV_DIABATIC][p] = (c.q[k] - qv[p]) / dt;
-      s[WF_QC_DIABATIC][p] = (c.qc0[k] - qc[p]) / dt;
-      qv[p] = c.q[k];
-      qc[p] = c.qc0[k];
-      s[WF_MOIST][3 * n3 + p] = c.qr0[k];
-      s[WF_MOIST][4 * n3 + p] = c.qc1[k];
-      s[WF_MOIST][5 * n3 + p] = c.qr1[k];
-      s[WF_MOIST][6 * n3 + p] = c.qr2[k];
+      s[WF_QV_DIABATIC][p] = (c.q[q] - qv[p]) / dt;
+      s[WF_QC_DIABATIC][p] = (c.qc0[q] - qc[p]) / dt;
+      qvnew = c.q[q];
+      qv[p] = qvnew;
+      qc[p] = c.qc0[q];
+      s[WF_MOIST][3 * n3 + p] = c.qr0[q];
+      s[WF_MOIST][4 * n3 + p] = c.qc1[q];
+      s[WF_MOIST][5 * n3 + p] = c.qr1[q];
+      s[WF_MOIST][6 * n3 + p] = c.qr2[q];
+    } else {
+      if (prep) {  // prepared but outside the scheme's block: zero tendencies
+        s[WF_H_DIABATIC][p] = 0.0f;
+        s[WF_QV_DIABATIC][p] = 0.0f;
+        s[WF_QC_DIABATIC][p] = 0.0f;
+      }
+      tnew = T[p];
+      qvnew = qv[p];
     }
+    eos_point(g, s, k, p, c2, tnew, qvnew);
+  }
+  if (run && sg.l == 0) {
     s[WF_RAINNC][c2] = pr.rain;
     s[WF_RAINNCV][c2] = pr.rainncv;
     s[WF_SNOWNC][c2] = pr.snow;
@@ -703,16 +937,7 @@ __global__ void __launch_bounds__(128) k_physics(Grid g, S s, float dt) {
     s[WF_GRAUPELNC][c2] = pr.graupel;
     s[WF_GRAUPELNCV][c2] = pr.graupelncv;
     s[WF_SR][c2] = pr.sr;
-  } else if (prep) {
-    // prepared but outside the scheme's block: zero tendencies
-    for (int k = 0; k < km; ++k) {
-      const size_t p = k * lev + c2;
-      s[WF_H_DIABATIC][p] = 0.0f;
-      s[WF_QV_DIABATIC][p] = 0.0f;
-      s[WF_QC_DIABATIC][p] = 0.0f;
-    }
   }
-  for (int k = 0; k < km; ++k) eos_point(g, s, k, k * lev + c2, c2);
 }
 
 // stand-alone WSM6 on caller arrays: columns [ids+1, ide-2) x [jds+1, jde-2),
@@ -723,52 +948,232 @@ struct Wsm6Args {
   float *rainnc, *rainncv, *snownc, *snowncv, *graupelnc, *graupelncv, *sr;
 };
 
-__global__ void __launch_bounds__(128) k_wsm6(Grid g, Wsm6Args a, float delt) {
-  WRF_COLUMN_INDEX(g, j, i);
-  if (j < g.jds + 1 || j >= g.jde - 2 || i < g.ids + 1 || i >= g.ide - 2) return;
-  const int km = g.nz - 1;
+template <int SEG, int NS>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_wsm6(Grid g, Wsm6Args a, float delt) {
+  constexpr int SPW = 32 / SEG, SPB = kWarpsPerBlock * SPW;
+  __shared__ SegScratch<SEG, NS> scratch[SPB];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int segw = lane / SEG;
+  Seg<SEG, NS> sg;
+  sg.l = lane % SEG;
+  sg.base = segw * SEG;
+  sg.km = g.nz - 1;
+  const int km = sg.km;
+  const int col = warp * SPW + segw;
+  const int j = g.jds + 1 + blockIdx.y;
+  const int i = g.ids + 1 + blockIdx.x * SPB + col;
+  const bool run = i < g.ide - 2 && j < g.jde - 2;
   const size_t lev = (size_t)g.ny * g.nx;
+  const int c2 = run ? g.i2(j, i) : 0;
+  WCol<NS> c;
+  dummy_column<NS>(c);
+  if (run) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      const int k = sg.k(q);
+      if (k >= km) continue;
+      const size_t p = k * lev + c2;
+      c.t[q] = a.th[p] * a.pii[p];
+      c.den[q] = a.rho[p];
+      c.p[q] = a.p[p];
+      c.delz[q] = a.dz8w[p];
+      c.q[q] = a.qv[p];
+      c.qc0[q] = a.qc[p];
+      c.qr0[q] = a.qr[p];
+      c.qc1[q] = a.qi[p];
+      c.qr1[q] = a.qs[p];
+      c.qr2[q] = a.qg[p];
+    }
+  }
+  Precip pr{run ? a.rainnc[c2] : 0.f, 0.f, run ? a.snownc[c2] : 0.f, 0.f, run ? a.graupelnc[c2] : 0.f, 0.f, 0.f};
+  float qr0s[NS];
+  wsm6_column_w<SEG, NS, true>(sg, c, delt, pr, scratch[col], qr0s);
+  if (!run) return;
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    const int k = sg.k(q);
+    if (k >= km) continue;
+    const size_t p = k * lev + c2;
+    a.th[p] = c.t[q] / a.pii[p];
+    a.qv[p] = c.q[q];
+    a.qc[p] = c.qc0[q];
+    a.qr[p] = c.qr0[q];
+    a.qi[p] = c.qc1[q];
+    a.qs[p] = c.qr1[q];
+    a.qg[p] = c.qr2[q];
+  }
+  if (sg.l == 0) {
+    a.rainnc[c2] = pr.rain;
+    a.rainncv[c2] = pr.rainncv;
+    a.snownc[c2] = pr.snow;
+    a.snowncv[c2] = pr.snowncv;
+    a.graupelnc[c2] = pr.graupel;
+    a.graupelncv[c2] = pr.graupelncv;
+    a.sr[c2] = pr.sr;
+  }
+}
+
+// Split form of the physics step for a single time-split loop (dt < 240 s):
+// k_wsm6_sed runs the column-coupled part (sedimentation of rain,
+// snow + graupel and ice, melting, precipitation) on warp segments and leaves
+// its state in WSM_T (temperature), WSM_QR0S (rain after the sedimentation)
+// and the moisture slots; k_wsm6_finish then runs the point processes, the
+// finish step and the equation of state one point per thread.  The
+// arithmetic is that of k_physics, operation for operation.
+template <int SEG, int NS>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_wsm6_sed(Grid g, S s, float dt) {
+  constexpr int SPW = 32 / SEG, SPB = kWarpsPerBlock * SPW;
+  __shared__ SegScratch<SEG, NS> scratch[SPB];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int segw = lane / SEG;
+  Seg<SEG, NS> sg;
+  sg.l = lane % SEG;
+  sg.base = segw * SEG;
+  sg.km = g.nz - 1;
+  const int km = sg.km;
+  const int col = warp * SPW + segw;
+  const int j = g.jds + 1 + blockIdx.y;
+  const int i = g.ids + 1 + blockIdx.x * SPB + col;
+  const bool run = i < g.ide - 2 && j < g.jde - 2;
+  const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
+  const int c2 = run ? g.i2(j, i) : 0;
+  float* M = s[WF_MOIST];
+  WCol<NS> c;
+  dummy_column<NS>(c);
+  if (run) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      const int k = sg.k(q);
+      if (k >= km) continue;
+      const size_t p = k * lev + c2;
+      const float th = s[WF_T][p] + (float)T0;
+      const float pfull = s[WF_P][p] + s[WF_PB][p];
+      c.t[q] = th * wpow(pfull / (float)P0, F(mp::RCP));
+      c.den[q] = 1.0f / (s[WF_AL][p] + s[WF_ALB][p]);
+      c.p[q] = pfull;
+      const float zlo = (s[WF_PH][p] + s[WF_PHB][p]) / (float)G;
+      const float zhi = (s[WF_PH][p + lev] + s[WF_PHB][p + lev]) / (float)G;
+      c.delz[q] = zhi - zlo;
+      c.q[q] = M[n3 + p];
+      c.qc0[q] = M[2 * n3 + p];
+      c.qr0[q] = M[3 * n3 + p];
+      c.qc1[q] = M[4 * n3 + p];
+      c.qr1[q] = M[5 * n3 + p];
+      c.qr2[q] = M[6 * n3 + p];
+    }
+  }
+  Precip pr{run ? s[WF_RAINNC][c2] : 0.f, 0.f, run ? s[WF_SNOWNC][c2] : 0.f, 0.f,
+            run ? s[WF_GRAUPELNC][c2] : 0.f, 0.f, 0.f};
+  float qr0s[NS];
+  wsm6_column_w<SEG, NS, false>(sg, c, dt, pr, scratch[col], qr0s);
+  if (!run) return;
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    const int k = sg.k(q);
+    if (k >= km) continue;
+    const size_t p = k * lev + c2;
+    s[WF_WSM_T][p] = c.t[q];
+    s[WF_WSM_QR0S][p] = qr0s[q];
+    M[3 * n3 + p] = c.qr0[q];
+    M[4 * n3 + p] = c.qc1[q];
+    M[5 * n3 + p] = c.qr1[q];
+    M[6 * n3 + p] = c.qr2[q];
+  }
+  if (sg.l == 0) {
+    s[WF_RAINNC][c2] = pr.rain;
+    s[WF_RAINNCV][c2] = pr.rainncv;
+    s[WF_SNOWNC][c2] = pr.snow;
+    s[WF_SNOWNCV][c2] = pr.snowncv;
+    s[WF_GRAUPELNC][c2] = pr.graupel;
+    s[WF_GRAUPELNCV][c2] = pr.graupelncv;
+    s[WF_SR][c2] = pr.sr;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_wsm6_finish(Grid g, S s, float dt, float dtcld) {
+  WRF_POINT_INDEX(g, k, j, i);
+  if (k >= g.nz - 1 || j < g.jds || j >= g.jde - 1 || i < g.ids || i >= g.ide - 1) return;
+  const bool run = j >= g.jds + 1 && j < g.jde - 2 && i >= g.ids + 1 && i < g.ide - 2;
+  const bool prep = j >= g.jds + 1 && i >= g.ids + 1;
+  const size_t n3 = g.n3();
   const int c2 = g.i2(j, i);
-  Column c;
-  for (int k = 0; k < km; ++k) {
-    const size_t p = k * lev + c2;
-    c.t[k] = a.th[p] * a.pii[p];
-    c.den[k] = a.rho[p];
-    c.p[k] = a.p[p];
-    c.delz[k] = a.dz8w[p];
-    c.q[k] = a.qv[p];
-    c.qc0[k] = a.qc[p];
-    c.qr0[k] = a.qr[p];
-    c.qc1[k] = a.qi[p];
-    c.qr1[k] = a.qs[p];
-    c.qr2[k] = a.qg[p];
+  const size_t p = (size_t)k * g.ny * g.nx + c2;
+  float* M = s[WF_MOIST];
+  float T = s[WF_T][p];
+  float qvnew = M[n3 + p];
+  if (run) {
+    const float th = T + (float)T0;
+    const float pfull = s[WF_P][p] + s[WF_PB][p];
+    const float pii = wpow(pfull / (float)P0, F(mp::RCP));
+    const float t0 = th * pii;
+    const float den = 1.0f / (s[WF_AL][p] + s[WF_ALB][p]);
+    const float denfac = sqrtf(1.0f / den * F(mp::DEN0));
+    float q = qvnew;
+    const float qcold = M[2 * n3 + p];
+    float qc0 = fmaxf(qcold, 0.0f);
+    const float cpm = q >= F(mp::QMIN) ? F(mp::CPV) * q + (1.0f - q) * F(mp::CPD)
+                                       : F(mp::CPD * (1.0 - mp::QMIN) + mp::CPV * mp::QMIN);
+    const float xl = F(mp::XLV0) - F(mp::XLV1) * (t0 - F(mp::T0C));
+    float qs0, qs1;
+    fpvs(t0, pfull, qs0, qs1);
+    const float qr0s = s[WF_WSM_QR0S][p];
+    const bool small = qr0s <= F(mp::QCRMIN);
+    const float rs0 = small ? F(mp::RSLOPERMAX) : 1.0f / wpow(F(mp::PIDN0R) / (qr0s * den), 0.25f);
+    const float r30 = small ? F(mp::RSLOPER3MAX) : rs0 * rs0 * rs0;
+    float t = s[WF_WSM_T][p];
+    float qc1 = M[4 * n3 + p], qr0 = M[3 * n3 + p], qr1 = M[5 * n3 + p], qr2 = M[6 * n3 + p];
+    wsm6_point(t, q, qc0, qc1, qr0, qr1, qr2, den, pfull, denfac, cpm, xl, qs0, qs1, rs0, r30, dtcld);
+    const float mpten = t / pii - th;
+    T = T + mpten;
+    s[WF_T][p] = T;
+    s[WF_H_DIABATIC][p] = mpten / dt;
+    s[WF_QV_DIABATIC][p] = (q - qvnew) / dt;
+    s[WF_QC_DIABATIC][p] = (qc0 - qcold) / dt;
+    qvnew = q;
+    M[n3 + p] = q;
+    M[2 * n3 + p] = qc0;
+    M[3 * n3 + p] = qr0;
+    M[4 * n3 + p] = qc1;
+    M[5 * n3 + p] = qr1;
+    M[6 * n3 + p] = qr2;
+  } else if (prep) {  // prepared but outside the scheme's block: zero tendencies
+    s[WF_H_DIABATIC][p] = 0.0f;
+    s[WF_QV_DIABATIC][p] = 0.0f;
+    s[WF_QC_DIABATIC][p] = 0.0f;
   }
-  Precip pr{a.rainnc[c2], 0.f, a.snownc[c2], 0.f, a.graupelnc[c2], 0.f, 0.f};
-  wsm6_column(c, km, delt, pr);
-  for (int k = 0; k < km; ++k) {
-    const size_t p = k * lev + c2;
-    a.th[p] = c.t[k] / a.pii[p];
-    a.qv[p] = c.q[k];
-    a.qc[p] = c.qc0[k];
-    a.qr[p] = c.qr0[k];
-    a.qi[p] = c.qc1[k];
-    a.qs[p] = c.qr1[k];
-    a.qg[p] = c.qr2[k];
-  }
-  a.rainnc[c2] = pr.rain;
-  a.rainncv[c2] = pr.rainncv;
-  a.snownc[c2] = pr.snow;
-  a.snowncv[c2] = pr.snowncv;
-  a.graupelnc[c2] = pr.graupel;
-  a.graupelncv[c2] = pr.graupelncv;
-  a.sr[c2] = pr.sr;
+  eos_point(g, s, k, p, c2, T, qvnew);
 }
 
 #undef F
 
+// 16-lane segments with 3 levels per lane hold up to 47 mass levels; deeper
+// columns use whole warps with 2 levels per lane (up to 63)
 int launch_physics(const Grid& g, const S& s, cudaStream_t st) {
-  const dim3 b(32, 4);
-  k_physics<<<col_grid(g, b), b, 0, st>>>(g, s, g.dt);
+  const int km = g.nz - 1;
+  const dim3 b(32 * kWarpsPerBlock);
+  const double loops = fmax(g.dtd / mp::DTCLDCR, 1.0);
+  if ((int)loops == 1) {
+    const float dtcld = (g.dtd <= mp::DTCLDCR) ? g.dt : (float)(1.0 * g.dtd / loops);
+    const int ncol = g.ide - 2 - (g.ids + 1), nrow = g.jde - 2 - (g.jds + 1);
+    if (km <= 47) {
+      constexpr int SPB = kWarpsPerBlock * 2;
+      k_wsm6_sed<16, 3><<<dim3((ncol + SPB - 1) / SPB, nrow), b, 0, st>>>(g, s, g.dt);
+    } else {
+      constexpr int SPB = kWarpsPerBlock;
+      k_wsm6_sed<32, 2><<<dim3((ncol + SPB - 1) / SPB, nrow), b, 0, st>>>(g, s, g.dt);
+    }
+    const dim3 b3(32, 4);
+    k_wsm6_finish<<<point_grid(g, b3), b3, 0, st>>>(g, s, g.dt, dtcld);
+    return 2;
+  }
+  const int ncol = g.ide - 1 - g.ids, nrow = g.jde - 1 - g.jds;
+  if (km <= 47) {
+    constexpr int SPB = kWarpsPerBlock * 2;
+    k_physics<16, 3><<<dim3((ncol + SPB - 1) / SPB, nrow), b, 0, st>>>(g, s, g.dt);
+  } else {
+    constexpr int SPB = kWarpsPerBlock;
+    k_physics<32, 2><<<dim3((ncol + SPB - 1) / SPB, nrow), b, 0, st>>>(g, s, g.dt);
+  }
   return 1;
 }
 
@@ -776,8 +1181,16 @@ int launch_physics(const Grid& g, const S& s, cudaStream_t st) {
 int launch_wsm6(const Grid& g, float* const* f, float delt, cudaStream_t st) {
   Wsm6Args a{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], f[10],
              f[11], f[12], f[13], f[14], f[15], f[16], f[17]};
-  const dim3 b(32, 4);
-  k_wsm6<<<col_grid(g, b), b, 0, st>>>(g, a, delt);
+  const int km = g.nz - 1;
+  const int ncol = g.ide - 2 - (g.ids + 1), nrow = g.jde - 2 - (g.jds + 1);
+  const dim3 b(32 * kWarpsPerBlock);
+  if (km <= 47) {
+    constexpr int SPB = kWarpsPerBlock * 2;
+    k_wsm6<16, 3><<<dim3((ncol + SPB - 1) / SPB, nrow), b, 0, st>>>(g, a, delt);
+  } else {
+    constexpr int SPB = kWarpsPerBlock;
+    k_wsm6<32, 2><<<dim3((ncol + SPB - 1) / SPB, nrow), b, 0, st>>>(g, a, delt);
+  }
   return 1;
 }
 

@@ -186,14 +186,32 @@ def test_nan_in_the_state_is_reported_not_fatal(small):
     assert s["nan_p"] > 0 and s["step"] == 1
 
 
+def test_two_split_microphysics_loops_coarse_grid():
+    """dt = 240 s makes WSM6 run two time-split loops (the fused physics
+    kernel); a 40 km grid keeps the acoustic steps stable."""
+    spec = synthetic.CaseSpec(n=28, nz=16, dx=40000.0, dt=240.0, nsteps=1, bdy_tend_amp=1.0e-4, seed=5)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    st, it = cuda_run(g, inputs, bdy, 1)
+    out = cuda_fields(st)
+    o64 = oracle_fields(g, inputs, bdy, np.float64, 1)
+    o32 = oracle_fields(g, inputs, bdy, np.float32, 1)
+    for k in out:
+        err, floor = rel_l2(out[k], o64[k]), rel_l2(o32[k], o64[k])
+        assert err <= K_FLOOR * floor + ABS_FLOOR, (k, err, floor)
+    assert it.status()["nan_p"] == 0
+
+
 def _ptr(t: torch.Tensor):
     assert t.is_cuda and t.is_contiguous() and t.dtype == torch.float32
     return ctypes.c_void_p(t.data_ptr())
 
 
-def test_wsm6_entry_point_matches_oracle(small):
+@pytest.mark.parametrize("delt", [45.0, 250.0])
+def test_wsm6_entry_point_matches_oracle(small, delt):
     """wrf_wsm6 on the physics inputs of a real stepped state against the
-    oracle's WSM6 in fp64 (fp32 floor from the oracle's fp32 run)."""
+    oracle's WSM6 in fp64 (fp32 floor from the oracle's fp32 run); 250 s
+    takes two time-split loops."""
     g, inputs, bdy = small
     m = OracleModel(g, inputs, bdy, np.float64)
     m.run(1)
@@ -207,7 +225,7 @@ def test_wsm6_entry_point_matches_oracle(small):
         a = {k: v.astype(dtype).copy() for k, v in arrays.items()}
         p2 = {k: v.astype(dtype).copy() for k, v in pre2.items()}
         OP.wsm6(g, a["th_phy"], a["q1"], a["q2"], a["q3"], a["q4"], a["q5"], a["q6"], a["rho"], a["pi_phy"],
-                a["p_phy"], a["dz8w"], float(g.dt), p2["rainnc"], p2["rainncv"], p2["snownc"], p2["snowncv"],
+                a["p_phy"], a["dz8w"], float(delt), p2["rainnc"], p2["rainncv"], p2["snownc"], p2["snowncv"],
                 p2["graupelnc"], p2["graupelncv"], p2["sr"])
         return a, p2
 
@@ -217,7 +235,7 @@ def test_wsm6_entry_point_matches_oracle(small):
     d2 = {k: torch.tensor(v, dtype=torch.float32, device="cuda") for k, v in pre2.items()}
     st = DeviceState(g, "cuda")
     L = N.lib()
-    rc = L.wrf_wsm6(ctypes.byref(st.cgrid), *[_ptr(dev[k]) for k in names], ctypes.c_float(g.dt),
+    rc = L.wrf_wsm6(ctypes.byref(st.cgrid), *[_ptr(dev[k]) for k in names], ctypes.c_float(delt),
                     *[_ptr(d2[k]) for k in ("rainnc", "rainncv", "snownc", "snowncv", "graupelnc", "graupelncv", "sr")],
                     ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     N.check(rc, "wrf_wsm6")
