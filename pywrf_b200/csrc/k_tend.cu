@@ -1,7 +1,7 @@
 // Large-step (RK stage) tendencies.
-//   k_advect  advect_u, advect_v, advect_w, advect_scalar(theta)
-//             (wrf_dynamics.py:1112-2028): 5th-order upwind-biased fluxes,
-//             3rd/2nd order on the rows next to each boundary
+//   k_advect  advect_u, advect_v, advect_w (wrf_dynamics.py:1112-1823):
+//             5th-order upwind-biased fluxes, 3rd/2nd order on the rows next
+//             to each boundary (theta and the moisture species: k_advect_tiled)
 //   k_forces  rhs_ph, horizontal_pressure_gradient, pg_buoy_w, coriolis,
 //             curvature (wrf_dynamics.py:2031-2620)
 //   k_addtend rk_addtend_dry + spec_bdytend (wrf_dynamics.py:3100-3148,
@@ -278,23 +278,7 @@ __global__ void k_advect(Grid g, S s) {
       t = t + 2.0f * s[WF_RDN][ktf - 1] * vf_w(g, w, ww, ktf, c);
     s[WF_RW_TEND][p] = t;
   }
-  // theta
-  advect_scalar_point(g, s, s[WF_T], s[WF_T_TEND], ru, rv, ww, k, j, i);
-}
-
-// scalar advection of the six moisture species with the time-averaged mass
-// fluxes (rk_scalar_tend, wrf_dynamics.py:3982-4051); advect_tend is zeroed
-// on [0, nz) x [jts, jte) x [its, ite) first
-__global__ void k_advect_moist(Grid g, S s) {
-  WRF_POINT_INDEX(g, k, j, i);
-  const size_t n3 = g.n3();
-  const size_t p = (size_t)g.i3(k, j, i);
-  const bool zreg = j >= g.jds && j < g.jde && i >= g.ids && i < g.ide;
-  for (int m = 1; m < 7; ++m) {
-    float* tend = s[WF_ADVECT_TEND] + m * n3;
-    if (zreg) tend[p] = 0.f;
-    advect_scalar_point(g, s, s[WF_MOIST] + m * n3, tend, s[WF_RU_M], s[WF_RV_M], s[WF_WW_M], k, j, i);
-  }
+  // theta: k_advect_tiled
 }
 
 // ------------------------------------------------------------------ forces
@@ -542,8 +526,9 @@ __global__ void k_advect_scalar(Grid g, S s, const float* q, float* tend, const 
 int launch_advect_forces(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_advect<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  const int n = launch_advect_theta_tiled(g, s, st);
   k_forces<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  return 2;
+  return 2 + n;
 }
 
 int launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st) {
@@ -559,10 +544,6 @@ int launch_advect_scalar(const Grid& g, const S& s, const float* field, float* t
   return 1;
 }
 
-int launch_advect_moist(const Grid& g, const S& s, cudaStream_t st) {
-  const dim3 b3(32, 4);
-  k_advect_moist<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  return 1;
-}
+int launch_advect_moist(const Grid& g, const S& s, cudaStream_t st) { return launch_advect_moist_tiled(g, s, st); }
 
 }  // namespace wrf

@@ -28,6 +28,10 @@ int launch_advect_forces(const Grid& g, const S& s, cudaStream_t st);
 int launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st);
 // moisture advection with the time-averaged fluxes (k_tend.cu)
 int launch_advect_moist(const Grid& g, const S& s, cudaStream_t st);
+// tiled scalar advection (k_advect_tiled.cu): the six moisture species with
+// ru_m / rv_m / ww_m into advect_tend, theta with ru / rv / ww into t_tend
+int launch_advect_moist_tiled(const Grid& g, const S& s, cudaStream_t st);
+int launch_advect_theta_tiled(const Grid& g, const S& s, cudaStream_t st);
 // stand-alone advect_scalar (k_tend.cu)
 int launch_advect_scalar(const Grid& g, const S& s, const float* field, float* tend, const float* ru,
                           const float* rv, const float* rom, cudaStream_t st);

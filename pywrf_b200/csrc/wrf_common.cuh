@@ -74,17 +74,29 @@ __device__ __forceinline__ float wlog(float a) { return logf(a); }
 // 1.0 if ua >= 0 else -1.0 (fortran_sign(1., ua), wrf_dynamics.py:1309-1311)
 __device__ __forceinline__ float sgnf(float ua) { return ua >= 0.f ? 1.f : -1.f; }
 
+// x / d, correctly rounded, for a constant d given r = RN(1/d): the quotient
+// estimate x*r is corrected once with the exact residual (Markstein's
+// theorem: with r within half an ulp of 1/d the result is the correctly
+// rounded quotient for normal results), a multiply and two FMAs in place of
+// a full IEEE division
+__device__ __forceinline__ float divc(float x, float d, float r) {
+  const float q = x * r;
+  return fmaf(fmaf(-q, d, x), r, q);
+}
+
 // 3rd-order upwind-biased face value (wrf_dynamics.py:1313-1320)
 __device__ __forceinline__ float flux3(float qm2, float qm1, float q0, float qp1, float ua) {
-  float f4 = (7.f * (q0 + qm1) - (qp1 + qm2)) / 12.f;
-  return f4 + sgnf(ua) * ((qp1 - qm2) - 3.f * (q0 - qm1)) / 12.f;
+  constexpr float r12 = 1.0f / 12.0f;
+  const float f4 = divc(7.f * (q0 + qm1) - (qp1 + qm2), 12.f, r12);
+  return f4 + divc(sgnf(ua) * ((qp1 - qm2) - 3.f * (q0 - qm1)), 12.f, r12);
 }
 
 // 5th-order upwind-biased face value (wrf_dynamics.py:1322-1329)
 __device__ __forceinline__ float flux5(float qm3, float qm2, float qm1, float q0, float qp1, float qp2,
                                        float ua) {
-  float f6 = (37.f * (q0 + qm1) - 8.f * (qp1 + qm2) + (qp2 + qm3)) / 60.f;
-  return f6 - sgnf(ua) * ((qp2 - qm3) - 5.f * (qp1 - qm2) + 10.f * (q0 - qm1)) / 60.f;
+  constexpr float r60 = 1.0f / 60.0f;
+  const float f6 = divc(37.f * (q0 + qm1) - 8.f * (qp1 + qm2) + (qp2 + qm3), 60.f, r60);
+  return f6 - divc(sgnf(ua) * ((qp2 - qm3) - 5.f * (qp1 - qm2) + 10.f * (q0 - qm1)), 60.f, r60);
 }
 
 #define WRF_POINT_INDEX(g, k, j, i)                          \
