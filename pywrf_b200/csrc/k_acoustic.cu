@@ -209,32 +209,24 @@ __global__ void k_advance_uv(Grid g, S s, float dts) {
 // Fused acoustic column update of one substep: advance_mu_t, advance_w,
 // sumflux, spec_bdyupdate of t / mu / muts / ph, calc_p_rho
 // (wrf_dynamics.py:3528-3839, 3269-3313; wrf_boundary.py:244-355).  A block
-// owns kColTX adjacent columns of one row and kColKT level groups: the
-// explicit parts run in parallel over levels through shared memory, the
-// vertical recurrences (column mass divergence sum, ww scan, Thomas sweeps)
-// run sequentially per column in the reference's order.  No column reads
-// another column's result of this kernel, so no grid-wide ordering is needed;
-// zero_grad_bdy(w) follows in k_zero_grad_w.
-constexpr int kColTX = 32, kColKT = 8;
+// owns kColTX adjacent columns of one row; thread (tx, tk) handles the levels
+// k = tk, tk + kColKT, ... of column tx.  The explicit parts run over levels
+// in parallel; the vertical recurrences (column mass divergence sum, ww scan,
+// Thomas sweeps) run sequentially per column in the reference's order, from
+// separate shared arrays so that their loads pipeline.  Small blocks and few
+// registers let several blocks share an SM, which overlaps one block's
+// sweeps with the memory phases of the others.  No column reads another
+// column's result of this kernel; zero_grad_bdy(w) follows in k_zero_grad_w.
+// Divisions by per-column constants use the correctly rounded form divc with
+// the column's reciprocals (__frcp_rn).
+constexpr int kColTX = 16, kColKT = 16;
 
-struct ColArrays {  // [nz][kColTX] slices of dynamic shared memory
-  float *dw, *ww, *t2av, *rhs, *a, *alpha, *gamma, *ph;
-  float *muave, *muts, *mu;
-};
-
-__device__ __forceinline__ ColArrays col_arrays(float* base, int nz) {
-  ColArrays c;
-  const int n = nz * kColTX;
-  c.dw = base; c.ww = base + n; c.t2av = base + 2 * n; c.rhs = base + 3 * n; c.a = base + 4 * n;
-  c.alpha = base + 5 * n; c.gamma = base + 6 * n; c.ph = base + 7 * n;
-  c.muave = base + 8 * n; c.muts = c.muave + kColTX; c.mu = c.muts + kColTX;
-  return c;
-}
-
-size_t acoustic_col_smem(int nz) { return (size_t)(8 * nz * kColTX + 3 * kColTX) * sizeof(float); }
-
-__global__ void __launch_bounds__(kColTX * kColKT) k_acoustic_col(Grid g, S s, float dts, int iteration, int nsub) {
-  extern __shared__ float smem_col[];
+__global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s, float dts, int iteration, int nsub) {
+  __shared__ float sdw[kMaxNz][kColTX], sww[kMaxNz][kColTX], st2av[kMaxNz][kColTX], srhs[kMaxNz][kColTX];
+  __shared__ float sa[kMaxNz][kColTX], salpha[kMaxNz][kColTX], sgamma[kMaxNz][kColTX], sph[kMaxNz][kColTX];
+  __shared__ float swd[kMaxNz][kColTX];
+  __shared__ float pdnw[kMaxNz], prdnw[kMaxNz], prdn[kMaxNz], pfnm[kMaxNz], pfnp[kMaxNz];
+  __shared__ float smuave[kColTX], smuts[kColTX], smu[kColTX];
   const int nz = g.nz, kend = nz - 1, nx = g.nx;
   const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde;
   const int tx = threadIdx.x % kColTX, tk = threadIdx.x / kColTX;
@@ -245,24 +237,25 @@ __global__ void __launch_bounds__(kColTX * kColKT) k_acoustic_col(Grid g, S s, f
   const bool spec = col && (((j == jds || j == jde - 2) && i < ide - 1) || (j >= jds + 1 && j < jde - 2 && (i == ids || i == ide - 2)));
   const bool mass = inner || spec;
   const int c = col ? g.i2(j, i) : 0;
-  const size_t lev = (size_t)g.ny * nx;
-  ColArrays sm = col_arrays(smem_col, nz);
-  auto A = [&](float* arr, int k) -> float& { return arr[k * kColTX + tx]; };
+  const int lev = g.ny * nx;
+  for (int e = threadIdx.x; e < nz; e += kColTX * kColKT) {
+    pdnw[e] = __ldg(&s[WF_DNW][e]);
+    prdnw[e] = __ldg(&s[WF_RDNW][e]);
+    prdn[e] = __ldg(&s[WF_RDN][e]);
+    pfnm[e] = __ldg(&s[WF_FNM][e]);
+    pfnp[e] = __ldg(&s[WF_FNP][e]);
+  }
   float* t = s[WF_T];
   const float* ft = s[WF_T_TEND];
   const float* t1 = s[WF_T_SAVE];
   float* ww = s[WF_WW];
   const float* ww1 = s[WF_WW1];
-  const float* dnw = s[WF_DNW];
-  const float* fnm = s[WF_FNM];
-  const float* fnp = s[WF_FNP];
-  const float* rdnw = s[WF_RDNW];
-  const float* rdn = s[WF_RDN];
   const float* u = s[WF_U];
   const float* v = s[WF_V];
-  const float msftx = col ? s[WF_MSFTX][c] : 1.f, msfty = col ? s[WF_MSFTY][c] : 1.f;
-  const float mut = col ? s[WF_MUT][c] : 1.f;
-  const float mu_tend = col ? s[WF_MU_TEND][c] : 0.f;
+  const float msftx = col ? __ldg(&s[WF_MSFTX][c]) : 1.f, msfty = col ? __ldg(&s[WF_MSFTY][c]) : 1.f;
+  const float mut = col ? __ldg(&s[WF_MUT][c]) : 1.f;
+  const float mu_tend = col ? __ldg(&s[WF_MU_TEND][c]) : 0.f;
+  const float r_msfty = __frcp_rn(msfty), r_mut = __frcp_rn(mut);
   const float ep = g.epssm;
   const float ep1 = (float)(1.0 + (double)ep), em1 = (float)(1.0 - (double)ep);
 
@@ -270,35 +263,39 @@ __global__ void __launch_bounds__(kColTX * kColKT) k_acoustic_col(Grid g, S s, f
   if (inner) {
     const float* u1 = s[WF_U_SAVE];
     const float* v1 = s[WF_V_SAVE];
-    const float* muu = s[WF_MUU];
-    const float* muv = s[WF_MUV];
-    const float* msfuy = s[WF_MSFUY];
-    const float* mvi = s[WF_MSFVX_INV];
+    const float muvn = __ldg(&s[WF_MUV][c + nx]), mvin = __ldg(&s[WF_MSFVX_INV][c + nx]);
+    const float muv0 = __ldg(&s[WF_MUV][c]), mvi0 = __ldg(&s[WF_MSFVX_INV][c]);
+    const float muup = __ldg(&s[WF_MUU][c + 1]), mfup = __ldg(&s[WF_MSFUY][c + 1]);
+    const float muu0 = __ldg(&s[WF_MUU][c]), mfu0 = __ldg(&s[WF_MSFUY][c]);
+    const float r_mfup = __frcp_rn(mfup), r_mfu0 = __frcp_rn(mfu0);
     const float rdx = g.rdx, rdy = g.rdy;
-    #pragma unroll 4
     for (int k = tk; k < kend; k += kColKT) {
-      const size_t p = k * lev + c;
-      A(sm.dw, k) = msftx * msfty *
-                    (rdy * ((__ldg(&v[p + nx]) + __ldg(&muv[c + nx]) * __ldg(&v1[p + nx]) * __ldg(&mvi[c + nx])) - (__ldg(&v[p]) + __ldg(&muv[c]) * __ldg(&v1[p]) * __ldg(&mvi[c]))) +
-                     rdx * ((__ldg(&u[p + 1]) + __ldg(&muu[c + 1]) * __ldg(&u1[p + 1]) / __ldg(&msfuy[c + 1])) - (__ldg(&u[p]) + __ldg(&muu[c]) * __ldg(&u1[p]) / __ldg(&msfuy[c]))));
+      const int p = k * lev + c;
+      sdw[k][tx] = msftx * msfty *
+                   (rdy * ((__ldg(&v[p + nx]) + muvn * __ldg(&v1[p + nx]) * mvin) - (__ldg(&v[p]) + muv0 * __ldg(&v1[p]) * mvi0)) +
+                    rdx * ((__ldg(&u[p + 1]) + divc(muup * __ldg(&u1[p + 1]), mfup, r_mfup)) -
+                           (__ldg(&u[p]) + divc(muu0 * __ldg(&u1[p]), mfu0, r_mfu0))));
     }
   } else if (spec) {
-    #pragma unroll 4
-    for (int k = tk; k < kend; k += kColKT) t[k * lev + c] = t[k * lev + c] + dts * __ldg(&ft[k * lev + c]);
+    for (int k = tk; k < kend; k += kColKT) {
+      const int p = k * lev + c;
+      t[p] = t[p] + dts * __ldg(&ft[p]);
+    }
     if (tk == 0) {
       const float mu = s[WF_MU][c] + dts * mu_tend;
       const float muts = s[WF_MUTS][c] + dts * mu_tend;
       s[WF_MU][c] = mu;
       s[WF_MUTS][c] = muts;
-      sm.mu[tx] = mu;
-      sm.muts[tx] = muts;
+      smu[tx] = mu;
+      smuts[tx] = muts;
     }
   }
   __syncthreads();
-  // --- B: column mass tendency and the ww scan (sequential, reference order)
+  // --- B: column mass tendency (sequential sum, reference order)
   if (inner && tk == 0) {
     float dmdt = 0.f;
-    for (int k = 0; k < kend; ++k) dmdt = dmdt + __ldg(&dnw[k]) * A(sm.dw, k);
+#pragma unroll 8
+    for (int k = 0; k < kend; ++k) dmdt = dmdt + pdnw[k] * sdw[k][tx];
     float mu = s[WF_MU][c];
     const float muave_old = mu;
     mu = mu + dts * (dmdt + mu_tend);
@@ -308,135 +305,149 @@ __global__ void __launch_bounds__(kColTX * kColKT) k_acoustic_col(Grid g, S s, f
     s[WF_MUDF][c] = dmdt + mu_tend;
     s[WF_MUTS][c] = muts;
     s[WF_MUAVE][c] = muave;
-    sm.mu[tx] = mu;
-    sm.muts[tx] = muts;
-    sm.muave[tx] = muave;
+    smu[tx] = mu;
+    smuts[tx] = muts;
+    smuave[tx] = muave;
+    swd[0][tx] = dmdt;  // broadcast dmdt to the level threads
+  }
+  __syncthreads();
+  // --- B2: increments of the ww scan in parallel, then the scan itself
+  if (inner) {
+    const float dmdt = swd[0][tx];
+    for (int k = tk + 1; k < kend; k += kColKT)
+      sww[k][tx] = divc(pdnw[k - 1] * (dmdt + sdw[k - 1][tx] + mu_tend), msfty, r_msfty);
+  }
+  __syncthreads();
+  if (inner && tk == 0) {
     float wprev = ww[c];
-    A(sm.ww, 0) = wprev;
+    sww[0][tx] = wprev;
+#pragma unroll 8
     for (int k = 1; k < kend; ++k) {
-      const float wk = wprev - __ldg(&dnw[k - 1]) * (dmdt + A(sm.dw, k - 1) + mu_tend) / msfty;
-      A(sm.ww, k) = wk;
-      wprev = wk;
+      wprev = wprev - sww[k][tx];
+      sww[k][tx] = wprev;
     }
   }
   __syncthreads();
-  // --- C: final ww (inner: scan - ww1), potential temperature (inner)
+  // --- C: final ww (inner: scan - ww1)
   if (col) {
-    #pragma unroll 4
     for (int k = tk; k < nz; k += kColKT) {
-      const size_t p = k * lev + c;
-      float w = ww[p];
+      const int p = k * lev + c;
+      float w;
       if (inner && k < kend) {
-        w = A(sm.ww, k) - __ldg(&ww1[p]);
+        w = sww[k][tx] - __ldg(&ww1[p]);
         ww[p] = w;
+      } else {
+        w = ww[p];
       }
-      A(sm.ww, k) = w;
+      sww[k][tx] = w;
     }
   }
   __syncthreads();
-  const float muave = inner ? sm.muave[tx] : 0.f;
-  const float muts = mass ? sm.muts[tx] : 1.f;
+  const float muave = inner ? smuave[tx] : 0.f;
+  const float muts = mass ? smuts[tx] : 1.f;
+  const float r_muts = __frcp_rn(muts);
+  // --- C2: potential temperature and t_2ave; D1: wdwn, phi, coefficients
   if (inner) {
     const float cy = (float)(0.5 * g.rdyd), cx = (float)(0.5 * g.rdxd);
-    auto wdtn = [&](int kk) {
-      if (kk == 0 || kk == nz - 1) return 0.f;
-      const size_t q = kk * lev + c;
-      return A(sm.ww, kk) * (__ldg(&fnm[kk]) * __ldg(&t1[q]) + __ldg(&fnp[kk]) * __ldg(&t1[q - lev]));
-    };
     float* t2a = s[WF_T_2SAVE];
-    #pragma unroll 4
     for (int k = tk; k < kend; k += kColKT) {
-      const size_t p = k * lev + c;
+      const int p = k * lev + c;
+      const float t10 = __ldg(&t1[p]);
+      // wdtn(kk) = ww(kk) (fnm t1(kk) + fnp t1(kk-1)), zero at the bottom and top
+      const float wup = (k + 1 == nz - 1) ? 0.f : sww[k + 1][tx] * (pfnm[k + 1] * __ldg(&t1[p + lev]) + pfnp[k + 1] * t10);
+      const float wdn = (k == 0) ? 0.f : sww[k][tx] * (pfnm[k] * t10 + pfnp[k] * __ldg(&t1[p - lev]));
       const float told = t[p];
       float tt = told + msfty * dts * __ldg(&ft[p]);
-      const float hy = cy * (__ldg(&v[p + nx]) * (__ldg(&t1[p + nx]) + __ldg(&t1[p])) - __ldg(&v[p]) * (__ldg(&t1[p]) + __ldg(&t1[p - nx])));
-      const float hx = cx * (__ldg(&u[p + 1]) * (__ldg(&t1[p + 1]) + __ldg(&t1[p])) - __ldg(&u[p]) * (__ldg(&t1[p]) + __ldg(&t1[p - 1])));
-      tt = tt - dts * msfty * (msftx * (hy + hx) + __ldg(&rdnw[k]) * (wdtn(k + 1) - wdtn(k)));
+      const float hy = cy * (__ldg(&v[p + nx]) * (__ldg(&t1[p + nx]) + t10) - __ldg(&v[p]) * (t10 + __ldg(&t1[p - nx])));
+      const float hx = cx * (__ldg(&u[p + 1]) * (__ldg(&t1[p + 1]) + t10) - __ldg(&u[p]) * (t10 + __ldg(&t1[p - 1])));
+      tt = tt - dts * msfty * (msftx * (hy + hx) + prdnw[k] * (wup - wdn));
       t[p] = tt;
-      // time-averaged theta of advance_w (t_2ave)
       float av = 0.5f * (ep1 * tt + em1 * told);
-      av = (av + muave * (float)T0) / (muts * ((float)T0 + __ldg(&t1[p])));
+      av = (av + muave * (float)T0) / (muts * ((float)T0 + t10));
       t2a[p] = av;
-      A(sm.t2av, k) = av;
+      st2av[k][tx] = av;
     }
-    // --- D: right-hand side of the phi equation, tridiagonal coefficients
     const float* ph1 = s[WF_PH_SAVE];
     const float* phb = s[WF_PHB];
-    const float* ph_tend = s[WF_PH_TEND];
-    const float* w = s[WF_W];
-    const float* ph = s[WF_PH];
-    auto wdwn = [&](int kk) {
-      const size_t q = kk * lev + c, qm = q - lev;
-      return 0.5f * (A(sm.ww, kk) + A(sm.ww, kk - 1)) * __ldg(&rdnw[kk - 1]) * (__ldg(&ph1[q]) - __ldg(&ph1[qm]) + __ldg(&phb[q]) - __ldg(&phb[qm]));
-    };
-    const float cw = (float)(0.5 * G * (1.0 - (double)ep));
-    #pragma unroll 4
     for (int k = tk; k < nz; k += kColKT) {
-      const size_t p = k * lev + c;
-      A(sm.ph, k) = ph[p];
-      A(sm.a, k) = __ldg(&s[WF_A][p]);
-      A(sm.alpha, k) = __ldg(&s[WF_ALPHA][p]);
-      A(sm.gamma, k) = __ldg(&s[WF_GAMMA][p]);
+      const int p = k * lev + c;
+      sph[k][tx] = s[WF_PH][p];
+      sa[k][tx] = __ldg(&s[WF_A][p]);
+      salpha[k][tx] = __ldg(&s[WF_ALPHA][p]);
+      sgamma[k][tx] = __ldg(&s[WF_GAMMA][p]);
+      // wdwn(k) = 0.5 (ww(k) + ww(k-1)) rdnw(k-1) (ph1(k) - ph1(k-1) + phb(k) - phb(k-1))
+      if (k >= 1 && k <= kend)
+        swd[k][tx] = 0.5f * (sww[k][tx] + sww[k - 1][tx]) * prdnw[k - 1] *
+                     (__ldg(&ph1[p]) - __ldg(&ph1[p - lev]) + __ldg(&phb[p]) - __ldg(&phb[p - lev]));
+    }
+  }
+  __syncthreads();
+  // --- D2: right-hand side of the phi equation (inner)
+  if (inner) {
+    const float cw = (float)(0.5 * G * (1.0 - (double)ep));
+    for (int k = tk; k < nz; k += kColKT) {
       if (k == 0) {
-        A(sm.rhs, 0) = 0.f;
+        srhs[0][tx] = 0.f;
         continue;
       }
-      float r = dts * (__ldg(&ph_tend[p]) + cw * w[p]);
-      if (k < kend) r = r - dts * (__ldg(&fnm[k]) * wdwn(k + 1) + __ldg(&fnp[k]) * wdwn(k));
-      A(sm.rhs, k) = ph[p] + msfty * r / mut;
+      const int p = k * lev + c;
+      float r = dts * (__ldg(&s[WF_PH_TEND][p]) + cw * s[WF_W][p]);
+      if (k < kend) r = r - dts * (pfnm[k] * swd[k + 1][tx] + pfnp[k] * swd[k][tx]);
+      srhs[k][tx] = sph[k][tx] + divc(msfty * r, mut, r_mut);
     }
   }
   __syncthreads();
   // --- E: explicit part of w (inner)
   if (inner) {
-    const float* w = s[WF_W];
     const float* c2a = s[WF_C2A];
-    const float* cqw = s[WF_CQW];
     const float* alt = s[WF_ALT];
-    const float* rw_tend = s[WF_RW_TEND];
     const float msft_inv = 1.0f / msfty;
     const float cp = (float)(0.5 * (double)dts * G);
     const float cq = (float)((double)dts * G);
-    #pragma unroll 4
+    if (tk == 0) {  // lower boundary: w from the terrain slope and near-surface winds
+      const float* ht = s[WF_HT];
+      auto cv = [&](int cc) { return g.cf1 * __ldg(&v[cc]) + g.cf2 * __ldg(&v[lev + cc]) + g.cf3 * __ldg(&v[2 * lev + cc]); };
+      auto cu = [&](int cc) { return g.cf1 * __ldg(&u[cc]) + g.cf2 * __ldg(&u[lev + cc]) + g.cf3 * __ldg(&u[2 * lev + cc]); };
+      const float h0 = __ldg(&ht[c]);
+      sdw[0][tx] = msfty * 0.5f * g.rdy * ((__ldg(&ht[c + nx]) - h0) * cv(c + nx) + (h0 - __ldg(&ht[c - nx])) * cv(c)) +
+                   msftx * 0.5f * g.rdx * ((__ldg(&ht[c + 1]) - h0) * cu(c + 1) + (h0 - __ldg(&ht[c - 1])) * cu(c));
+    }
     for (int k = tk; k <= kend; k += kColKT) {
-      const size_t p = k * lev + c;
+      if (k < 1) continue;
+      const int p = k * lev + c;
+      const float wk = s[WF_W][p], rwk = __ldg(&s[WF_RW_TEND][p]);
+      const float c2m = __ldg(&c2a[p - lev]), alm = __ldg(&alt[p - lev]);
+      const float rdnw_m = prdnw[k - 1];
       float wl;
-      if (k == 0) {  // lower boundary: w from the terrain slope and near-surface winds
-        const float* ht = s[WF_HT];
-        auto cv = [&](int cc) { return g.cf1 * __ldg(&v[cc]) + g.cf2 * __ldg(&v[lev + cc]) + g.cf3 * __ldg(&v[2 * lev + cc]); };
-        auto cu = [&](int cc) { return g.cf1 * __ldg(&u[cc]) + g.cf2 * __ldg(&u[lev + cc]) + g.cf3 * __ldg(&u[2 * lev + cc]); };
-        wl = msfty * 0.5f * g.rdy * ((__ldg(&ht[c + nx]) - __ldg(&ht[c])) * cv(c + nx) + (__ldg(&ht[c]) - __ldg(&ht[c - nx])) * cv(c)) +
-             msftx * 0.5f * g.rdx * ((__ldg(&ht[c + 1]) - __ldg(&ht[c])) * cu(c + 1) + (__ldg(&ht[c]) - __ldg(&ht[c - 1])) * cu(c));
-      } else if (k < kend) {
-        const float X1 = __ldg(&c2a[p]) * __ldg(&rdnw[k]) / mut *
-                         (ep1 * (A(sm.rhs, k + 1) - A(sm.rhs, k)) + em1 * (A(sm.ph, k + 1) - A(sm.ph, k)));
-        const float X2 = __ldg(&c2a[p - lev]) * __ldg(&rdnw[k - 1]) / mut *
-                         (ep1 * (A(sm.rhs, k) - A(sm.rhs, k - 1)) + em1 * (A(sm.ph, k) - A(sm.ph, k - 1)));
-        wl = w[p] + dts * __ldg(&rw_tend[p]) + msft_inv * __ldg(&cqw[p]) * (cp * __ldg(&rdn[k]) * (X1 - X2)) +
-             cq * msft_inv *
-                 (__ldg(&rdn[k]) * (__ldg(&c2a[p]) * __ldg(&alt[p]) * A(sm.t2av, k) - __ldg(&c2a[p - lev]) * __ldg(&alt[p - lev]) * A(sm.t2av, k - 1)) - muave);
+      if (k < kend) {
+        const float c2k = __ldg(&c2a[p]), alk = __ldg(&alt[p]);
+        const float X1 = divc(c2k * prdnw[k], mut, r_mut) * (ep1 * (srhs[k + 1][tx] - srhs[k][tx]) + em1 * (sph[k + 1][tx] - sph[k][tx]));
+        const float X2 = divc(c2m * rdnw_m, mut, r_mut) * (ep1 * (srhs[k][tx] - srhs[k - 1][tx]) + em1 * (sph[k][tx] - sph[k - 1][tx]));
+        wl = wk + dts * rwk + msft_inv * __ldg(&s[WF_CQW][p]) * (cp * prdn[k] * (X1 - X2)) +
+             cq * msft_inv * (prdn[k] * (c2k * alk * st2av[k][tx] - c2m * alm * st2av[k - 1][tx]) - muave);
       } else {
-        const size_t pm = p - lev;
         const float cm = (float)(-0.5 * (double)dts * G);
-        wl = w[p] + dts * __ldg(&rw_tend[p]) +
-             msft_inv * (cm / mut * (__ldg(&rdnw[kend - 1]) * __ldg(&rdnw[kend - 1])) * 2.0f * __ldg(&c2a[pm]) *
-                             (ep1 * (A(sm.rhs, kend) - A(sm.rhs, kend - 1)) + em1 * (A(sm.ph, kend) - A(sm.ph, kend - 1))) -
-                         cq * (2.0f * __ldg(&rdnw[kend - 1]) * __ldg(&c2a[pm]) * __ldg(&alt[pm]) * A(sm.t2av, kend - 1) + muave));
+        wl = wk + dts * rwk +
+             msft_inv * (divc(cm, mut, r_mut) * (rdnw_m * rdnw_m) * 2.0f * c2m *
+                             (ep1 * (srhs[kend][tx] - srhs[kend - 1][tx]) + em1 * (sph[kend][tx] - sph[kend - 1][tx])) -
+                         cq * (2.0f * rdnw_m * c2m * alm * st2av[kend - 1][tx] + muave));
       }
-      A(sm.dw, k) = wl;
+      sdw[k][tx] = wl;
     }
   }
   __syncthreads();
   // --- F: Thomas sweeps (sequential per column)
   if (inner && tk == 0) {
-    float prev = A(sm.dw, 0);
+    float prev = sdw[0][tx];
+#pragma unroll 8
     for (int k = 1; k <= kend; ++k) {
-      prev = (A(sm.dw, k) - A(sm.a, k) * prev) * A(sm.alpha, k);
-      A(sm.dw, k) = prev;
+      prev = (sdw[k][tx] - sa[k][tx] * prev) * salpha[k][tx];
+      sdw[k][tx] = prev;
     }
+#pragma unroll 8
     for (int k = kend - 1; k >= 1; --k) {
-      prev = A(sm.dw, k) - A(sm.gamma, k) * prev;
-      A(sm.dw, k) = prev;
+      prev = sdw[k][tx] - sgamma[k][tx] * prev;
+      sdw[k][tx] = prev;
     }
   }
   __syncthreads();
@@ -446,42 +457,42 @@ __global__ void __launch_bounds__(kColTX * kColKT) k_acoustic_col(Grid g, S s, f
     float* w = s[WF_W];
     const float* ph1 = s[WF_PH_SAVE];
     const float* phb = s[WF_PHB];
-    const float* wsave = s[WF_W_SAVE];
     const float gf = (float)G;
+    constexpr float r_g = 1.0f / (float)G, r_hd = 1.0f / 5000.0f;
     const float hdepth = 5000.0f;
     const float dampmag = (float)((double)dts * 0.2);
-    const float htop = (__ldg(&ph1[kend * lev + c]) + __ldg(&phb[kend * lev + c])) / gf;
+    const float htop = divc(__ldg(&ph1[kend * lev + c]) + __ldg(&phb[kend * lev + c]), gf, r_g);
     const float hbot = htop - hdepth;
     const float hpi = (float)(0.5 * 3.14159265359);
-    #pragma unroll 4
     for (int k = tk; k < nz; k += kColKT) {
-      const size_t p = k * lev + c;
+      const int p = k * lev + c;
       if (k == 0) {
-        w[c] = A(sm.dw, 0);
+        w[c] = sdw[0][tx];
         continue;
       }
-      const float hk = (__ldg(&ph1[p]) + __ldg(&phb[p])) / gf;
+      const float hk = divc(__ldg(&ph1[p]) + __ldg(&phb[p]), gf, r_g);
       float dwd = 0.f;
       if (hk >= hbot) {
-        const float sn = sinf(hpi * (hk - hbot) / hdepth);
+        const float sn = sinf(divc(hpi * (hk - hbot), hdepth, r_hd));
         dwd = dampmag * (sn * sn);
       }
-      const float wk = (A(sm.dw, k) - dwd * mut * __ldg(&wsave[p])) / (1.0f + dwd);
+      const float num = sdw[k][tx] - dwd * mut * __ldg(&s[WF_W_SAVE][p]);
+      const float wk = dwd == 0.f ? num : num / (1.0f + dwd);  // x / 1 == x
       w[p] = wk;
-      const float phk = A(sm.rhs, k) + msfty * 0.5f * dts * gf * ep1 * wk / muts;
+      const float phk = srhs[k][tx] + divc(msfty * 0.5f * dts * gf * ep1 * wk, muts, r_muts);
       ph[p] = phk;
-      A(sm.ph, k) = phk;
+      sph[k][tx] = phk;
     }
   } else if (spec) {
     const float mu_old = muts - dts * mu_tend;
     const float* ph_save = s[WF_PH_SAVE];
     const float* ph_tend = s[WF_PH_TEND];
-    #pragma unroll 4
     for (int k = tk; k < nz; k += kColKT) {
-      const size_t p = k * lev + c;
-      const float phk = ph[p] * mu_old / muts + dts * __ldg(&ph_tend[p]) / muts + ph_save[p] * (mu_old / muts - 1.0f);
+      const int p = k * lev + c;
+      const float phk = divc(ph[p] * mu_old, muts, r_muts) + divc(dts * __ldg(&ph_tend[p]), muts, r_muts) +
+                        __ldg(&ph_save[p]) * (divc(mu_old, muts, r_muts) - 1.0f);
       ph[p] = phk;
-      A(sm.ph, k) = phk;
+      sph[k][tx] = phk;
     }
   }
   if (col) {
@@ -489,19 +500,22 @@ __global__ void __launch_bounds__(kColTX * kColKT) k_acoustic_col(Grid g, S s, f
     float* rv_m = s[WF_RV_M];
     float* ww_m = s[WF_WW_M];
     const bool ur = j < jde - 1, vr = i < ide - 1, wr = ur && vr;
-    #pragma unroll 4
+    const bool last = iteration == nsub;
+    const float muuc = last && ur ? __ldg(&s[WF_MUU][c]) : 0.f, mfuc = last && ur ? __ldg(&s[WF_MSFUY][c]) : 1.f;
+    const float muvc = last && vr ? __ldg(&s[WF_MUV][c]) : 0.f, mvic = last && vr ? __ldg(&s[WF_MSFVX_INV][c]) : 0.f;
+    const float r_nsub = __frcp_rn((float)nsub), r_mfuc = __frcp_rn(mfuc);
     for (int k = tk; k < nz; k += kColKT) {
-      const size_t p = k * lev + c;
+      const int p = k * lev + c;
       float a = iteration == 1 ? 0.f : ru_m[p];
       float b = iteration == 1 ? 0.f : rv_m[p];
       float cc = iteration == 1 ? 0.f : ww_m[p];
       if (k < nz - 1 && ur) a = a + __ldg(&u[p]);
       if (k < nz - 1 && vr) b = b + __ldg(&v[p]);
-      if (wr) cc = cc + A(sm.ww, k);
-      if (iteration == nsub) {
-        if (k < nz - 1 && ur) a = a / (float)nsub + s[WF_MUU][c] * s[WF_U_SAVE][p] / s[WF_MSFUY][c];
-        if (k < nz - 1 && vr) b = b / (float)nsub + s[WF_MUV][c] * s[WF_V_SAVE][p] * s[WF_MSFVX_INV][c];
-        if (wr) cc = cc / (float)nsub + __ldg(&ww1[p]);
+      if (wr) cc = cc + sww[k][tx];
+      if (last) {
+        if (k < nz - 1 && ur) a = divc(a, (float)nsub, r_nsub) + divc(muuc * __ldg(&s[WF_U_SAVE][p]), mfuc, r_mfuc);
+        if (k < nz - 1 && vr) b = divc(b, (float)nsub, r_nsub) + muvc * __ldg(&s[WF_V_SAVE][p]) * mvic;
+        if (wr) cc = divc(cc, (float)nsub, r_nsub) + __ldg(&ww1[p]);
       }
       ru_m[p] = a;
       rv_m[p] = b;
@@ -511,44 +525,48 @@ __global__ void __launch_bounds__(kColTX * kColKT) k_acoustic_col(Grid g, S s, f
   __syncthreads();
   // --- H: calc_p_rho with divergence damping (mass columns)
   if (mass) {
-    const float mu = sm.mu[tx];
-    const float* alt = s[WF_ALT];
-    const float* c2a = s[WF_C2A];
+    const float mu = smu[tx];
     float* al = s[WF_AL];
     float* pp = s[WF_P];
     float* pm1 = s[WF_PM1];
-    #pragma unroll 4
     for (int k = tk; k < kend; k += kColKT) {
-      const size_t p = k * lev + c;
-      const float altk = __ldg(&alt[p]), t1k = __ldg(&t1[p]);
-      const float alk = -1.0f / muts * (altk * mu + __ldg(&rdnw[k]) * (A(sm.ph, k + 1) - A(sm.ph, k)));
+      const int p = k * lev + c;
+      const float altk = __ldg(&s[WF_ALT][p]), t1k = __ldg(&t1[p]);
+      const float alk = -r_muts * (altk * mu + prdnw[k] * (sph[k + 1][tx] - sph[k][tx]));
       al[p] = alk;
-      const float pnew = __ldg(&c2a[p]) * (altk * (t[p] - mu * t1k) / (muts * ((float)T0 + t1k)) - alk);
+      const float pnew = __ldg(&s[WF_C2A][p]) * (altk * (t[p] - mu * t1k) / (muts * ((float)T0 + t1k)) - alk);
       pp[p] = pnew + g.smdiv * (pnew - pm1[p]);
       pm1[p] = pnew;
     }
   }
 }
 
-// zero_grad_bdy(w) on the specified rows, all levels (wrf_boundary.py:358-400)
+// zero_grad_bdy(w) on the specified rows, all levels (wrf_boundary.py:358-400);
+// one thread per ring point: rows jbs and jbe-1 (columns [ibs, ibe)), then
+// columns ibs and ibe-1 (rows (jbs, jbe-1))
 __global__ void k_zero_grad_w(Grid g, S s) {
-  WRF_POINT_INDEX(g, k, j, i);
-  const int nx = g.nx;
   const int ibs = g.ids, ibe = g.ide - 1, jbs = g.jds, jbe = g.jde - 1;
-  int sj = -1, si = -1;
-  if (j == jbs || j == jbe - 1) {
-    if (i >= ibs && i < ibe) {
-      sj = (j == jbs) ? jbs + 1 : jbe - 2;
-      si = (i == ibs) ? ibs + 1 : (i == ibe - 1 ? ibe - 2 : i);
-    }
-  } else if (j > jbs && j < jbe - 1 && (i == ibs || i == ibe - 1)) {
+  const int nxr = ibe - ibs, nyr = jbe - jbs - 2;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (r >= 2 * nxr + 2 * nyr) return;
+  int j, i, sj, si;
+  if (r < 2 * nxr) {
+    const bool top = r >= nxr;
+    i = ibs + (top ? r - nxr : r);
+    j = top ? jbe - 1 : jbs;
+    sj = top ? jbe - 2 : jbs + 1;
+    si = (i == ibs) ? ibs + 1 : (i == ibe - 1 ? ibe - 2 : i);
+  } else {
+    const int q = r - 2 * nxr;
+    const bool east = q >= nyr;
+    j = jbs + 1 + (east ? q - nyr : q);
+    i = east ? ibe - 1 : ibs;
     sj = j;
-    si = (i == ibs) ? ibs + 1 : ibe - 2;
+    si = east ? ibe - 2 : ibs + 1;
   }
-  if (sj < 0) return;
   float* w = s[WF_W];
-  const size_t base = (size_t)k * g.ny * nx;
-  w[base + (size_t)j * nx + i] = w[base + (size_t)sj * nx + si];
+  const size_t base = (size_t)k * g.ny * g.nx;
+  w[base + (size_t)j * g.nx + i] = w[base + (size_t)sj * g.nx + si];
 }
 
 __global__ void k_mu_uv_1(Grid g, S s) {
@@ -605,17 +623,10 @@ int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cu
 int launch_substep(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_advance_uv<<<point_grid(g, b3), b3, 0, st>>>(g, s, dts);
-  const size_t smem = acoustic_col_smem(g.nz);
-  static unsigned attr_set = 0;  // one bit per device
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (smem > 48 * 1024 && dev < 32 && !(attr_set & (1u << dev))) {
-    cudaFuncSetAttribute(k_acoustic_col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set |= 1u << dev;
-  }
   const dim3 gc((g.ide - g.ids + kColTX - 1) / kColTX, g.jde - g.jds);
-  k_acoustic_col<<<gc, kColTX * kColKT, smem, st>>>(g, s, dts, iteration, nsub);
-  k_zero_grad_w<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  k_acoustic_col<<<gc, kColTX * kColKT, 0, st>>>(g, s, dts, iteration, nsub);
+  const int nring = 2 * (g.ide - 1 - g.ids) + 2 * (g.jde - 1 - g.jds - 2);
+  k_zero_grad_w<<<dim3((nring + 127) / 128, g.nz), 128, 0, st>>>(g, s);
   return 3;
 }
 
