@@ -56,7 +56,7 @@ NCU_TRAFFIC = {}
 def parse():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", type=int, default=1, help="synthetic workload id (1: 240x240x41)")
@@ -171,15 +171,20 @@ def run_reference(a):
 
 # --------------------------------------------------------------------- GPU arm
 
+# compulsory 3-D field passes of k_acoustic_col (one acoustic substep): reads
+# u v u_save v_save t t_tend t_save ww ww1 ph_save phb ph a alpha gamma
+# ph_tend w c2a alt cqw rw_tend w_save pm1 (23) + ru_m rv_m ww_m after the
+# first substep of a stage (3); writes t t_2save ww ph w ru_m rv_m ww_m al p
+# pm1 (11).  A step has 3 first substeps and 4 later ones.
+COL_PASSES_PER_STEP = 3 * (23 + 11) + 4 * (26 + 11)
+COL_LAUNCHES_PER_STEP = 7
+
+
 def algorithmic_bytes(g):
-    """Compulsory HBM bytes of the kernels whose roofline is reported:
-    fp32 3-D passes x 4 B x points (+ the 2-D precipitation fields)."""
+    """Compulsory HBM bytes per launch of the dominant kernel: fp32 3-D
+    passes x 4 B x points of the allocation."""
     n3 = g.nx * g.ny * g.nz
-    n2 = g.nx * g.ny
-    # k_physics: reads t p pb al alb ph phb + 6 species (13 fields), writes t,
-    # 3 diabatic tendencies, 6 species, al, p (12 fields); 7 2-D precip
-    # fields read+write and muts, mu
-    return {"k_physics": 25 * 4 * n3 + (2 * 7 + 2) * 4 * n2}
+    return {"k_acoustic_col": COL_PASSES_PER_STEP / COL_LAUNCHES_PER_STEP * 4 * n3}
 
 
 def run_ours(a):
@@ -201,16 +206,7 @@ def run_ours(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from pywrf_b200.replicas import barrier, job_rate, max_over_ranks
 
     spec = synthetic.spec_for_config(a.config, seed=rank)
     g = synthetic.grid_for(spec)
@@ -240,7 +236,7 @@ def run_ours(a):
     barrier()
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms)
-    value = world * a.steps / (ms_max / 1e3)
+    value = job_rate(a.steps, ms_max, world)
     clocks = cs.summary()
 
     # per-phase device time of eager steps (probe events on the launch stream)
@@ -260,20 +256,22 @@ def run_ours(a):
         prev = start
         for name, e in evs:
             key = name.split(".", 1)[1] if name.startswith("s") and "." in name else name
-            key = "sub" if key.startswith("sub") else key
+            if key.startswith("sub"):
+                key = "sub." + key.split(".")[1] if key.count(".") else "sub.bc"
             phase_ms[key] = phase_ms.get(key, 0.0) + prev.elapsed_time(e) / a.phase_steps
             prev = e
     nan = it.status()["nan_p"]
 
-    # roofline of the dominant single-kernel phase (k_physics = phase "mp")
+    # roofline of the dominant kernel, k_acoustic_col (the "sub.col" phases:
+    # that kernel alone, 7 launches per step)
     hbm, peak_kind = peaks()
     ab = algorithmic_bytes(g)
-    k_ms = phase_ms.get("mp", float("nan"))
-    achieved = ab["k_physics"] / (k_ms / 1e3) / 1e9
-    traffic = NCU_TRAFFIC.get("k_physics")
-    roofline = {"kernel": "k_physics", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+    k_ms = phase_ms.get("sub.col", float("nan")) / COL_LAUNCHES_PER_STEP
+    achieved = ab["k_acoustic_col"] / (k_ms / 1e3) / 1e9
+    traffic = NCU_TRAFFIC.get("k_acoustic_col")
+    roofline = {"kernel": "k_acoustic_col", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_kind,
-                "algorithmic_bytes": ab["k_physics"], "kernel_ms": k_ms}
+                "algorithmic_bytes": ab["k_acoustic_col"], "kernel_ms": k_ms}
     step_bytes = 662 * 4 * g.nx * g.ny * g.nz
     step_ms = ms_max / a.steps
     whole = {"ledger_bytes_per_step": step_bytes, "achieved_gbs": step_bytes / (step_ms / 1e3) / 1e9,
@@ -303,7 +301,7 @@ def run_ours(a):
         barrier()
         e_ms = max_over_ranks(h0.elapsed_time(h1))
         nbytes = sum(host[k].numel() * host[k].element_size() for k in E2E_FIELDS)
-        e2e = {"value": world * ke / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+        e2e = {"value": job_rate(ke, e_ms, world), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": ke}
 
     cpu = None

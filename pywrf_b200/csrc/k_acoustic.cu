@@ -620,14 +620,22 @@ int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cu
   return 4;
 }
 
-int launch_substep(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st) {
+int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_advance_uv<<<point_grid(g, b3), b3, 0, st>>>(g, s, dts);
+  return 1;
+}
+
+int launch_acoustic_col(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st) {
   const dim3 gc((g.ide - g.ids + kColTX - 1) / kColTX, g.jde - g.jds);
   k_acoustic_col<<<gc, kColTX * kColKT, 0, st>>>(g, s, dts, iteration, nsub);
+  return 1;
+}
+
+int launch_zero_grad_w(const Grid& g, const S& s, cudaStream_t st) {
   const int nring = 2 * (g.ide - 1 - g.ids) + 2 * (g.jde - 1 - g.jds - 2);
   k_zero_grad_w<<<dim3((nring + 127) / 128, g.nz), 128, 0, st>>>(g, s);
-  return 3;
+  return 1;
 }
 
 int launch_small_step_finish(const Grid& g, const S& s, float dts, int nsub, int rk_step, cudaStream_t st) {

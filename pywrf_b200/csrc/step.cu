@@ -186,7 +186,15 @@ struct Driver {
       snprintf(tag, sizeof tag, "s%d.acprep", rk);
       phase(tag);
       for (int it = 1; it <= nsub; ++it) {
-        n += launch_substep(g, s, dts_rk, it, nsub, st);
+        // advance_uv, then the column update (mu/theta, w/phi, sumflux,
+        // p/al), then zero_grad_bdy(w) and the halo copies
+        n += launch_advance_uv(g, s, dts_rk, st);
+        snprintf(tag, sizeof tag, "s%d.sub%d.uv", rk, it);
+        phase(tag);
+        n += launch_acoustic_col(g, s, dts_rk, it, nsub, st);
+        snprintf(tag, sizeof tag, "s%d.sub%d.col", rk, it);
+        phase(tag);
+        n += launch_zero_grad_w(g, s, st);
         bc({{WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}}, {{WF_MUTS, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
         snprintf(tag, sizeof tag, "s%d.sub%d", rk, it);
         phase(tag);

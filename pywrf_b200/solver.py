@@ -121,7 +121,9 @@ class WrfSolver:
         class _View(dict):
             def __missing__(self, key):
                 v = ds[key]
-                v = np.asarray(getattr(v, "data", v))
+                if not isinstance(v, np.ndarray):   # xarray DataArray (or alike): its .data
+                    v = getattr(v, "data", v)
+                v = np.asarray(v)
                 self[key] = v
                 return v
         return _View()

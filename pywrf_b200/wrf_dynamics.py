@@ -1,0 +1,53 @@
+"""Drop-in for ``pywrf.wrf_dynamics.advect_scalar`` (reference signature).
+
+``advect_scalar(...)`` takes the arguments of the reference function
+(pywrf/wrf_dynamics.py:1841-1850), adds the flux-form advection of ``field``
+to ``tendency`` on the GPU through ``wrf_advect_scalar``
+(include/pywrf_b200.h) and returns ``tendency``.  Tensors must be contiguous
+float32 CUDA tensors; there is no CPU path.  The index arguments must be the
+solver's (the 5-cell frame with tile = patch = domain); ``rdzw`` is the 1-D
+``rdnw`` profile the solver passes, ``fzm``/``fzp`` the ``fnm``/``fnp``
+profiles.  ``field_old``, ``c1``, ``c2``, ``mut``, ``time_step``, ``msfux``,
+``msfuy``, ``msfvx`` and ``msfvy`` are accepted and unused, as in the reference
+(its map-factor form uses ``msftx`` only).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _native as N
+from .config import Grid
+from .state import make_cgrid
+
+
+def _need(name, t):
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+        raise TypeError(f"{name}: a contiguous float32 CUDA tensor is required (no CPU path)")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def advect_scalar(field, field_old, tendency, ru, rv, rom, c1, c2, mut, time_step, msfux, msfuy, msfvx, msfvy,
+                  msftx, msfty, fzm, fzp, rdx, rdy, rdzw, ids, ide, jds, jde, kds, kde, ims, ime, jms, jme,
+                  kms, kme, its, ite, jts, jte, kts, kte):
+    """advect_scalar (pywrf/wrf_dynamics.py:1841-2028) on the GPU."""
+    nz, ny, nx = field.shape
+    if (ids, jds, ide, jde) != (5, 5, nx - 5, ny - 5) or (its, ite, jts, jte) != (ids, ide, jds, jde) \
+            or (kts, kte) != (0, nz):
+        raise NotImplementedError("advect_scalar: only the solver's 5-cell frame with tile = domain is supported")
+    for nm, t in (("tendency", tendency), ("ru", ru), ("rv", rv), ("rom", rom)):
+        if tuple(t.shape) != (nz, ny, nx):
+            raise ValueError(f"{nm}: shape {tuple(t.shape)} != {(nz, ny, nx)}")
+    g = Grid.make(nx, ny, nz, 1.0 / float(rdx), 1.0 / float(rdy), 1.0)
+    cg = make_cgrid(g, {"cf1": 0.0, "cf2": 0.0, "cf3": 0.0, "cfn": 0.0, "cfn1": 0.0})
+    # the kernels read rdx/rdy as float(1/dx): rebuild dx so that 1/dx == rdx
+    cg.dx = 1.0 / float(rdx)
+    cg.dy = 1.0 / float(rdy)
+    with torch.cuda.device(field.device):
+        rc = N.lib().wrf_advect_scalar(ctypes.byref(cg), _need("field", field), _need("tendency", tendency),
+                                       _need("ru", ru), _need("rv", rv), _need("rom", rom), _need("msftx", msftx),
+                                       _need("fzm", fzm), _need("fzp", fzp), _need("rdzw", rdzw),
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    N.check(rc, "wrf_advect_scalar")
+    return tendency

@@ -1,0 +1,104 @@
+"""The reference-signature shims (pywrf_b200.wrf_physics / wrf_dynamics)
+called as the reference solver calls them, checked against the oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import SMALL, rel_l2
+from oracle import dynamics as OD
+from oracle import physics as OP
+from oracle.model import OracleModel
+from pywrf_b200 import synthetic, wrf_dynamics, wrf_physics
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def stepped():
+    if not torch.cuda.is_available():
+        pytest.fail("these tests need a CUDA device")
+    spec = synthetic.CaseSpec(**SMALL)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    m = OracleModel(g, inputs, bdy, np.float64)
+    m.run(1)
+    return g, m.st
+
+
+def test_wsm6_shim_with_the_solver_arguments(stepped):
+    g, s = stepped
+    s = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in s.items()}
+    OP.moist_physics_prep_em(g, s)
+    names = ("th_phy", "q1", "q2", "q3", "q4", "q5", "q6", "rho", "pi_phy", "p_phy", "dz8w")
+    base = {k: (s["moist"][int(k[1])] if k.startswith("q") else s[k]).copy() for k in names}
+    pre2 = {k: s[k].copy() for k in ("rainnc", "rainncv", "snownc", "snowncv", "graupelnc", "graupelncv", "sr")}
+
+    def oracle(dtype):
+        a = {k: v.astype(dtype) for k, v in base.items()}
+        b = {k: v.astype(dtype) for k, v in pre2.items()}
+        OP.wsm6(g, a["th_phy"], a["q1"], a["q2"], a["q3"], a["q4"], a["q5"], a["q6"], a["rho"], a["pi_phy"],
+                a["p_phy"], a["dz8w"], float(g.dt), b["rainnc"], b["rainncv"], b["snownc"], b["snowncv"],
+                b["graupelnc"], b["graupelncv"], b["sr"])
+        return a, b
+
+    o64, _ = oracle(np.float64)
+    o32, _ = oracle(np.float32)
+    d = {k: torch.tensor(v, dtype=torch.float32, device="cuda") for k, v in base.items()}
+    d2 = {k: torch.tensor(v, dtype=torch.float32, device="cuda") for k, v in pre2.items()}
+    refl = torch.zeros_like(d["th_phy"])
+    ids, ide, jds, jde, kds, kde = g.ids + 1, g.ide - 1, g.jds + 1, g.jde - 1, 0, g.nz
+    out = wrf_physics.wsm6(d["th_phy"], d["q1"], d["q2"], d["q3"], d["q4"], d["q5"], d["q6"], d["rho"], d["pi_phy"],
+                           d["p_phy"], d["dz8w"], float(g.dt), 9.81, 1004.5, 1846.4, 287.0, 461.6,
+                           273.149993896484375, 0.608362436294555664, 0.621750414371490479, 1.0e-15, 2850000.0,
+                           2500000.0, 350000.0, 1.28, 1000.0, 4190.0, 2106.0, 610.78,
+                           d2["rainnc"], d2["rainncv"], d2["snownc"], d2["snowncv"], d2["sr"], refl, 1, 1,
+                           d2["graupelnc"], d2["graupelncv"], 0, 0, 0, 0, 0, 0,
+                           ids, ide, jds, jde, kds, kde, 0, g.nx, 0, g.ny, 0, g.nz, ids, ide, jds, jde, kds, kde)
+    torch.cuda.synchronize()
+    assert out[0] is d["th_phy"] and out[7] is d2["rainnc"] and out[11] is d2["graupelnc"]
+    for k in names[:7]:
+        err, floor = rel_l2(d[k].cpu().numpy(), o64[k]), rel_l2(o32[k], o64[k])
+        assert err <= 3.0 * floor + 1e-7, (k, err, floor)
+
+
+def test_wsm6_shim_rejects_other_tiles_and_constants(stepped):
+    g, _ = stepped
+    z = torch.zeros((g.nz, g.ny, g.nx), device="cuda")
+    z2 = torch.zeros((g.ny, g.nx), device="cuda")
+    args = [z] * 11 + [45.0, 9.81, 1004.5, 1846.4, 287.0, 461.6, 273.149993896484375, 0.608362436294555664,
+                       0.621750414371490479, 1.0e-15, 2850000.0, 2500000.0, 350000.0, 1.28, 1000.0, 4190.0, 2106.0,
+                       610.78] + [z2] * 5 + [z, 1, 1] + [z2] * 2 + [0] * 6
+    with pytest.raises(NotImplementedError):
+        wrf_physics.wsm6(*args, 5, g.nx - 5, 5, g.ny - 5, 0, g.nz, 0, g.nx, 0, g.ny, 0, g.nz, 5, g.nx - 5, 5,
+                         g.ny - 5, 0, g.nz)
+    bad = list(args)
+    bad[12] = 9.8
+    with pytest.raises(ValueError):
+        wrf_physics.wsm6(*bad, 6, g.nx - 6, 6, g.ny - 6, 0, g.nz, 0, g.nx, 0, g.ny, 0, g.nz, 6, g.nx - 6, 6,
+                         g.ny - 6, 0, g.nz)
+    with pytest.raises(TypeError):
+        wrf_physics.wsm6(*([z.cpu()] + args[1:]), 6, g.nx - 6, 6, g.ny - 6, 0, g.nz, 0, g.nx, 0, g.ny, 0, g.nz,
+                         6, g.nx - 6, 6, g.ny - 6, 0, g.nz)
+
+
+def test_advect_scalar_shim_with_the_solver_arguments(stepped):
+    g, s = stepped
+    ref64 = np.zeros_like(s["t"])
+    OD.advect_scalar(g, s["t"], ref64, s["ru"], s["rv"], s["ww"], s["msftx"], s["fnm"], s["fnp"], s["rdnw"])
+    s32 = {k: s[k].astype(np.float32) for k in ("t", "ru", "rv", "ww", "msftx", "fnm", "fnp", "rdnw")}
+    ref32 = np.zeros_like(s32["t"])
+    OD.advect_scalar(g, s32["t"], ref32, s32["ru"], s32["rv"], s32["ww"], s32["msftx"], s32["fnm"], s32["fnp"],
+                     s32["rdnw"])
+    d = {k: torch.tensor(v, device="cuda") for k, v in s32.items()}
+    tend = torch.zeros_like(d["t"])
+    one = torch.ones((g.ny, g.nx), device="cuda")
+    idx = (g.ids, g.ide, g.jds, g.jde, 0, g.nz, 0, g.nx, 0, g.ny, 0, g.nz, g.ids, g.ide, g.jds, g.jde, 0, g.nz)
+    out = wrf_dynamics.advect_scalar(d["t"], d["t"], tend, d["ru"], d["rv"], d["ww"], None, None, None, g.dt,
+                                     one, one, one, one, d["msftx"], one, d["fnm"], d["fnp"], 1.0 / g.dx,
+                                     1.0 / g.dy, d["rdnw"], *idx)
+    torch.cuda.synchronize()
+    assert out is tend
+    err, floor = rel_l2(tend.cpu().numpy(), ref64), rel_l2(ref32, ref64)
+    assert err <= 3.0 * floor + 1e-9, (err, floor)

@@ -159,6 +159,29 @@ def test_config1_one_step_vs_reference_summary():
     assert it.status()["nan_p"] == 0
 
 
+def test_wrf_solver_drop_in(small):
+    """pywrf_b200.WrfSolver as the reference is used: subclass, override
+    _load_datasets, solve(); the fields match the fp64 reference fixtures."""
+    from pywrf_b200 import WrfSolver
+
+    spec = synthetic.CaseSpec(**SMALL)
+    inputs, bdy = synthetic.build(spec)
+
+    class Run(WrfSolver):
+        def _load_datasets(self):
+            return inputs, bdy, None
+
+    res = Run(nsteps=SMALL["nsteps"], dt=spec.dt, p_top=spec.p_top, dx=spec.dx, dy=spec.dx).solve()
+    assert set(res) == {"u", "v", "w", "t", "ph", "mu", "moist"}
+    assert all(t.is_cuda for t in res.values())
+    r64, r32 = load_npz("small_ref64.npz"), load_npz("small_ref32.npz")
+    got = {k: res[k].cpu().numpy() for k in ("u", "v", "w", "t", "ph", "mu")}
+    got["qv"] = res["moist"][1].cpu().numpy()
+    for k, v in got.items():
+        err, floor = rel_l2(v, r64[k]), rel_l2(r32[k], r64[k])
+        assert err <= K_FLOOR * floor + ABS_FLOOR, (k, err, floor)
+
+
 def test_graph_replay_equals_eager_bitwise(small):
     g, inputs, bdy = small
     a, _ = cuda_run(g, inputs, bdy, 2, graph=False)
