@@ -135,6 +135,20 @@ int wrf_wsm6(const WrfGrid* g, float* th, float* qv, float* qc, float* qr, float
              float delt, float* rainnc, float* rainncv, float* snownc, float* snowncv,
              float* graupelnc, float* graupelncv, float* sr, void* stream);
 
+/* wrf_wsm6's computation without caller scratch and without any device
+ * allocation; no counterpart in the reference.  For callers that pass only
+ * the scheme's own arrays and must not allocate device memory themselves:
+ * its two intermediate fields live in a fixed file-scope device array of
+ * 2 x 2,097,152 floats (16 MiB), enough for the block of a 240x240x41 grid.
+ * Larger blocks, and delt >= 240 s (two time-split loops), return WRF_EINVAL.
+ * The first call on a device looks up the array's address (make it before
+ * any stream capture on that device); calls that overlap on the GPU share
+ * the array and race. */
+int wrf_wsm6_noalloc(const WrfGrid* g, float* th, float* qv, float* qc, float* qr, float* qi, float* qs,
+                     float* qg, const float* rho, const float* pii, const float* p, const float* dz8w,
+                     float delt, float* rainnc, float* rainncv, float* snownc, float* snowncv,
+                     float* graupelnc, float* graupelncv, float* sr, void* stream);
+
 /* copies the 16 device status words to host memory (synchronises the stream) */
 int wrf_status_read(const WrfState* s, void* stream, int* out16);
 

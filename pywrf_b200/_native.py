@@ -66,6 +66,8 @@ def lib() -> ctypes.CDLL:
     L.wrf_advect_scalar.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 9 + [vp]
     L.wrf_wsm6.restype = ip
     L.wrf_wsm6.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 11 + [ctypes.c_float] + [vp] * 7 + [vp]
+    L.wrf_wsm6_noalloc.restype = ip
+    L.wrf_wsm6_noalloc.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 11 + [ctypes.c_float] + [vp] * 7 + [vp]
     L.wrf_status_read.restype = ip
     L.wrf_status_read.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int)]
     L.wrf_last_launch_count.restype = ip

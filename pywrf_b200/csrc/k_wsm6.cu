@@ -15,6 +15,7 @@
 // Arithmetic is IEEE float32 in the reference's operation order; constant
 // sub-expressions the reference forms from python floats are formed in double
 // and rounded once, as the reference does.
+#include <mutex>
 #include "kernels.cuh"
 
 namespace wrf {
@@ -1144,6 +1145,129 @@ __global__ void __launch_bounds__(128) k_wsm6_finish(Grid g, S s, float dt, floa
   eos_point(g, s, k, p, c2, T, qvnew);
 }
 
+// ------------------------------------------------------------- no-alloc WSM6
+// wrf_wsm6_noalloc computes wrf_wsm6's result with the split kernels, whose
+// intermediate temperature and rain live in a fixed, file-scope device array
+// instead of caller memory: for callers that hand over only the scheme's own
+// arrays (the reference's wsm6 / microphysics_driver arguments have no room
+// for scratch) and must not allocate device memory on their own (an
+// allocation synchronises the device and can fail part-way through an
+// integration).  Limit: kNoAllocMaxPoints points of the scheme's block
+// ((nz-1) x (jde-jds-3) x (ide-ids-3)); 240x240x41 needs 2,061,160.  Nothing
+// in the array needs to start at zero: each call writes every element it
+// reads.  The array is shared by all calls on a device, so calls whose
+// kernels overlap on the GPU (e.g. on two streams) race.
+constexpr size_t kNoAllocMaxPoints = size_t(1) << 21;  // per intermediate field
+static __device__ __align__(256) float g_wsm6_scratch[2 * kNoAllocMaxPoints];
+
+// column part of WSM6 on caller arrays: writes the scratch (temperature,
+// rain after the sedimentation), qr / qi / qs / qg after the sedimentation
+// and melting, and the precipitation
+template <int SEG, int NS>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_wsm6_sed_args(Grid g, Wsm6Args a, float delt, float* scr_t,
+                                                                       float* scr_qr0s) {
+  constexpr int SPW = 32 / SEG, SPB = kWarpsPerBlock * SPW;
+  __shared__ SegScratch<SEG, NS> scratch[SPB];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int segw = lane / SEG;
+  Seg<SEG, NS> sg;
+  sg.l = lane % SEG;
+  sg.base = segw * SEG;
+  sg.km = g.nz - 1;
+  const int km = sg.km;
+  const int col = warp * SPW + segw;
+  const int i0 = g.ids + 1, j0 = g.jds + 1;
+  const int ncol = g.ide - 2 - i0, nrow = g.jde - 2 - j0;
+  const int j = j0 + blockIdx.y;
+  const int i = i0 + blockIdx.x * SPB + col;
+  const bool run = i < g.ide - 2 && j < g.jde - 2;
+  const size_t lev = (size_t)g.ny * g.nx;
+  const int c2 = run ? g.i2(j, i) : 0;
+  WCol<NS> c;
+  dummy_column<NS>(c);
+  if (run) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      const int k = sg.k(q);
+      if (k >= km) continue;
+      const size_t p = k * lev + c2;
+      c.t[q] = a.th[p] * a.pii[p];
+      c.den[q] = a.rho[p];
+      c.p[q] = a.p[p];
+      c.delz[q] = a.dz8w[p];
+      c.q[q] = a.qv[p];
+      c.qc0[q] = a.qc[p];
+      c.qr0[q] = a.qr[p];
+      c.qc1[q] = a.qi[p];
+      c.qr1[q] = a.qs[p];
+      c.qr2[q] = a.qg[p];
+    }
+  }
+  Precip pr{run ? a.rainnc[c2] : 0.f, 0.f, run ? a.snownc[c2] : 0.f, 0.f, run ? a.graupelnc[c2] : 0.f, 0.f, 0.f};
+  float qr0s[NS];
+  wsm6_column_w<SEG, NS, false>(sg, c, delt, pr, scratch[col], qr0s);
+  if (!run) return;
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    const int k = sg.k(q);
+    if (k >= km) continue;
+    const size_t p = k * lev + c2;
+    const size_t b = ((size_t)k * nrow + (j - j0)) * ncol + (i - i0);
+    scr_t[b] = c.t[q];
+    scr_qr0s[b] = qr0s[q];
+    a.qr[p] = c.qr0[q];
+    a.qi[p] = c.qc1[q];
+    a.qs[p] = c.qr1[q];
+    a.qg[p] = c.qr2[q];
+  }
+  if (sg.l == 0) {
+    a.rainnc[c2] = pr.rain;
+    a.rainncv[c2] = pr.rainncv;
+    a.snownc[c2] = pr.snow;
+    a.snowncv[c2] = pr.snowncv;
+    a.graupelnc[c2] = pr.graupel;
+    a.graupelncv[c2] = pr.graupelncv;
+    a.sr[c2] = pr.sr;
+  }
+}
+
+// point processes of WSM6 on caller arrays, one thread per point of the block
+__global__ void __launch_bounds__(128) k_wsm6_finish_args(Grid g, Wsm6Args a, float dtcld, const float* scr_t,
+                                                          const float* scr_qr0s) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const int i0 = g.ids + 1, j0 = g.jds + 1;
+  if (k >= g.nz - 1 || j < j0 || j >= g.jde - 2 || i < i0 || i >= g.ide - 2) return;
+  const int ncol = g.ide - 2 - i0, nrow = g.jde - 2 - j0;
+  const size_t p = (size_t)k * g.ny * g.nx + g.i2(j, i);
+  const size_t b = ((size_t)k * nrow + (j - j0)) * ncol + (i - i0);
+  const float pii = a.pii[p];
+  const float t0 = a.th[p] * pii;
+  const float den = a.rho[p];
+  const float pfull = a.p[p];
+  const float denfac = sqrtf(1.0f / den * F(mp::DEN0));
+  float q = a.qv[p];
+  float qc0 = fmaxf(a.qc[p], 0.0f);
+  const float cpm = q >= F(mp::QMIN) ? F(mp::CPV) * q + (1.0f - q) * F(mp::CPD)
+                                     : F(mp::CPD * (1.0 - mp::QMIN) + mp::CPV * mp::QMIN);
+  const float xl = F(mp::XLV0) - F(mp::XLV1) * (t0 - F(mp::T0C));
+  float qs0, qs1;
+  fpvs(t0, pfull, qs0, qs1);
+  const float qr0s = scr_qr0s[b];
+  const bool small = qr0s <= F(mp::QCRMIN);
+  const float rs0 = small ? F(mp::RSLOPERMAX) : 1.0f / wpow(F(mp::PIDN0R) / (qr0s * den), 0.25f);
+  const float r30 = small ? F(mp::RSLOPER3MAX) : rs0 * rs0 * rs0;
+  float t = scr_t[b];
+  float qc1 = a.qi[p], qr0 = a.qr[p], qr1 = a.qs[p], qr2 = a.qg[p];
+  wsm6_point(t, q, qc0, qc1, qr0, qr1, qr2, den, pfull, denfac, cpm, xl, qs0, qs1, rs0, r30, dtcld);
+  a.th[p] = t / pii;
+  a.qv[p] = q;
+  a.qc[p] = qc0;
+  a.qr[p] = qr0;
+  a.qi[p] = qc1;
+  a.qs[p] = qr1;
+  a.qg[p] = qr2;
+}
+
 #undef F
 
 // 16-lane segments with 3 levels per lane hold up to 47 mass levels; deeper
@@ -1192,6 +1316,60 @@ int launch_wsm6(const Grid& g, float* const* f, float delt, cudaStream_t st) {
     k_wsm6<32, 2><<<dim3((ncol + SPB - 1) / SPB, nrow), b, 0, st>>>(g, a, delt);
   }
   return 1;
+}
+
+// The scratch's device address is looked up once per device, by the first
+// call on that device (cudaGetSymbolAddress, with the device current); that
+// first call should come before any stream capture on the device.
+int launch_wsm6_noalloc(const Grid& g, float* const* f, float delt, cudaStream_t st, const char** err) {
+  const int km = g.nz - 1;
+  const int ncol = g.ide - 2 - (g.ids + 1), nrow = g.jde - 2 - (g.jds + 1);
+  const size_t npts = (size_t)km * (size_t)nrow * (size_t)ncol;
+  if (npts > kNoAllocMaxPoints) {
+    *err = "wrf_wsm6_noalloc: the scheme's block exceeds the fixed scratch (2097152 points per field)";
+    return WRF_EINVAL;
+  }
+  const double loops = fmax((double)delt / mp::DTCLDCR, 1.0);
+  if ((int)loops != 1) {
+    *err = "wrf_wsm6_noalloc: delt >= 240 s needs two time-split loops; use wrf_wsm6";
+    return WRF_EINVAL;
+  }
+  constexpr int kMaxDev = 64;
+  static float* scratch[kMaxDev] = {};
+  static std::mutex setup;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) {
+    *err = "wrf_wsm6_noalloc: no current CUDA device (or device index >= 64)";
+    return WRF_ECUDA;
+  }
+  float* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(setup);
+    if (!scratch[dev]) {
+      void* ptr = nullptr;
+      const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_wsm6_scratch);
+      if (rc != cudaSuccess || !ptr) {
+        *err = "wrf_wsm6_noalloc: cudaGetSymbolAddress of the scratch array failed";
+        return WRF_ECUDA;
+      }
+      scratch[dev] = static_cast<float*>(ptr);
+    }
+    base = scratch[dev];
+  }
+  Wsm6Args a{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], f[10],
+             f[11], f[12], f[13], f[14], f[15], f[16], f[17]};
+  const dim3 b(32 * kWarpsPerBlock);
+  if (km <= 47) {
+    constexpr int SPB = kWarpsPerBlock * 2;
+    k_wsm6_sed_args<16, 3><<<dim3((ncol + SPB - 1) / SPB, nrow), b, 0, st>>>(g, a, delt, base, base + kNoAllocMaxPoints);
+  } else {
+    constexpr int SPB = kWarpsPerBlock;
+    k_wsm6_sed_args<32, 2><<<dim3((ncol + SPB - 1) / SPB, nrow), b, 0, st>>>(g, a, delt, base, base + kNoAllocMaxPoints);
+  }
+  const float dtcld = ((double)delt <= mp::DTCLDCR) ? delt : (float)(1.0 * (double)delt / loops);
+  const dim3 b3(32, 4);
+  k_wsm6_finish_args<<<point_grid(g, b3), b3, 0, st>>>(g, a, dtcld, base, base + kNoAllocMaxPoints);
+  return 2;
 }
 
 }  // namespace wrf

@@ -51,5 +51,7 @@ int launch_bdy_final(const Grid& g, const S& s, cudaStream_t st);
 // microphysics (k_wsm6.cu)
 int launch_physics(const Grid& g, const S& s, cudaStream_t st);
 int launch_wsm6(const Grid& g, float* const* f, float delt, cudaStream_t st);
+// WSM6 with a fixed file-scope device scratch (returns kernels or WRF_E*, *err set)
+int launch_wsm6_noalloc(const Grid& g, float* const* f, float delt, cudaStream_t st, const char** err);
 
 }  // namespace wrf

@@ -309,6 +309,26 @@ int wrf_wsm6(const WrfGrid* gin, float* th, float* qv, float* qc, float* qr, flo
   return check_launch("wsm6");
 }
 
+int wrf_wsm6_noalloc(const WrfGrid* gin, float* th, float* qv, float* qc, float* qr, float* qi, float* qs,
+                     float* qg, const float* rho, const float* pii, const float* p, const float* dz8w, float delt,
+                     float* rainnc, float* rainncv, float* snownc, float* snowncv, float* graupelnc,
+                     float* graupelncv, float* sr, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  float* f[18] = {th, qv, qc, qr, qi, qs, qg, const_cast<float*>(rho), const_cast<float*>(pii),
+                  const_cast<float*>(p), const_cast<float*>(dz8w), rainnc, rainncv, snownc, snowncv,
+                  graupelnc, graupelncv, sr};
+  for (float* x : f)
+    if (!x) return fail(WRF_EINVAL, "null argument");
+  if (!(delt > 0.f)) return fail(WRF_EINVAL, "delt must be > 0");
+  cudaGetLastError();
+  const char* err = nullptr;
+  rc = launch_wsm6_noalloc(g, f, delt, static_cast<cudaStream_t>(stream), &err);
+  if (rc < 0) return fail(rc, err ? err : "wrf_wsm6_noalloc failed");
+  return check_launch("wsm6_noalloc");
+}
+
 int wrf_status_read(const WrfState* sin, void* stream, int* out16) {
   if (!sin || !sin->f[WF_STATUS] || !out16) return fail(WRF_EINVAL, "null argument");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
