@@ -3,11 +3,13 @@
 // mass fluxes (rk_scalar_tend, wrf_dynamics.py:3982-4051) and theta with the
 // stage's coupled velocities.
 //
-// A block owns a TX x TY tile of columns and marches up through KCH levels.
-// For each level the species' values of the tile and its 3-cell halo are
-// staged in shared memory, every x and y face flux is formed once, and the
-// vertical face flux is carried from one level to the next (each thread keeps
-// a 7-level window of its column).  Face fluxes use the reference's orders:
+// A block of TX x TY threads owns (TX-1) x (TY-1) columns and marches up
+// through KCH levels.  For each level the species' values of the tile and its
+// halo are staged in shared memory (cp.async, double-buffered: the next level
+// streams in while this one computes) and every thread forms exactly one x face
+// flux and one y face flux (the tile's TX x TY faces); the vertical face flux
+// is carried from one level to the next (each thread keeps a 7-level window
+// of its column).  Face fluxes use the reference's orders:
 // 5th order inside, 3rd order on the second face and 2nd order on the first
 // face from each boundary; the tendency is accumulated y, then x, then z.
 #include "kernels.cuh"
@@ -15,7 +17,8 @@
 namespace wrf {
 
 constexpr int kAdvTX = 32, kAdvTY = 8, kAdvKCH = 10;
-constexpr int kHX = kAdvTX + 6, kHY = kAdvTY + 6;
+constexpr int kAdvCX = kAdvTX - 1, kAdvCY = kAdvTY - 1;  // cells per tile; faces = threads
+constexpr int kHX = kAdvTX + 5, kHY = kAdvTY + 5;        // staged tile: faces - 3 .. faces + 2
 
 // up to six scalars; a block takes the group blockIdx.z % ngroup of NSP of them
 struct AdvArgs {
@@ -69,11 +72,11 @@ __device__ __forceinline__ float zface(int ktf, const float* fnm, const float* f
 // region are set to zero, as the reference zeroes advect_tend first)
 template <int NSP, bool ACCUM>
 __global__ void __launch_bounds__(kAdvTX * kAdvTY) k_advect_tiled(Grid g, S s, AdvArgs a) {
-  __shared__ float tq[NSP][kHY][kHX];
-  __shared__ float fx[NSP][kAdvTY][kAdvTX + 1];
-  __shared__ float fy[NSP][kAdvTY + 1][kAdvTX];
+  __shared__ float tq[2][NSP][kHY][kHX];  // double buffer: level k computes while k+1 loads
+  __shared__ float fx[NSP][kAdvTY][kAdvTX];
+  __shared__ float fy[NSP][kAdvTY][kAdvTX];
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = g.ids + blockIdx.x * kAdvTX, j0 = g.jds + blockIdx.y * kAdvTY;
+  const int i0 = g.ids + blockIdx.x * kAdvCX, j0 = g.jds + blockIdx.y * kAdvCY;
   const int i = i0 + tx, j = j0 + ty;
   const int nx = g.nx, ny = g.ny, ktf = g.nz - 1;
   const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde;
@@ -87,8 +90,11 @@ __global__ void __launch_bounds__(kAdvTX * kAdvTY) k_advect_tiled(Grid g, S s, A
     qs[m] = a.q[grp * NSP + m];
     ts[m] = a.tend[grp * NSP + m];
   }
-  const bool cell = i < ide - 1 && j < jde - 1;          // advected column
-  const bool zreg = i < ide && j < jde;                  // zeroed column
+  const bool inner = tx < kAdvCX && ty < kAdvCY;
+  const bool cell = inner && i < ide - 1 && j < jde - 1;  // advected column
+  const bool zreg = inner && i < ide && j < jde;          // zeroed column
+  const bool xf = j < jde - 1 && i >= ids + 1 && i <= ide - 2;  // x face i of row j is used
+  const bool yf = i < ide - 1 && j >= jds + 1 && j <= jde - 2;  // y face j of column i is used
   const bool doy = j >= jds + 1 && j < jde - 2;
   const bool dox = i >= ids + 1 && i < ide - 2;
   const int c = g.i2(min(j, ny - 1), min(i, nx - 1));
@@ -109,37 +115,42 @@ __global__ void __launch_bounds__(kAdvTX * kAdvTY) k_advect_tiled(Grid g, S s, A
     const float r = cell && k0 < g.nz ? __ldg(&a.rom[k0 * lev + c]) : 0.f;
     fbot[m] = zface(ktf, fnm, fnp, win[m], k0, k0, r);
   }
-  for (int k = k0; k < k1; ++k) {
-    __syncthreads();
-    // stage the tile and its halo for every species
+  // asynchronous copy of a level's tile (and halo) of every species into a
+  // buffer; points outside the allocation are zero-filled
+  auto stage = [&](int k, int buf) {
     for (int e = ty * kAdvTX + tx; e < kHY * kHX; e += kAdvTX * kAdvTY) {
       const int yy = e / kHX, xx = e % kHX;
       const int jj = j0 - 3 + yy, ii = i0 - 3 + xx;
       const bool in = jj >= 0 && jj < ny && ii >= 0 && ii < nx;
-      const size_t p = (size_t)k * lev + (size_t)jj * nx + ii;
+      const size_t p = in ? (size_t)k * lev + (size_t)jj * nx + ii : 0;
 #pragma unroll
-      for (int m = 0; m < NSP; ++m) tq[m][yy][xx] = in ? __ldg(&qs[m][p]) : 0.f;
+      for (int m = 0; m < NSP; ++m) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(&tq[buf][m][yy][xx]);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(qs[m] + p), "r"(in ? 4 : 0));
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  if (k0 < k1) stage(k0, 0);
+  for (int k = k0; k < k1; ++k) {
+    const int buf = (k - k0) & 1;
+    if (k + 1 < k1) {
+      stage(k + 1, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;\n" ::);
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::);
     }
     __syncthreads();
     const size_t pc = (size_t)k * lev + c;
     if (k < ktf) {
-      // x faces: every thread its left face, the last column also the right one
-      const float rl = cell ? __ldg(&a.ru[pc]) : 0.f;
-      const bool right = tx == kAdvTX - 1 && i + 1 < ide;
-      const float rr = right ? __ldg(&a.ru[pc + 1]) : 0.f;
-      const float rs3 = __ldg(&a.ru[(size_t)k * lev + (size_t)min(j, ny - 1) * nx + (ide - 2)]);
-      const bool yb = cell && j >= jds + 1;
-      const float rb = yb ? __ldg(&a.rv[pc]) : 0.f;
-      const bool top = ty == kAdvTY - 1 && j + 1 < jde;
-      const float rt = top && i < nx ? __ldg(&a.rv[pc + nx]) : 0.f;
+      // one x face (i, between i-1 and i) and one y face (j) per thread
+      const float rl = xf ? __ldg(&a.ru[pc]) : 0.f;
+      const float rs3 = xf ? __ldg(&a.ru[(size_t)k * lev + (size_t)j * nx + (ide - 2)]) : 0.f;
+      const float rb = yf ? __ldg(&a.rv[pc]) : 0.f;
 #pragma unroll
       for (int m = 0; m < NSP; ++m) {
-        const float* row = &tq[m][ty + 3][0];
-        fx[m][ty][tx] = cell ? xface(g, row, i0, i, rl, rs3) : 0.f;
-        if (right) fx[m][ty][tx + 1] = xface(g, row, i0, i + 1, rr, rs3);
-        const float* colp = &tq[m][0][tx + 3];
-        fy[m][ty][tx] = yb ? yface(g, colp, j0, j, rb) : 0.f;
-        if (top) fy[m][ty + 1][tx] = yface(g, colp, j0, j + 1, rt);
+        fx[m][ty][tx] = xf ? xface(g, &tq[buf][m][ty + 3][0], i0, i, rl, rs3) : 0.f;
+        fy[m][ty][tx] = yf ? yface(g, &tq[buf][m][0][tx + 3], j0, j, rb) : 0.f;
       }
     }
     __syncthreads();
@@ -176,7 +187,7 @@ int launch_advect_moist_tiled(const Grid& g, const S& s, cudaStream_t st) {
   a.rom = s[WF_WW_M];
   a.ngroup = 3;
   const dim3 b(kAdvTX, kAdvTY);
-  const dim3 gr((g.ide - g.ids + kAdvTX - 1) / kAdvTX, (g.jde - g.jds + kAdvTY - 1) / kAdvTY,
+  const dim3 gr((g.ide - g.ids + kAdvCX - 1) / kAdvCX, (g.jde - g.jds + kAdvCY - 1) / kAdvCY,
                 3 * ((g.nz + kAdvKCH - 1) / kAdvKCH));
   k_advect_tiled<2, false><<<gr, b, 0, st>>>(g, s, a);
   return 1;
@@ -191,7 +202,7 @@ int launch_advect_theta_tiled(const Grid& g, const S& s, cudaStream_t st) {
   a.rom = s[WF_WW];
   a.ngroup = 1;
   const dim3 b(kAdvTX, kAdvTY);
-  const dim3 gr((g.ide - g.ids + kAdvTX - 1) / kAdvTX, (g.jde - g.jds + kAdvTY - 1) / kAdvTY,
+  const dim3 gr((g.ide - g.ids + kAdvCX - 1) / kAdvCX, (g.jde - g.jds + kAdvCY - 1) / kAdvCY,
                 (g.nz + kAdvKCH - 1) / kAdvKCH);
   k_advect_tiled<1, true><<<gr, b, 0, st>>>(g, s, a);
   return 1;
