@@ -48,9 +48,11 @@ FALLBACK_HBM_GBS = 6650.0
 # prognostic fields a host-driven caller moves in and out each step (e2e)
 E2E_FIELDS = ("u", "v", "w", "t", "ph", "mu", "p", "al", "moist")
 
-# DRAM bytes per launch of the dominant kernel from one ncu capture (profiles/),
-# None until captured
-NCU_TRAFFIC = {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# dominant kernel from one ncu --set full capture of this workload
+# (profiles/k_acoustic_col_and_advection_240x240x41.md): the stage-1 launch,
+# 202.0 MB read + 72.9 MB written, against 321 MB algorithmic for that launch
+NCU_TRAFFIC = {"k_acoustic_col": 274.835456e6}
 
 
 def parse():

@@ -1,0 +1,375 @@
+// BF16 GEMM on the 5th-generation tensor cores (tcgen05) with fused epilogues,
+// the dense part of the per-column microphysics network:
+//
+//   C[m, n] = sum_k A[m, k] * B[n, k]      A: M x K, B: N x K, both bf16 row-major
+//
+// (both operands K-major; a product with a transposed operand is fed the
+// transposed copy that the producing epilogue writes).  One CTA computes one
+// 128 x 128 tile of C, or its part of the K range when the reduction is split:
+//
+//   warp 0, one lane   TMA producer: 128 x 64 tiles of A and B into a
+//                      3-stage ring of 128-byte-swizzled shared buffers
+//   warp 1, one lane   MMA issuer: tcgen05.mma.cta_group::1.kind::f16,
+//                      M = 128, N = 128, K = 16 per instruction, fp32
+//                      accumulator in tensor memory (128 lanes x 128 columns);
+//                      tcgen05.commit frees each ring slot and finally
+//                      signals the epilogue
+//   warps 0-3          epilogue: tcgen05.ld of the warp's 32 accumulator
+//                      lanes (= tile rows), bias / GELU / GELU' and the stores
+//
+// Every wait on an mbarrier is bounded (kWaitCycles); a wait that runs out
+// sets *err, the CTA skips its stores, frees its tensor memory and returns.
+// No load uses cluster multicast.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <mutex>
+#include "kernels.cuh"
+#include "tc_gemm.cuh"
+
+namespace wrf {
+namespace tc {
+
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3, kThreads = 128;
+constexpr uint32_t kTileBytes = BM * BK * 2;         // 16 KB per operand tile
+constexpr uint32_t kStageBytes = 2 * kTileBytes;
+constexpr uint32_t kTmemCols = BN;                   // fp32 accumulator: 128 lanes x BN columns
+constexpr size_t kSmemBytes = STAGES * kStageBytes + 1024 + 128;
+constexpr long long kWaitCycles = 4000000000LL;      // ~2 s at the boost clock
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait for the phase of the given parity to complete
+__device__ __noinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+  const long long t0 = clock64();
+  for (uint32_t it = 0;; ++it) {
+    if (mbar_try(b, parity)) return true;
+    if ((it & 255u) == 255u && clock64() - t0 > kWaitCycles) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// shared-memory matrix descriptor of a K-major tile written by TMA with
+// 128-byte swizzle: rows of 128 B (64 bf16), 8-row groups 1024 B apart
+__device__ __forceinline__ uint64_t desc_k_sw128(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);  // start address, 16-byte units
+  d |= (uint64_t)1 << 16;                            // leading byte offset (unused by swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;                  // stride byte offset: 8 rows x 128 B
+  d |= (uint64_t)1 << 46;                            // descriptor version of sm_100
+  d |= (uint64_t)2 << 61;                            // 128-byte swizzle
+  return d;
+}
+
+// instruction descriptor: bf16 x bf16 -> fp32, both K-major, M = 128, N = BN
+constexpr uint32_t kIdesc = (1u << 4)                  // accumulator format f32
+                            | (1u << 7)                // A bf16
+                            | (1u << 10)               // B bf16
+                            | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// 16 consecutive fp32 accumulator columns of this thread's lane (the wait
+// for the load is part of the same asm statement, so no use can precede it)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__device__ __forceinline__ void store_row16_bf16(__nv_bfloat16* dst, const float (&v)[16]) {
+  uint4 a, b;
+  a.x = pack_bf16x2(v[0], v[1]);   a.y = pack_bf16x2(v[2], v[3]);
+  a.z = pack_bf16x2(v[4], v[5]);   a.w = pack_bf16x2(v[6], v[7]);
+  b.x = pack_bf16x2(v[8], v[9]);   b.y = pack_bf16x2(v[10], v[11]);
+  b.z = pack_bf16x2(v[12], v[13]); b.w = pack_bf16x2(v[14], v[15]);
+  reinterpret_cast<uint4*>(dst)[0] = a;
+  reinterpret_cast<uint4*>(dst)[1] = b;
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gemm_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, int M, int N, int K,
+              int kb_per_split, GemmEpi e) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + STAGES * kTileBytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * kStageBytes);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+  const int kb_total = (K + BK - 1) / BK;
+  const int kb0 = blockIdx.z * kb_per_split;
+  const int nkb = min(kb_per_split, kb_total - kb0);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ta)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tb)) : "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (nkb > 0 && warp == 0 && lane == 0) {
+    // producer
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % STAGES;
+      const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+      if (!mbar_wait(&empty[s], ph ^ 1u)) {
+        atomicExch(abort_flag, 1);
+        break;
+      }
+      mbar_expect_tx(&full[s], kStageBytes);
+      tma_load_2d(sA + s * kTileBytes, &ta, (kb0 + kb) * BK, m0, &full[s]);
+      tma_load_2d(sB + s * kTileBytes, &tb, (kb0 + kb) * BK, n0, &full[s]);
+    }
+  } else if (nkb > 0 && warp == 1 && lane == 0) {
+    // MMA issuer
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % STAGES;
+      const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+      if (!mbar_wait(&full[s], ph)) {
+        atomicExch(abort_flag, 1);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(sA + s * kTileBytes), b0 = smem_u32(sB + s * kTileBytes);
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk)
+        umma_bf16(tmem, desc_k_sw128(a0 + kk * 32), desc_k_sw128(b0 + kk * 32), (kb | kk) != 0 ? 1u : 0u);
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);  // arrives once every MMA issued above has completed
+  }
+  __syncwarp();
+
+  // epilogue
+  // (the outcome is made uniform over the CTA: tcgen05.ld is warp-collective)
+  if (!(nkb > 0 && mbar_wait(done, 0))) atomicExch(abort_flag, 1);
+  tc_fence_after();
+  __syncthreads();
+  const bool ok = *abort_flag == 0;
+  if (!ok && threadIdx.x == 0 && e.err) atomicExch(e.err, 1);
+  if (ok) {
+    const int r = warp * 32 + lane;
+    const int m = m0 + r;
+    const bool row = m < M;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int c = 0; c < BN / 16; ++c) {
+      const int n = n0 + c * 16;
+      if (n >= N) break;  // N is a multiple of 16
+      float v[16];
+      tmem_ld16(trow + (uint32_t)(c * 16), v);
+      if (!row) continue;
+      if (e.bias) {
+#pragma unroll
+        for (int t = 0; t < 16; ++t) v[t] += __ldg(&e.bias[n + t]);
+      }
+      switch (e.kind) {
+        case EPI_F32: {
+          float* o = static_cast<float*>(e.out) + (size_t)blockIdx.z * e.split_stride + (size_t)m * e.ldo + n;
+#pragma unroll
+          for (int t = 0; t < 16; t += 4) *reinterpret_cast<float4*>(o + t) = make_float4(v[t], v[t + 1], v[t + 2], v[t + 3]);
+          break;
+        }
+        case EPI_BIAS_GELU: {
+          if (e.out_z) store_row16_bf16(e.out_z + (size_t)m * e.ldo + n, v);
+#pragma unroll
+          for (int t = 0; t < 16; ++t) v[t] = gelu(v[t]);
+          store_row16_bf16(static_cast<__nv_bfloat16*>(e.out) + (size_t)m * e.ldo + n, v);
+          break;
+        }
+        case EPI_GELU_BWD: {
+          const __nv_bfloat16* z = e.aux + (size_t)m * e.ldo + n;
+#pragma unroll
+          for (int t = 0; t < 16; ++t) v[t] *= gelu_grad(__bfloat162float(z[t]));
+          store_row16_bf16(static_cast<__nv_bfloat16*>(e.out) + (size_t)m * e.ldo + n, v);
+          break;
+        }
+        default:  // EPI_BF16
+          store_row16_bf16(static_cast<__nv_bfloat16*>(e.out) + (size_t)m * e.ldo + n, v);
+          break;
+      }
+      if (e.out_t) {  // transposed copy [N][ldt] of what was stored (bf16)
+#pragma unroll
+        for (int t = 0; t < 16; ++t) e.out_t[(size_t)(n + t) * e.ldt + m] = __float2bfloat16_rn(v[t]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------- host side
+using EncodeTiled = decltype(&cuTensorMapEncodeTiled);
+
+EncodeTiled encoder(const char** err) {
+  static EncodeTiled fn = nullptr;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p) {
+      *err = "cuTensorMapEncodeTiled is not available from the driver";
+      return nullptr;
+    }
+    fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+// 2-D bf16 row-major [rows][cols] operand, 128 x 64 boxes, 128-byte swizzle;
+// rows past the end read as zeros
+bool make_map(CUtensorMap* map, const void* ptr, int rows, int cols, const char** err) {
+  EncodeTiled enc = encoder(err);
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    *err = "cuTensorMapEncodeTiled rejected an operand (pointer alignment or shape)";
+    return false;
+  }
+  return true;
+}
+
+}  // namespace tc
+
+int launch_gemm_tc(const void* A, const void* B, int M, int N, int K, int splits, const GemmEpi& e, cudaStream_t st,
+                   const char** err) {
+  using namespace tc;
+  if (!A || !B || !e.out) { *err = "gemm: null operand"; return WRF_EINVAL; }
+  if (M < 1 || N < 16 || K < 64 || (N % 16) || (K % 64)) {
+    *err = "gemm: needs M >= 1, N a multiple of 16, K a multiple of 64";
+    return WRF_EINVAL;
+  }
+  if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15u) {
+    *err = "gemm: operands must be 16-byte aligned";
+    return WRF_EINVAL;
+  }
+  if (e.ldo < N || (e.ldo % 8) || (reinterpret_cast<uintptr_t>(e.out) & 15u)) {
+    *err = "gemm: output leading dimension must be >= N and a multiple of 8, output 16-byte aligned";
+    return WRF_EINVAL;
+  }
+  if (e.kind < EPI_F32 || e.kind > EPI_BF16 || (e.kind == EPI_GELU_BWD && !e.aux) ||
+      (e.out_t && e.ldt < M) || (e.kind != EPI_F32 && splits != 1)) {
+    *err = "gemm: bad epilogue (kind, aux, transposed leading dimension, or a split reduction with a bf16 output)";
+    return WRF_EINVAL;
+  }
+  const int kb_total = K / BK;
+  if (splits < 1) splits = 1;
+  if (splits > kb_total) splits = kb_total;
+  const int kper = (kb_total + splits - 1) / splits;
+  splits = (kb_total + kper - 1) / kper;  // every split gets at least one k block
+  CUtensorMap ma, mb;
+  if (!make_map(&ma, A, M, K, err) || !make_map(&mb, B, N, K, err)) return WRF_EINVAL;
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) != cudaSuccess) {
+      *err = "gemm: cannot reserve the shared memory of the tile ring";
+      return WRF_ECUDA;
+    }
+    attr_set = true;
+  }
+  const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, splits);
+  k_gemm_tc<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, M, N, K, kper, e);
+  return 1;
+}
+
+int gemm_splits_used(int K, int splits) {
+  const int kb_total = K / tc::BK;
+  if (splits < 1) splits = 1;
+  if (splits > kb_total) splits = kb_total;
+  const int kper = (kb_total + splits - 1) / splits;
+  return (kb_total + kper - 1) / kper;
+}
+
+}  // namespace wrf
