@@ -21,6 +21,11 @@ Extra keys of the JSON line:
   cpu_baseline  the numpy oracle (a restatement of the reference's CPU path)
                 timed on this host for one step of the same workload
   clocks        SM clock samples taken during the timed region
+  surrogate     the per-column network in place of WSM6: trained on the GPU
+                on harvested WSM6 increments, then one unseen state run for
+                1 h with the plain and the surrogate step (speed, hydrometeor
+                mass and precipitation errors, tensor-core roofline)
+  adjoint       not built yet
 ``--impl reference`` times that CPU path alone (rank 0; other ranks exit).
 """
 from __future__ import annotations
@@ -40,7 +45,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "RK3 steps/s @240x240x41"
+METRIC = "RK3 steps/s @240x240x41: surrogate vs plain WSM6 at <=2% err; fwd+adj steps/s"
 UNIT = "steps/s"
 WORKLOAD = "240x240x41 synthetic moist ARW, plain WSM6, dt=45 s, 4 acoustic substeps, seeded bdy tendencies"
 FALLBACK_HBM_GBS = 6650.0
@@ -65,6 +70,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--phase-steps", type=int, default=3, help="eager steps timed per phase for the roofline")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the network (harvest, training, surrogate run)")
+    ap.add_argument("--sur-seeds", type=int, default=5, help="integrations harvested for the network's training set")
+    ap.add_argument("--sur-harvest-steps", type=int, default=80)
+    ap.add_argument("--sur-epochs", type=int, default=20)
+    ap.add_argument("--sur-steps", type=int, default=80, help="steps of the surrogate-vs-plain comparison (80 = 1 h)")
     return ap.parse_args()
 
 
@@ -306,6 +316,12 @@ def run_ours(a):
         e2e = {"value": job_rate(ke, e_ms, world), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": ke}
 
+    sur = None
+    if world > 1:
+        sur = {"unavailable": "measured at one GPU only (the replicas run the plain step)"}
+    elif not a.no_surrogate:
+        sur = run_surrogate(a, hbm)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         sec, sample = cpu_reference_step_time(a.config, 1, 0)
@@ -321,11 +337,130 @@ def run_ours(a):
                            "grid_point_updates_per_s": value * g.nx * g.ny * g.nz},
                 "gpu_launches": launches * a.steps, "launches_per_step": launches,
                 "roofline": roofline, "step_roofline": whole, "phases_ms": phase_ms,
-                "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan}
+                "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan,
+                "surrogate": sur, "adjoint": {"unavailable": "the hand-written adjoint kernels are not built yet"}}
         print(json.dumps(line), flush=True)
     it._graph = None
     if world > 1:
         dist.destroy_process_group()
+
+
+def hydrometeor_budget(st, g):
+    """Dry-air-mass-weighted totals of qc..qg (kg per m^2, summed over the
+    mass points) and the domain sum of accumulated precipitation."""
+    import torch
+    ids, ide, jds, jde, nz = g.ids, g.ide, g.jds, g.jde, g.nz
+    mu = (st["mu"] + st["mub"])[jds:jde - 1, ids:ide - 1].double()
+    dnw = st["dnw"][:nz - 1].double().abs()
+    out = {}
+    for m, name in enumerate(("qc", "qr", "qi", "qs", "qg"), start=2):
+        q = st["moist"][m, :nz - 1, jds:jde - 1, ids:ide - 1].double()
+        out[name] = float((q * dnw[:, None, None] * mu[None]).sum() / 9.81)
+    out["hydrometeors"] = sum(out[k] for k in ("qc", "qr", "qi", "qs", "qg"))
+    out["rainnc"] = float(st["rainnc"][jds:jde - 1, ids:ide - 1].double().sum())
+    return out
+
+
+def run_surrogate(a, hbm_peak):
+    """Train the per-column network on harvested WSM6 increments (all on the
+    tensor-core kernels), then integrate one unseen 240x240x41 state for
+    --sur-steps steps with the plain step and with the surrogate step (WSM6
+    every 10th step and on rejected columns) and compare their speed and
+    their hydrometeor mass and precipitation."""
+    import torch
+    from pywrf_b200 import surrogate, synthetic
+    from pywrf_b200.solver import Integrator
+    from pywrf_b200.state import DeviceState
+
+    def spec_for(seed):
+        return synthetic.spec_for_config(1, seed=seed)
+
+    t0 = time.time()
+    raw_in, raw_out, lay = surrogate.harvest(range(a.sur_seeds), a.sur_harvest_steps, spec_for, per_step=5000)
+    torch.cuda.synchronize()
+    t_harvest = time.time() - t0
+    spec = spec_for(100)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    st_plain = DeviceState.from_inputs(g, inputs, bdy, device="cuda")
+    st_sur = DeviceState.from_inputs(g, inputs, bdy, device="cuda")
+    net = surrogate.MlpNet(lay, hidden=512, device="cuda", seed=0)
+    net.fit_normalisation(raw_in, raw_out)
+    x, t = surrogate.standardise(net, st_plain.cgrid, raw_in, raw_out)
+    nrows = int(raw_in.shape[0])
+    del raw_in, raw_out
+    tr = surrogate.Trainer(net, batch=8192, splits=4, lr=1e-3)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    losses = tr.fit(x, t, epochs=a.sur_epochs, lr_end=1e-4)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    train_flop = 3 * 2 * (nrows - nrows % tr.batch) * a.sur_epochs * sum(
+        net.dims[i] * net.dims[i + 1] for i in range(4))
+    del x, t, tr
+
+    def timed(fn, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn(n)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    it = Integrator(st_plain)
+    it.capture()
+    ms_plain = timed(lambda n: [it.replay() for _ in range(n)], a.sur_steps)
+    si = surrogate.SurrogateIntegrator(st_sur, net, judge_every=10)
+    si.capture()
+    si.capture_mlp()
+    ms_sur = timed(lambda n: si.run(n, graph=True), a.sur_steps)
+    rejected_last = si.rejected()
+    bp, bs = hydrometeor_budget(st_plain, g), hydrometeor_budget(st_sur, g)
+    rel = {k: abs(bs[k] - bp[k]) / abs(bp[k]) if bp[k] else None for k in bp}
+
+    # the four tensor-core products of one surrogate call, alone
+    L = lay
+    flop = 2 * L["ncols"] * sum(net.dims[i] * net.dims[i + 1] for i in range(4))
+    tr1 = surrogate.Trainer(net, batch=8192, splits=1)
+    xin = si.x[:L["ncols"] - L["ncols"] % 8192]
+
+    def fwd(n):
+        for _ in range(n):
+            for s0 in range(0, xin.shape[0], 8192):
+                tr1.forward(xin[s0:s0 + 8192])
+    fwd(2)
+    ms_fwd = timed(fwd, 10) / 10 * L["ncols"] / xin.shape[0]
+    peak = peaks_tensor()
+    it._graph = None
+    si._graph = None
+    si._mlp_graph = None
+    return {
+        "plain_steps_per_s": a.sur_steps / (ms_plain / 1e3),
+        "surrogate_steps_per_s": a.sur_steps / (ms_sur / 1e3),
+        "speedup": ms_plain / ms_sur,
+        "judge_every": 10, "steps": a.sur_steps, "eval_seed": 100,
+        "rel_err_1h": rel, "plain_budget": bp, "surrogate_budget": bs,
+        "rejected_columns_last_step": rejected_last, "columns": L["ncols"],
+        "network": {"dims": net.dims, "dtype": "bf16 weights/activations, fp32 accumulate (tcgen05)"},
+        "training": {"rows": nrows, "seeds": a.sur_seeds, "harvest_steps": a.sur_harvest_steps,
+                     "epochs": a.sur_epochs, "batch": 8192, "loss_first": losses[0], "loss_last": losses[-1],
+                     "harvest_s": t_harvest, "train_s": t_train, "train_tflops": train_flop / t_train / 1e12},
+        "tensor_roofline": {"kernel": "k_gemm_tc (4 layers, one call)", "bound": "tensor",
+                            "achieved": flop / (ms_fwd / 1e3) / 1e12, "peak": peak[0], "unit": "TFLOP/s",
+                            "frac": flop / (ms_fwd / 1e3) / 1e12 / peak[0], "peak_source": peak[1],
+                            "flop_per_call": flop, "ms_per_call": ms_fwd},
+    }
+
+
+def peaks_tensor():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if d.get("bf16_tflops"):
+            return float(d["bf16_tflops"]), "measured (burst)"
+    return 1590.0, "fallback"
 
 
 def main():

@@ -156,6 +156,78 @@ int wrf_status_read(const WrfState* s, void* stream, int* out16);
  * reference has no counterpart; used to report launch counts) */
 int wrf_last_launch_count(void);
 
+/* ------------------------------------------------------------------------
+ * Per-column microphysics network: a learned stand-in for wsm6
+ * (pywrf/wrf_physics.py:137-1214).  The reference has no counterpart of
+ * anything below; the layout of the network's rows is given by
+ * wrf_mlp_layout.  A column is a mass column of the WSM6 block
+ * (i in [ids+1, ide-2), j in [jds+1, jde-2)), numbered
+ * (j - jds - 1) * ncx + (i - ids - 1).
+ * ------------------------------------------------------------------------ */
+#define WRF_MLP_LAYERS 4
+
+typedef struct WrfMlpNet {
+  int dims[WRF_MLP_LAYERS + 1];    /* widths: d0 (input), hidden x 3, d4 (output) */
+  const void* w[WRF_MLP_LAYERS];   /* bf16 [dims[l+1]][dims[l]] */
+  const float* b[WRF_MLP_LAYERS];  /* fp32 [dims[l+1]] */
+  const float* norm;               /* fp32 [2 d0 + 2 d4]: input mean, input 1/std, output mean, output std */
+  float tol_neg;                   /* gate: a species below -tol_neg (kg/kg) before clipping rejects the column */
+  float tol_sat;                   /* gate: qv above (1 + tol_sat) x saturation over water rejects the column */
+} WrfMlpNet;
+
+typedef struct WrfMlpWork {        /* caller-owned device scratch of one surrogate call */
+  int capacity;                    /* columns the buffers hold (>= ncols) */
+  void* x;                         /* bf16 [capacity][d0] */
+  void* h[2];                      /* bf16 [capacity][max hidden width] */
+  float* y;                        /* fp32 [capacity][d4] */
+  int* list;                       /* int [16 + capacity]: [0] rejected columns, [16..] their j * nx + i */
+  int* err;                        /* int: set to 1 if a tensor-core kernel's bounded wait ran out */
+} WrfMlpWork;
+
+/* one-time set-up of the network's kernels on the current device; call it
+ * before capturing any of the calls below into a CUDA graph */
+int wrf_mlp_init(void);
+
+/* out8 = km, ncx, ncy, ncols, nfeat (9 km), d0, nout (7 km + 3), d4 */
+int wrf_mlp_layout(const WrfGrid* g, int* out8);
+
+/* wrf_rk3_step with the microphysics call replaced by the network: features,
+ * four tcgen05 GEMMs, apply with the positivity / supersaturation gate, and
+ * WSM6 (the fused column kernel) on the rejected columns */
+int wrf_rk3_step_mlp(const WrfGrid* g, const WrfState* s, const WrfMlpNet* net, const WrfMlpWork* work,
+                     void* stream, wrf_probe_fn probe, void* user);
+
+/* network rows of the state's columns: x (bf16, standardised with norm) if
+ * raw is NULL, else raw (fp32 [ncols][10 km]: T p rho qv qc qr qi qs qg theta') */
+int wrf_mlp_features(const WrfGrid* g, const WrfState* s, const float* norm, void* x, float* raw, void* stream);
+/* raw increments [ncols][nout] of one microphysics call, given the raw rows before it */
+int wrf_mlp_targets(const WrfGrid* g, const WrfState* s, const float* raw_in, float* raw_out, void* stream);
+/* n raw rows -> bf16 inputs [n][d0] and fp32 standardised targets [n][d4] */
+int wrf_mlp_normalize(const WrfGrid* g, const float* norm, const float* raw_in, const float* raw_out, long long n,
+                      void* x, float* t, void* stream);
+
+/* out = a b^T on the tensor cores (a: m x k, b: n x k, bf16 row-major; n a
+ * multiple of 16, k of 64) with epilogue epi: 0 fp32 (+ bias; a split
+ * reduction writes `splits` partial sums split_stride apart), 1 bf16
+ * gelu(acc + bias) with the pre-activation in out_z, 2 bf16 acc * gelu'(aux),
+ * 3 bf16 (+ bias); out_t (optional) receives the stored values transposed */
+int wrf_gemm_bf16(const void* a, const void* b, int m, int n, int k, int splits, int epi, const float* bias,
+                  const void* aux, void* out, int ldo, long long split_stride, void* out_z, void* out_t, int ldt,
+                  int* err, void* stream);
+/* number of partial sums wrf_gemm_bf16 writes for a requested split count */
+int wrf_gemm_splits(int k, int splits);
+/* dy = scale (y - t) (zero beyond column nvalid), row-major and transposed; *loss += sum (y - t)^2 */
+int wrf_mse_grad(const float* y, const float* t, int m, int n, int nvalid, float scale, void* dy, void* dyt,
+                 float* loss, void* stream);
+/* out[r] = sum of row r of a bf16 [rows][cols] */
+int wrf_rowsum_bf16(const void* a, int rows, int cols, float* out, void* stream);
+/* Adam step (decoupled weight decay wd) on fp32 w [r][c] with the gradient summed from nsplit partials;
+ * refreshes the bf16 copy wb [r][c] and the transposed copy wtb [c][r] (either may be NULL) */
+int wrf_adam(float* w, const float* gpart, int nsplit, long long split_stride, float* m, float* v, int r, int c,
+             void* wb, void* wtb, float lr, float beta1, float beta2, float eps, float wd, int step, void* stream);
+/* out [c][r] = a [r][c]^T (bf16) */
+int wrf_transpose_bf16(const void* a, int r, int c, void* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

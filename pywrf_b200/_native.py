@@ -33,6 +33,23 @@ class WrfGridC(ctypes.Structure):
 
 PROBE_FN = ctypes.CFUNCTYPE(None, ctypes.c_char_p, ctypes.c_void_p)
 
+WRF_MLP_LAYERS = 4
+EPI_F32, EPI_BIAS_GELU, EPI_GELU_BWD, EPI_BF16 = 0, 1, 2, 3
+
+
+class WrfMlpNetC(ctypes.Structure):
+    """``WrfMlpNet`` of include/pywrf_b200.h"""
+    _fields_ = [("dims", ctypes.c_int * (WRF_MLP_LAYERS + 1)), ("w", ctypes.c_void_p * WRF_MLP_LAYERS),
+                ("b", ctypes.c_void_p * WRF_MLP_LAYERS), ("norm", ctypes.c_void_p), ("tol_neg", ctypes.c_float),
+                ("tol_sat", ctypes.c_float)]
+
+
+class WrfMlpWorkC(ctypes.Structure):
+    """``WrfMlpWork`` of include/pywrf_b200.h"""
+    _fields_ = [("capacity", ctypes.c_int), ("x", ctypes.c_void_p), ("h", ctypes.c_void_p * 2),
+                ("y", ctypes.c_void_p), ("list", ctypes.c_void_p), ("err", ctypes.c_void_p)]
+
+
 _lib = None
 _names: list[str] | None = None
 _kinds: list[int] | None = None
@@ -71,6 +88,31 @@ def lib() -> ctypes.CDLL:
     L.wrf_status_read.restype = ip
     L.wrf_status_read.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int)]
     L.wrf_last_launch_count.restype = ip
+    G = ctypes.POINTER(WrfGridC)
+    ll, f32 = ctypes.c_longlong, ctypes.c_float
+    L.wrf_mlp_init.restype = ip
+    L.wrf_mlp_layout.restype = ip
+    L.wrf_mlp_layout.argtypes = [G, ctypes.POINTER(ctypes.c_int)]
+    L.wrf_rk3_step_mlp.restype = ip
+    L.wrf_rk3_step_mlp.argtypes = [G, vp, ctypes.POINTER(WrfMlpNetC), ctypes.POINTER(WrfMlpWorkC), vp, PROBE_FN, vp]
+    L.wrf_mlp_features.restype = ip
+    L.wrf_mlp_features.argtypes = [G, vp, vp, vp, vp, vp]
+    L.wrf_mlp_targets.restype = ip
+    L.wrf_mlp_targets.argtypes = [G, vp, vp, vp, vp]
+    L.wrf_mlp_normalize.restype = ip
+    L.wrf_mlp_normalize.argtypes = [G, vp, vp, vp, ll, vp, vp, vp]
+    L.wrf_gemm_bf16.restype = ip
+    L.wrf_gemm_bf16.argtypes = [vp, vp, ip, ip, ip, ip, ip, vp, vp, vp, ip, ll, vp, vp, ip, vp, vp]
+    L.wrf_gemm_splits.restype = ip
+    L.wrf_gemm_splits.argtypes = [ip, ip]
+    L.wrf_mse_grad.restype = ip
+    L.wrf_mse_grad.argtypes = [vp, vp, ip, ip, ip, f32, vp, vp, vp, vp]
+    L.wrf_rowsum_bf16.restype = ip
+    L.wrf_rowsum_bf16.argtypes = [vp, ip, ip, vp, vp]
+    L.wrf_adam.restype = ip
+    L.wrf_adam.argtypes = [vp, vp, ip, ll, vp, vp, ip, ip, vp, vp, f32, f32, f32, f32, f32, ip, vp]
+    L.wrf_transpose_bf16.restype = ip
+    L.wrf_transpose_bf16.argtypes = [vp, ip, ip, vp, vp]
     _lib = L
     return L
 

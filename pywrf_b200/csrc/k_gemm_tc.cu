@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       float v[16];
       tmem_ld16(trow + (uint32_t)(c * 16), v);
       if (!row) continue;
-      if (e.bias) {
+      if (e.bias && blockIdx.z == 0) {  // (once over the partial sums of a split reduction)
 #pragma unroll
         for (int t = 0; t < 16; ++t) v[t] += __ldg(&e.bias[n + t]);
       }
@@ -323,6 +323,23 @@ bool make_map(CUtensorMap* map, const void* ptr, int rows, int cols, const char*
 
 }  // namespace tc
 
+// the kernel's dynamic shared-memory limit, set once per device (the first
+// call should come before any stream capture)
+int gemm_prepare_device() {
+  constexpr int kMaxDev = 64;
+  static bool done[kMaxDev] = {};
+  static std::mutex mu;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return WRF_ECUDA;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return WRF_OK;
+  if (cudaFuncSetAttribute(tc::k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kSmemBytes) !=
+      cudaSuccess)
+    return WRF_ECUDA;
+  done[dev] = true;
+  return WRF_OK;
+}
+
 int launch_gemm_tc(const void* A, const void* B, int M, int N, int K, int splits, const GemmEpi& e, cudaStream_t st,
                    const char** err) {
   using namespace tc;
@@ -351,13 +368,9 @@ int launch_gemm_tc(const void* A, const void* B, int M, int N, int K, int splits
   splits = (kb_total + kper - 1) / kper;  // every split gets at least one k block
   CUtensorMap ma, mb;
   if (!make_map(&ma, A, M, K, err) || !make_map(&mb, B, N, K, err)) return WRF_EINVAL;
-  static bool attr_set = false;
-  if (!attr_set) {
-    if (cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) != cudaSuccess) {
-      *err = "gemm: cannot reserve the shared memory of the tile ring";
-      return WRF_ECUDA;
-    }
-    attr_set = true;
+  if (gemm_prepare_device() != WRF_OK) {
+    *err = "gemm: cannot reserve the shared memory of the tile ring";
+    return WRF_ECUDA;
   }
   const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, splits);
   k_gemm_tc<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, M, N, K, kper, e);

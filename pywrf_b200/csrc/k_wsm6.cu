@@ -17,6 +17,8 @@
 // and rounded once, as the reference does.
 #include <mutex>
 #include "kernels.cuh"
+#include "mlp.cuh"
+#include "tc_gemm.cuh"
 
 namespace wrf {
 namespace mp {
@@ -836,11 +838,17 @@ __device__ __forceinline__ void dummy_column(WCol<NS>& c) {
 }
 
 // moist_physics_prep_em + wsm6 + moist_physics_finish_em + calc_p_rho_phi;
-// block (x, y): SPB consecutive mass columns of row jds + y
-template <int SEG, int NS>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_physics(Grid g, S s, float dt) {
+// block (x, y): SPB consecutive mass columns of row jds + y.  With kList, the
+// columns are those of a list instead (list[0] entries from list[16], each
+// j * nx + i of a column of the scheme's block): the fallback of the
+// surrogate microphysics for the columns its gate rejected.
+template <int SEG, int NS, bool kList = false>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_physics(Grid g, S s, float dt, const int* list = nullptr) {
   constexpr int SPW = 32 / SEG, SPB = kWarpsPerBlock * SPW;
   __shared__ SegScratch<SEG, NS> scratch[SPB];
+  if constexpr (kList) {
+    if ((int)blockIdx.x * SPB >= __ldg(list)) return;  // whole block past the list (uniform exit)
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int segw = lane / SEG;
   Seg<SEG, NS> sg;
@@ -849,11 +857,22 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_physics(Grid g, S s, fl
   sg.km = g.nz - 1;
   const int km = sg.km;
   const int col = warp * SPW + segw;
-  const int j = g.jds + blockIdx.y;
-  const int i = g.ids + blockIdx.x * SPB + col;
-  const bool mass = i < g.ide - 1 && j < g.jde - 1;
-  const bool run = mass && j >= g.jds + 1 && j < g.jde - 2 && i >= g.ids + 1 && i < g.ide - 2;
-  const bool prep = mass && j >= g.jds + 1 && i >= g.ids + 1;
+  int j, i;
+  bool mass, run, prep;
+  if constexpr (kList) {
+    const int idx = blockIdx.x * SPB + col;
+    run = idx < __ldg(list);
+    const int code = run ? __ldg(list + 16 + idx) : 0;
+    j = code / g.nx;
+    i = code - j * g.nx;
+    mass = prep = run;
+  } else {
+    j = g.jds + blockIdx.y;
+    i = g.ids + blockIdx.x * SPB + col;
+    mass = i < g.ide - 1 && j < g.jde - 1;
+    run = mass && j >= g.jds + 1 && j < g.jde - 2 && i >= g.ids + 1 && i < g.ide - 2;
+    prep = mass && j >= g.jds + 1 && i >= g.ids + 1;
+  }
   const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
   const int c2 = mass ? g.i2(j, i) : 0;
   float* T = s[WF_T];
@@ -1268,6 +1287,108 @@ __global__ void __launch_bounds__(128) k_wsm6_finish_args(Grid g, Wsm6Args a, fl
   a.qg[p] = qr2;
 }
 
+// ------------------------------------------------------ surrogate microphysics
+// Apply the network's outputs (increments of theta, qv..qg per level and the
+// step's precipitation, standardised) to the mass points of the scheme's
+// block, with the gate: a column is rejected when an output is not finite,
+// when a species would go below -tol_neg before clipping, or when the new qv
+// exceeds saturation over water by more than the fraction tol_sat.  Rejected
+// columns are appended to list (count in list[0], entries j * nx + i from
+// list[16]) and left untouched; k_physics<..., true> then runs WSM6 on them.
+// Every other mass point gets the finish step (diabatic tendencies; zero
+// outside the block) and the equation of state, as k_wsm6_finish does.
+// Block: 32 consecutive mass columns of one row (lane) x 8 warps over levels.
+__global__ void __launch_bounds__(256) k_mlp_apply(Grid g, S s, MlpLayout L, const float* norm, const float* y,
+                                                   float tol_neg, float tol_sat, float dt, int* list) {
+  __shared__ int sflag[32];
+  const int tx = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = g.ids + blockIdx.x * 32 + tx, j = g.jds + blockIdx.y;
+  const bool mass = i < g.ide - 1;
+  const bool run = mass && j >= g.jds + 1 && j < g.jde - 2 && i >= g.ids + 1 && i < g.ide - 2;
+  const bool prep = mass && j >= g.jds + 1 && i >= g.ids + 1;
+  const int km = L.km;
+  const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
+  const int c2 = mass ? g.i2(j, i) : 0;
+  const size_t col = run ? (size_t)(j - g.jds - 1) * L.ncx + (i - g.ids - 1) : 0;
+  const float* yr = y + col * L.d4;
+  const float* omean = norm + norm_out_mean(L);
+  const float* ostd = norm + norm_out_std(L);
+  float* T = s[WF_T];
+  float* M = s[WF_MOIST];
+  auto inc = [&](int o) { return yr[o] * ostd[o] + omean[o]; };
+  if (w == 0) sflag[tx] = 0;
+  __syncthreads();
+  if (run) {
+    bool bad = false;
+    for (int k = w; k < km; k += 8) {
+      const size_t p = k * lev + c2;
+      const float dth = inc(k);
+      const float tnew = T[p] + dth;
+      bad = bad || !isfinite(dth);
+      float qvn = 0.f;
+      for (int m = 1; m < 7; ++m) {
+        const float d = inc(m * km + k);
+        const float qn = M[m * n3 + p] + d;
+        bad = bad || !isfinite(d) || qn < -tol_neg;
+        if (m == 1) qvn = fmaxf(qn, 0.f);
+      }
+      const float pfull = s[WF_P][p] + s[WF_PB][p];
+      const float tk = (tnew + (float)T0) * wpow(pfull / (float)P0, F(mp::RCP));
+      float qs0, qs1;
+      fpvs(tk, pfull, qs0, qs1);
+      bad = bad || !(qvn <= qs0 * (1.0f + tol_sat));
+    }
+    if (w == 0)
+      for (int o = 0; o < kOutPrecip; ++o) bad = bad || !isfinite(inc(kOutVars * km + o));
+    if (bad) atomicOr(&sflag[tx], 1);
+  }
+  __syncthreads();
+  const bool rejected = run && sflag[tx] != 0;
+  if (rejected && w == 0) {
+    const int slot = atomicAdd(list, 1);
+    list[16 + slot] = c2;
+  }
+  if (!mass || rejected) return;
+  for (int k = w; k < km; k += 8) {
+    const size_t p = k * lev + c2;
+    float tnew, qvnew;
+    if (run) {
+      const float dth = inc(k);
+      tnew = T[p] + dth;
+      T[p] = tnew;
+      s[WF_H_DIABATIC][p] = dth / dt;
+      const float qv0 = M[n3 + p], qc0 = M[2 * n3 + p];
+      float qn[7];
+      for (int m = 1; m < 7; ++m) qn[m] = fmaxf(M[m * n3 + p] + inc(m * km + k), 0.0f);
+      s[WF_QV_DIABATIC][p] = (qn[1] - qv0) / dt;
+      s[WF_QC_DIABATIC][p] = (qn[2] - qc0) / dt;
+      for (int m = 1; m < 7; ++m) M[m * n3 + p] = qn[m];
+      qvnew = qn[1];
+    } else {
+      if (prep) {
+        s[WF_H_DIABATIC][p] = 0.0f;
+        s[WF_QV_DIABATIC][p] = 0.0f;
+        s[WF_QC_DIABATIC][p] = 0.0f;
+      }
+      tnew = T[p];
+      qvnew = M[n3 + p];
+    }
+    eos_point(g, s, k, p, c2, tnew, qvnew);
+  }
+  if (run && w == 0) {
+    const float rain = fmaxf(inc(kOutVars * km + 0), 0.0f);
+    const float snow = fmaxf(inc(kOutVars * km + 1), 0.0f);
+    const float graupel = fmaxf(inc(kOutVars * km + 2), 0.0f);
+    s[WF_RAINNCV][c2] = rain;
+    s[WF_SNOWNCV][c2] = snow;
+    s[WF_GRAUPELNCV][c2] = graupel;
+    s[WF_RAINNC][c2] = s[WF_RAINNC][c2] + rain;
+    s[WF_SNOWNC][c2] = s[WF_SNOWNC][c2] + snow;
+    s[WF_GRAUPELNC][c2] = s[WF_GRAUPELNC][c2] + graupel;
+    s[WF_SR][c2] = rain > 0.f ? (snow + graupel) / (rain + 1.0e-12f) : 0.0f;
+  }
+}
+
 #undef F
 
 // 16-lane segments with 3 levels per lane hold up to 47 mass levels; deeper
@@ -1370,6 +1491,65 @@ int launch_wsm6_noalloc(const Grid& g, float* const* f, float delt, cudaStream_t
   const dim3 b3(32, 4);
   k_wsm6_finish_args<<<point_grid(g, b3), b3, 0, st>>>(g, a, dtcld, base, base + kNoAllocMaxPoints);
   return 2;
+}
+
+
+int launch_physics_mlp(const Grid& g, const S& s, const MlpNetDev& net, const MlpWorkDev& work, cudaStream_t st,
+                       const char** err) {
+  const MlpLayout L = MlpLayout::make(g.nx, g.ny, g.nz, g.ids, g.ide, g.jds, g.jde);
+  if (net.dims[0] != L.d0 || net.dims[kMlpLayers] != L.d4) {
+    *err = "surrogate: the network's input / output widths do not match this grid's column layout";
+    return WRF_EINVAL;
+  }
+  for (int l = 1; l < kMlpLayers; ++l)
+    if (net.dims[l] < 64 || net.dims[l] % 64) {
+      *err = "surrogate: hidden widths must be multiples of 64";
+      return WRF_EINVAL;
+    }
+  for (int l = 0; l < kMlpLayers; ++l)
+    if (!net.w[l] || !net.b[l]) {
+      *err = "surrogate: null weight or bias";
+      return WRF_EINVAL;
+    }
+  if (!net.norm || !work.x || !work.h[0] || !work.h[1] || !work.y || !work.list || work.capacity < L.ncols) {
+    *err = "surrogate: null buffer, or work capacity below the block's column count";
+    return WRF_EINVAL;
+  }
+  int n = 0;
+  if (cudaMemsetAsync(work.list, 0, 16 * sizeof(int), st) != cudaSuccess) {
+    *err = "surrogate: memset of the fallback list failed";
+    return WRF_ECUDA;
+  }
+  int r = launch_mlp_features(g, s, L, net.norm, work.x, nullptr, st);
+  if (r < 0) { *err = "surrogate: feature kernel set-up failed"; return r; }
+  n += r;
+  const void* in = work.x;
+  for (int l = 0; l < kMlpLayers; ++l) {
+    const bool last = l == kMlpLayers - 1;
+    GemmEpi e{};
+    e.kind = last ? EPI_F32 : EPI_BIAS_GELU;
+    e.bias = net.b[l];
+    e.out = last ? static_cast<void*>(work.y) : work.h[l & 1];
+    e.ldo = net.dims[l + 1];
+    e.err = work.err;
+    r = launch_gemm_tc(in, net.w[l], L.ncols, net.dims[l + 1], net.dims[l], 1, e, st, err);
+    if (r < 0) return r;
+    n += r;
+    in = e.out;
+  }
+  k_mlp_apply<<<dim3((g.ide - 1 - g.ids + 31) / 32, g.jde - 1 - g.jds), 256, 0, st>>>(
+      g, s, L, net.norm, work.y, net.tol_neg, net.tol_sat, g.dt, work.list);
+  ++n;
+  const int km = g.nz - 1;
+  const dim3 b(32 * kWarpsPerBlock);
+  if (km <= 47) {
+    constexpr int SPB = kWarpsPerBlock * 2;
+    k_physics<16, 3, true><<<(L.ncols + SPB - 1) / SPB, b, 0, st>>>(g, s, g.dt, work.list);
+  } else {
+    constexpr int SPB = kWarpsPerBlock;
+    k_physics<32, 2, true><<<(L.ncols + SPB - 1) / SPB, b, 0, st>>>(g, s, g.dt, work.list);
+  }
+  return n + 1;
 }
 
 }  // namespace wrf

@@ -10,6 +10,8 @@
 #include <cctype>
 #include <string>
 #include "kernels.cuh"
+#include "mlp.cuh"
+#include "tc_gemm.cuh"
 
 namespace wrf {
 namespace {
@@ -96,6 +98,8 @@ struct Driver {
   cudaStream_t st;
   wrf_probe_fn probe;
   void* user;
+  const MlpNetDev* net = nullptr;   // surrogate microphysics when set
+  const MlpWorkDev* work = nullptr;
   int rc = WRF_OK;
   int n = 0;  // kernels enqueued
 
@@ -218,8 +222,18 @@ struct Driver {
       snprintf(tag, sizeof tag, "s%d.moist", rk);
       phase(tag);
     }
-    // microphysics (solver.py:1714-1766)
-    n += launch_physics(g, s, st);
+    // microphysics (solver.py:1714-1766), or its learned stand-in
+    if (net) {
+      const char* err = nullptr;
+      const int r = launch_physics_mlp(g, s, *net, *work, st, &err);
+      if (r < 0) {
+        rc = fail(r, err ? err : "surrogate microphysics failed");
+        return;
+      }
+      n += r;
+    } else {
+      n += launch_physics(g, s, st);
+    }
     phase("mp");
     // end-of-step boundaries (solver.py:1776-1910)
     bc({{WF_U_1, 'U'}, {WF_U, 'U'}, {WF_V_1, 'V'}, {WF_V, 'V'}, {WF_W_1, 'w'}, {WF_W, 'w'}, {WF_T_1, 'p'},
@@ -336,6 +350,168 @@ int wrf_status_read(const WrfState* sin, void* stream, int* out16) {
     return check_launch("status_read");
   if (cudaStreamSynchronize(st) != cudaSuccess) return check_launch("status_read");
   return WRF_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- network
+namespace {
+MlpLayout layout_of(const Grid& g) { return MlpLayout::make(g.nx, g.ny, g.nz, g.ids, g.ide, g.jds, g.jde); }
+int ret_launch(int r, const char* err, const char* where) {
+  if (r < 0) return fail(r, err ? err : where);
+  return check_launch(where);
+}
+}  // namespace
+
+extern "C" {
+
+int wrf_mlp_init(void) {
+  if (mlp_prepare_device() != WRF_OK) return fail(WRF_ECUDA, "mlp_init: cannot set the kernels' shared-memory limits");
+  return WRF_OK;
+}
+
+int wrf_mlp_layout(const WrfGrid* gin, int* out8) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!out8) return fail(WRF_EINVAL, "null argument");
+  const MlpLayout L = layout_of(g);
+  const int v[8] = {L.km, L.ncx, L.ncy, L.ncols, L.nfeat, L.d0, L.nout, L.d4};
+  for (int i = 0; i < 8; ++i) out8[i] = v[i];
+  return WRF_OK;
+}
+
+int wrf_rk3_step_mlp(const WrfGrid* gin, const WrfState* sin, const WrfMlpNet* net, const WrfMlpWork* work,
+                     void* stream, wrf_probe_fn probe, void* user) {
+  if (!net || !work) return fail(WRF_EINVAL, "null network or work buffers");
+  MlpNetDev nd;
+  for (int l = 0; l <= kMlpLayers; ++l) nd.dims[l] = net->dims[l];
+  for (int l = 0; l < kMlpLayers; ++l) {
+    nd.w[l] = net->w[l];
+    nd.b[l] = net->b[l];
+  }
+  nd.norm = net->norm;
+  nd.tol_neg = net->tol_neg;
+  nd.tol_sat = net->tol_sat;
+  MlpWorkDev wd;
+  wd.capacity = work->capacity;
+  wd.x = work->x;
+  wd.h[0] = work->h[0];
+  wd.h[1] = work->h[1];
+  wd.y = work->y;
+  wd.list = work->list;
+  wd.err = work->err;
+  Driver d;
+  int rc = make_grid(gin, d.g);
+  if (rc) return rc;
+  rc = make_state(sin, d.s);
+  if (rc) return rc;
+  d.st = static_cast<cudaStream_t>(stream);
+  d.probe = probe;
+  d.user = user;
+  d.bdy_interval = gin->bdy_interval;
+  d.net = &nd;
+  d.work = &wd;
+  cudaGetLastError();
+  d.run();
+  g_last_launches = d.n;
+  return d.rc;
+}
+
+int wrf_mlp_features(const WrfGrid* gin, const WrfState* sin, const float* norm, void* x, float* raw, void* stream) {
+  Grid g;
+  S s;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  rc = make_state(sin, s);
+  if (rc) return rc;
+  if (!raw && (!x || !norm)) return fail(WRF_EINVAL, "null argument");
+  cudaGetLastError();
+  const int r = launch_mlp_features(g, s, layout_of(g), norm, x, raw, static_cast<cudaStream_t>(stream));
+  return ret_launch(r, nullptr, "mlp_features");
+}
+
+int wrf_mlp_targets(const WrfGrid* gin, const WrfState* sin, const float* raw_in, float* raw_out, void* stream) {
+  Grid g;
+  S s;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  rc = make_state(sin, s);
+  if (rc) return rc;
+  if (!raw_in || !raw_out) return fail(WRF_EINVAL, "null argument");
+  cudaGetLastError();
+  return ret_launch(launch_mlp_targets(g, s, layout_of(g), raw_in, raw_out, static_cast<cudaStream_t>(stream)),
+                    nullptr, "mlp_targets");
+}
+
+int wrf_mlp_normalize(const WrfGrid* gin, const float* norm, const float* raw_in, const float* raw_out, long long n,
+                      void* x, float* t, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!norm || !raw_in || !raw_out || !x || !t || n < 0) return fail(WRF_EINVAL, "null argument or n < 0");
+  cudaGetLastError();
+  return ret_launch(launch_mlp_normalize(layout_of(g), norm, raw_in, raw_out, n, x, t,
+                                         static_cast<cudaStream_t>(stream)),
+                    nullptr, "mlp_normalize");
+}
+
+int wrf_gemm_bf16(const void* a, const void* b, int m, int n, int k, int splits, int epi, const float* bias,
+                  const void* aux, void* out, int ldo, long long split_stride, void* out_z, void* out_t, int ldt,
+                  int* err, void* stream) {
+  GemmEpi e{};
+  e.kind = epi;
+  e.bias = bias;
+  e.aux = static_cast<const __nv_bfloat16*>(aux);
+  e.out = out;
+  e.ldo = ldo;
+  e.split_stride = split_stride;
+  e.out_z = static_cast<__nv_bfloat16*>(out_z);
+  e.out_t = static_cast<__nv_bfloat16*>(out_t);
+  e.ldt = ldt;
+  e.err = err;
+  if (epi == EPI_F32 && gemm_splits_used(k, splits) > 1 && split_stride < (long long)m * ldo)
+    return fail(WRF_EINVAL, "gemm: split_stride smaller than one partial sum");
+  if (epi == EPI_F32 && (split_stride % 4)) return fail(WRF_EINVAL, "gemm: split_stride must be a multiple of 4");
+  cudaGetLastError();
+  const char* msg = nullptr;
+  const int r = launch_gemm_tc(a, b, m, n, k, splits, e, static_cast<cudaStream_t>(stream), &msg);
+  return ret_launch(r, msg, "gemm_bf16");
+}
+
+int wrf_gemm_splits(int k, int splits) { return gemm_splits_used(k, splits); }
+
+int wrf_mse_grad(const float* y, const float* t, int m, int n, int nvalid, float scale, void* dy, void* dyt,
+                 float* loss, void* stream) {
+  if (!y || !t || !dy || !dyt || !loss || m < 1 || n < 1) return fail(WRF_EINVAL, "null argument or empty matrix");
+  cudaGetLastError();
+  return ret_launch(launch_mse_grad(y, t, m, n, nvalid, scale, dy, dyt, loss, static_cast<cudaStream_t>(stream)),
+                    nullptr, "mse_grad");
+}
+
+int wrf_rowsum_bf16(const void* a, int rows, int cols, float* out, void* stream) {
+  if (!a || !out || rows < 1 || cols < 1) return fail(WRF_EINVAL, "null argument or empty matrix");
+  cudaGetLastError();
+  return ret_launch(launch_rowsum_bf16(a, rows, cols, out, static_cast<cudaStream_t>(stream)), nullptr,
+                    "rowsum_bf16");
+}
+
+int wrf_adam(float* w, const float* gpart, int nsplit, long long split_stride, float* m, float* v, int r, int c,
+             void* wb, void* wtb, float lr, float beta1, float beta2, float eps, float wd, int step, void* stream) {
+  if (!w || !gpart || !m || !v || r < 1 || c < 1 || nsplit < 1 || step < 1)
+    return fail(WRF_EINVAL, "null argument, empty matrix, or step < 1");
+  const float bc1 = (float)(1.0 - pow((double)beta1, step)), bc2 = (float)(1.0 - pow((double)beta2, step));
+  cudaGetLastError();
+  return ret_launch(launch_adam(w, gpart, nsplit, split_stride, m, v, r, c, wb, wtb, lr, beta1, beta2, eps, wd, bc1,
+                                bc2, static_cast<cudaStream_t>(stream)),
+                    nullptr, "adam");
+}
+
+int wrf_transpose_bf16(const void* a, int r, int c, void* out, void* stream) {
+  if (!a || !out || r < 1 || c < 1) return fail(WRF_EINVAL, "null argument or empty matrix");
+  cudaGetLastError();
+  return ret_launch(launch_transpose_bf16(a, r, c, out, static_cast<cudaStream_t>(stream)), nullptr,
+                    "transpose_bf16");
 }
 
 }  // extern "C"

@@ -29,6 +29,8 @@ struct GemmEpi {
 // C = A B^T on the tensor cores; returns kernels enqueued (1) or WRF_E* with *err
 int launch_gemm_tc(const void* A, const void* B, int M, int N, int K, int splits, const GemmEpi& e, cudaStream_t st,
                    const char** err);
+// one-time per-device set-up of the GEMM kernel (WRF_OK or WRF_ECUDA)
+int gemm_prepare_device();
 // number of K splits launch_gemm_tc uses for a requested count
 int gemm_splits_used(int K, int splits);
 
