@@ -180,8 +180,12 @@ typedef struct WrfMlpWork {        /* caller-owned device scratch of one surroga
   void* x;                         /* bf16 [capacity][d0] */
   void* h[2];                      /* bf16 [capacity][max hidden width] */
   float* y;                        /* fp32 [capacity][d4] */
-  int* list;                       /* int [16 + capacity]: [0] rejected columns, [16..] their j * nx + i */
+  int* list;                       /* int [16 + capacity]: [0] rejected columns, [1] quiet columns (no
+                                      condensate, subsaturated: zero increments without the network),
+                                      [2] [3] [4] rejections for positivity / supersaturation / a non-finite
+                                      output, [16..] the rejected columns' j * nx + i */
   int* err;                        /* int: set to 1 if a tensor-core kernel's bounded wait ran out */
+  void* colstat;                   /* optional uint8 [capacity]: 0 network, 1 quiet, 2 rejected */
 } WrfMlpWork;
 
 /* one-time set-up of the network's kernels on the current device; call it
@@ -196,6 +200,10 @@ int wrf_mlp_layout(const WrfGrid* g, int* out8);
  * WSM6 (the fused column kernel) on the rejected columns */
 int wrf_rk3_step_mlp(const WrfGrid* g, const WrfState* s, const WrfMlpNet* net, const WrfMlpWork* work,
                      void* stream, wrf_probe_fn probe, void* user);
+
+/* the network alone on m rows: x bf16 [m][d0] -> y fp32 [m][d4] (h0, h1: bf16 [m][max hidden]) */
+int wrf_mlp_forward(const WrfMlpNet* net, const void* x, int m, void* h0, void* h1, float* y, int* err,
+                    void* stream);
 
 /* network rows of the state's columns: x (bf16, standardised with norm) if
  * raw is NULL, else raw (fp32 [ncols][10 km]: T p rho qv qc qr qi qs qg theta') */

@@ -47,7 +47,8 @@ class WrfMlpNetC(ctypes.Structure):
 class WrfMlpWorkC(ctypes.Structure):
     """``WrfMlpWork`` of include/pywrf_b200.h"""
     _fields_ = [("capacity", ctypes.c_int), ("x", ctypes.c_void_p), ("h", ctypes.c_void_p * 2),
-                ("y", ctypes.c_void_p), ("list", ctypes.c_void_p), ("err", ctypes.c_void_p)]
+                ("y", ctypes.c_void_p), ("list", ctypes.c_void_p), ("err", ctypes.c_void_p),
+                ("colstat", ctypes.c_void_p)]
 
 
 _lib = None
@@ -95,6 +96,8 @@ def lib() -> ctypes.CDLL:
     L.wrf_mlp_layout.argtypes = [G, ctypes.POINTER(ctypes.c_int)]
     L.wrf_rk3_step_mlp.restype = ip
     L.wrf_rk3_step_mlp.argtypes = [G, vp, ctypes.POINTER(WrfMlpNetC), ctypes.POINTER(WrfMlpWorkC), vp, PROBE_FN, vp]
+    L.wrf_mlp_forward.restype = ip
+    L.wrf_mlp_forward.argtypes = [ctypes.POINTER(WrfMlpNetC), vp, ip, vp, vp, vp, vp, vp]
     L.wrf_mlp_features.restype = ip
     L.wrf_mlp_features.argtypes = [G, vp, vp, vp, vp, vp]
     L.wrf_mlp_targets.restype = ip

@@ -1290,17 +1290,31 @@ __global__ void __launch_bounds__(128) k_wsm6_finish_args(Grid g, Wsm6Args a, fl
 // ------------------------------------------------------ surrogate microphysics
 // Apply the network's outputs (increments of theta, qv..qg per level and the
 // step's precipitation, standardised) to the mass points of the scheme's
-// block, with the gate: a column is rejected when an output is not finite,
-// when a species would go below -tol_neg before clipping, or when the new qv
-// exceeds saturation over water by more than the fraction tol_sat.  Rejected
-// columns are appended to list (count in list[0], entries j * nx + i from
-// list[16]) and left untouched; k_physics<..., true> then runs WSM6 on them.
-// Every other mass point gets the finish step (diabatic tendencies; zero
-// outside the block) and the equation of state, as k_wsm6_finish does.
+// block.  Per column, in this order:
+//   quiet     no condensate at any level and qv below saturation (over ice
+//             where T < T0, else over water) at every level: WSM6 has no
+//             process to run there, so the column takes zero increments
+//             whatever the network says;
+//   rejected  (the gate) an output is not finite, a species would go below
+//             -tol_neg before clipping, or the new qv exceeds saturation over
+//             water by more than the fraction tol_sat: the column is left
+//             untouched and appended to list (entries j * nx + i from
+//             list[16]); k_physics<..., true> then runs WSM6 on it;
+//   network   otherwise: the increments (species clipped at zero).
+// The step's precipitation is clipped to [0, condensate within kMlpMaxFall *
+// dt of the ground] (all species for rainncv, snow + ice for snowncv, graupel
+// for graupelncv): nothing else can reach the ground in one step.
+// Counters: list[0] rejected, list[1] quiet, list[2] rejected for
+// positivity, list[3] for supersaturation, list[4] for a non-finite output.
+// colstat (optional) receives 0 network / 1 quiet / 2 rejected per column.
+// Every other mass point gets the finish step (zero diabatic tendencies) and
+// the equation of state, as in k_wsm6_finish.
 // Block: 32 consecutive mass columns of one row (lane) x 8 warps over levels.
 __global__ void __launch_bounds__(256) k_mlp_apply(Grid g, S s, MlpLayout L, const float* norm, const float* y,
-                                                   float tol_neg, float tol_sat, float dt, int* list) {
-  __shared__ int sflag[32];
+                                                   float tol_neg, float tol_sat, float dt, int* list,
+                                                   unsigned char* colstat) {
+  __shared__ int sbad[32], squiet[32];
+  __shared__ float scap[3][32];   // precipitable condensate near the ground: all, snow + ice, graupel (kg m-2)
   const int tx = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = g.ids + blockIdx.x * 32 + tx, j = g.jds + blockIdx.y;
   const bool mass = i < g.ide - 1;
@@ -1316,43 +1330,83 @@ __global__ void __launch_bounds__(256) k_mlp_apply(Grid g, S s, MlpLayout L, con
   float* T = s[WF_T];
   float* M = s[WF_MOIST];
   auto inc = [&](int o) { return yr[o] * ostd[o] + omean[o]; };
-  if (w == 0) sflag[tx] = 0;
+  if (w == 0) {
+    sbad[tx] = 0;
+    squiet[tx] = 1;
+    scap[0][tx] = scap[1][tx] = scap[2][tx] = 0.f;
+  }
   __syncthreads();
   if (run) {
-    bool bad = false;
+    int bad = 0, quiet = 1;
+    const float* php = s[WF_PH];
+    const float* phb = s[WF_PHB];
+    const float zs = (php[c2] + phb[c2]) / (float)G;
+    const float reach = kMlpMaxFall * dt;
+    float cap_all = 0.f, cap_snow = 0.f, cap_graupel = 0.f;
     for (int k = w; k < km; k += 8) {
       const size_t p = k * lev + c2;
+      // condensate that can reach the ground within the step (levels whose
+      // bottom lies within kMlpMaxFall * dt of it), kg m-2
+      const float zb = (php[p] + phb[p]) / (float)G, zt = (php[p + lev] + phb[p + lev]) / (float)G;
+      if (zb - zs < reach) {
+        const float rdz = (zt - zb) / (s[WF_AL][p] + s[WF_ALB][p]);
+        const float qr = fmaxf(M[3 * n3 + p], 0.f), qi = fmaxf(M[4 * n3 + p], 0.f);
+        const float qsn = fmaxf(M[5 * n3 + p], 0.f), qg = fmaxf(M[6 * n3 + p], 0.f);
+        cap_all += (qr + qi + qsn + qg) * rdz;
+        cap_snow += (qi + qsn) * rdz;
+        cap_graupel += qg * rdz;
+      }
+      const float pfull = s[WF_P][p] + s[WF_PB][p];
+      const float pii = wpow(pfull / (float)P0, F(mp::RCP));
+      float qs0, qs1;
+      fpvs((T[p] + (float)T0) * pii, pfull, qs0, qs1);
+      float cond = 0.f;
+      for (int m = 2; m < 7; ++m) cond = fmaxf(cond, fabsf(M[m * n3 + p]));
+      if (cond != 0.f || !(M[n3 + p] < qs1)) quiet = 0;
       const float dth = inc(k);
       const float tnew = T[p] + dth;
-      bad = bad || !isfinite(dth);
+      if (!isfinite(dth)) bad |= 4;
       float qvn = 0.f;
       for (int m = 1; m < 7; ++m) {
         const float d = inc(m * km + k);
         const float qn = M[m * n3 + p] + d;
-        bad = bad || !isfinite(d) || qn < -tol_neg;
+        if (!isfinite(d)) bad |= 4;
+        if (qn < -tol_neg) bad |= 1;
         if (m == 1) qvn = fmaxf(qn, 0.f);
       }
-      const float pfull = s[WF_P][p] + s[WF_PB][p];
-      const float tk = (tnew + (float)T0) * wpow(pfull / (float)P0, F(mp::RCP));
-      float qs0, qs1;
-      fpvs(tk, pfull, qs0, qs1);
-      bad = bad || !(qvn <= qs0 * (1.0f + tol_sat));
+      fpvs((tnew + (float)T0) * pii, pfull, qs0, qs1);
+      if (!(qvn <= qs0 * (1.0f + tol_sat))) bad |= 2;
     }
     if (w == 0)
-      for (int o = 0; o < kOutPrecip; ++o) bad = bad || !isfinite(inc(kOutVars * km + o));
-    if (bad) atomicOr(&sflag[tx], 1);
+      for (int o = 0; o < kOutPrecip; ++o)
+        if (!isfinite(inc(kOutVars * km + o))) bad |= 4;
+    if (bad) atomicOr(&sbad[tx], bad);
+    if (!quiet) atomicAnd(&squiet[tx], 0);
+    atomicAdd(&scap[0][tx], cap_all);
+    atomicAdd(&scap[1][tx], cap_snow);
+    atomicAdd(&scap[2][tx], cap_graupel);
   }
   __syncthreads();
-  const bool rejected = run && sflag[tx] != 0;
-  if (rejected && w == 0) {
-    const int slot = atomicAdd(list, 1);
-    list[16 + slot] = c2;
+  const bool quiet = run && squiet[tx] != 0;
+  const int bad = run && !quiet ? sbad[tx] : 0;
+  const bool rejected = bad != 0;
+  if (run && w == 0) {
+    if (quiet) atomicAdd(list + 1, 1);
+    if (rejected) {
+      const int slot = atomicAdd(list, 1);
+      list[16 + slot] = c2;
+      if (bad & 1) atomicAdd(list + 2, 1);
+      if (bad & 2) atomicAdd(list + 3, 1);
+      if (bad & 4) atomicAdd(list + 4, 1);
+    }
+    if (colstat) colstat[col] = quiet ? 1 : (rejected ? 2 : 0);
   }
   if (!mass || rejected) return;
+  const bool net = run && !quiet;
   for (int k = w; k < km; k += 8) {
     const size_t p = k * lev + c2;
     float tnew, qvnew;
-    if (run) {
+    if (net) {
       const float dth = inc(k);
       tnew = T[p] + dth;
       T[p] = tnew;
@@ -1376,9 +1430,10 @@ __global__ void __launch_bounds__(256) k_mlp_apply(Grid g, S s, MlpLayout L, con
     eos_point(g, s, k, p, c2, tnew, qvnew);
   }
   if (run && w == 0) {
-    const float rain = fmaxf(inc(kOutVars * km + 0), 0.0f);
-    const float snow = fmaxf(inc(kOutVars * km + 1), 0.0f);
-    const float graupel = fmaxf(inc(kOutVars * km + 2), 0.0f);
+    // precipitation of the step, bounded by what can fall out of the column
+    const float rain = net ? fminf(fmaxf(inc(kOutVars * km + 0), 0.0f), scap[0][tx]) : 0.0f;
+    const float snow = net ? fminf(fmaxf(inc(kOutVars * km + 1), 0.0f), scap[1][tx]) : 0.0f;
+    const float graupel = net ? fminf(fmaxf(inc(kOutVars * km + 2), 0.0f), scap[2][tx]) : 0.0f;
     s[WF_RAINNCV][c2] = rain;
     s[WF_SNOWNCV][c2] = snow;
     s[WF_GRAUPELNCV][c2] = graupel;
@@ -1494,6 +1549,27 @@ int launch_wsm6_noalloc(const Grid& g, float* const* f, float delt, cudaStream_t
 }
 
 
+int launch_mlp_forward(const MlpNetDev& net, const void* x, int m, void* h0, void* h1, float* y, int* errflag,
+                       cudaStream_t st, const char** err) {
+  int n = 0;
+  const void* in = x;
+  void* h[2] = {h0, h1};
+  for (int l = 0; l < kMlpLayers; ++l) {
+    const bool last = l == kMlpLayers - 1;
+    GemmEpi e{};
+    e.kind = last ? EPI_F32 : EPI_BIAS_GELU;
+    e.bias = net.b[l];
+    e.out = last ? static_cast<void*>(y) : h[l & 1];
+    e.ldo = net.dims[l + 1];
+    e.err = errflag;
+    const int r = launch_gemm_tc(in, net.w[l], m, net.dims[l + 1], net.dims[l], 1, e, st, err);
+    if (r < 0) return r;
+    n += r;
+    in = e.out;
+  }
+  return n;
+}
+
 int launch_physics_mlp(const Grid& g, const S& s, const MlpNetDev& net, const MlpWorkDev& work, cudaStream_t st,
                        const char** err) {
   const MlpLayout L = MlpLayout::make(g.nx, g.ny, g.nz, g.ids, g.ide, g.jds, g.jde);
@@ -1523,22 +1599,12 @@ int launch_physics_mlp(const Grid& g, const S& s, const MlpNetDev& net, const Ml
   int r = launch_mlp_features(g, s, L, net.norm, work.x, nullptr, st);
   if (r < 0) { *err = "surrogate: feature kernel set-up failed"; return r; }
   n += r;
-  const void* in = work.x;
-  for (int l = 0; l < kMlpLayers; ++l) {
-    const bool last = l == kMlpLayers - 1;
-    GemmEpi e{};
-    e.kind = last ? EPI_F32 : EPI_BIAS_GELU;
-    e.bias = net.b[l];
-    e.out = last ? static_cast<void*>(work.y) : work.h[l & 1];
-    e.ldo = net.dims[l + 1];
-    e.err = work.err;
-    r = launch_gemm_tc(in, net.w[l], L.ncols, net.dims[l + 1], net.dims[l], 1, e, st, err);
-    if (r < 0) return r;
-    n += r;
-    in = e.out;
-  }
+  r = launch_mlp_forward(net, work.x, L.ncols, work.h[0], work.h[1], work.y, work.err, st, err);
+  if (r < 0) return r;
+  n += r;
   k_mlp_apply<<<dim3((g.ide - 1 - g.ids + 31) / 32, g.jde - 1 - g.jds), 256, 0, st>>>(
-      g, s, L, net.norm, work.y, net.tol_neg, net.tol_sat, g.dt, work.list);
+      g, s, L, net.norm, work.y, net.tol_neg, net.tol_sat, g.dt, work.list,
+      static_cast<unsigned char*>(work.colstat));
   ++n;
   const int km = g.nz - 1;
   const dim3 b(32 * kWarpsPerBlock);

@@ -22,6 +22,8 @@ constexpr int kRawVars = 10;       // the features + theta perturbation (harvest
 constexpr int kOutVars = 7;        // theta qv qc qr qi qs qg increments
 constexpr int kOutPrecip = 3;      // rainncv snowncv graupelncv
 constexpr float kLogFloor = 1.0e-12f;
+// upper bound of the scheme's fall speeds (m/s) used to bound one step's precipitation
+constexpr float kMlpMaxFall = 15.0f;
 
 struct MlpLayout {
   int km, ncx, ncy, ncols;
@@ -62,8 +64,9 @@ struct MlpWorkDev {
   void* x;        // bf16 [capacity][d0]
   void* h[2];     // bf16 [capacity][hidden]
   float* y;       // fp32 [capacity][d4]
-  int* list;      // [0] fallback count, [16 + n] flat column index j * nx + i
+  int* list;      // [0] rejected count, [1..4] quiet / rejection-reason counters, [16 + n] j * nx + i
   int* err;       // wait-timeout flag of the GEMMs
+  void* colstat;  // optional uint8 [capacity]: 0 network, 1 quiet, 2 rejected
 };
 
 // one-time per-device set-up of the network's kernels (shared-memory limits);
@@ -86,6 +89,9 @@ int launch_adam(float* w, const float* gpart, int nsplit, long long split_stride
                 void* wb, void* wtb, float lr, float b1, float b2, float eps, float wd, float bc1, float bc2,
                 cudaStream_t st);
 int launch_transpose_bf16(const void* a, int R, int C, void* out, cudaStream_t st);
+// the network's four products on m rows: x -> h0 -> h1 -> h0 -> y (bias + GELU fused)
+int launch_mlp_forward(const MlpNetDev& net, const void* x, int m, void* h0, void* h1, float* y, int* errflag,
+                       cudaStream_t st, const char** err);
 // surrogate microphysics of one step: features, the network, apply + gate, WSM6 on flagged columns
 int launch_physics_mlp(const Grid& g, const S& s, const MlpNetDev& net, const MlpWorkDev& work, cudaStream_t st,
                        const char** err);

@@ -381,9 +381,10 @@ int wrf_mlp_layout(const WrfGrid* gin, int* out8) {
   return WRF_OK;
 }
 
-int wrf_rk3_step_mlp(const WrfGrid* gin, const WrfState* sin, const WrfMlpNet* net, const WrfMlpWork* work,
-                     void* stream, wrf_probe_fn probe, void* user) {
-  if (!net || !work) return fail(WRF_EINVAL, "null network or work buffers");
+}  // extern "C"
+
+namespace {
+MlpNetDev net_of(const WrfMlpNet* net) {
   MlpNetDev nd;
   for (int l = 0; l <= kMlpLayers; ++l) nd.dims[l] = net->dims[l];
   for (int l = 0; l < kMlpLayers; ++l) {
@@ -393,6 +394,28 @@ int wrf_rk3_step_mlp(const WrfGrid* gin, const WrfState* sin, const WrfMlpNet* n
   nd.norm = net->norm;
   nd.tol_neg = net->tol_neg;
   nd.tol_sat = net->tol_sat;
+  return nd;
+}
+}  // namespace
+
+extern "C" {
+
+int wrf_mlp_forward(const WrfMlpNet* net, const void* x, int m, void* h0, void* h1, float* y, int* err,
+                    void* stream) {
+  if (!net || !x || !h0 || !h1 || !y || m < 1) return fail(WRF_EINVAL, "null argument or m < 1");
+  for (int l = 0; l < kMlpLayers; ++l)
+    if (!net->w[l] || !net->b[l]) return fail(WRF_EINVAL, "null weight or bias");
+  const MlpNetDev nd = net_of(net);
+  cudaGetLastError();
+  const char* msg = nullptr;
+  const int r = launch_mlp_forward(nd, x, m, h0, h1, y, err, static_cast<cudaStream_t>(stream), &msg);
+  return ret_launch(r, msg, "mlp_forward");
+}
+
+int wrf_rk3_step_mlp(const WrfGrid* gin, const WrfState* sin, const WrfMlpNet* net, const WrfMlpWork* work,
+                     void* stream, wrf_probe_fn probe, void* user) {
+  if (!net || !work) return fail(WRF_EINVAL, "null network or work buffers");
+  const MlpNetDev nd = net_of(net);
   MlpWorkDev wd;
   wd.capacity = work->capacity;
   wd.x = work->x;
@@ -401,6 +424,7 @@ int wrf_rk3_step_mlp(const WrfGrid* gin, const WrfState* sin, const WrfMlpNet* n
   wd.y = work->y;
   wd.list = work->list;
   wd.err = work->err;
+  wd.colstat = work->colstat;
   Driver d;
   int rc = make_grid(gin, d.g);
   if (rc) return rc;

@@ -74,6 +74,7 @@ class MlpNet:
         self.norm[d0:2 * d0] = 1.0
         self.norm[2 * d0 + d4:] = 1.0
         self.adam_step = 0
+        self.precip_weight = 4.0
 
     def fit_normalisation(self, raw_in: torch.Tensor, raw_out: torch.Tensor) -> None:
         """Standardisation from harvested raw rows (dataset preparation):
@@ -95,6 +96,9 @@ class MlpNet:
             blk = ostd[v * km:(v + 1) * km]
             blk.copy_(torch.where(blk > 0, blk.clamp_min(0.01 * float(blk.max())), blk))
         ostd = torch.where(ostd > 0, ostd, 0.0)
+        # the three precipitation outputs (one value per column against 40
+        # per species) weigh precip_weight^2 more in the standardised loss
+        ostd[7 * km:] = ostd[7 * km:] / self.precip_weight
         n = torch.zeros(2 * d0 + 2 * d4, dtype=torch.float64, device=self.device)
         n[:nfeat] = mean
         n[d0:d0 + nfeat] = rstd
@@ -295,6 +299,7 @@ class SurrogateIntegrator(Integrator):
         self.y = torch.empty(cap, net.dims[4], device=dev)
         self.list = torch.zeros(16 + cap, dtype=torch.int32, device=dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.colstat = torch.zeros(cap, dtype=torch.uint8, device=dev)
         self.work = N.WrfMlpWorkC()
         self.work.capacity = cap
         self.work.x = self.x.data_ptr()
@@ -303,6 +308,7 @@ class SurrogateIntegrator(Integrator):
         self.work.y = self.y.data_ptr()
         self.work.list = self.list.data_ptr()
         self.work.err = self.err.data_ptr()
+        self.work.colstat = self.colstat.data_ptr()
         self.netc = net.cstruct(tol_neg, tol_sat)
         self._mlp_graph: torch.cuda.CUDAGraph | None = None
         self.nstep = 0
@@ -353,6 +359,14 @@ class SurrogateIntegrator(Integrator):
     def rejected(self) -> int:
         """Columns the gate rejected in the last surrogate step."""
         return int(self.list[0])
+
+    def column_stats(self) -> dict[str, int]:
+        """Counters of the last surrogate step: rejected columns, quiet
+        columns (zero increments without the network), and rejections by
+        reason (a column can have several)."""
+        v = self.list[:5].tolist()
+        return {"rejected": v[0], "quiet": v[1], "rejected_positivity": v[2], "rejected_supersaturation": v[3],
+                "rejected_nonfinite": v[4], "columns": int(self.colstat.numel())}
 
 
 def harvest(seeds, nsteps: int, spec_for, per_step: int = 5000, busy_share: float = 0.8, device: str = "cuda",

@@ -195,6 +195,45 @@ def test_surrogate_with_every_column_rejected_equals_the_plain_step(small_case):
         assert d <= 1e-6 * scale, (k, d)
 
 
+def test_quiet_columns_take_exactly_what_wsm6_does(small_case):
+    """Columns without condensate and below saturation bypass the network;
+    WSM6 leaves them unchanged too, so after one step they equal the plain
+    step's columns (theta to one rounding of t / pii - th).  The moist
+    synthetic state is supersaturated over ice near its cold top in every
+    column, so the case is made dry (no vapour, no cloud, dry boundaries)."""
+    g, inputs, bdy = small_case
+    inputs, bdy = dict(inputs), dict(bdy)
+    for key in ("QVAPOR", "QCLOUD"):
+        inputs[key] = np.zeros_like(np.asarray(inputs[key]))
+    for key in [k for k in bdy if k.startswith("QVAPOR_")]:
+        bdy[key] = np.zeros_like(np.asarray(bdy[key]))
+    plain = DeviceState.from_inputs(g, inputs, bdy, device="cuda")
+    Integrator(plain).step()
+    sur = DeviceState.from_inputs(g, inputs, bdy, device="cuda")
+    net = surrogate.MlpNet(surrogate.layout(sur), hidden=128, device="cuda", seed=5)
+    si = surrogate.SurrogateIntegrator(sur, net, judge_every=0, tol_neg=1e3, tol_sat=1e3)   # gate open
+    si.step_mlp()
+    torch.cuda.synchronize()
+    lay = surrogate.layout(sur)
+    stat = si.colstat.view(lay["ncy"], lay["ncx"])
+    quiet = stat == 1
+    assert int(quiet.sum()) == lay["ncols"]
+    assert si.column_stats()["quiet"] == lay["ncols"] and si.rejected() == 0
+    js, is_ = g.jds + 1, g.ids + 1
+    sl = (slice(js, js + lay["ncy"]), slice(is_, is_ + lay["ncx"]))
+    km = lay["km"]
+    for k, base in (("t", None), ("p", "pb"), ("al", "alb")):
+        a, b = plain[k][:km][:, sl[0], sl[1]], sur[k][:km][:, sl[0], sl[1]]
+        full = a + plain[base][:km][:, sl[0], sl[1]] if base else a + 300.0
+        d = float((a - b).abs()[:, quiet].max())
+        assert d <= 1e-6 * float(full.abs().max()), (k, d)   # p, al: a few roundings of the full value
+    for m in range(1, 7):
+        a, b = plain["moist"][m, :km][:, sl[0], sl[1]], sur["moist"][m, :km][:, sl[0], sl[1]]
+        assert torch.equal(a[:, quiet], b[:, quiet]), m
+    for k in ("rainnc", "rainncv", "sr"):
+        assert torch.equal(plain[k][sl][quiet], sur[k][sl][quiet]), k
+
+
 def test_surrogate_step_runs_in_a_graph_and_keeps_the_state_finite(small_case):
     g, inputs, bdy = small_case
     st = DeviceState.from_inputs(g, inputs, bdy, device="cuda")
