@@ -129,6 +129,15 @@ int wrf_rk3_step(const WrfGrid* g, const WrfState* s, void* stream, wrf_probe_fn
 int wrf_advect_scalar(const WrfGrid* g, const float* field, float* tend, const float* ru,
                       const float* rv, const float* rom, const float* msftx, const float* fzm,
                       const float* fzp, const float* rdzw, void* stream);
+/* Adjoint of wrf_advect_scalar (reverse mode): given the cotangent tend_bar of
+ * the updated tendency, accumulates (+=) the cotangents of field, ru, rv and
+ * rom.  The cotangent of the incoming tendency is tend_bar itself.  The
+ * reference obtains this product from torch autograd through
+ * wrf_dynamics.py:1841-2028. */
+int wrf_advect_scalar_adj(const WrfGrid* g, const float* field, const float* ru, const float* rv,
+                          const float* rom, const float* msftx, const float* fzm, const float* fzp,
+                          const float* rdzw, const float* tend_bar, float* field_bar, float* ru_bar,
+                          float* rv_bar, float* rom_bar, void* stream);
 /* wrf_physics.py:94-136 microphysics_driver -> wsm6 on the solver's column block */
 int wrf_wsm6(const WrfGrid* g, float* th, float* qv, float* qc, float* qr, float* qi, float* qs,
              float* qg, const float* rho, const float* pii, const float* p, const float* dz8w,

@@ -82,6 +82,8 @@ def lib() -> ctypes.CDLL:
     L.wrf_rk3_step.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, PROBE_FN, vp]
     L.wrf_advect_scalar.restype = ip
     L.wrf_advect_scalar.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 9 + [vp]
+    L.wrf_advect_scalar_adj.restype = ip
+    L.wrf_advect_scalar_adj.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 13 + [vp]
     L.wrf_wsm6.restype = ip
     L.wrf_wsm6.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 11 + [ctypes.c_float] + [vp] * 7 + [vp]
     L.wrf_wsm6_noalloc.restype = ip

@@ -1,0 +1,215 @@
+// Hand-written adjoints of step operators (reverse mode, one cotangent per call).
+//
+//   k_advect_scalar_adj  adjoint of advect_scalar (wrf_dynamics.py:1841-2028,
+//                        forward: k_advect_scalar / k_advect_tiled) with
+//                        respect to the advected field and the three mass
+//                        fluxes ru, rv, rom.
+//
+// Forward, per mass point c of [ids, ide-1) x [jds, jde-1) x [0, nz-1):
+//   tend(c) -= a_y(c) (Fy(j+1) - Fy(j)) + a_x(c) (Fx(i+1) - Fx(i)) + rdnw(k) (Fz(k+1) - Fz(k))
+// with a_y = msftx rdy on rows [jds+1, jde-2) (else 0), a_x likewise, and each
+// face flux F = r Phi(q; sign r), Phi the 5th-, 3rd- or 2nd-order face value
+// the reference selects for that face (fortran_sign(1, r) upwinding; minus
+// sign of rom vertically).  The sign is piecewise constant, so
+//   Fbar(f)  = a(cell above f) tbar(cell above) - a(cell below f) tbar(cell below)
+//   qbar(m) += sum over faces f whose stencil holds m of Fbar(f) r(f) dPhi_f/dq(m)
+//   rbar(f) += Fbar(f) Phi(f)
+// Each output element is written by one thread (a gather over the faces that
+// touch it), so results do not depend on scheduling; tend's own cotangent is
+// tbar unchanged (the caller passes it through).
+#include "kernels.cuh"
+
+namespace wrf {
+namespace {
+
+// dPhi/dq at stencil offset o = m - f of a 5th-order face (o in [-3, 2]),
+// Phi = (37(q0+qm1) - 8(qp1+qm2) + (qp2+qm3))/60 - s ((qp2-qm3) - 5(qp1-qm2) + 10(q0-qm1))/60
+__device__ __forceinline__ float w5(int o, float s) {
+  switch (o) {
+    case -3: return (1.f + s) * (1.f / 60.f);
+    case -2: return (-8.f - 5.f * s) * (1.f / 60.f);
+    case -1: return (37.f + 10.f * s) * (1.f / 60.f);
+    case 0: return (37.f - 10.f * s) * (1.f / 60.f);
+    case 1: return (-8.f + 5.f * s) * (1.f / 60.f);
+    case 2: return (1.f - s) * (1.f / 60.f);
+    default: return 0.f;
+  }
+}
+
+// 3rd-order face, o in [-2, 1]:
+// Phi = (7(q0+qm1) - (qp1+qm2))/12 + s ((qp1-qm2) - 3(q0-qm1))/12
+__device__ __forceinline__ float w3(int o, float s) {
+  switch (o) {
+    case -2: return (-1.f - s) * (1.f / 12.f);
+    case -1: return (7.f + 3.f * s) * (1.f / 12.f);
+    case 0: return (7.f - 3.f * s) * (1.f / 12.f);
+    case 1: return (-1.f + s) * (1.f / 12.f);
+    default: return 0.f;
+  }
+}
+
+// order class of a horizontal face index f in [lo, hi) (lo = ids or jds,
+// hi = ide or jde): 5, 3, 2, or 0 (no flux), as in fqx_s / fqy_s
+__device__ __forceinline__ int horder(int f, int lo, int hi) {
+  if (f >= lo + 3 && f < hi - 3) return 5;
+  if (f == lo + 2 || f == hi - 3) return 3;
+  if (f == lo + 1 || f == hi - 2) return 2;
+  return 0;
+}
+
+// vertical face kf (as in vf_s): 5, 3, 1 (the fnm / fnp average), or 0
+__device__ __forceinline__ int vorder(int kf, int ktf) {
+  if (kf >= 3 && kf < ktf - 2) return 5;
+  if (kf == 2 || kf == ktf - 2) return 3;
+  if (kf == 1 || kf == ktf - 1) return 1;
+  return 0;
+}
+
+struct AdvArgs0 {
+  const float *q, *ru, *rv, *rom, *msftx, *fnm, *fnp, *rdnw;
+};
+
+}  // namespace
+
+__global__ void k_advect_scalar_adj(Grid g, AdvArgs0 a, const float* tbar, float* qbar, float* rubar, float* rvbar,
+                                    float* rombar) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde, nz = g.nz, ktf = nz - 1, nx = g.nx;
+  const size_t lev = (size_t)g.ny * nx;
+  const int c = g.i2(j, i);
+  const size_t p = (size_t)k * lev + c;
+  // the update set and the per-cell coefficients of each direction
+  auto inset = [&](int kk, int jj, int ii) {
+    return kk >= 0 && kk < ktf && ii >= ids && ii < ide - 1 && jj >= jds && jj < jde - 1;
+  };
+  auto tb = [&](int kk, int jj, int ii) { return tbar[(size_t)kk * lev + (size_t)jj * nx + ii]; };
+  auto ay = [&](int kk, int jj, int ii) {
+    return (inset(kk, jj, ii) && jj >= jds + 1 && jj < jde - 2) ? a.msftx[(size_t)jj * nx + ii] * g.rdy : 0.f;
+  };
+  auto ax = [&](int kk, int jj, int ii) {
+    return (inset(kk, jj, ii) && ii >= ids + 1 && ii < ide - 2) ? a.msftx[(size_t)jj * nx + ii] * g.rdx : 0.f;
+  };
+  auto az = [&](int kk, int jj, int ii) { return inset(kk, jj, ii) ? a.rdnw[kk] : 0.f; };
+  // face cotangents
+  auto fby = [&](int kk, int jf, int ii) {
+    float v = 0.f;
+    if (jf < g.ny) { const float cf = ay(kk, jf, ii); if (cf != 0.f) v += cf * tb(kk, jf, ii); }
+    if (jf >= 1) { const float cf = ay(kk, jf - 1, ii); if (cf != 0.f) v -= cf * tb(kk, jf - 1, ii); }
+    return v;
+  };
+  auto fbx = [&](int kk, int jj, int f) {
+    float v = 0.f;
+    if (f < nx) { const float cf = ax(kk, jj, f); if (cf != 0.f) v += cf * tb(kk, jj, f); }
+    if (f >= 1) { const float cf = ax(kk, jj, f - 1); if (cf != 0.f) v -= cf * tb(kk, jj, f - 1); }
+    return v;
+  };
+  auto fbz = [&](int kf, int jj, int ii) {
+    float v = 0.f;
+    if (kf < nz) { const float cf = az(kf, jj, ii); if (cf != 0.f) v += cf * tb(kf, jj, ii); }
+    if (kf >= 1) { const float cf = az(kf - 1, jj, ii); if (cf != 0.f) v -= cf * tb(kf - 1, jj, ii); }
+    return v;
+  };
+  const float* q = a.q;
+
+  // --- field cotangent: gather over the faces whose stencil holds (k, j, i)
+  float acc = 0.f;
+  for (int jf = j - 2; jf <= j + 3; ++jf) {
+    if (jf < 0 || jf >= g.ny) continue;
+    const int ord = horder(jf, jds, jde);
+    if (!ord) continue;
+    const float fb = fby(k, jf, i);
+    if (fb == 0.f) continue;
+    const float r = a.rv[(size_t)k * lev + (size_t)jf * nx + i];
+    const int o = j - jf;
+    const float w = ord == 5 ? w5(o, sgnf(r)) : ord == 3 ? w3(o, sgnf(r)) : ((o == 0 || o == -1) ? 0.5f : 0.f);
+    acc += fb * r * w;
+  }
+  for (int f = i - 2; f <= i + 3; ++f) {
+    if (f < 0 || f >= nx) continue;
+    const int ord = horder(f, ids, ide);
+    if (!ord) continue;
+    const float fb = fbx(k, j, f);
+    if (fb == 0.f) continue;
+    const size_t row = (size_t)k * lev + (size_t)j * nx;
+    const float r = a.ru[row + f];
+    const float rs = f == ide - 3 ? a.ru[row + ide - 2] : r;  // the reference's sign source of that face
+    const int o = i - f;
+    const float w = ord == 5 ? w5(o, sgnf(rs)) : ord == 3 ? w3(o, sgnf(rs)) : ((o == 0 || o == -1) ? 0.5f : 0.f);
+    acc += fb * r * w;
+  }
+  for (int kf = k - 2; kf <= k + 3; ++kf) {
+    if (kf < 0 || kf >= nz) continue;
+    const int ord = vorder(kf, ktf);
+    if (!ord) continue;
+    const float fb = fbz(kf, j, i);
+    if (fb == 0.f) continue;
+    const float r = a.rom[(size_t)kf * lev + c];
+    const int o = k - kf;
+    float w;
+    if (ord == 5) w = w5(o, sgnf(-r));
+    else if (ord == 3) w = w3(o, sgnf(-r));
+    else w = o == 0 ? a.fnm[kf] : (o == -1 ? a.fnp[kf] : 0.f);
+    acc += fb * r * w;
+  }
+  if (acc != 0.f) qbar[p] += acc;
+
+  // --- flux cotangents of the faces owned by this point: rbar = Fbar Phi
+  auto Q = [&](size_t base, int off, int st) { return q[base + (size_t)((long long)off * st)]; };
+  {  // y face jf = j at (k, i)
+    const int ord = horder(j, jds, jde);
+    if (ord && k < nz) {
+      const float fb = fby(k, j, i);
+      if (fb != 0.f) {
+        const float r = a.rv[p];
+        const size_t b = p;
+        float phi;
+        if (ord == 5) phi = flux5(Q(b, -3, nx), Q(b, -2, nx), Q(b, -1, nx), Q(b, 0, nx), Q(b, 1, nx), Q(b, 2, nx), r);
+        else if (ord == 3) phi = flux3(Q(b, -2, nx), Q(b, -1, nx), Q(b, 0, nx), Q(b, 1, nx), r);
+        else phi = 0.5f * (Q(b, 0, nx) + Q(b, -1, nx));
+        rvbar[p] += fb * phi;
+      }
+    }
+  }
+  {  // x face f = i at (k, j)
+    const int ord = horder(i, ids, ide);
+    if (ord) {
+      const float fb = fbx(k, j, i);
+      if (fb != 0.f) {
+        const size_t row = (size_t)k * lev + (size_t)j * nx;
+        const float rs = i == ide - 3 ? a.ru[row + ide - 2] : a.ru[p];
+        float phi;
+        if (ord == 5) phi = flux5(Q(p, -3, 1), Q(p, -2, 1), Q(p, -1, 1), Q(p, 0, 1), Q(p, 1, 1), Q(p, 2, 1), rs);
+        else if (ord == 3) phi = flux3(Q(p, -2, 1), Q(p, -1, 1), Q(p, 0, 1), Q(p, 1, 1), rs);
+        else phi = 0.5f * (Q(p, 0, 1) + Q(p, -1, 1));
+        rubar[p] += fb * phi;
+      }
+    }
+  }
+  {  // vertical face kf = k at (j, i)
+    const int ord = vorder(k, ktf);
+    if (ord) {
+      const float fb = fbz(k, j, i);
+      if (fb != 0.f) {
+        const float r = a.rom[p];
+        const int st = (int)lev;
+        float phi;
+        if (ord == 5) phi = flux5(Q(p, -3, st), Q(p, -2, st), Q(p, -1, st), Q(p, 0, st), Q(p, 1, st), Q(p, 2, st), -r);
+        else if (ord == 3) phi = flux3(Q(p, -2, st), Q(p, -1, st), Q(p, 0, st), Q(p, 1, st), -r);
+        else phi = a.fnm[k] * Q(p, 0, st) + a.fnp[k] * Q(p, -1, st);
+        rombar[p] += fb * phi;
+      }
+    }
+  }
+}
+
+int launch_advect_scalar_adj(const Grid& g, const float* q, const float* ru, const float* rv, const float* rom,
+                             const float* msftx, const float* fnm, const float* fnp, const float* rdnw,
+                             const float* tbar, float* qbar, float* rubar, float* rvbar, float* rombar,
+                             cudaStream_t st) {
+  const dim3 b3(32, 4);
+  AdvArgs0 a{q, ru, rv, rom, msftx, fnm, fnp, rdnw};
+  k_advect_scalar_adj<<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, qbar, rubar, rvbar, rombar);
+  return 1;
+}
+
+}  // namespace wrf

@@ -36,6 +36,13 @@ int launch_advect_theta_tiled(const Grid& g, const S& s, cudaStream_t st);
 int launch_advect_scalar(const Grid& g, const S& s, const float* field, float* tend, const float* ru,
                           const float* rv, const float* rom, cudaStream_t st);
 
+// adjoint of advect_scalar w.r.t. the field and ru / rv / rom (k_adjoint.cu);
+// accumulates into qbar, rubar, rvbar, rombar
+int launch_advect_scalar_adj(const Grid& g, const float* q, const float* ru, const float* rv, const float* rom,
+                             const float* msftx, const float* fnm, const float* fnp, const float* rdnw,
+                             const float* tbar, float* qbar, float* rubar, float* rvbar, float* rombar,
+                             cudaStream_t st);
+
 // acoustic steps (k_acoustic.cu)
 int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cudaStream_t st);
 int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st);

@@ -305,6 +305,22 @@ int wrf_advect_scalar(const WrfGrid* gin, const float* field, float* tend, const
   return check_launch("advect_scalar");
 }
 
+int wrf_advect_scalar_adj(const WrfGrid* gin, const float* field, const float* ru, const float* rv, const float* rom,
+                          const float* msftx, const float* fzm, const float* fzp, const float* rdzw,
+                          const float* tend_bar, float* field_bar, float* ru_bar, float* rv_bar, float* rom_bar,
+                          void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!field || !ru || !rv || !rom || !msftx || !fzm || !fzp || !rdzw || !tend_bar || !field_bar || !ru_bar ||
+      !rv_bar || !rom_bar)
+    return fail(WRF_EINVAL, "null argument");
+  cudaGetLastError();
+  launch_advect_scalar_adj(g, field, ru, rv, rom, msftx, fzm, fzp, rdzw, tend_bar, field_bar, ru_bar, rv_bar, rom_bar,
+                           static_cast<cudaStream_t>(stream));
+  return check_launch("advect_scalar_adj");
+}
+
 int wrf_wsm6(const WrfGrid* gin, float* th, float* qv, float* qc, float* qr, float* qi, float* qs, float* qg,
              const float* rho, const float* pii, const float* p, const float* dz8w, float delt, float* rainnc,
              float* rainncv, float* snownc, float* snowncv, float* graupelnc, float* graupelncv, float* sr,
