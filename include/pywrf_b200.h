@@ -138,6 +138,30 @@ int wrf_advect_scalar_adj(const WrfGrid* g, const float* field, const float* ru,
                           const float* rom, const float* msftx, const float* fzm, const float* fzp,
                           const float* rdzw, const float* tend_bar, float* field_bar, float* ru_bar,
                           float* rv_bar, float* rom_bar, void* stream);
+/* wrf_boundary.py:52-147 relax_bdytend on one field: tend += the relaxation
+ * toward bdy + dtbc * bdy_tend over the zone rows 1..3.  bdy8: device arrays
+ * xs xe ys ye (values) and txs txe tys tye (tendencies) in the solver's
+ * permuted layout ([nz][ny][5] and [nz][5][nx]); variable: the reference's
+ * stagger letter ('u', 'v', 'h' / 'm' for all nz levels, else nz - 1), with
+ * the weights fcx / gcx the solver passes (solver.py:440-441). */
+int wrf_relax_bdytend(const WrfGrid* g, const float* field, float* tend, const float* const* bdy8,
+                      char variable, float dtbc, void* stream);
+/* its adjoint w.r.t. the field: field_bar += d(tend)/d(field)^T tend_bar (the
+ * operator is linear in the field; no counterpart in the reference, which
+ * gets it from torch autograd) */
+int wrf_relax_bdytend_adj(const WrfGrid* g, const float* tend_bar, float* field_bar, char variable,
+                          void* stream);
+/* The vertically implicit w solve of advance_w (wrf_dynamics.py:3761-3767)
+ * on ncol columns of nz levels ([nz][ncol] arrays, any column stride folded
+ * into ncol): forward sweep w(k) = (x(k) - a(k) w(k-1)) alpha(k), then
+ * w(k) -= gamma(k) w(k+1); w(0) = x(0).  The reference runs it inline. */
+int wrf_vsolve_w(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma,
+                 float* w, void* stream);
+/* its adjoint (the transposed solve and the coefficient cotangents):
+ * accumulates (+=) into x_bar, a_bar, alpha_bar, gamma_bar given w_bar */
+int wrf_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma,
+                     const float* w_bar, float* x_bar, float* a_bar, float* alpha_bar, float* gamma_bar,
+                     void* stream);
 /* wrf_physics.py:94-136 microphysics_driver -> wsm6 on the solver's column block */
 int wrf_wsm6(const WrfGrid* g, float* th, float* qv, float* qc, float* qr, float* qi, float* qs,
              float* qg, const float* rho, const float* pii, const float* p, const float* dz8w,

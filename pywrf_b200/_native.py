@@ -84,6 +84,15 @@ def lib() -> ctypes.CDLL:
     L.wrf_advect_scalar.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 9 + [vp]
     L.wrf_advect_scalar_adj.restype = ip
     L.wrf_advect_scalar_adj.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 13 + [vp]
+    L.wrf_relax_bdytend.restype = ip
+    L.wrf_relax_bdytend.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.POINTER(ctypes.c_void_p), ctypes.c_char,
+                                    ctypes.c_float, vp]
+    L.wrf_relax_bdytend_adj.restype = ip
+    L.wrf_relax_bdytend_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_char, vp]
+    L.wrf_vsolve_w.restype = ip
+    L.wrf_vsolve_w.argtypes = [ip, ip] + [vp] * 5 + [vp]
+    L.wrf_vsolve_w_adj.restype = ip
+    L.wrf_vsolve_w_adj.argtypes = [ip, ip] + [vp] * 9 + [vp]
     L.wrf_wsm6.restype = ip
     L.wrf_wsm6.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 11 + [ctypes.c_float] + [vp] * 7 + [vp]
     L.wrf_wsm6_noalloc.restype = ip

@@ -8,6 +8,12 @@ operators keeps no tape of the forward's intermediates.
 * :class:`AdvectScalar` -- ``tendency + advect(field; ru, rv, rom)``
   (pywrf/wrf_dynamics.py:1841-2028); gradients with respect to the field, the
   incoming tendency and the three mass fluxes.
+* :class:`RelaxBdytend` -- ``tendency + relax(field)`` toward the lateral
+  boundary values (pywrf/wrf_boundary.py:52-147); gradients with respect to
+  the field and the incoming tendency (the boundary arrays are data).
+* :class:`VSolveW` -- the vertically implicit w solve of advance_w
+  (pywrf/wrf_dynamics.py:3761-3767); gradients with respect to the
+  right-hand side and the coefficients a, alpha, gamma (the transposed solve).
 """
 from __future__ import annotations
 
@@ -69,3 +75,78 @@ class AdvectScalar(torch.autograd.Function):
 def advect_scalar(field, tendency, ru, rv, rom, msftx, fnm, fnp, rdnw, rdx, rdy):
     """Differentiable ``tendency + advect(field)`` on the GPU."""
     return AdvectScalar.apply(field, tendency, ru, rv, rom, msftx, fnm, fnp, rdnw, rdx, rdy)
+
+
+BDY_NAMES = ("xs", "xe", "ys", "ye", "txs", "txe", "tys", "tye")
+
+
+class RelaxBdytend(torch.autograd.Function):
+    """out = tendency + relax_bdytend(field) for one stagger letter."""
+
+    @staticmethod
+    def forward(ctx, field, tendency, variable: str, dtbc: float, *bdy8):
+        nz, ny, nx = field.shape
+        cg = scalar_grid(field.shape, 1.0 / 9000.0, 1.0 / 9000.0)
+        out = tendency.detach().clone()
+        arr = (ctypes.c_void_p * 8)(*[_ptr(b).value for b in bdy8])
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(field.device):
+            rc = N.lib().wrf_relax_bdytend(ctypes.byref(cg), _ptr(field), _ptr(out), arr, variable.encode(),
+                                           float(dtbc), stream)
+        N.check(rc, "wrf_relax_bdytend")
+        ctx.cg, ctx.variable = cg, variable
+        ctx.shape = (nz, ny, nx)
+        ctx.device = field.device
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        gout = gout.contiguous()
+        fb = torch.zeros(ctx.shape, dtype=torch.float32, device=ctx.device)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(ctx.device):
+            rc = N.lib().wrf_relax_bdytend_adj(ctypes.byref(ctx.cg), _ptr(gout), _ptr(fb), ctx.variable.encode(),
+                                               stream)
+        N.check(rc, "wrf_relax_bdytend_adj")
+        return (fb, gout, None, None) + (None,) * 8
+
+
+def relax_bdytend(field, tendency, variable: str, dtbc: float, bdy: dict):
+    """Differentiable ``tendency + relax_bdytend(field)``; ``bdy`` maps
+    xs xe ys ye txs txe tys tye to the boundary arrays (solver layout)."""
+    return RelaxBdytend.apply(field, tendency, variable, dtbc, *[bdy[k] for k in BDY_NAMES])
+
+
+class VSolveW(torch.autograd.Function):
+    """w = implicit solve of (x; a, alpha, gamma) per column; arrays [nz, ...]."""
+
+    @staticmethod
+    def forward(ctx, x, a, alpha, gamma):
+        nz = x.shape[0]
+        ncol = x.numel() // nz
+        w = torch.empty_like(x)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(x.device):
+            rc = N.lib().wrf_vsolve_w(ncol, nz, _ptr(x), _ptr(a), _ptr(alpha), _ptr(gamma), _ptr(w), stream)
+        N.check(rc, "wrf_vsolve_w")
+        ctx.save_for_backward(x, a, alpha, gamma)
+        return w
+
+    @staticmethod
+    def backward(ctx, gw):
+        x, a, alpha, gamma = ctx.saved_tensors
+        nz = x.shape[0]
+        ncol = x.numel() // nz
+        gw = gw.contiguous()
+        gx, ga, gal, gg = (torch.zeros_like(x) for _ in range(4))
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(x.device):
+            rc = N.lib().wrf_vsolve_w_adj(ncol, nz, _ptr(x), _ptr(a), _ptr(alpha), _ptr(gamma), _ptr(gw), _ptr(gx),
+                                          _ptr(ga), _ptr(gal), _ptr(gg), stream)
+        N.check(rc, "wrf_vsolve_w_adj")
+        return gx, ga, gal, gg
+
+
+def vsolve_w(x, a, alpha, gamma):
+    """Differentiable implicit w solve (all columns of [nz, ...] arrays)."""
+    return VSolveW.apply(x, a, alpha, gamma)

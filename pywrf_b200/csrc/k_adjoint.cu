@@ -17,7 +17,27 @@
 // Each output element is written by one thread (a gather over the faces that
 // touch it), so results do not depend on scheduling; tend's own cotangent is
 // tbar unchanged (the caller passes it through).
+//
+//   k_relax_field / k_relax_field_adj  relax_bdytend (wrf_boundary.py:52-147)
+//                        on one field, and its adjoint with respect to the
+//                        field: at a relaxation point P of distance b,
+//   tend(P) += fcx_b f0 - gcx_b (f1 + f2 + f3 + f4 - 4 f0),  fN = bdy_N - field(N)
+//                        so field(P) carries -(fcx_b + 4 gcx_b) and each of its
+//                        four neighbours +gcx_b.  The adjoint gathers, for each
+//                        point m, its own term and its neighbours' terms.
+//
+//   k_vsolve_w / k_vsolve_w_adj  the vertically implicit w solve of
+//                        advance_w (wrf_dynamics.py:3761-3767) on every
+//                        column, and its transposed (adjoint) solve with
+//                        respect to the right-hand side and the coefficients
+//                        a, alpha, gamma of calc_coef_w:
+//   y(0) = x(0);  y(k) = (x(k) - a(k) y(k-1)) alpha(k),  k = 1..nz-1
+//   w(nz-1) = y(nz-1);  w(k) = y(k) - gamma(k) w(k+1),  k = nz-2..1;  w(0) = y(0)
+//                        The reverse sweep runs the two recurrences backwards
+//                        (one thread per column; the column's y and w are
+//                        recomputed into local arrays).
 #include "kernels.cuh"
+#include "relax.cuh"
 
 namespace wrf {
 namespace {
@@ -200,6 +220,138 @@ __global__ void k_advect_scalar_adj(Grid g, AdvArgs0 a, const float* tbar, float
       }
     }
   }
+}
+
+// stagger of a relaxed field: the bounds of relax_bdytend's zones and levels
+// ('u': ibe = ide, 'v': jbe = jde, 'h'/'m': all nz levels, else nz - 1)
+struct RelaxShape {
+  int ibe, jbe, nk;
+};
+
+__host__ __device__ inline RelaxShape relax_shape(const Grid& g, char var) {
+  RelaxShape r{g.ide - 1, g.jde - 1, g.nz - 1};
+  if (var == 'u') r.ibe = g.ide;
+  if (var == 'v') r.jbe = g.jde;
+  if (var == 'h' || var == 'm') r.nk = g.nz;
+  return r;
+}
+
+__global__ void k_relax_field(Grid g, S s, RelaxShape r, const float* field, float* tend, float dtbc) {
+  WRF_POINT_INDEX(g, k, j, i);
+  if (k >= r.nk) return;
+  const int nx = g.nx, ny = g.ny;
+  float* o = tend + ((size_t)k * ny + j) * nx + i;
+  relax_point(g, s, 0, k, j, i, r.ibe, r.jbe, r.nk,
+              [&](int kk, int jj, int ii) { return field[((size_t)kk * ny + jj) * nx + ii]; }, dtbc, o);
+}
+
+__global__ void k_relax_field_adj(Grid g, RelaxShape r, const float* tbar, float* fbar) {
+  WRF_POINT_INDEX(g, k, j, i);
+  if (k >= r.nk) return;
+  const int nx = g.nx, ny = g.ny;
+  const size_t p = ((size_t)k * ny + j) * nx + i;
+  float acc = 0.f;
+  const int b0 = relax_zone_b(g, j, i, r.ibe, r.jbe);
+  if (b0) acc -= (kFcx[b0] + 4.0f * kGcx[b0]) * tbar[p];
+  const int dj[4] = {0, 0, -1, 1}, di[4] = {-1, 1, 0, 0};
+  for (int n = 0; n < 4; ++n) {
+    const int jj = j + dj[n], ii = i + di[n];
+    if (jj < 0 || jj >= ny || ii < 0 || ii >= nx) continue;
+    const int b = relax_zone_b(g, jj, ii, r.ibe, r.jbe);
+    if (b) acc += kGcx[b] * tbar[((size_t)k * ny + jj) * nx + ii];
+  }
+  if (acc != 0.f) fbar[p] += acc;
+}
+
+int launch_relax_field(const Grid& g, const float* field, float* tend, const float* const* bdy8, char var, float dtbc,
+                       cudaStream_t st) {
+  S s{};
+  for (int q = 0; q < 8; ++q) s.f[q] = const_cast<float*>(bdy8[q]);
+  const dim3 b3(32, 4);
+  k_relax_field<<<point_grid(g, b3), b3, 0, st>>>(g, s, relax_shape(g, var), field, tend, dtbc);
+  return 1;
+}
+
+int launch_relax_field_adj(const Grid& g, const float* tbar, float* fbar, char var, cudaStream_t st) {
+  const dim3 b3(32, 4);
+  k_relax_field_adj<<<point_grid(g, b3), b3, 0, st>>>(g, relax_shape(g, var), tbar, fbar);
+  return 1;
+}
+
+__global__ void k_vsolve_w(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma,
+                           float* w) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const size_t lev = (size_t)ncol;
+  const int kend = nz - 1;
+  float prev = x[c];
+  w[c] = prev;
+  for (int k = 1; k <= kend; ++k) {
+    const size_t p = k * lev + c;
+    prev = (x[p] - a[p] * prev) * alpha[p];
+    w[p] = prev;
+  }
+  for (int k = kend - 1; k >= 1; --k) {
+    const size_t p = k * lev + c;
+    prev = w[p] - gamma[p] * prev;
+    w[p] = prev;
+  }
+}
+
+__global__ void k_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const float* alpha,
+                               const float* gamma, const float* wbar, float* xbar, float* abar, float* alphabar,
+                               float* gammabar) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const size_t lev = (size_t)ncol;
+  const int kend = nz - 1;
+  float y[kMaxNz], z[kMaxNz], zb[kMaxNz], yb[kMaxNz];
+  // forward recomputation
+  y[0] = x[c];
+  for (int k = 1; k <= kend; ++k) {
+    const size_t p = k * lev + c;
+    y[k] = (x[p] - a[p] * y[k - 1]) * alpha[p];
+  }
+  z[kend] = y[kend];
+  for (int k = kend - 1; k >= 1; --k) z[k] = y[k] - gamma[k * lev + c] * z[k + 1];
+  z[0] = y[0];
+  for (int k = 0; k <= kend; ++k) {
+    zb[k] = wbar[k * lev + c];
+    yb[k] = 0.f;
+  }
+  // back-substitution in reverse (it computed k = kend-1 down to 1)
+  for (int k = 1; k <= kend - 1; ++k) {
+    const size_t p = k * lev + c;
+    yb[k] += zb[k];
+    gammabar[p] += -z[k + 1] * zb[k];
+    zb[k + 1] += -gamma[p] * zb[k];
+  }
+  yb[kend] += zb[kend];
+  yb[0] += zb[0];
+  // forward sweep in reverse (it computed k = 1 up to kend)
+  for (int k = kend; k >= 1; --k) {
+    const size_t p = k * lev + c;
+    const float al = alpha[p], ak = a[p];
+    xbar[p] += al * yb[k];
+    abar[p] += -y[k - 1] * al * yb[k];
+    alphabar[p] += (x[p] - ak * y[k - 1]) * yb[k];
+    yb[k - 1] += -ak * al * yb[k];
+  }
+  xbar[c] += yb[0];
+}
+
+int launch_vsolve_w(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma, float* w,
+                    cudaStream_t st) {
+  k_vsolve_w<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, x, a, alpha, gamma, w);
+  return 1;
+}
+
+int launch_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma,
+                        const float* wbar, float* xbar, float* abar, float* alphabar, float* gammabar,
+                        cudaStream_t st) {
+  k_vsolve_w_adj<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, x, a, alpha, gamma, wbar, xbar, abar, alphabar,
+                                                      gammabar);
+  return 1;
 }
 
 int launch_advect_scalar_adj(const Grid& g, const float* q, const float* ru, const float* rv, const float* rom,

@@ -43,6 +43,20 @@ int launch_advect_scalar_adj(const Grid& g, const float* q, const float* ru, con
                              const float* tbar, float* qbar, float* rubar, float* rvbar, float* rombar,
                              cudaStream_t st);
 
+// relax_bdytend on one field (bdy8: xs xe ys ye txs txe tys tye device
+// arrays) and its adjoint w.r.t. the field (k_adjoint.cu)
+int launch_relax_field(const Grid& g, const float* field, float* tend, const float* const* bdy8, char var, float dtbc,
+                       cudaStream_t st);
+int launch_relax_field_adj(const Grid& g, const float* tbar, float* fbar, char var, cudaStream_t st);
+
+// the implicit w solve of advance_w on ncol columns of nz levels, and its
+// adjoint (accumulates into xbar, abar, alphabar, gammabar) (k_adjoint.cu)
+int launch_vsolve_w(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma, float* w,
+                    cudaStream_t st);
+int launch_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma,
+                        const float* wbar, float* xbar, float* abar, float* alphabar, float* gammabar,
+                        cudaStream_t st);
+
 // acoustic steps (k_acoustic.cu)
 int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cudaStream_t st);
 int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st);

@@ -321,6 +321,50 @@ int wrf_advect_scalar_adj(const WrfGrid* gin, const float* field, const float* r
   return check_launch("advect_scalar_adj");
 }
 
+int wrf_relax_bdytend(const WrfGrid* gin, const float* field, float* tend, const float* const* bdy8, char variable,
+                      float dtbc, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!field || !tend || !bdy8) return fail(WRF_EINVAL, "null argument");
+  for (int q = 0; q < 8; ++q)
+    if (!bdy8[q]) return fail(WRF_EINVAL, "null boundary array");
+  cudaGetLastError();
+  launch_relax_field(g, field, tend, bdy8, variable, dtbc, static_cast<cudaStream_t>(stream));
+  return check_launch("relax_bdytend");
+}
+
+int wrf_relax_bdytend_adj(const WrfGrid* gin, const float* tend_bar, float* field_bar, char variable, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!tend_bar || !field_bar) return fail(WRF_EINVAL, "null argument");
+  cudaGetLastError();
+  launch_relax_field_adj(g, tend_bar, field_bar, variable, static_cast<cudaStream_t>(stream));
+  return check_launch("relax_bdytend_adj");
+}
+
+int wrf_vsolve_w(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma, float* w,
+                 void* stream) {
+  if (!x || !a || !alpha || !gamma || !w) return fail(WRF_EINVAL, "null argument");
+  if (ncol < 1 || nz < 3 || nz > kMaxNz) return fail(WRF_EINVAL, "vsolve_w: needs ncol >= 1 and 3 <= nz <= 64");
+  cudaGetLastError();
+  launch_vsolve_w(ncol, nz, x, a, alpha, gamma, w, static_cast<cudaStream_t>(stream));
+  return check_launch("vsolve_w");
+}
+
+int wrf_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma,
+                     const float* w_bar, float* x_bar, float* a_bar, float* alpha_bar, float* gamma_bar,
+                     void* stream) {
+  if (!x || !a || !alpha || !gamma || !w_bar || !x_bar || !a_bar || !alpha_bar || !gamma_bar)
+    return fail(WRF_EINVAL, "null argument");
+  if (ncol < 1 || nz < 3 || nz > kMaxNz) return fail(WRF_EINVAL, "vsolve_w_adj: needs ncol >= 1 and 3 <= nz <= 64");
+  cudaGetLastError();
+  launch_vsolve_w_adj(ncol, nz, x, a, alpha, gamma, w_bar, x_bar, a_bar, alpha_bar, gamma_bar,
+                      static_cast<cudaStream_t>(stream));
+  return check_launch("vsolve_w_adj");
+}
+
 int wrf_wsm6(const WrfGrid* gin, float* th, float* qv, float* qc, float* qr, float* qi, float* qs, float* qg,
              const float* rho, const float* pii, const float* p, const float* dz8w, float delt, float* rainnc,
              float* rainncv, float* snownc, float* snowncv, float* graupelnc, float* graupelncv, float* sr,

@@ -1,15 +1,20 @@
-"""Golden cotangents of advect_scalar from the reference's own autograd.
+"""Golden cotangents of step operators from the reference's own autograd.
 
 Usage:  python tests/golden/make_golden_adjoint.py [--reference /path/to/PyWRF]
 
-Runs the unmodified reference ``pywrf.wrf_dynamics.advect_scalar``
-(wrf_dynamics.py:1841-2028) in float64 on CPU with ``requires_grad`` on the
-advected field and the three mass fluxes, back-propagates a seeded random
-cotangent of the returned tendency with torch autograd, and writes
-``adv_scalar_adj_ref64.npz`` next to this script: the inputs, the cotangent,
-the forward tendency and the four gradients.  Grid 24x24x12 in the solver's
-5-cell frame; fluxes of both signs so that both upwind branches are taken.
-This script is the only producer of the fixture and is never run by the tests.
+Runs unmodified reference functions in float64 on CPU with ``requires_grad``
+on their differentiable inputs, back-propagates a seeded random cotangent of
+the returned tendency with torch autograd, and writes next to this script:
+
+* ``adv_scalar_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.advect_scalar``
+  (wrf_dynamics.py:1841-2028) w.r.t. the advected field and the three mass
+  fluxes (fluxes of both signs, so both upwind branches are taken);
+* ``relax_adj_ref64.npz`` -- ``pywrf.wrf_boundary.relax_bdytend``
+  (wrf_boundary.py:52-147) w.r.t. the field, for the staggers 't', 'u', 'v'
+  and 'h', with the solver's fcx / gcx (solver.py:440-441).
+
+Grid 24x24x12 in the solver's 5-cell frame.  This script is the only producer
+of the fixtures and is never run by the tests.
 """
 from __future__ import annotations
 
@@ -79,6 +84,41 @@ def main() -> None:
     save["dy"] = np.array(g.dy)
     np.savez_compressed(os.path.join(HERE, "adv_scalar_adj_ref64.npz"), **save)
     print("wrote adv_scalar_adj_ref64.npz", {k: float(np.abs(v).max()) for k, v in save.items() if k.startswith("grad")})
+
+    # relax_bdytend
+    bnd = importlib_bdy()
+    rng = np.random.default_rng(12)
+    shape = (NZ, N, N)
+    gcx = torch.tensor([0., 1.1111111e-3, 7.4074074e-4, 3.7037037e-4, 0.], dtype=torch.float64)
+    fcx = torch.tensor([0., 5.5555557e-3, 3.7037039e-3, 1.8518519e-3, 0.], dtype=torch.float64)
+    out = {"dtbc": np.array(135.0)}
+    for var in ("t", "u", "v", "h"):
+        field = torch.tensor(300.0 + rng.standard_normal(shape), dtype=torch.float64, requires_grad=True)
+        arrs = [rng.standard_normal((NZ, N, 5)) + 300.0, rng.standard_normal((NZ, N, 5)) + 300.0,
+                rng.standard_normal((NZ, 5, N)) + 300.0, rng.standard_normal((NZ, 5, N)) + 300.0,
+                1e-3 * rng.standard_normal((NZ, N, 5)), 1e-3 * rng.standard_normal((NZ, N, 5)),
+                1e-3 * rng.standard_normal((NZ, 5, N)), 1e-3 * rng.standard_normal((NZ, 5, N))]
+        tb = [torch.tensor(a, dtype=torch.float64) for a in arrs]
+        tend0 = torch.tensor(rng.standard_normal(shape), dtype=torch.float64)
+        cot = rng.standard_normal(shape)
+        res = bnd.relax_bdytend(field, tend0.clone(), *tb, var, 5, 1, 4, 135.0, fcx, gcx,
+                                ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, 0, N, 0, N, 0, NZ,
+                                ids, ide, jds, jde, 0, NZ)
+        (res * torch.tensor(cot)).sum().backward()
+        out[f"{var}_field"] = field.detach().numpy()
+        out[f"{var}_tend0"] = tend0.numpy()
+        for nm, a in zip(("xs", "xe", "ys", "ye", "txs", "txe", "tys", "tye"), arrs):
+            out[f"{var}_{nm}"] = a
+        out[f"{var}_cot"] = cot
+        out[f"{var}_tend"] = res.detach().numpy()
+        out[f"{var}_grad_field"] = field.grad.numpy()
+    np.savez_compressed(os.path.join(HERE, "relax_adj_ref64.npz"), **out)
+    print("wrote relax_adj_ref64.npz")
+
+
+def importlib_bdy():
+    import importlib
+    return importlib.import_module("pywrf.wrf_boundary")
 
 
 if __name__ == "__main__":

@@ -69,3 +69,47 @@ def test_advect_scalar_adjoint_identity_at_64x64x41():
     lhs = float((a_dq * C["c"].double()).sum())
     rhs = float((C["dq"].double() * qv.grad.double()).sum())
     assert abs(lhs - rhs) <= 1e-5 * (abs(lhs) + abs(rhs)), (lhs, rhs)
+
+
+@pytest.mark.parametrize("var", ["t", "u", "v", "h"])
+def test_relax_bdytend_and_adjoint_match_reference_autograd(var):
+    Z = load_npz("relax_adj_ref64.npz")
+    field = _cuda(Z[f"{var}_field"]).requires_grad_(True)
+    tend0 = _cuda(Z[f"{var}_tend0"]).requires_grad_(True)
+    bdy = {k: _cuda(Z[f"{var}_{k}"]) for k in adjoint.BDY_NAMES}
+    out = adjoint.relax_bdytend(field, tend0, var, float(Z["dtbc"]), bdy)
+    assert rel_l2(out.detach().cpu().numpy(), Z[f"{var}_tend"]) < 1e-6
+    (out * _cuda(Z[f"{var}_cot"])).sum().backward()
+    err = rel_l2(field.grad.cpu().numpy(), Z[f"{var}_grad_field"])
+    assert err < 1e-6, err
+
+
+def _vsolve_torch(x, a, alpha, gamma):
+    """The reference's two loops (wrf_dynamics.py:3761-3767) in torch."""
+    w = [x[0]]
+    for k in range(1, x.shape[0]):
+        w.append((x[k] - a[k] * w[k - 1]) * alpha[k])
+    out = list(w)
+    for k in range(x.shape[0] - 2, 0, -1):
+        out[k] = w[k] - gamma[k] * out[k + 1]
+    return torch.stack(out)
+
+
+def test_vsolve_w_and_its_transposed_solve_match_autograd():
+    g = torch.Generator().manual_seed(31)
+    nz, ny, nx = 41, 20, 24
+    x = torch.randn(nz, ny, nx, generator=g, dtype=torch.float64)
+    a = 0.3 * torch.rand(nz, ny, nx, generator=g, dtype=torch.float64)
+    alpha = 0.5 + 0.5 * torch.rand(nz, ny, nx, generator=g, dtype=torch.float64)
+    gamma = 0.3 * torch.rand(nz, ny, nx, generator=g, dtype=torch.float64)
+    cot = torch.randn(nz, ny, nx, generator=g, dtype=torch.float64)
+    ref_in = [t.clone().requires_grad_(True) for t in (x, a, alpha, gamma)]
+    ref = _vsolve_torch(*ref_in)
+    (ref * cot).sum().backward()
+    gpu_in = [t.float().cuda().requires_grad_(True) for t in (x, a, alpha, gamma)]
+    w = adjoint.vsolve_w(*gpu_in)
+    assert rel_l2(w.detach().cpu().numpy(), ref.detach().numpy()) < 1e-6
+    (w * cot.float().cuda()).sum().backward()
+    for name, r, t in zip(("x", "a", "alpha", "gamma"), ref_in, gpu_in):
+        err = rel_l2(t.grad.cpu().numpy(), r.grad.numpy())
+        assert err < 1e-5, (name, err)

@@ -8,6 +8,7 @@ from __future__ import annotations
 import numpy as np
 
 from helpers import load_npz
+from oracle import boundary as OB
 from oracle import dynamics as OD
 from pywrf_b200 import synthetic
 
@@ -47,3 +48,30 @@ def test_golden_gradients_match_oracle_finite_differences():
         fd = float(((_tend(g, **plus) - _tend(g, **minus)) * Z["cot"]).sum()) / (2 * eps)
         an = float((d * Z["grad_" + name]).sum())
         assert abs(fd - an) <= 1e-6 * abs(an) + 1e-9, (name, fd, an)
+
+
+R = load_npz("relax_adj_ref64.npz")
+FCX = np.array([0., 5.5555557e-3, 3.7037039e-3, 1.8518519e-3, 0.])
+GCX = np.array([0., 1.1111111e-3, 7.4074074e-4, 3.7037037e-4, 0.])
+
+
+def _relax(g, var, field):
+    t = R[f"{var}_tend0"].copy()
+    bd = {k: R[f"{var}_{k}"] for k in ("xs", "xe", "ys", "ye", "txs", "txe", "tys", "tye")}
+    OB.relax_bdytend(g, field, t, bd, var, float(R["dtbc"]), FCX, GCX)
+    return t
+
+
+def test_relax_golden_pinned_by_the_oracle():
+    """The oracle's relax_bdytend reproduces the reference's tendency on the
+    fixture, and (being linear in the field) its finite differences give the
+    golden gradient's directional derivatives."""
+    g = _grid()
+    rng = np.random.default_rng(4)
+    for var in ("t", "u", "v", "h"):
+        f = R[f"{var}_field"]
+        assert np.abs(_relax(g, var, f) - R[f"{var}_tend"]).max() <= 1e-12 * np.abs(R[f"{var}_tend"]).max()
+        d = rng.standard_normal(f.shape)
+        fd = float(((_relax(g, var, f + d) - _relax(g, var, f - d)) * R[f"{var}_cot"]).sum()) / 2.0
+        an = float((d * R[f"{var}_grad_field"]).sum())
+        assert abs(fd - an) <= 1e-9 * abs(an), (var, fd, an)
