@@ -221,7 +221,16 @@ __global__ void k_advance_uv(Grid g, S s, float dts) {
 // the column's reciprocals (__frcp_rn).
 constexpr int kColTX = 16, kColKT = 16;
 
-__global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s, float dts, int iteration, int nsub) {
+// NQ = ceil(nz / kColKT) level slots per thread.  Phases that store to global
+// memory first load every slot's operands into registers and only then
+// compute and store: the loads of a thread's levels are then all in flight at
+// once (the compiler cannot hoist a later level's loads above an earlier
+// level's stores through possibly aliasing field pointers).
+#ifndef WRF_COL_MINB
+#define WRF_COL_MINB 4
+#endif
+template <int NQ>
+__global__ void __launch_bounds__(kColTX * kColKT, WRF_COL_MINB) k_acoustic_col(Grid g, S s, float dts, int iteration, int nsub) {
   __shared__ float sdw[kMaxNz][kColTX], sww[kMaxNz][kColTX], st2av[kMaxNz][kColTX], srhs[kMaxNz][kColTX];
   __shared__ float sa[kMaxNz][kColTX], salpha[kMaxNz][kColTX], sgamma[kMaxNz][kColTX], sph[kMaxNz][kColTX];
   __shared__ float swd[kMaxNz][kColTX];
@@ -269,12 +278,28 @@ __global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s
     const float muu0 = __ldg(&s[WF_MUU][c]), mfu0 = __ldg(&s[WF_MSFUY][c]);
     const float r_mfup = __frcp_rn(mfup), r_mfu0 = __frcp_rn(mfu0);
     const float rdx = g.rdx, rdy = g.rdy;
-    for (int k = tk; k < kend; k += kColKT) {
+    float vn[NQ], v1n[NQ], v0[NQ], v10[NQ], ue[NQ], u1e[NQ], u0[NQ], u10[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= kend) continue;
       const int p = k * lev + c;
+      vn[q] = __ldg(&v[p + nx]);
+      v1n[q] = __ldg(&v1[p + nx]);
+      v0[q] = __ldg(&v[p]);
+      v10[q] = __ldg(&v1[p]);
+      ue[q] = __ldg(&u[p + 1]);
+      u1e[q] = __ldg(&u1[p + 1]);
+      u0[q] = __ldg(&u[p]);
+      u10[q] = __ldg(&u1[p]);
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= kend) continue;
       sdw[k][tx] = msftx * msfty *
-                   (rdy * ((__ldg(&v[p + nx]) + muvn * __ldg(&v1[p + nx]) * mvin) - (__ldg(&v[p]) + muv0 * __ldg(&v1[p]) * mvi0)) +
-                    rdx * ((__ldg(&u[p + 1]) + divc(muup * __ldg(&u1[p + 1]), mfup, r_mfup)) -
-                           (__ldg(&u[p]) + divc(muu0 * __ldg(&u1[p]), mfu0, r_mfu0))));
+                   (rdy * ((vn[q] + muvn * v1n[q] * mvin) - (v0[q] + muv0 * v10[q] * mvi0)) +
+                    rdx * ((ue[q] + divc(muup * u1e[q], mfup, r_mfup)) - (u0[q] + divc(muu0 * u10[q], mfu0, r_mfu0))));
     }
   } else if (spec) {
     for (int k = tk; k < kend; k += kColKT) {
@@ -330,14 +355,20 @@ __global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s
   __syncthreads();
   // --- C: final ww (inner: scan - ww1)
   if (col) {
-    for (int k = tk; k < nz; k += kColKT) {
-      const int p = k * lev + c;
-      float w;
+    float wv[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k < nz) wv[q] = (inner && k < kend) ? __ldg(&ww1[k * lev + c]) : ww[k * lev + c];
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
+      float w = wv[q];
       if (inner && k < kend) {
-        w = sww[k][tx] - __ldg(&ww1[p]);
-        ww[p] = w;
-      } else {
-        w = ww[p];
+        w = sww[k][tx] - w;
+        ww[k * lev + c] = w;
       }
       sww[k][tx] = w;
     }
@@ -350,48 +381,98 @@ __global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s
   if (inner) {
     const float cy = (float)(0.5 * g.rdyd), cx = (float)(0.5 * g.rdxd);
     float* t2a = s[WF_T_2SAVE];
-    for (int k = tk; k < kend; k += kColKT) {
+    float t10[NQ], tup[NQ], tdn[NQ], told[NQ], ftk[NQ], vn[NQ], tn[NQ], v0[NQ], ts[NQ], ue[NQ], te[NQ], u0[NQ],
+        tw[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= kend) continue;
       const int p = k * lev + c;
-      const float t10 = __ldg(&t1[p]);
+      t10[q] = __ldg(&t1[p]);
+      tup[q] = (k + 1 == nz - 1) ? 0.f : __ldg(&t1[p + lev]);
+      tdn[q] = (k == 0) ? 0.f : __ldg(&t1[p - lev]);
+      told[q] = t[p];
+      ftk[q] = __ldg(&ft[p]);
+      vn[q] = __ldg(&v[p + nx]);
+      tn[q] = __ldg(&t1[p + nx]);
+      v0[q] = __ldg(&v[p]);
+      ts[q] = __ldg(&t1[p - nx]);
+      ue[q] = __ldg(&u[p + 1]);
+      te[q] = __ldg(&t1[p + 1]);
+      u0[q] = __ldg(&u[p]);
+      tw[q] = __ldg(&t1[p - 1]);
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= kend) continue;
+      const int p = k * lev + c;
       // wdtn(kk) = ww(kk) (fnm t1(kk) + fnp t1(kk-1)), zero at the bottom and top
-      const float wup = (k + 1 == nz - 1) ? 0.f : sww[k + 1][tx] * (pfnm[k + 1] * __ldg(&t1[p + lev]) + pfnp[k + 1] * t10);
-      const float wdn = (k == 0) ? 0.f : sww[k][tx] * (pfnm[k] * t10 + pfnp[k] * __ldg(&t1[p - lev]));
-      const float told = t[p];
-      float tt = told + msfty * dts * __ldg(&ft[p]);
-      const float hy = cy * (__ldg(&v[p + nx]) * (__ldg(&t1[p + nx]) + t10) - __ldg(&v[p]) * (t10 + __ldg(&t1[p - nx])));
-      const float hx = cx * (__ldg(&u[p + 1]) * (__ldg(&t1[p + 1]) + t10) - __ldg(&u[p]) * (t10 + __ldg(&t1[p - 1])));
+      const float wup = (k + 1 == nz - 1) ? 0.f : sww[k + 1][tx] * (pfnm[k + 1] * tup[q] + pfnp[k + 1] * t10[q]);
+      const float wdn = (k == 0) ? 0.f : sww[k][tx] * (pfnm[k] * t10[q] + pfnp[k] * tdn[q]);
+      float tt = told[q] + msfty * dts * ftk[q];
+      const float hy = cy * (vn[q] * (tn[q] + t10[q]) - v0[q] * (t10[q] + ts[q]));
+      const float hx = cx * (ue[q] * (te[q] + t10[q]) - u0[q] * (t10[q] + tw[q]));
       tt = tt - dts * msfty * (msftx * (hy + hx) + prdnw[k] * (wup - wdn));
       t[p] = tt;
-      float av = 0.5f * (ep1 * tt + em1 * told);
-      av = (av + muave * (float)T0) / (muts * ((float)T0 + t10));
+      float av = 0.5f * (ep1 * tt + em1 * told[q]);
+      av = (av + muave * (float)T0) / (muts * ((float)T0 + t10[q]));
       t2a[p] = av;
       st2av[k][tx] = av;
     }
     const float* ph1 = s[WF_PH_SAVE];
     const float* phb = s[WF_PHB];
-    for (int k = tk; k < nz; k += kColKT) {
+    float phv[NQ], av[NQ], alv[NQ], gav[NQ], p1[NQ], p1m[NQ], pb[NQ], pbm[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
       const int p = k * lev + c;
-      sph[k][tx] = s[WF_PH][p];
-      sa[k][tx] = __ldg(&s[WF_A][p]);
-      salpha[k][tx] = __ldg(&s[WF_ALPHA][p]);
-      sgamma[k][tx] = __ldg(&s[WF_GAMMA][p]);
+      phv[q] = s[WF_PH][p];
+      av[q] = __ldg(&s[WF_A][p]);
+      alv[q] = __ldg(&s[WF_ALPHA][p]);
+      gav[q] = __ldg(&s[WF_GAMMA][p]);
+      if (k >= 1 && k <= kend) {
+        p1[q] = __ldg(&ph1[p]);
+        p1m[q] = __ldg(&ph1[p - lev]);
+        pb[q] = __ldg(&phb[p]);
+        pbm[q] = __ldg(&phb[p - lev]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
+      sph[k][tx] = phv[q];
+      sa[k][tx] = av[q];
+      salpha[k][tx] = alv[q];
+      sgamma[k][tx] = gav[q];
       // wdwn(k) = 0.5 (ww(k) + ww(k-1)) rdnw(k-1) (ph1(k) - ph1(k-1) + phb(k) - phb(k-1))
       if (k >= 1 && k <= kend)
-        swd[k][tx] = 0.5f * (sww[k][tx] + sww[k - 1][tx]) * prdnw[k - 1] *
-                     (__ldg(&ph1[p]) - __ldg(&ph1[p - lev]) + __ldg(&phb[p]) - __ldg(&phb[p - lev]));
+        swd[k][tx] = 0.5f * (sww[k][tx] + sww[k - 1][tx]) * prdnw[k - 1] * (p1[q] - p1m[q] + pb[q] - pbm[q]);
     }
   }
   __syncthreads();
   // --- D2: right-hand side of the phi equation (inner)
   if (inner) {
     const float cw = (float)(0.5 * G * (1.0 - (double)ep));
-    for (int k = tk; k < nz; k += kColKT) {
+    float ptv[NQ], wv[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k < 1 || k >= nz) continue;
+      ptv[q] = __ldg(&s[WF_PH_TEND][k * lev + c]);
+      wv[q] = s[WF_W][k * lev + c];
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
       if (k == 0) {
         srhs[0][tx] = 0.f;
         continue;
       }
-      const int p = k * lev + c;
-      float r = dts * (__ldg(&s[WF_PH_TEND][p]) + cw * s[WF_W][p]);
+      float r = dts * (ptv[q] + cw * wv[q]);
       if (k < kend) r = r - dts * (pfnm[k] * swd[k + 1][tx] + pfnp[k] * swd[k][tx]);
       srhs[k][tx] = sph[k][tx] + divc(msfty * r, mut, r_mut);
     }
@@ -412,18 +493,35 @@ __global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s
       sdw[0][tx] = msfty * 0.5f * g.rdy * ((__ldg(&ht[c + nx]) - h0) * cv(c + nx) + (h0 - __ldg(&ht[c - nx])) * cv(c)) +
                    msftx * 0.5f * g.rdx * ((__ldg(&ht[c + 1]) - h0) * cu(c + 1) + (h0 - __ldg(&ht[c - 1])) * cu(c));
     }
-    for (int k = tk; k <= kend; k += kColKT) {
-      if (k < 1) continue;
+    float wkv[NQ], rwv[NQ], c2mv[NQ], almv[NQ], c2kv[NQ], alkv[NQ], cqv[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k < 1 || k > kend) continue;
       const int p = k * lev + c;
-      const float wk = s[WF_W][p], rwk = __ldg(&s[WF_RW_TEND][p]);
-      const float c2m = __ldg(&c2a[p - lev]), alm = __ldg(&alt[p - lev]);
+      wkv[q] = s[WF_W][p];
+      rwv[q] = __ldg(&s[WF_RW_TEND][p]);
+      c2mv[q] = __ldg(&c2a[p - lev]);
+      almv[q] = __ldg(&alt[p - lev]);
+      if (k < kend) {
+        c2kv[q] = __ldg(&c2a[p]);
+        alkv[q] = __ldg(&alt[p]);
+        cqv[q] = __ldg(&s[WF_CQW][p]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k < 1 || k > kend) continue;
+      const float wk = wkv[q], rwk = rwv[q];
+      const float c2m = c2mv[q], alm = almv[q];
       const float rdnw_m = prdnw[k - 1];
       float wl;
       if (k < kend) {
-        const float c2k = __ldg(&c2a[p]), alk = __ldg(&alt[p]);
+        const float c2k = c2kv[q], alk = alkv[q];
         const float X1 = divc(c2k * prdnw[k], mut, r_mut) * (ep1 * (srhs[k + 1][tx] - srhs[k][tx]) + em1 * (sph[k + 1][tx] - sph[k][tx]));
         const float X2 = divc(c2m * rdnw_m, mut, r_mut) * (ep1 * (srhs[k][tx] - srhs[k - 1][tx]) + em1 * (sph[k][tx] - sph[k - 1][tx]));
-        wl = wk + dts * rwk + msft_inv * __ldg(&s[WF_CQW][p]) * (cp * prdn[k] * (X1 - X2)) +
+        wl = wk + dts * rwk + msft_inv * cqv[q] * (cp * prdn[k] * (X1 - X2)) +
              cq * msft_inv * (prdn[k] * (c2k * alk * st2av[k][tx] - c2m * alm * st2av[k - 1][tx]) - muave);
       } else {
         const float cm = (float)(-0.5 * (double)dts * G);
@@ -464,19 +562,32 @@ __global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s
     const float htop = divc(__ldg(&ph1[kend * lev + c]) + __ldg(&phb[kend * lev + c]), gf, r_g);
     const float hbot = htop - hdepth;
     const float hpi = (float)(0.5 * 3.14159265359);
-    for (int k = tk; k < nz; k += kColKT) {
+    float p1v[NQ], pbv[NQ], wsv[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k < 1 || k >= nz) continue;
+      const int p = k * lev + c;
+      p1v[q] = __ldg(&ph1[p]);
+      pbv[q] = __ldg(&phb[p]);
+      wsv[q] = __ldg(&s[WF_W_SAVE][p]);
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
       const int p = k * lev + c;
       if (k == 0) {
         w[c] = sdw[0][tx];
         continue;
       }
-      const float hk = divc(__ldg(&ph1[p]) + __ldg(&phb[p]), gf, r_g);
+      const float hk = divc(p1v[q] + pbv[q], gf, r_g);
       float dwd = 0.f;
       if (hk >= hbot) {
         const float sn = sinf(divc(hpi * (hk - hbot), hdepth, r_hd));
         dwd = dampmag * (sn * sn);
       }
-      const float num = sdw[k][tx] - dwd * mut * __ldg(&s[WF_W_SAVE][p]);
+      const float num = sdw[k][tx] - dwd * mut * wsv[q];
       const float wk = dwd == 0.f ? num : num / (1.0f + dwd);  // x / 1 == x
       w[p] = wk;
       const float phk = srhs[k][tx] + divc(msfty * 0.5f * dts * gf * ep1 * wk, muts, r_muts);
@@ -487,10 +598,23 @@ __global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s
     const float mu_old = muts - dts * mu_tend;
     const float* ph_save = s[WF_PH_SAVE];
     const float* ph_tend = s[WF_PH_TEND];
-    for (int k = tk; k < nz; k += kColKT) {
+    float phv[NQ], ptv[NQ], psv[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
       const int p = k * lev + c;
-      const float phk = divc(ph[p] * mu_old, muts, r_muts) + divc(dts * __ldg(&ph_tend[p]), muts, r_muts) +
-                        __ldg(&ph_save[p]) * (divc(mu_old, muts, r_muts) - 1.0f);
+      phv[q] = ph[p];
+      ptv[q] = __ldg(&ph_tend[p]);
+      psv[q] = __ldg(&ph_save[p]);
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
+      const int p = k * lev + c;
+      const float phk = divc(phv[q] * mu_old, muts, r_muts) + divc(dts * ptv[q], muts, r_muts) +
+                        psv[q] * (divc(mu_old, muts, r_muts) - 1.0f);
       ph[p] = phk;
       sph[k][tx] = phk;
     }
@@ -504,18 +628,35 @@ __global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s
     const float muuc = last && ur ? __ldg(&s[WF_MUU][c]) : 0.f, mfuc = last && ur ? __ldg(&s[WF_MSFUY][c]) : 1.f;
     const float muvc = last && vr ? __ldg(&s[WF_MUV][c]) : 0.f, mvic = last && vr ? __ldg(&s[WF_MSFVX_INV][c]) : 0.f;
     const float r_nsub = __frcp_rn((float)nsub), r_mfuc = __frcp_rn(mfuc);
-    for (int k = tk; k < nz; k += kColKT) {
+    float am[NQ], bm[NQ], cm[NQ], uv[NQ], vv[NQ], us[NQ], vs[NQ], w1[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
       const int p = k * lev + c;
-      float a = iteration == 1 ? 0.f : ru_m[p];
-      float b = iteration == 1 ? 0.f : rv_m[p];
-      float cc = iteration == 1 ? 0.f : ww_m[p];
-      if (k < nz - 1 && ur) a = a + __ldg(&u[p]);
-      if (k < nz - 1 && vr) b = b + __ldg(&v[p]);
+      am[q] = iteration == 1 ? 0.f : ru_m[p];
+      bm[q] = iteration == 1 ? 0.f : rv_m[p];
+      cm[q] = iteration == 1 ? 0.f : ww_m[p];
+      const bool lv = k < nz - 1;
+      uv[q] = lv && ur ? __ldg(&u[p]) : 0.f;
+      vv[q] = lv && vr ? __ldg(&v[p]) : 0.f;
+      us[q] = last && lv && ur ? __ldg(&s[WF_U_SAVE][p]) : 0.f;
+      vs[q] = last && lv && vr ? __ldg(&s[WF_V_SAVE][p]) : 0.f;
+      w1[q] = last && wr ? __ldg(&ww1[p]) : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
+      const int p = k * lev + c;
+      float a = am[q], b = bm[q], cc = cm[q];
+      if (k < nz - 1 && ur) a = a + uv[q];
+      if (k < nz - 1 && vr) b = b + vv[q];
       if (wr) cc = cc + sww[k][tx];
       if (last) {
-        if (k < nz - 1 && ur) a = divc(a, (float)nsub, r_nsub) + divc(muuc * __ldg(&s[WF_U_SAVE][p]), mfuc, r_mfuc);
-        if (k < nz - 1 && vr) b = divc(b, (float)nsub, r_nsub) + muvc * __ldg(&s[WF_V_SAVE][p]) * mvic;
-        if (wr) cc = divc(cc, (float)nsub, r_nsub) + __ldg(&ww1[p]);
+        if (k < nz - 1 && ur) a = divc(a, (float)nsub, r_nsub) + divc(muuc * us[q], mfuc, r_mfuc);
+        if (k < nz - 1 && vr) b = divc(b, (float)nsub, r_nsub) + muvc * vs[q] * mvic;
+        if (wr) cc = divc(cc, (float)nsub, r_nsub) + w1[q];
       }
       ru_m[p] = a;
       rv_m[p] = b;
@@ -529,13 +670,27 @@ __global__ void __launch_bounds__(kColTX * kColKT, 6) k_acoustic_col(Grid g, S s
     float* al = s[WF_AL];
     float* pp = s[WF_P];
     float* pm1 = s[WF_PM1];
-    for (int k = tk; k < kend; k += kColKT) {
+    float altv[NQ], t1v[NQ], c2v[NQ], tv[NQ], pmv[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= kend) continue;
       const int p = k * lev + c;
-      const float altk = __ldg(&s[WF_ALT][p]), t1k = __ldg(&t1[p]);
-      const float alk = -r_muts * (altk * mu + prdnw[k] * (sph[k + 1][tx] - sph[k][tx]));
+      altv[q] = __ldg(&s[WF_ALT][p]);
+      t1v[q] = __ldg(&t1[p]);
+      c2v[q] = __ldg(&s[WF_C2A][p]);
+      tv[q] = t[p];
+      pmv[q] = pm1[p];
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= kend) continue;
+      const int p = k * lev + c;
+      const float alk = -r_muts * (altv[q] * mu + prdnw[k] * (sph[k + 1][tx] - sph[k][tx]));
       al[p] = alk;
-      const float pnew = __ldg(&s[WF_C2A][p]) * (altk * (t[p] - mu * t1k) / (muts * ((float)T0 + t1k)) - alk);
-      pp[p] = pnew + g.smdiv * (pnew - pm1[p]);
+      const float pnew = c2v[q] * (altv[q] * (tv[q] - mu * t1v[q]) / (muts * ((float)T0 + t1v[q])) - alk);
+      pp[p] = pnew + g.smdiv * (pnew - pmv[q]);
       pm1[p] = pnew;
     }
   }
@@ -628,7 +783,10 @@ int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st) {
 
 int launch_acoustic_col(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st) {
   const dim3 gc((g.ide - g.ids + kColTX - 1) / kColTX, g.jde - g.jds);
-  k_acoustic_col<<<gc, kColTX * kColKT, 0, st>>>(g, s, dts, iteration, nsub);
+  if (g.nz <= 3 * kColKT)
+    k_acoustic_col<3><<<gc, kColTX * kColKT, 0, st>>>(g, s, dts, iteration, nsub);
+  else
+    k_acoustic_col<4><<<gc, kColTX * kColKT, 0, st>>>(g, s, dts, iteration, nsub);
   return 1;
 }
 
