@@ -162,6 +162,17 @@ int wrf_vsolve_w(int ncol, int nz, const float* x, const float* a, const float* 
 int wrf_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const float* alpha, const float* gamma,
                      const float* w_bar, float* x_bar, float* a_bar, float* alpha_bar, float* gamma_bar,
                      void* stream);
+/* wrf_dynamics.py:3316-3388 calc_coef_w on the mass columns [ids, ide-1) x
+ * [jds, jde-1): the tridiagonal coefficients a, alpha, gamma of the implicit
+ * w solve from mut (2-D), cqw, c2a (3-D), rdn, rdnw (profiles); epssm and
+ * top_lid from the grid */
+int wrf_coef_w(const WrfGrid* g, const float* mut, const float* cqw, const float* c2a, const float* rdn,
+               const float* rdnw, float dts, float* a, float* alpha, float* gamma, void* stream);
+/* its adjoint w.r.t. mut, cqw and c2a (accumulates into the *_bar outputs);
+ * the reference obtains it from torch autograd */
+int wrf_coef_w_adj(const WrfGrid* g, const float* mut, const float* cqw, const float* c2a, const float* rdn,
+                   const float* rdnw, float dts, const float* a_bar, const float* alpha_bar,
+                   const float* gamma_bar, float* mut_bar, float* cqw_bar, float* c2a_bar, void* stream);
 /* wrf_physics.py:94-136 microphysics_driver -> wsm6 on the solver's column block */
 int wrf_wsm6(const WrfGrid* g, float* th, float* qv, float* qc, float* qr, float* qi, float* qs,
              float* qg, const float* rho, const float* pii, const float* p, const float* dz8w,

@@ -93,6 +93,10 @@ def lib() -> ctypes.CDLL:
     L.wrf_vsolve_w.argtypes = [ip, ip] + [vp] * 5 + [vp]
     L.wrf_vsolve_w_adj.restype = ip
     L.wrf_vsolve_w_adj.argtypes = [ip, ip] + [vp] * 9 + [vp]
+    L.wrf_coef_w.restype = ip
+    L.wrf_coef_w.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 5 + [ctypes.c_float] + [vp] * 3 + [vp]
+    L.wrf_coef_w_adj.restype = ip
+    L.wrf_coef_w_adj.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 5 + [ctypes.c_float] + [vp] * 6 + [vp]
     L.wrf_wsm6.restype = ip
     L.wrf_wsm6.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 11 + [ctypes.c_float] + [vp] * 7 + [vp]
     L.wrf_wsm6_noalloc.restype = ip

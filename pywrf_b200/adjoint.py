@@ -11,6 +11,9 @@ operators keeps no tape of the forward's intermediates.
 * :class:`RelaxBdytend` -- ``tendency + relax(field)`` toward the lateral
   boundary values (pywrf/wrf_boundary.py:52-147); gradients with respect to
   the field and the incoming tendency (the boundary arrays are data).
+* :class:`CoefW` -- calc_coef_w (pywrf/wrf_dynamics.py:3316-3388): the
+  implicit solve's coefficients a, alpha, gamma from mut, cqw, c2a;
+  gradients with respect to those three.
 * :class:`VSolveW` -- the vertically implicit w solve of advance_w
   (pywrf/wrf_dynamics.py:3761-3767); gradients with respect to the
   right-hand side and the coefficients a, alpha, gamma (the transposed solve).
@@ -150,3 +153,43 @@ class VSolveW(torch.autograd.Function):
 def vsolve_w(x, a, alpha, gamma):
     """Differentiable implicit w solve (all columns of [nz, ...] arrays)."""
     return VSolveW.apply(x, a, alpha, gamma)
+
+
+class CoefW(torch.autograd.Function):
+    """(a, alpha, gamma) = calc_coef_w(mut, cqw, c2a) on the mass columns."""
+
+    @staticmethod
+    def forward(ctx, mut, cqw, c2a, rdn, rdnw, dts: float, epssm: float, top_lid: bool, rdx: float, rdy: float):
+        cg = scalar_grid(cqw.shape, rdx, rdy)
+        cg.epssm = float(epssm)
+        cg.top_lid = int(bool(top_lid))
+        a, alpha, gamma = (torch.zeros_like(cqw) for _ in range(3))
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(cqw.device):
+            rc = N.lib().wrf_coef_w(ctypes.byref(cg), _ptr(mut), _ptr(cqw), _ptr(c2a), _ptr(rdn), _ptr(rdnw),
+                                    float(dts), _ptr(a), _ptr(alpha), _ptr(gamma), stream)
+        N.check(rc, "wrf_coef_w")
+        ctx.save_for_backward(mut, cqw, c2a, rdn, rdnw)
+        ctx.cg, ctx.dts = cg, float(dts)
+        return a, alpha, gamma
+
+    @staticmethod
+    def backward(ctx, ga, galpha, ggamma):
+        mut, cqw, c2a, rdn, rdnw = ctx.saved_tensors
+        z = torch.zeros_like(cqw)
+        ga = z if ga is None else ga.contiguous()
+        galpha = z if galpha is None else galpha.contiguous()
+        ggamma = z if ggamma is None else ggamma.contiguous()
+        mb, cb, c2b = torch.zeros_like(mut), torch.zeros_like(cqw), torch.zeros_like(c2a)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(cqw.device):
+            rc = N.lib().wrf_coef_w_adj(ctypes.byref(ctx.cg), _ptr(mut), _ptr(cqw), _ptr(c2a), _ptr(rdn), _ptr(rdnw),
+                                        ctx.dts, _ptr(ga), _ptr(galpha), _ptr(ggamma), _ptr(mb), _ptr(cb), _ptr(c2b),
+                                        stream)
+        N.check(rc, "wrf_coef_w_adj")
+        return mb, cb, c2b, None, None, None, None, None, None, None
+
+
+def coef_w(mut, cqw, c2a, rdn, rdnw, dts, epssm=0.1, top_lid=False, rdx=1.0 / 9000.0, rdy=1.0 / 9000.0):
+    """Differentiable calc_coef_w: returns (a, alpha, gamma)."""
+    return CoefW.apply(mut, cqw, c2a, rdn, rdnw, dts, epssm, top_lid, rdx, rdy)

@@ -775,6 +775,22 @@ int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cu
   return 4;
 }
 
+int launch_coef_w(const Grid& g, const float* mut, const float* cqw, const float* c2a, const float* rdn,
+                  const float* rdnw, float dts, float* a, float* alpha, float* gamma, cudaStream_t st) {
+  S s{};
+  s.f[WF_MUT] = const_cast<float*>(mut);
+  s.f[WF_CQW] = const_cast<float*>(cqw);
+  s.f[WF_C2A] = const_cast<float*>(c2a);
+  s.f[WF_RDN] = const_cast<float*>(rdn);
+  s.f[WF_RDNW] = const_cast<float*>(rdnw);
+  s.f[WF_A] = a;
+  s.f[WF_ALPHA] = alpha;
+  s.f[WF_GAMMA] = gamma;
+  const dim3 b2(32, 8);
+  k_coef_w<<<col_grid(g, b2), b2, 0, st>>>(g, s, dts);
+  return 1;
+}
+
 int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_advance_uv<<<point_grid(g, b3), b3, 0, st>>>(g, s, dts);

@@ -36,6 +36,12 @@
 //                        The reverse sweep runs the two recurrences backwards
 //                        (one thread per column; the column's y and w are
 //                        recomputed into local arrays).
+//
+//   k_coef_w_adj         adjoint of calc_coef_w (wrf_dynamics.py:3316-3388)
+//                        with respect to cqw, c2a and mut: the column's
+//                        forward recurrence alpha(k) = 1 / (b(k) - a(k)
+//                        gamma(k-1)), gamma(k) = c(k) alpha(k) is recomputed
+//                        into local arrays and run backwards.
 #include "kernels.cuh"
 #include "relax.cuh"
 
@@ -351,6 +357,88 @@ int launch_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const 
                         cudaStream_t st) {
   k_vsolve_w_adj<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, nz, x, a, alpha, gamma, wbar, xbar, abar, alphabar,
                                                       gammabar);
+  return 1;
+}
+
+// one column of calc_coef_w's adjoint; the forward is k_coef_w (k_acoustic.cu)
+__global__ void k_coef_w_adj(Grid g, const float* mut_, const float* cqw, const float* c2a, const float* rdn,
+                             const float* rdnw, float dts, const float* abar, const float* alphabar,
+                             const float* gammabar, float* mutbar, float* cqwbar, float* c2abar) {
+  WRF_COLUMN_INDEX(g, j, i);
+  if (j < g.jds || j >= g.jde - 1 || i < g.ids || i >= g.ide - 1) return;
+  const int nz = g.nz;
+  const int c = g.i2(j, i);
+  const size_t lev = (size_t)g.ny * g.nx;
+  const double cofd = (0.5 * (double)dts * G * (1.0 + (double)g.epssm)) * (0.5 * (double)dts * G * (1.0 + (double)g.epssm));
+  const float cof = (float)cofd, cofm2 = (float)(-2.0 * cofd), cof2 = (float)(2.0 * cofd);
+  const float mut = mut_[c];
+  const float mm = mut * mut;
+  const float lid = g.top_lid ? 0.f : 1.f;
+  float ak[kMaxNz], bk[kMaxNz], ck[kMaxNz], al[kMaxNz], gm[kMaxNz];
+  // forward recomputation (k_coef_w's arithmetic)
+  const float c2t = c2a[(nz - 2) * lev + c], rwt = rdnw[nz - 2];
+  const float atop = cofm2 * (rwt * rwt) * c2t * lid / mm;
+  gm[0] = 0.f;
+  for (int k = 1; k < nz - 1; ++k) {
+    const size_t p = k * lev + c;
+    const float cw = cqw[p];
+    ak[k] = k >= 2 ? -cw * cof * rdn[k] * rdnw[k - 1] * c2a[p - lev] / mm : 0.f;
+    bk[k] = 1.0f + cw * cof * rdn[k] * (rdnw[k] * c2a[p] / mm + rdnw[k - 1] * c2a[p - lev] / mm);
+    ck[k] = -cw * cof * rdn[k] * rdnw[k] * c2a[p] / mm;
+    al[k] = 1.0f / (bk[k] - ak[k] * gm[k - 1]);
+    gm[k] = ck[k] * al[k];
+  }
+  const float btop = 1.0f + cof2 * (rwt * rwt) * c2t / mm;
+  const float altop = 1.0f / (btop - atop * gm[nz - 2]);
+  // reverse
+  float mmb = 0.f, c2tb = 0.f;
+  float gmb = 0.f;  // cotangent of gm[k] flowing down from level k+1
+  {
+    const float alb = alphabar[(nz - 1) * lev + c];
+    const float bb = -altop * altop * alb;
+    const float atb = abar[(nz - 1) * lev + c] + altop * altop * gm[nz - 2] * alb;
+    gmb = altop * altop * atop * alb;
+    // btop = 1 + cof2 rwt^2 c2t / mm ; atop = cofm2 rwt^2 c2t lid / mm
+    c2tb += bb * cof2 * (rwt * rwt) / mm + atb * cofm2 * (rwt * rwt) * lid / mm;
+    mmb += -bb * (btop - 1.0f) / mm - atb * atop / mm;
+  }
+  float c2b_next = 0.f;  // cotangent of c2a at level k (from the k+1 step's c2a(k) terms)
+  for (int k = nz - 2; k >= 1; --k) {
+    const size_t p = k * lev + c;
+    const float cw = cqw[p];
+    const float g_k = gammabar[p] + gmb;               // total cotangent of gm[k]
+    const float ccb = g_k * al[k];
+    const float alb = alphabar[p] + g_k * ck[k];        // total cotangent of al[k]
+    const float a2 = al[k] * al[k];
+    const float bb = -a2 * alb;
+    const float akb = (k >= 2 ? abar[p] : 0.f) + a2 * gm[k - 1] * alb;
+    gmb = a2 * ak[k] * alb;                             // to gm[k-1]
+    const float base = cof * rdn[k] / mm;
+    const float c2k = c2a[p], c2m = c2a[p - lev];
+    // cqw
+    float cwb = bb * base * (rdnw[k] * c2k + rdnw[k - 1] * c2m) - ccb * base * rdnw[k] * c2k;
+    if (k >= 2) cwb += -akb * base * rdnw[k - 1] * c2m;
+    cqwbar[p] += cwb;
+    // c2a(k) and c2a(k-1)
+    float c2kb = bb * cw * base * rdnw[k] - ccb * cw * base * rdnw[k] + c2b_next;
+    float c2mb = bb * cw * base * rdnw[k - 1];
+    if (k >= 2) c2mb += -akb * cw * base * rdnw[k - 1];
+    if (k == nz - 2) c2kb += c2tb;
+    c2abar[p] += c2kb;
+    c2b_next = c2mb;
+    // mm
+    mmb += -bb * (bk[k] - 1.0f) / mm - ccb * ck[k] / mm - (k >= 2 ? akb * ak[k] / mm : 0.f);
+  }
+  c2abar[c] += c2b_next;  // c2a(0), from level 1
+  mutbar[c] += mmb * 2.0f * mut;
+}
+
+int launch_coef_w_adj(const Grid& g, const float* mut, const float* cqw, const float* c2a, const float* rdn,
+                      const float* rdnw, float dts, const float* abar, const float* alphabar, const float* gammabar,
+                      float* mutbar, float* cqwbar, float* c2abar, cudaStream_t st) {
+  const dim3 b2(32, 8);
+  k_coef_w_adj<<<col_grid(g, b2), b2, 0, st>>>(g, mut, cqw, c2a, rdn, rdnw, dts, abar, alphabar, gammabar, mutbar,
+                                               cqwbar, c2abar);
   return 1;
 }
 

@@ -57,6 +57,14 @@ int launch_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const 
                         const float* wbar, float* xbar, float* abar, float* alphabar, float* gammabar,
                         cudaStream_t st);
 
+// calc_coef_w's adjoint w.r.t. cqw, c2a and mut (accumulates) (k_adjoint.cu)
+int launch_coef_w_adj(const Grid& g, const float* mut, const float* cqw, const float* c2a, const float* rdn,
+                      const float* rdnw, float dts, const float* abar, const float* alphabar, const float* gammabar,
+                      float* mutbar, float* cqwbar, float* c2abar, cudaStream_t st);
+// calc_coef_w alone on caller arrays (k_acoustic.cu)
+int launch_coef_w(const Grid& g, const float* mut, const float* cqw, const float* c2a, const float* rdn,
+                  const float* rdnw, float dts, float* a, float* alpha, float* gamma, cudaStream_t st);
+
 // acoustic steps (k_acoustic.cu)
 int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cudaStream_t st);
 int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st);

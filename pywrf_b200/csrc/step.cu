@@ -365,6 +365,31 @@ int wrf_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const flo
   return check_launch("vsolve_w_adj");
 }
 
+int wrf_coef_w(const WrfGrid* gin, const float* mut, const float* cqw, const float* c2a, const float* rdn,
+               const float* rdnw, float dts, float* a, float* alpha, float* gamma, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!mut || !cqw || !c2a || !rdn || !rdnw || !a || !alpha || !gamma) return fail(WRF_EINVAL, "null argument");
+  cudaGetLastError();
+  launch_coef_w(g, mut, cqw, c2a, rdn, rdnw, dts, a, alpha, gamma, static_cast<cudaStream_t>(stream));
+  return check_launch("coef_w");
+}
+
+int wrf_coef_w_adj(const WrfGrid* gin, const float* mut, const float* cqw, const float* c2a, const float* rdn,
+                   const float* rdnw, float dts, const float* a_bar, const float* alpha_bar, const float* gamma_bar,
+                   float* mut_bar, float* cqw_bar, float* c2a_bar, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!mut || !cqw || !c2a || !rdn || !rdnw || !a_bar || !alpha_bar || !gamma_bar || !mut_bar || !cqw_bar || !c2a_bar)
+    return fail(WRF_EINVAL, "null argument");
+  cudaGetLastError();
+  launch_coef_w_adj(g, mut, cqw, c2a, rdn, rdnw, dts, a_bar, alpha_bar, gamma_bar, mut_bar, cqw_bar, c2a_bar,
+                    static_cast<cudaStream_t>(stream));
+  return check_launch("coef_w_adj");
+}
+
 int wrf_wsm6(const WrfGrid* gin, float* th, float* qv, float* qc, float* qr, float* qi, float* qs, float* qg,
              const float* rho, const float* pii, const float* p, const float* dz8w, float delt, float* rainnc,
              float* rainncv, float* snownc, float* snowncv, float* graupelnc, float* graupelncv, float* sr,

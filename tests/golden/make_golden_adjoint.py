@@ -11,7 +11,14 @@ the returned tendency with torch autograd, and writes next to this script:
   fluxes (fluxes of both signs, so both upwind branches are taken);
 * ``relax_adj_ref64.npz`` -- ``pywrf.wrf_boundary.relax_bdytend``
   (wrf_boundary.py:52-147) w.r.t. the field, for the staggers 't', 'u', 'v'
-  and 'h', with the solver's fcx / gcx (solver.py:440-441).
+  and 'h', with the solver's fcx / gcx (solver.py:440-441);
+* ``coefw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_coef_w``
+  (wrf_dynamics.py:3316-3388): the reference's autograd cannot differentiate
+  it (the recurrence updates ``gamma`` in place between its reads, and
+  backward() raises), so the fixture holds central finite differences of the
+  reference's float64 forward instead: for L = sum(a ca + alpha cal + gamma cg)
+  with seeded cotangents, the directional derivatives of L along 3 seeded
+  directions in each of mut, cqw and c2a.
 
 Grid 24x24x12 in the solver's 5-cell frame.  This script is the only producer
 of the fixtures and is never run by the tests.
@@ -114,6 +121,43 @@ def main() -> None:
         out[f"{var}_grad_field"] = field.grad.numpy()
     np.savez_compressed(os.path.join(HERE, "relax_adj_ref64.npz"), **out)
     print("wrote relax_adj_ref64.npz")
+
+    # calc_coef_w
+    rng = np.random.default_rng(13)
+    mut = torch.tensor(8.0e4 + 1.0e3 * rng.standard_normal((N, N)), dtype=torch.float64)
+    cqw = torch.tensor(0.99 + 0.005 * rng.standard_normal(shape), dtype=torch.float64)
+    c2a = torch.tensor(1.6e5 + 1.0e4 * rng.standard_normal(shape), dtype=torch.float64)
+    rdn = torch.tensor(-(35.0 + 10.0 * rng.random(NZ)), dtype=torch.float64)
+    rdnw = torch.tensor(-(35.0 + 10.0 * rng.random(NZ)), dtype=torch.float64)
+    a0, al0, g0 = (torch.zeros(shape, dtype=torch.float64) for _ in range(3))
+    one1 = torch.ones(NZ, dtype=torch.float64)
+    dts, epssm = 11.25, 0.1
+    ca, cal, cg = (rng.standard_normal(shape) for _ in range(3))
+    tca, tcal, tcg = torch.tensor(ca), torch.tensor(cal), torch.tensor(cg)
+    base = {"mut": mut.detach().clone(), "cqw": cqw.detach().clone(), "c2a": c2a.detach().clone()}
+
+    def loss(x):
+        bufs = [torch.zeros(shape, dtype=torch.float64) for _ in range(3)]
+        a_, al_, g_ = dyn.calc_coef_w(*bufs, x["mut"], one1, one1 * 0, one1, one1 * 0, one1, one1 * 0, one1,
+                                      one1 * 0, x["cqw"], rdn, rdnw, x["c2a"], dts, 9.81, epssm, False,
+                                      ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+        return float((a_ * tca).sum() + (al_ * tcal).sum() + (g_ * tcg).sum()), (a_, al_, g_)
+
+    _, (a_, al_, g_) = loss(base)
+    save = dict(mut=base["mut"].numpy(), cqw=base["cqw"].numpy(), c2a=base["c2a"].numpy(), rdn=rdn.numpy(),
+                rdnw=rdnw.numpy(), dts=np.array(dts), epssm=np.array(epssm), a=a_.numpy(), alpha=al_.numpy(),
+                gamma=g_.numpy(), cot_a=ca, cot_alpha=cal, cot_gamma=cg)
+    for name in ("mut", "cqw", "c2a"):
+        for r in range(3):
+            d = rng.standard_normal(tuple(base[name].shape))
+            eps = 1e-6 * float(base[name].abs().max())
+            xp, xm = dict(base), dict(base)
+            xp[name] = base[name] + eps * torch.tensor(d)
+            xm[name] = base[name] - eps * torch.tensor(d)
+            save[f"dir_{name}_{r}"] = d
+            save[f"fd_{name}_{r}"] = np.array((loss(xp)[0] - loss(xm)[0]) / (2 * eps))
+    np.savez_compressed(os.path.join(HERE, "coefw_adj_ref64.npz"), **save)
+    print("wrote coefw_adj_ref64.npz")
 
 
 def importlib_bdy():

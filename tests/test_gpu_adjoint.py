@@ -113,3 +113,25 @@ def test_vsolve_w_and_its_transposed_solve_match_autograd():
     for name, r, t in zip(("x", "a", "alpha", "gamma"), ref_in, gpu_in):
         err = rel_l2(t.grad.cpu().numpy(), r.grad.numpy())
         assert err < 1e-5, (name, err)
+
+
+def test_coef_w_and_its_adjoint_against_the_reference():
+    """calc_coef_w's coefficients against the reference's, and the adjoint's
+    directional derivatives against central finite differences of the
+    reference's float64 forward (tests/golden/coefw_adj_ref64.npz)."""
+    W = load_npz("coefw_adj_ref64.npz")
+    mut = _cuda(W["mut"]).requires_grad_(True)
+    cqw = _cuda(W["cqw"]).requires_grad_(True)
+    c2a = _cuda(W["c2a"]).requires_grad_(True)
+    a, al, ga = adjoint.coef_w(mut, cqw, c2a, _cuda(W["rdn"]), _cuda(W["rdnw"]), float(W["dts"]),
+                               epssm=float(W["epssm"]))
+    for mine, ref in ((a, W["a"]), (al, W["alpha"]), (ga, W["gamma"])):
+        assert rel_l2(mine.detach().cpu().numpy(), ref) < 1e-5
+    L = (a * _cuda(W["cot_a"])).sum() + (al * _cuda(W["cot_alpha"])).sum() + (ga * _cuda(W["cot_gamma"])).sum()
+    L.backward()
+    for name, t in (("mut", mut), ("cqw", cqw), ("c2a", c2a)):
+        gr = t.grad.double().cpu().numpy()
+        for r in range(3):
+            an = float((gr * W[f"dir_{name}_{r}"]).sum())
+            fd = float(W[f"fd_{name}_{r}"])
+            assert abs(an - fd) <= 2e-4 * abs(fd), (name, r, an, fd)

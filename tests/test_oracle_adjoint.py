@@ -75,3 +75,38 @@ def test_relax_golden_pinned_by_the_oracle():
         fd = float(((_relax(g, var, f + d) - _relax(g, var, f - d)) * R[f"{var}_cot"]).sum()) / 2.0
         an = float((d * R[f"{var}_grad_field"]).sum())
         assert abs(fd - an) <= 1e-9 * abs(an), (var, fd, an)
+
+
+W = load_npz("coefw_adj_ref64.npz")
+
+
+def _coefw(g, mut, cqw, c2a):
+    a, al, ga = (np.zeros_like(W["cqw"]) for _ in range(3))
+    OD.calc_coef_w(g, a, al, ga, mut, cqw, W["rdn"], W["rdnw"], c2a, float(W["dts"]), float(W["epssm"]))
+    return a, al, ga
+
+
+def test_coefw_fixture_pinned_by_the_oracle():
+    """The oracle's calc_coef_w reproduces the reference's coefficients on the
+    fixture, and its central finite differences reproduce the fixture's
+    (made from the reference's forward: its autograd cannot differentiate
+    calc_coef_w, which updates gamma in place)."""
+    g = _grid()
+    a, al, ga = _coefw(g, W["mut"], W["cqw"], W["c2a"])
+    for mine, ref in ((a, W["a"]), (al, W["alpha"]), (ga, W["gamma"])):
+        assert np.abs(mine - ref).max() <= 1e-12 * max(np.abs(ref).max(), 1.0)
+    base = {"mut": W["mut"], "cqw": W["cqw"], "c2a": W["c2a"]}
+
+    def loss(x):
+        a, al, ga = _coefw(g, x["mut"], x["cqw"], x["c2a"])
+        return float((a * W["cot_a"]).sum() + (al * W["cot_alpha"]).sum() + (ga * W["cot_gamma"]).sum())
+
+    for name in base:
+        d = W[f"dir_{name}_0"]
+        eps = 1e-6 * float(np.abs(base[name]).max())
+        xp, xm = dict(base), dict(base)
+        xp[name] = base[name] + eps * d
+        xm[name] = base[name] - eps * d
+        fd = (loss(xp) - loss(xm)) / (2 * eps)
+        ref = float(W[f"fd_{name}_0"])
+        assert abs(fd - ref) <= 1e-6 * abs(ref), (name, fd, ref)
