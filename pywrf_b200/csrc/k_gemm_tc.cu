@@ -8,7 +8,7 @@
 // 128 x 128 tile of C, or its part of the K range when the reduction is split:
 //
 //   warp 0, one lane   TMA producer: 128 x 64 tiles of A and B into a
-//                      3-stage ring of 128-byte-swizzled shared buffers
+//                      2-stage ring of 128-byte-swizzled shared buffers (3 CTAs per SM)
 //   warp 1, one lane   MMA issuer: tcgen05.mma.cta_group::1.kind::f16,
 //                      M = 128, N = 128, K = 16 per instruction, fp32
 //                      accumulator in tensor memory (128 lanes x 128 columns);
@@ -29,7 +29,14 @@
 namespace wrf {
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3, kThreads = 128;
+#ifndef WRF_GEMM_STAGES
+#define WRF_GEMM_STAGES 2
+#endif
+#ifndef WRF_GEMM_WARPS
+#define WRF_GEMM_WARPS 4
+#endif
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = WRF_GEMM_STAGES, kWarps = WRF_GEMM_WARPS, kThreads = 32 * kWarps;
+static_assert(kWarps == 4 || kWarps == 8, "the epilogue maps 4 or 8 warps onto the 4 TMEM lane groups");
 constexpr uint32_t kTileBytes = BM * BK * 2;         // 16 KB per operand tile
 constexpr uint32_t kStageBytes = 2 * kTileBytes;
 constexpr uint32_t kTmemCols = BN;                   // fp32 accumulator: 128 lanes x BN columns
@@ -229,11 +236,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   const bool ok = *abort_flag == 0;
   if (!ok && threadIdx.x == 0 && e.err) atomicExch(e.err, 1);
   if (ok) {
-    const int r = warp * 32 + lane;
+    // warp w reads TMEM lane group w % 4 (rows 32 (w % 4) ..); with 8 warps
+    // the two warps of a lane group take half of the columns each
+    const int lg = warp & 3;
+    constexpr int kChunks = BN / 16 / (kWarps / 4);
+    const int c0 = (warp >> 2) * kChunks;
+    const int r = lg * 32 + lane;
     const int m = m0 + r;
     const bool row = m < M;
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    for (int c = 0; c < BN / 16; ++c) {
+    const uint32_t trow = tmem + ((uint32_t)(lg * 32) << 16);
+    for (int c = c0; c < c0 + kChunks; ++c) {
       const int n = n0 + c * 16;
       if (n >= N) break;  // N is a multiple of 16
       float v[16];

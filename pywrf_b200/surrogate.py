@@ -410,3 +410,50 @@ def standardise(net: MlpNet, cgrid, raw_in: torch.Tensor, raw_out: torch.Tensor)
     N.check(N.lib().wrf_mlp_normalize(ctypes.byref(cgrid), _p(net.norm), _p(raw_in), _p(raw_out), n, _p(x), _p(t),
                                       _stream_handle(None)), "wrf_mlp_normalize")
     return x, t
+
+
+def time_forward(cols: int = 51529, hidden: int = 512, km: int = 40, reps: int = 20, device: str = "cuda") -> dict:
+    """CUDA-event time of the network's inference chain (``wrf_mlp_forward``:
+    four tcgen05 products, bias + GELU fused) on ``cols`` random rows of a
+    randomly initialised network of the 240x240x41 layout."""
+    nfeat, nout = 9 * km, 7 * km + 3
+    lay = dict(km=km, ncx=0, ncy=0, ncols=cols, nfeat=nfeat, d0=(nfeat + 63) // 64 * 64, nout=nout,
+               d4=(nout + 63) // 64 * 64)
+    net = MlpNet(lay, hidden=hidden, device=device)
+    g = torch.Generator().manual_seed(1)
+    x = torch.randn(cols, lay["d0"], generator=g).to(torch.bfloat16).to(device)
+    h0 = torch.empty(cols, hidden, dtype=torch.bfloat16, device=device)
+    h1 = torch.empty_like(h0)
+    y = torch.empty(cols, lay["d4"], device=device)
+    err = torch.zeros(1, dtype=torch.int32, device=device)
+    c = net.cstruct()
+    L = N.lib()
+
+    def run(n):
+        for _ in range(n):
+            N.check(L.wrf_mlp_forward(ctypes.byref(c), _p(x), cols, _p(h0), _p(h1), _p(y), _p(err),
+                                      _stream_handle(None)), "wrf_mlp_forward")
+    run(3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    run(reps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    flop = 2 * cols * sum(net.dims[i] * net.dims[i + 1] for i in range(LAYERS))
+    if int(err):
+        raise RuntimeError("a tensor-core kernel's bounded wait ran out")
+    return {"cols": cols, "dims": net.dims, "ms": ms, "tflops": flop / (ms / 1e3) / 1e12}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="time the network's inference chain on the tensor cores")
+    ap.add_argument("--cols", type=int, default=51529)
+    ap.add_argument("--hidden", type=int, default=512)
+    ap.add_argument("--reps", type=int, default=20)
+    a = ap.parse_args()
+    print(json.dumps(time_forward(a.cols, a.hidden, reps=a.reps)))
