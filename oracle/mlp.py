@@ -2,10 +2,11 @@
 
 The reference has no learned part: this module restates, in numpy float64,
 the network the CUDA path trains and evaluates (a 4-layer perceptron with
-GELU(x) = x Phi(x), bf16 weights and activations, fp32 accumulation) so that
+GELU activations, bf16 weights and activations, fp32 accumulation) so that
 the tensor-core forward, input-gradient and weight-gradient products and the
-fused epilogues can be checked.  The bf16 roundings sit where the CUDA path
-stores bf16 (inputs, weights, pre-activations, activations, output and
+fused epilogues can be checked.  GELU is the tanh form
+0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), as in the CUDA epilogues.
+The bf16 roundings sit where the CUDA path stores bf16 (inputs, weights, pre-activations, activations, output and
 hidden gradients); everything else is exact, so the comparison tolerance only
 covers accumulation order and the rare value that rounds to the neighbouring
 bf16.  Only tests/ import this module.
@@ -13,7 +14,6 @@ bf16.  Only tests/ import this module.
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 
 def bf16(a: np.ndarray) -> np.ndarray:
@@ -24,12 +24,17 @@ def bf16(a: np.ndarray) -> np.ndarray:
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+_C, _A = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    """GELU in its tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))."""
+    return 0.5 * x * (1.0 + np.tanh(_C * x * (1.0 + _A * x * x)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+    th = np.tanh(_C * x * (1.0 + _A * x * x))
+    return 0.5 * (1.0 + th) + 0.5 * x * (1.0 - th * th) * _C * (1.0 + 3.0 * _A * x * x)
 
 
 def forward(x, w, b):

@@ -32,6 +32,15 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # p0*pp - pb ...) for no measurable gain in these memory-bound kernels.
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                      "-I" + INCLUDE, "-I" + CSRC]
+# the network's tensor-core products have no reference operation order to
+# follow: their epilogues may contract multiply-adds
+FMAD_SOURCES = {"k_gemm_tc.cu"}
+
+
+def flags_for(src: str) -> list[str]:
+    if os.path.basename(src) in FMAD_SOURCES:
+        return [f if f != "-fmad=false" else "-fmad=true" for f in NVCC_FLAGS]
+    return list(NVCC_FLAGS)
 
 
 def nvcc_path() -> str:
@@ -66,7 +75,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
 
     def compile_one(so):
         s, o = so
-        cmd = [nvcc] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", s, "-o", o]
+        cmd = [nvcc] + flags_for(s) + (["-Xptxas", "-v"] if verbose else []) + ["-c", s, "-o", o]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {os.path.basename(s)}:\n{r.stderr}")
