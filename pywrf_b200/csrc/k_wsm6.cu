@@ -1040,10 +1040,16 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_wsm6(Grid g, Wsm6Args a
 // and the moisture slots; k_wsm6_finish then runs the point processes, the
 // finish step and the equation of state one point per thread.  The
 // arithmetic is that of k_physics, operation for operation.
-template <int SEG, int NS>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_wsm6_sed(Grid g, S s, float dt) {
+// With kList, the columns are those of a list (list[0] entries from
+// list[16], each j * nx + i of a column of the scheme's block): the WSM6
+// fallback of the surrogate microphysics for the columns its gate rejected.
+template <int SEG, int NS, bool kList = false>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_wsm6_sed(Grid g, S s, float dt, const int* list = nullptr) {
   constexpr int SPW = 32 / SEG, SPB = kWarpsPerBlock * SPW;
   __shared__ SegScratch<SEG, NS> scratch[SPB];
+  if constexpr (kList) {
+    if ((int)blockIdx.x * SPB >= __ldg(list)) return;  // whole block past the list (uniform exit)
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int segw = lane / SEG;
   Seg<SEG, NS> sg;
@@ -1052,9 +1058,19 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_wsm6_sed(Grid g, S s, f
   sg.km = g.nz - 1;
   const int km = sg.km;
   const int col = warp * SPW + segw;
-  const int j = g.jds + 1 + blockIdx.y;
-  const int i = g.ids + 1 + blockIdx.x * SPB + col;
-  const bool run = i < g.ide - 2 && j < g.jde - 2;
+  int j, i;
+  bool run;
+  if constexpr (kList) {
+    const int idx = blockIdx.x * SPB + col;
+    run = idx < __ldg(list);
+    const int code = run ? __ldg(list + 16 + idx) : 0;
+    j = code / g.nx;
+    i = code - j * g.nx;
+  } else {
+    j = g.jds + 1 + blockIdx.y;
+    i = g.ids + 1 + blockIdx.x * SPB + col;
+    run = i < g.ide - 2 && j < g.jde - 2;
+  }
   const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
   const int c2 = run ? g.i2(j, i) : 0;
   float* M = s[WF_MOIST];
@@ -1110,11 +1126,10 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_wsm6_sed(Grid g, S s, f
   }
 }
 
-__global__ void __launch_bounds__(128) k_wsm6_finish(Grid g, S s, float dt, float dtcld) {
-  WRF_POINT_INDEX(g, k, j, i);
-  if (k >= g.nz - 1 || j < g.jds || j >= g.jde - 1 || i < g.ids || i >= g.ide - 1) return;
-  const bool run = j >= g.jds + 1 && j < g.jde - 2 && i >= g.ids + 1 && i < g.ide - 2;
-  const bool prep = j >= g.jds + 1 && i >= g.ids + 1;
+// one mass point of the finish kernel: run = in the scheme's block, prep =
+// prepared by moist_physics_prep_em (zero tendencies outside the block)
+__device__ __forceinline__ void wsm6_finish_point(const Grid& g, const S& s, int k, int j, int i, float dt,
+                                                  float dtcld, bool run, bool prep) {
   const size_t n3 = g.n3();
   const int c2 = g.i2(j, i);
   const size_t p = (size_t)k * g.ny * g.nx + c2;
@@ -1162,6 +1177,26 @@ __global__ void __launch_bounds__(128) k_wsm6_finish(Grid g, S s, float dt, floa
     s[WF_QC_DIABATIC][p] = 0.0f;
   }
   eos_point(g, s, k, p, c2, T, qvnew);
+}
+
+__global__ void __launch_bounds__(128) k_wsm6_finish(Grid g, S s, float dt, float dtcld) {
+  WRF_POINT_INDEX(g, k, j, i);
+  if (k >= g.nz - 1 || j < g.jds || j >= g.jde - 1 || i < g.ids || i >= g.ide - 1) return;
+  const bool run = j >= g.jds + 1 && j < g.jde - 2 && i >= g.ids + 1 && i < g.ide - 2;
+  const bool prep = j >= g.jds + 1 && i >= g.ids + 1;
+  wsm6_finish_point(g, s, k, j, i, dt, dtcld, run, prep);
+}
+
+// the finish kernel on the listed columns (see k_wsm6_sed's list mode):
+// thread x = list entry, block y = level
+__global__ void __launch_bounds__(128) k_wsm6_finish_list(Grid g, S s, float dt, float dtcld, const int* list) {
+  const int n = __ldg(list);
+  if ((int)(blockIdx.x * blockDim.x) >= n) return;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (idx >= n) return;
+  const int code = __ldg(list + 16 + idx);
+  const int j = code / g.nx, i = code - j * g.nx;
+  wsm6_finish_point(g, s, k, j, i, dt, dtcld, true, true);
 }
 
 // ------------------------------------------------------------- no-alloc WSM6
@@ -1299,7 +1334,9 @@ __global__ void __launch_bounds__(128) k_wsm6_finish_args(Grid g, Wsm6Args a, fl
 //             -tol_neg before clipping, or the new qv exceeds saturation over
 //             water by more than the fraction tol_sat: the column is left
 //             untouched and appended to list (entries j * nx + i from
-//             list[16]); k_physics<..., true> then runs WSM6 on it;
+//             list[16]); WSM6 then runs on it (k_wsm6_sed and
+//             k_wsm6_finish_list in list mode, or k_physics in list mode for
+//             two time-split loops);
 //   network   otherwise: the increments (species clipped at zero).
 // The step's precipitation is clipped to [0, condensate within kMlpMaxFall *
 // dt of the ground] (all species for rainncv, snow + ice for snowncv, graupel
@@ -1606,8 +1643,23 @@ int launch_physics_mlp(const Grid& g, const S& s, const MlpNetDev& net, const Ml
       g, s, L, net.norm, work.y, net.tol_neg, net.tol_sat, g.dt, work.list,
       static_cast<unsigned char*>(work.colstat));
   ++n;
+  // WSM6 on the rejected columns: the split kernels when one time-split loop
+  // suffices (as in launch_physics), else the fused column kernel
   const int km = g.nz - 1;
   const dim3 b(32 * kWarpsPerBlock);
+  const double loops = fmax(g.dtd / mp::DTCLDCR, 1.0);
+  if ((int)loops == 1) {
+    const float dtcld = (g.dtd <= mp::DTCLDCR) ? g.dt : (float)(1.0 * g.dtd / loops);
+    if (km <= 47) {
+      constexpr int SPB = kWarpsPerBlock * 2;
+      k_wsm6_sed<16, 3, true><<<(L.ncols + SPB - 1) / SPB, b, 0, st>>>(g, s, g.dt, work.list);
+    } else {
+      constexpr int SPB = kWarpsPerBlock;
+      k_wsm6_sed<32, 2, true><<<(L.ncols + SPB - 1) / SPB, b, 0, st>>>(g, s, g.dt, work.list);
+    }
+    k_wsm6_finish_list<<<dim3((L.ncols + 127) / 128, km), 128, 0, st>>>(g, s, g.dt, dtcld, work.list);
+    return n + 2;
+  }
   if (km <= 47) {
     constexpr int SPB = kWarpsPerBlock * 2;
     k_physics<16, 3, true><<<(L.ncols + SPB - 1) / SPB, b, 0, st>>>(g, s, g.dt, work.list);
