@@ -109,16 +109,24 @@ __global__ void k_p_rho0(Grid g, S s) {
   s[WF_PM1][p] = pnew;
 }
 
-__global__ void k_coef_w(Grid g, S s, float dts) {
-  WRF_COLUMN_INDEX(g, j, i);
-  if (j < g.jds || j >= g.jde - 1 || i < g.ids || i >= g.ide - 1) return;
+// calc_coef_w: a block owns 16 adjacent mass columns of one row and 16 level
+// groups; the per-level coefficients a, b, c are formed in parallel into
+// shared memory, one thread per column runs the recurrence alpha = 1 / (b - a
+// gamma), gamma = c alpha in the reference's order, and the levels are stored
+// in parallel again.
+constexpr int kCwTX = 16, kCwKT = 16;
+
+__global__ void __launch_bounds__(kCwTX * kCwKT) k_coef_w(Grid g, S s, float dts) {
+  __shared__ float sa[kMaxNz][kCwTX], sb[kMaxNz][kCwTX], sc[kMaxNz][kCwTX];
+  __shared__ float stop[2][kCwTX];  // atop, alpha at the top
+  const int tx = threadIdx.x % kCwTX, tk = threadIdx.x / kCwTX;
+  const int i = g.ids + blockIdx.x * kCwTX + tx, j = g.jds + blockIdx.y;
+  const bool col = i < g.ide - 1;
   const int nz = g.nz;
-  const int c = g.i2(j, i);
+  const int c = col ? g.i2(j, i) : g.i2(j, g.ids);
   const size_t lev = (size_t)g.ny * g.nx;
   const double cofd = (0.5 * (double)dts * G * (1.0 + (double)g.epssm)) * (0.5 * (double)dts * G * (1.0 + (double)g.epssm));
   const float cof = (float)cofd, cofm2 = (float)(-2.0 * cofd), cof2 = (float)(2.0 * cofd);
-  const float mut = s[WF_MUT][c];
-  const float mm = mut * mut;
   const float* cqw = s[WF_CQW];
   const float* c2a = s[WF_C2A];
   const float* rdn = s[WF_RDN];
@@ -126,30 +134,49 @@ __global__ void k_coef_w(Grid g, S s, float dts) {
   float* a = s[WF_A];
   float* alpha = s[WF_ALPHA];
   float* gamma = s[WF_GAMMA];
-  const float lid = g.top_lid ? 0.f : 1.f;
-  a[lev + c] = 0.f;
-  const float atop = cofm2 * (rdnw[nz - 2] * rdnw[nz - 2]) * c2a[(nz - 2) * lev + c] * lid / mm;
-  a[(nz - 1) * lev + c] = atop;
-  gamma[c] = 0.f;
-  float gm = 0.f;
-  for (int k = 1; k < nz - 1; ++k) {
-    const size_t p = k * lev + c;
-    const float cw = cqw[p];
-    float ak = 0.f;
-    if (k >= 2) {
-      ak = -cw * cof * rdn[k] * rdnw[k - 1] * c2a[p - lev] / mm;
-      a[p] = ak;
+  const float mut = col ? s[WF_MUT][c] : 1.f;
+  const float mm = mut * mut;
+  if (col) {
+    for (int k = 1 + tk; k < nz - 1; k += kCwKT) {
+      const size_t p = k * lev + c;
+      const float cw = __ldg(&cqw[p]), c2k = __ldg(&c2a[p]), c2m = __ldg(&c2a[p - lev]);
+      sa[k][tx] = k >= 2 ? -cw * cof * rdn[k] * rdnw[k - 1] * c2m / mm : 0.f;
+      sb[k][tx] = 1.0f + cw * cof * rdn[k] * (rdnw[k] * c2k / mm + rdnw[k - 1] * c2m / mm);
+      sc[k][tx] = -cw * cof * rdn[k] * rdnw[k] * c2k / mm;
     }
-    const float b = 1.0f + cw * cof * rdn[k] * (rdnw[k] * c2a[p] / mm + rdnw[k - 1] * c2a[p - lev] / mm);
-    const float cc = -cw * cof * rdn[k] * rdnw[k] * c2a[p] / mm;
-    const float al = 1.0f / (b - ak * gm);
-    alpha[p] = al;
-    gm = cc * al;
-    gamma[p] = gm;
   }
-  const float btop = 1.0f + cof2 * (rdnw[nz - 2] * rdnw[nz - 2]) * c2a[(nz - 2) * lev + c] / mm;
-  alpha[(nz - 1) * lev + c] = 1.0f / (btop - atop * gm);
-  gamma[(nz - 1) * lev + c] = 0.f;
+  __syncthreads();
+  if (col && tk == 0) {
+    const float lid = g.top_lid ? 0.f : 1.f;
+    const float c2t = __ldg(&c2a[(nz - 2) * lev + c]);
+    const float atop = cofm2 * (rdnw[nz - 2] * rdnw[nz - 2]) * c2t * lid / mm;
+    float gm = 0.f;
+    for (int k = 1; k < nz - 1; ++k) {
+      const float al = 1.0f / (sb[k][tx] - sa[k][tx] * gm);
+      sb[k][tx] = al;  // alpha(k)
+      gm = sc[k][tx] * al;
+      sc[k][tx] = gm;  // gamma(k)
+    }
+    const float btop = 1.0f + cof2 * (rdnw[nz - 2] * rdnw[nz - 2]) * c2t / mm;
+    stop[0][tx] = atop;
+    stop[1][tx] = 1.0f / (btop - atop * gm);
+  }
+  __syncthreads();
+  if (!col) return;
+  for (int k = tk; k < nz; k += kCwKT) {
+    const size_t p = k * lev + c;
+    if (k == 0) {
+      gamma[p] = 0.f;
+    } else if (k < nz - 1) {
+      a[p] = k >= 2 ? sa[k][tx] : 0.f;
+      alpha[p] = sb[k][tx];
+      gamma[p] = sc[k][tx];
+    } else {
+      a[p] = stop[0][tx];
+      alpha[p] = stop[1][tx];
+      gamma[p] = 0.f;
+    }
+  }
 }
 
 __global__ void k_advance_uv(Grid g, S s, float dts) {
@@ -771,7 +798,7 @@ int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cu
   k_ssp2d<<<col_grid(g, b2), b2, 0, st>>>(g, s, rk_step);
   k_ssp3d<<<point_grid(g, b3), b3, 0, st>>>(g, s, rk_step);
   k_p_rho0<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  k_coef_w<<<col_grid(g, b2), b2, 0, st>>>(g, s, dts);
+  k_coef_w<<<dim3((g.ide - 1 - g.ids + kCwTX - 1) / kCwTX, g.jde - 1 - g.jds), kCwTX * kCwKT, 0, st>>>(g, s, dts);
   return 4;
 }
 
@@ -786,8 +813,7 @@ int launch_coef_w(const Grid& g, const float* mut, const float* cqw, const float
   s.f[WF_A] = a;
   s.f[WF_ALPHA] = alpha;
   s.f[WF_GAMMA] = gamma;
-  const dim3 b2(32, 8);
-  k_coef_w<<<col_grid(g, b2), b2, 0, st>>>(g, s, dts);
+  k_coef_w<<<dim3((g.ide - 1 - g.ids + kCwTX - 1) / kCwTX, g.jde - 1 - g.jds), kCwTX * kCwKT, 0, st>>>(g, s, dts);
   return 1;
 }
 

@@ -74,34 +74,63 @@ __global__ void k_rk_prep3d(Grid g, S s) {
   if (mrow && mcol) s[WF_RW][p] = s[WF_W][p] * s[WF_MUT][c] / s[WF_MSFT][c];
 }
 
-__global__ void k_ww_cp(Grid g, S s) {
-  WRF_COLUMN_INDEX(g, j, i);
-  if (j < g.jds || j >= g.jde - 1 || i < g.ids || i >= g.ide - 1) return;
+// calc_ww_cp: a block owns 16 adjacent mass columns of one row and 16 level
+// groups; the per-level divergences are formed in parallel into shared
+// memory, then one thread per column forms the column sum and the upward scan
+// in the reference's order, and the levels are stored in parallel again.
+constexpr int kWwTX = 16, kWwKT = 16, kWwQ = (kMaxNz + kWwKT - 1) / kWwKT;
+
+__global__ void __launch_bounds__(kWwTX * kWwKT) k_ww_cp(Grid g, S s) {
+  __shared__ float sdv[kMaxNz][kWwTX], sww[kMaxNz][kWwTX];
+  const int tx = threadIdx.x % kWwTX, tk = threadIdx.x / kWwTX;
+  const int i = g.ids + blockIdx.x * kWwTX + tx, j = g.jds + blockIdx.y;
+  const bool col = i < g.ide - 1;
   const int ktf = g.nz - 1;
-  const int c = g.i2(j, i), ce = c + 1, cn = c + g.nx;
+  const int c = col ? g.i2(j, i) : g.i2(j, g.ids), ce = c + 1, cn = c + g.nx;
   const float* u = s[WF_U];
   const float* v = s[WF_V];
-  const float muu0 = s[WF_MUU][c], muu1 = s[WF_MUU][ce], mfu0 = s[WF_MSFUY][c], mfu1 = s[WF_MSFUY][ce];
-  const float muv0 = s[WF_MUV][c], muv1 = s[WF_MUV][cn], mfv0 = s[WF_MSFVX_INV][c], mfv1 = s[WF_MSFVX_INV][cn];
-  const float msftx = s[WF_MSFTX][c];
   const float* dnw = s[WF_DNW];
   const float* c1h = s[WF_C1H];
-  const float rdx = g.rdx, rdy = g.rdy;
   const size_t lev = (size_t)g.ny * g.nx;
-  auto divv = [&](int k) {
-    const size_t p = k * lev + c;
-    const float fu1 = muu1 * u[p + 1] / mfu1, fu0 = muu0 * u[p] / mfu0;
-    const float fv1 = muv1 * v[p + g.nx] * mfv1, fv0 = muv0 * v[p] * mfv0;
-    return (msftx * dnw[k]) * (rdx * (fu1 - fu0) + rdy * (fv1 - fv0));
-  };
-  float dmdt = 0.f;
-  for (int k = 0; k < ktf; ++k) dmdt = dmdt + divv(k);
-  float* ww = s[WF_WW];
-  float wk = ww[c];
-  for (int k = 0; k < ktf - 1; ++k) {
-    wk = wk - (dnw[k] * c1h[k]) * dmdt - divv(k);
-    ww[(k + 1) * lev + c] = wk;
+  if (col) {
+    const float muu0 = s[WF_MUU][c], muu1 = s[WF_MUU][ce], mfu0 = s[WF_MSFUY][c], mfu1 = s[WF_MSFUY][ce];
+    const float muv0 = s[WF_MUV][c], muv1 = s[WF_MUV][cn], mfv0 = s[WF_MSFVX_INV][c], mfv1 = s[WF_MSFVX_INV][cn];
+    const float msftx = s[WF_MSFTX][c];
+    const float rdx = g.rdx, rdy = g.rdy;
+    float ue[kWwQ], u0[kWwQ], vn[kWwQ], v0[kWwQ];
+#pragma unroll
+    for (int q = 0; q < kWwQ; ++q) {
+      const int k = tk + q * kWwKT;
+      if (k >= ktf) continue;
+      const size_t p = k * lev + c;
+      ue[q] = __ldg(&u[p + 1]);
+      u0[q] = __ldg(&u[p]);
+      vn[q] = __ldg(&v[p + g.nx]);
+      v0[q] = __ldg(&v[p]);
+    }
+#pragma unroll
+    for (int q = 0; q < kWwQ; ++q) {
+      const int k = tk + q * kWwKT;
+      if (k >= ktf) continue;
+      const float fu1 = muu1 * ue[q] / mfu1, fu0 = muu0 * u0[q] / mfu0;
+      const float fv1 = muv1 * vn[q] * mfv1, fv0 = muv0 * v0[q] * mfv0;
+      sdv[k][tx] = (msftx * dnw[k]) * (rdx * (fu1 - fu0) + rdy * (fv1 - fv0));
+    }
   }
+  __syncthreads();
+  float* ww = s[WF_WW];
+  if (col && tk == 0) {
+    float dmdt = 0.f;
+    for (int k = 0; k < ktf; ++k) dmdt = dmdt + sdv[k][tx];
+    float wk = ww[c];
+    for (int k = 0; k < ktf - 1; ++k) {
+      wk = wk - (dnw[k] * c1h[k]) * dmdt - sdv[k][tx];
+      sww[k + 1][tx] = wk;
+    }
+  }
+  __syncthreads();
+  if (col)
+    for (int k = 1 + tk; k < ktf; k += kWwKT) ww[k * lev + c] = sww[k][tx];
 }
 
 __global__ void k_diff_metrics(Grid g, S s) {
@@ -421,7 +450,7 @@ int launch_prep(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);
   k_rk_prep2d<<<col_grid(g, b2), b2, 0, st>>>(g, s);
   k_rk_prep3d<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  k_ww_cp<<<col_grid(g, b2), b2, 0, st>>>(g, s);
+  k_ww_cp<<<dim3((g.ide - 1 - g.ids + kWwTX - 1) / kWwTX, g.jde - 1 - g.jds), kWwTX * kWwKT, 0, st>>>(g, s);
   return 3;
 }
 
