@@ -123,6 +123,44 @@ const char* wrf_last_error(void);
  * so the call can be captured once in a CUDA graph and replayed. */
 int wrf_rk3_step(const WrfGrid* g, const WrfState* s, void* stream, wrf_probe_fn probe, void* user);
 
+/* The same step one phase at a time, for a caller that drives the RK3 loop
+ * itself as WrfSolver.solve does (pywrf/solver.py:709-1910).  Calling, in
+ * this order,
+ *   wrf_step_begin;
+ *   for rk_step = 1, 2, 3:
+ *     wrf_rk_prep(rk_step); if rk_step == 1: wrf_diff_stage1;
+ *     wrf_tend_stage(rk_step); wrf_acoustic_prep(rk_step);
+ *     for iteration = 1 .. nsub: wrf_acoustic_substep(rk_step, iteration)
+ *       (nsub = 1, soundsteps / 2, soundsteps for rk_step 1, 2, 3);
+ *     wrf_acoustic_finish(rk_step); wrf_moist_stage(rk_step);
+ *   wrf_microphysics; wrf_step_end
+ * enqueues exactly the kernels of one wrf_rk3_step.  The phases:
+ *   step_begin        boundary time of the step (solver.py:713-718)
+ *   rk_prep           rk_step_prep and its halo copies (solver.py:736-778)
+ *   diff_stage1       first stage only: physics tendencies zeroed, diffusion
+ *                     metrics, deformation, eddy viscosities (solver.py:880-985)
+ *   tend_stage        advection, pressure gradient, buoyancy, Coriolis,
+ *                     curvature; first-stage horizontal diffusion and
+ *                     relaxation; rk_addtend_dry (solver.py:987-1256)
+ *   acoustic_prep     small_step_prep, calc_p_rho, calc_coef_w (solver.py:1258-1345)
+ *   acoustic_substep  advance_uv, advance_mu_t, advance_w, sumflux,
+ *                     calc_p_rho, lateral updates (solver.py:1350-1492)
+ *   acoustic_finish   small_step_finish (solver.py:1494-1546)
+ *   moist_stage       moisture transport and update (solver.py:1548-1710)
+ *   microphysics      WSM6 and calc_p_rho_phi (solver.py:1714-1766)
+ *   step_end          end-of-step lateral boundaries (solver.py:1776-1910)
+ * rk_step outside 1..3 or an iteration outside 1..nsub is WRF_EINVAL. */
+int wrf_step_begin(const WrfGrid* g, const WrfState* s, void* stream);
+int wrf_rk_prep(const WrfGrid* g, const WrfState* s, int rk_step, void* stream);
+int wrf_diff_stage1(const WrfGrid* g, const WrfState* s, void* stream);
+int wrf_tend_stage(const WrfGrid* g, const WrfState* s, int rk_step, void* stream);
+int wrf_acoustic_prep(const WrfGrid* g, const WrfState* s, int rk_step, void* stream);
+int wrf_acoustic_substep(const WrfGrid* g, const WrfState* s, int rk_step, int iteration, void* stream);
+int wrf_acoustic_finish(const WrfGrid* g, const WrfState* s, int rk_step, void* stream);
+int wrf_moist_stage(const WrfGrid* g, const WrfState* s, int rk_step, void* stream);
+int wrf_microphysics(const WrfGrid* g, const WrfState* s, void* stream);
+int wrf_step_end(const WrfGrid* g, const WrfState* s, void* stream);
+
 /* Reference function-level entry points (same arguments as the step
  * driver; each runs exactly the reference function named). */
 /* wrf_dynamics.py:1841-2028 advect_scalar: tend += flux-form advection of field */

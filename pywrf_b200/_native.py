@@ -80,6 +80,15 @@ def lib() -> ctypes.CDLL:
     L.wrf_last_error.restype = ctypes.c_char_p
     L.wrf_rk3_step.restype = ip
     L.wrf_rk3_step.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, PROBE_FN, vp]
+    G0 = ctypes.POINTER(WrfGridC)
+    for name in ("wrf_step_begin", "wrf_diff_stage1", "wrf_microphysics", "wrf_step_end"):
+        getattr(L, name).restype = ip
+        getattr(L, name).argtypes = [G0, vp, vp]
+    for name in ("wrf_rk_prep", "wrf_tend_stage", "wrf_acoustic_prep", "wrf_acoustic_finish", "wrf_moist_stage"):
+        getattr(L, name).restype = ip
+        getattr(L, name).argtypes = [G0, vp, ip, vp]
+    L.wrf_acoustic_substep.restype = ip
+    L.wrf_acoustic_substep.argtypes = [G0, vp, ip, ip, vp]
     L.wrf_advect_scalar.restype = ip
     L.wrf_advect_scalar.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 9 + [vp]
     L.wrf_advect_scalar_adj.restype = ip

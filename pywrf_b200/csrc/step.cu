@@ -136,93 +136,133 @@ struct Driver {
     n += launch_bc(g, b, st);
   }
 
-  void run() {
-    const float dt = g.dt;
+  // dt_rk, dts_rk and the substep count of RK stage rk (solver.py:722-735)
+  void stage(int rk, float& dt_rk, float& dts_rk, int& nsub) const {
     const float dts = (float)(g.dtd / g.soundsteps);
+    if (rk == 1) { dt_rk = (float)(g.dtd / 3.0); dts_rk = dt_rk; nsub = 1; }
+    else if (rk == 2) { dt_rk = (float)(0.5 * g.dtd); dts_rk = dts; nsub = g.soundsteps / 2; }
+    else { dt_rk = g.dt; dts_rk = dts; nsub = g.soundsteps; }
+  }
+
+  // boundary time of the step from the device step counter (solver.py:713)
+  void step_begin() {
+    if (rc != WRF_OK) return;
     k_step_begin<<<1, 1, 0, st>>>(s[WF_DSCAL], reinterpret_cast<const int*>(s[WF_STATUS]), bdy_interval, g.dtd);
     ++n;
-    if (!ok("step_begin")) return;
+    ok("step_begin");
+  }
+  // rk_step_prep (solver.py:736-778)
+  void rk_prep(int rk) {
+    if (rc != WRF_OK) return;
     char tag[32];
-    for (int rk = 1; rk <= 3; ++rk) {
-      float dt_rk, dts_rk;
-      int nsub;
-      if (rk == 1) { dt_rk = (float)(g.dtd / 3.0); dts_rk = dt_rk; nsub = 1; }
-      else if (rk == 2) { dt_rk = (float)(0.5 * g.dtd); dts_rk = dts; nsub = g.soundsteps / 2; }
-      else { dt_rk = dt; dts_rk = dts; nsub = g.soundsteps; }
-      // rk_step_prep (solver.py:736-778)
-      n += launch_prep(g, s, st);
-      bc({{WF_RU, 'u'}, {WF_RV, 'v'}, {WF_RW, 'w'}, {WF_WW, 'w'}, {WF_PHP, 'w'}, {WF_ALT, 't'}, {WF_P, 'p'},
-          {WF_AL, 'p'}, {WF_PH, 'w'}},
-         {{WF_MUU, 'u'}, {WF_MUV, 'v'}, {WF_MUT, 't'}});
-      snprintf(tag, sizeof tag, "s%d.prep", rk);
-      phase(tag);
-      if (rk == 1) {
-        // physics tendencies start from zero; diffusion metrics and eddy viscosities
-        zero3(WF_RU_TENDF); zero3(WF_RV_TENDF); zero3(WF_RW_TENDF); zero3(WF_PH_TENDF); zero3(WF_T_TENDF);
-        zero2(WF_MU_TENDF);
-        zero4(WF_MOIST_TEND);
-        n += launch_diff_metrics(g, s, st);
-        bc({{WF_RDZW, 'w'}, {WF_ZX, 'e'}, {WF_ZY, 'f'}});
-        n += launch_km(g, s, st);
-        bc({{WF_XKMH, 't'}, {WF_XKHH, 't'}});
-        snprintf(tag, sizeof tag, "s%d.km", rk);
-        phase(tag);
-      }
-      zero3(WF_RU_TEND); zero3(WF_RV_TEND); zero3(WF_RW_TEND); zero3(WF_T_TEND); zero3(WF_PH_TEND);
-      zero3(WF_U_SAVE); zero3(WF_V_SAVE); zero3(WF_W_SAVE); zero3(WF_PH_SAVE); zero3(WF_T_SAVE);
-      zero2(WF_MU_TEND); zero2(WF_MU_SAVE);
-      n += launch_advect_forces(g, s, st);
-      snprintf(tag, sizeof tag, "s%d.forces", rk);
-      phase(tag);
-      if (rk == 1) {
-        n += launch_hdiff_relax(g, s, st);
-        snprintf(tag, sizeof tag, "s%d.diff", rk);
-        phase(tag);
-      }
-      n += launch_addtend(g, s, rk, st);
-      snprintf(tag, sizeof tag, "s%d.tend", rk);
-      phase(tag);
-      // acoustic set-up (solver.py:1258-1345)
-      n += launch_small_step_prep(g, s, rk, dts_rk, st);
-      bc({{WF_RU_TEND, 'u'}, {WF_RV_TEND, 'v'}, {WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}, {WF_T_1, 't'},
-          {WF_T_SAVE, 't'}},
-         {{WF_MU_1, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
-      snprintf(tag, sizeof tag, "s%d.acprep", rk);
-      phase(tag);
-      for (int it = 1; it <= nsub; ++it) {
-        // advance_uv, then the column update (mu/theta, w/phi, sumflux,
-        // p/al), then zero_grad_bdy(w) and the halo copies
-        n += launch_advance_uv(g, s, dts_rk, st);
-        snprintf(tag, sizeof tag, "s%d.sub%d.uv", rk, it);
-        phase(tag);
-        n += launch_acoustic_col(g, s, dts_rk, it, nsub, st);
-        snprintf(tag, sizeof tag, "s%d.sub%d.col", rk, it);
-        phase(tag);
-        n += launch_zero_grad_w(g, s, st);
-        bc({{WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}}, {{WF_MUTS, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
-        snprintf(tag, sizeof tag, "s%d.sub%d", rk, it);
-        phase(tag);
-      }
-      n += launch_small_step_finish(g, s, dts_rk, nsub, rk, st);
-      if (rk == 3)
-        bc({{WF_RU_M, 'u'}, {WF_RV_M, 'v'}, {WF_WW_M, 'w'}}, {{WF_MUT, 't'}, {WF_MUTS, 't'}});
-      snprintf(tag, sizeof tag, "s%d.acfinish", rk);
-      phase(tag);
-      // moisture transport (solver.py:1548-1604)
-      n += launch_advect_moist(g, s, st);
-      if (rk == 1) {
-        n += launch_hdiff_moist(g, s, st);
-        n += launch_relax_qv(g, s, st);
-      }
-      n += launch_moist(g, s, rk, dt_rk, st);
-      if (rk < 3) {
-        bc({{WF_U, 'U'}, {WF_V, 'V'}, {WF_W, 'w'}, {WF_T, 'p'}, {WF_PH, 'w'}}, {{WF_MU, 't'}});
-        bc_moist();
-      }
-      snprintf(tag, sizeof tag, "s%d.moist", rk);
-      phase(tag);
+    n += launch_prep(g, s, st);
+    bc({{WF_RU, 'u'}, {WF_RV, 'v'}, {WF_RW, 'w'}, {WF_WW, 'w'}, {WF_PHP, 'w'}, {WF_ALT, 't'}, {WF_P, 'p'},
+        {WF_AL, 'p'}, {WF_PH, 'w'}},
+       {{WF_MUU, 'u'}, {WF_MUV, 'v'}, {WF_MUT, 't'}});
+    snprintf(tag, sizeof tag, "s%d.prep", rk);
+    phase(tag);
+  }
+  // first stage: physics tendencies start from zero; diffusion metrics and
+  // eddy viscosities (solver.py:880-985)
+  void diff_stage1() {
+    if (rc != WRF_OK) return;
+    zero3(WF_RU_TENDF); zero3(WF_RV_TENDF); zero3(WF_RW_TENDF); zero3(WF_PH_TENDF); zero3(WF_T_TENDF);
+    zero2(WF_MU_TENDF);
+    zero4(WF_MOIST_TEND);
+    n += launch_diff_metrics(g, s, st);
+    bc({{WF_RDZW, 'w'}, {WF_ZX, 'e'}, {WF_ZY, 'f'}});
+    n += launch_km(g, s, st);
+    bc({{WF_XKMH, 't'}, {WF_XKHH, 't'}});
+    phase("s1.km");
+  }
+  // large-step tendencies: advection and forces, first-stage diffusion and
+  // relaxation, rk_addtend_dry (solver.py:987-1256)
+  void tend_stage(int rk) {
+    if (rc != WRF_OK) return;
+    char tag[32];
+    zero3(WF_RU_TEND); zero3(WF_RV_TEND); zero3(WF_RW_TEND); zero3(WF_T_TEND); zero3(WF_PH_TEND);
+    zero3(WF_U_SAVE); zero3(WF_V_SAVE); zero3(WF_W_SAVE); zero3(WF_PH_SAVE); zero3(WF_T_SAVE);
+    zero2(WF_MU_TEND); zero2(WF_MU_SAVE);
+    n += launch_advect_forces(g, s, st);
+    snprintf(tag, sizeof tag, "s%d.forces", rk);
+    phase(tag);
+    if (rk == 1) {
+      n += launch_hdiff_relax(g, s, st);
+      phase("s1.diff");
     }
-    // microphysics (solver.py:1714-1766), or its learned stand-in
+    n += launch_addtend(g, s, rk, st);
+    snprintf(tag, sizeof tag, "s%d.tend", rk);
+    phase(tag);
+  }
+  // acoustic set-up (solver.py:1258-1345)
+  void acoustic_prep(int rk) {
+    if (rc != WRF_OK) return;
+    char tag[32];
+    float dt_rk, dts_rk;
+    int nsub;
+    stage(rk, dt_rk, dts_rk, nsub);
+    n += launch_small_step_prep(g, s, rk, dts_rk, st);
+    bc({{WF_RU_TEND, 'u'}, {WF_RV_TEND, 'v'}, {WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}, {WF_T_1, 't'},
+        {WF_T_SAVE, 't'}},
+       {{WF_MU_1, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
+    snprintf(tag, sizeof tag, "s%d.acprep", rk);
+    phase(tag);
+  }
+  // one acoustic substep: advance_uv, then the column update (mu/theta,
+  // w/phi, sumflux, p/al), then zero_grad_bdy(w) and the halo copies
+  // (solver.py:1350-1492)
+  void acoustic_substep(int rk, int it) {
+    if (rc != WRF_OK) return;
+    char tag[32];
+    float dt_rk, dts_rk;
+    int nsub;
+    stage(rk, dt_rk, dts_rk, nsub);
+    n += launch_advance_uv(g, s, dts_rk, st);
+    snprintf(tag, sizeof tag, "s%d.sub%d.uv", rk, it);
+    phase(tag);
+    n += launch_acoustic_col(g, s, dts_rk, it, nsub, st);
+    snprintf(tag, sizeof tag, "s%d.sub%d.col", rk, it);
+    phase(tag);
+    n += launch_zero_grad_w(g, s, st);
+    bc({{WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}}, {{WF_MUTS, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
+    snprintf(tag, sizeof tag, "s%d.sub%d", rk, it);
+    phase(tag);
+  }
+  // small_step_finish (solver.py:1494-1546)
+  void acoustic_finish(int rk) {
+    if (rc != WRF_OK) return;
+    char tag[32];
+    float dt_rk, dts_rk;
+    int nsub;
+    stage(rk, dt_rk, dts_rk, nsub);
+    n += launch_small_step_finish(g, s, dts_rk, nsub, rk, st);
+    if (rk == 3) bc({{WF_RU_M, 'u'}, {WF_RV_M, 'v'}, {WF_WW_M, 'w'}}, {{WF_MUT, 't'}, {WF_MUTS, 't'}});
+    snprintf(tag, sizeof tag, "s%d.acfinish", rk);
+    phase(tag);
+  }
+  // moisture transport and the stage's halo copies (solver.py:1548-1710)
+  void moist_stage(int rk) {
+    if (rc != WRF_OK) return;
+    char tag[32];
+    float dt_rk, dts_rk;
+    int nsub;
+    stage(rk, dt_rk, dts_rk, nsub);
+    n += launch_advect_moist(g, s, st);
+    if (rk == 1) {
+      n += launch_hdiff_moist(g, s, st);
+      n += launch_relax_qv(g, s, st);
+    }
+    n += launch_moist(g, s, rk, dt_rk, st);
+    if (rk < 3) {
+      bc({{WF_U, 'U'}, {WF_V, 'V'}, {WF_W, 'w'}, {WF_T, 'p'}, {WF_PH, 'w'}}, {{WF_MU, 't'}});
+      bc_moist();
+    }
+    snprintf(tag, sizeof tag, "s%d.moist", rk);
+    phase(tag);
+  }
+  // microphysics (solver.py:1714-1766), or its learned stand-in
+  void microphysics() {
+    if (rc != WRF_OK) return;
     if (net) {
       const char* err = nullptr;
       const int r = launch_physics_mlp(g, s, *net, *work, st, &err);
@@ -235,7 +275,10 @@ struct Driver {
       n += launch_physics(g, s, st);
     }
     phase("mp");
-    // end-of-step boundaries (solver.py:1776-1910)
+  }
+  // end-of-step boundaries and the step counter (solver.py:1776-1910)
+  void step_end() {
+    if (rc != WRF_OK) return;
     bc({{WF_U_1, 'U'}, {WF_U, 'U'}, {WF_V_1, 'V'}, {WF_V, 'V'}, {WF_W_1, 'w'}, {WF_W, 'w'}, {WF_T_1, 'p'},
         {WF_T, 'p'}, {WF_PH_1, 'w'}, {WF_PH, 'w'}},
        {{WF_MU_1, 't'}, {WF_MU, 't'}});
@@ -244,6 +287,24 @@ struct Driver {
     k_step_end<<<1, 1, 0, st>>>(reinterpret_cast<int*>(s[WF_STATUS]));
     ++n;
     phase("end");
+  }
+
+  void run() {
+    step_begin();
+    for (int rk = 1; rk <= 3; ++rk) {
+      float dt_rk, dts_rk;
+      int nsub;
+      stage(rk, dt_rk, dts_rk, nsub);
+      rk_prep(rk);
+      if (rk == 1) diff_stage1();
+      tend_stage(rk);
+      acoustic_prep(rk);
+      for (int it = 1; it <= nsub; ++it) acoustic_substep(rk, it);
+      acoustic_finish(rk);
+      moist_stage(rk);
+    }
+    microphysics();
+    step_end();
   }
   int bdy_interval = 360;
 };
@@ -285,6 +346,69 @@ int wrf_rk3_step(const WrfGrid* gin, const WrfState* sin, void* stream, wrf_prob
   d.run();
   g_last_launches = d.n;
   return d.rc;
+}
+
+}  // extern "C"
+
+namespace {
+// one phase of the step on a fresh driver (no probe)
+template <typename F>
+int run_phase(const WrfGrid* gin, const WrfState* sin, void* stream, int rk, int it, F body) {
+  Driver d;
+  int rc = make_grid(gin, d.g);
+  if (rc) return rc;
+  rc = make_state(sin, d.s);
+  if (rc) return rc;
+  if (rk != 0) {
+    if (rk < 1 || rk > 3) return fail(WRF_EINVAL, "rk_step must be 1, 2 or 3");
+    float dt_rk, dts_rk;
+    int nsub;
+    d.stage(rk, dt_rk, dts_rk, nsub);
+    if (it != 0 && (it < 1 || it > nsub)) return fail(WRF_EINVAL, "acoustic iteration outside 1 .. substeps of the stage");
+  }
+  d.st = static_cast<cudaStream_t>(stream);
+  d.probe = nullptr;
+  d.user = nullptr;
+  d.bdy_interval = gin->bdy_interval;
+  cudaGetLastError();
+  body(d);
+  g_last_launches = d.n;
+  return d.rc;
+}
+}  // namespace
+
+extern "C" {
+
+int wrf_step_begin(const WrfGrid* g, const WrfState* s, void* stream) {
+  return run_phase(g, s, stream, 0, 0, [](Driver& d) { d.step_begin(); });
+}
+int wrf_rk_prep(const WrfGrid* g, const WrfState* s, int rk_step, void* stream) {
+  return run_phase(g, s, stream, rk_step, 0, [&](Driver& d) { d.rk_prep(rk_step); });
+}
+int wrf_diff_stage1(const WrfGrid* g, const WrfState* s, void* stream) {
+  return run_phase(g, s, stream, 0, 0, [](Driver& d) { d.diff_stage1(); });
+}
+int wrf_tend_stage(const WrfGrid* g, const WrfState* s, int rk_step, void* stream) {
+  return run_phase(g, s, stream, rk_step, 0, [&](Driver& d) { d.tend_stage(rk_step); });
+}
+int wrf_acoustic_prep(const WrfGrid* g, const WrfState* s, int rk_step, void* stream) {
+  return run_phase(g, s, stream, rk_step, 0, [&](Driver& d) { d.acoustic_prep(rk_step); });
+}
+int wrf_acoustic_substep(const WrfGrid* g, const WrfState* s, int rk_step, int iteration, void* stream) {
+  if (iteration < 1) return fail(WRF_EINVAL, "acoustic iteration outside 1 .. substeps of the stage");
+  return run_phase(g, s, stream, rk_step, iteration, [&](Driver& d) { d.acoustic_substep(rk_step, iteration); });
+}
+int wrf_acoustic_finish(const WrfGrid* g, const WrfState* s, int rk_step, void* stream) {
+  return run_phase(g, s, stream, rk_step, 0, [&](Driver& d) { d.acoustic_finish(rk_step); });
+}
+int wrf_moist_stage(const WrfGrid* g, const WrfState* s, int rk_step, void* stream) {
+  return run_phase(g, s, stream, rk_step, 0, [&](Driver& d) { d.moist_stage(rk_step); });
+}
+int wrf_microphysics(const WrfGrid* g, const WrfState* s, void* stream) {
+  return run_phase(g, s, stream, 0, 0, [](Driver& d) { d.microphysics(); });
+}
+int wrf_step_end(const WrfGrid* g, const WrfState* s, void* stream) {
+  return run_phase(g, s, stream, 0, 0, [](Driver& d) { d.step_end(); });
 }
 
 int wrf_advect_scalar(const WrfGrid* gin, const float* field, float* tend, const float* ru, const float* rv,

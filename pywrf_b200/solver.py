@@ -51,6 +51,29 @@ class Integrator:
             rc = self.lib.wrf_rk3_step(ctypes.byref(self.state.cgrid), self.state.ptr, _stream_handle(stream), cb, None)
         N.check(rc, "wrf_rk3_step")
 
+    def step_phases(self, stream: torch.cuda.Stream | None = None) -> None:
+        """One time step through the phase entry points (``wrf_step_begin`` ..
+        ``wrf_step_end``), in the order of the reference's RK3 loop
+        (pywrf/solver.py:709-1910); enqueues the same kernels as :meth:`step`."""
+        L, g, sp = self.lib, ctypes.byref(self.state.cgrid), self.state.ptr
+        with torch.cuda.device(self.state.device):
+            h = _stream_handle(stream)
+            N.check(L.wrf_step_begin(g, sp, h), "wrf_step_begin")
+            soundsteps = self.state.cgrid.soundsteps
+            for rk in (1, 2, 3):
+                N.check(L.wrf_rk_prep(g, sp, rk, h), "wrf_rk_prep")
+                if rk == 1:
+                    N.check(L.wrf_diff_stage1(g, sp, h), "wrf_diff_stage1")
+                N.check(L.wrf_tend_stage(g, sp, rk, h), "wrf_tend_stage")
+                N.check(L.wrf_acoustic_prep(g, sp, rk, h), "wrf_acoustic_prep")
+                nsub = 1 if rk == 1 else (soundsteps // 2 if rk == 2 else soundsteps)
+                for it in range(1, nsub + 1):
+                    N.check(L.wrf_acoustic_substep(g, sp, rk, it, h), "wrf_acoustic_substep")
+                N.check(L.wrf_acoustic_finish(g, sp, rk, h), "wrf_acoustic_finish")
+                N.check(L.wrf_moist_stage(g, sp, rk, h), "wrf_moist_stage")
+            N.check(L.wrf_microphysics(g, sp, h), "wrf_microphysics")
+            N.check(L.wrf_step_end(g, sp, h), "wrf_step_end")
+
     def capture(self) -> None:
         """Record one step into a CUDA graph (the step number lives on the
         device, so the same graph serves every step)."""

@@ -1,4 +1,5 @@
-"""Drop-in for ``pywrf.wrf_dynamics.advect_scalar`` (reference signature).
+"""Drop-ins for ``pywrf.wrf_dynamics.advect_scalar`` and ``calc_coef_w``
+(reference signatures).
 
 ``advect_scalar(...)`` takes the arguments of the reference function
 (pywrf/wrf_dynamics.py:1841-1850), adds the flux-form advection of ``field``
@@ -51,3 +52,28 @@ def advect_scalar(field, field_old, tendency, ru, rv, rom, c1, c2, mut, time_ste
                                        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     N.check(rc, "wrf_advect_scalar")
     return tendency
+
+
+def calc_coef_w(a, alpha, gamma, mut, c1h, c2h, c1f, c2f, c3h, c4h, c3f, c4f, cqw, rdn, rdnw, c2a, dts, g, epssm,
+                top_lid, ids, ide, jds, jde, kds, kde, ims, ime, jms, jme, kms, kme, its, ite, jts, jte, kts, kte):
+    """calc_coef_w (pywrf/wrf_dynamics.py:3316-3388) on the GPU through
+    ``wrf_coef_w``: fills a, alpha, gamma on the mass columns and returns
+    them.  The c1h..c4f arguments are accepted and unused, as in the
+    reference; g must be the solver's 9.81."""
+    nz, ny, nx = cqw.shape
+    if (ids, jds, ide, jde) != (5, 5, nx - 5, ny - 5) or (its, ite, jts, jte) != (ids, ide, jds, jde) \
+            or (kts, kte) != (0, nz):
+        raise NotImplementedError("calc_coef_w: only the solver's 5-cell frame with tile = domain is supported")
+    if abs(float(g) - 9.81) > 1e-6:
+        raise ValueError("calc_coef_w: the kernels use the solver's g = 9.81")
+    gr = Grid.make(nx, ny, nz, 9000.0, 9000.0, 1.0)
+    cg = make_cgrid(gr, {"cf1": 0.0, "cf2": 0.0, "cf3": 0.0, "cfn": 0.0, "cfn1": 0.0})
+    cg.epssm = float(epssm)
+    cg.top_lid = int(bool(top_lid))
+    with torch.cuda.device(cqw.device):
+        rc = N.lib().wrf_coef_w(ctypes.byref(cg), _need("mut", mut), _need("cqw", cqw), _need("c2a", c2a),
+                                _need("rdn", rdn), _need("rdnw", rdnw), float(dts), _need("a", a),
+                                _need("alpha", alpha), _need("gamma", gamma),
+                                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    N.check(rc, "wrf_coef_w")
+    return a, alpha, gamma

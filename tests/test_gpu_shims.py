@@ -102,3 +102,47 @@ def test_advect_scalar_shim_with_the_solver_arguments(stepped):
     assert out is tend
     err, floor = rel_l2(tend.cpu().numpy(), ref64), rel_l2(ref32, ref64)
     assert err <= 3.0 * floor + 1e-9, (err, floor)
+
+
+def _cuda(a):
+    return torch.tensor(np.asarray(a), dtype=torch.float32, device="cuda").contiguous()
+
+
+def test_calc_coef_w_shim_against_the_reference():
+    """The reference-signature calc_coef_w against the reference's own
+    coefficients (tests/golden/coefw_adj_ref64.npz, float64)."""
+    from helpers import load_npz
+    W = load_npz("coefw_adj_ref64.npz")
+    nz, n = W["cqw"].shape[0], W["cqw"].shape[1]
+    a, al, ga = (torch.zeros(nz, n, n, device="cuda") for _ in range(3))
+    one = torch.ones(nz, device="cuda")
+    idx = (5, n - 5, 5, n - 5, 0, nz, 0, n, 0, n, 0, nz, 5, n - 5, 5, n - 5, 0, nz)
+    out = wrf_dynamics.calc_coef_w(a, al, ga, _cuda(W["mut"]), one, one, one, one, one, one, one, one, _cuda(W["cqw"]),
+                                   _cuda(W["rdn"]), _cuda(W["rdnw"]), _cuda(W["c2a"]), float(W["dts"]), 9.81,
+                                   float(W["epssm"]), False, *idx)
+    torch.cuda.synchronize()
+    assert out[0] is a and out[1] is al and out[2] is ga
+    for mine, ref in ((a, W["a"]), (al, W["alpha"]), (ga, W["gamma"])):
+        assert rel_l2(mine.cpu().numpy(), ref) < 1e-5
+
+
+@pytest.mark.parametrize("var", ["t", "u", "v", "h"])
+def test_relax_bdytend_shim_against_the_reference(var):
+    """The reference-signature relax_bdytend against the reference's own
+    tendency (tests/golden/relax_adj_ref64.npz, float64)."""
+    from helpers import load_npz
+    from pywrf_b200 import wrf_boundary
+    Z = load_npz("relax_adj_ref64.npz")
+    field = _cuda(Z[f"{var}_field"])
+    tend = _cuda(Z[f"{var}_tend0"])
+    nz, n = field.shape[0], field.shape[1]
+    bdy = [_cuda(Z[f"{var}_{k}"]) for k in ("xs", "xe", "ys", "ye", "txs", "txe", "tys", "tye")]
+    idx = (5, n - 5, 5, n - 5, 0, nz, 0, n, 0, n, 0, nz, 0, n, 0, n, 0, nz, 5, n - 5, 5, n - 5, 0, nz)
+    out = wrf_boundary.relax_bdytend(field, tend, *bdy, var, 5, 1, 4, float(Z["dtbc"]), wrf_boundary.FCX,
+                                     wrf_boundary.GCX, *idx)
+    torch.cuda.synchronize()
+    assert out is tend
+    assert rel_l2(tend.cpu().numpy(), Z[f"{var}_tend"]) < 1e-6
+    with pytest.raises(ValueError):
+        wrf_boundary.relax_bdytend(field, tend, *bdy, var, 5, 1, 4, 1.0, [0.0, 1.0, 2.0, 3.0, 0.0],
+                                   wrf_boundary.GCX, *idx)
