@@ -43,6 +43,7 @@ extern "C" {
 /* status words (WF_STATUS) */
 #define WRF_ST_NAN_P 0        /* NaN points met in the diagnosed p (summed over RK stages) */
 #define WRF_ST_STEP 1         /* completed steps (device step counter) */
+#define WRF_ST_WAIT 2         /* thread blocks whose bounded wait on a tile load ran out (tiled advection) */
 
 /* the persistent state of one integration, in table order */
 #define WRF_FIELD_TABLE(X) \

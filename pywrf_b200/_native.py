@@ -21,6 +21,7 @@ WRF_KSF, WRF_KSI = 20, 21
 
 WRF_ST_NAN_P = 0
 WRF_ST_STEP = 1
+WRF_ST_WAIT = 2
 
 
 class WrfGridC(ctypes.Structure):

@@ -27,6 +27,7 @@
 #include <mutex>
 #include "kernels.cuh"
 #include "tc_gemm.cuh"
+#include "tma.cuh"
 
 namespace wrf {
 namespace tc {
@@ -45,29 +46,10 @@ constexpr uint32_t kTmemCols = BN;                   // fp32 accumulator: 128 la
 constexpr size_t kSmemBytes = STAGES * kStageBytes + 1024 + 128;
 constexpr long long kWaitCycles = 4000000000LL;      // ~2 s at the boost clock
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
+using tma::mbar_expect_tx;
+using tma::mbar_init;
+using tma::mbar_try;
+using tma::smem_u32;
 
 // bounded wait for the phase of the given parity to complete
 __device__ __noinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
@@ -479,24 +461,8 @@ __global__ void __launch_bounds__(kPThreads, 1)
 }
 
 // ---------------------------------------------------------------- host side
-using EncodeTiled = decltype(&cuTensorMapEncodeTiled);
-
-EncodeTiled encoder(const char** err) {
-  static EncodeTiled fn = nullptr;
-  static std::mutex mu;
-  std::lock_guard<std::mutex> lock(mu);
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !p) {
-      *err = "cuTensorMapEncodeTiled is not available from the driver";
-      return nullptr;
-    }
-    fn = reinterpret_cast<EncodeTiled>(p);
-  }
-  return fn;
-}
+using tma::EncodeTiled;
+using tma::encoder;
 
 // 2-D bf16 row-major [rows][cols] operand, 128 x 64 boxes, 128-byte swizzle;
 // rows past the end read as zeros

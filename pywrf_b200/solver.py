@@ -107,7 +107,7 @@ class Integrator:
             torch.cuda.current_stream().synchronize()
             rc = self.lib.wrf_status_read(self.state.ptr, _stream_handle(None), out)
         N.check(rc, "wrf_status_read")
-        return {"nan_p": out[N.WRF_ST_NAN_P], "step": out[N.WRF_ST_STEP]}
+        return {"nan_p": out[N.WRF_ST_NAN_P], "step": out[N.WRF_ST_STEP], "wait_timeouts": out[N.WRF_ST_WAIT]}
 
 
 class WrfSolver:

@@ -81,7 +81,7 @@ def test_small_two_steps_vs_reference_fp64(small):
         if not err <= K_FLOOR * floor + ABS_FLOOR:
             bad.append((k, err, floor))
     assert not bad, bad
-    assert it.status() == {"nan_p": 0, "step": SMALL["nsteps"]}
+    assert it.status() == {"nan_p": 0, "step": SMALL["nsteps"], "wait_timeouts": 0}
 
 
 def test_small_one_step_north_star_tolerance(small):
@@ -99,6 +99,28 @@ def test_small_one_step_north_star_tolerance(small):
         if floor < 3e-6:
             assert err < 1e-5, (k, err, floor)
         assert err <= K_FLOOR * floor + ABS_FLOOR, (k, err, floor)
+
+
+def test_rows_not_a_multiple_of_16_bytes_vs_oracle_fp64():
+    """nx = 30 (rows of 120 bytes, no tensor-map tiles): the tiled advection
+    takes its cp.async form; two steps match the fp64 oracle within the fp32
+    oracle's own error, field by field, as the tensor-map form does on the
+    other grids."""
+    spec = synthetic.CaseSpec(**{**SMALL, "n": 30, "seed": 11})
+    g = synthetic.grid_for(spec)
+    assert g.nx % 4 != 0
+    inputs, bdy = synthetic.build(spec)
+    st, it = cuda_run(g, inputs, bdy, 2)
+    out = cuda_fields(st)
+    o64 = oracle_fields(g, inputs, bdy, np.float64, 2)
+    o32 = oracle_fields(g, inputs, bdy, np.float32, 2)
+    bad = []
+    for k in out:
+        err, floor = rel_l2(out[k], o64[k]), rel_l2(o32[k], o64[k])
+        if not err <= K_FLOOR * floor + ABS_FLOOR:
+            bad.append((k, err, floor))
+    assert not bad, bad
+    assert it.status() == {"nan_p": 0, "step": 2, "wait_timeouts": 0}
 
 
 def test_config0_ten_steps_vs_oracle_fp64(config0):
