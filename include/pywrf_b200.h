@@ -168,6 +168,18 @@ int wrf_step_end(const WrfGrid* g, const WrfState* s, void* stream);
 int wrf_advect_scalar(const WrfGrid* g, const float* field, float* tend, const float* ru,
                       const float* rv, const float* rom, const float* msftx, const float* fzm,
                       const float* fzp, const float* rdzw, void* stream);
+/* wrf_dynamics.py:1112-1331 advect_u, 1332-1534 advect_v, 1535-1823
+ * advect_w: tend += the flux-form advection of one momentum component
+ * (component 0: field = u, msf = msfux; 1: field = v, msf = msfvy,
+ * msf2 = msfvx; 2: field = w, msf = msftx), with the coupled velocities ru,
+ * rv, rom, the profiles fzm, fzp and rdz (rdnw for u and v, rdn for w).
+ * form 0 runs the fastest kernel the arrays allow (the tiled tensor-map
+ * kernel when nx is a multiple of 4 and the arrays are 16-byte aligned),
+ * form 1 the one-thread-per-point kernel; both perform the reference's
+ * operations in the reference's order. */
+int wrf_advect_momentum(const WrfGrid* g, int component, const float* field, float* tend, const float* ru,
+                        const float* rv, const float* rom, const float* msf, const float* msf2, const float* fzm,
+                        const float* fzp, const float* rdz, int form, void* stream);
 /* Adjoint of wrf_advect_scalar (reverse mode): given the cotangent tend_bar of
  * the updated tendency, accumulates (+=) the cotangents of field, ru, rv and
  * rom.  The cotangent of the incoming tendency is tend_bar itself.  The

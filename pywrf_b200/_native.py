@@ -92,6 +92,8 @@ def lib() -> ctypes.CDLL:
     L.wrf_acoustic_substep.argtypes = [G0, vp, ip, ip, vp]
     L.wrf_advect_scalar.restype = ip
     L.wrf_advect_scalar.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 9 + [vp]
+    L.wrf_advect_momentum.restype = ip
+    L.wrf_advect_momentum.argtypes = [ctypes.POINTER(WrfGridC), ctypes.c_int] + [vp] * 10 + [ctypes.c_int, vp]
     L.wrf_advect_scalar_adj.restype = ip
     L.wrf_advect_scalar_adj.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 13 + [vp]
     L.wrf_relax_bdytend.restype = ip

@@ -61,13 +61,36 @@ __device__ __forceinline__ float xface(const Grid& g, const float* row /* row[x'
   return 0.f;
 }
 
+// The face f (between cells f-1 and f) of [lo, hi) from the six values
+// q[0..5] = q(f-3 .. f+2), the cases of xface / yface in their priority
+// order but without a branch: every lane forms the 5th-, 3rd- and 2nd-order
+// values and keeps its own, so a warp whose faces straddle a boundary does
+// not run the cases one after another.  The hi-3 face takes its upwind sign
+// from s3 (ru at ide-2 for x faces, r for y faces); the 2nd-order faces are
+// r2 * (q(f) + q(f-1)) (r2 = 0.5 r for a scalar).
+__device__ __forceinline__ float face_sel(const float* q, int stride, int f, int lo, int hi, float r, float s3,
+                                         float r2) {
+  const float q0 = q[0], q1 = q[stride], q2 = q[2 * stride], q3 = q[3 * stride], q4 = q[4 * stride],
+              q5 = q[5 * stride];
+  const float v5 = r * flux5(q0, q1, q2, q3, q4, q5, r);
+  const float v3 = r * flux3(q1, q2, q3, q4, (f == hi - 3 && f != lo + 2) ? s3 : r);
+  const float v2 = r2 * (q3 + q2);
+  float v = 0.f;  // lowest priority first
+  v = f == hi - 3 ? v3 : v;
+  v = f == hi - 2 ? v2 : v;
+  v = f == lo + 2 ? v3 : v;
+  v = f == lo + 1 ? v2 : v;
+  v = (f >= lo + 3 && f < hi - 3) ? v5 : v;
+  return v;
+}
+
 // vertical face kf from the column window w[0..6] = q(kc-3 .. kc+3), kf in {kc, kc+1}
 // (wrf_dynamics.py:1991-2015)
 __device__ __forceinline__ float zface(int ktf, const float* fnm, const float* fnp, const float* w, int kc, int kf, float r) {
   auto Q = [&](int kk) { return w[kk - kc + 3]; };
   if (kf >= 3 && kf < ktf - 2) return r * flux5(Q(kf - 3), Q(kf - 2), Q(kf - 1), Q(kf), Q(kf + 1), Q(kf + 2), -r);
-  if (kf == 1) return r * (__ldg(&fnm[1]) * Q(1) + __ldg(&fnp[1]) * Q(0));
-  if (kf == 2) return r * flux3(Q(0), Q(1), Q(2), Q(3), -r);
+  if (kf == 1) return r * (__ldg(&fnm[1]) * Q(kf) + __ldg(&fnp[1]) * Q(kf - 1));
+  if (kf == 2) return r * flux3(Q(kf - 2), Q(kf - 1), Q(kf), Q(kf + 1), -r);
   if (kf == ktf - 2) return r * flux3(Q(kf - 2), Q(kf - 1), Q(kf), Q(kf + 1), -r);
   if (kf == ktf - 1) return r * (__ldg(&fnm[kf]) * Q(kf) + __ldg(&fnp[kf]) * Q(kf - 1));
   return 0.f;
@@ -302,14 +325,12 @@ __global__ void __launch_bounds__(kTTX * kTTY, WRF_ADV_MINB) k_advect_tma(Grid g
     if (ACCUM) tma::prefetch_map(&a.tend);
   }
   __syncthreads();
-  auto issue_q = [&](int k) {
-    const int r = (k - k0) % kTRing;
+  auto issue_q = [&](int k, int r) {
     tma::mbar_expect_tx(&sm.qbar[r], NSP * kQBytes);
 #pragma unroll
     for (int m = 0; m < NSP; ++m) tma::load_4d(sm.q[r][m], &a.q, qx, j0 - 3, k, qw + m, &sm.qbar[r]);
   };
-  auto issue_a = [&](int k) {
-    const int r = (k - k0) % kARing;
+  auto issue_a = [&](int k, int r) {
     tma::mbar_expect_tx(&sm.abar[r], NA * kABytes);
     tma::load_4d(sm.aux[r][0], &a.ru, ax, j0, k, 0, &sm.abar[r]);
     tma::load_4d(sm.aux[r][1], &a.rv, ax, j0, k, 0, &sm.abar[r]);
@@ -322,8 +343,8 @@ __global__ void __launch_bounds__(kTTX * kTTY, WRF_ADV_MINB) k_advect_tma(Grid g
   // levels issued so far (thread 0's record, for the bounded drain on abort)
   int q_hi = k0 - 1, a_hi = k0 - 1;
   if (tid == 0) {
-    for (int k = k0; k < min(k0 + kTRing - 1, k1); ++k) issue_q(k);
-    for (int k = k0; k < min(k0 + kARing - 1, k1); ++k) issue_a(k);
+    for (int k = k0; k < min(k0 + kTRing - 1, k1); ++k) issue_q(k, k - k0);
+    for (int k = k0; k < min(k0 + kARing - 1, k1); ++k) issue_a(k, k - k0);
     q_hi = min(k0 + kTRing - 1, k1) - 1;
     a_hi = min(k0 + kARing - 1, k1) - 1;
   }
@@ -348,14 +369,28 @@ __global__ void __launch_bounds__(kTTX * kTTY, WRF_ADV_MINB) k_advect_tma(Grid g
     fbot[m] = zface(ktf, fnm, fnp, win[m], k0, k0, rbot);
   }
   int kstop = k1;  // the level at which a bounded wait ran out (k1: none did)
+  // ring slots and phase parities of levels k and k+3 (scalars) and k (the rest)
+  int qs = 0, q3s = 3 % kTRing, as = 0;
+  uint32_t qp = 0, q3p = 3 / kTRing, ap = 0;
+  auto next = [](int& slot, uint32_t& par, int ring) {
+    if (++slot == ring) {
+      slot = 0;
+      par ^= 1u;
+    }
+  };
+  // this thread's offsets in a scalar tile and in a per-level box
+  const int offX = (ty + 3) * kQW + oq + tx;  // x face: q(i-3) of row j
+  const int offY = ty * kQW + oq + 3 + tx;    // y face: q(j-3) of column i
+  const int offC = offX + 3;                  // the cell itself
+  const int offA = ty * kAW + oa + tx;
+  float* tb[NSP];
+#pragma unroll
+  for (int m = 0; m < NSP; ++m) tb[m] = a.tout[grp * NSP + m] + (size_t)k0 * lev + c;
   for (int k = k0; k < k1; ++k) {
-    const int it = k - k0;
     const float rdk = __ldg(&rdnw[k]);
-    bool ok = tma::mbar_wait_bounded(&sm.qbar[it % kTRing], (it / kTRing) & 1, kAdvWaitCycles);
-    ok = ok && tma::mbar_wait_bounded(&sm.abar[it % kARing], (it / kARing) & 1, kAdvWaitCycles);
-    if (k + 3 < k1)
-      ok = ok && tma::mbar_wait_bounded(&sm.qbar[(it + 3) % kTRing], ((it + 3) / kTRing) & 1,
-                                        kAdvWaitCycles);
+    bool ok = tma::mbar_wait_bounded(&sm.qbar[qs], qp, kAdvWaitCycles);
+    ok = ok && tma::mbar_wait_bounded(&sm.abar[as], ap, kAdvWaitCycles);
+    if (k + 3 < k1) ok = ok && tma::mbar_wait_bounded(&sm.qbar[q3s], q3p, kAdvWaitCycles);
     if (__syncthreads_or(!ok)) {
       kstop = k;
       break;
@@ -363,36 +398,35 @@ __global__ void __launch_bounds__(kTTX * kTTY, WRF_ADV_MINB) k_advect_tma(Grid g
     // every thread is past level k-1: its ring slots take levels k+kTRing-1 / k+kARing-1
     if (tid == 0) {
       if (k + kTRing - 1 < k1) {
-        issue_q(k + kTRing - 1);
+        issue_q(k + kTRing - 1, qs == 0 ? kTRing - 1 : qs - 1);
         q_hi = k + kTRing - 1;
       }
       if (k + kARing - 1 < k1) {
-        issue_a(k + kARing - 1);
+        issue_a(k + kARing - 1, as == 0 ? kARing - 1 : as - 1);
         a_hi = k + kARing - 1;
       }
     }
-    const float* A = sm.aux[it % kARing][0];
+    const float* A = sm.aux[as][0];
+    const float* T0 = sm.q[qs][0];
     if (k < ktf) {
+      const float rl = A[offA];
+      const float rb = A[kASlot + offA];
+      const float rs3 = rs3in ? A[ty * kAW + rs3x] : 0.f;
 #pragma unroll
       for (int m = 0; m < NSP; ++m) {
-        const float* T = sm.q[it % kTRing][m];
+        const float* T = T0 + m * kQSlot;
         // x face i0 + tx of row ty; y face j0 + ty of column tx
-        const float* row = T + (ty + 3) * kQW + oq;
-        const float rl = A[ty * kAW + oa + tx];
-        const float rs3 = rs3in ? A[ty * kAW + rs3x] : 0.f;
         if (xin) {
-          const float* Q = row + tx;
+          const float* Q = T + offX;
           sm.fx[m][ty][tx] = rl * flux5(Q[0], Q[1], Q[2], Q[3], Q[4], Q[5], rl);
         } else {
-          sm.fx[m][ty][tx] = xface(g, row, i0, i, rl, rs3);
+          sm.fx[m][ty][tx] = face_sel(T + offX, 1, i, ids, ide, rl, rs3, 0.5f * rl);
         }
-        const float* col = T + tx + 3 + oq;
-        const float rb = A[kASlot + ty * kAW + oa + tx];
         if (yin) {
-          const float* Q = col + ty * kQW;
+          const float* Q = T + offY;
           sm.fy[m][ty][tx] = rb * flux5(Q[0], Q[kQW], Q[2 * kQW], Q[3 * kQW], Q[4 * kQW], Q[5 * kQW], rb);
         } else {
-          sm.fy[m][ty][tx] = yface<kQW>(g, col, j0, j, rb);
+          sm.fy[m][ty][tx] = yface<kQW>(g, T + tx + 3 + oq, j0, j, rb);
         }
         if (ty == 6 && tx < kTTY) {  // east faces i0 + 32, row tx
           const float* erow = T + (tx + 3) * kQW + oq;
@@ -402,11 +436,12 @@ __global__ void __launch_bounds__(kTTX * kTTY, WRF_ADV_MINB) k_advect_tma(Grid g
             const float* Q = erow + kTTX;
             sm.fx[m][tx][kTTX] = re * flux5(Q[0], Q[1], Q[2], Q[3], Q[4], Q[5], re);
           } else {
-            sm.fx[m][tx][kTTX] = xface(g, erow, i0, i0 + kTTX, re, rse);
+            sm.fx[m][tx][kTTX] = face_sel(erow + kTTX, 1, i0 + kTTX, ids, ide, re, rse, 0.5f * re);
           }
         }
         if (ty == 7) {  // north faces j0 + 8, column tx
           const float rn = A[kASlot + kTTY * kAW + oa + tx];
+          const float* col = T + tx + 3 + oq;
           if (yin) {
             const float* Q = col + kTTY * kQW;
             sm.fy[m][kTTY][tx] = rn * flux5(Q[0], Q[kQW], Q[2 * kQW], Q[3 * kQW], Q[4 * kQW], Q[5 * kQW], rn);
@@ -417,32 +452,36 @@ __global__ void __launch_bounds__(kTTX * kTTY, WRF_ADV_MINB) k_advect_tma(Grid g
       }
     }
     __syncthreads();
-    const float rtop = A[2 * kASlot + ty * kAW + oa + tx];
+    const float rtop = A[2 * kASlot + offA];
+    const float* T3 = sm.q[q3s][0];
 #pragma unroll
     for (int m = 0; m < NSP; ++m) {
       // q(k+3): from the ring inside the chunk, else the direct loads
       if (k + 3 < k1) {
-        win[m][6] = sm.q[(it + 3) % kTRing][m][(ty + 3) * kQW + oq + 3 + tx];
+        win[m][6] = T3[m * kQSlot + offC];
       } else {
         win[m][6] = wtop[m][0];
         wtop[m][0] = wtop[m][1];
         wtop[m][1] = wtop[m][2];
       }
       const float ftop = zface(ktf, fnm, fnp, win[m], k, k + 1, rtop);
-      float* tout = a.tout[grp * NSP + m] + (size_t)k * lev + c;
       if (cell && k < ktf) {
-        float t = ACCUM ? A[(3 + m) * kASlot + ty * kAW + oa + tx] : 0.f;
+        float t = ACCUM ? A[(3 + m) * kASlot + offA] : 0.f;
         if (doy) t = t - cy * (sm.fy[m][ty + 1][tx] - sm.fy[m][ty][tx]);
         if (dox) t = t - cx * (sm.fx[m][ty][tx + 1] - sm.fx[m][ty][tx]);
         t = t - rdk * (ftop - fbot[m]);
-        *tout = t;
+        *tb[m] = t;
       } else if (!ACCUM && zreg) {
-        *tout = 0.f;
+        *tb[m] = 0.f;
       }
+      tb[m] += lev;
       fbot[m] = ftop;
 #pragma unroll
       for (int d = 0; d < 6; ++d) win[m][d] = win[m][d + 1];
     }
+    next(qs, qp, kTRing);
+    next(q3s, q3p, kTRing);
+    next(as, ap, kARing);
   }
   if (kstop < k1 && tid == 0) {
     // let the copies still in flight land before the block's shared memory
@@ -451,8 +490,375 @@ __global__ void __launch_bounds__(kTTX * kTTY, WRF_ADV_MINB) k_advect_tma(Grid g
       tma::mbar_wait_bounded(&sm.qbar[(k - k0) % kTRing], ((k - k0) / kTRing) & 1, kAdvWaitCycles);
     for (int k = kstop; k <= a_hi; ++k)
       tma::mbar_wait_bounded(&sm.abar[(k - k0) % kARing], ((k - k0) / kARing) & 1, kAdvWaitCycles);
-    atomicAdd(reinterpret_cast<int*>(s[WF_STATUS]) + WRF_ST_WAIT, 1);
+    if (s[WF_STATUS]) atomicAdd(reinterpret_cast<int*>(s[WF_STATUS]) + WRF_ST_WAIT, 1);
   }
+}
+
+// ------------------------------------------------------------------------
+// Momentum advection, TMA form: advect_u, advect_v, advect_w
+// (wrf_dynamics.py:1112-1823) on the same plan as the scalar kernel above -
+// one launch, blockIdx.z = component * chunks + chunk; a 32 x 8 tile of the
+// component's cells per block, its field tile (box 44 x 14) and the level's
+// coupled velocities and tendency (boxes 40 x 10 from x = floor4(i0 - 1),
+// y = j0 - 1, so that the i-1 and j-1 neighbours of every face are in the box)
+// streamed through mbarrier rings.  Face formulas and their order are those of
+// the point kernel (k_tend.cu: fqx_u .. vf_w); boundary blocks take the
+// branch-free select forms.
+
+// the face f of a momentum component normal to it (u in x, v in y) of
+// [lo, hi) from q[0..5] = q(f-3 .. f+2) and the coupled velocities ra, rb
+// either side (wrf_dynamics.py:1212-1246, 1373-1407): upwind 2nd order at
+// lo+1 and hi-1, 3rd order at lo+2 and hi-2, 5th order between
+__device__ __forceinline__ float face_normal(const float* q, int stride, int f, int lo, int hi, float ra, float rb) {
+  const float q0 = q[0], q1 = q[stride], q2 = q[2 * stride], q3 = q[3 * stride], q4 = q[4 * stride],
+              q5 = q[5 * stride];
+  const float vel = 0.5f * (ra + rb);
+  const float r4 = 0.25f * (ra + rb);
+  const float v5 = vel * flux5(q0, q1, q2, q3, q4, q5, vel);
+  const float v3 = vel * flux3(q1, q2, q3, q4, vel);
+  const float vl = r4 * (q3 + (q3 < 0.f ? q3 : q2));
+  const float vh = r4 * (q2 + (q2 > 0.f ? q2 : q3));
+  float v = 0.f;  // lowest priority first
+  v = f == hi - 2 ? v3 : v;
+  v = f == hi - 1 ? vh : v;
+  v = f == lo + 2 ? v3 : v;
+  v = f == lo + 1 ? vl : v;
+  v = (f >= lo + 3 && f < hi - 2) ? v5 : v;
+  return v;
+}
+
+// vertical face of v (vf_v, wrf_dynamics.py:1482-1524): zface with +vel on the ktf-2 face
+__device__ __forceinline__ float zface_v(int ktf, const float* fnm, const float* fnp, const float* w, int kc, int kf,
+                                         float r) {
+  auto Q = [&](int kk) { return w[kk - kc + 3]; };
+  if (kf >= 3 && kf < ktf - 2) return r * flux5(Q(kf - 3), Q(kf - 2), Q(kf - 1), Q(kf), Q(kf + 1), Q(kf + 2), -r);
+  if (kf == 1) return r * (__ldg(&fnm[1]) * Q(kf) + __ldg(&fnp[1]) * Q(kf - 1));
+  if (kf == 2) return r * flux3(Q(kf - 2), Q(kf - 1), Q(kf), Q(kf + 1), -r);
+  if (kf == ktf - 2) return r * flux3(Q(kf - 2), Q(kf - 1), Q(kf), Q(kf + 1), r);
+  if (kf == ktf - 1) return r * (__ldg(&fnm[kf]) * Q(kf) + __ldg(&fnp[kf]) * Q(kf - 1));
+  return 0.f;
+}
+
+// vertical face of w at mass level kf (vf_w, wrf_dynamics.py:1773-1811),
+// ra = rom(kf), rb = rom(kf-1)
+__device__ __forceinline__ float zface_w(int ktf, const float* w, int kc, int kf, float ra, float rb) {
+  auto W = [&](int kk) { return w[kk - kc + 3]; };
+  if (kf >= 3 && kf < ktf - 1) {
+    const float v = 0.5f * (ra + rb);
+    return v * flux5(W(kf - 3), W(kf - 2), W(kf - 1), W(kf), W(kf + 1), W(kf + 2), -v);
+  }
+  if (kf == 1) return 0.25f * (ra + rb) * (W(kf) + W(kf - 1));
+  if (kf == 2) {
+    const float v = 0.5f * (ra + rb);
+    return v * flux3(W(kf - 2), W(kf - 1), W(kf), W(kf + 1), -v);
+  }
+  if (kf == ktf - 1) {
+    const float v = 0.5f * (ra + rb);
+    return v * flux3(W(kf - 2), W(kf - 1), W(kf), W(kf + 1), v);
+  }
+  if (kf == ktf) return 0.25f * (ra + rb) * (W(kf) + W(kf - 1));
+  return 0.f;
+}
+
+constexpr int kMW = 40, kMH = kTTY + 2;        // per-level box of the momentum kernel
+constexpr uint32_t kMBytes = kMW * kMH * 4;
+constexpr int kMSlot = 416;                    // floats per box slot (1664 B)
+constexpr int kMomKCH = 10;
+static_assert(kMBytes <= kMSlot * 4 && (kMSlot * 4) % 128 == 0, "a ring slot holds one box");
+
+struct MomTmaArgs {
+  CUtensorMap q[3];               // u, v, w: box kQW x kQH
+  CUtensorMap ru, rv, rom;        // box kMW x kMH
+  CUtensorMap tend[3];            // ru_tend, rv_tend, rw_tend
+  const float* qg[3];
+  float* tout[3];
+  const float* romg;
+  int nchunk, comp0;  // blockIdx.z = (component - comp0) * nchunk + chunk
+};
+
+// per-level boxes: u, v: ru(k) rv(k) rom(k+1) tend(k); w: ru(k) ru(k-1) rv(k)
+// rv(k-1) rom(k+1) tend(k) (at the top level ru, rv of ktf-1 and ktf-2)
+template <int C>
+struct MomLayout {
+  static constexpr int NA = C == 2 ? 6 : 4;
+};
+constexpr int kMomSmemFloats = kTRing * kQSlot + kARing * 6 * kMSlot + kTTY * (kTTX + 1) + (kTTY + 1) * kTTX;
+
+template <int C>
+__device__ __forceinline__ void advect_mom_block(const Grid& g, const S& s, const MomTmaArgs& a, float* smf,
+                                                 uint64_t* qbar, uint64_t* abar, int chunk) {
+  constexpr int NA = MomLayout<C>::NA;
+  float* sq = smf;                                      // [kTRing][kQSlot]
+  float* saux = smf + kTRing * kQSlot;                  // [kARing][NA][kMSlot]
+  float (*fx)[kTTX + 1] = reinterpret_cast<float (*)[kTTX + 1]>(saux + kARing * 6 * kMSlot);
+  float (*fy)[kTTX] = reinterpret_cast<float (*)[kTTX]>(saux + kARing * 6 * kMSlot + kTTY * (kTTX + 1));
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTTX + tx;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, ktf = nz - 1;
+  const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde;
+  const int i0 = ids + blockIdx.x * kTTX, j0 = jds + blockIdx.y * kTTY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int qx = (i0 - 3) & ~3, mx = (i0 - 1) & ~3;
+  const int oq = i0 - 3 - qx, om = i0 - mx;  // om in 1..4
+  const size_t lev = (size_t)ny * nx;
+  // levels: u, v 0 .. ktf-1; w 1 .. ktf
+  const int kb = C == 2 ? 1 : 0, nlev = ktf;
+  const int k0 = kb + chunk * nlev / a.nchunk, k1 = kb + (chunk + 1) * nlev / a.nchunk;
+  bool cell, doy, dox;
+  float msf_y, msf_x, zfac = 0.f;
+  const int c = min(j, ny - 1) * nx + min(i, nx - 1);
+  if (C == 0) {
+    cell = j < jde - 1 && i >= ids + 1 && i < ide - 1;
+    doy = j >= jds + 1 && j < jde - 2;
+    dox = true;
+    const float m = cell ? __ldg(&s[WF_MSFUX][c]) : 0.f;
+    msf_y = m * g.rdy;
+    msf_x = m * g.rdx;
+  } else if (C == 1) {
+    cell = j >= jds + 1 && j < jde - 1 && i < ide - 1;
+    doy = true;
+    dox = i >= ids + 1 && i < ide - 2;
+    const float my = cell ? __ldg(&s[WF_MSFVY][c]) : 0.f;
+    const float mxv = cell ? __ldg(&s[WF_MSFVX][c]) : 1.f;
+    msf_y = my * g.rdy;
+    msf_x = my * g.rdx;
+    zfac = my / mxv;
+  } else {
+    cell = j < jde - 1 && i < ide - 1;
+    doy = j >= jds + 1 && j < jde - 2;
+    dox = i >= ids + 1 && i < ide - 2;
+    const float m = cell ? __ldg(&s[WF_MSFTX][c]) : 0.f;
+    msf_y = m * g.rdy;
+    msf_x = m * g.rdx;
+  }
+  // whole block in the 5th-order region of its faces (x faces i0 .. i0+32, y faces j0 .. j0+8)
+  const bool xin = C == 0 ? (i0 >= ids + 3 && i0 + kTTX < ide - 2) : (i0 >= ids + 3 && i0 + kTTX < ide - 3);
+  const bool yin = C == 1 ? (j0 >= jds + 3 && j0 + kTTY < jde - 2) : (j0 >= jds + 3 && j0 + kTTY < jde - 3);
+  const float* fnm = s[WF_FNM];
+  const float* fnp = s[WF_FNP];
+  const float* rdz = C == 2 ? s[WF_RDN] : s[WF_RDNW];
+
+  if (tid == 0) {
+    for (int r = 0; r < kTRing; ++r) tma::mbar_init(&qbar[r], 1);
+    for (int r = 0; r < kARing; ++r) tma::mbar_init(&abar[r], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tma::prefetch_map(&a.q[C]);
+    tma::prefetch_map(&a.ru);
+    tma::prefetch_map(&a.rv);
+    tma::prefetch_map(&a.rom);
+    tma::prefetch_map(&a.tend[C]);
+  }
+  __syncthreads();
+  auto issue_q = [&](int k, int r) {
+    tma::mbar_expect_tx(&qbar[r], kQBytes);
+    tma::load_4d(sq + r * kQSlot, &a.q[C], qx, j0 - 3, k, 0, &qbar[r]);
+  };
+  auto issue_a = [&](int k, int r) {
+    float* d = saux + r * NA * kMSlot;
+    tma::mbar_expect_tx(&abar[r], NA * kMBytes);
+    if (C == 2) {
+      const int kr = k < ktf ? k : ktf - 1;  // wvel's levels: k, k-1 (top: ktf-1, ktf-2)
+      tma::load_4d(d + 0 * kMSlot, &a.ru, mx, j0 - 1, kr, 0, &abar[r]);
+      tma::load_4d(d + 1 * kMSlot, &a.ru, mx, j0 - 1, kr - 1, 0, &abar[r]);
+      tma::load_4d(d + 2 * kMSlot, &a.rv, mx, j0 - 1, kr, 0, &abar[r]);
+      tma::load_4d(d + 3 * kMSlot, &a.rv, mx, j0 - 1, kr - 1, 0, &abar[r]);
+      tma::load_4d(d + 4 * kMSlot, &a.rom, mx, j0 - 1, k + 1, 0, &abar[r]);  // k + 1 == nz reads zeros
+      tma::load_4d(d + 5 * kMSlot, &a.tend[C], mx, j0 - 1, k, 0, &abar[r]);
+    } else {
+      tma::load_4d(d + 0 * kMSlot, &a.ru, mx, j0 - 1, k, 0, &abar[r]);
+      tma::load_4d(d + 1 * kMSlot, &a.rv, mx, j0 - 1, k, 0, &abar[r]);
+      tma::load_4d(d + 2 * kMSlot, &a.rom, mx, j0 - 1, k + 1, 0, &abar[r]);
+      tma::load_4d(d + 3 * kMSlot, &a.tend[C], mx, j0 - 1, k, 0, &abar[r]);
+    }
+  };
+  int q_hi = k0 - 1, a_hi = k0 - 1;
+  if (tid == 0) {
+    for (int k = k0; k < min(k0 + kTRing - 1, k1); ++k) issue_q(k, k - k0);
+    for (int k = k0; k < min(k0 + kARing - 1, k1); ++k) issue_a(k, k - k0);
+    q_hi = min(k0 + kTRing - 1, k1) - 1;
+    a_hi = min(k0 + kARing - 1, k1) - 1;
+  }
+  // column window of the component, its values above the chunk, the bottom-face flux
+  const float* qg = a.qg[C];
+  float win[7], wtop[3];
+#pragma unroll
+  for (int d = 0; d < 7; ++d) {
+    const int kk = k0 - 3 + d;
+    win[d] = (cell && kk >= 0 && kk < nz) ? __ldg(&qg[kk * lev + c]) : 0.f;
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int kk = k1 + d;
+    wtop[d] = (cell && kk < nz) ? __ldg(&qg[kk * lev + c]) : 0.f;
+  }
+  float fbot, rprev = 0.f;
+  {
+    const float* rom = a.romg;
+    if (C == 0) {
+      const float vel = cell ? 0.5f * (__ldg(&rom[k0 * lev + c]) + __ldg(&rom[k0 * lev + c - 1])) : 0.f;
+      fbot = zface(ktf, fnm, fnp, win, k0, k0, vel);
+    } else if (C == 1) {
+      const float vel = cell ? 0.5f * (__ldg(&rom[k0 * lev + c]) + __ldg(&rom[k0 * lev + c - nx])) : 0.f;
+      fbot = zface_v(ktf, fnm, fnp, win, k0, k0, vel);
+    } else {
+      rprev = cell ? __ldg(&rom[k0 * lev + c]) : 0.f;
+      const float rb = cell ? __ldg(&rom[(k0 - 1) * lev + c]) : 0.f;
+      fbot = zface_w(ktf, win, k0, k0, rprev, rb);
+    }
+  }
+  int kstop = k1;
+  int qs = 0, q3s = 3 % kTRing, as = 0;
+  uint32_t qp = 0, q3p = 3 / kTRing, ap = 0;
+  auto next = [](int& slot, uint32_t& par, int ring) {
+    if (++slot == ring) {
+      slot = 0;
+      par ^= 1u;
+    }
+  };
+  const int offX = (ty + 3) * kQW + oq + tx;  // x face f = i: q(f-3) of row j
+  const int offY = ty * kQW + oq + 3 + tx;    // y face jf = j: q(jf-3) of column i
+  const int offC = offX + 3;                  // the cell
+  const int oA = (ty + 1) * kMW + om + tx;    // (j, i) in a per-level box; -1: i-1, -kMW: j-1
+  float* tb = a.tout[C] + (size_t)k0 * lev + c;
+  for (int k = k0; k < k1; ++k) {
+    const float rdk = __ldg(&rdz[C == 2 && k == ktf ? ktf - 1 : k]);
+    bool ok = tma::mbar_wait_bounded(&qbar[qs], qp, kAdvWaitCycles);
+    ok = ok && tma::mbar_wait_bounded(&abar[as], ap, kAdvWaitCycles);
+    if (k + 3 < k1) ok = ok && tma::mbar_wait_bounded(&qbar[q3s], q3p, kAdvWaitCycles);
+    if (__syncthreads_or(!ok)) {
+      kstop = k;
+      break;
+    }
+    if (tid == 0) {
+      if (k + kTRing - 1 < k1) {
+        issue_q(k + kTRing - 1, qs == 0 ? kTRing - 1 : qs - 1);
+        q_hi = k + kTRing - 1;
+      }
+      if (k + kARing - 1 < k1) {
+        issue_a(k + kARing - 1, as == 0 ? kARing - 1 : as - 1);
+        a_hi = k + kARing - 1;
+      }
+    }
+    const float* A = saux + as * NA * kMSlot;
+    const float* T = sq + qs * kQSlot;
+    // w's interpolation of ru / rv to level k (top: extrapolated from ktf-1, ktf-2)
+    float c0 = 0.f, c1 = 0.f;
+    if (C == 2) {
+      if (k < ktf) {
+        c0 = __ldg(&fnm[k]);
+        c1 = __ldg(&fnp[k]);
+      } else {
+        c0 = 2.0f - __ldg(&fnm[ktf - 1]);
+        c1 = -__ldg(&fnp[ktf - 1]);
+      }
+    }
+    // the faces west / south of the cell, and the tile's east / north faces
+    auto xflux = [&](const float* Q, int f, int o) -> float {  // o: box index of (row, f)
+      if (C == 0) {
+        const float ra = A[o], rb = A[o - 1];
+        if (xin) {
+          const float vel = 0.5f * (ra + rb);
+          return vel * flux5(Q[0], Q[1], Q[2], Q[3], Q[4], Q[5], vel);
+        }
+        return face_normal(Q, 1, f, ids, ide, ra, rb);
+      } else if (C == 1) {
+        const float R = A[o] + A[o - kMW];
+        const float w = 0.5f * R;
+        if (xin) return w * flux5(Q[0], Q[1], Q[2], Q[3], Q[4], Q[5], w);
+        return face_sel(Q, 1, f, ids, ide, w, w, 0.25f * R);
+      } else {
+        const float vel = c0 * A[o] + c1 * A[kMSlot + o];
+        if (xin) return vel * flux5(Q[0], Q[1], Q[2], Q[3], Q[4], Q[5], vel);
+        return face_sel(Q, 1, f, ids, ide, vel, vel, 0.5f * vel);
+      }
+    };
+    auto yflux = [&](const float* Q, int f, int o) -> float {  // o: box index of (f, column)
+      if (C == 0) {
+        const float ra = A[kMSlot + o], rb = A[kMSlot + o - 1];
+        const float vel = 0.5f * (ra + rb);
+        if (yin) return vel * flux5(Q[0], Q[kQW], Q[2 * kQW], Q[3 * kQW], Q[4 * kQW], Q[5 * kQW], vel);
+        return face_sel(Q, kQW, f, jds, jde, vel, 0.0f, 0.25f * (ra + rb));
+      } else if (C == 1) {
+        const float ra = A[kMSlot + o], rb = A[kMSlot + o - kMW];
+        if (yin) {
+          const float vel = 0.5f * (ra + rb);
+          return vel * flux5(Q[0], Q[kQW], Q[2 * kQW], Q[3 * kQW], Q[4 * kQW], Q[5 * kQW], vel);
+        }
+        return face_normal(Q, kQW, f, jds, jde, ra, rb);
+      } else {
+        const float vel = c0 * A[2 * kMSlot + o] + c1 * A[3 * kMSlot + o];
+        if (yin) return vel * flux5(Q[0], Q[kQW], Q[2 * kQW], Q[3 * kQW], Q[4 * kQW], Q[5 * kQW], vel);
+        return face_sel(Q, kQW, f, jds, jde, vel, vel, 0.5f * vel);
+      }
+    };
+    const bool faces = C == 2 || k < ktf;
+    if (faces) {
+      fx[ty][tx] = xflux(T + offX, i, oA);
+      fy[ty][tx] = yflux(T + offY, j, oA);
+      if (ty == 6 && tx < kTTY)  // east faces i0 + 32, row tx
+        fx[tx][kTTX] = xflux(T + (tx + 3) * kQW + oq + kTTX, i0 + kTTX, (tx + 1) * kMW + om + kTTX);
+      if (ty == 7)  // north faces j0 + 8, column tx
+        fy[kTTY][tx] = yflux(T + kTTY * kQW + oq + 3 + tx, j0 + kTTY, (kTTY + 1) * kMW + om + tx);
+    }
+    __syncthreads();
+    // q(k+3): from the ring inside the chunk, else the direct loads
+    if (k + 3 < k1) {
+      win[6] = sq[q3s * kQSlot + offC];
+    } else {
+      win[6] = wtop[0];
+      wtop[0] = wtop[1];
+      wtop[1] = wtop[2];
+    }
+    float ftop = 0.f;
+    if (C == 0) {
+      ftop = zface(ktf, fnm, fnp, win, k, k + 1, 0.5f * (A[2 * kMSlot + oA] + A[2 * kMSlot + oA - 1]));
+    } else if (C == 1) {
+      ftop = zface_v(ktf, fnm, fnp, win, k, k + 1, 0.5f * (A[2 * kMSlot + oA] + A[2 * kMSlot + oA - kMW]));
+    } else if (k < ktf) {
+      const float ra = A[4 * kMSlot + oA];
+      ftop = zface_w(ktf, win, k, k + 1, ra, rprev);
+      rprev = ra;
+    }
+    if (cell) {
+      float t = A[(NA - 1) * kMSlot + oA];
+      if (doy) t = t - msf_y * (fy[ty + 1][tx] - fy[ty][tx]);
+      if (dox) t = t - msf_x * (fx[ty][tx + 1] - fx[ty][tx]);
+      if (C == 1) {
+        t = t - (zfac * rdk) * (ftop - fbot);
+      } else if (C == 2 && k == ktf) {
+        t = t + 2.0f * rdk * fbot;
+      } else {
+        t = t - rdk * (ftop - fbot);
+      }
+      *tb = t;
+    }
+    tb += lev;
+    fbot = ftop;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) win[d] = win[d + 1];
+    next(qs, qp, kTRing);
+    next(q3s, q3p, kTRing);
+    next(as, ap, kARing);
+  }
+  if (kstop < k1 && tid == 0) {
+    for (int k = kstop; k <= q_hi; ++k)
+      tma::mbar_wait_bounded(&qbar[(k - k0) % kTRing], ((k - k0) / kTRing) & 1, kAdvWaitCycles);
+    for (int k = kstop; k <= a_hi; ++k)
+      tma::mbar_wait_bounded(&abar[(k - k0) % kARing], ((k - k0) / kARing) & 1, kAdvWaitCycles);
+    if (s[WF_STATUS]) atomicAdd(reinterpret_cast<int*>(s[WF_STATUS]) + WRF_ST_WAIT, 1);
+  }
+}
+
+__global__ void __launch_bounds__(kTTX * kTTY, WRF_ADV_MINB) k_advect_mom_tma(Grid g, S s,
+                                                                             const __grid_constant__ MomTmaArgs a) {
+  __shared__ __align__(128) float smf[kMomSmemFloats];
+  __shared__ uint64_t qbar[kTRing], abar[kARing];
+  const int comp = a.comp0 + blockIdx.z / a.nchunk, chunk = blockIdx.z % a.nchunk;
+  if (comp == 0)
+    advect_mom_block<0>(g, s, a, smf, qbar, abar, chunk);
+  else if (comp == 1)
+    advect_mom_block<1>(g, s, a, smf, qbar, abar, chunk);
+  else
+    advect_mom_block<2>(g, s, a, smf, qbar, abar, chunk);
 }
 
 namespace {
@@ -473,6 +879,33 @@ bool aux_maps(AdvTmaArgs& a, const Grid& g, const float* ru, const float* rv, co
          tma::encode_f32_4d(&a.rom, rom, g.nx, g.ny, g.nz, 1, kAW, kAH, &err);
 }
 }  // namespace
+
+// advection of the momentum components comp0 .. comp0+ncomp-1 (0 u, 1 v,
+// 2 w) into ru_tend / rv_tend / rw_tend (TMA form); returns 0 (nothing
+// launched) when the arrays do not allow tensor maps
+int launch_advect_mom_tma(const Grid& g, const S& s, int comp0, int ncomp, cudaStream_t st) {
+  if (!tma_form(g) || g.nz < 4 || comp0 < 0 || ncomp < 1 || comp0 + ncomp > 3) return 0;
+  MomTmaArgs a{};
+  const char* err = nullptr;
+  const int f[3] = {WF_U, WF_V, WF_W}, t[3] = {WF_RU_TEND, WF_RV_TEND, WF_RW_TEND};
+  for (int m = comp0; m < comp0 + ncomp; ++m) {
+    if (!tma::encode_f32_4d(&a.q[m], s[f[m]], g.nx, g.ny, g.nz, 1, kQW, kQH, &err) ||
+        !tma::encode_f32_4d(&a.tend[m], s[t[m]], g.nx, g.ny, g.nz, 1, kMW, kMH, &err))
+      return 0;
+    a.qg[m] = s[f[m]];
+    a.tout[m] = s[t[m]];
+  }
+  if (!tma::encode_f32_4d(&a.ru, s[WF_RU], g.nx, g.ny, g.nz, 1, kMW, kMH, &err) ||
+      !tma::encode_f32_4d(&a.rv, s[WF_RV], g.nx, g.ny, g.nz, 1, kMW, kMH, &err) ||
+      !tma::encode_f32_4d(&a.rom, s[WF_WW], g.nx, g.ny, g.nz, 1, kMW, kMH, &err))
+    return 0;
+  a.romg = s[WF_WW];
+  a.nchunk = min((g.nz - 1 + kMomKCH - 1) / kMomKCH, g.nz - 1);
+  a.comp0 = comp0;
+  const dim3 gr((g.ide - g.ids + kTTX - 1) / kTTX, (g.jde - g.jds + kTTY - 1) / kTTY, ncomp * a.nchunk);
+  k_advect_mom_tma<<<gr, dim3(kTTX, kTTY), 0, st>>>(g, s, a);
+  return 1;
+}
 
 int launch_advect_moist_tiled(const Grid& g, const S& s, cudaStream_t st) {
   const size_t n3 = g.n3();

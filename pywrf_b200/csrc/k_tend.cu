@@ -1,5 +1,6 @@
 // Large-step (RK stage) tendencies.
-//   k_advect  advect_u, advect_v, advect_w (wrf_dynamics.py:1112-1823):
+//   k_advect  advect_u, advect_v, advect_w (wrf_dynamics.py:1112-1823) for rows
+//             that are not a multiple of 16 bytes (else k_advect_mom_tma):
 //             5th-order upwind-biased fluxes, 3rd/2nd order on the rows next
 //             to each boundary (theta and the moisture species: k_advect_tiled)
 //   k_forces  rhs_ph, horizontal_pressure_gradient, pg_buoy_w, coriolis,
@@ -236,7 +237,8 @@ __device__ __forceinline__ void advect_scalar_point(const Grid& g, const S& s, c
   tend[p] = t;
 }
 
-__global__ void k_advect(Grid g, S s) {
+// comps: bit 0 u, bit 1 v, bit 2 w
+__global__ void k_advect(Grid g, S s, int comps) {
   WRF_POINT_INDEX(g, k, j, i);
   const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde, ktf = g.nz - 1;
   const int c = g.i2(j, i);
@@ -246,7 +248,7 @@ __global__ void k_advect(Grid g, S s) {
   const float* ww = s[WF_WW];
   const float rdx = g.rdx, rdy = g.rdy;
   // u
-  if (k < ktf && j >= jds && j < jde - 1 && i >= ids + 1 && i < ide - 1) {
+  if ((comps & 1) && k < ktf && j >= jds && j < jde - 1 && i >= ids + 1 && i < ide - 1) {
     const float* u = s[WF_U];
     const float msfux = s[WF_MSFUX][c];
     float t = s[WF_RU_TEND][p];
@@ -256,7 +258,7 @@ __global__ void k_advect(Grid g, S s) {
     s[WF_RU_TEND][p] = t;
   }
   // v
-  if (k < ktf && j >= jds + 1 && j < jde - 1 && i >= ids && i < ide - 1) {
+  if ((comps & 2) && k < ktf && j >= jds + 1 && j < jde - 1 && i >= ids && i < ide - 1) {
     const float* v = s[WF_V];
     const float msfvy = s[WF_MSFVY][c];
     float t = s[WF_RV_TEND][p];
@@ -266,7 +268,7 @@ __global__ void k_advect(Grid g, S s) {
     s[WF_RV_TEND][p] = t;
   }
   // w (levels 1..ktf)
-  if (k >= 1 && j >= jds && j < jde - 1 && i >= ids && i < ide - 1) {
+  if ((comps & 4) && k >= 1 && j >= jds && j < jde - 1 && i >= ids && i < ide - 1) {
     const float* w = s[WF_W];
     const float msftx = s[WF_MSFTX][c];
     float t = s[WF_RW_TEND][p];
@@ -523,12 +525,19 @@ __global__ void k_advect_scalar(Grid g, S s, const float* q, float* tend, const 
   advect_scalar_point(g, s, q, tend, ru, rv, rom, k, j, i);
 }
 
+int launch_advect_mom_point(const Grid& g, const S& s, int comps, cudaStream_t st) {
+  const dim3 b3(32, 4);
+  k_advect<<<point_grid(g, b3), b3, 0, st>>>(g, s, comps);
+  return 1;
+}
+
 int launch_advect_forces(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
-  k_advect<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  const int n = launch_advect_theta_tiled(g, s, st);
+  int n = launch_advect_mom_tma(g, s, 0, 3, st);
+  if (n == 0) n = launch_advect_mom_point(g, s, 7, st);
+  n += launch_advect_theta_tiled(g, s, st);
   k_forces<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  return 2 + n;
+  return n + 1;
 }
 
 int launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st) {

@@ -32,6 +32,12 @@ int launch_advect_moist(const Grid& g, const S& s, cudaStream_t st);
 // ru_m / rv_m / ww_m into advect_tend, theta with ru / rv / ww into t_tend
 int launch_advect_moist_tiled(const Grid& g, const S& s, cudaStream_t st);
 int launch_advect_theta_tiled(const Grid& g, const S& s, cudaStream_t st);
+// advect_u / advect_v / advect_w of the components comp0 .. comp0+ncomp-1
+// (0 u, 1 v, 2 w) in one tiled TMA launch (k_advect_tiled.cu); 0 (nothing
+// launched) when nx is not a multiple of 4 or a map is refused
+int launch_advect_mom_tma(const Grid& g, const S& s, int comp0, int ncomp, cudaStream_t st);
+// the same with one thread per point (k_tend.cu), components as a bit mask
+int launch_advect_mom_point(const Grid& g, const S& s, int comps, cudaStream_t st);
 // stand-alone advect_scalar (k_tend.cu)
 int launch_advect_scalar(const Grid& g, const S& s, const float* field, float* tend, const float* ru,
                           const float* rv, const float* rom, cudaStream_t st);

@@ -429,6 +429,38 @@ int wrf_advect_scalar(const WrfGrid* gin, const float* field, float* tend, const
   return check_launch("advect_scalar");
 }
 
+int wrf_advect_momentum(const WrfGrid* gin, int component, const float* field, float* tend, const float* ru,
+                        const float* rv, const float* rom, const float* msf, const float* msf2, const float* fzm,
+                        const float* fzp, const float* rdz, int form, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (component < 0 || component > 2 || (form != 0 && form != 1))
+    return fail(WRF_EINVAL, "advect_momentum: component 0..2, form 0 or 1");
+  if (!field || !tend || !ru || !rv || !rom || !msf || (component == 1 && !msf2) || !fzm || !fzp || !rdz)
+    return fail(WRF_EINVAL, "null argument");
+  S s{};
+  const int fld[3] = {WF_U, WF_V, WF_W}, tnd[3] = {WF_RU_TEND, WF_RV_TEND, WF_RW_TEND};
+  s.f[fld[component]] = const_cast<float*>(field);
+  s.f[tnd[component]] = tend;
+  s.f[WF_RU] = const_cast<float*>(ru);
+  s.f[WF_RV] = const_cast<float*>(rv);
+  s.f[WF_WW] = const_cast<float*>(rom);
+  if (component == 0) s.f[WF_MSFUX] = const_cast<float*>(msf);
+  if (component == 1) {
+    s.f[WF_MSFVY] = const_cast<float*>(msf);
+    s.f[WF_MSFVX] = const_cast<float*>(msf2);
+  }
+  if (component == 2) s.f[WF_MSFTX] = const_cast<float*>(msf);
+  s.f[WF_FNM] = const_cast<float*>(fzm);
+  s.f[WF_FNP] = const_cast<float*>(fzp);
+  s.f[component == 2 ? WF_RDN : WF_RDNW] = const_cast<float*>(rdz);
+  cudaGetLastError();
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (form == 1 || launch_advect_mom_tma(g, s, component, 1, st) == 0) launch_advect_mom_point(g, s, 1 << component, st);
+  return check_launch("advect_momentum");
+}
+
 int wrf_advect_scalar_adj(const WrfGrid* gin, const float* field, const float* ru, const float* rv, const float* rom,
                           const float* msftx, const float* fzm, const float* fzp, const float* rdzw,
                           const float* tend_bar, float* field_bar, float* ru_bar, float* rv_bar, float* rom_bar,

@@ -1,5 +1,5 @@
-"""Drop-ins for ``pywrf.wrf_dynamics.advect_scalar`` and ``calc_coef_w``
-(reference signatures).
+"""Drop-ins for ``pywrf.wrf_dynamics.advect_scalar``, ``advect_u``,
+``advect_v``, ``advect_w`` and ``calc_coef_w`` (reference signatures).
 
 ``advect_scalar(...)`` takes the arguments of the reference function
 (pywrf/wrf_dynamics.py:1841-1850), adds the flux-form advection of ``field``
@@ -52,6 +52,64 @@ def advect_scalar(field, field_old, tendency, ru, rv, rom, c1, c2, mut, time_ste
                                        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     N.check(rc, "wrf_advect_scalar")
     return tendency
+
+
+def _check_frame(name, field, its, ite, jts, jte, kts, kte, ids, ide, jds, jde):
+    nz, ny, nx = field.shape
+    if (ids, jds, ide, jde) != (5, 5, nx - 5, ny - 5) or (its, ite, jts, jte) != (ids, ide, jds, jde) \
+            or (kts, kte) != (0, nz):
+        raise NotImplementedError(f"{name}: only the solver's 5-cell frame with tile = domain is supported")
+    return nz, ny, nx
+
+
+def _advect_momentum(component, field, tendency, ru, rv, rom, msf, msf2, fzm, fzp, rdx, rdy, rdz, form=0):
+    """tendency += advection of one momentum component (0 u, 1 v, 2 w)
+    through ``wrf_advect_momentum``; form 1 forces the one-thread-per-point
+    kernel (the same operations as the tiled one)."""
+    nz, ny, nx = field.shape
+    for nm, t in (("tendency", tendency), ("ru", ru), ("rv", rv), ("rom", rom)):
+        if tuple(t.shape) != (nz, ny, nx):
+            raise ValueError(f"{nm}: shape {tuple(t.shape)} != {(nz, ny, nx)}")
+    g = Grid.make(nx, ny, nz, 1.0 / float(rdx), 1.0 / float(rdy), 1.0)
+    cg = make_cgrid(g, {"cf1": 0.0, "cf2": 0.0, "cf3": 0.0, "cfn": 0.0, "cfn1": 0.0})
+    cg.dx = 1.0 / float(rdx)
+    cg.dy = 1.0 / float(rdy)
+    with torch.cuda.device(field.device):
+        rc = N.lib().wrf_advect_momentum(
+            ctypes.byref(cg), int(component), _need("field", field), _need("tendency", tendency), _need("ru", ru),
+            _need("rv", rv), _need("rom", rom), _need("msf", msf),
+            _need("msf2", msf2) if msf2 is not None else None, _need("fzm", fzm), _need("fzp", fzp),
+            _need("rdz", rdz), int(form), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    N.check(rc, "wrf_advect_momentum")
+    return tendency
+
+
+def advect_u(u, u_old, tendency, ru, rv, rom, c1, c2, mut, time_step, msfux, msfuy, msfvx, msfvy, msftx, msfty,
+             fzm, fzp, rdx, rdy, rdzw, ids, ide, jds, jde, kds, kde, ims, ime, jms, jme, kms, kme, its, ite, jts,
+             jte, kts, kte):
+    """advect_u (pywrf/wrf_dynamics.py:1112-1331) on the GPU: tendency +=
+    the advection of u, returned.  u_old, c1, c2, mut, time_step and the map
+    factors other than msfux are accepted and unused, as in the reference."""
+    _check_frame("advect_u", u, its, ite, jts, jte, kts, kte, ids, ide, jds, jde)
+    return _advect_momentum(0, u, tendency, ru, rv, rom, msfux, None, fzm, fzp, rdx, rdy, rdzw)
+
+
+def advect_v(v, v_old, tendency, ru, rv, rom, c1, c2, mut, time_step, msfux, msfuy, msfvx, msfvy, msftx, msfty,
+             fzm, fzp, rdx, rdy, rdzw, ids, ide, jds, jde, kds, kde, ims, ime, jms, jme, kms, kme, its, ite, jts,
+             jte, kts, kte):
+    """advect_v (pywrf/wrf_dynamics.py:1332-1534) on the GPU (map factors
+    msfvy and msfvx)."""
+    _check_frame("advect_v", v, its, ite, jts, jte, kts, kte, ids, ide, jds, jde)
+    return _advect_momentum(1, v, tendency, ru, rv, rom, msfvy, msfvx, fzm, fzp, rdx, rdy, rdzw)
+
+
+def advect_w(w, w_old, tendency, ru, rv, rom, c1, c2, mut, time_step, msfux, msfuy, msfvx, msfvy, msftx, msfty,
+             fzm, fzp, rdx, rdy, rdzu, ids, ide, jds, jde, kds, kde, ims, ime, jms, jme, kms, kme, its, ite, jts,
+             jte, kts, kte):
+    """advect_w (pywrf/wrf_dynamics.py:1535-1823) on the GPU (map factor
+    msftx; rdzu is the rdn profile the solver passes)."""
+    _check_frame("advect_w", w, its, ite, jts, jte, kts, kte, ids, ide, jds, jde)
+    return _advect_momentum(2, w, tendency, ru, rv, rom, msftx, None, fzm, fzp, rdx, rdy, rdzu)
 
 
 def calc_coef_w(a, alpha, gamma, mut, c1h, c2h, c1f, c2f, c3h, c4h, c3f, c4f, cqw, rdn, rdnw, c2a, dts, g, epssm,

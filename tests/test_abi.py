@@ -93,5 +93,7 @@ def test_null_arguments_of_function_entry_points_are_rejected():
     assert rc == N.WRF_EINVAL
     rc = L.wrf_advect_scalar(ctypes.byref(_cgrid()), *([None] * 9), None)
     assert rc == N.WRF_EINVAL
+    rc = L.wrf_advect_momentum(ctypes.byref(_cgrid()), 0, *([None] * 10), 0, None)
+    assert rc == N.WRF_EINVAL
     rc = L.wrf_status_read(None, None, None)
     assert rc == N.WRF_EINVAL
