@@ -251,6 +251,18 @@ int wrf_status_read(const WrfState* s, void* stream, int* out16);
  * reference has no counterpart; used to report launch counts) */
 int wrf_last_launch_count(void);
 
+/* Kernel forms for cross-checks (process-wide; no counterpart in the
+ * reference).  WRF_FORM_FAST (the default) runs the tiled tensor-map kernels
+ * where the arrays allow them; WRF_FORM_POINT runs, for the same launches, the
+ * one-thread-per-point (momentum advection, advance_uv) and cp.async-tiled
+ * (scalar advection) kernels.  Both forms perform the reference's operations
+ * in the same order and give bit-identical results.  A CUDA graph keeps the
+ * form that was set when it was captured.  Returns the previous form, or
+ * WRF_EINVAL for an unknown one. */
+#define WRF_FORM_FAST 0
+#define WRF_FORM_POINT 1
+int wrf_set_kernel_form(int form);
+
 /* ------------------------------------------------------------------------
  * Per-column microphysics network: a learned stand-in for wsm6
  * (pywrf/wrf_physics.py:137-1214).  The reference has no counterpart of

@@ -22,6 +22,8 @@ WRF_KSF, WRF_KSI = 20, 21
 WRF_ST_NAN_P = 0
 WRF_ST_STEP = 1
 WRF_ST_WAIT = 2
+WRF_FORM_FAST = 0
+WRF_FORM_POINT = 1
 
 
 class WrfGridC(ctypes.Structure):
@@ -92,6 +94,8 @@ def lib() -> ctypes.CDLL:
     L.wrf_acoustic_substep.argtypes = [G0, vp, ip, ip, vp]
     L.wrf_advect_scalar.restype = ip
     L.wrf_advect_scalar.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 9 + [vp]
+    L.wrf_set_kernel_form.restype = ip
+    L.wrf_set_kernel_form.argtypes = [ctypes.c_int]
     L.wrf_advect_momentum.restype = ip
     L.wrf_advect_momentum.argtypes = [ctypes.POINTER(WrfGridC), ctypes.c_int] + [vp] * 10 + [ctypes.c_int, vp]
     L.wrf_advect_scalar_adj.restype = ip

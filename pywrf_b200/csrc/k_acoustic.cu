@@ -10,6 +10,7 @@
 // The vertical recurrences (mass divergence sum, ww scan, Thomas sweeps) run
 // sequentially per column in the reference's order.
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace wrf {
 
@@ -230,6 +231,221 @@ __global__ void k_advance_uv(Grid g, S s, float dts) {
     s[WF_V][p] = v - dts * s[WF_CQV][p] * dp + mudf_xy;
   } else if (((j == jds || j == jde - 1) && i >= ids && i < ide - 1) || (j >= jds + 1 && j < jde - 1 && (i == ids || i == ide - 2))) {
     s[WF_V][p] = s[WF_V][p] + dts * s[WF_RV_TEND][p];   // spec_bdyupdate(v)
+  }
+}
+
+// advance_uv, tensor-map form (nx a multiple of 4): a block of 32 x 8
+// threads owns 32 x 8 columns (u and v points (j, i)) and a chunk of levels.
+// Per level one thread loads boxes of alt, al, pb, php at k and ph, p at k+1
+// (40 x 9 from x = floor4(i0 - 1), y = j0 - 1: every point's i-1 and j-1
+// neighbours) into an mbarrier ring two levels ahead; ph(k), p(k) and the
+// vertical pressure averages dpn(k) come from the level below in registers
+// (each is the same operation on the same operands as in k_advance_uv), and
+// the thread's own u, v, tendencies and cq are loaded a level ahead.  Every
+// wait on a box is bounded; a block whose wait runs out stops, drains its
+// copies and adds 1 to STATUS[WRF_ST_WAIT].
+constexpr int kUvTX = 32, kUvTY = 8, kUvBW = 40, kUvBH = kUvTY + 1;
+constexpr int kUvNB = 6;                 // boxes per level: alt al pb php (k), ph p (k+1)
+constexpr int kUvSlot = 384;             // floats per box slot (1536 B >= 40 x 9 x 4)
+constexpr int kUvRing = 3, kUvKCH = 7;
+constexpr uint32_t kUvBytes = kUvBW * kUvBH * 4;
+constexpr long long kUvWaitCycles = 4000000000LL;
+static_assert(kUvBytes <= kUvSlot * 4, "a ring slot holds one box");
+
+struct UvTmaArgs {
+  CUtensorMap alt, al, pb, php, ph, pp;
+  int nchunk;
+};
+
+__global__ void __launch_bounds__(kUvTX * kUvTY, 4) k_advance_uv_tma(Grid g, S s, float dts,
+                                                                     const __grid_constant__ UvTmaArgs a) {
+  __shared__ __align__(128) float box[kUvRing][kUvNB][kUvSlot];
+  __shared__ uint64_t bar[kUvRing];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kUvTX + tx;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, ktf = nz - 1;
+  const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde;
+  const int i0 = ids + blockIdx.x * kUvTX, j0 = jds + blockIdx.y * kUvTY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int mx = (i0 - 1) & ~3, om = i0 - mx;
+  const int k0 = blockIdx.z * ktf / a.nchunk, k1 = (blockIdx.z + 1) * ktf / a.nchunk;
+  const size_t lev = (size_t)ny * nx;
+  const bool uin = j >= jds + 1 && j < jde - 2 && i >= ids + 1 && i < ide - 1;
+  const bool uspec = ((j == jds || j == jde - 2) && i >= ids && i < ide) ||
+                     (j >= jds + 1 && j < jde - 2 && (i == ids || i == ide - 1));
+  const bool vin = j >= jds + 1 && j < jde - 1 && i >= ids + 1 && i < ide - 2;
+  const bool vspec = ((j == jds || j == jde - 1) && i >= ids && i < ide - 1) ||
+                     (j >= jds + 1 && j < jde - 1 && (i == ids || i == ide - 2));
+  const bool wu = uin || uspec, wv = vin || vspec;
+  const int c = min(j, ny - 1) * nx + min(i, nx - 1);
+  const float* pp = s[WF_P];
+  const float* ph = s[WF_PH];
+  const float* fnm = s[WF_FNM];
+  const float* fnp = s[WF_FNP];
+  const float* rdnw = s[WF_RDNW];
+  float* U = s[WF_U];
+  float* V = s[WF_V];
+  const float* rut = s[WF_RU_TEND];
+  const float* rvt = s[WF_RV_TEND];
+  const float* cqu = s[WF_CQU];
+  const float* cqv = s[WF_CQV];
+  const float rdx = g.rdx, rdy = g.rdy;
+
+  if (tid == 0) {
+    for (int r = 0; r < kUvRing; ++r) tma::mbar_init(&bar[r], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int k, int r) {
+    tma::mbar_expect_tx(&bar[r], kUvNB * kUvBytes);
+    tma::load_4d(box[r][0], &a.alt, mx, j0 - 1, k, 0, &bar[r]);
+    tma::load_4d(box[r][1], &a.al, mx, j0 - 1, k, 0, &bar[r]);
+    tma::load_4d(box[r][2], &a.pb, mx, j0 - 1, k, 0, &bar[r]);
+    tma::load_4d(box[r][3], &a.php, mx, j0 - 1, k, 0, &bar[r]);
+    tma::load_4d(box[r][4], &a.ph, mx, j0 - 1, k + 1, 0, &bar[r]);
+    tma::load_4d(box[r][5], &a.pp, mx, j0 - 1, k + 1, 0, &bar[r]);
+  };
+  int hi = k0 - 1;
+  if (tid == 0) {
+    for (int k = k0; k < min(k0 + kUvRing - 1, k1); ++k) issue(k, k - k0);
+    hi = min(k0 + kUvRing - 1, k1) - 1;
+  }
+  // per-column constants, in the association order of k_advance_uv
+  float mudf_u = 0.f, cu = 0.f, ru = 0.f, muav_u = 0.f, mudf_v = 0.f, cv = 0.f, rv = 0.f, muav_v = 0.f;
+  if (uin) {
+    const float* mudf = s[WF_MUDF];
+    const float* mu = s[WF_MU];
+    mudf_u = (float)(-(double)g.emdiv * g.dxd) * (__ldg(&mudf[c]) - __ldg(&mudf[c - 1])) / __ldg(&s[WF_MSFUY][c]);
+    const float r = __ldg(&s[WF_MSFUX][c]) / __ldg(&s[WF_MSFUY][c]);
+    cu = r * 0.5f * rdx * __ldg(&s[WF_MUU][c]);
+    ru = r * rdx;
+    muav_u = 0.5f * (__ldg(&mu[c - 1]) + __ldg(&mu[c]));
+  }
+  if (vin) {
+    const float* mudf = s[WF_MUDF];
+    const float* mu = s[WF_MU];
+    mudf_v = (float)(-(double)g.emdiv * g.dyd) * (__ldg(&mudf[c]) - __ldg(&mudf[c - nx])) * __ldg(&s[WF_MSFVX_INV][c]);
+    const float r = __ldg(&s[WF_MSFVY][c]) / __ldg(&s[WF_MSFVX][c]);
+    cv = r * 0.5f * rdy * __ldg(&s[WF_MUV][c]);
+    rv = r * rdy;
+    muav_v = 0.5f * (__ldg(&mu[c - nx]) + __ldg(&mu[c]));
+  }
+  // ph(k), p(k) at (j, i), (j, i-1), (j-1, i) and dpn(k) of the u and v points
+  const int cw = (uin || vin) ? c - 1 : c, cs = (uin || vin) ? c - nx : c;
+  float ph_c = 0.f, ph_w = 0.f, ph_s = 0.f, p_c = 0.f, p_w = 0.f, p_s = 0.f, dpn_u = 0.f, dpn_v = 0.f;
+  if (uin || vin) {
+    const size_t q = (size_t)k0 * lev;
+    ph_c = __ldg(&ph[q + c]);
+    ph_w = __ldg(&ph[q + cw]);
+    ph_s = __ldg(&ph[q + cs]);
+    p_c = __ldg(&pp[q + c]);
+    p_w = __ldg(&pp[q + cw]);
+    p_s = __ldg(&pp[q + cs]);
+    if (k0 == 0) {  // dpn(0): cf1..cf3 over the three lowest levels
+      const float a1 = __ldg(&pp[lev + c]), a2 = __ldg(&pp[2 * lev + c]);
+      const float w1 = __ldg(&pp[lev + cw]), w2 = __ldg(&pp[2 * lev + cw]);
+      const float s1 = __ldg(&pp[lev + cs]), s2 = __ldg(&pp[2 * lev + cs]);
+      dpn_u = 0.5f * (g.cf1 * (p_c + p_w) + g.cf2 * (a1 + w1) + g.cf3 * (a2 + w2));
+      dpn_v = 0.5f * (g.cf1 * (p_c + p_s) + g.cf2 * (a1 + s1) + g.cf3 * (a2 + s2));
+    } else if (k0 < nz - 1) {
+      const float fm = __ldg(&fnm[k0]), fp = __ldg(&fnp[k0]);
+      const size_t qm = q - lev;
+      dpn_u = 0.5f * (fm * (p_c + p_w) + fp * (__ldg(&pp[qm + c]) + __ldg(&pp[qm + cw])));
+      dpn_v = 0.5f * (fm * (p_c + p_s) + fp * (__ldg(&pp[qm + c]) + __ldg(&pp[qm + cs])));
+    }
+  }
+  // the thread's own values at the next level, loaded a level ahead
+  auto own = [&](int k, float& u, float& rt, float& v, float& vt, float& qu, float& qv) {
+    const size_t p = (size_t)k * lev + c;
+    u = wu ? U[p] : 0.f;
+    rt = wu ? __ldg(&rut[p]) : 0.f;
+    qu = uin ? __ldg(&cqu[p]) : 0.f;
+    v = wv ? V[p] : 0.f;
+    vt = wv ? __ldg(&rvt[p]) : 0.f;
+    qv = vin ? __ldg(&cqv[p]) : 0.f;
+  };
+  float u0, rt0, v0, vt0, qu0, qv0;
+  own(k0, u0, rt0, v0, vt0, qu0, qv0);
+  const int oA = (ty + 1) * kUvBW + om + tx;
+  int kstop = k1, slot = 0;
+  uint32_t par = 0;
+  for (int k = k0; k < k1; ++k) {
+    float u1 = 0.f, rt1 = 0.f, v1 = 0.f, vt1 = 0.f, qu1 = 0.f, qv1 = 0.f;
+    if (k + 1 < k1) own(k + 1, u1, rt1, v1, vt1, qu1, qv1);
+    const float rdk = __ldg(&rdnw[k]);
+    const float fm1 = k + 1 < nz - 1 ? __ldg(&fnm[k + 1]) : 0.f, fp1 = k + 1 < nz - 1 ? __ldg(&fnp[k + 1]) : 0.f;
+    const bool ok = tma::mbar_wait_bounded(&bar[slot], par, kUvWaitCycles);
+    if (__syncthreads_or(!ok)) {
+      kstop = k;
+      break;
+    }
+    // every thread is past level k-1: its slot takes level k + kUvRing - 1
+    if (tid == 0 && k + kUvRing - 1 < k1) {
+      issue(k + kUvRing - 1, slot == 0 ? kUvRing - 1 : slot - 1);
+      hi = k + kUvRing - 1;
+    }
+    const float* B = box[slot][0];
+    const size_t p = (size_t)k * lev + c;
+    float pu_c = 0.f, pu_w = 0.f, pu_s = 0.f, hu_c = 0.f, hu_w = 0.f, hu_s = 0.f;
+    if (uin || vin) {
+      hu_c = B[4 * kUvSlot + oA];
+      pu_c = B[5 * kUvSlot + oA];
+      hu_w = B[4 * kUvSlot + oA - 1];
+      pu_w = B[5 * kUvSlot + oA - 1];
+      hu_s = B[4 * kUvSlot + oA - kUvBW];
+      pu_s = B[5 * kUvSlot + oA - kUvBW];
+    }
+    float unew = 0.f, vnew = 0.f;
+    if (uin) {
+      const float u = u0 + dts * rt0;
+      const float alt_c = B[oA], alt_w = B[oA - 1];
+      const float al_c = B[kUvSlot + oA], al_w = B[kUvSlot + oA - 1];
+      const float pb_c = B[2 * kUvSlot + oA], pb_w = B[2 * kUvSlot + oA - 1];
+      const float php_c = B[3 * kUvSlot + oA], php_w = B[3 * kUvSlot + oA - 1];
+      const float dpn_up = k + 1 == nz - 1 ? 0.f : 0.5f * (fm1 * (pu_c + pu_w) + fp1 * (p_c + p_w));
+      float dp = cu * (((hu_c - hu_w) + (ph_c - ph_w)) + (alt_c + alt_w) * (p_c - p_w) + (al_c + al_w) * (pb_c - pb_w));
+      dp = dp + ru * (php_c - php_w) * (rdk * (dpn_up - dpn_u) - muav_u);
+      unew = u - dts * qu0 * dp + mudf_u;
+      dpn_u = dpn_up;
+    } else if (uspec) {
+      unew = u0 + dts * rt0;  // spec_bdyupdate(u)
+    }
+    if (vin) {
+      const float v = v0 + dts * vt0;
+      const float alt_c = B[oA], alt_s = B[oA - kUvBW];
+      const float al_c = B[kUvSlot + oA], al_s = B[kUvSlot + oA - kUvBW];
+      const float pb_c = B[2 * kUvSlot + oA], pb_s = B[2 * kUvSlot + oA - kUvBW];
+      const float php_c = B[3 * kUvSlot + oA], php_s = B[3 * kUvSlot + oA - kUvBW];
+      const float dpn_up = k + 1 == nz - 1 ? 0.f : 0.5f * (fm1 * (pu_c + pu_s) + fp1 * (p_c + p_s));
+      float dp = cv * (((hu_c - hu_s) + (ph_c - ph_s)) + (alt_c + alt_s) * (p_c - p_s) + (al_c + al_s) * (pb_c - pb_s));
+      dp = dp + rv * (php_c - php_s) * (rdk * (dpn_up - dpn_v) - muav_v);
+      vnew = v - dts * qv0 * dp + mudf_v;
+      dpn_v = dpn_up;
+    } else if (vspec) {
+      vnew = v0 + dts * vt0;  // spec_bdyupdate(v)
+    }
+    if (wu) U[p] = unew;
+    if (wv) V[p] = vnew;
+    ph_c = hu_c;
+    ph_w = hu_w;
+    ph_s = hu_s;
+    p_c = pu_c;
+    p_w = pu_w;
+    p_s = pu_s;
+    u0 = u1;
+    rt0 = rt1;
+    v0 = v1;
+    vt0 = vt1;
+    qu0 = qu1;
+    qv0 = qv1;
+    if (++slot == kUvRing) {
+      slot = 0;
+      par ^= 1u;
+    }
+  }
+  if (kstop < k1 && tid == 0) {
+    for (int k = kstop; k <= hi; ++k)
+      tma::mbar_wait_bounded(&bar[(k - k0) % kUvRing], ((k - k0) / kUvRing) & 1, kUvWaitCycles);
+    if (s[WF_STATUS]) atomicAdd(reinterpret_cast<int*>(s[WF_STATUS]) + WRF_ST_WAIT, 1);
   }
 }
 
@@ -818,6 +1034,20 @@ int launch_coef_w(const Grid& g, const float* mut, const float* cqw, const float
 }
 
 int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st) {
+  if (kernel_form() == WRF_FORM_FAST && g.nx % 4 == 0 && g.nz >= 4) {
+    UvTmaArgs a{};
+    const char* err = nullptr;
+    const int f[6] = {WF_ALT, WF_AL, WF_PB, WF_PHP, WF_PH, WF_P};
+    CUtensorMap* m[6] = {&a.alt, &a.al, &a.pb, &a.php, &a.ph, &a.pp};
+    bool ok = true;
+    for (int e = 0; e < 6 && ok; ++e) ok = tma::encode_f32_4d(m[e], s[f[e]], g.nx, g.ny, g.nz, 1, kUvBW, kUvBH, &err);
+    if (ok) {
+      a.nchunk = min((g.nz - 1 + kUvKCH - 1) / kUvKCH, g.nz - 1);
+      const dim3 gr((g.ide + 1 - g.ids + kUvTX - 1) / kUvTX, (g.jde - g.jds + kUvTY - 1) / kUvTY, a.nchunk);
+      k_advance_uv_tma<<<gr, dim3(kUvTX, kUvTY), 0, st>>>(g, s, dts, a);
+      return 1;
+    }
+  }
   const dim3 b3(32, 4);
   k_advance_uv<<<point_grid(g, b3), b3, 0, st>>>(g, s, dts);
   return 1;

@@ -864,7 +864,7 @@ __global__ void __launch_bounds__(kTTX * kTTY, WRF_ADV_MINB) k_advect_mom_tma(Gr
 namespace {
 // the TMA form applies when every row is a multiple of 16 bytes and the
 // arrays are 16-byte aligned (the encoder checks the bases)
-bool tma_form(const Grid& g) { return g.nx % 4 == 0 && g.ids >= 0 && g.jds >= 0; }
+bool tma_form(const Grid& g) { return kernel_form() == WRF_FORM_FAST && g.nx % 4 == 0 && g.ids >= 0 && g.jds >= 0; }
 
 int nchunks(const Grid& g) { return (g.nz + kTKCH - 1) / kTKCH; }
 

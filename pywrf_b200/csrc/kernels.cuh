@@ -9,6 +9,10 @@ namespace wrf {
 // column kernels keep one vertical column per thread in local arrays
 constexpr int kMaxNz = 64;
 
+// the kernel form wrf_set_kernel_form selected (WRF_FORM_FAST or WRF_FORM_POINT)
+int kernel_form();
+int set_kernel_form(int form);  // returns the previous form
+
 // rk_step_prep: calculate_full, calc_mu_uv, couple_momentum, calc_ww_cp,
 // calc_cq, calc_alt, calc_php (k_prep.cu)
 int launch_prep(const Grid& g, const S& s, cudaStream_t st);

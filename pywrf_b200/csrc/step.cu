@@ -5,6 +5,7 @@
 // allocates nothing and never synchronises (a probe callback may).  The
 // boundary time of the step is derived on the device from the step counter
 // STATUS[WRF_ST_STEP], so one captured CUDA graph replays every step.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <cctype>
@@ -314,6 +315,14 @@ struct Driver {
 
 using namespace wrf;
 
+namespace wrf {
+namespace {
+std::atomic<int> g_form{WRF_FORM_FAST};
+}
+int kernel_form() { return g_form.load(std::memory_order_relaxed); }
+int set_kernel_form(int form) { return g_form.exchange(form); }
+}  // namespace wrf
+
 extern "C" {
 
 int wrf_field_count(void) { return WF_COUNT; }
@@ -331,6 +340,11 @@ int wrf_field_kind(int id) {
 const char* wrf_last_error(void) { return g_err.c_str(); }
 
 int wrf_last_launch_count(void) { return g_last_launches; }
+
+int wrf_set_kernel_form(int form) {
+  if (form != WRF_FORM_FAST && form != WRF_FORM_POINT) return fail(WRF_EINVAL, "unknown kernel form");
+  return wrf::set_kernel_form(form);
+}
 
 int wrf_rk3_step(const WrfGrid* gin, const WrfState* sin, void* stream, wrf_probe_fn probe, void* user) {
   Driver d;

@@ -46,6 +46,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, 
 }
 
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, long long limit_cycles) {
+  if (mbar_try(b, parity)) return true;  // the common case: no clock read
   const long long t0 = clock64();
   for (uint32_t it = 0;; ++it) {
     if (mbar_try(b, parity)) return true;

@@ -97,3 +97,10 @@ def test_null_arguments_of_function_entry_points_are_rejected():
     assert rc == N.WRF_EINVAL
     rc = L.wrf_status_read(None, None, None)
     assert rc == N.WRF_EINVAL
+
+
+def test_kernel_form_switch():
+    L = N.lib()
+    assert L.wrf_set_kernel_form(7) == N.WRF_EINVAL
+    assert L.wrf_set_kernel_form(N.WRF_FORM_POINT) == N.WRF_FORM_FAST
+    assert L.wrf_set_kernel_form(N.WRF_FORM_FAST) == N.WRF_FORM_POINT
