@@ -47,6 +47,9 @@ __global__ void k_ssp2d(Grid g, S s, int rk_step) {
   }
 }
 
+// all operands are loaded before any store (the stores would otherwise hold
+// back the later fields' loads); in stage 1 the *_1 copies are the values
+// just read
 __global__ void k_ssp3d(Grid g, S s, int rk_step) {
   WRF_POINT_INDEX(g, k, j, i);
   const int nz = g.nz, ktf = nz - 1;
@@ -54,36 +57,68 @@ __global__ void k_ssp3d(Grid g, S s, int rk_step) {
   const int c = g.i2(j, i);
   const size_t p = (size_t)k * g.ny * g.nx + c;
   const bool t2 = j >= jts && j < jme && i >= its && i < ime;
-  if (k < ktf && j >= jts && j < jme && i >= its && i < ieu) {
-    const float u2 = s[WF_U][p];
-    if (rk_step == 1) s[WF_U_1][p] = u2;
-    s[WF_U_SAVE][p] = u2;
-    s[WF_U][p] = (s[WF_MUUS][c] * s[WF_U_1][p] - s[WF_MUU][c] * u2) / s[WF_MSFUY][c];
+  const bool du = k < ktf && j >= jts && j < jme && i >= its && i < ieu;
+  const bool dv = k < ktf && j >= jts && j < jev && i >= its && i < ime;
+  const bool r1 = rk_step == 1;
+  float u2 = 0.f, u1 = 0.f, muus = 0.f, muu = 0.f, mfuy = 1.f;
+  if (du) {
+    u2 = s[WF_U][p];
+    u1 = r1 ? u2 : s[WF_U_1][p];
+    muus = s[WF_MUUS][c];
+    muu = s[WF_MUU][c];
+    mfuy = s[WF_MSFUY][c];
   }
-  if (k < ktf && j >= jts && j < jev && i >= its && i < ime) {
-    const float v2 = s[WF_V][p];
-    if (rk_step == 1) s[WF_V_1][p] = v2;
+  float v2 = 0.f, v1 = 0.f, muvs = 0.f, muv = 0.f, mvxi = 0.f;
+  if (dv) {
+    v2 = s[WF_V][p];
+    v1 = r1 ? v2 : s[WF_V_1][p];
+    muvs = s[WF_MUVS][c];
+    muv = s[WF_MUV][c];
+    mvxi = s[WF_MSFVX_INV][c];
+  }
+  float muts = 0.f, mut = 0.f, pbv = 0.f, ppv = 0.f, altv = 1.f, t2v = 0.f, t1 = 0.f;
+  float w2 = 0.f, w1 = 0.f, mfty = 1.f, ph2 = 0.f, ph1 = 0.f, wwv = 0.f;
+  if (t2) {
+    muts = s[WF_MUTS][c];
+    mut = s[WF_MUT][c];
+    if (k < ktf) {
+      pbv = s[WF_PB][p];
+      ppv = s[WF_P][p];
+      altv = s[WF_ALT][p];
+      t2v = s[WF_T][p];
+      t1 = r1 ? t2v : s[WF_T_1][p];
+    }
+    w2 = s[WF_W][p];
+    w1 = r1 ? w2 : s[WF_W_1][p];
+    mfty = s[WF_MSFTY][c];
+    ph2 = s[WF_PH][p];
+    ph1 = r1 ? ph2 : s[WF_PH_1][p];
+    wwv = s[WF_WW][p];
+  }
+  if (du) {
+    if (r1) s[WF_U_1][p] = u2;
+    s[WF_U_SAVE][p] = u2;
+    s[WF_U][p] = (muus * u1 - muu * u2) / mfuy;
+  }
+  if (dv) {
+    if (r1) s[WF_V_1][p] = v2;
     s[WF_V_SAVE][p] = v2;
-    s[WF_V][p] = (s[WF_MUVS][c] * s[WF_V_1][p] - s[WF_MUV][c] * v2) * s[WF_MSFVX_INV][c];
+    s[WF_V][p] = (muvs * v1 - muv * v2) * mvxi;
   }
   if (t2) {
-    const float muts = s[WF_MUTS][c], mut = s[WF_MUT][c];
     if (k < ktf) {
-      s[WF_C2A][p] = (float)CPOVCV * (s[WF_PB][p] + s[WF_P][p]) / s[WF_ALT][p];
-      const float t2v = s[WF_T][p];
-      if (rk_step == 1) s[WF_T_1][p] = t2v;
+      s[WF_C2A][p] = (float)CPOVCV * (pbv + ppv) / altv;
+      if (r1) s[WF_T_1][p] = t2v;
       s[WF_T_SAVE][p] = t2v;
-      s[WF_T][p] = muts * s[WF_T_1][p] - mut * t2v;
+      s[WF_T][p] = muts * t1 - mut * t2v;
     }
-    const float w2 = s[WF_W][p];
-    if (rk_step == 1) s[WF_W_1][p] = w2;
+    if (r1) s[WF_W_1][p] = w2;
     s[WF_W_SAVE][p] = w2;
-    s[WF_W][p] = (muts * s[WF_W_1][p] - mut * w2) / s[WF_MSFTY][c];
-    const float ph2 = s[WF_PH][p];
-    if (rk_step == 1) s[WF_PH_1][p] = ph2;
+    s[WF_W][p] = (muts * w1 - mut * w2) / mfty;
+    if (r1) s[WF_PH_1][p] = ph2;
     s[WF_PH_SAVE][p] = ph2;
-    s[WF_PH][p] = s[WF_PH_1][p] - ph2;
-    s[WF_WW1][p] = s[WF_WW][p];
+    s[WF_PH][p] = ph1 - ph2;
+    s[WF_WW1][p] = wwv;
   }
 }
 
@@ -99,12 +134,15 @@ __global__ void k_p_rho0(Grid g, S s) {
   float* pp = s[WF_P];
   float pnew = pp[p];
   if (k < ktf && j >= g.jds && j < g.jde - 1 && i >= g.ids && i < g.ide - 1) {
+    // operands first, then the stores
     const float muts = s[WF_MUTS][c], mu = s[WF_MU][c];
     const float alt = s[WF_ALT][p], t1 = s[WF_T_SAVE][p];
     const float* ph = s[WF_PH];
-    const float al = -1.0f / muts * (alt * mu + s[WF_RDNW][k] * (ph[p + lev] - ph[p]));
+    const float phu = ph[p + lev], phk = ph[p], rdnw = s[WF_RDNW][k];
+    const float c2 = s[WF_C2A][p], tk = s[WF_T][p];
+    const float al = -1.0f / muts * (alt * mu + rdnw * (phu - phk));
+    pnew = c2 * (alt * (tk - mu * t1) / (muts * ((float)T0 + t1)) - al);
     s[WF_AL][p] = al;
-    pnew = s[WF_C2A][p] * (alt * (s[WF_T][p] - mu * t1) / (muts * ((float)T0 + t1)) - al);
     pp[p] = pnew;
   }
   s[WF_PM1][p] = pnew;
@@ -984,28 +1022,68 @@ __global__ void k_mu_uv_1(Grid g, S s) {
   }
 }
 
+// operands first, then the stores (a store would hold back the later
+// fields' loads)
 __global__ void k_ssfinish(Grid g, S s, float dts, int nsub, int rk_step) {
   WRF_POINT_INDEX(g, k, j, i);
   const int nz = g.nz;
   const int jts = g.jds, jme = g.jde - 1, its = g.ids, ime = g.ide - 1, ieu = g.ide, jev = g.jde;
   const int c = g.i2(j, i);
   const size_t p = (size_t)k * g.ny * g.nx + c;
-  if (k < nz - 1 && j >= jts && j < jev && i >= its && i < ime)
-    s[WF_V][p] = (s[WF_MSFVX][c] * s[WF_V][p] + s[WF_V_SAVE][p] * s[WF_MUV][c]) / s[WF_MUVS][c];
-  if (k < nz - 1 && j >= jts && j < jme && i >= its && i < ieu)
-    s[WF_U][p] = (s[WF_MSFUY][c] * s[WF_U][p] + s[WF_U_SAVE][p] * s[WF_MUU][c]) / s[WF_MUUS][c];
-  if (j >= jts && j < jme && i >= its && i < ime) {
-    const float mut = s[WF_MUT][c], muts = s[WF_MUTS][c];
-    s[WF_W][p] = (s[WF_MSFTY][c] * s[WF_W][p] + s[WF_W_SAVE][p] * mut) / muts;
-    s[WF_PH][p] = s[WF_PH][p] + s[WF_PH_SAVE][p];
-    s[WF_WW][p] = s[WF_WW][p] + s[WF_WW1][p];
+  const bool dv = k < nz - 1 && j >= jts && j < jev && i >= its && i < ime;
+  const bool du = k < nz - 1 && j >= jts && j < jme && i >= its && i < ieu;
+  const bool m3 = j >= jts && j < jme && i >= its && i < ime;
+  float vv = 0.f, vs = 0.f, mfvx = 0.f, muv = 0.f, muvs = 1.f;
+  if (dv) {
+    vv = s[WF_V][p];
+    vs = s[WF_V_SAVE][p];
+    mfvx = s[WF_MSFVX][c];
+    muv = s[WF_MUV][c];
+    muvs = s[WF_MUVS][c];
+  }
+  float uu = 0.f, us = 0.f, mfuy = 0.f, muu = 0.f, muus = 1.f;
+  if (du) {
+    uu = s[WF_U][p];
+    us = s[WF_U_SAVE][p];
+    mfuy = s[WF_MSFUY][c];
+    muu = s[WF_MUU][c];
+    muus = s[WF_MUUS][c];
+  }
+  float mut = 0.f, muts = 1.f, mfty = 0.f, ww = 0.f, wsv = 0.f, phv = 0.f, phs = 0.f, wwv = 0.f, ww1 = 0.f;
+  float tv = 0.f, ts = 0.f, hd = 0.f, muv0 = 0.f, mus0 = 0.f;
+  if (m3) {
+    mut = s[WF_MUT][c];
+    muts = s[WF_MUTS][c];
+    mfty = s[WF_MSFTY][c];
+    ww = s[WF_W][p];
+    wsv = s[WF_W_SAVE][p];
+    phv = s[WF_PH][p];
+    phs = s[WF_PH_SAVE][p];
+    wwv = s[WF_WW][p];
+    ww1 = s[WF_WW1][p];
+    if (k < nz - 1) {
+      tv = s[WF_T][p];
+      ts = s[WF_T_SAVE][p];
+      if (rk_step == 3) hd = s[WF_H_DIABATIC][p];
+    }
+    if (k == 0) {
+      muv0 = s[WF_MU][c];
+      mus0 = s[WF_MU_SAVE][c];
+    }
+  }
+  if (dv) s[WF_V][p] = (mfvx * vv + vs * muv) / muvs;
+  if (du) s[WF_U][p] = (mfuy * uu + us * muu) / muus;
+  if (m3) {
+    s[WF_W][p] = (mfty * ww + wsv * mut) / muts;
+    s[WF_PH][p] = phv + phs;
+    s[WF_WW][p] = wwv + ww1;
     if (k < nz - 1) {
       if (rk_step < 3)
-        s[WF_T][p] = (s[WF_T][p] + s[WF_T_SAVE][p] * mut) / muts;
+        s[WF_T][p] = (tv + ts * mut) / muts;
       else
-        s[WF_T][p] = (s[WF_T][p] - (float)((double)dts * nsub) * mut * s[WF_H_DIABATIC][p] + s[WF_T_SAVE][p] * mut) / muts;
+        s[WF_T][p] = (tv - (float)((double)dts * nsub) * mut * hd + ts * mut) / muts;
     }
-    if (k == 0) s[WF_MU][c] = s[WF_MU][c] + s[WF_MU_SAVE][c];
+    if (k == 0) s[WF_MU][c] = muv0 + mus0;
   }
 }
 

@@ -39,6 +39,9 @@ __global__ void k_hdiff_moist(Grid g, S s) {
   }
 }
 
+// every species' operands are loaded before any store, so that the loads of
+// the six species are in flight together (a store to one species' field would
+// otherwise hold back the next species' loads)
 __global__ void k_moist_update(Grid g, S s, int rk_step, float dt) {
   WRF_POINT_INDEX(g, k, j, i);
   const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
@@ -52,16 +55,25 @@ __global__ void k_moist_update(Grid g, S s, int rk_step, float dt) {
     munew = s[WF_MU][c] + s[WF_MUB][c];
     msfty = s[WF_MSFTY][c];
   }
-  for (int m = 1; m < 7; ++m) {
-    float* q = s[WF_MOIST] + m * n3;
-    float* qold = s[WF_MOIST_OLD] + m * n3;
-    const float cur = q[p];
-    if (rk_step == 1) qold[p] = cur;
+  float* q = s[WF_MOIST];
+  float* qold = s[WF_MOIST_OLD];
+  float cur[6], adv[6], mt[6], qo[6];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const size_t o = (size_t)(m + 1) * n3 + p;
+    cur[m] = q[o];
+    adv[m] = inner ? s[WF_ADVECT_TEND][o] : 0.f;
+    mt[m] = full ? s[WF_MOIST_TEND][o] : 0.f;
+    qo[m] = (full && rk_step != 1) ? qold[o] : cur[m];
+  }
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const size_t o = (size_t)(m + 1) * n3 + p;
+    if (rk_step == 1) qold[o] = cur[m];
     if (!full) continue;
-    float tend = inner ? s[WF_ADVECT_TEND][m * n3 + p] * msfty : 0.f;
-    tend = tend + s[WF_MOIST_TEND][m * n3 + p];
-    const float qo = rk_step == 1 ? cur : qold[p];
-    q[p] = (muold * qo + dt * tend) / munew;
+    float tend = inner ? adv[m] * msfty : 0.f;
+    tend = tend + mt[m];
+    q[o] = (muold * qo[m] + dt * tend) / munew;
   }
 }
 

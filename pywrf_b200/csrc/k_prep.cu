@@ -44,34 +44,68 @@ __device__ __forceinline__ float qsum7(const float* moist, size_t n3, int p) {
   return q;
 }
 
+// operands first, then the stores: the moisture sums of the point and of its
+// west, south and lower neighbours are each formed once (the stores between
+// them would otherwise make the compiler reload them)
 __global__ void k_rk_prep3d(Grid g, S s) {
   WRF_POINT_INDEX(g, k, j, i);
   const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde, nz = g.nz;
   const int p = g.i3(k, j, i);
   const int c = g.i2(j, i);
   const size_t n3 = g.n3();
+  const int lev = g.ny * g.nx;
   const float* moist = s[WF_MOIST];
   const bool mrow = j >= jds && j < jde - 1;
   const bool mcol = i >= ids && i < ide - 1;
-  if (k < nz - 1) {
-    if (mrow && i >= ids && i < ide) {
-      s[WF_RU][p] = s[WF_U][p] * s[WF_MUU][c] / s[WF_MSFU][c];
-      s[WF_CQU][p] = 1.0f / (1.0f + 0.5f * (qsum7(moist, n3, p) + qsum7(moist, n3, p - 1)));
-    }
-    if (j >= jds && j < jde && mcol) {
-      s[WF_RV][p] = s[WF_V][p] * s[WF_MUV][c] * s[WF_MSFVX_INV][c];
-      s[WF_CQV][p] = 1.0f / (1.0f + 0.5f * (qsum7(moist, n3, p) + qsum7(moist, n3, p - g.nx)));
-    }
-    if (mrow && mcol) {
-      s[WF_ALT][p] = s[WF_AL][p] + s[WF_ALB][p];
-      const float* phb = s[WF_PHB];
-      const float* ph = s[WF_PH];
-      const int q = p + g.ny * g.nx;
-      s[WF_PHP][p] = 0.5f * (phb[p] + phb[q] + ph[p] + ph[q]);
-      if (k >= 1) s[WF_CQW][p] = 0.5f * (qsum7(moist, n3, p) + qsum7(moist, n3, p - g.ny * g.nx));
-    }
+  const bool du = k < nz - 1 && mrow && i >= ids && i < ide;
+  const bool dv = k < nz - 1 && j >= jds && j < jde && mcol;
+  const bool dm = k < nz - 1 && mrow && mcol;
+  const bool dw = dm && k >= 1;
+  const bool dr = mrow && mcol;
+  const float qp = (du || dv || dw) ? qsum7(moist, n3, p) : 0.f;
+  const float qw = du ? qsum7(moist, n3, p - 1) : 0.f;
+  const float qs = dv ? qsum7(moist, n3, p - g.nx) : 0.f;
+  const float qb = dw ? qsum7(moist, n3, p - lev) : 0.f;
+  float uu = 0.f, muu = 0.f, mfu = 1.f, vv = 0.f, muv = 0.f, mvxi = 0.f;
+  if (du) {
+    uu = s[WF_U][p];
+    muu = s[WF_MUU][c];
+    mfu = s[WF_MSFU][c];
   }
-  if (mrow && mcol) s[WF_RW][p] = s[WF_W][p] * s[WF_MUT][c] / s[WF_MSFT][c];
+  if (dv) {
+    vv = s[WF_V][p];
+    muv = s[WF_MUV][c];
+    mvxi = s[WF_MSFVX_INV][c];
+  }
+  float alv = 0.f, albv = 0.f, phb0 = 0.f, phb1 = 0.f, ph0 = 0.f, ph1 = 0.f;
+  if (dm) {
+    alv = s[WF_AL][p];
+    albv = s[WF_ALB][p];
+    phb0 = s[WF_PHB][p];
+    phb1 = s[WF_PHB][p + lev];
+    ph0 = s[WF_PH][p];
+    ph1 = s[WF_PH][p + lev];
+  }
+  float wv = 0.f, mutv = 0.f, mft = 1.f;
+  if (dr) {
+    wv = s[WF_W][p];
+    mutv = s[WF_MUT][c];
+    mft = s[WF_MSFT][c];
+  }
+  if (du) {
+    s[WF_RU][p] = uu * muu / mfu;
+    s[WF_CQU][p] = 1.0f / (1.0f + 0.5f * (qp + qw));
+  }
+  if (dv) {
+    s[WF_RV][p] = vv * muv * mvxi;
+    s[WF_CQV][p] = 1.0f / (1.0f + 0.5f * (qp + qs));
+  }
+  if (dm) {
+    s[WF_ALT][p] = alv + albv;
+    s[WF_PHP][p] = 0.5f * (phb0 + phb1 + ph0 + ph1);
+    if (k >= 1) s[WF_CQW][p] = 0.5f * (qp + qb);
+  }
+  if (dr) s[WF_RW][p] = wv * mutv / mft;
 }
 
 // calc_ww_cp: a block owns 16 adjacent mass columns of one row and 16 level

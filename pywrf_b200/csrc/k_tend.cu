@@ -477,45 +477,102 @@ __global__ void k_addtend(Grid g, S s, int rk_step) {
     if (j >= jds && j < jbe && i == ids) t = xs0(btxs + 0, k, j);
     if (j >= jds && j < jbe && i == ibe - 1) t = xs0(btxs + 1, k, j);
   };
-  if (k < nz - 1 && j >= jds && j < jde - 1 && i >= ids && i < ide) {  // u
-    float tf = s[WF_RU_TENDF][p];
-    if (rk_step == 1) { tf = tf + s[WF_U_SAVE][p] * s[WF_MSFUY][c]; s[WF_RU_TENDF][p] = tf; }
-    float t = s[WF_RU_TEND][p] + tf / s[WF_MSFUY][c];
-    spec(t, WF_U_BTXS, ide, jde - 1);
-    s[WF_RU_TEND][p] = t;
+  // operands first, then the specified-row overrides, then the stores (a
+  // store would hold back the later fields' loads)
+  const bool r1 = rk_step == 1;
+  const bool du = k < nz - 1 && j >= jds && j < jde - 1 && i >= ids && i < ide;
+  const bool dv = k < nz - 1 && j >= jds && j < jde && i >= ids && i < ide - 1;
+  const bool dt = mass && k < nz - 1;
+  const bool dmu = mass && k == 0;
+  float tfu = 0.f, usv = 0.f, mfuy = 1.f, rtu = 0.f;
+  if (du) {
+    tfu = s[WF_RU_TENDF][p];
+    mfuy = s[WF_MSFUY][c];
+    if (r1) usv = s[WF_U_SAVE][p];
+    rtu = s[WF_RU_TEND][p];
   }
-  if (k < nz - 1 && j >= jds && j < jde && i >= ids && i < ide - 1) {  // v
-    float tf = s[WF_RV_TENDF][p];
-    if (rk_step == 1) { tf = tf + s[WF_V_SAVE][p] * s[WF_MSFVX][c]; s[WF_RV_TENDF][p] = tf; }
-    float t = s[WF_RV_TEND][p] + tf * s[WF_MSFVX_INV][c];
-    spec(t, WF_V_BTXS, ide - 1, jde);
-    s[WF_RV_TEND][p] = t;
+  float tfv = 0.f, vsv = 0.f, mfvx = 0.f, mvxi = 0.f, rtv = 0.f;
+  if (dv) {
+    tfv = s[WF_RV_TENDF][p];
+    if (r1) {
+      vsv = s[WF_V_SAVE][p];
+      mfvx = s[WF_MSFVX][c];
+    }
+    mvxi = s[WF_MSFVX_INV][c];
+    rtv = s[WF_RV_TEND][p];
+  }
+  float msfty = 1.f, tfw = 0.f, wsv = 0.f, rtw = 0.f, tfp = 0.f, phs = 0.f, rtp = 0.f;
+  float tft = 0.f, tsv = 0.f, rtt = 0.f, mutc = 0.f, hd = 0.f, mut0 = 0.f, mutf0 = 0.f;
+  if (mass) {
+    msfty = s[WF_MSFTY][c];
+    tfw = s[WF_RW_TENDF][p];
+    rtw = s[WF_RW_TEND][p];
+    tfp = s[WF_PH_TENDF][p];
+    rtp = s[WF_PH_TEND][p];
+    if (r1) {
+      wsv = s[WF_W_SAVE][p];
+      phs = s[WF_PH_SAVE][p];
+    }
+  }
+  if (dt) {
+    tft = s[WF_T_TENDF][p];
+    if (r1) tsv = s[WF_T_SAVE][p];
+    rtt = s[WF_T_TEND][p];
+    mutc = s[WF_MUT][c];
+    hd = s[WF_H_DIABATIC][p];
+  }
+  if (dmu) {
+    mut0 = s[WF_MU_TEND][c];
+    mutf0 = s[WF_MU_TENDF][c];
+  }
+  float ou = 0.f, ov = 0.f, ow = 0.f, oph = 0.f, ot = 0.f, omu = 0.f;
+  if (du) {  // u
+    if (r1) tfu = tfu + usv * mfuy;
+    ou = rtu + tfu / mfuy;
+    spec(ou, WF_U_BTXS, ide, jde - 1);
+  }
+  if (dv) {  // v
+    if (r1) tfv = tfv + vsv * mfvx;
+    ov = rtv + tfv * mvxi;
+    spec(ov, WF_V_BTXS, ide - 1, jde);
   }
   if (mass) {
-    const float msfty = s[WF_MSFTY][c];
-    float tf = s[WF_RW_TENDF][p];
-    if (rk_step == 1) { tf = tf + s[WF_W_SAVE][p] * msfty; s[WF_RW_TENDF][p] = tf; }
-    s[WF_RW_TEND][p] = s[WF_RW_TEND][p] + tf / msfty;
-    tf = s[WF_PH_TENDF][p];
-    if (rk_step == 1) { tf = tf + s[WF_PH_SAVE][p]; s[WF_PH_TENDF][p] = tf; }
-    float t = s[WF_PH_TEND][p] + tf / msfty;
-    spec(t, WF_PH_BTXS, ide - 1, jde - 1);
-    s[WF_PH_TEND][p] = t;
-    if (k < nz - 1) {
-      tf = s[WF_T_TENDF][p];
-      if (rk_step == 1) { tf = tf + s[WF_T_SAVE][p]; s[WF_T_TENDF][p] = tf; }
-      t = s[WF_T_TEND][p] + tf / msfty + s[WF_MUT][c] * s[WF_H_DIABATIC][p] / msfty;
-      spec(t, WF_T_BTXS, ide - 1, jde - 1);
-      s[WF_T_TEND][p] = t;
-    }
-    if (k == 0) {
-      t = s[WF_MU_TEND][c] + s[WF_MU_TENDF][c];
-      spec(t, WF_MU_BTXS, ide - 1, jde - 1);
-      s[WF_MU_TEND][c] = t;
-    }
-  } else if (k < nz) {
-    // specified rows that lie outside the mass region (none for mass fields)
+    if (r1) tfw = tfw + wsv * msfty;
+    ow = rtw + tfw / msfty;
+    if (r1) tfp = tfp + phs;
+    oph = rtp + tfp / msfty;
+    spec(oph, WF_PH_BTXS, ide - 1, jde - 1);
   }
+  if (dt) {
+    if (r1) tft = tft + tsv;
+    ot = rtt + tft / msfty + mutc * hd / msfty;
+    spec(ot, WF_T_BTXS, ide - 1, jde - 1);
+  }
+  if (dmu) {
+    omu = mut0 + mutf0;
+    spec(omu, WF_MU_BTXS, ide - 1, jde - 1);
+  }
+  if (du) {
+    if (r1) s[WF_RU_TENDF][p] = tfu;
+    s[WF_RU_TEND][p] = ou;
+  }
+  if (dv) {
+    if (r1) s[WF_RV_TENDF][p] = tfv;
+    s[WF_RV_TEND][p] = ov;
+  }
+  if (mass) {
+    if (r1) {
+      s[WF_RW_TENDF][p] = tfw;
+      s[WF_PH_TENDF][p] = tfp;
+    }
+    s[WF_RW_TEND][p] = ow;
+    s[WF_PH_TEND][p] = oph;
+  }
+  if (dt) {
+    if (r1) s[WF_T_TENDF][p] = tft;
+    s[WF_T_TEND][p] = ot;
+  }
+  if (dmu) s[WF_MU_TEND][c] = omu;
 }
 
 // stand-alone advect_scalar on caller arrays (s carries msftx, fnm, fnp, rdnw)
