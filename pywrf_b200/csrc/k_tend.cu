@@ -593,7 +593,7 @@ int launch_advect_forces(const Grid& g, const S& s, cudaStream_t st) {
   int n = launch_advect_mom_tma(g, s, 0, 3, st);
   if (n == 0) n = launch_advect_mom_point(g, s, 7, st);
   n += launch_advect_theta_tiled(g, s, st);
-  k_forces<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  if (launch_forces_tma(g, s, st) == 0) k_forces<<<point_grid(g, b3), b3, 0, st>>>(g, s);
   return n + 1;
 }
 

@@ -28,6 +28,10 @@ int launch_relax_qv(const Grid& g, const S& s, cudaStream_t st);
 // advection of u, v, w, theta and the pressure-gradient / buoyancy /
 // Coriolis / curvature forces (k_tend.cu)
 int launch_advect_forces(const Grid& g, const S& s, cudaStream_t st);
+// k_forces in its tiled tensor-map form (k_forces_tma.cu); 0 (nothing
+// launched) when nx is not a multiple of 4, a map is refused or the point form
+// is selected
+int launch_forces_tma(const Grid& g, const S& s, cudaStream_t st);
 // rk_addtend_dry + spec_bdytend (k_tend.cu)
 int launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st);
 // moisture advection with the time-averaged fluxes (k_tend.cu)
