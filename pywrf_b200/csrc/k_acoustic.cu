@@ -285,19 +285,23 @@ __global__ void k_advance_uv(Grid g, S s, float dts) {
 constexpr int kUvTX = 32, kUvTY = 8, kUvBW = 40, kUvBH = kUvTY + 1;
 constexpr int kUvNB = 6;                 // boxes per level: alt al pb php (k), ph p (k+1)
 constexpr int kUvSlot = 384;             // floats per box slot (1536 B >= 40 x 9 x 4)
+constexpr int kUvOW = 36, kUvOH = kUvTY;  // the thread's own u, ru_tend, v, rv_tend, cqu, cqv at k
+constexpr int kUvNO = 6, kUvOSlot = kUvOW * kUvOH;  // 1152 B, a 128-byte multiple
 constexpr int kUvRing = 3, kUvKCH = 7;
-constexpr uint32_t kUvBytes = kUvBW * kUvBH * 4;
+constexpr uint32_t kUvBytes = kUvNB * kUvBW * kUvBH * 4 + kUvNO * kUvOW * kUvOH * 4;
 constexpr long long kUvWaitCycles = 4000000000LL;
-static_assert(kUvBytes <= kUvSlot * 4, "a ring slot holds one box");
+static_assert(kUvBW * kUvBH <= kUvSlot && (kUvOSlot * 4) % 128 == 0, "ring slots hold one box, 128-byte aligned");
 
 struct UvTmaArgs {
   CUtensorMap alt, al, pb, php, ph, pp;
+  CUtensorMap own[kUvNO];  // u, ru_tend, v, rv_tend, cqu, cqv
   int nchunk;
 };
 
 __global__ void __launch_bounds__(kUvTX * kUvTY, 4) k_advance_uv_tma(Grid g, S s, float dts,
                                                                      const __grid_constant__ UvTmaArgs a) {
   __shared__ __align__(128) float box[kUvRing][kUvNB][kUvSlot];
+  __shared__ __align__(128) float obox[kUvRing][kUvNO][kUvOSlot];
   __shared__ uint64_t bar[kUvRing];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kUvTX + tx;
   const int nx = g.nx, ny = g.ny, nz = g.nz, ktf = nz - 1;
@@ -305,6 +309,7 @@ __global__ void __launch_bounds__(kUvTX * kUvTY, 4) k_advance_uv_tma(Grid g, S s
   const int i0 = ids + blockIdx.x * kUvTX, j0 = jds + blockIdx.y * kUvTY;
   const int i = i0 + tx, j = j0 + ty;
   const int mx = (i0 - 1) & ~3, om = i0 - mx;
+  const int ox = i0 & ~3, oo = i0 - ox;
   const int k0 = blockIdx.z * ktf / a.nchunk, k1 = (blockIdx.z + 1) * ktf / a.nchunk;
   const size_t lev = (size_t)ny * nx;
   const bool uin = j >= jds + 1 && j < jde - 2 && i >= ids + 1 && i < ide - 1;
@@ -322,10 +327,6 @@ __global__ void __launch_bounds__(kUvTX * kUvTY, 4) k_advance_uv_tma(Grid g, S s
   const float* rdnw = s[WF_RDNW];
   float* U = s[WF_U];
   float* V = s[WF_V];
-  const float* rut = s[WF_RU_TEND];
-  const float* rvt = s[WF_RV_TEND];
-  const float* cqu = s[WF_CQU];
-  const float* cqv = s[WF_CQV];
   const float rdx = g.rdx, rdy = g.rdy;
 
   if (tid == 0) {
@@ -334,13 +335,14 @@ __global__ void __launch_bounds__(kUvTX * kUvTY, 4) k_advance_uv_tma(Grid g, S s
   }
   __syncthreads();
   auto issue = [&](int k, int r) {
-    tma::mbar_expect_tx(&bar[r], kUvNB * kUvBytes);
+    tma::mbar_expect_tx(&bar[r], kUvBytes);
     tma::load_4d(box[r][0], &a.alt, mx, j0 - 1, k, 0, &bar[r]);
     tma::load_4d(box[r][1], &a.al, mx, j0 - 1, k, 0, &bar[r]);
     tma::load_4d(box[r][2], &a.pb, mx, j0 - 1, k, 0, &bar[r]);
     tma::load_4d(box[r][3], &a.php, mx, j0 - 1, k, 0, &bar[r]);
     tma::load_4d(box[r][4], &a.ph, mx, j0 - 1, k + 1, 0, &bar[r]);
     tma::load_4d(box[r][5], &a.pp, mx, j0 - 1, k + 1, 0, &bar[r]);
+    for (int f = 0; f < kUvNO; ++f) tma::load_4d(obox[r][f], &a.own[f], ox, j0, k, 0, &bar[r]);
   };
   int hi = k0 - 1;
   if (tid == 0) {
@@ -391,24 +393,11 @@ __global__ void __launch_bounds__(kUvTX * kUvTY, 4) k_advance_uv_tma(Grid g, S s
       dpn_v = 0.5f * (fm * (p_c + p_s) + fp * (__ldg(&pp[qm + c]) + __ldg(&pp[qm + cs])));
     }
   }
-  // the thread's own values at the next level, loaded a level ahead
-  auto own = [&](int k, float& u, float& rt, float& v, float& vt, float& qu, float& qv) {
-    const size_t p = (size_t)k * lev + c;
-    u = wu ? U[p] : 0.f;
-    rt = wu ? __ldg(&rut[p]) : 0.f;
-    qu = uin ? __ldg(&cqu[p]) : 0.f;
-    v = wv ? V[p] : 0.f;
-    vt = wv ? __ldg(&rvt[p]) : 0.f;
-    qv = vin ? __ldg(&cqv[p]) : 0.f;
-  };
-  float u0, rt0, v0, vt0, qu0, qv0;
-  own(k0, u0, rt0, v0, vt0, qu0, qv0);
   const int oA = (ty + 1) * kUvBW + om + tx;
+  const int oO = ty * kUvOW + oo + tx;  // (j, i) in an own-value box
   int kstop = k1, slot = 0;
   uint32_t par = 0;
   for (int k = k0; k < k1; ++k) {
-    float u1 = 0.f, rt1 = 0.f, v1 = 0.f, vt1 = 0.f, qu1 = 0.f, qv1 = 0.f;
-    if (k + 1 < k1) own(k + 1, u1, rt1, v1, vt1, qu1, qv1);
     const float rdk = __ldg(&rdnw[k]);
     const float fm1 = k + 1 < nz - 1 ? __ldg(&fnm[k + 1]) : 0.f, fp1 = k + 1 < nz - 1 ? __ldg(&fnp[k + 1]) : 0.f;
     const bool ok = tma::mbar_wait_bounded(&bar[slot], par, kUvWaitCycles);
@@ -423,6 +412,8 @@ __global__ void __launch_bounds__(kUvTX * kUvTY, 4) k_advance_uv_tma(Grid g, S s
     }
     const float* B = box[slot][0];
     const size_t p = (size_t)k * lev + c;
+    const float u0 = obox[slot][0][oO], rt0 = obox[slot][1][oO], v0 = obox[slot][2][oO];
+    const float vt0 = obox[slot][3][oO], qu0 = obox[slot][4][oO], qv0 = obox[slot][5][oO];
     float pu_c = 0.f, pu_w = 0.f, pu_s = 0.f, hu_c = 0.f, hu_w = 0.f, hu_s = 0.f;
     if (uin || vin) {
       hu_c = B[4 * kUvSlot + oA];
@@ -469,12 +460,6 @@ __global__ void __launch_bounds__(kUvTX * kUvTY, 4) k_advance_uv_tma(Grid g, S s
     p_c = pu_c;
     p_w = pu_w;
     p_s = pu_s;
-    u0 = u1;
-    rt0 = rt1;
-    v0 = v1;
-    vt0 = vt1;
-    qu0 = qu1;
-    qv0 = qv1;
     if (++slot == kUvRing) {
       slot = 0;
       par ^= 1u;
@@ -1119,6 +1104,9 @@ int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st) {
     CUtensorMap* m[6] = {&a.alt, &a.al, &a.pb, &a.php, &a.ph, &a.pp};
     bool ok = true;
     for (int e = 0; e < 6 && ok; ++e) ok = tma::encode_f32_4d(m[e], s[f[e]], g.nx, g.ny, g.nz, 1, kUvBW, kUvBH, &err);
+    const int fo[kUvNO] = {WF_U, WF_RU_TEND, WF_V, WF_RV_TEND, WF_CQU, WF_CQV};
+    for (int e = 0; e < kUvNO && ok; ++e)
+      ok = tma::encode_f32_4d(&a.own[e], s[fo[e]], g.nx, g.ny, g.nz, 1, kUvOW, kUvOH, &err);
     if (ok) {
       a.nchunk = min((g.nz - 1 + kUvKCH - 1) / kUvKCH, g.nz - 1);
       const dim3 gr((g.ide + 1 - g.ids + kUvTX - 1) / kUvTX, (g.jde - g.jds + kUvTY - 1) / kUvTY, a.nchunk);
