@@ -5,6 +5,7 @@
 // allocates nothing and never synchronises (a probe callback may).  The
 // boundary time of the step is derived on the device from the step counter
 // STATUS[WRF_ST_STEP], so one captured CUDA graph replays every step.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -93,6 +94,31 @@ __global__ void k_step_begin(float* dscal, const int* status, int bdy_interval, 
 
 __global__ void k_step_end(int* status) { status[WRF_ST_STEP] += 1; }
 
+// zeroes a batch of fields in one launch (in place of one memset node per
+// field in the captured step): blockIdx.y picks the field, the blocks of x
+// stride over it with 16-byte stores
+constexpr int kZeroMax = 16;
+struct ZeroBatch {
+  float* p[kZeroMax];
+  unsigned long long n[kZeroMax];  // floats
+  int count;
+};
+__global__ void __launch_bounds__(256) k_zero_batch(ZeroBatch b) {
+  const int f = blockIdx.y;
+  float* p = b.p[f];
+  const unsigned long long n = b.n[f];
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long t0 = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) {
+    const unsigned long long n4 = n / 4;
+    float4* q = reinterpret_cast<float4*>(p);
+    for (unsigned long long e = t0; e < n4; e += stride) q[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (unsigned long long e = n4 * 4 + t0; e < n; e += stride) p[e] = 0.f;
+  } else {
+    for (unsigned long long e = t0; e < n; e += stride) p[e] = 0.f;
+  }
+}
+
 struct Driver {
   Grid g;
   S s;
@@ -104,17 +130,24 @@ struct Driver {
   int rc = WRF_OK;
   int n = 0;  // kernels enqueued
 
-  size_t b3() const { return g.n3() * sizeof(float); }
-  size_t b2() const { return g.n2() * sizeof(float); }
 
   bool ok(const char* where) {
     if (rc != WRF_OK) return false;
     rc = check_launch(where);
     return rc == WRF_OK;
   }
-  void zero3(int id) { if (rc == WRF_OK && cudaMemsetAsync(s[id], 0, b3(), st) != cudaSuccess) rc = check_launch("memset"); }
-  void zero2(int id) { if (rc == WRF_OK && cudaMemsetAsync(s[id], 0, b2(), st) != cudaSuccess) rc = check_launch("memset"); }
-  void zero4(int id) { if (rc == WRF_OK && cudaMemsetAsync(s[id], 0, 7 * b3(), st) != cudaSuccess) rc = check_launch("memset"); }
+  // zero the listed fields (id, kind: 3 = [nz][ny][nx], 2 = [ny][nx], 4 = the 7 moisture slots) in one launch
+  void zero(std::initializer_list<std::pair<int, int>> fields) {
+    if (rc != WRF_OK) return;
+    ZeroBatch b{};
+    for (auto& e : fields) {
+      b.p[b.count] = s[e.first];
+      b.n[b.count] = e.second == 2 ? g.n2() : (e.second == 4 ? 7 * g.n3() : g.n3());
+      ++b.count;
+    }
+    k_zero_batch<<<dim3(std::min<unsigned>(592u, (unsigned)((g.n3() / 4 + 255) / 256)), b.count), 256, 0, st>>>(b);
+    ++n;
+  }
   void phase(const char* name) {
     if (!ok(name)) return;
     if (probe) probe(name, user);
@@ -167,9 +200,8 @@ struct Driver {
   // eddy viscosities (solver.py:880-985)
   void diff_stage1() {
     if (rc != WRF_OK) return;
-    zero3(WF_RU_TENDF); zero3(WF_RV_TENDF); zero3(WF_RW_TENDF); zero3(WF_PH_TENDF); zero3(WF_T_TENDF);
-    zero2(WF_MU_TENDF);
-    zero4(WF_MOIST_TEND);
+    zero({{WF_RU_TENDF, 3}, {WF_RV_TENDF, 3}, {WF_RW_TENDF, 3}, {WF_PH_TENDF, 3}, {WF_T_TENDF, 3}, {WF_MU_TENDF, 2},
+          {WF_MOIST_TEND, 4}});
     n += launch_diff_metrics(g, s, st);
     bc({{WF_RDZW, 'w'}, {WF_ZX, 'e'}, {WF_ZY, 'f'}});
     n += launch_km(g, s, st);
@@ -181,9 +213,8 @@ struct Driver {
   void tend_stage(int rk) {
     if (rc != WRF_OK) return;
     char tag[32];
-    zero3(WF_RU_TEND); zero3(WF_RV_TEND); zero3(WF_RW_TEND); zero3(WF_T_TEND); zero3(WF_PH_TEND);
-    zero3(WF_U_SAVE); zero3(WF_V_SAVE); zero3(WF_W_SAVE); zero3(WF_PH_SAVE); zero3(WF_T_SAVE);
-    zero2(WF_MU_TEND); zero2(WF_MU_SAVE);
+    zero({{WF_RU_TEND, 3}, {WF_RV_TEND, 3}, {WF_RW_TEND, 3}, {WF_T_TEND, 3}, {WF_PH_TEND, 3}, {WF_U_SAVE, 3},
+          {WF_V_SAVE, 3}, {WF_W_SAVE, 3}, {WF_PH_SAVE, 3}, {WF_T_SAVE, 3}, {WF_MU_TEND, 2}, {WF_MU_SAVE, 2}});
     n += launch_advect_forces(g, s, st);
     snprintf(tag, sizeof tag, "s%d.forces", rk);
     phase(tag);
