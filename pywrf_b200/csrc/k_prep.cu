@@ -406,8 +406,42 @@ __global__ void k_hdiff(Grid g, S s) {
 
 // relaxation of u, v, ph (mass-weighted), theta (mass-weighted) and mu at
 // the first RK stage (pywrf/solver.py:1143-1203)
-__global__ void k_relax(Grid g, S s) {
-  WRF_POINT_INDEX(g, k, j, i);
+// The lateral relaxation and the specified rows only act on points within a
+// few cells of the domain edge.  In ring mode a kernel runs one thread per
+// point of the band: rows [jds, jds+5) and [jde-5, jde) over columns
+// [ids, ide], then columns [ids, ids+5) and [ide-5, ide] of the rows
+// between - every point those updates touch, once, when the domain spans at
+// least 10 rows and 11 columns (else the kernels run over every point).
+__device__ __forceinline__ bool ring_point(const Grid& g, int r, int& j, int& i) {
+  const int w = g.ide + 1 - g.ids;
+  if (r < 10 * w) {
+    const int rr = r / w;
+    i = g.ids + (r - rr * w);
+    j = rr < 5 ? g.jds + rr : g.jde - 10 + rr;
+    return true;
+  }
+  r -= 10 * w;
+  if (r >= (g.jde - g.jds - 10) * 11) return false;
+  const int cc = r % 11;
+  j = g.jds + 5 + r / 11;
+  i = cc < 5 ? g.ids + cc : g.ide - 10 + cc;
+  return true;
+}
+bool ring_fits(const Grid& g) { return g.jde - g.jds >= 10 && g.ide - g.ids >= 11; }
+int ring_size(const Grid& g) { return 10 * (g.ide + 1 - g.ids) + (g.jde - g.jds - 10) * 11; }
+
+// (k, j, i) of this thread, in ring mode or over every point; false when none
+__device__ __forceinline__ bool relax_index(const Grid& g, int ring, int& k, int& j, int& i) {
+  k = blockIdx.z;
+  if (ring) return ring_point(g, blockIdx.x * blockDim.x + threadIdx.x, j, i);
+  i = blockIdx.x * blockDim.x + threadIdx.x;
+  j = blockIdx.y * blockDim.y + threadIdx.y;
+  return i < g.nx && j < g.ny;
+}
+
+__global__ void k_relax(Grid g, S s, int ring) {
+  int k, j, i;
+  if (!relax_index(g, ring, k, j, i)) return;
   const float dtbc = s[WF_DSCAL][DS_DTBC];
   const int nz = g.nz;
   const size_t lev = (size_t)g.ny * g.nx;
@@ -444,8 +478,9 @@ __global__ void k_relax(Grid g, S s) {
 
 // relaxation + specified tendency of qv at the first stage (relax_bdy_scalar,
 // spec_bdy_scalar: wrf_boundary.py:413-467, 189-241); rq = qv * mut
-__global__ void k_relax_qv(Grid g, S s) {
-  WRF_POINT_INDEX(g, k, j, i);
+__global__ void k_relax_qv(Grid g, S s, int ring) {
+  int k, j, i;
+  if (!relax_index(g, ring, k, j, i)) return;
   if (k >= g.nz - 1) return;
   const float dtbc = s[WF_DSCAL][DS_DTBC];
   const size_t n3 = g.n3();
@@ -505,13 +540,19 @@ int launch_diff_metrics(const Grid& g, const S& s, cudaStream_t st) {
 int launch_hdiff_relax(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_hdiff<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  k_relax<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  if (ring_fits(g))
+    k_relax<<<dim3((ring_size(g) + 127) / 128, 1, g.nz), 128, 0, st>>>(g, s, 1);
+  else
+    k_relax<<<point_grid(g, b3), b3, 0, st>>>(g, s, 0);
   return 2;
 }
 
 int launch_relax_qv(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
-  k_relax_qv<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  if (ring_fits(g))
+    k_relax_qv<<<dim3((ring_size(g) + 127) / 128, 1, g.nz), 128, 0, st>>>(g, s, 1);
+  else
+    k_relax_qv<<<point_grid(g, b3), b3, 0, st>>>(g, s, 0);
   return 1;
 }
 
