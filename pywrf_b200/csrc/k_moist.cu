@@ -84,6 +84,22 @@ __global__ void k_eos_flowdep(Grid g, S s, int do_flowdep) {
   const int c = g.i2(j, i);
   const size_t p = k * lev + c;
   const int its = g.ids, jts = g.jds, itf = g.ide - 1, jtf = g.jde - 1;
+  // the equation of state's operands, loaded before the flow-dependent
+  // boundary copies store (they write other moisture slots)
+  const bool eos = k < nz - 1 && j >= jts && j < g.jde - 1 && i >= its && i < g.ide - 1;
+  float phu = 0.f, phk = 0.f, muts = 1.f, mu = 0.f, alb = 0.f, rdk = 0.f, qv = 0.f, tk = 0.f, pbk = 0.f;
+  if (eos) {
+    const float* ph = s[WF_PH];
+    phu = ph[p + lev];
+    phk = ph[p];
+    muts = s[WF_MUTS][c];
+    mu = s[WF_MU][c];
+    alb = s[WF_ALB][p];
+    rdk = s[WF_RDNW][k];
+    qv = s[WF_MOIST][n3 + p];
+    tk = s[WF_T][p];
+    pbk = s[WF_PB][p];
+  }
   if (do_flowdep && k < nz - 1) {
     // zero inflow / zero-gradient outflow for qc..qg on the outer row
     const float* um = s[WF_RU_M];
@@ -112,22 +128,27 @@ __global__ void k_eos_flowdep(Grid g, S s, int do_flowdep) {
       }
     }
   }
-  if (k < nz - 1 && j >= jts && j < g.jde - 1 && i >= its && i < g.ide - 1) {
-    const float* ph = s[WF_PH];
-    const float muts = s[WF_MUTS][c], mu = s[WF_MU][c];
-    const float alb = s[WF_ALB][p];
-    const float al = -1.0f / muts * (alb * mu + s[WF_RDNW][k] * (ph[p + lev] - ph[p]));
+  if (eos) {
+    const float al = -1.0f / muts * (alb * mu + rdk * (phu - phk));
+    const float qvf = 1.0f + (float)RVOVRD * qv;
+    const float temp = ((float)R_D * ((float)T0 + tk) * qvf) / ((float)P0 * (al + alb));
+    const float pv = wpow_eos(temp, (float)CPOVCV) * (float)P0 - pbk;
     s[WF_AL][p] = al;
-    const float qvf = 1.0f + (float)RVOVRD * s[WF_MOIST][n3 + p];
-    const float temp = ((float)R_D * ((float)T0 + s[WF_T][p]) * qvf) / ((float)P0 * (al + alb));
-    const float pv = wpow_eos(temp, (float)CPOVCV) * (float)P0 - s[WF_PB][p];
     s[WF_P][p] = pv;
     if (isnan(pv)) atomicAdd(reinterpret_cast<int*>(s[WF_STATUS]) + WRF_ST_NAN_P, 1);
   }
 }
 
-__global__ void k_bdy_final(Grid g, S s) {
-  WRF_POINT_INDEX(g, k, j, i);
+__global__ void k_bdy_final(Grid g, S s, int ring) {
+  int k, j, i;
+  k = blockIdx.z;
+  if (ring) {
+    if (!ring_point(g, blockIdx.x * blockDim.x + threadIdx.x, j, i)) return;
+  } else {
+    i = blockIdx.x * blockDim.x + threadIdx.x;
+    j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+  }
   const int nz = g.nz, nx = g.nx, ny = g.ny;
   const size_t lev = (size_t)ny * nx, n3 = g.n3();
   const int c = g.i2(j, i);
@@ -204,7 +225,10 @@ int launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st) {
 
 int launch_bdy_final(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);
-  k_bdy_final<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  if (ring_fits(g))
+    k_bdy_final<<<dim3((ring_size(g) + 127) / 128, 1, g.nz), 128, 0, st>>>(g, s, 1);
+  else
+    k_bdy_final<<<point_grid(g, b3), b3, 0, st>>>(g, s, 0);
   k_w_surface<<<col_grid(g, b2), b2, 0, st>>>(g, s);
   return 2;
 }

@@ -406,30 +406,6 @@ __global__ void k_hdiff(Grid g, S s) {
 
 // relaxation of u, v, ph (mass-weighted), theta (mass-weighted) and mu at
 // the first RK stage (pywrf/solver.py:1143-1203)
-// The lateral relaxation and the specified rows only act on points within a
-// few cells of the domain edge.  In ring mode a kernel runs one thread per
-// point of the band: rows [jds, jds+5) and [jde-5, jde) over columns
-// [ids, ide], then columns [ids, ids+5) and [ide-5, ide] of the rows
-// between - every point those updates touch, once, when the domain spans at
-// least 10 rows and 11 columns (else the kernels run over every point).
-__device__ __forceinline__ bool ring_point(const Grid& g, int r, int& j, int& i) {
-  const int w = g.ide + 1 - g.ids;
-  if (r < 10 * w) {
-    const int rr = r / w;
-    i = g.ids + (r - rr * w);
-    j = rr < 5 ? g.jds + rr : g.jde - 10 + rr;
-    return true;
-  }
-  r -= 10 * w;
-  if (r >= (g.jde - g.jds - 10) * 11) return false;
-  const int cc = r % 11;
-  j = g.jds + 5 + r / 11;
-  i = cc < 5 ? g.ids + cc : g.ide - 10 + cc;
-  return true;
-}
-bool ring_fits(const Grid& g) { return g.jde - g.jds >= 10 && g.ide - g.ids >= 11; }
-int ring_size(const Grid& g) { return 10 * (g.ide + 1 - g.ids) + (g.jde - g.jds - 10) * 11; }
-
 // (k, j, i) of this thread, in ring mode or over every point; false when none
 __device__ __forceinline__ bool relax_index(const Grid& g, int ring, int& k, int& j, int& i) {
   k = blockIdx.z;

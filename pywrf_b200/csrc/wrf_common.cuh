@@ -110,6 +110,30 @@ __device__ __forceinline__ float flux5(float qm3, float qm2, float qm1, float q0
   const int j = blockIdx.y * blockDim.y + threadIdx.y;       \
   if (i >= (g).nx || j >= (g).ny) return;
 
+// The lateral relaxation, the specified rows and the final boundary values
+// only act on points within a few cells of the domain edge.  In ring mode a kernel runs one thread per
+// point of the band: rows [jds, jds+5) and [jde-5, jde) over columns
+// [ids, ide], then columns [ids, ids+5) and [ide-5, ide] of the rows
+// between - every point those updates touch, once, when the domain spans at
+// least 10 rows and 11 columns (else the kernels run over every point).
+__device__ __forceinline__ bool ring_point(const Grid& g, int r, int& j, int& i) {
+  const int w = g.ide + 1 - g.ids;
+  if (r < 10 * w) {
+    const int rr = r / w;
+    i = g.ids + (r - rr * w);
+    j = rr < 5 ? g.jds + rr : g.jde - 10 + rr;
+    return true;
+  }
+  r -= 10 * w;
+  if (r >= (g.jde - g.jds - 10) * 11) return false;
+  const int cc = r % 11;
+  j = g.jds + 5 + r / 11;
+  i = cc < 5 ? g.ids + cc : g.ide - 10 + cc;
+  return true;
+}
+inline bool ring_fits(const Grid& g) { return g.jde - g.jds >= 10 && g.ide - g.ids >= 11; }
+inline int ring_size(const Grid& g) { return 10 * (g.ide + 1 - g.ids) + (g.jde - g.jds - 10) * 11; }
+
 inline dim3 point_grid(const Grid& g, dim3 b) { return dim3((g.nx + b.x - 1) / b.x, (g.ny + b.y - 1) / b.y, g.nz); }
 inline dim3 col_grid(const Grid& g, dim3 b) { return dim3((g.nx + b.x - 1) / b.x, (g.ny + b.y - 1) / b.y, 1); }
 
