@@ -30,13 +30,18 @@ __global__ void k_hdiff_moist(Grid g, S s) {
   const float mkrdym = (msfvy[c] * mvi[c]) * 0.5f * (K[p] + K[p - nx]) * 0.5f * (mut[c] + mut[c - nx]) * rdy;
   const float mkrdyp = (msfvy[c + nx] * mvi[c + nx]) * 0.5f * (K[p + nx] + K[p]) * 0.5f * (mut[c + nx] + mut[c]) * rdy;
   const float mrdy = s[WF_MSFTX][c] * s[WF_MSFTY][c] * rdy;
-  for (int m = 1; m < 7; ++m) {
-    const float* f = s[WF_MOIST] + m * n3;
-    float* tend = s[WF_MOIST_TEND] + m * n3;
+  // all six species' updates are formed before any is stored
+  float o[6];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const float* f = s[WF_MOIST] + (m + 1) * n3;
+    const float* tend = s[WF_MOIST_TEND] + (m + 1) * n3;
     const float fc = f[p];
-    tend[p] = tend[p] + (mrdx * (mkrdxp * (f[p + 1] - fc) - mkrdxm * (fc - f[p - 1])) +
-                         mrdy * (mkrdyp * (f[p + nx] - fc) - mkrdym * (fc - f[p - nx])));
+    o[m] = tend[p] + (mrdx * (mkrdxp * (f[p + 1] - fc) - mkrdxm * (fc - f[p - 1])) +
+                      mrdy * (mkrdyp * (f[p + nx] - fc) - mkrdym * (fc - f[p - nx])));
   }
+#pragma unroll
+  for (int m = 0; m < 6; ++m) s[WF_MOIST_TEND][(m + 1) * n3 + p] = o[m];
 }
 
 // every species' operands are loaded before any store, so that the loads of

@@ -237,21 +237,25 @@ __global__ void k_deform(Grid g, S s) {
   const float* zy = s[WF_ZY];
   const float* rdzw = s[WF_RDZW];
   const int nx = g.nx;
-  if (j >= jds && j < jde - 1 && i >= ids && i < ide - 1) {
+  // the three components are formed before any is stored
+  float o11 = 0.f, o22 = 0.f, o12 = 0.f;
+  const bool d1 = j >= jds && j < jde - 1 && i >= ids && i < ide - 1;
+  const bool d2 = j >= jds + 1 && j < jde - 1 && i >= ids + 1 && i < ide - 1;
+  if (d1) {
     const float mm = s[WF_MSFTX][c] * s[WF_MSFTY][c];
     HatPair hu{s[WF_U], s[WF_MSFUY], s[WF_MSFUY], c, c + 1};
     const float d = hatavg(g, s, hu, k + 1, lev, cft1, cft2) - hatavg(g, s, hu, k, lev, cft1, cft2);
     const float zsum = zx[p] + zx[p + 1] + zx[p + lev] + zx[p + lev + 1];
     float t1 = d * (0.25f * zsum * rdzw[p]);
     t1 = mm * (g.rdx * (hat(hu, k, lev, true) - hat(hu, k, lev, false)) - t1);
-    s[WF_DEFOR11][p] = 2.0f * t1;
+    o11 = 2.0f * t1;
     HatPair hv{s[WF_V], s[WF_MSFVX], s[WF_MSFVX], c, c + nx};
     const float dv = hatavg(g, s, hv, k + 1, lev, cft1, cft2) - hatavg(g, s, hv, k, lev, cft1, cft2);
     const float zys = zy[p] + zy[p + nx] + zy[p + lev] + zy[p + lev + nx];
     t1 = mm * (g.rdy * (hat(hv, k, lev, true) - hat(hv, k, lev, false)) - dv * (0.25f * zys * rdzw[p]));
-    s[WF_DEFOR22][p] = 2.0f * t1;
+    o22 = 2.0f * t1;
   }
-  if (j >= jds + 1 && j < jde - 1 && i >= ids + 1 && i < ide - 1) {
+  if (d2) {
     const float* msfux = s[WF_MSFUX];
     const float* msfvy = s[WF_MSFVY];
     const float mm = 0.25f * (msfux[c - nx] + msfux[c]) * (msfvy[c - 1] + msfvy[c]);
@@ -264,8 +268,13 @@ __global__ void k_deform(Grid g, S s) {
     d = hatavg(g, s, hv, k + 1, lev, cft1, cft2) - hatavg(g, s, hv, k, lev, cft1, cft2);
     rsum = rdzw[p] + rdzw[p - nx] + rdzw[p - nx - 1] + rdzw[p - 1];
     t1 = d * (0.25f * (zx[p - nx] + zx[p] + zx[p + lev - nx] + zx[p + lev]) * 0.25f * rsum);
-    s[WF_DEFOR12][p] = d12 + mm * (g.rdx * (hat(hv, k, lev, true) - hat(hv, k, lev, false)) - t1);
+    o12 = d12 + mm * (g.rdx * (hat(hv, k, lev, true) - hat(hv, k, lev, false)) - t1);
   }
+  if (d1) {
+    s[WF_DEFOR11][p] = o11;
+    s[WF_DEFOR22][p] = o22;
+  }
+  if (d2) s[WF_DEFOR12][p] = o12;
 }
 
 __global__ void k_defor12_bc(Grid g, S s) {
@@ -337,8 +346,11 @@ __global__ void k_hdiff(Grid g, S s) {
   const float* msfvx_inv = s[WF_MSFVX_INV];
   const float* K = s[WF_XKMH];
   const float rdx = g.rdx, rdy = g.rdy;
-  auto apply = [&](float* tend, const float* f, const float* base, float mkrdxm, float mkrdxp, float mrdx,
-                   float mkrdym, float mkrdyp, float mrdy) {
+  // the four updated tendencies are stored at the end, so that no store
+  // separates the parts' loads (they share mut, K and the map factors)
+  float o_u = 0.f, o_v = 0.f, o_w = 0.f, o_t = 0.f;
+  auto apply = [&](const float* tend, const float* f, const float* base, float mkrdxm, float mkrdxp, float mrdx,
+                   float mkrdym, float mkrdyp, float mrdy) -> float {
     float dxp, dxm, dyp, dym;
     const float fc = f[p];
     if (!base) {
@@ -350,9 +362,13 @@ __global__ void k_hdiff(Grid g, S s) {
       dyp = f[p + nx] - fc - base[p + nx] + b;
       dym = fc - f[p - nx] - b + base[p - nx];
     }
-    tend[p] = tend[p] + (mrdx * (mkrdxp * dxp - mkrdxm * dxm) + mrdy * (mkrdyp * dyp - mkrdym * dym));
+    return tend[p] + (mrdx * (mkrdxp * dxp - mkrdxm * dxm) + mrdy * (mkrdyp * dyp - mkrdym * dym));
   };
-  if (j >= jds + 1 && j < jde - 2 && i >= ids + 1 && i < ide - 1) {  // u
+  const bool du = j >= jds + 1 && j < jde - 2 && i >= ids + 1 && i < ide - 1;
+  const bool dv = j >= jds + 1 && j < jde - 1 && i >= ids + 1 && i < ide - 2;
+  const bool dw = k >= 1 && j >= jds + 1 && j < jde - 2 && i >= ids + 1 && i < ide - 2;
+  const bool dt = j >= jds + 1 && j < jde - 2 && i >= ids + 1 && i < ide - 2;
+  if (du) {  // u
     const float mkrdxm = (msftx[c - 1] / msfty[c - 1]) * mut[c - 1] * K[p - 1] * rdx;
     const float mkrdxp = (msftx[c] / msfty[c]) * mut[c] * K[p] * rdx;
     const float mrdx = msfux[c] * msfuy[c] * rdx;
@@ -363,9 +379,9 @@ __global__ void k_hdiff(Grid g, S s) {
                          (mut[c] + mut[c + nx] + mut[c + nx - 1] + mut[c - 1]) * 0.25f *
                          (K[p] + K[p + nx] + K[p + nx - 1] + K[p - 1]) * rdy;
     const float mrdy = msfux[c] * msfuy[c] * rdy;
-    apply(s[WF_RU_TENDF], s[WF_U], nullptr, mkrdxm, mkrdxp, mrdx, mkrdym, mkrdyp, mrdy);
+    o_u = apply(s[WF_RU_TENDF], s[WF_U], nullptr, mkrdxm, mkrdxp, mrdx, mkrdym, mkrdyp, mrdy);
   }
-  if (j >= jds + 1 && j < jde - 1 && i >= ids + 1 && i < ide - 2) {  // v
+  if (dv) {  // v
     const float mkrdxm = ((msfvx[c] + msfvx[c - 1]) / (msfvy[c] + msfvy[c - 1])) * 0.25f *
                          (mut[c] + mut[c - nx] + mut[c - nx - 1] + mut[c - 1]) * 0.25f *
                          (K[p] + K[p - nx] + K[p - nx - 1] + K[p - 1]) * rdx;
@@ -376,9 +392,9 @@ __global__ void k_hdiff(Grid g, S s) {
     const float mkrdym = (msfty[c - nx] / msftx[c - nx]) * K[p - nx] * rdy;
     const float mkrdyp = (msfty[c] / msftx[c]) * K[p] * rdy;
     const float mrdy = msfvx[c] * msfvy[c] * rdy;
-    apply(s[WF_RV_TENDF], s[WF_V], nullptr, mkrdxm, mkrdxp, mrdx, mkrdym, mkrdyp, mrdy);
+    o_v = apply(s[WF_RV_TENDF], s[WF_V], nullptr, mkrdxm, mkrdxp, mrdx, mkrdym, mkrdyp, mrdy);
   }
-  if (k >= 1 && j >= jds + 1 && j < jde - 2 && i >= ids + 1 && i < ide - 2) {  // w
+  if (dw) {  // w
     const float mkrdxm = (msfux[c] / msfuy[c]) * 0.25f * (mut[c] + mut[c - 1] + mut[c] + mut[c - 1]) * 0.25f *
                          (K[p] + K[p - 1] + K[p - lev] + K[p - lev - 1]) * rdx;
     const float mkrdxp = (msfux[c + 1] / msfuy[c + 1]) * 0.25f * (mut[c + 1] + mut[c] + mut[c + 1] + mut[c]) * 0.25f *
@@ -389,9 +405,9 @@ __global__ void k_hdiff(Grid g, S s) {
     const float mkrdyp = (msfvy[c + nx] / msfvx[c + nx]) * 0.25f * (mut[c + nx] + mut[c] + mut[c + nx] + mut[c]) *
                          0.25f * (K[p + nx] + K[p] + K[p - lev + nx] + K[p - lev]) * rdy;
     const float mrdy = msftx[c] * msfty[c] * rdy;
-    apply(s[WF_RW_TENDF], s[WF_W], nullptr, mkrdxm, mkrdxp, mrdx, mkrdym, mkrdyp, mrdy);
+    o_w = apply(s[WF_RW_TENDF], s[WF_W], nullptr, mkrdxm, mkrdxp, mrdx, mkrdym, mkrdyp, mrdy);
   }
-  if (j >= jds + 1 && j < jde - 2 && i >= ids + 1 && i < ide - 2) {  // theta (xkhh, minus t_init)
+  if (dt) {  // theta (xkhh, minus t_init)
     const float* Kh = s[WF_XKHH];
     const float mkrdxm = (msfux[c] / msfuy[c]) * 0.5f * (Kh[p] + Kh[p - 1]) * 0.5f * (mut[c] + mut[c - 1]) * rdx;
     const float mkrdxp = (msfux[c + 1] / msfuy[c + 1]) * 0.5f * (Kh[p + 1] + Kh[p]) * 0.5f * (mut[c + 1] + mut[c]) * rdx;
@@ -400,8 +416,12 @@ __global__ void k_hdiff(Grid g, S s) {
     const float mkrdyp = (msfvy[c + nx] * msfvx_inv[c + nx]) * 0.5f * (Kh[p + nx] + Kh[p]) * 0.5f *
                          (mut[c + nx] + mut[c]) * rdy;
     const float mrdy = msftx[c] * msfty[c] * rdy;
-    apply(s[WF_T_TENDF], s[WF_T], s[WF_T_INIT], mkrdxm, mkrdxp, mrdx, mkrdym, mkrdyp, mrdy);
+    o_t = apply(s[WF_T_TENDF], s[WF_T], s[WF_T_INIT], mkrdxm, mkrdxp, mrdx, mkrdym, mkrdyp, mrdy);
   }
+  if (du) s[WF_RU_TENDF][p] = o_u;
+  if (dv) s[WF_RV_TENDF][p] = o_v;
+  if (dw) s[WF_RW_TENDF][p] = o_w;
+  if (dt) s[WF_T_TENDF][p] = o_t;
 }
 
 // relaxation of u, v, ph (mass-weighted), theta (mass-weighted) and mu at
