@@ -204,7 +204,7 @@ __device__ __forceinline__ float hat(const HatPair& h, int k, size_t lev, bool s
   return h.f[k * lev + pc] / m;
 }
 
-__device__ float hatavg(const Grid& g, const S& s, const HatPair& h, int kk, size_t lev, float cft1, float cft2) {
+__device__ __forceinline__ float hatavg(const Grid& g, const S& s, const HatPair& h, int kk, size_t lev, float cft1, float cft2) {
   const int ktf = g.nz - 1;
   if (kk >= 1 && kk < ktf) {
     const float fnm = s[WF_FNM][kk], fnp = s[WF_FNP][kk];
