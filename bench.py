@@ -305,7 +305,7 @@ def run_ours(a):
         for _ in range(ke):
             for k in E2E_FIELDS:
                 st[k].copy_(host[k], non_blocking=True)
-            it.step()
+            it.run(1)  # the public stepping call: one replay of the captured step
             for k in E2E_FIELDS:
                 host[k].copy_(st[k], non_blocking=True)
         h1.record(cur)

@@ -12,7 +12,7 @@ struct BcItem {
   int two_d;
 };
 
-constexpr int kBcMax = 16;
+constexpr int kBcMax = 24;
 struct BcBatch {
   int n = 0;
   BcItem item[kBcMax];

@@ -152,21 +152,22 @@ struct Driver {
     if (!ok(name)) return;
     if (probe) probe(name, user);
   }
-  void bc(std::initializer_list<std::pair<int, char>> f3, std::initializer_list<std::pair<int, char>> f2 = {}) {
+  // halo copies of the listed 3-D and 2-D fields (and, with moist, of the
+  // six moisture species) in as few launches as the batch allows
+  void bc(std::initializer_list<std::pair<int, char>> f3, std::initializer_list<std::pair<int, char>> f2 = {},
+          bool moist = false) {
     BcBatch b;
-    for (auto& e : f3) {
-      if (b.n == kBcMax) { n += launch_bc(g, b, st); b.n = 0; }
-      b.add(bc_item(g, s[e.first], e.second, false));
-    }
-    for (auto& e : f2) {
-      if (b.n == kBcMax) { n += launch_bc(g, b, st); b.n = 0; }
-      b.add(bc_item(g, s[e.first], e.second, true));
-    }
-    n += launch_bc(g, b, st);
-  }
-  void bc_moist() {
-    BcBatch b;
-    for (int m = 1; m < 7; ++m) b.add(bc_item(g, s[WF_MOIST] + m * g.n3(), 'p', false));
+    auto add = [&](const BcItem& it) {
+      if (b.n == kBcMax) {
+        n += launch_bc(g, b, st);
+        b.n = 0;
+      }
+      b.add(it);
+    };
+    for (auto& e : f3) add(bc_item(g, s[e.first], e.second, false));
+    for (auto& e : f2) add(bc_item(g, s[e.first], e.second, true));
+    if (moist)
+      for (int m = 1; m < 7; ++m) add(bc_item(g, s[WF_MOIST] + m * g.n3(), 'p', false));
     n += launch_bc(g, b, st);
   }
 
@@ -286,8 +287,7 @@ struct Driver {
     }
     n += launch_moist(g, s, rk, dt_rk, st);
     if (rk < 3) {
-      bc({{WF_U, 'U'}, {WF_V, 'V'}, {WF_W, 'w'}, {WF_T, 'p'}, {WF_PH, 'w'}}, {{WF_MU, 't'}});
-      bc_moist();
+      bc({{WF_U, 'U'}, {WF_V, 'V'}, {WF_W, 'w'}, {WF_T, 'p'}, {WF_PH, 'w'}}, {{WF_MU, 't'}}, true);
     }
     snprintf(tag, sizeof tag, "s%d.moist", rk);
     phase(tag);
@@ -313,8 +313,7 @@ struct Driver {
     if (rc != WRF_OK) return;
     bc({{WF_U_1, 'U'}, {WF_U, 'U'}, {WF_V_1, 'V'}, {WF_V, 'V'}, {WF_W_1, 'w'}, {WF_W, 'w'}, {WF_T_1, 'p'},
         {WF_T, 'p'}, {WF_PH_1, 'w'}, {WF_PH, 'w'}},
-       {{WF_MU_1, 't'}, {WF_MU, 't'}});
-    bc_moist();
+       {{WF_MU_1, 't'}, {WF_MU, 't'}}, true);
     n += launch_bdy_final(g, s, st);
     k_step_end<<<1, 1, 0, st>>>(reinterpret_cast<int*>(s[WF_STATUS]));
     ++n;
