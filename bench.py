@@ -25,7 +25,7 @@ Extra keys of the JSON line:
                 on harvested WSM6 increments, then one unseen state run for
                 1 h with the plain and the surrogate step (speed, hydrometeor
                 mass and precipitation errors, tensor-core roofline)
-  adjoint       not built yet
+  adjoint       unavailable: operator adjoints only (no whole-step adjoint)
 ``--impl reference`` times that CPU path alone (rank 0; other ranks exit).
 """
 from __future__ import annotations
@@ -55,9 +55,10 @@ E2E_FIELDS = ("u", "v", "w", "t", "ph", "mu", "p", "al", "moist")
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
 # dominant kernel from one ncu --set full capture of this workload
-# (profiles/k_acoustic_col_and_advection_240x240x41.md): the stage-1 launch,
-# 201.5 MB read + 71.8 MB written, against 321 MB algorithmic for that launch
-NCU_TRAFFIC = {"k_acoustic_col": 273.29408e6}
+# (profiles/k_acoustic_col_and_tma_stencils_240x240x41.md): the stage-1
+# launch, 201.5 MB read + 74.0 MB written, against 321 MB algorithmic for that
+# launch
+NCU_TRAFFIC = {"k_acoustic_col": 275.5e6}
 
 
 def parse():
@@ -338,7 +339,10 @@ def run_ours(a):
                 "gpu_launches": launches * a.steps, "launches_per_step": launches,
                 "roofline": roofline, "step_roofline": whole, "phases_ms": phase_ms,
                 "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan,
-                "surrogate": sur, "adjoint": {"unavailable": "the hand-written adjoint kernels are not built yet"}}
+                "surrogate": sur,
+                "adjoint": {"unavailable": "no whole-step adjoint yet: hand-written reverse-mode kernels exist for "
+                                           "advect_scalar, relax_bdytend, calc_coef_w and the implicit w solve "
+                                           "(pywrf_b200.adjoint), not for the step they compose"}}
         print(json.dumps(line), flush=True)
     it._graph = None
     if world > 1:
