@@ -533,6 +533,30 @@ __global__ void __launch_bounds__(kColTX * kColKT, WRF_COL_MINB) k_acoustic_col(
   const float r_msfty = __frcp_rn(msfty), r_mut = __frcp_rn(mut);
   const float ep = g.epssm;
   const float ep1 = (float)(1.0 + (double)ep), em1 = (float)(1.0 - (double)ep);
+#ifndef WRF_COL_NOPREFETCH
+  // Ask L2 for what the later phases of this thread's levels will load: the
+  // requests need no registers, and the phases after the column sweeps then
+  // find their operands in L2 instead of waiting on DRAM one phase at a time.
+  if (col) {
+    auto pf = [](const float* a) { asm volatile("prefetch.global.L2 [%0];" ::"l"(a)); };
+    const float* fields[] = {ww1, ww, t1, t, ft, s[WF_PH], s[WF_A], s[WF_ALPHA], s[WF_GAMMA], s[WF_PH_SAVE],
+                             s[WF_PHB], s[WF_PH_TEND], s[WF_W], s[WF_RW_TEND], s[WF_C2A], s[WF_ALT], s[WF_CQW],
+                             s[WF_W_SAVE], s[WF_PM1], s[WF_RU_M], s[WF_RV_M], s[WF_WW_M]};
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int k = tk + q * kColKT;
+      if (k >= nz) continue;
+      const int p = k * lev + c;
+#pragma unroll
+      for (const float* f : fields) pf(f + p);
+      if (inner) {
+        pf(t1 + p + nx);
+        pf(t1 + p - nx);
+        pf(v + p + nx);
+      }
+    }
+  }
+#endif
 
   // --- A: horizontal mass-flux divergence per level (inner) / spec t, mu, muts
   if (inner) {
