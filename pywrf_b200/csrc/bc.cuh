@@ -16,6 +16,7 @@ constexpr int kBcMax = 24;
 struct BcBatch {
   int n = 0;
   BcItem item[kBcMax];
+  float* zgw = nullptr;  // w, when the launch also applies zero_grad_bdy(w)
   void add(const BcItem& it) { item[n++] = it; }
 };
 

@@ -5,7 +5,6 @@
 //   k_advance_uv        advance_uv + spec_bdyupdate(u), (v)
 //   k_acoustic_col      advance_mu_t, advance_w, sumflux, spec_bdyupdate of
 //                       t / mu / muts / ph and calc_p_rho of one substep
-//   k_zero_grad_w       zero_grad_bdy(w)
 //   k_mu_uv_1 / k_ssfinish  calc_mu_uv_1, small_step_finish
 // The vertical recurrences (mass divergence sum, ww scan, Thomas sweeps) run
 // sequentially per column in the reference's order.
@@ -482,7 +481,8 @@ __global__ void __launch_bounds__(kUvTX * kUvTY, 4) k_advance_uv_tma(Grid g, S s
 // separate shared arrays so that their loads pipeline.  Small blocks and few
 // registers let several blocks share an SM, which overlaps one block's
 // sweeps with the memory phases of the others.  No column reads another
-// column's result of this kernel; zero_grad_bdy(w) follows in k_zero_grad_w.
+// column's result of this kernel; zero_grad_bdy(w) follows in the substep's
+// halo launch (k_bc).
 // Divisions by per-column constants use the correctly rounded form divc with
 // the column's reciprocals (__frcp_rn).
 constexpr int kColTX = 16, kColKT = 16;
@@ -986,33 +986,6 @@ __global__ void __launch_bounds__(kColTX * kColKT, WRF_COL_MINB) k_acoustic_col(
   }
 }
 
-// zero_grad_bdy(w) on the specified rows, all levels (wrf_boundary.py:358-400);
-// one thread per ring point: rows jbs and jbe-1 (columns [ibs, ibe)), then
-// columns ibs and ibe-1 (rows (jbs, jbe-1))
-__global__ void k_zero_grad_w(Grid g, S s) {
-  const int ibs = g.ids, ibe = g.ide - 1, jbs = g.jds, jbe = g.jde - 1;
-  const int nxr = ibe - ibs, nyr = jbe - jbs - 2;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
-  if (r >= 2 * nxr + 2 * nyr) return;
-  int j, i, sj, si;
-  if (r < 2 * nxr) {
-    const bool top = r >= nxr;
-    i = ibs + (top ? r - nxr : r);
-    j = top ? jbe - 1 : jbs;
-    sj = top ? jbe - 2 : jbs + 1;
-    si = (i == ibs) ? ibs + 1 : (i == ibe - 1 ? ibe - 2 : i);
-  } else {
-    const int q = r - 2 * nxr;
-    const bool east = q >= nyr;
-    j = jbs + 1 + (east ? q - nyr : q);
-    i = east ? ibe - 1 : ibs;
-    sj = j;
-    si = east ? ibe - 2 : ibs + 1;
-  }
-  float* w = s[WF_W];
-  const size_t base = (size_t)k * g.ny * g.nx;
-  w[base + (size_t)j * g.nx + i] = w[base + (size_t)sj * g.nx + si];
-}
 
 __global__ void k_mu_uv_1(Grid g, S s) {
   WRF_COLUMN_INDEX(g, j, i);
@@ -1152,11 +1125,6 @@ int launch_acoustic_col(const Grid& g, const S& s, float dts, int iteration, int
   return 1;
 }
 
-int launch_zero_grad_w(const Grid& g, const S& s, cudaStream_t st) {
-  const int nring = 2 * (g.ide - 1 - g.ids) + 2 * (g.jde - 1 - g.jds - 2);
-  k_zero_grad_w<<<dim3((nring + 127) / 128, g.nz), 128, 0, st>>>(g, s);
-  return 1;
-}
 
 int launch_small_step_finish(const Grid& g, const S& s, float dts, int nsub, int rk_step, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);

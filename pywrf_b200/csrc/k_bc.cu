@@ -13,8 +13,42 @@ namespace wrf {
 // one block per (level, field): the x sides first (their rows reach 4 rows
 // into the y halo and read the values the y sides will overwrite), then the
 // y sides, separated by a block barrier
+// zero_grad_bdy(w) on the specified rows of level k (wrf_boundary.py:358-400):
+// rows jbs and jbe-1 (columns [ibs, ibe)), then columns ibs and ibe-1 (rows
+// (jbs, jbe-1)) take the value of their inner neighbour; the sources are never
+// ring points, so the copies are independent
+__device__ __forceinline__ void zero_grad_w_level(const Grid& g, float* w, int k) {
+  const int ibs = g.ids, ibe = g.ide - 1, jbs = g.jds, jbe = g.jde - 1;
+  const int nxr = ibe - ibs, nyr = jbe - jbs - 2;
+  const size_t base = (size_t)k * g.ny * g.nx;
+  for (int r = threadIdx.x; r < 2 * nxr + 2 * nyr; r += blockDim.x) {
+    int j, i, sj, si;
+    if (r < 2 * nxr) {
+      const bool top = r >= nxr;
+      i = ibs + (top ? r - nxr : r);
+      j = top ? jbe - 1 : jbs;
+      sj = top ? jbe - 2 : jbs + 1;
+      si = (i == ibs) ? ibs + 1 : (i == ibe - 1 ? ibe - 2 : i);
+    } else {
+      const int q = r - 2 * nxr;
+      const bool east = q >= nyr;
+      j = jbs + 1 + (east ? q - nyr : q);
+      i = east ? ibe - 1 : ibs;
+      sj = j;
+      si = east ? ibe - 2 : ibs + 1;
+    }
+    w[base + (size_t)j * g.nx + i] = w[base + (size_t)sj * g.nx + si];
+  }
+}
+
+// one block per (level, field); with b.zgw set, the blocks of the extra row
+// f == b.n apply zero_grad_bdy(w) (w is never one of the batch's fields)
 __global__ void __launch_bounds__(256) k_bc(Grid g, BcBatch b) {
   const int k = blockIdx.x, f = blockIdx.y;
+  if (b.zgw && f == b.n) {
+    if (k < g.nz) zero_grad_w_level(g, b.zgw, k);
+    return;
+  }
   const BcItem it = b.item[f];
   if (k >= it.k_end) return;  // whole block
   float* d = it.ptr + (it.two_d ? 0 : (size_t)k * g.ny * g.nx);
@@ -81,10 +115,10 @@ BcItem bc_item(const Grid& g, float* ptr, char var, bool two_d) {
 }
 
 int launch_bc(const Grid& g, const BcBatch& b, cudaStream_t st) {
-  if (b.n == 0) return 0;
-  int kmax = 1;
+  if (b.n == 0 && !b.zgw) return 0;
+  int kmax = b.zgw ? g.nz : 1;
   for (int f = 0; f < b.n; ++f) kmax = b.item[f].k_end > kmax ? b.item[f].k_end : kmax;
-  k_bc<<<dim3(kmax, b.n), 256, 0, st>>>(g, b);
+  k_bc<<<dim3(kmax, b.n + (b.zgw ? 1 : 0)), 256, 0, st>>>(g, b);
   return 1;
 }
 

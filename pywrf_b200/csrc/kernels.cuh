@@ -83,7 +83,6 @@ int launch_coef_w(const Grid& g, const float* mut, const float* cqw, const float
 int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cudaStream_t st);
 int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st);
 int launch_acoustic_col(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st);
-int launch_zero_grad_w(const Grid& g, const S& s, cudaStream_t st);
 int launch_small_step_finish(const Grid& g, const S& s, float dts, int nsub, int rk_step, cudaStream_t st);
 
 // moisture (k_moist.cu)

@@ -155,7 +155,7 @@ struct Driver {
   // halo copies of the listed 3-D and 2-D fields (and, with moist, of the
   // six moisture species) in as few launches as the batch allows
   void bc(std::initializer_list<std::pair<int, char>> f3, std::initializer_list<std::pair<int, char>> f2 = {},
-          bool moist = false) {
+          bool moist = false, bool zero_grad_w = false) {
     BcBatch b;
     auto add = [&](const BcItem& it) {
       if (b.n == kBcMax) {
@@ -168,6 +168,7 @@ struct Driver {
     for (auto& e : f2) add(bc_item(g, s[e.first], e.second, true));
     if (moist)
       for (int m = 1; m < 7; ++m) add(bc_item(g, s[WF_MOIST] + m * g.n3(), 'p', false));
+    if (zero_grad_w) b.zgw = s[WF_W];
     n += launch_bc(g, b, st);
   }
 
@@ -256,8 +257,8 @@ struct Driver {
     n += launch_acoustic_col(g, s, dts_rk, it, nsub, st);
     snprintf(tag, sizeof tag, "s%d.sub%d.col", rk, it);
     phase(tag);
-    n += launch_zero_grad_w(g, s, st);
-    bc({{WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}}, {{WF_MUTS, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}});
+    // zero_grad_bdy(w) rides in the halo launch (disjoint fields)
+    bc({{WF_PH, 'w'}, {WF_AL, 'p'}, {WF_P, 'p'}}, {{WF_MUTS, 't'}, {WF_MU, 't'}, {WF_MUDF, 't'}}, false, true);
     snprintf(tag, sizeof tag, "s%d.sub%d", rk, it);
     phase(tag);
   }
