@@ -189,6 +189,18 @@ int wrf_advect_scalar_adj(const WrfGrid* g, const float* field, const float* ru,
                           const float* rom, const float* msftx, const float* fzm, const float* fzp,
                           const float* rdzw, const float* tend_bar, float* field_bar, float* ru_bar,
                           float* rv_bar, float* rom_bar, void* stream);
+/* Adjoint of wrf_advect_momentum (reverse mode): given the cotangent tend_bar
+ * of the updated tendency, accumulates (+=) the cotangents of the advected
+ * component (field) and of ru, rv and rom; the arguments are those of
+ * wrf_advect_momentum.  The reference obtains this product from torch
+ * autograd through wrf_dynamics.py:1112-1331 (advect_u) and 1332-1534
+ * (advect_v); its advect_w (1535-1823) cannot be differentiated by its
+ * autograd (an in-place update of a saved operand), the product is the
+ * same transpose of the linearised operator. */
+int wrf_advect_momentum_adj(const WrfGrid* g, int component, const float* field, const float* ru,
+                            const float* rv, const float* rom, const float* msf, const float* msf2,
+                            const float* fzm, const float* fzp, const float* rdz, const float* tend_bar,
+                            float* field_bar, float* ru_bar, float* rv_bar, float* rom_bar, void* stream);
 /* wrf_boundary.py:52-147 relax_bdytend on one field: tend += the relaxation
  * toward bdy + dtbc * bdy_tend over the zone rows 1..3.  bdy8: device arrays
  * xs xe ys ye (values) and txs txe tys tye (tendencies) in the solver's
@@ -253,9 +265,11 @@ int wrf_last_launch_count(void);
 
 /* Kernel forms for cross-checks (process-wide; no counterpart in the
  * reference).  WRF_FORM_FAST (the default) runs the tiled tensor-map kernels
- * where the arrays allow them; WRF_FORM_POINT runs, for the same launches, the
- * one-thread-per-point (momentum advection, advance_uv) and cp.async-tiled
- * (scalar advection) kernels.  Both forms perform the reference's operations
+ * where the arrays allow them, and the boundary relaxation over the boundary
+ * band only; WRF_FORM_POINT runs, for the same launches, the
+ * one-thread-per-point (momentum advection, advance_uv, forces) and
+ * cp.async-tiled (scalar advection) kernels and the relaxation over every
+ * point.  Both forms perform the reference's operations
  * in the same order and give bit-identical results.  A CUDA graph keeps the
  * form that was set when it was captured.  Returns the previous form, or
  * WRF_EINVAL for an unknown one. */

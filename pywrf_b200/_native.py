@@ -98,6 +98,8 @@ def lib() -> ctypes.CDLL:
     L.wrf_set_kernel_form.argtypes = [ctypes.c_int]
     L.wrf_advect_momentum.restype = ip
     L.wrf_advect_momentum.argtypes = [ctypes.POINTER(WrfGridC), ctypes.c_int] + [vp] * 10 + [ctypes.c_int, vp]
+    L.wrf_advect_momentum_adj.restype = ip
+    L.wrf_advect_momentum_adj.argtypes = [ctypes.POINTER(WrfGridC), ctypes.c_int] + [vp] * 14 + [vp]
     L.wrf_advect_scalar_adj.restype = ip
     L.wrf_advect_scalar_adj.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 13 + [vp]
     L.wrf_relax_bdytend.restype = ip

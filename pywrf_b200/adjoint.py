@@ -8,6 +8,9 @@ operators keeps no tape of the forward's intermediates.
 * :class:`AdvectScalar` -- ``tendency + advect(field; ru, rv, rom)``
   (pywrf/wrf_dynamics.py:1841-2028); gradients with respect to the field, the
   incoming tendency and the three mass fluxes.
+* :class:`AdvectMomentum` -- ``tendency + advect_u / advect_v / advect_w``
+  (pywrf/wrf_dynamics.py:1112-1823); gradients with respect to the advected
+  component, the incoming tendency and ru, rv, rom.
 * :class:`RelaxBdytend` -- ``tendency + relax(field)`` toward the lateral
   boundary values (pywrf/wrf_boundary.py:52-147); gradients with respect to
   the field and the incoming tendency (the boundary arrays are data).
@@ -78,6 +81,51 @@ class AdvectScalar(torch.autograd.Function):
 def advect_scalar(field, tendency, ru, rv, rom, msftx, fnm, fnp, rdnw, rdx, rdy):
     """Differentiable ``tendency + advect(field)`` on the GPU."""
     return AdvectScalar.apply(field, tendency, ru, rv, rom, msftx, fnm, fnp, rdnw, rdx, rdy)
+
+
+class AdvectMomentum(torch.autograd.Function):
+    """out = tendency + flux-form advection of one momentum component
+    (0 u with msf = msfux, 1 v with msf = msfvy and msf2 = msfvx, 2 w with
+    msf = msftx; rdz = rdnw for u and v, rdn for w)."""
+
+    @staticmethod
+    def forward(ctx, component: int, field, tendency, ru, rv, rom, msf, msf2, fzm, fzp, rdz, rdx: float, rdy: float):
+        if component not in (0, 1, 2):
+            raise ValueError("component must be 0 (u), 1 (v) or 2 (w)")
+        if component == 1 and msf2 is None:
+            raise ValueError("advect_v needs msf2 (msfvx)")
+        cg = scalar_grid(field.shape, rdx, rdy)
+        out = tendency.detach().clone()
+        m2 = _ptr(msf2) if msf2 is not None else None
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(field.device):
+            rc = N.lib().wrf_advect_momentum(ctypes.byref(cg), int(component), _ptr(field), _ptr(out), _ptr(ru),
+                                             _ptr(rv), _ptr(rom), _ptr(msf), m2, _ptr(fzm), _ptr(fzp), _ptr(rdz),
+                                             0, stream)
+        N.check(rc, "wrf_advect_momentum")
+        ctx.save_for_backward(field, ru, rv, rom, msf, msf if msf2 is None else msf2, fzm, fzp, rdz)
+        ctx.cg, ctx.component, ctx.has_msf2 = cg, int(component), msf2 is not None
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        field, ru, rv, rom, msf, msf2, fzm, fzp, rdz = ctx.saved_tensors
+        gout = gout.contiguous()
+        qb, rub, rvb, romb = (torch.zeros_like(field) for _ in range(4))
+        m2 = _ptr(msf2) if ctx.has_msf2 else None
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(field.device):
+            rc = N.lib().wrf_advect_momentum_adj(ctypes.byref(ctx.cg), ctx.component, _ptr(field), _ptr(ru), _ptr(rv),
+                                                 _ptr(rom), _ptr(msf), m2, _ptr(fzm), _ptr(fzp), _ptr(rdz), _ptr(gout),
+                                                 _ptr(qb), _ptr(rub), _ptr(rvb), _ptr(romb), stream)
+        N.check(rc, "wrf_advect_momentum_adj")
+        return None, qb, gout, rub, rvb, romb, None, None, None, None, None, None, None
+
+
+def advect_momentum(component, field, tendency, ru, rv, rom, msf, msf2, fzm, fzp, rdz, rdx, rdy):
+    """Differentiable ``tendency + advect_{u,v,w}(field)`` on the GPU
+    (component 0, 1, 2)."""
+    return AdvectMomentum.apply(component, field, tendency, ru, rv, rom, msf, msf2, fzm, fzp, rdz, rdx, rdy)
 
 
 BDY_NAMES = ("xs", "xe", "ys", "ye", "txs", "txe", "tys", "tye")

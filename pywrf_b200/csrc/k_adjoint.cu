@@ -18,6 +18,23 @@
 // touch it), so results do not depend on scheduling; tend's own cotangent is
 // tbar unchanged (the caller passes it through).
 //
+//   k_advect_mom_adj<C>  adjoint of advect_u (C = 0, wrf_dynamics.py:1112-1331),
+//                        advect_v (1, :1332-1534) and advect_w (2, :1535-1823),
+//                        forward k_advect / k_advect_mom_tma, with respect to
+//                        the advected component and ru, rv, rom.  Every face
+//                        flux of those operators is a product F = V Phi of a
+//                        velocity V linear in one of ru / rv / rom (a two-point
+//                        average, or the fnm / fnp interpolation of advect_w's
+//                        horizontal faces) and a face value Phi linear in the
+//                        component for fixed upwind choices (the sign of V, or
+//                        of the component itself at advect_u's / advect_v's
+//                        outermost faces).  face_lin<C, D> lists both linear
+//                        forms of a face; the kernel gathers, per point, over
+//                        the faces whose lists hold it:
+//   qbar(m) += sum_f Fbar(f) V(f) dPhi_f/dq(m),  rbar(n) += sum_f Fbar(f) Phi(f) dV_f/dr(n)
+//                        with Fbar(f) from the tendency cotangent of the cells
+//                        either side of f (one writer per output element).
+//
 //   k_relax_field / k_relax_field_adj  relax_bdytend (wrf_boundary.py:52-147)
 //                        on one field, and its adjoint with respect to the
 //                        field: at a relaxation point P of distance b,
@@ -439,6 +456,291 @@ int launch_coef_w_adj(const Grid& g, const float* mut, const float* cqw, const f
   const dim3 b2(32, 8);
   k_coef_w_adj<<<col_grid(g, b2), b2, 0, st>>>(g, mut, cqw, c2a, rdn, rdnw, dts, abar, alphabar, gammabar, mutbar,
                                                cqwbar, c2abar);
+  return 1;
+}
+
+// ------------------------------------------------------- momentum advection
+
+namespace {
+
+// the linear forms of one face flux F = V Phi: Phi = sum qc[n] q[qi[n]],
+// V = sum rc[n] r[ri[n]] (r: ru for x faces, rv for y faces, rom for z faces)
+struct FaceLin {
+  int nq = 0, nr = 0;
+  size_t qi[6];
+  float qc[6];
+  size_t ri[2];
+  float rc[2];
+};
+
+struct MomAdjArgs {
+  const float *q, *ru, *rv, *rom, *msf, *msf2, *fzm, *fzp, *rdz;
+};
+
+__device__ __forceinline__ size_t off(size_t b, int o, size_t st) {
+  return (size_t)((long long)b + (long long)o * (long long)st);
+}
+__device__ __forceinline__ void put5(FaceLin& L, size_t b, size_t st, float s) {
+  L.nq = 6;
+  for (int o = -3; o <= 2; ++o) {
+    L.qi[o + 3] = off(b, o, st);
+    L.qc[o + 3] = w5(o, s);
+  }
+}
+__device__ __forceinline__ void put3(FaceLin& L, size_t b, size_t st, float s) {
+  L.nq = 4;
+  for (int o = -2; o <= 1; ++o) {
+    L.qi[o + 2] = off(b, o, st);
+    L.qc[o + 2] = w3(o, s);
+  }
+}
+__device__ __forceinline__ void put2(FaceLin& L, size_t i0, float c0, size_t i1, float c1) {
+  L.nq = 2;
+  L.qi[0] = i0;
+  L.qc[0] = c0;
+  L.qi[1] = i1;
+  L.qc[1] = c1;
+}
+// V = c0 r[i0] + c1 r[i1], returned
+__device__ __forceinline__ float putr(FaceLin& L, const float* r, size_t i0, float c0, size_t i1, float c1) {
+  L.nr = 2;
+  L.ri[0] = i0;
+  L.rc[0] = c0;
+  L.ri[1] = i1;
+  L.rc[1] = c1;
+  return c0 * r[i0] + c1 * r[i1];
+}
+
+// Face D (0 y, 1 x, 2 z) of component C at (k, j, i): the face index is j,
+// i or k along D.  Returns false where the forward has no flux.  The cases
+// and their order are those of fqy_u .. vf_w (k_tend.cu).
+template <int C, int D>
+__device__ bool face_lin(const Grid& g, const MomAdjArgs& a, int k, int j, int i, FaceLin& L) {
+  const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde, ktf = g.nz - 1, nx = g.nx;
+  const size_t lev = (size_t)g.ny * nx;
+  const size_t p = (size_t)k * lev + (size_t)j * nx + i;
+  const float* q = a.q;
+  if (D == 0) {  // y faces, rv
+    const int jf = j;
+    float v;
+    if (C == 0) {
+      v = putr(L, a.rv, p, 0.5f, p - 1, 0.5f);
+      if (jf >= jds + 3 && jf < jde - 3) put5(L, p, nx, sgnf(v));
+      else if (jf == jds + 1) put2(L, p, 0.5f, p - nx, 0.5f);
+      else if (jf == jds + 2) put3(L, p, nx, sgnf(v));
+      else if (jf == jde - 2) put2(L, p, 0.5f, p - nx, 0.5f);
+      else if (jf == jde - 3) put3(L, p, nx, 1.0f);  // the reference's sign source there is 0
+      else return false;
+    } else if (C == 1) {
+      v = putr(L, a.rv, p, 0.5f, p - nx, 0.5f);
+      if (jf >= jds + 3 && jf < jde - 2) put5(L, p, nx, sgnf(v));
+      else if (jf == jds + 1) {
+        if (q[p] < 0.f) put2(L, p, 1.0f, p - nx, 0.0f);
+        else put2(L, p, 0.5f, p - nx, 0.5f);
+      } else if (jf == jds + 2) put3(L, p, nx, sgnf(v));
+      else if (jf == jde - 1) {
+        if (q[p - nx] > 0.f) put2(L, p - nx, 1.0f, p, 0.0f);
+        else put2(L, p - nx, 0.5f, p, 0.5f);
+      } else if (jf == jde - 2) put3(L, p, nx, sgnf(v));
+      else return false;
+    } else {
+      if (k < 1) return false;
+      v = k < ktf ? putr(L, a.rv, p, a.fzm[k], p - lev, a.fzp[k])
+                  : putr(L, a.rv, p - lev, 2.0f - a.fzm[ktf - 1], p - 2 * lev, -a.fzp[ktf - 1]);
+      if (jf >= jds + 3 && jf < jde - 3) put5(L, p, nx, sgnf(v));
+      else if (jf == jds + 1) put2(L, p, 0.5f, p - nx, 0.5f);
+      else if (jf == jds + 2) put3(L, p, nx, sgnf(v));
+      else if (jf == jde - 2) put2(L, p, 0.5f, p - nx, 0.5f);
+      else if (jf == jde - 3) put3(L, p, nx, sgnf(v));
+      else return false;
+    }
+    return true;
+  } else if (D == 1) {  // x faces, ru
+    const int f = i;
+    float v;
+    if (C == 0) {
+      v = putr(L, a.ru, p, 0.5f, p - 1, 0.5f);
+      if (f >= ids + 3 && f < ide - 2) put5(L, p, 1, sgnf(v));
+      else if (f == ids + 1) {
+        if (q[p] < 0.f) put2(L, p, 1.0f, p - 1, 0.0f);
+        else put2(L, p, 0.5f, p - 1, 0.5f);
+      } else if (f == ids + 2) put3(L, p, 1, sgnf(v));
+      else if (f == ide - 1) {
+        if (q[p - 1] > 0.f) put2(L, p - 1, 1.0f, p, 0.0f);
+        else put2(L, p - 1, 0.5f, p, 0.5f);
+      } else if (f == ide - 2) put3(L, p, 1, sgnf(v));
+      else return false;
+    } else if (C == 1) {
+      v = putr(L, a.ru, p, 0.5f, p - nx, 0.5f);
+      if (f >= ids + 3 && f < ide - 3) put5(L, p, 1, sgnf(v));
+      else if (f == ids + 1) put2(L, p, 0.5f, p - 1, 0.5f);
+      else if (f == ids + 2) put3(L, p, 1, sgnf(v));
+      else if (f == ide - 2) put2(L, p, 0.5f, p - 1, 0.5f);
+      else if (f == ide - 3) put3(L, p, 1, sgnf(v));
+      else return false;
+    } else {
+      if (k < 1) return false;
+      v = k < ktf ? putr(L, a.ru, p, a.fzm[k], p - lev, a.fzp[k])
+                  : putr(L, a.ru, p - lev, 2.0f - a.fzm[ktf - 1], p - 2 * lev, -a.fzp[ktf - 1]);
+      if (f >= ids + 3 && f < ide - 3) put5(L, p, 1, sgnf(v));
+      else if (f == ids + 1) put2(L, p, 0.5f, p - 1, 0.5f);
+      else if (f == ids + 2) put3(L, p, 1, sgnf(v));
+      else if (f == ide - 2) put2(L, p, 0.5f, p - 1, 0.5f);
+      else if (f == ide - 3) put3(L, p, 1, sgnf(v));
+      else return false;
+    }
+    return true;
+  } else {  // vertical faces, rom
+    const int kf = k;
+    if (kf < 1) return false;
+    if (C == 0 || C == 1) {
+      const size_t nb = C == 0 ? 1 : (size_t)nx;  // the second rom point: i-1 (u) or j-1 (v)
+      const float v = putr(L, a.rom, p, 0.5f, p - nb, 0.5f);
+      if (kf >= 3 && kf < ktf - 2) put5(L, p, lev, sgnf(-v));
+      else if (kf == 1) put2(L, p, a.fzm[kf], p - lev, a.fzp[kf]);
+      else if (kf == 2) put3(L, p, lev, sgnf(-v));
+      else if (kf == ktf - 2) put3(L, p, lev, C == 0 ? sgnf(-v) : sgnf(v));
+      else if (kf == ktf - 1) put2(L, p, a.fzm[kf], p - lev, a.fzp[kf]);
+      else return false;
+    } else {
+      const float v = putr(L, a.rom, p, 0.5f, p - lev, 0.5f);
+      if (kf >= 3 && kf < ktf - 1) put5(L, p, lev, sgnf(-v));
+      else if (kf == 1) put2(L, p, 0.5f, p - lev, 0.5f);
+      else if (kf == 2) put3(L, p, lev, sgnf(-v));
+      else if (kf == ktf - 1) put3(L, p, lev, sgnf(v));
+      else if (kf == ktf) put2(L, p, 0.5f, p - lev, 0.5f);
+      else return false;
+    }
+    return true;
+  }
+}
+
+// the tendency coefficient of direction D in cell (k, j, i) of component C
+// (0 outside the cells that direction updates); advect_w's top cell, which
+// adds 2 rdz(ktf-1) F(ktf), is handled by fbar
+template <int C, int D>
+__device__ __forceinline__ float cell_coef(const Grid& g, const MomAdjArgs& a, int k, int j, int i) {
+  const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde, ktf = g.nz - 1;
+  if (k < 0 || j < 0 || i < 0 || j >= g.ny || i >= g.nx) return 0.f;
+  const int c = j * g.nx + i;
+  if (C == 0) {
+    if (!(k < ktf && j >= jds && j < jde - 1 && i >= ids + 1 && i < ide - 1)) return 0.f;
+    if (D == 0) return (j >= jds + 1 && j < jde - 2) ? a.msf[c] * g.rdy : 0.f;
+    if (D == 1) return a.msf[c] * g.rdx;
+    return a.rdz[k];
+  } else if (C == 1) {
+    if (!(k < ktf && j >= jds + 1 && j < jde - 1 && i >= ids && i < ide - 1)) return 0.f;
+    if (D == 0) return a.msf[c] * g.rdy;
+    if (D == 1) return (i >= ids + 1 && i < ide - 2) ? a.msf[c] * g.rdx : 0.f;
+    return (a.msf[c] / a.msf2[c]) * a.rdz[k];
+  } else {
+    if (!(k >= 1 && k <= ktf && j >= jds && j < jde - 1 && i >= ids && i < ide - 1)) return 0.f;
+    if (D == 0) return (j >= jds + 1 && j < jde - 2) ? a.msf[c] * g.rdy : 0.f;
+    if (D == 1) return (i >= ids + 1 && i < ide - 2) ? a.msf[c] * g.rdx : 0.f;
+    return k < ktf ? a.rdz[k] : 0.f;
+  }
+}
+
+// Fbar of face D at (k, j, i): each cell subtracts coef (F(upper) - F(lower))
+template <int C, int D>
+__device__ float fbar(const Grid& g, const MomAdjArgs& a, const float* tbar, int k, int j, int i) {
+  if (k < 0 || k >= g.nz || j < 0 || j >= g.ny || i < 0 || i >= g.nx) return 0.f;
+  const size_t lev = (size_t)g.ny * g.nx;
+  auto tb = [&](int kk, int jj, int ii) { return tbar[(size_t)kk * lev + (size_t)jj * g.nx + ii]; };
+  float v = 0.f;
+  const float c0 = cell_coef<C, D>(g, a, k, j, i);
+  if (c0 != 0.f) v += c0 * tb(k, j, i);
+  const int k1 = D == 2 ? k - 1 : k, j1 = D == 0 ? j - 1 : j, i1 = D == 1 ? i - 1 : i;
+  const float c1 = cell_coef<C, D>(g, a, k1, j1, i1);
+  if (c1 != 0.f) v -= c1 * tb(k1, j1, i1);
+  if (C == 2 && D == 2 && k == g.nz - 1) {  // advect_w's top cell: tend += 2 rdz(ktf-1) F(ktf)
+    const int ktf = g.nz - 1;
+    if (j >= g.jds && j < g.jde - 1 && i >= g.ids && i < g.ide - 1) v += 2.0f * a.rdz[ktf - 1] * tb(ktf, j, i);
+  }
+  return v;
+}
+
+// the field cotangent at m = (k, j, i) from the faces of direction D
+template <int C, int D>
+__device__ float gather_q(const Grid& g, const MomAdjArgs& a, const float* tbar, int k, int j, int i, size_t m) {
+  const float* r = D == 0 ? a.rv : D == 1 ? a.ru : a.rom;
+  float acc = 0.f;
+  for (int o = -2; o <= 3; ++o) {
+    const int kf = D == 2 ? k + o : k, jf = D == 0 ? j + o : j, f = D == 1 ? i + o : i;
+    const float fb = fbar<C, D>(g, a, tbar, kf, jf, f);
+    if (fb == 0.f) continue;
+    FaceLin L;
+    if (!face_lin<C, D>(g, a, kf, jf, f, L)) continue;
+    float w = 0.f;
+    for (int n = 0; n < L.nq; ++n)
+      if (L.qi[n] == m) w += L.qc[n];
+    if (w == 0.f) continue;
+    float v = 0.f;
+    for (int n = 0; n < L.nr; ++n) v += L.rc[n] * r[L.ri[n]];
+    acc += fb * v * w;
+  }
+  return acc;
+}
+
+// the cotangent of the D-direction velocity (ru, rv, rom) at n = (k, j, i):
+// the faces whose velocity holds n lie at offsets 0 / +1 in each direction,
+// and advect_w's horizontal faces at the top level also read levels
+// ktf-1 and ktf-2
+template <int C, int D>
+__device__ float gather_r(const Grid& g, const MomAdjArgs& a, const float* tbar, int k, int j, int i, size_t n) {
+  const int ktf = g.nz - 1;
+  float acc = 0.f;
+  const int nk = (C == 2 && D != 2 && k != ktf && k + 1 != ktf) ? 3 : 2;
+  for (int dk = 0; dk < nk; ++dk) {
+    const int kf = dk < 2 ? k + dk : ktf;
+    for (int dj = 0; dj < 2; ++dj)
+      for (int di = 0; di < 2; ++di) {
+        const float fb = fbar<C, D>(g, a, tbar, kf, j + dj, i + di);
+        if (fb == 0.f) continue;
+        FaceLin L;
+        if (!face_lin<C, D>(g, a, kf, j + dj, i + di, L)) continue;
+        float w = 0.f;
+        for (int e = 0; e < L.nr; ++e)
+          if (L.ri[e] == n) w += L.rc[e];
+        if (w == 0.f) continue;
+        float phi = 0.f;
+        for (int e = 0; e < L.nq; ++e) phi += L.qc[e] * a.q[L.qi[e]];
+        acc += fb * phi * w;
+      }
+  }
+  return acc;
+}
+
+}  // namespace
+
+template <int C>
+__global__ void k_advect_mom_adj(Grid g, MomAdjArgs a, const float* tbar, float* qbar, float* rubar, float* rvbar,
+                                 float* rombar) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const size_t m = ((size_t)k * g.ny + j) * g.nx + i;
+  const float aq = gather_q<C, 0>(g, a, tbar, k, j, i, m) + gather_q<C, 1>(g, a, tbar, k, j, i, m) +
+                   gather_q<C, 2>(g, a, tbar, k, j, i, m);
+  if (aq != 0.f) qbar[m] += aq;
+  const float arv = gather_r<C, 0>(g, a, tbar, k, j, i, m);
+  if (arv != 0.f) rvbar[m] += arv;
+  const float aru = gather_r<C, 1>(g, a, tbar, k, j, i, m);
+  if (aru != 0.f) rubar[m] += aru;
+  const float arom = gather_r<C, 2>(g, a, tbar, k, j, i, m);
+  if (arom != 0.f) rombar[m] += arom;
+}
+
+int launch_advect_mom_adj(const Grid& g, int component, const float* q, const float* ru, const float* rv,
+                          const float* rom, const float* msf, const float* msf2, const float* fzm, const float* fzp,
+                          const float* rdz, const float* tbar, float* qbar, float* rubar, float* rvbar,
+                          float* rombar, cudaStream_t st) {
+  const dim3 b3(32, 4);
+  const MomAdjArgs a{q, ru, rv, rom, msf, msf2, fzm, fzp, rdz};
+  if (component == 0)
+    k_advect_mom_adj<0><<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, qbar, rubar, rvbar, rombar);
+  else if (component == 1)
+    k_advect_mom_adj<1><<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, qbar, rubar, rvbar, rombar);
+  else
+    k_advect_mom_adj<2><<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, qbar, rubar, rvbar, rombar);
   return 1;
 }
 

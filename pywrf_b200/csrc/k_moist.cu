@@ -230,7 +230,7 @@ int launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st) {
 
 int launch_bdy_final(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);
-  if (ring_fits(g))
+  if (kernel_form() == WRF_FORM_FAST && ring_fits(g))
     k_bdy_final<<<dim3((ring_size(g) + 127) / 128, 1, g.nz), 128, 0, st>>>(g, s, 1);
   else
     k_bdy_final<<<point_grid(g, b3), b3, 0, st>>>(g, s, 0);

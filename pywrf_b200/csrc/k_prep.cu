@@ -536,7 +536,7 @@ int launch_diff_metrics(const Grid& g, const S& s, cudaStream_t st) {
 int launch_hdiff_relax(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_hdiff<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  if (ring_fits(g))
+  if (kernel_form() == WRF_FORM_FAST && ring_fits(g))
     k_relax<<<dim3((ring_size(g) + 127) / 128, 1, g.nz), 128, 0, st>>>(g, s, 1);
   else
     k_relax<<<point_grid(g, b3), b3, 0, st>>>(g, s, 0);
@@ -545,7 +545,7 @@ int launch_hdiff_relax(const Grid& g, const S& s, cudaStream_t st) {
 
 int launch_relax_qv(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
-  if (ring_fits(g))
+  if (kernel_form() == WRF_FORM_FAST && ring_fits(g))
     k_relax_qv<<<dim3((ring_size(g) + 127) / 128, 1, g.nz), 128, 0, st>>>(g, s, 1);
   else
     k_relax_qv<<<point_grid(g, b3), b3, 0, st>>>(g, s, 0);

@@ -52,6 +52,10 @@ int launch_advect_scalar(const Grid& g, const S& s, const float* field, float* t
 
 // adjoint of advect_scalar w.r.t. the field and ru / rv / rom (k_adjoint.cu);
 // accumulates into qbar, rubar, rvbar, rombar
+int launch_advect_mom_adj(const Grid& g, int component, const float* q, const float* ru, const float* rv,
+                          const float* rom, const float* msf, const float* msf2, const float* fzm, const float* fzp,
+                          const float* rdz, const float* tbar, float* qbar, float* rubar, float* rvbar,
+                          float* rombar, cudaStream_t st);
 int launch_advect_scalar_adj(const Grid& g, const float* q, const float* ru, const float* rv, const float* rom,
                              const float* msftx, const float* fnm, const float* fnp, const float* rdnw,
                              const float* tbar, float* qbar, float* rubar, float* rvbar, float* rombar,

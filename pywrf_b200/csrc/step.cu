@@ -522,6 +522,23 @@ int wrf_advect_scalar_adj(const WrfGrid* gin, const float* field, const float* r
   return check_launch("advect_scalar_adj");
 }
 
+int wrf_advect_momentum_adj(const WrfGrid* gin, int component, const float* field, const float* ru, const float* rv,
+                            const float* rom, const float* msf, const float* msf2, const float* fzm, const float* fzp,
+                            const float* rdz, const float* tend_bar, float* field_bar, float* ru_bar, float* rv_bar,
+                            float* rom_bar, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (component < 0 || component > 2) return fail(WRF_EINVAL, "advect_momentum_adj: component 0..2");
+  if (!field || !ru || !rv || !rom || !msf || (component == 1 && !msf2) || !fzm || !fzp || !rdz || !tend_bar ||
+      !field_bar || !ru_bar || !rv_bar || !rom_bar)
+    return fail(WRF_EINVAL, "null argument");
+  cudaGetLastError();
+  launch_advect_mom_adj(g, component, field, ru, rv, rom, msf, msf2, fzm, fzp, rdz, tend_bar, field_bar, ru_bar,
+                        rv_bar, rom_bar, static_cast<cudaStream_t>(stream));
+  return check_launch("advect_momentum_adj");
+}
+
 int wrf_relax_bdytend(const WrfGrid* gin, const float* field, float* tend, const float* const* bdy8, char variable,
                       float dtbc, void* stream) {
   Grid g;

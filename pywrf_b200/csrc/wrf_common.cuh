@@ -115,7 +115,8 @@ __device__ __forceinline__ float flux5(float qm3, float qm2, float qm1, float q0
 // point of the band: rows [jds, jds+5) and [jde-5, jde) over columns
 // [ids, ide], then columns [ids, ids+5) and [ide-5, ide] of the rows
 // between - every point those updates touch, once, when the domain spans at
-// least 10 rows and 11 columns (else the kernels run over every point).
+// least 10 rows and 11 columns (else, and in the WRF_FORM_POINT cross-check
+// form, the kernels run over every point).
 __device__ __forceinline__ bool ring_point(const Grid& g, int r, int& j, int& i) {
   const int w = g.ide + 1 - g.ids;
   if (r < 10 * w) {

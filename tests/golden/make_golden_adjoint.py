@@ -12,6 +12,14 @@ the returned tendency with torch autograd, and writes next to this script:
 * ``relax_adj_ref64.npz`` -- ``pywrf.wrf_boundary.relax_bdytend``
   (wrf_boundary.py:52-147) w.r.t. the field, for the staggers 't', 'u', 'v'
   and 'h', with the solver's fcx / gcx (solver.py:440-441);
+* ``adv_mom_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.advect_u`` / ``advect_v``
+  / ``advect_w`` (wrf_dynamics.py:1112-1823) w.r.t. the advected component
+  and the three coupled velocities ru, rv, rom (both signs everywhere, so the
+  upwind choices and the sign-selected boundary values of advect_u / advect_v
+  take both branches); advect_w's backward() raises in the reference (its
+  vertical part rewrites ``vel`` in place after a product saved it), so for
+  w the fixture holds central finite differences of the reference's float64
+  forward along 3 seeded directions per input (``mom_direction``);
 * ``coefw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_coef_w``
   (wrf_dynamics.py:3316-3388): the reference's autograd cannot differentiate
   it (the recurrence updates ``gamma`` in place between its reads, and
@@ -58,9 +66,95 @@ def inputs(seed: int = 11) -> dict[str, np.ndarray]:
     }
 
 
+def mom_direction(n: int, r: int, shape) -> np.ndarray:
+    """Direction r of input n (field, ru, rv, rom) of the advect_w finite
+    differences (regenerated by the tests, not stored)."""
+    return np.random.default_rng(7000 + 10 * n + r).standard_normal(shape)
+
+
+def momentum(dyn, g) -> None:
+    """advect_u / advect_v / advect_w with autograd (adv_mom_adj_ref64.npz)."""
+    import torch
+
+    rng = np.random.default_rng(14)
+    shape = (NZ, N, N)
+    ids, ide, jds, jde = 5, N - 5, 5, N - 5
+    save = {"dx": np.array(g.dx), "dy": np.array(g.dy)}
+    prof = {"fnm": 0.45 + 0.1 * rng.random(NZ), "fnp": 0.45 + 0.1 * rng.random(NZ),
+            "rdnw": -(8.0 + 4.0 * rng.random(NZ)), "rdn": -(8.0 + 4.0 * rng.random(NZ))}
+    prof = {k: v.astype(np.float32) for k, v in prof.items()}
+    save.update(prof)
+    ones2 = torch.ones((N, N), dtype=torch.float64)
+    one1 = torch.ones(NZ, dtype=torch.float64)
+    fn = {"u": dyn.advect_u, "v": dyn.advect_v, "w": dyn.advect_w}
+    for comp in ("u", "v", "w"):
+        d = {
+            "field": 4.0 * rng.standard_normal(shape) + (2.0 if comp == "u" else 0.0),
+            "ru": 20.0 * rng.standard_normal(shape) + 5.0,
+            "rv": 20.0 * rng.standard_normal(shape) - 5.0,
+            "rom": 2.0 * rng.standard_normal(shape),
+            "msf": 1.0 + 0.05 * rng.random((N, N)),
+            "msf2": 1.0 + 0.05 * rng.random((N, N)),
+            "cot": rng.standard_normal(shape),
+        }
+        # float32-representable inputs, stored as float32 (the float64 forward
+        # of the stored values is then exactly what the fixture records)
+        d = {k: v.astype(np.float32) for k, v in d.items()}
+        t = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
+        for k in ("field", "ru", "rv", "rom"):
+            t[k].requires_grad_(True)
+        # map factors in the reference's argument order msfux, msfuy, msfvx, msfvy, msftx, msfty:
+        # advect_u reads msfux, advect_v msfvx and msfvy, advect_w msftx
+        msfs = [ones2] * 6
+        if comp == "u":
+            msfs[0] = t["msf"]
+        elif comp == "v":
+            msfs[3], msfs[2] = t["msf"], t["msf2"]
+        else:
+            msfs[4] = t["msf"]
+        rdz = torch.tensor(prof["rdn" if comp == "w" else "rdnw"], dtype=torch.float64)
+        fnm, fnp = (torch.tensor(prof[k], dtype=torch.float64) for k in ("fnm", "fnp"))
+        def run(x):
+            return fn[comp](x["field"], x["field"], torch.zeros(shape, dtype=torch.float64), x["ru"], x["rv"],
+                            x["rom"], one1, one1 * 0.0, ones2, int(g.dt), *msfs, fnm, fnp, 1.0 / g.dx, 1.0 / g.dy,
+                            rdz, ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+
+        for k, v in d.items():
+            save[f"{comp}_{k}"] = v
+        if comp != "w":
+            out = run(t)
+            (out * t["cot"]).sum().backward()
+            save[f"{comp}_tend"] = out.detach().numpy()
+            for k in ("field", "ru", "rv", "rom"):
+                save[f"{comp}_grad_{k}"] = t[k].grad.numpy()
+            continue
+        # advect_w: the reference's vertical part rewrites ``vel`` in place
+        # after a product saved it (wrf_dynamics.py:1788), so backward()
+        # raises; the fixture holds central differences of its float64
+        # forward instead (exact up to rounding: the operator is bilinear in
+        # (field, velocities) with piecewise-constant upwind choices)
+        base = {k: t[k].detach().clone() for k in ("field", "ru", "rv", "rom")}
+        with torch.no_grad():
+            save["w_tend"] = run(base).numpy()
+            cot = t["cot"]
+            for n_, name in enumerate(("field", "ru", "rv", "rom")):
+                for r in range(3):
+                    dirn = mom_direction(n_, r, shape)
+                    eps = 1e-6 * float(base[name].abs().max())
+                    xp, xm = dict(base), dict(base)
+                    xp[name] = base[name] + eps * torch.tensor(dirn)
+                    xm[name] = base[name] - eps * torch.tensor(dirn)
+                    save[f"w_fd_{name}_{r}"] = np.array(
+                        float(((run(xp) - run(xm)) * cot).sum()) / (2 * eps))
+    np.savez_compressed(os.path.join(HERE, "adv_mom_adj_ref64.npz"), **save)
+    print("wrote adv_mom_adj_ref64.npz")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default=None)
+    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum"), default=None,
+                    help="write one fixture only")
     a = ap.parse_args()
     if a.reference:
         os.environ["PYWRF_REFERENCE_ROOT"] = a.reference
@@ -70,6 +164,11 @@ def main() -> None:
     spec = synthetic.CaseSpec(n=N, nz=NZ)
     g = synthetic.grid_for(spec)
     _cp, dyn, _phy, _bdy, _solver = refharness.load_reference(g, dtype="float64")
+    if a.only == "momentum":
+        momentum(dyn, g)
+        return
+    if a.only is not None:
+        raise SystemExit("--only: momentum is the fixture that can be written on its own")
     d = inputs()
     t = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
     for k in ("field", "ru", "rv", "rom"):
@@ -158,6 +257,7 @@ def main() -> None:
             save[f"fd_{name}_{r}"] = np.array((loss(xp)[0] - loss(xm)[0]) / (2 * eps))
     np.savez_compressed(os.path.join(HERE, "coefw_adj_ref64.npz"), **save)
     print("wrote coefw_adj_ref64.npz")
+    momentum(dyn, g)
 
 
 def importlib_bdy():

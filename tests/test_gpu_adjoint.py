@@ -135,3 +135,104 @@ def test_coef_w_and_its_adjoint_against_the_reference():
             an = float((gr * W[f"dir_{name}_{r}"]).sum())
             fd = float(W[f"fd_{name}_{r}"])
             assert abs(an - fd) <= 2e-4 * abs(fd), (name, r, an, fd)
+
+
+def _mom_dir(n, r, shape):
+    # the directions of make_golden_adjoint.mom_direction
+    return np.random.default_rng(7000 + 10 * n + r).standard_normal(shape)
+
+
+@pytest.mark.parametrize("comp", ["u", "v", "w"])
+def test_advect_momentum_adjoint_matches_the_reference(comp):
+    """advect_u / advect_v: the hand-written adjoint against the reference's
+    autograd gradients; advect_w (whose reference backward raises): its
+    directional derivatives against central differences of the reference's
+    float64 forward (tests/golden/adv_mom_adj_ref64.npz)."""
+    M = load_npz("adv_mom_adj_ref64.npz")
+    c = {"u": 0, "v": 1, "w": 2}[comp]
+    t = {k: _cuda(M[f"{comp}_{k}"]) for k in ("field", "ru", "rv", "rom", "msf", "msf2", "cot")}
+    for k in ("field", "ru", "rv", "rom"):
+        t[k].requires_grad_(True)
+    prof = {k: _cuda(M[k]) for k in ("fnm", "fnp", "rdnw", "rdn")}
+    tend0 = torch.zeros_like(t["field"], requires_grad=True)
+    out = adjoint.advect_momentum(c, t["field"], tend0, t["ru"], t["rv"], t["rom"], t["msf"],
+                                  t["msf2"] if comp == "v" else None, prof["fnm"], prof["fnp"],
+                                  prof["rdn" if comp == "w" else "rdnw"], 1.0 / float(M["dx"]), 1.0 / float(M["dy"]))
+    assert rel_l2(out.detach().cpu().numpy(), M[f"{comp}_tend"]) < 1e-6
+    (out * t["cot"]).sum().backward()
+    assert torch.equal(tend0.grad, t["cot"])
+    for n, k in enumerate(("field", "ru", "rv", "rom")):
+        gr = t[k].grad.double().cpu().numpy()
+        if comp != "w":
+            err = rel_l2(gr, M[f"{comp}_grad_{k}"])
+            assert err < 1e-5, (comp, k, err)
+        else:
+            for r in range(3):
+                an = float((gr * _mom_dir(n, r, gr.shape)).sum())
+                fd = float(M[f"w_fd_{k}_{r}"])
+                assert abs(an - fd) <= 1e-4 * abs(fd), (k, r, an, fd)
+
+
+@pytest.mark.parametrize("comp", ["u", "v", "w"])
+def test_advect_momentum_adjoint_at_64x64x41(comp):
+    """At 64x64x41: (1) the identity <A dq, c> = <dq, A^T c> for the field
+    (positive fields keep advect_u's / advect_v's sign-selected boundary
+    values on one branch, so the operator is linear in the field there);
+    (2) the velocity cotangents' directional derivatives against central
+    differences of the oracle's float64 forward."""
+    from oracle import dynamics as OD
+    from pywrf_b200 import synthetic
+
+    c = {"u": 0, "v": 1, "w": 2}[comp]
+    nz, n = 41, 64
+    shp = (nz, n, n)
+    rng = np.random.default_rng(41 + c)
+    q = 10.0 + 2.0 * np.abs(rng.standard_normal(shp))
+    vel = {"ru": 15.0 * rng.standard_normal(shp) + 3.0, "rv": 15.0 * rng.standard_normal(shp),
+           "rom": rng.standard_normal(shp)}
+    msf = 1.0 + 0.02 * rng.random((n, n))
+    msf2 = 1.0 + 0.02 * rng.random((n, n))
+    fnm = 0.5 + 0.05 * rng.random(nz)
+    fnp = 1.0 - fnm
+    rdz = -(10.0 + rng.random(nz))
+    cot = rng.standard_normal(shp)
+    dq = np.abs(rng.standard_normal(shp))
+    f32 = lambda a: np.asarray(a, np.float32).astype(np.float64)  # noqa: E731
+    q, msf, msf2, fnm, fnp, rdz, cot, dq = map(f32, (q, msf, msf2, fnm, fnp, rdz, cot, dq))
+    vel = {k: f32(v) for k, v in vel.items()}
+    C = {k: _cuda(v) for k, v in dict(q=q, msf=msf, msf2=msf2, fnm=fnm, fnp=fnp, rdz=rdz, cot=cot, dq=dq,
+                                      **vel).items()}
+    zero = torch.zeros_like(C["q"])
+
+    def fwd(field, ru, rv, rom):
+        return adjoint.advect_momentum(c, field, zero, ru, rv, rom, C["msf"], C["msf2"] if c == 1 else None,
+                                       C["fnm"], C["fnp"], C["rdz"], 1.0 / 9000.0, 1.0 / 9000.0)
+
+    leaves = {k: C[k].clone().requires_grad_(True) for k in ("q", "ru", "rv", "rom")}
+    (fwd(leaves["q"], leaves["ru"], leaves["rv"], leaves["rom"]) * C["cot"]).sum().backward()
+    a_dq = fwd(C["dq"], C["ru"], C["rv"], C["rom"]).double()
+    lhs = float((a_dq * C["cot"].double()).sum())
+    rhs = float((C["dq"].double() * leaves["q"].grad.double()).sum())
+    assert abs(lhs - rhs) <= 1e-5 * (abs(lhs) + abs(rhs)), (lhs, rhs)
+
+    g = synthetic.grid_for(synthetic.CaseSpec(n=n, nz=nz))
+
+    def oracle(x):
+        t = np.zeros(shp)
+        if c == 0:
+            OD.advect_u(g, q, t, x["ru"], x["rv"], x["rom"], msf, fnm, fnp, rdz)
+        elif c == 1:
+            OD.advect_v(g, q, t, x["ru"], x["rv"], x["rom"], msf2, msf, fnm, fnp, rdz)
+        else:
+            OD.advect_w(g, q, t, x["ru"], x["rv"], x["rom"], msf, fnm, fnp, rdz)
+        return t
+
+    for k in ("ru", "rv", "rom"):
+        d = rng.standard_normal(shp)
+        eps = 1e-6 * float(np.abs(vel[k]).max())
+        xp, xm = dict(vel), dict(vel)
+        xp[k] = vel[k] + eps * d
+        xm[k] = vel[k] - eps * d
+        fd = float(((oracle(xp) - oracle(xm)) * cot).sum()) / (2 * eps)
+        an = float((leaves[k].grad.double().cpu().numpy() * d).sum())
+        assert abs(an - fd) <= 1e-4 * abs(fd), (comp, k, an, fd)

@@ -1,7 +1,8 @@
 """Whole steps with the tiled tensor-map kernels (WRF_FORM_FAST) against the
-same steps with the one-thread-per-point and cp.async forms (WRF_FORM_POINT):
-every field of the state must agree to the bit, since both forms perform the
-reference's operations in the same order.  Grids: 28x28x16 (partial tiles,
+same steps with the one-thread-per-point and cp.async forms (WRF_FORM_POINT,
+which also runs the boundary relaxation over every point instead of the
+boundary band): every field of the state must agree to the bit, since both
+forms perform the reference's operations in the same order.  Grids: 28x28x16 (partial tiles,
 boundary blocks only) and 108x108x41 (interior blocks on the branch-free
 paths, several level chunks per kernel)."""
 from __future__ import annotations

@@ -110,3 +110,54 @@ def test_coefw_fixture_pinned_by_the_oracle():
         fd = (loss(xp) - loss(xm)) / (2 * eps)
         ref = float(W[f"fd_{name}_0"])
         assert abs(fd - ref) <= 1e-6 * abs(ref), (name, fd, ref)
+
+
+M = load_npz("adv_mom_adj_ref64.npz")
+
+
+def _mom_dir(n, r, shape):
+    # the directions of make_golden_adjoint.mom_direction
+    return np.random.default_rng(7000 + 10 * n + r).standard_normal(shape)
+
+
+def _mom(g, comp, field, ru, rv, rom):
+    t = np.zeros_like(field, dtype=np.float64)
+    f64 = {k: np.asarray(v, np.float64) for k, v in dict(field=field, ru=ru, rv=rv, rom=rom).items()}
+    prof = {k: M[k].astype(np.float64) for k in ("fnm", "fnp", "rdnw", "rdn")}
+    msf = M[f"{comp}_msf"].astype(np.float64)
+    if comp == "u":
+        OD.advect_u(g, f64["field"], t, f64["ru"], f64["rv"], f64["rom"], msf, prof["fnm"], prof["fnp"], prof["rdnw"])
+    elif comp == "v":
+        OD.advect_v(g, f64["field"], t, f64["ru"], f64["rv"], f64["rom"], M["v_msf2"].astype(np.float64), msf,
+                    prof["fnm"], prof["fnp"], prof["rdnw"])
+    else:
+        OD.advect_w(g, f64["field"], t, f64["ru"], f64["rv"], f64["rom"], msf, prof["fnm"], prof["fnp"], prof["rdn"])
+    return t
+
+
+def test_momentum_fixture_pinned_by_the_oracle():
+    """advect_u / advect_v / advect_w: the oracle reproduces the reference's
+    tendencies on the fixture; for u and v the golden autograd gradients'
+    directional derivatives equal the oracle's central differences, and for w
+    (whose reference backward raises) the oracle's central differences equal
+    the fixture's, made from the reference's float64 forward."""
+    g = _grid()
+    assert g.dx == float(M["dx"])
+    names = ("field", "ru", "rv", "rom")
+    for comp in ("u", "v", "w"):
+        base = {k: M[f"{comp}_{k}"].astype(np.float64) for k in names}
+        ref = M[f"{comp}_tend"]
+        assert np.abs(_mom(g, comp, **base) - ref).max() <= 1e-12 * np.abs(ref).max(), comp
+        cot = M[f"{comp}_cot"].astype(np.float64)
+        for n, name in enumerate(names):
+            d = _mom_dir(n, 0, base[name].shape)
+            eps = 1e-6 * float(np.abs(base[name]).max())
+            xp, xm = dict(base), dict(base)
+            xp[name] = base[name] + eps * d
+            xm[name] = base[name] - eps * d
+            fd = float(((_mom(g, comp, **xp) - _mom(g, comp, **xm)) * cot).sum()) / (2 * eps)
+            if comp == "w":
+                want = float(M[f"w_fd_{name}_0"])
+            else:
+                want = float((d * M[f"{comp}_grad_{name}"]).sum())
+            assert abs(fd - want) <= 1e-6 * abs(want) + 1e-9, (comp, name, fd, want)
