@@ -189,6 +189,22 @@ int wrf_advect_scalar_adj(const WrfGrid* g, const float* field, const float* ru,
                           const float* rom, const float* msftx, const float* fzm, const float* fzp,
                           const float* rdzw, const float* tend_bar, float* field_bar, float* ru_bar,
                           float* rv_bar, float* rom_bar, void* stream);
+/* wrf_dynamics.py:3391-3525 advance_uv followed by spec_bdyupdate of u and
+ * v (wrf_boundary.py:244-290), as the acoustic substep calls them
+ * (solver.py:1350-1377): u and v of the state table are updated in place
+ * from the table's ru_tend, rv_tend, p, pb, ph, php, alt, al, mu, muu, muv,
+ * cqu, cqv, mudf, msfux, msfuy, msfvx, msfvx_inv, msfvy, fnm, fnp, rdnw and
+ * the grid's emdiv, cf1..cf3 (spec_zone 1); fields it does not read may be
+ * null.  Runs the kernel of the form wrf_set_kernel_form selects. */
+int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream);
+/* Its adjoint (reverse mode): sbar holds, under the same field ids, the
+ * cotangents of the updated u and v (which are also those of the incoming
+ * u and v: du'/du = 1) and accumulates (+=) those of ru_tend, rv_tend, p, pb,
+ * ph, php, alt, al, mu, muu, muv, cqu, cqv and mudf, all required.  The
+ * reference's autograd cannot differentiate advance_uv (an in-place update
+ * of a saved operand), so the product is checked against finite differences
+ * of its forward. */
+int wrf_advance_uv_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float dts, void* stream);
 /* Adjoint of wrf_advect_momentum (reverse mode): given the cotangent tend_bar
  * of the updated tendency, accumulates (+=) the cotangents of the advected
  * component (field) and of ru, rv and rom; the arguments are those of

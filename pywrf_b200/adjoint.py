@@ -11,6 +11,11 @@ operators keeps no tape of the forward's intermediates.
 * :class:`AdvectMomentum` -- ``tendency + advect_u / advect_v / advect_w``
   (pywrf/wrf_dynamics.py:1112-1823); gradients with respect to the advected
   component, the incoming tendency and ru, rv, rom.
+* :class:`AdvanceUV` -- advance_uv followed by spec_bdyupdate of u and v
+  (pywrf/wrf_dynamics.py:3391-3525, pywrf/wrf_boundary.py:244-290), the
+  horizontal-momentum part of the acoustic substep; gradients with respect to
+  u, v, ru_tend, rv_tend, p, pb, ph, php, alt, al, mu, muu, muv, cqu, cqv and
+  mudf (map factors and vertical profiles are data).
 * :class:`RelaxBdytend` -- ``tendency + relax(field)`` toward the lateral
   boundary values (pywrf/wrf_boundary.py:52-147); gradients with respect to
   the field and the incoming tendency (the boundary arrays are data).
@@ -126,6 +131,63 @@ def advect_momentum(component, field, tendency, ru, rv, rom, msf, msf2, fzm, fzp
     """Differentiable ``tendency + advect_{u,v,w}(field)`` on the GPU
     (component 0, 1, 2)."""
     return AdvectMomentum.apply(component, field, tendency, ru, rv, rom, msf, msf2, fzm, fzp, rdz, rdx, rdy)
+
+
+UV_INPUTS = ("u", "v", "ru_tend", "rv_tend", "p", "pb", "ph", "php", "alt", "al", "mu", "muu", "muv", "cqu", "cqv",
+             "mudf")
+UV_DATA = ("msfux", "msfuy", "msfvx", "msfvx_inv", "msfvy", "fnm", "fnp", "rdnw")
+
+
+def _table(named: dict):
+    """A state table (WrfState) holding the given fields by name."""
+    names = N.field_names()
+    arr = (ctypes.c_void_p * len(names))()
+    for k, t in named.items():
+        arr[names.index(k)] = _ptr(t).value
+    return arr
+
+
+class AdvanceUV(torch.autograd.Function):
+    """(u', v') = advance_uv + spec_bdyupdate(u), (v); the tensors follow
+    UV_INPUTS then UV_DATA, ``scal`` = (dts, emdiv, cf1, cf2, cf3, rdx, rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, *tensors):
+        dts, emdiv, cf1, cf2, cf3, rdx, rdy = (float(x) for x in scal)
+        named = dict(zip(UV_INPUTS + UV_DATA, tensors))
+        cg = scalar_grid(named["u"].shape, rdx, rdy)
+        cg.emdiv, cg.cf1, cg.cf2, cg.cf3 = emdiv, cf1, cf2, cf3
+        u_new, v_new = named["u"].detach().clone(), named["v"].detach().clone()
+        tab = _table({**named, "u": u_new, "v": v_new})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(u_new.device):
+            rc = N.lib().wrf_advance_uv(ctypes.byref(cg), tab, dts, stream)
+        N.check(rc, "wrf_advance_uv")
+        ctx.save_for_backward(*tensors)
+        ctx.cg, ctx.dts = cg, dts
+        return u_new, v_new
+
+    @staticmethod
+    def backward(ctx, gu, gv):
+        tensors = ctx.saved_tensors
+        named = dict(zip(UV_INPUTS + UV_DATA, tensors))
+        gu = torch.zeros_like(named["u"]) if gu is None else gu.contiguous()
+        gv = torch.zeros_like(named["v"]) if gv is None else gv.contiguous()
+        bars = {k: torch.zeros_like(named[k]) for k in UV_INPUTS[2:]}
+        tab = _table(named)
+        btab = _table({"u": gu, "v": gv, **bars})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(gu.device):
+            rc = N.lib().wrf_advance_uv_adj(ctypes.byref(ctx.cg), tab, btab, ctx.dts, stream)
+        N.check(rc, "wrf_advance_uv_adj")
+        return (None, gu, gv) + tuple(bars[k] for k in UV_INPUTS[2:]) + (None,) * len(UV_DATA)
+
+
+def advance_uv(inputs: dict, data: dict, dts, emdiv, cf1, cf2, cf3, rdx, rdy):
+    """Differentiable advance_uv + spec_bdyupdate(u), (v) on the GPU:
+    ``inputs`` maps UV_INPUTS, ``data`` UV_DATA to tensors; returns (u', v')."""
+    return AdvanceUV.apply((dts, emdiv, cf1, cf2, cf3, rdx, rdy), *[inputs[k] for k in UV_INPUTS],
+                           *[data[k] for k in UV_DATA])
 
 
 BDY_NAMES = ("xs", "xe", "ys", "ye", "txs", "txe", "tys", "tye")

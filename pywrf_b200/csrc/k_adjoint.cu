@@ -35,6 +35,23 @@
 //                        with Fbar(f) from the tendency cotangent of the cells
 //                        either side of f (one writer per output element).
 //
+//   k_advance_uv_adj / k_advance_uv_adj_col  adjoint of advance_uv
+//                        (wrf_dynamics.py:3391-3525) with spec_bdyupdate of
+//                        u and v (wrf_boundary.py:244-290), forward
+//                        k_advance_uv / k_advance_uv_tma.  At an updated
+//                        u point, u' = u + dts ru_tend - dts cqu dp + mudf_xy
+//                        with dp = A B + C D:
+//     A = r rdx muu / 2,  B = dph(k+1) + dph(k) + (alt + alt_w) dp_x + (al + al_w) dpb_x,
+//     C = r rdx dphp_x,   D = rdnw(k) (dpn(k+1) - dpn(k)) - (mu + mu_w) / 2
+//                        (r = msfux / msfuy, _w the west neighbour, _x the
+//                        difference to it, dpn the vertical pressure average
+//                        of the two columns); v likewise in y.  The point
+//                        kernel gathers the 3-D cotangents from the u and v
+//                        points whose stencils hold the point, the column
+//                        kernel sums the 2-D ones (muu, muv, mu, mudf) over
+//                        the levels.  The cotangents of u and v pass through
+//                        (du'/du = 1).
+//
 //   k_relax_field / k_relax_field_adj  relax_bdytend (wrf_boundary.py:52-147)
 //                        on one field, and its adjoint with respect to the
 //                        field: at a relaxation point P of distance b,
@@ -243,6 +260,169 @@ __global__ void k_advect_scalar_adj(Grid g, AdvArgs0 a, const float* tbar, float
       }
     }
   }
+}
+
+// ------------------------------------------------------------ advance_uv
+
+namespace {
+
+// the points advance_uv updates (spec_zone 1) and the specified rows that
+// spec_bdyupdate updates, as in k_advance_uv
+__device__ __forceinline__ bool uv_in(const Grid& g, int V, int j, int i) {
+  return V == 0 ? (j >= g.jds + 1 && j < g.jde - 2 && i >= g.ids + 1 && i < g.ide - 1)
+                : (j >= g.jds + 1 && j < g.jde - 1 && i >= g.ids + 1 && i < g.ide - 2);
+}
+__device__ __forceinline__ bool uv_spec(const Grid& g, int V, int j, int i) {
+  const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde;
+  return V == 0 ? (((j == jds || j == jde - 2) && i >= ids && i < ide) ||
+                   (j >= jds + 1 && j < jde - 2 && (i == ids || i == ide - 1)))
+                : (((j == jds || j == jde - 1) && i >= ids && i < ide - 1) ||
+                   (j >= jds + 1 && j < jde - 1 && (i == ids || i == ide - 2)));
+}
+
+__device__ __forceinline__ float uv_dpn(const Grid& g, const S& s, int kk, size_t ca, size_t cb) {
+  const size_t lev = (size_t)g.ny * g.nx;
+  const float* pp = s[WF_P];
+  if (kk == 0)
+    return 0.5f * (g.cf1 * (pp[ca] + pp[cb]) + g.cf2 * (pp[lev + ca] + pp[lev + cb]) + g.cf3 * (pp[2 * lev + ca] + pp[2 * lev + cb]));
+  if (kk == g.nz - 1) return 0.f;
+  return 0.5f * (s[WF_FNM][kk] * (pp[kk * lev + ca] + pp[kk * lev + cb]) +
+                 s[WF_FNP][kk] * (pp[(kk - 1) * lev + ca] + pp[(kk - 1) * lev + cb]));
+}
+
+// d dpn(kk) / d p(k) at either column of the pair
+__device__ __forceinline__ float uv_dpn_coef(const Grid& g, const S& s, int kk, int k) {
+  if (kk == 0) return k == 0 ? 0.5f * g.cf1 : k == 1 ? 0.5f * g.cf2 : k == 2 ? 0.5f * g.cf3 : 0.f;
+  if (kk < 0 || kk >= g.nz - 1) return 0.f;
+  if (k == kk) return 0.5f * s[WF_FNM][kk];
+  if (k == kk - 1) return 0.5f * s[WF_FNP][kk];
+  return 0.f;
+}
+
+// the factors of dp at an updated point of u (V = 0) or v (V = 1), the
+// cotangent ub of its new value and dpb = d L / d dp
+struct UvTerm {
+  float ub, dpb, A, B, Cf, C, D;
+};
+
+__device__ UvTerm uv_term(const Grid& g, const S& s, const S& b, float dts, int V, int k, int j, int i) {
+  const size_t lev = (size_t)g.ny * g.nx;
+  const size_t c = (size_t)j * g.nx + i, p = k * lev + c, no = V ? (size_t)g.nx : 1;
+  const float* ph = s[WF_PH];
+  const float* pp = s[WF_P];
+  const float* alt = s[WF_ALT];
+  const float* al = s[WF_AL];
+  const float* pb = s[WF_PB];
+  const float* php = s[WF_PHP];
+  const float* mu = s[WF_MU];
+  const float r = V ? s[WF_MSFVY][c] / s[WF_MSFVX][c] : s[WF_MSFUX][c] / s[WF_MSFUY][c];
+  const float rd = V ? g.rdy : g.rdx;
+  UvTerm t;
+  t.ub = b[V ? WF_V : WF_U][p];
+  t.dpb = -dts * s[V ? WF_CQV : WF_CQU][p] * t.ub;
+  t.A = r * 0.5f * rd * s[V ? WF_MUV : WF_MUU][c];
+  t.B = ((ph[p + lev] - ph[p + lev - no]) + (ph[p] - ph[p - no])) + (alt[p] + alt[p - no]) * (pp[p] - pp[p - no]) +
+        (al[p] + al[p - no]) * (pb[p] - pb[p - no]);
+  t.Cf = r * rd;
+  t.C = t.Cf * (php[p] - php[p - no]);
+  t.D = s[WF_RDNW][k] * (uv_dpn(g, s, k + 1, c, c - no) - uv_dpn(g, s, k, c, c - no)) - 0.5f * (mu[c - no] + mu[c]);
+  return t;
+}
+
+}  // namespace
+
+__global__ void k_advance_uv_adj(Grid g, S s, S b, float dts) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const int ktf = g.nz - 1, nx = g.nx;
+  const size_t lev = (size_t)g.ny * nx;
+  const size_t m = (size_t)k * lev + (size_t)j * nx + i;
+  if (k < ktf) {
+    if (uv_in(g, 0, j, i) || uv_spec(g, 0, j, i)) b[WF_RU_TEND][m] += dts * b[WF_U][m];
+    if (uv_in(g, 1, j, i) || uv_spec(g, 1, j, i)) b[WF_RV_TEND][m] += dts * b[WF_V][m];
+  }
+  float aph = 0.f, aalt = 0.f, aal = 0.f, apb = 0.f, aphp = 0.f, ap = 0.f;
+  for (int V = 0; V < 2; ++V) {
+    const size_t no = V ? (size_t)nx : 1;
+    // the points P = (kP, j + V e, i + (1 - V) e), e = 0 (m is P's own
+    // column, sign +) or 1 (m is P's west / south neighbour, sign -)
+    for (int e = 0; e < 2; ++e) {
+      const int jP = j + V * e, iP = i + (1 - V) * e;
+      if (jP >= g.ny || iP >= nx || !uv_in(g, V, jP, iP)) continue;
+      const float sg = e == 0 ? 1.f : -1.f;
+      for (int kP = k - 2; kP <= k + 1; ++kP) {
+        if (kP < 0 || kP >= ktf) continue;
+        const UvTerm t = uv_term(g, s, b, dts, V, kP, jP, iP);
+        if (t.dpb == 0.f) continue;
+        const float Bb = t.dpb * t.A, Db = t.dpb * t.C;
+        const size_t P = (size_t)kP * lev + (size_t)jP * nx + iP;
+        if (kP == k || kP == k - 1) aph += sg * Bb;  // ph at kP and kP + 1
+        if (kP == k) {
+          aalt += Bb * (s[WF_P][P] - s[WF_P][P - no]);
+          aal += Bb * (s[WF_PB][P] - s[WF_PB][P - no]);
+          apb += sg * Bb * (s[WF_AL][P] + s[WF_AL][P - no]);
+          ap += sg * Bb * (s[WF_ALT][P] + s[WF_ALT][P - no]);
+          aphp += sg * t.dpb * t.Cf * t.D;
+        }
+        // p through dpn(kP + 1) - dpn(kP) (both columns of the pair, sign +)
+        const float rw = s[WF_RDNW][kP] * Db;
+        ap += rw * (uv_dpn_coef(g, s, kP + 1, k) - uv_dpn_coef(g, s, kP, k));
+      }
+    }
+  }
+  if (k < ktf) {
+    if (uv_in(g, 0, j, i)) {
+      const UvTerm t = uv_term(g, s, b, dts, 0, k, j, i);
+      b[WF_CQU][m] += -dts * (t.A * t.B + t.C * t.D) * t.ub;
+    }
+    if (uv_in(g, 1, j, i)) {
+      const UvTerm t = uv_term(g, s, b, dts, 1, k, j, i);
+      b[WF_CQV][m] += -dts * (t.A * t.B + t.C * t.D) * t.ub;
+    }
+  }
+  if (aph != 0.f) b[WF_PH][m] += aph;
+  if (aalt != 0.f) b[WF_ALT][m] += aalt;
+  if (aal != 0.f) b[WF_AL][m] += aal;
+  if (apb != 0.f) b[WF_PB][m] += apb;
+  if (aphp != 0.f) b[WF_PHP][m] += aphp;
+  if (ap != 0.f) b[WF_P][m] += ap;
+}
+
+__global__ void k_advance_uv_adj_col(Grid g, S s, S b, float dts) {
+  WRF_COLUMN_INDEX(g, j, i);
+  const int ktf = g.nz - 1, nx = g.nx;
+  const size_t c = (size_t)j * nx + i;
+  const float eu = (float)(-(double)g.emdiv * g.dxd), ev = (float)(-(double)g.emdiv * g.dyd);
+  float amuu = 0.f, amuv = 0.f, amu = 0.f, amudf = 0.f;
+  for (int V = 0; V < 2; ++V)
+    for (int e = 0; e < 2; ++e) {
+      const int jP = j + V * e, iP = i + (1 - V) * e;
+      if (jP >= g.ny || iP >= nx || !uv_in(g, V, jP, iP)) continue;
+      const size_t cP = (size_t)jP * nx + iP;
+      const float sg = e == 0 ? 1.f : -1.f;
+      const float em = V ? ev * s[WF_MSFVX_INV][cP] : eu / s[WF_MSFUY][cP];
+      for (int k = 0; k < ktf; ++k) {
+        const UvTerm t = uv_term(g, s, b, dts, V, k, jP, iP);
+        if (e == 0) {
+          const float r = V ? s[WF_MSFVY][cP] / s[WF_MSFVX][cP] : s[WF_MSFUX][cP] / s[WF_MSFUY][cP];
+          const float d = t.dpb * (r * 0.5f * (V ? g.rdy : g.rdx)) * t.B;
+          if (V) amuv += d;
+          else amuu += d;
+        }
+        amu += -0.5f * t.dpb * t.C;
+        amudf += sg * t.ub * em;
+      }
+    }
+  if (amuu != 0.f) b[WF_MUU][c] += amuu;
+  if (amuv != 0.f) b[WF_MUV][c] += amuv;
+  if (amu != 0.f) b[WF_MU][c] += amu;
+  if (amudf != 0.f) b[WF_MUDF][c] += amudf;
+}
+
+int launch_advance_uv_adj(const Grid& g, const S& s, const S& b, float dts, cudaStream_t st) {
+  const dim3 b3(32, 4), b2(32, 8);
+  k_advance_uv_adj<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, dts);
+  k_advance_uv_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, dts);
+  return 2;
 }
 
 // stagger of a relaxed field: the bounds of relax_bdytend's zones and levels

@@ -522,6 +522,48 @@ int wrf_advect_scalar_adj(const WrfGrid* gin, const float* field, const float* r
   return check_launch("advect_scalar_adj");
 }
 
+namespace {
+// the forward operands of advance_uv in the state table
+constexpr int kUvOperands[] = {WF_U, WF_V, WF_RU_TEND, WF_RV_TEND, WF_P, WF_PB, WF_PH, WF_PHP, WF_ALT, WF_AL, WF_MU,
+                               WF_MUU, WF_MUV, WF_CQU, WF_CQV, WF_MUDF, WF_MSFUX, WF_MSFUY, WF_MSFVX, WF_MSFVX_INV,
+                               WF_MSFVY, WF_FNM, WF_FNP, WF_RDNW};
+// the cotangents it reads (U, V) and accumulates
+constexpr int kUvCotangents[] = {WF_U, WF_V, WF_RU_TEND, WF_RV_TEND, WF_P, WF_PB, WF_PH, WF_PHP, WF_ALT, WF_AL,
+                                 WF_MU, WF_MUU, WF_MUV, WF_CQU, WF_CQV, WF_MUDF};
+
+int state_of(const WrfState* in, const int* ids, int n, S& s) {
+  if (!in) return fail(WRF_EINVAL, "null state");
+  s = S{};
+  for (int q = 0; q < WF_COUNT; ++q) s.f[q] = static_cast<float*>(in->f[q]);
+  for (int e = 0; e < n; ++e)
+    if (!s.f[ids[e]]) return fail(WRF_EINVAL, "a field the operator needs is null");
+  return 0;
+}
+}  // namespace
+
+int wrf_advance_uv(const WrfGrid* gin, const WrfState* sin, float dts, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s;
+  if ((rc = state_of(sin, kUvOperands, sizeof(kUvOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_advance_uv(g, s, dts, static_cast<cudaStream_t>(stream));
+  return check_launch("advance_uv");
+}
+
+int wrf_advance_uv_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dts, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s, b;
+  if ((rc = state_of(sin, kUvOperands, sizeof(kUvOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kUvCotangents, sizeof(kUvCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_advance_uv_adj(g, s, b, dts, static_cast<cudaStream_t>(stream));
+  return check_launch("advance_uv_adj");
+}
+
 int wrf_advect_momentum_adj(const WrfGrid* gin, int component, const float* field, const float* ru, const float* rv,
                             const float* rom, const float* msf, const float* msf2, const float* fzm, const float* fzp,
                             const float* rdz, const float* tend_bar, float* field_bar, float* ru_bar, float* rv_bar,

@@ -20,6 +20,14 @@ the returned tendency with torch autograd, and writes next to this script:
   vertical part rewrites ``vel`` in place after a product saved it), so for
   w the fixture holds central finite differences of the reference's float64
   forward along 3 seeded directions per input (``mom_direction``);
+* ``advuv_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.advance_uv``
+  (wrf_dynamics.py:3391-3525) followed by ``spec_bdyupdate`` of u and v
+  (wrf_boundary.py:244-290), as the acoustic substep calls them
+  (solver.py:1350-1377): the reference's autograd cannot differentiate
+  advance_uv (``dpxy`` is rewritten for v after u's update saved a view of
+  it), so the fixture holds central differences of the float64 forward of
+  L = sum(u' cot_u + v' cot_v) along 3 seeded directions (``uv_direction``)
+  in each of the 16 differentiable inputs;
 * ``coefw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_coef_w``
   (wrf_dynamics.py:3316-3388): the reference's autograd cannot differentiate
   it (the recurrence updates ``gamma`` in place between its reads, and
@@ -64,6 +72,80 @@ def inputs(seed: int = 11) -> dict[str, np.ndarray]:
         "rdnw": -(8.0 + 4.0 * rng.random(NZ)),
         "cot": rng.standard_normal(shape),
     }
+
+
+UV3 = ("u", "ru_tend", "v", "rv_tend", "p", "pb", "ph", "php", "alt", "al", "cqu", "cqv")
+UV2 = ("mu", "muu", "muv", "mudf")
+
+
+def uv_direction(n: int, r: int, shape) -> np.ndarray:
+    """Direction r of input n (UV3 + UV2) of the advance_uv finite
+    differences (regenerated by the tests, not stored)."""
+    return np.random.default_rng(8000 + 100 * n + r).standard_normal(shape)
+
+
+def advance_uv(dyn, bnd, g) -> None:
+    """advance_uv + spec_bdyupdate(u), (v): central differences
+    (advuv_adj_ref64.npz)."""
+    import torch
+
+    rng = np.random.default_rng(15)
+    sh, s2 = (NZ, N, N), (N, N)
+    kk = np.arange(NZ, dtype=np.float64)[:, None, None]
+    d = {
+        "u": 10.0 + 3.0 * rng.standard_normal(sh), "ru_tend": 0.05 * rng.standard_normal(sh),
+        "v": 3.0 * rng.standard_normal(sh), "rv_tend": 0.05 * rng.standard_normal(sh),
+        "p": 100.0 * rng.standard_normal(sh), "pb": 8.0e4 - 5.0e3 * kk + 100.0 * rng.standard_normal(sh),
+        "ph": 50.0 * rng.standard_normal(sh), "php": 1.0e3 * (kk + 1.0) + 10.0 * rng.standard_normal(sh),
+        "alt": 1.0 + 0.05 * rng.standard_normal(sh), "al": 0.01 * rng.standard_normal(sh),
+        "cqu": 1.0 + 0.01 * rng.standard_normal(sh), "cqv": 1.0 + 0.01 * rng.standard_normal(sh),
+        "mu": 100.0 * rng.standard_normal(s2), "muu": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "muv": 8.0e4 + 1.0e3 * rng.standard_normal(s2), "mudf": 10.0 * rng.standard_normal(s2),
+        "msfux": 1.0 + 0.02 * rng.random(s2), "msfuy": 1.0 + 0.02 * rng.random(s2),
+        "msfvx": 1.0 + 0.02 * rng.random(s2), "msfvy": 1.0 + 0.02 * rng.random(s2),
+        "fnm": 0.45 + 0.1 * rng.random(NZ), "rdnw": -(10.0 + rng.random(NZ)),
+        "cot_u": rng.standard_normal(sh), "cot_v": rng.standard_normal(sh),
+    }
+    d["fnp"] = 1.0 - d["fnm"]
+    d = {k: v.astype(np.float32) for k, v in d.items()}
+    d["msfvx_inv"] = (1.0 / d["msfvx"].astype(np.float64)).astype(np.float32)
+    sc = {"dts": 11.25, "emdiv": 0.01, "cf1": 1.5, "cf2": -0.625, "cf3": 0.125}
+    t = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
+    one1 = torch.ones(NZ, dtype=torch.float64)
+    ids, ide, jds, jde = 5, N - 5, 5, N - 5
+    idx = (ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+    bidx = (ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+
+    def run(x):
+        u, v = dyn.advance_uv(x["u"], x["ru_tend"], x["v"], x["rv_tend"], x["p"], x["pb"], x["ph"], x["php"],
+                              x["alt"], x["al"], x["mu"], x["muu"], x["cqu"], x["muv"], x["cqv"], x["mudf"],
+                              one1, one1 * 0, one1, one1 * 0, one1, one1 * 0, one1, one1 * 0,
+                              x["msfux"], x["msfuy"], x["msfvx"], x["msfvx_inv"], x["msfvy"], 1.0 / g.dx,
+                              1.0 / g.dy, sc["dts"], sc["cf1"], sc["cf2"], sc["cf3"], x["fnm"], x["fnp"],
+                              sc["emdiv"], x["rdnw"], 1, True, False, *idx)
+        u = bnd.spec_bdyupdate(u, x["ru_tend"], sc["dts"], "u", 1, *bidx)
+        v = bnd.spec_bdyupdate(v, x["rv_tend"], sc["dts"], "v", 1, *bidx)
+        return u, v
+
+    save = dict(d)
+    save.update({k: np.array(v) for k, v in sc.items()})
+    save["dx"], save["dy"] = np.array(g.dx), np.array(g.dy)
+    with torch.no_grad():
+        u, v = run(t)
+        save["u_new"], save["v_new"] = u.numpy(), v.numpy()
+        cu, cv = t["cot_u"], t["cot_v"]
+        for n_, name in enumerate(UV3 + UV2):
+            for r in range(3):
+                dirn = torch.tensor(uv_direction(n_, r, d[name].shape))
+                eps = 1e-6 * float(t[name].abs().max())
+                xp, xm = dict(t), dict(t)
+                xp[name] = t[name] + eps * dirn
+                xm[name] = t[name] - eps * dirn
+                up, vp = run(xp)
+                um, vm = run(xm)
+                save[f"fd_{name}_{r}"] = np.array(float(((up - um) * cu).sum() + ((vp - vm) * cv).sum()) / (2 * eps))
+    np.savez_compressed(os.path.join(HERE, "advuv_adj_ref64.npz"), **save)
+    print("wrote advuv_adj_ref64.npz")
 
 
 def mom_direction(n: int, r: int, shape) -> np.ndarray:
@@ -153,7 +235,7 @@ def momentum(dyn, g) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default=None)
-    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum"), default=None,
+    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv"), default=None,
                     help="write one fixture only")
     a = ap.parse_args()
     if a.reference:
@@ -167,8 +249,11 @@ def main() -> None:
     if a.only == "momentum":
         momentum(dyn, g)
         return
+    if a.only == "advance_uv":
+        advance_uv(dyn, importlib_bdy(), g)
+        return
     if a.only is not None:
-        raise SystemExit("--only: momentum is the fixture that can be written on its own")
+        raise SystemExit("--only: momentum and advance_uv are the fixtures that can be written on their own")
     d = inputs()
     t = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
     for k in ("field", "ru", "rv", "rom"):
@@ -258,6 +343,7 @@ def main() -> None:
     np.savez_compressed(os.path.join(HERE, "coefw_adj_ref64.npz"), **save)
     print("wrote coefw_adj_ref64.npz")
     momentum(dyn, g)
+    advance_uv(dyn, importlib_bdy(), g)
 
 
 def importlib_bdy():

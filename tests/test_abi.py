@@ -99,6 +99,11 @@ def test_null_arguments_of_function_entry_points_are_rejected():
     assert rc == N.WRF_EINVAL
     rc = L.wrf_advect_momentum_adj(ctypes.byref(_cgrid()), 3, *([None] * 14), None)
     assert rc == N.WRF_EINVAL
+    rc = L.wrf_advance_uv(ctypes.byref(_cgrid()), None, ctypes.c_float(1.0), None)
+    assert rc == N.WRF_EINVAL
+    empty = (ctypes.c_void_p * L.wrf_field_count())()
+    rc = L.wrf_advance_uv_adj(ctypes.byref(_cgrid()), empty, empty, ctypes.c_float(1.0), None)
+    assert rc == N.WRF_EINVAL
     rc = L.wrf_status_read(None, None, None)
     assert rc == N.WRF_EINVAL
 

@@ -236,3 +236,39 @@ def test_advect_momentum_adjoint_at_64x64x41(comp):
         fd = float(((oracle(xp) - oracle(xm)) * cot).sum()) / (2 * eps)
         an = float((leaves[k].grad.double().cpu().numpy() * d).sum())
         assert abs(an - fd) <= 1e-4 * abs(fd), (comp, k, an, fd)
+
+
+def _uv_dir(n, r, shape):
+    # the directions of make_golden_adjoint.uv_direction
+    return np.random.default_rng(8000 + 100 * n + r).standard_normal(shape)
+
+
+@pytest.mark.parametrize("form", ["fast", "point"])
+def test_advance_uv_and_its_adjoint_against_the_reference(form):
+    """advance_uv + spec_bdyupdate(u), (v): u', v' against the reference's
+    on the fixture (both kernel forms), and the adjoint's directional
+    derivatives against central differences of the reference's float64
+    forward (tests/golden/advuv_adj_ref64.npz; its autograd cannot
+    differentiate advance_uv)."""
+    from pywrf_b200 import _native as N
+
+    V = load_npz("advuv_adj_ref64.npz")
+    inputs = {k: _cuda(V[k]).requires_grad_(True) for k in adjoint.UV_INPUTS}
+    data = {k: _cuda(V[k]) for k in adjoint.UV_DATA}
+    prev = N.lib().wrf_set_kernel_form(N.WRF_FORM_FAST if form == "fast" else N.WRF_FORM_POINT)
+    try:
+        u, v = adjoint.advance_uv(inputs, data, float(V["dts"]), float(V["emdiv"]), float(V["cf1"]),
+                                  float(V["cf2"]), float(V["cf3"]), 1.0 / float(V["dx"]), 1.0 / float(V["dy"]))
+    finally:
+        N.lib().wrf_set_kernel_form(prev)
+    assert rel_l2(u.detach().cpu().numpy(), V["u_new"]) < 1e-6
+    assert rel_l2(v.detach().cpu().numpy(), V["v_new"]) < 1e-6
+    ((u * _cuda(V["cot_u"])).sum() + (v * _cuda(V["cot_v"])).sum()).backward()
+    names = ("u", "ru_tend", "v", "rv_tend", "p", "pb", "ph", "php", "alt", "al", "cqu", "cqv",
+             "mu", "muu", "muv", "mudf")
+    for n, name in enumerate(names):
+        gr = inputs[name].grad.double().cpu().numpy()
+        for r in range(3):
+            an = float((gr * _uv_dir(n, r, gr.shape)).sum())
+            fd = float(V[f"fd_{name}_{r}"])
+            assert abs(an - fd) <= 1e-4 * abs(fd), (name, r, an, fd)

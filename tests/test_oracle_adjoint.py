@@ -161,3 +161,49 @@ def test_momentum_fixture_pinned_by_the_oracle():
             else:
                 want = float((d * M[f"{comp}_grad_{name}"]).sum())
             assert abs(fd - want) <= 1e-6 * abs(want) + 1e-9, (comp, name, fd, want)
+
+
+V = load_npz("advuv_adj_ref64.npz")
+UV3 = ("u", "ru_tend", "v", "rv_tend", "p", "pb", "ph", "php", "alt", "al", "cqu", "cqv")
+UV2 = ("mu", "muu", "muv", "mudf")
+
+
+def _uv_dir(n, r, shape):
+    # the directions of make_golden_adjoint.uv_direction
+    return np.random.default_rng(8000 + 100 * n + r).standard_normal(shape)
+
+
+def _advance_uv(g, x):
+    x = {k: np.array(v, np.float64) for k, v in x.items()}
+    c = {k: V[k].astype(np.float64) for k in ("msfux", "msfuy", "msfvx", "msfvx_inv", "msfvy", "fnm", "fnp", "rdnw")}
+    u, v = OD.advance_uv(g, x["u"], x["ru_tend"], x["v"], x["rv_tend"], x["p"], x["pb"], x["ph"], x["php"], x["alt"],
+                         x["al"], x["mu"], x["muu"], x["cqu"], x["muv"], x["cqv"], x["mudf"], c["msfux"], c["msfuy"],
+                         c["msfvx"], c["msfvx_inv"], c["msfvy"], float(V["dts"]), float(V["cf1"]), float(V["cf2"]),
+                         float(V["cf3"]), c["fnm"], c["fnp"], float(V["emdiv"]), c["rdnw"])
+    OB.spec_bdyupdate(g, u, x["ru_tend"], float(V["dts"]), "u")
+    OB.spec_bdyupdate(g, v, x["rv_tend"], float(V["dts"]), "v")
+    return u, v
+
+
+def test_advance_uv_fixture_pinned_by_the_oracle():
+    """advance_uv + spec_bdyupdate(u), (v): the oracle reproduces the
+    reference's u, v on the fixture, and its central differences reproduce
+    the fixture's (made from the reference's float64 forward: its autograd
+    cannot differentiate advance_uv)."""
+    g = _grid()
+    base = {k: V[k].astype(np.float64) for k in UV3 + UV2}
+    u, v = _advance_uv(g, base)
+    for mine, ref in ((u, V["u_new"]), (v, V["v_new"])):
+        assert np.abs(mine - ref).max() <= 1e-12 * np.abs(ref).max()
+    cu, cv = V["cot_u"].astype(np.float64), V["cot_v"].astype(np.float64)
+    for n, name in enumerate(UV3 + UV2):
+        d = _uv_dir(n, 0, base[name].shape)
+        eps = 1e-6 * float(np.abs(base[name]).max())
+        xp, xm = dict(base), dict(base)
+        xp[name] = base[name] + eps * d
+        xm[name] = base[name] - eps * d
+        up, vp = _advance_uv(g, xp)
+        um, vm = _advance_uv(g, xm)
+        fd = float(((up - um) * cu).sum() + ((vp - vm) * cv).sum()) / (2 * eps)
+        ref = float(V[f"fd_{name}_0"])
+        assert abs(fd - ref) <= 1e-6 * abs(ref) + 1e-9, (name, fd, ref)
