@@ -205,6 +205,18 @@ int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream)
  * of a saved operand), so the product is checked against finite differences
  * of its forward. */
 int wrf_advance_uv_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float dts, void* stream);
+/* wrf_dynamics.py:3269-3313 calc_p_rho on the state table, in place: al, p
+ * and pm1 from ph, alt, t_2 (field T), t_1 (T_SAVE), c2a, mu, mut (MUTS)
+ * and rdnw, with the grid's smdiv; step 0 sets pm1 to a copy of the whole
+ * new p, a later step applies the divergence damping p += smdiv (p - pm1)
+ * and keeps the undamped p in pm1 (the acoustic substep's use). */
+int wrf_calc_p_rho(const WrfGrid* g, const WrfState* s, int step, void* stream);
+/* Its adjoint: sbar's AL, P, PM1 hold the cotangents of the updated al, p,
+ * pm1 and are rewritten to those of the incoming al, p, pm1; the cotangents
+ * of ph, alt, T, T_SAVE, c2a (3-D) and mu, MUTS (2-D) are accumulated (+=).
+ * The reference obtains this product from torch autograd through
+ * wrf_dynamics.py:3269-3313. */
+int wrf_calc_p_rho_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, int step, void* stream);
 /* Adjoint of wrf_advect_momentum (reverse mode): given the cotangent tend_bar
  * of the updated tendency, accumulates (+=) the cotangents of the advected
  * component (field) and of ru, rv and rom; the arguments are those of

@@ -98,6 +98,10 @@ def lib() -> ctypes.CDLL:
     L.wrf_set_kernel_form.argtypes = [ctypes.c_int]
     L.wrf_advect_momentum.restype = ip
     L.wrf_advect_momentum.argtypes = [ctypes.POINTER(WrfGridC), ctypes.c_int] + [vp] * 10 + [ctypes.c_int, vp]
+    L.wrf_calc_p_rho.restype = ip
+    L.wrf_calc_p_rho.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_int, vp]
+    L.wrf_calc_p_rho_adj.restype = ip
+    L.wrf_calc_p_rho_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_int, vp]
     L.wrf_advance_uv.restype = ip
     L.wrf_advance_uv.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_float, vp]
     L.wrf_advance_uv_adj.restype = ip

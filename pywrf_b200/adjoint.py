@@ -16,6 +16,9 @@ operators keeps no tape of the forward's intermediates.
   horizontal-momentum part of the acoustic substep; gradients with respect to
   u, v, ru_tend, rv_tend, p, pb, ph, php, alt, al, mu, muu, muv, cqu, cqv and
   mudf (map factors and vertical profiles are data).
+* :class:`CalcPRho` -- calc_p_rho (pywrf/wrf_dynamics.py:3269-3313): al, p,
+  pm1 from ph, alt, t_2, t_1, c2a, pm1, mu, mut at a given acoustic step;
+  gradients with respect to all ten.
 * :class:`RelaxBdytend` -- ``tendency + relax(field)`` toward the lateral
   boundary values (pywrf/wrf_boundary.py:52-147); gradients with respect to
   the field and the incoming tendency (the boundary arrays are data).
@@ -188,6 +191,55 @@ def advance_uv(inputs: dict, data: dict, dts, emdiv, cf1, cf2, cf3, rdx, rdy):
     ``inputs`` maps UV_INPUTS, ``data`` UV_DATA to tensors; returns (u', v')."""
     return AdvanceUV.apply((dts, emdiv, cf1, cf2, cf3, rdx, rdy), *[inputs[k] for k in UV_INPUTS],
                            *[data[k] for k in UV_DATA])
+
+
+PRHO_INPUTS = ("al", "p", "ph", "alt", "t_2", "t_1", "c2a", "pm1", "mu", "mut")
+# the state-table names of calc_p_rho's arguments in the acoustic substep
+_PRHO_FIELD = {"t_2": "t", "t_1": "t_save", "mut": "muts"}
+
+
+class CalcPRho(torch.autograd.Function):
+    """(al', p', pm1') = calc_p_rho(...) at acoustic step ``step``; the
+    tensors follow PRHO_INPUTS then rdnw, ``scal`` = (smdiv, step, rdx, rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, *tensors):
+        smdiv, step, rdx, rdy = float(scal[0]), int(scal[1]), float(scal[2]), float(scal[3])
+        named = dict(zip(PRHO_INPUTS + ("rdnw",), tensors))
+        cg = scalar_grid(named["p"].shape, rdx, rdy)
+        cg.smdiv = smdiv
+        outs = {k: named[k].detach().clone() for k in ("al", "p", "pm1")}
+        tab = _table({_PRHO_FIELD.get(k, k): v for k, v in {**named, **outs}.items()})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(outs["p"].device):
+            rc = N.lib().wrf_calc_p_rho(ctypes.byref(cg), tab, step, stream)
+        N.check(rc, "wrf_calc_p_rho")
+        ctx.save_for_backward(*tensors)
+        ctx.cg, ctx.step = cg, step
+        return outs["al"], outs["p"], outs["pm1"]
+
+    @staticmethod
+    def backward(ctx, gal, gp, gpm1):
+        tensors = ctx.saved_tensors
+        named = dict(zip(PRHO_INPUTS + ("rdnw",), tensors))
+        out_b = {}
+        for k, gk in (("al", gal), ("p", gp), ("pm1", gpm1)):
+            out_b[k] = torch.zeros_like(named[k]) if gk is None else gk.contiguous().clone()
+        bars = {k: torch.zeros_like(named[k]) for k in PRHO_INPUTS if k not in out_b}
+        tab = _table({_PRHO_FIELD.get(k, k): v for k, v in named.items()})
+        btab = _table({_PRHO_FIELD.get(k, k): v for k, v in {**out_b, **bars}.items()})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(named["p"].device):
+            rc = N.lib().wrf_calc_p_rho_adj(ctypes.byref(ctx.cg), tab, btab, ctx.step, stream)
+        N.check(rc, "wrf_calc_p_rho_adj")
+        allb = {**out_b, **bars}
+        return (None,) + tuple(allb[k] for k in PRHO_INPUTS) + (None,)
+
+
+def calc_p_rho(inputs: dict, rdnw, smdiv, step, rdx=1.0 / 9000.0, rdy=1.0 / 9000.0):
+    """Differentiable calc_p_rho on the GPU: ``inputs`` maps PRHO_INPUTS to
+    tensors; returns (al', p', pm1')."""
+    return CalcPRho.apply((smdiv, step, rdx, rdy), *[inputs[k] for k in PRHO_INPUTS], rdnw)
 
 
 BDY_NAMES = ("xs", "xe", "ys", "ye", "txs", "txe", "tys", "tye")

@@ -52,6 +52,18 @@
 //                        the levels.  The cotangents of u and v pass through
 //                        (du'/du = 1).
 //
+//   k_calc_p_rho / k_calc_p_rho_adj*  calc_p_rho (wrf_dynamics.py:3269-3313)
+//                        on the mass points: al = -(alt mu + rdnw dph) / mut,
+//                        p1 = c2a (alt (t_2 - mu t_1) / (mut (t0 + t_1)) - al),
+//                        then p = p1, pm1 = p (the whole array) at step 0, or
+//                        p = p1 + smdiv (p1 - pm1), pm1 = p1 after it.  The
+//                        adjoint runs in three passes - the 3-D cotangents
+//                        (ph gathered from the two cells either side of a
+//                        level), the 2-D ones (mu, mut summed over the column)
+//                        and last the in-place rewrite of the cotangents of
+//                        al, p, pm1 from those of the outputs to those of the
+//                        inputs - so no pass reads what another writes.
+//
 //   k_relax_field / k_relax_field_adj  relax_bdytend (wrf_boundary.py:52-147)
 //                        on one field, and its adjoint with respect to the
 //                        field: at a relaxation point P of distance b,
@@ -423,6 +435,134 @@ int launch_advance_uv_adj(const Grid& g, const S& s, const S& b, float dts, cuda
   k_advance_uv_adj<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, dts);
   k_advance_uv_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, dts);
   return 2;
+}
+
+// ------------------------------------------------------------ calc_p_rho
+// state-table operands: al AL, p P, ph PH, alt ALT, t_2 T, t_1 T_SAVE,
+// c2a C2A, pm1 PM1, mu MU, mut MUTS, rdnw RDNW (the acoustic substep's
+// arguments, solver.py calc_p_rho calls)
+
+namespace {
+
+__device__ __forceinline__ bool prho_in(const Grid& g, int k, int j, int i) {
+  return k < g.nz - 1 && j >= g.jds && j < g.jde - 1 && i >= g.ids && i < g.ide - 1;
+}
+
+// forward values at a mass point and the cotangents that reach p1 and al
+struct PrhoTerm {
+  float al, N, Dn, X, p1, p1b, Ab;
+};
+
+__device__ PrhoTerm prho_term(const Grid& g, const S& s, const S& b, int step, int k, int j, int i) {
+  const size_t lev = (size_t)g.ny * g.nx;
+  const size_t c = (size_t)j * g.nx + i, p = k * lev + c;
+  const float mut = s[WF_MUTS][c], mu = s[WF_MU][c];
+  const float alt = s[WF_ALT][p], t1 = s[WF_T_SAVE][p], t2 = s[WF_T][p], c2 = s[WF_C2A][p];
+  PrhoTerm t;
+  t.al = -1.0f / mut * (alt * mu + s[WF_RDNW][k] * (s[WF_PH][p + lev] - s[WF_PH][p]));
+  t.N = t2 - mu * t1;
+  t.Dn = mut * ((float)T0 + t1);
+  t.X = alt * t.N / t.Dn;
+  t.p1 = c2 * (t.X - t.al);
+  const float Pb = b[WF_P][p], Mb = b[WF_PM1][p];
+  t.p1b = step == 0 ? Pb + Mb : (1.0f + g.smdiv) * Pb + Mb;
+  t.Ab = b[WF_AL][p] - c2 * t.p1b;
+  return t;
+}
+
+}  // namespace
+
+__global__ void k_calc_p_rho(Grid g, S s, int step) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const size_t lev = (size_t)g.ny * g.nx;
+  const int c = g.i2(j, i);
+  const size_t p = k * lev + c;
+  float* pp = s[WF_P];
+  if (prho_in(g, k, j, i)) {
+    const float muts = s[WF_MUTS][c], mu = s[WF_MU][c];
+    const float alt = s[WF_ALT][p], t1 = s[WF_T_SAVE][p];
+    const float al = -1.0f / muts * (alt * mu + s[WF_RDNW][k] * (s[WF_PH][p + lev] - s[WF_PH][p]));
+    const float p1 = s[WF_C2A][p] * (alt * (s[WF_T][p] - mu * t1) / (muts * ((float)T0 + t1)) - al);
+    s[WF_AL][p] = al;
+    if (step == 0) {
+      pp[p] = p1;
+      s[WF_PM1][p] = p1;
+    } else {
+      pp[p] = p1 + g.smdiv * (p1 - s[WF_PM1][p]);
+      s[WF_PM1][p] = p1;
+    }
+  } else if (step == 0) {
+    s[WF_PM1][p] = pp[p];  // pm1 is a copy of the whole p
+  }
+}
+
+__global__ void k_calc_p_rho_adj(Grid g, S s, S b, int step) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const size_t lev = (size_t)g.ny * g.nx;
+  const int c = g.i2(j, i);
+  const size_t p = k * lev + c;
+  const float mut = s[WF_MUTS][c], mu = s[WF_MU][c];
+  if (prho_in(g, k, j, i)) {
+    const PrhoTerm t = prho_term(g, s, b, step, k, j, i);
+    const float alt = s[WF_ALT][p], t1 = s[WF_T_SAVE][p];
+    const float Xb = s[WF_C2A][p] * t.p1b;
+    b[WF_C2A][p] += t.p1b * (t.X - t.al);
+    b[WF_ALT][p] += Xb * t.N / t.Dn + t.Ab * (-mu / mut);
+    b[WF_T][p] += Xb * alt / t.Dn;
+    b[WF_T_SAVE][p] += Xb * alt * (-mu) / t.Dn - Xb * t.X / ((float)T0 + t1);
+  }
+  // ph(k): +rdnw(k) / mut from cell k, -rdnw(k-1) / mut from cell k-1
+  float aph = 0.f;
+  if (prho_in(g, k, j, i)) aph += prho_term(g, s, b, step, k, j, i).Ab * (s[WF_RDNW][k] / mut);
+  if (k >= 1 && prho_in(g, k - 1, j, i)) aph -= prho_term(g, s, b, step, k - 1, j, i).Ab * (s[WF_RDNW][k - 1] / mut);
+  if (aph != 0.f) b[WF_PH][p] += aph;
+}
+
+__global__ void k_calc_p_rho_adj_col(Grid g, S s, S b, int step) {
+  WRF_COLUMN_INDEX(g, j, i);
+  if (!prho_in(g, 0, j, i)) return;
+  const size_t lev = (size_t)g.ny * g.nx;
+  const int c = g.i2(j, i);
+  const float mut = s[WF_MUTS][c];
+  float amu = 0.f, amut = 0.f;
+  for (int k = 0; k < g.nz - 1; ++k) {
+    const size_t p = k * lev + c;
+    const PrhoTerm t = prho_term(g, s, b, step, k, j, i);
+    const float alt = s[WF_ALT][p], t1 = s[WF_T_SAVE][p];
+    const float Xb = s[WF_C2A][p] * t.p1b;
+    amu += Xb * alt * (-t1) / t.Dn + t.Ab * (-alt / mut);
+    amut += -Xb * t.X / mut + t.Ab * (-t.al / mut);
+  }
+  b[WF_MU][c] += amu;
+  b[WF_MUTS][c] += amut;
+}
+
+__global__ void k_calc_p_rho_adj_out(Grid g, S b, int step) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const size_t p = (size_t)k * g.ny * g.nx + g.i2(j, i);
+  if (prho_in(g, k, j, i)) {
+    const float Pb = b[WF_P][p];
+    b[WF_AL][p] = 0.f;
+    b[WF_P][p] = 0.f;
+    b[WF_PM1][p] = step == 0 ? 0.f : -g.smdiv * Pb;
+  } else if (step == 0) {
+    b[WF_P][p] = b[WF_P][p] + b[WF_PM1][p];
+    b[WF_PM1][p] = 0.f;
+  }
+}
+
+int launch_calc_p_rho(const Grid& g, const S& s, int step, cudaStream_t st) {
+  const dim3 b3(32, 4);
+  k_calc_p_rho<<<point_grid(g, b3), b3, 0, st>>>(g, s, step);
+  return 1;
+}
+
+int launch_calc_p_rho_adj(const Grid& g, const S& s, const S& b, int step, cudaStream_t st) {
+  const dim3 b3(32, 4), b2(32, 8);
+  k_calc_p_rho_adj<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, step);
+  k_calc_p_rho_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, step);
+  k_calc_p_rho_adj_out<<<point_grid(g, b3), b3, 0, st>>>(g, b, step);
+  return 3;
 }
 
 // stagger of a relaxed field: the bounds of relax_bdytend's zones and levels

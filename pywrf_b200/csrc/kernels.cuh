@@ -53,6 +53,8 @@ int launch_advect_scalar(const Grid& g, const S& s, const float* field, float* t
 // adjoint of advect_scalar w.r.t. the field and ru / rv / rom (k_adjoint.cu);
 // accumulates into qbar, rubar, rvbar, rombar
 int launch_advance_uv_adj(const Grid& g, const S& s, const S& b, float dts, cudaStream_t st);
+int launch_calc_p_rho(const Grid& g, const S& s, int step, cudaStream_t st);
+int launch_calc_p_rho_adj(const Grid& g, const S& s, const S& b, int step, cudaStream_t st);
 int launch_advect_mom_adj(const Grid& g, int component, const float* q, const float* ru, const float* rv,
                           const float* rom, const float* msf, const float* msf2, const float* fzm, const float* fzp,
                           const float* rdz, const float* tbar, float* qbar, float* rubar, float* rvbar,

@@ -541,6 +541,36 @@ int state_of(const WrfState* in, const int* ids, int n, S& s) {
 }
 }  // namespace
 
+namespace {
+constexpr int kPrhoOperands[] = {WF_AL, WF_P, WF_PH, WF_ALT, WF_T, WF_T_SAVE, WF_C2A, WF_PM1, WF_MU, WF_MUTS, WF_RDNW};
+constexpr int kPrhoCotangents[] = {WF_AL, WF_P, WF_PH, WF_ALT, WF_T, WF_T_SAVE, WF_C2A, WF_PM1, WF_MU, WF_MUTS};
+}  // namespace
+
+int wrf_calc_p_rho(const WrfGrid* gin, const WrfState* sin, int step, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (step < 0) return fail(WRF_EINVAL, "calc_p_rho: step >= 0");
+  S s;
+  if ((rc = state_of(sin, kPrhoOperands, sizeof(kPrhoOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_calc_p_rho(g, s, step, static_cast<cudaStream_t>(stream));
+  return check_launch("calc_p_rho");
+}
+
+int wrf_calc_p_rho_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, int step, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (step < 0) return fail(WRF_EINVAL, "calc_p_rho_adj: step >= 0");
+  S s, b;
+  if ((rc = state_of(sin, kPrhoOperands, sizeof(kPrhoOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kPrhoCotangents, sizeof(kPrhoCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_calc_p_rho_adj(g, s, b, step, static_cast<cudaStream_t>(stream));
+  return check_launch("calc_p_rho_adj");
+}
+
 int wrf_advance_uv(const WrfGrid* gin, const WrfState* sin, float dts, void* stream) {
   Grid g;
   int rc = make_grid(gin, g);

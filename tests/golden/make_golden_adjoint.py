@@ -28,6 +28,9 @@ the returned tendency with torch autograd, and writes next to this script:
   it), so the fixture holds central differences of the float64 forward of
   L = sum(u' cot_u + v' cot_v) along 3 seeded directions (``uv_direction``)
   in each of the 16 differentiable inputs;
+* ``prho_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_p_rho``
+  (wrf_dynamics.py:3269-3313) at step 0 and step 1 with autograd w.r.t.
+  al, p, ph, alt, t_2, t_1, c2a, pm1, mu and mut;
 * ``coefw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_coef_w``
   (wrf_dynamics.py:3316-3388): the reference's autograd cannot differentiate
   it (the recurrence updates ``gamma`` in place between its reads, and
@@ -148,6 +151,49 @@ def advance_uv(dyn, bnd, g) -> None:
     print("wrote advuv_adj_ref64.npz")
 
 
+PRHO_IN = ("al", "p", "ph", "alt", "t_2", "t_1", "c2a", "pm1", "mu", "mut")
+
+
+def calc_p_rho(dyn, g) -> None:
+    """calc_p_rho at step 0 and 1 with autograd (prho_adj_ref64.npz)."""
+    import torch
+
+    rng = np.random.default_rng(16)
+    sh, s2 = (NZ, N, N), (N, N)
+    kk = np.arange(NZ, dtype=np.float64)[:, None, None]
+    d = {
+        "al": 0.01 * rng.standard_normal(sh), "p": 100.0 * rng.standard_normal(sh),
+        "ph": 2.0e3 * kk + 50.0 * rng.standard_normal(sh), "alt": 1.0 + 0.05 * rng.standard_normal(sh),
+        "t_2": 100.0 * rng.standard_normal(sh), "t_1": 5.0 * rng.standard_normal(sh),
+        "c2a": 1.6e5 + 1.0e4 * rng.standard_normal(sh), "pm1": 100.0 * rng.standard_normal(sh),
+        "mu": 100.0 * rng.standard_normal(s2), "mut": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "rdnw": -(10.0 + rng.random(NZ)),
+        "cot_al": rng.standard_normal(sh), "cot_p": rng.standard_normal(sh), "cot_pm1": rng.standard_normal(sh),
+    }
+    d = {k: v.astype(np.float32) for k, v in d.items()}
+    save = dict(d)
+    save["smdiv"] = np.array(0.1)
+    save["dx"], save["dy"] = np.array(g.dx), np.array(g.dy)
+    one1 = torch.ones(NZ, dtype=torch.float64)
+    ids, ide, jds, jde = 5, N - 5, 5, N - 5
+    for step in (0, 1):
+        t = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
+        for k in PRHO_IN:
+            t[k].requires_grad_(True)
+        al, p, pm1 = dyn.calc_p_rho(t["al"].clone(), t["p"].clone(), t["ph"], t["alt"], t["t_2"], t["t_1"], t["c2a"],
+                                    t["pm1"].clone(), t["mu"], t["mut"], one1, one1 * 0, one1, one1 * 0, one1,
+                                    one1 * 0, one1, one1 * 0, one1, 300.0, t["rdnw"], one1, 0.1, True, step,
+                                    ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+        ((al * t["cot_al"]).sum() + (p * t["cot_p"]).sum() + (pm1 * t["cot_pm1"]).sum()).backward()
+        for nm, v in (("al", al), ("p", p), ("pm1", pm1)):
+            save[f"s{step}_{nm}_new"] = v.detach().numpy()
+        for k in PRHO_IN:
+            gk = t[k].grad
+            save[f"s{step}_grad_{k}"] = np.zeros(d[k].shape) if gk is None else gk.numpy()
+    np.savez_compressed(os.path.join(HERE, "prho_adj_ref64.npz"), **save)
+    print("wrote prho_adj_ref64.npz")
+
+
 def mom_direction(n: int, r: int, shape) -> np.ndarray:
     """Direction r of input n (field, ru, rv, rom) of the advect_w finite
     differences (regenerated by the tests, not stored)."""
@@ -235,7 +281,7 @@ def momentum(dyn, g) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default=None)
-    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv"), default=None,
+    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv", "calc_p_rho"), default=None,
                     help="write one fixture only")
     a = ap.parse_args()
     if a.reference:
@@ -252,8 +298,11 @@ def main() -> None:
     if a.only == "advance_uv":
         advance_uv(dyn, importlib_bdy(), g)
         return
+    if a.only == "calc_p_rho":
+        calc_p_rho(dyn, g)
+        return
     if a.only is not None:
-        raise SystemExit("--only: momentum and advance_uv are the fixtures that can be written on their own")
+        raise SystemExit("--only: momentum, advance_uv and calc_p_rho are the fixtures that can be written alone")
     d = inputs()
     t = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
     for k in ("field", "ru", "rv", "rom"):
@@ -344,6 +393,7 @@ def main() -> None:
     print("wrote coefw_adj_ref64.npz")
     momentum(dyn, g)
     advance_uv(dyn, importlib_bdy(), g)
+    calc_p_rho(dyn, g)
 
 
 def importlib_bdy():

@@ -272,3 +272,26 @@ def test_advance_uv_and_its_adjoint_against_the_reference(form):
             an = float((gr * _uv_dir(n, r, gr.shape)).sum())
             fd = float(V[f"fd_{name}_{r}"])
             assert abs(an - fd) <= 1e-4 * abs(fd), (name, r, an, fd)
+
+
+@pytest.mark.parametrize("step", [0, 1])
+def test_calc_p_rho_and_its_adjoint_match_reference_autograd(step):
+    """calc_p_rho at acoustic step 0 (pm1 = p) and 1 (divergence damping):
+    al, p, pm1 against the reference's, and the hand-written adjoint against
+    its autograd gradients (tests/golden/prho_adj_ref64.npz)."""
+    P = load_npz("prho_adj_ref64.npz")
+    inputs = {k: _cuda(P[k]).requires_grad_(True) for k in adjoint.PRHO_INPUTS}
+    al, p, pm1 = adjoint.calc_p_rho(inputs, _cuda(P["rdnw"]), float(P["smdiv"]), step,
+                                    1.0 / float(P["dx"]), 1.0 / float(P["dy"]))
+    for nm, mine in (("al", al), ("p", p), ("pm1", pm1)):
+        assert rel_l2(mine.detach().cpu().numpy(), P[f"s{step}_{nm}_new"]) < 1e-6, nm
+    L = (al * _cuda(P["cot_al"])).sum() + (p * _cuda(P["cot_p"])).sum() + (pm1 * _cuda(P["cot_pm1"])).sum()
+    L.backward()
+    for k in adjoint.PRHO_INPUTS:
+        ref = P[f"s{step}_grad_{k}"]
+        mine = inputs[k].grad.cpu().numpy()
+        if not np.any(ref):
+            assert not np.any(mine), k
+            continue
+        err = rel_l2(mine, ref)
+        assert err < 1e-5, (step, k, err)

@@ -207,3 +207,44 @@ def test_advance_uv_fixture_pinned_by_the_oracle():
         fd = float(((up - um) * cu).sum() + ((vp - vm) * cv).sum()) / (2 * eps)
         ref = float(V[f"fd_{name}_0"])
         assert abs(fd - ref) <= 1e-6 * abs(ref) + 1e-9, (name, fd, ref)
+
+
+P = load_npz("prho_adj_ref64.npz")
+PRHO_IN = ("al", "p", "ph", "alt", "t_2", "t_1", "c2a", "pm1", "mu", "mut")
+
+
+def _prho(g, x, step):
+    x = {k: np.array(v, np.float64) for k, v in x.items()}
+    pm1 = OD.calc_p_rho(g, x["al"], x["p"], x["ph"], x["alt"], x["t_2"], x["t_1"], x["c2a"], x["pm1"], x["mu"],
+                        x["mut"], P["rdnw"].astype(np.float64), float(P["smdiv"]), step)
+    return x["al"], x["p"], pm1
+
+
+def test_calc_p_rho_fixture_pinned_by_the_oracle():
+    """calc_p_rho at step 0 and 1: the oracle reproduces the reference's al,
+    p, pm1 on the fixture, and its central differences give the golden
+    autograd gradients' directional derivatives."""
+    g = _grid()
+    rng = np.random.default_rng(5)
+    base = {k: P[k].astype(np.float64) for k in PRHO_IN}
+    cot = {k: P[f"cot_{k}"].astype(np.float64) for k in ("al", "p", "pm1")}
+    for step in (0, 1):
+        outs = _prho(g, base, step)
+        for nm, mine in zip(("al", "p", "pm1"), outs):
+            ref = P[f"s{step}_{nm}_new"]
+            assert np.abs(mine - ref).max() <= 1e-12 * np.abs(ref).max(), (step, nm)
+
+        def loss(x):
+            return sum(float((o * cot[nm]).sum()) for nm, o in zip(("al", "p", "pm1"), _prho(g, x, step)))
+
+        for name in PRHO_IN:
+            d = rng.standard_normal(base[name].shape)
+            # a larger step than for the bilinear operators: the loss is
+            # ~1e7, and the operator is smooth (rational in t_1 and mut)
+            eps = 1e-4 * float(np.abs(base[name]).max())
+            xp, xm = dict(base), dict(base)
+            xp[name] = base[name] + eps * d
+            xm[name] = base[name] - eps * d
+            fd = (loss(xp) - loss(xm)) / (2 * eps)
+            an = float((d * P[f"s{step}_grad_{name}"].astype(np.float64)).sum())
+            assert abs(fd - an) <= 1e-5 * abs(an) + 1e-9, (step, name, fd, an)
