@@ -205,6 +205,23 @@ int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream)
  * of a saved operand), so the product is checked against finite differences
  * of its forward. */
 int wrf_advance_uv_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float dts, void* stream);
+/* wrf_dynamics.py:3528-3638 advance_mu_t on the state table, in place, with
+ * the solver's arguments (solver.py:1380-1393): ww (WW), ww_1 (WW1), u,
+ * u_1 (U_SAVE), v, v_1 (V_SAVE), mu, mut, muave, muts, muu, muv, mudf, t,
+ * t_1 (T_SAVE), t_ave (T_2SAVE), ft (T_TEND), mu_tend and the profiles dnw,
+ * fnm, fnp, rdnw and map factors msfuy, msfvx_inv, msftx, msfty, with the
+ * grid's epssm; updates ww, t, t_2save, mu, muts, mudf and muave. */
+int wrf_advance_mu_t(const WrfGrid* g, const WrfState* s, float dts, void* stream);
+/* Its adjoint: sbar holds, under the same ids, the cotangents of the seven
+ * updated fields (rewritten to those of the inputs of the same name) and
+ * accumulates (+=) those of ww_1, u, u_1, v, v_1, mut, muu, muv, t_1, ft,
+ * mu_tend.  work: caller-owned scratch of nz*ny*nx floats.  ref_no_grad != 0
+ * reproduces the reference's autograd, which runs the mu / muts / mudf /
+ * muave update under torch.no_grad() (wrf_dynamics.py:3597-3604): those
+ * four outputs then pass their cotangents to the inputs of the same name and
+ * nothing else; ref_no_grad = 0 gives the derivative of the operator. */
+int wrf_advance_mu_t_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float dts,
+                         int ref_no_grad, float* work, void* stream);
 /* wrf_dynamics.py:3269-3313 calc_p_rho on the state table, in place: al, p
  * and pm1 from ph, alt, t_2 (field T), t_1 (T_SAVE), c2a, mu, mut (MUTS)
  * and rdnw, with the grid's smdiv; step 0 sets pm1 to a copy of the whole

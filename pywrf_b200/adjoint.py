@@ -19,6 +19,11 @@ operators keeps no tape of the forward's intermediates.
 * :class:`CalcPRho` -- calc_p_rho (pywrf/wrf_dynamics.py:3269-3313): al, p,
   pm1 from ph, alt, t_2, t_1, c2a, pm1, mu, mut at a given acoustic step;
   gradients with respect to all ten.
+* :class:`AdvanceMuT` -- advance_mu_t (pywrf/wrf_dynamics.py:3528-3638): the
+  column mass, eta-velocity and theta update of the acoustic substep;
+  gradients with respect to its 18 array inputs, either of the operator
+  (default) or as the reference's autograd gives them (``ref_no_grad``: its
+  mu / muts / mudf / muave update runs under ``torch.no_grad()``).
 * :class:`RelaxBdytend` -- ``tendency + relax(field)`` toward the lateral
   boundary values (pywrf/wrf_boundary.py:52-147); gradients with respect to
   the field and the incoming tendency (the boundary arrays are data).
@@ -191,6 +196,63 @@ def advance_uv(inputs: dict, data: dict, dts, emdiv, cf1, cf2, cf3, rdx, rdy):
     ``inputs`` maps UV_INPUTS, ``data`` UV_DATA to tensors; returns (u', v')."""
     return AdvanceUV.apply((dts, emdiv, cf1, cf2, cf3, rdx, rdy), *[inputs[k] for k in UV_INPUTS],
                            *[data[k] for k in UV_DATA])
+
+
+MUT_INPUTS = ("ww", "ww_1", "u", "u_1", "v", "v_1", "t", "t_1", "t_ave", "ft", "mu", "mut", "muave", "muts", "muu",
+              "muv", "mudf", "mu_tend")
+MUT_DATA = ("dnw", "fnm", "fnp", "rdnw", "msfuy", "msfvx_inv", "msftx", "msfty")
+MUT_OUTPUTS = ("ww", "t", "t_ave", "muave", "muts", "mudf", "mu")
+# the state-table names of advance_mu_t's arguments in the acoustic substep
+_MUT_FIELD = {"ww_1": "ww1", "u_1": "u_save", "v_1": "v_save", "t_1": "t_save", "t_ave": "t_2save", "ft": "t_tend"}
+
+
+class AdvanceMuT(torch.autograd.Function):
+    """The seven outputs MUT_OUTPUTS of advance_mu_t; the tensors follow
+    MUT_INPUTS then MUT_DATA, ``scal`` = (dts, epssm, rdx, rdy, ref_no_grad)."""
+
+    @staticmethod
+    def forward(ctx, scal, *tensors):
+        dts, epssm, rdx, rdy = (float(x) for x in scal[:4])
+        named = dict(zip(MUT_INPUTS + MUT_DATA, tensors))
+        cg = scalar_grid(named["ww"].shape, rdx, rdy)
+        cg.epssm = epssm
+        outs = {k: named[k].detach().clone() for k in MUT_OUTPUTS}
+        tab = _table({_MUT_FIELD.get(k, k): v for k, v in {**named, **outs}.items()})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(outs["ww"].device):
+            rc = N.lib().wrf_advance_mu_t(ctypes.byref(cg), tab, dts, stream)
+        N.check(rc, "wrf_advance_mu_t")
+        ctx.save_for_backward(*tensors)
+        ctx.cg, ctx.dts, ctx.ref_no_grad = cg, dts, int(bool(scal[4]))
+        return tuple(outs[k] for k in MUT_OUTPUTS)
+
+    @staticmethod
+    def backward(ctx, *gouts):
+        tensors = ctx.saved_tensors
+        named = dict(zip(MUT_INPUTS + MUT_DATA, tensors))
+        bars = {}
+        for k, gk in zip(MUT_OUTPUTS, gouts):
+            bars[k] = torch.zeros_like(named[k]) if gk is None else gk.contiguous().clone()
+        for k in MUT_INPUTS:
+            if k not in bars:
+                bars[k] = torch.zeros_like(named[k])
+        work = torch.empty_like(named["ww"])
+        tab = _table({_MUT_FIELD.get(k, k): v for k, v in named.items()})
+        btab = _table({_MUT_FIELD.get(k, k): v for k, v in bars.items()})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(work.device):
+            rc = N.lib().wrf_advance_mu_t_adj(ctypes.byref(ctx.cg), tab, btab, ctx.dts, ctx.ref_no_grad, _ptr(work),
+                                              stream)
+        N.check(rc, "wrf_advance_mu_t_adj")
+        return (None,) + tuple(bars[k] for k in MUT_INPUTS) + (None,) * len(MUT_DATA)
+
+
+def advance_mu_t(inputs: dict, data: dict, dts, epssm, rdx=1.0 / 9000.0, rdy=1.0 / 9000.0, ref_no_grad=False):
+    """Differentiable advance_mu_t on the GPU: ``inputs`` maps MUT_INPUTS,
+    ``data`` MUT_DATA to tensors; returns a dict of MUT_OUTPUTS."""
+    outs = AdvanceMuT.apply((dts, epssm, rdx, rdy, ref_no_grad), *[inputs[k] for k in MUT_INPUTS],
+                            *[data[k] for k in MUT_DATA])
+    return dict(zip(MUT_OUTPUTS, outs))
 
 
 PRHO_INPUTS = ("al", "p", "ph", "alt", "t_2", "t_1", "c2a", "pm1", "mu", "mut")

@@ -64,6 +64,28 @@
 //                        al, p, pm1 from those of the outputs to those of the
 //                        inputs - so no pass reads what another writes.
 //
+//   k_advance_mu_t / k_advance_mu_t_adj_*  advance_mu_t (wrf_dynamics.py:
+//                        3528-3638) on the columns [ids+1, ide-2) x [jds+1,
+//                        jde-2): the horizontal divergence dvdxi(k), its
+//                        column sum dmdt, the mu / mudf / muts / muave update,
+//                        the ww scan W(k) = W(k-1) - dnw(k-1) (dmdt + dvdxi(k-1)
+//                        + mu_tend) / msfty (ww' = W - ww_1) and the theta
+//                        update with the fluxes wdtn = ww' (fnm t_1 + fnp t_1).
+//                        The adjoint: (1) per column, the cotangent of
+//                        dvdxi at every level into the caller's work array
+//                        (reverse ww scan as a suffix sum); (2) per point, the
+//                        gathers of u, v, u_1, v_1 and the horizontal part of
+//                        t_1 from the columns whose stencils hold the point;
+//                        (3) per column, muu, muv from the work array, the
+//                        column-local cotangents and the in-place rewrite of
+//                        those of the outputs (ww, t, t_ave, mu, muts, mudf,
+//                        muave) to those of the inputs.  With ref_no_grad the
+//                        mu / muts / mudf / muave update is treated as the
+//                        reference's autograd sees it (computed under
+//                        torch.no_grad(): each passes its cotangent to the
+//                        input of the same name and nothing to dmdt, mut or
+//                        mu_tend).
+//
 //   k_relax_field / k_relax_field_adj  relax_bdytend (wrf_boundary.py:52-147)
 //                        on one field, and its adjoint with respect to the
 //                        field: at a relaxation point P of distance b,
@@ -562,6 +584,257 @@ int launch_calc_p_rho_adj(const Grid& g, const S& s, const S& b, int step, cudaS
   k_calc_p_rho_adj<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, step);
   k_calc_p_rho_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, step);
   k_calc_p_rho_adj_out<<<point_grid(g, b3), b3, 0, st>>>(g, b, step);
+  return 3;
+}
+
+// ------------------------------------------------------------ advance_mu_t
+// state-table operands: ww WW, ww_1 WW1, u U, u_1 U_SAVE, v V, v_1 V_SAVE,
+// mu MU, mut MUT, muave MUAVE, muts MUTS, muu MUU, muv MUV, mudf MUDF, t T,
+// t_1 T_SAVE, t_ave T_2SAVE, ft T_TEND, mu_tend MU_TEND (solver.py:1380-1393)
+
+namespace {
+
+__device__ __forceinline__ bool mut_in(const Grid& g, int j, int i) {
+  return j >= g.jds + 1 && j < g.jde - 2 && i >= g.ids + 1 && i < g.ide - 2;
+}
+
+__device__ __forceinline__ float mut_dvdxi(const Grid& g, const S& s, int k, int j, int i) {
+  const int nx = g.nx;
+  const size_t c = (size_t)j * nx + i, p = (size_t)k * g.ny * nx + c;
+  const float vn = s[WF_V][p + nx] + s[WF_MUV][c + nx] * s[WF_V_SAVE][p + nx] * s[WF_MSFVX_INV][c + nx];
+  const float vs = s[WF_V][p] + s[WF_MUV][c] * s[WF_V_SAVE][p] * s[WF_MSFVX_INV][c];
+  const float ue = s[WF_U][p + 1] + s[WF_MUU][c + 1] * s[WF_U_SAVE][p + 1] / s[WF_MSFUY][c + 1];
+  const float uw = s[WF_U][p] + s[WF_MUU][c] * s[WF_U_SAVE][p] / s[WF_MSFUY][c];
+  return s[WF_MSFTX][c] * s[WF_MSFTY][c] * (g.rdy * (vn - vs) + g.rdx * (ue - uw));
+}
+
+// a column's forward values: dvdxi, dmdt and the new ww (ww' = W - ww_1)
+struct MutCol {
+  float dv[kMaxNz], wwp[kMaxNz];
+  float dmdt;
+};
+
+__device__ void mut_column(const Grid& g, const S& s, int j, int i, MutCol& m) {
+  const int ktf = g.nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
+  const float* dnw = s[WF_DNW];
+  m.dmdt = 0.f;
+  for (int k = 0; k < ktf; ++k) {
+    m.dv[k] = mut_dvdxi(g, s, k, j, i);
+    m.dmdt = m.dmdt + dnw[k] * m.dv[k];
+  }
+  const float mt = s[WF_MU_TEND][c], msfty = s[WF_MSFTY][c];
+  float W = s[WF_WW][c];
+  m.wwp[0] = W - s[WF_WW1][c];
+  for (int k = 1; k < ktf; ++k) {
+    W = W - dnw[k - 1] * (m.dmdt + m.dv[k - 1] + mt) / msfty;
+    m.wwp[k] = W - s[WF_WW1][k * lev + c];
+  }
+}
+
+// the cotangents of wdtn(kk), kk in [1, ktf), and of ww'(k), k in [0, ktf)
+__device__ void mut_ww_bar(const Grid& g, const S& s, const S& b, float dts, int j, int i, const MutCol& m,
+                           float* wdb, float* wwb) {
+  const int ktf = g.nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
+  const float dm = dts * s[WF_MSFTY][c];
+  const float* rdnw = s[WF_RDNW];
+  const float* t1 = s[WF_T_SAVE];
+  for (int k = 0; k < ktf; ++k) {
+    wdb[k] = 0.f;
+    if (k >= 1) wdb[k] = -dm * rdnw[k - 1] * b[WF_T][(k - 1) * lev + c] + dm * rdnw[k] * b[WF_T][k * lev + c];
+    const float tavg = k >= 1 ? s[WF_FNM][k] * t1[k * lev + c] + s[WF_FNP][k] * t1[(k - 1) * lev + c] : 0.f;
+    wwb[k] = b[WF_WW][k * lev + c] + (k >= 1 ? wdb[k] * tavg : 0.f);
+  }
+}
+
+// mu' is the new mu; the cotangent reaching it from mu', muts', muave'
+__device__ __forceinline__ float mut_mu_bar(const Grid& g, const S& b, size_t c) {
+  const float ep1 = (float)(1.0 + (double)g.epssm);
+  return b[WF_MU][c] + b[WF_MUTS][c] + 0.5f * ep1 * b[WF_MUAVE][c];
+}
+
+}  // namespace
+
+__global__ void k_advance_mu_t(Grid g, S s, float dts) {
+  WRF_COLUMN_INDEX(g, j, i);
+  if (!mut_in(g, j, i)) return;
+  const int ktf = g.nz - 1, nx = g.nx;
+  const size_t lev = (size_t)g.ny * nx, c = (size_t)j * nx + i;
+  MutCol m;
+  mut_column(g, s, j, i, m);
+  const float ep1 = (float)(1.0 + (double)g.epssm), em1 = (float)(1.0 - (double)g.epssm);
+  const float mu0 = s[WF_MU][c], mt = s[WF_MU_TEND][c];
+  const float mu1 = mu0 + dts * (m.dmdt + mt);
+  s[WF_MU][c] = mu1;
+  s[WF_MUDF][c] = m.dmdt + mt;
+  s[WF_MUTS][c] = s[WF_MUT][c] + mu1;
+  s[WF_MUAVE][c] = 0.5f * (ep1 * mu1 + em1 * mu0);
+  for (int k = 0; k < ktf; ++k) s[WF_WW][k * lev + c] = m.wwp[k];
+  const float msfty = s[WF_MSFTY][c], msftx = s[WF_MSFTX][c], rdx = g.rdx, rdy = g.rdy;
+  const float* t1 = s[WF_T_SAVE];
+  const float* u = s[WF_U];
+  const float* v = s[WF_V];
+  auto wdtn = [&](int k) {
+    if (k < 1 || k >= ktf) return 0.f;
+    return m.wwp[k] * (s[WF_FNM][k] * t1[k * lev + c] + s[WF_FNP][k] * t1[(k - 1) * lev + c]);
+  };
+  for (int k = 0; k < ktf; ++k) {
+    const size_t p = k * lev + c;
+    const float tk = s[WF_T][p];
+    s[WF_T_2SAVE][p] = tk;
+    const float t1v = tk + msfty * dts * s[WF_T_TEND][p];
+    const float h = 0.5f * rdy * (v[p + nx] * (t1[p + nx] + t1[p]) - v[p] * (t1[p] + t1[p - nx])) +
+                    0.5f * rdx * (u[p + 1] * (t1[p + 1] + t1[p]) - u[p] * (t1[p] + t1[p - 1]));
+    s[WF_T][p] = t1v - dts * msfty * (msftx * h + s[WF_RDNW][k] * (wdtn(k + 1) - wdtn(k)));
+  }
+}
+
+__global__ void k_advance_mu_t_adj_dv(Grid g, S s, S b, float dts, int ref_no_grad, float* work) {
+  WRF_COLUMN_INDEX(g, j, i);
+  if (!mut_in(g, j, i)) return;
+  const int ktf = g.nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
+  MutCol m;
+  mut_column(g, s, j, i, m);
+  float wdb[kMaxNz], wwb[kMaxNz], qb[kMaxNz];
+  mut_ww_bar(g, s, b, dts, j, i, m, wdb, wwb);
+  const float msfty = s[WF_MSFTY][c];
+  float S_ = 0.f, qsum = 0.f;
+  for (int k = ktf - 1; k >= 1; --k) {
+    S_ += wwb[k];
+    qb[k - 1] = -s[WF_DNW][k - 1] / msfty * S_;
+    qsum += qb[k - 1];
+  }
+  const float dmdtb = qsum + (ref_no_grad ? 0.f : dts * mut_mu_bar(g, b, c) + b[WF_MUDF][c]);
+  for (int k = 0; k < ktf; ++k) work[k * lev + c] = (k <= ktf - 2 ? qb[k] : 0.f) + s[WF_DNW][k] * dmdtb;
+}
+
+__global__ void k_advance_mu_t_adj_pt(Grid g, S s, S b, float dts, const float* work) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const int ktf = g.nz - 1, nx = g.nx;
+  if (k >= ktf) return;
+  const size_t lev = (size_t)g.ny * nx, c = (size_t)j * nx + i, p = k * lev + c;
+  const float rdx = g.rdx, rdy = g.rdy;
+  auto mm = [&](size_t cc) { return s[WF_MSFTX][cc] * s[WF_MSFTY][cc]; };
+  // divergence: u, u_1 at columns i (east face of column i-1, sign +) and
+  // (west face of column i, sign -); v, v_1 likewise in y
+  float ub = 0.f, vb = 0.f;
+  if (i >= 1 && mut_in(g, j, i - 1)) ub += mm(c - 1) * rdx * work[p - 1];
+  if (mut_in(g, j, i)) ub -= mm(c) * rdx * work[p];
+  if (j >= 1 && mut_in(g, j - 1, i)) vb += mm(c - nx) * rdy * work[p - nx];
+  if (mut_in(g, j, i)) vb -= mm(c) * rdy * work[p];
+  float u1b = ub * s[WF_MUU][c] / s[WF_MSFUY][c];
+  float v1b = vb * s[WF_MUV][c] * s[WF_MSFVX_INV][c];
+  // theta fluxes: Hb(P) = -dts msfty msftx tbar at the updated columns P
+  auto hb = [&](int jj, int ii) {
+    if (jj < 0 || ii < 0 || jj >= g.ny || ii >= nx || !mut_in(g, jj, ii)) return 0.f;
+    const size_t cc = (size_t)jj * nx + ii;
+    return -dts * s[WF_MSFTY][cc] * s[WF_MSFTX][cc] * b[WF_T][k * lev + cc];
+  };
+  const float hc = hb(j, i), hs = hb(j - 1, i), hn = hb(j + 1, i), hw = hb(j, i - 1), he = hb(j, i + 1);
+  const float* t1 = s[WF_T_SAVE];
+  const float* u = s[WF_U];
+  const float* v = s[WF_V];
+  if (hs != 0.f || hc != 0.f) vb += 0.5f * rdy * (t1[p] + t1[p - nx]) * (hs - hc);
+  if (hw != 0.f || hc != 0.f) ub += 0.5f * rdx * (t1[p] + t1[p - 1]) * (hw - hc);
+  float t1b = 0.f;
+  if (hs != 0.f) t1b += 0.5f * rdy * hs * v[p];
+  if (hc != 0.f) t1b += 0.5f * rdy * hc * (v[p + nx] - v[p]) + 0.5f * rdx * hc * (u[p + 1] - u[p]);
+  if (hn != 0.f) t1b -= 0.5f * rdy * hn * v[p + nx];
+  if (hw != 0.f) t1b += 0.5f * rdx * hw * u[p];
+  if (he != 0.f) t1b -= 0.5f * rdx * he * u[p + 1];
+  if (ub != 0.f) b[WF_U][p] += ub;
+  if (vb != 0.f) b[WF_V][p] += vb;
+  if (u1b != 0.f) b[WF_U_SAVE][p] += u1b;
+  if (v1b != 0.f) b[WF_V_SAVE][p] += v1b;
+  if (t1b != 0.f) b[WF_T_SAVE][p] += t1b;
+}
+
+__global__ void k_advance_mu_t_adj_col(Grid g, S s, S b, float dts, int ref_no_grad, const float* work) {
+  WRF_COLUMN_INDEX(g, j, i);
+  const int ktf = g.nz - 1, nx = g.nx;
+  const size_t lev = (size_t)g.ny * nx, c = (size_t)j * nx + i;
+  const float rdx = g.rdx, rdy = g.rdy;
+  // muu, muv: the u / v terms of the divergence at this column
+  {
+    float amuu = 0.f, amuv = 0.f;
+    const bool w = i >= 1 && mut_in(g, j, i - 1), o = mut_in(g, j, i), sth = j >= 1 && mut_in(g, j - 1, i);
+    if (w || o || sth) {
+      const float mw = w ? s[WF_MSFTX][c - 1] * s[WF_MSFTY][c - 1] : 0.f;
+      const float mo = o ? s[WF_MSFTX][c] * s[WF_MSFTY][c] : 0.f;
+      const float ms = sth ? s[WF_MSFTX][c - nx] * s[WF_MSFTY][c - nx] : 0.f;
+      for (int k = 0; k < ktf; ++k) {
+        const size_t p = k * lev + c;
+        float ub = 0.f, vb = 0.f;
+        if (w) ub += mw * rdx * work[p - 1];
+        if (o) ub -= mo * rdx * work[p];
+        if (sth) vb += ms * rdy * work[p - nx];
+        if (o) vb -= mo * rdy * work[p];
+        amuu += ub * s[WF_U_SAVE][p] / s[WF_MSFUY][c];
+        amuv += vb * s[WF_V_SAVE][p] * s[WF_MSFVX_INV][c];
+      }
+      if (amuu != 0.f) b[WF_MUU][c] += amuu;
+      if (amuv != 0.f) b[WF_MUV][c] += amuv;
+    }
+  }
+  if (!mut_in(g, j, i)) return;
+  MutCol m;
+  mut_column(g, s, j, i, m);
+  float wdb[kMaxNz], wwb[kMaxNz];
+  mut_ww_bar(g, s, b, dts, j, i, m, wdb, wwb);
+  const float msfty = s[WF_MSFTY][c];
+  // ww, ww_1 (the scan passes every ww' cotangent down to ww(0))
+  float wsum = 0.f, qsum = 0.f, S_ = 0.f;
+  for (int k = ktf - 1; k >= 1; --k) {
+    S_ += wwb[k];
+    qsum += -s[WF_DNW][k - 1] / msfty * S_;
+  }
+  for (int k = 0; k < ktf; ++k) {
+    wsum += wwb[k];
+    b[WF_WW1][k * lev + c] += -wwb[k];
+    if (k >= 1) b[WF_WW][k * lev + c] = 0.f;
+  }
+  b[WF_WW][c] = wsum;
+  // theta: t_ave = t, ft, the vertical fluxes' t_1
+  for (int k = 0; k < ktf; ++k) {
+    const size_t p = k * lev + c;
+    const float tb = b[WF_T][p];
+    b[WF_T_TEND][p] += msfty * dts * tb;
+    b[WF_T][p] = tb + b[WF_T_2SAVE][p];
+    b[WF_T_2SAVE][p] = 0.f;
+    if (k >= 1) {
+      b[WF_T_SAVE][p] += wdb[k] * m.wwp[k] * s[WF_FNM][k];
+      b[WF_T_SAVE][p - lev] += wdb[k] * m.wwp[k] * s[WF_FNP][k];
+    }
+  }
+  // the mu update
+  if (ref_no_grad) {
+    b[WF_MU_TEND][c] += qsum;
+  } else {
+    const float em1 = (float)(1.0 - (double)g.epssm);
+    const float mub = mut_mu_bar(g, b, c);
+    b[WF_MU_TEND][c] += qsum + dts * mub + b[WF_MUDF][c];
+    b[WF_MUT][c] += b[WF_MUTS][c];
+    b[WF_MU][c] = mub + 0.5f * em1 * b[WF_MUAVE][c];
+    b[WF_MUTS][c] = 0.f;
+    b[WF_MUDF][c] = 0.f;
+    b[WF_MUAVE][c] = 0.f;
+  }
+}
+
+int launch_advance_mu_t(const Grid& g, const S& s, float dts, cudaStream_t st) {
+  const dim3 b2(32, 4);
+  k_advance_mu_t<<<col_grid(g, b2), b2, 0, st>>>(g, s, dts);
+  return 1;
+}
+
+int launch_advance_mu_t_adj(const Grid& g, const S& s, const S& b, float dts, int ref_no_grad, float* work,
+                            cudaStream_t st) {
+  const dim3 b2(32, 4), b3(32, 4);
+  k_advance_mu_t_adj_dv<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, dts, ref_no_grad, work);
+  k_advance_mu_t_adj_pt<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, dts, work);
+  k_advance_mu_t_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, dts, ref_no_grad, work);
   return 3;
 }
 

@@ -546,6 +546,40 @@ constexpr int kPrhoOperands[] = {WF_AL, WF_P, WF_PH, WF_ALT, WF_T, WF_T_SAVE, WF
 constexpr int kPrhoCotangents[] = {WF_AL, WF_P, WF_PH, WF_ALT, WF_T, WF_T_SAVE, WF_C2A, WF_PM1, WF_MU, WF_MUTS};
 }  // namespace
 
+namespace {
+constexpr int kMutOperands[] = {WF_WW, WF_WW1, WF_U, WF_U_SAVE, WF_V, WF_V_SAVE, WF_MU, WF_MUT, WF_MUAVE, WF_MUTS,
+                                WF_MUU, WF_MUV, WF_MUDF, WF_T, WF_T_SAVE, WF_T_2SAVE, WF_T_TEND, WF_MU_TEND,
+                                WF_DNW, WF_FNM, WF_FNP, WF_RDNW, WF_MSFUY, WF_MSFVX_INV, WF_MSFTX, WF_MSFTY};
+constexpr int kMutCotangents[] = {WF_WW, WF_WW1, WF_U, WF_U_SAVE, WF_V, WF_V_SAVE, WF_MU, WF_MUT, WF_MUAVE,
+                                  WF_MUTS, WF_MUU, WF_MUV, WF_MUDF, WF_T, WF_T_SAVE, WF_T_2SAVE, WF_T_TEND,
+                                  WF_MU_TEND};
+}  // namespace
+
+int wrf_advance_mu_t(const WrfGrid* gin, const WrfState* sin, float dts, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s;
+  if ((rc = state_of(sin, kMutOperands, sizeof(kMutOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_advance_mu_t(g, s, dts, static_cast<cudaStream_t>(stream));
+  return check_launch("advance_mu_t");
+}
+
+int wrf_advance_mu_t_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dts, int ref_no_grad,
+                         float* work, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!work) return fail(WRF_EINVAL, "advance_mu_t_adj: null work array");
+  S s, b;
+  if ((rc = state_of(sin, kMutOperands, sizeof(kMutOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kMutCotangents, sizeof(kMutCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_advance_mu_t_adj(g, s, b, dts, ref_no_grad ? 1 : 0, work, static_cast<cudaStream_t>(stream));
+  return check_launch("advance_mu_t_adj");
+}
+
 int wrf_calc_p_rho(const WrfGrid* gin, const WrfState* sin, int step, void* stream) {
   Grid g;
   int rc = make_grid(gin, g);

@@ -31,6 +31,13 @@ the returned tendency with torch autograd, and writes next to this script:
 * ``prho_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_p_rho``
   (wrf_dynamics.py:3269-3313) at step 0 and step 1 with autograd w.r.t.
   al, p, ph, alt, t_2, t_1, c2a, pm1, mu and mut;
+* ``mut_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.advance_mu_t``
+  (wrf_dynamics.py:3528-3638) w.r.t. its 18 array inputs: the reference's
+  autograd gradients (``grad_*``; its mu / muts / mudf / muave updates run
+  under ``torch.no_grad()``, so those outputs pass their cotangents straight
+  to the inputs of the same name and give mut, mu_tend and the divergence
+  nothing) and, for the operator itself, central differences of the float64
+  forward along 3 seeded directions per input (``mut_direction``);
 * ``coefw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_coef_w``
   (wrf_dynamics.py:3316-3388): the reference's autograd cannot differentiate
   it (the recurrence updates ``gamma`` in place between its reads, and
@@ -194,6 +201,90 @@ def calc_p_rho(dyn, g) -> None:
     print("wrote prho_adj_ref64.npz")
 
 
+MUT3 = ("ww", "ww_1", "u", "u_1", "v", "v_1", "t", "t_1", "t_ave", "ft")
+MUT2 = ("mu", "mut", "muave", "muts", "muu", "muv", "mudf", "mu_tend")
+MUT_OUT = ("ww", "t", "t_ave", "muave", "muts", "mudf", "mu")
+
+
+def mut_direction(n: int, r: int, shape) -> np.ndarray:
+    """Direction r of input n (MUT3 + MUT2) of the advance_mu_t finite
+    differences (regenerated by the tests, not stored)."""
+    return np.random.default_rng(9000 + 100 * n + r).standard_normal(shape)
+
+
+def advance_mu_t(dyn, g) -> None:
+    """advance_mu_t: autograd and central differences (mut_adj_ref64.npz)."""
+    import torch
+
+    rng = np.random.default_rng(17)
+    sh, s2 = (NZ, N, N), (N, N)
+    d = {
+        "ww": 5.0 * rng.standard_normal(sh), "ww_1": 5.0 * rng.standard_normal(sh),
+        "u": 10.0 + 3.0 * rng.standard_normal(sh), "u_1": 10.0 + 3.0 * rng.standard_normal(sh),
+        "v": 3.0 * rng.standard_normal(sh), "v_1": 3.0 * rng.standard_normal(sh),
+        "t": 100.0 * rng.standard_normal(sh), "t_1": 2.0 + 5.0 * rng.standard_normal(sh),
+        "t_ave": 100.0 * rng.standard_normal(sh), "ft": 0.1 * rng.standard_normal(sh),
+        "mu": 100.0 * rng.standard_normal(s2), "mut": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "muave": 100.0 * rng.standard_normal(s2), "muts": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "muu": 8.0e4 + 1.0e3 * rng.standard_normal(s2), "muv": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "mudf": 10.0 * rng.standard_normal(s2), "mu_tend": 0.1 * rng.standard_normal(s2),
+        "msfuy": 1.0 + 0.02 * rng.random(s2), "msfvx_inv": 1.0 + 0.02 * rng.random(s2),
+        "msftx": 1.0 + 0.02 * rng.random(s2), "msfty": 1.0 + 0.02 * rng.random(s2),
+        "fnm": 0.45 + 0.1 * rng.random(NZ), "rdnw": -(10.0 + rng.random(NZ)),
+    }
+    d["fnp"] = 1.0 - d["fnm"]
+    d["dnw"] = 1.0 / d["rdnw"]
+    for o_ in MUT_OUT:
+        d[f"cot_{o_}"] = rng.standard_normal(sh if o_ in MUT3 else s2)
+    d = {k: v.astype(np.float32) for k, v in d.items()}
+    sc = {"dts": 11.25, "epssm": 0.1}
+    save = dict(d)
+    save.update({k: np.array(v) for k, v in sc.items()})
+    save["dx"], save["dy"] = np.array(g.dx), np.array(g.dy)
+    one1 = torch.ones(NZ, dtype=torch.float64)
+    ids, ide, jds, jde = 5, N - 5, 5, N - 5
+
+    def run(x):
+        o = dyn.advance_mu_t(x["ww"], x["ww_1"], x["u"], x["u_1"], x["v"], x["v_1"], x["mu"], x["mut"], x["muave"],
+                             x["muts"], x["muu"], x["muv"], x["mudf"], one1, one1 * 0, one1, one1 * 0, one1,
+                             one1 * 0, one1, one1 * 0, None, None, None, x["t"], x["t_1"], x["t_ave"], x["ft"],
+                             x["mu_tend"], 1.0 / g.dx, 1.0 / g.dy, sc["dts"], sc["epssm"], x["dnw"], x["fnm"],
+                             x["fnp"], x["rdnw"], x["msfuy"], x["msfuy"], x["msfvx_inv"], x["msfvx_inv"],
+                             x["msfvx_inv"], x["msftx"], x["msfty"], 1,
+                             ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+        ww, _w1, t, t_ave, _a, _b, _c, muave, muts, mudf, mu = o
+        return {"ww": ww, "t": t, "t_ave": t_ave, "muave": muave, "muts": muts, "mudf": mudf, "mu": mu}
+
+    def loss(x):
+        outs = run(x)
+        return sum((outs[o_] * x[f"cot_{o_}"]).sum() for o_ in MUT_OUT)
+
+    t = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
+    for k in MUT3 + MUT2:
+        t[k].requires_grad_(True)
+    outs = run(t)
+    for o_ in MUT_OUT:
+        save[f"{o_}_new"] = outs[o_].detach().numpy()
+    sum((outs[o_] * t[f"cot_{o_}"]).sum() for o_ in MUT_OUT).backward()
+    for k in MUT3 + MUT2:
+        gk = t[k].grad
+        save[f"grad_{k}"] = np.zeros(d[k].shape) if gk is None else gk.numpy()
+    base = {k: v.detach().clone() for k, v in t.items()}
+    with torch.no_grad():
+        for n_, name in enumerate(MUT3 + MUT2):
+            for r in range(3):
+                dirn = torch.tensor(mut_direction(n_, r, d[name].shape))
+                # at most cubic in the inputs: a step of 1e-4 keeps the
+                # truncation error near 1e-8 and the cancellation small
+                eps = 1e-4 * float(base[name].abs().max())
+                xp, xm = dict(base), dict(base)
+                xp[name] = base[name] + eps * dirn
+                xm[name] = base[name] - eps * dirn
+                save[f"fd_{name}_{r}"] = np.array(float(loss(xp) - loss(xm)) / (2 * eps))
+    np.savez_compressed(os.path.join(HERE, "mut_adj_ref64.npz"), **save)
+    print("wrote mut_adj_ref64.npz")
+
+
 def mom_direction(n: int, r: int, shape) -> np.ndarray:
     """Direction r of input n (field, ru, rv, rom) of the advect_w finite
     differences (regenerated by the tests, not stored)."""
@@ -281,7 +372,7 @@ def momentum(dyn, g) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default=None)
-    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv", "calc_p_rho"), default=None,
+    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv", "calc_p_rho", "advance_mu_t"), default=None,
                     help="write one fixture only")
     a = ap.parse_args()
     if a.reference:
@@ -301,8 +392,11 @@ def main() -> None:
     if a.only == "calc_p_rho":
         calc_p_rho(dyn, g)
         return
+    if a.only == "advance_mu_t":
+        advance_mu_t(dyn, g)
+        return
     if a.only is not None:
-        raise SystemExit("--only: momentum, advance_uv and calc_p_rho are the fixtures that can be written alone")
+        raise SystemExit("--only: scalar, relax and coefw are written together (no --only)")
     d = inputs()
     t = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
     for k in ("field", "ru", "rv", "rom"):
@@ -394,6 +488,7 @@ def main() -> None:
     momentum(dyn, g)
     advance_uv(dyn, importlib_bdy(), g)
     calc_p_rho(dyn, g)
+    advance_mu_t(dyn, g)
 
 
 def importlib_bdy():

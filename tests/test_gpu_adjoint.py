@@ -295,3 +295,41 @@ def test_calc_p_rho_and_its_adjoint_match_reference_autograd(step):
             continue
         err = rel_l2(mine, ref)
         assert err < 1e-5, (step, k, err)
+
+
+def _mut_dir(n, r, shape):
+    # the directions of make_golden_adjoint.mut_direction
+    return np.random.default_rng(9000 + 100 * n + r).standard_normal(shape)
+
+
+@pytest.mark.parametrize("ref_no_grad", [True, False], ids=["reference_autograd", "operator"])
+def test_advance_mu_t_and_its_adjoint(ref_no_grad):
+    """advance_mu_t: the seven outputs against the reference's; with
+    ref_no_grad the adjoint against the reference's autograd gradients (its
+    mu update runs under torch.no_grad()), without it the adjoint's
+    directional derivatives against central differences of the reference's
+    float64 forward (tests/golden/mut_adj_ref64.npz)."""
+    T = load_npz("mut_adj_ref64.npz")
+    inputs = {k: _cuda(T[k]).requires_grad_(True) for k in adjoint.MUT_INPUTS}
+    data = {k: _cuda(T[k]) for k in adjoint.MUT_DATA}
+    outs = adjoint.advance_mu_t(inputs, data, float(T["dts"]), float(T["epssm"]), 1.0 / float(T["dx"]),
+                                1.0 / float(T["dy"]), ref_no_grad=ref_no_grad)
+    for k in adjoint.MUT_OUTPUTS:
+        assert rel_l2(outs[k].detach().cpu().numpy(), T[f"{k}_new"]) < 1e-6, k
+    sum((outs[k] * _cuda(T[f"cot_{k}"])).sum() for k in adjoint.MUT_OUTPUTS).backward()
+    names = ("ww", "ww_1", "u", "u_1", "v", "v_1", "t", "t_1", "t_ave", "ft",
+             "mu", "mut", "muave", "muts", "muu", "muv", "mudf", "mu_tend")
+    for n, k in enumerate(names):
+        gr = inputs[k].grad.double().cpu().numpy()
+        if ref_no_grad:
+            ref = T[f"grad_{k}"]
+            if not np.any(ref):
+                assert not np.any(gr), k
+                continue
+            err = rel_l2(gr, ref)
+            assert err < 1e-5, (k, err)
+        else:
+            for r in range(3):
+                an = float((gr * _mut_dir(n, r, gr.shape)).sum())
+                fd = float(T[f"fd_{k}_{r}"])
+                assert abs(an - fd) <= 1e-4 * abs(fd), (k, r, an, fd)

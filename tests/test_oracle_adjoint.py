@@ -248,3 +248,51 @@ def test_calc_p_rho_fixture_pinned_by_the_oracle():
             fd = (loss(xp) - loss(xm)) / (2 * eps)
             an = float((d * P[f"s{step}_grad_{name}"].astype(np.float64)).sum())
             assert abs(fd - an) <= 1e-5 * abs(an) + 1e-9, (step, name, fd, an)
+
+
+T = load_npz("mut_adj_ref64.npz")
+MUT3 = ("ww", "ww_1", "u", "u_1", "v", "v_1", "t", "t_1", "t_ave", "ft")
+MUT2 = ("mu", "mut", "muave", "muts", "muu", "muv", "mudf", "mu_tend")
+MUT_OUT = ("ww", "t", "t_ave", "muave", "muts", "mudf", "mu")
+# the oracle's state-dict names of advance_mu_t's arguments
+_MUT_ST = {"ww_1": "ww1", "u_1": "u_save", "v_1": "v_save", "t_1": "t_save", "t_ave": "t_2save", "ft": "t_tend"}
+
+
+def _mut_dir(n, r, shape):
+    # the directions of make_golden_adjoint.mut_direction
+    return np.random.default_rng(9000 + 100 * n + r).standard_normal(shape)
+
+
+def _advance_mu_t(g, x):
+    st = {_MUT_ST.get(k, k): np.array(v, np.float64) for k, v in x.items()}
+    for k in ("msftx", "msfty", "msfuy", "msfvx_inv", "dnw", "fnm", "fnp", "rdnw"):
+        st[k] = T[k].astype(np.float64)
+    OD.advance_mu_t(g, st, float(T["dts"]), float(T["epssm"]), 1)
+    return {o: st[_MUT_ST.get(o, o)] for o in MUT_OUT}
+
+
+def test_advance_mu_t_fixture_pinned_by_the_oracle():
+    """advance_mu_t: the oracle reproduces the reference's seven outputs on
+    the fixture, and its central differences equal the fixture's (of the
+    reference's float64 forward)."""
+    g = _grid()
+    base = {k: T[k].astype(np.float64) for k in MUT3 + MUT2}
+    outs = _advance_mu_t(g, base)
+    for o in MUT_OUT:
+        ref = T[f"{o}_new"]
+        assert np.abs(outs[o] - ref).max() <= 1e-12 * np.abs(ref).max(), o
+    cot = {o: T[f"cot_{o}"].astype(np.float64) for o in MUT_OUT}
+
+    def loss(x):
+        out = _advance_mu_t(g, x)
+        return sum(float((out[o] * cot[o]).sum()) for o in MUT_OUT)
+
+    for n, name in enumerate(MUT3 + MUT2):
+        d = _mut_dir(n, 0, base[name].shape)
+        eps = 1e-4 * float(np.abs(base[name]).max())  # the fixture's step
+        xp, xm = dict(base), dict(base)
+        xp[name] = base[name] + eps * d
+        xm[name] = base[name] - eps * d
+        fd = (loss(xp) - loss(xm)) / (2 * eps)
+        ref = float(T[f"fd_{name}_0"])
+        assert abs(fd - ref) <= 1e-6 * abs(ref) + 1e-9, (name, fd, ref)
