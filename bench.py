@@ -341,7 +341,7 @@ def run_ours(a):
                 "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan,
                 "surrogate": sur,
                 "adjoint": {"unavailable": "no whole-step adjoint yet: hand-written reverse-mode kernels exist for "
-                                           "advect_scalar, advect_u/v/w, relax_bdytend, advance_uv, calc_p_rho, "
+                                           "advect_scalar, advect_u/v/w, relax_bdytend, advance_uv, advance_mu_t, calc_p_rho, "
                                            "calc_coef_w and the implicit w solve (pywrf_b200.adjoint), not for "
                                            "the step they compose"}}
         print(json.dumps(line), flush=True)
