@@ -1,5 +1,6 @@
 """Drop-ins for ``pywrf.wrf_dynamics.advect_scalar``, ``advect_u``,
-``advect_v``, ``advect_w`` and ``calc_coef_w`` (reference signatures).
+``advect_v``, ``advect_w``, ``calc_coef_w``, ``calc_p_rho`` and
+``advance_mu_t`` (reference signatures).
 
 ``advect_scalar(...)`` takes the arguments of the reference function
 (pywrf/wrf_dynamics.py:1841-1850), adds the flux-form advection of ``field``
@@ -135,3 +136,67 @@ def calc_coef_w(a, alpha, gamma, mut, c1h, c2h, c1f, c2f, c3h, c4h, c3f, c4f, cq
                                 ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     N.check(rc, "wrf_coef_w")
     return a, alpha, gamma
+
+
+def _frame(name, shape, ids, ide, jds, jde, its, ite, jts, jte, kts, kte):
+    nz, ny, nx = shape
+    if (ids, jds, ide, jde) != (5, 5, nx - 5, ny - 5) or (its, ite, jts, jte) != (ids, ide, jds, jde) \
+            or (kts, kte) != (0, nz):
+        raise NotImplementedError(f"{name}: only the solver's 5-cell frame with tile = domain is supported")
+
+
+def _state_call(fn_name, cg, named, *args):
+    from .adjoint import _table  # the state-table builder shared with the adjoints
+
+    dev = next(iter(named.values())).device
+    with torch.cuda.device(dev):
+        rc = getattr(N.lib(), fn_name)(ctypes.byref(cg), _table(named), *args,
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    N.check(rc, fn_name)
+
+
+def calc_p_rho(al_ori, p_ori, ph, alt, t_2, t_1, c2a, pm1, mu, mut, c1h, c2h, c1f, c2f, c3h, c4h, c3f, c4f, znu, t0,
+               rdnw, dnw, smdiv, non_hydrostatic, step, ids, ide, jds, jde, kds, kde, ims, ime, jms, jme, kms, kme,
+               its, ite, jts, jte, kts, kte):
+    """calc_p_rho (pywrf/wrf_dynamics.py:3269-3313) on the GPU through
+    ``wrf_calc_p_rho``: returns new (al, p, pm1) like the reference - at step
+    0 pm1 is a new copy of the new p, at a later step the caller's pm1 is
+    updated in place and returned.  c1h..c4f, znu and dnw are accepted and
+    unused, as in the reference; t0 must be the solver's 300."""
+    _frame("calc_p_rho", p_ori.shape, ids, ide, jds, jde, its, ite, jts, jte, kts, kte)
+    if abs(float(t0) - 300.0) > 1e-9:
+        raise ValueError("calc_p_rho: the kernels use the solver's t0 = 300")
+    nz, ny, nx = p_ori.shape
+    cg = make_cgrid(Grid.make(nx, ny, nz, 9000.0, 9000.0, 1.0), {"cf1": 0.0, "cf2": 0.0, "cf3": 0.0, "cfn": 0.0,
+                                                                 "cfn1": 0.0})
+    cg.smdiv = float(smdiv)
+    al, p = al_ori.clone(), p_ori.clone()
+    pm1_out = torch.empty_like(p) if int(step) == 0 else pm1
+    _state_call("wrf_calc_p_rho", cg, {"al": al, "p": p, "ph": ph, "alt": alt, "t": t_2, "t_save": t_1, "c2a": c2a,
+                                       "pm1": pm1_out, "mu": mu, "muts": mut, "rdnw": rdnw}, int(step))
+    return al, p, pm1_out
+
+
+def advance_mu_t(ww_ori, ww_1, u, u_1, v, v_1, mu_ori, mut, muave_ori, muts_ori, muu, muv, mudf_ori, c1h, c2h, c1f,
+                 c2f, c3h, c4h, c3f, c4f, uam, vam, wwam, t_ori, t_1, t_ave_ori, ft, mu_tend, rdx, rdy, dts, epssm,
+                 dnw, fnm, fnp, rdnw, msfux, msfuy, msfvx, msfvx_inv, msfvy, msftx, msfty, step, ids, ide, jds, jde,
+                 kds, kde, ims, ime, jms, jme, kms, kme, its, ite, jts, jte, kts, kte):
+    """advance_mu_t (pywrf/wrf_dynamics.py:3528-3638) on the GPU through
+    ``wrf_advance_mu_t``: returns (ww, ww_1, t, t_ave, uam, vam, wwam, muave,
+    muts, mudf, mu) like the reference, the updated ones as new tensors.
+    c1h..c4f, msfux, msfvx, msfvy and step are accepted and unused, as in the
+    reference."""
+    _frame("advance_mu_t", ww_ori.shape, ids, ide, jds, jde, its, ite, jts, jte, kts, kte)
+    nz, ny, nx = ww_ori.shape
+    cg = make_cgrid(Grid.make(nx, ny, nz, 1.0 / float(rdx), 1.0 / float(rdy), 1.0),
+                    {"cf1": 0.0, "cf2": 0.0, "cf3": 0.0, "cfn": 0.0, "cfn1": 0.0})
+    cg.dx, cg.dy = 1.0 / float(rdx), 1.0 / float(rdy)
+    cg.epssm = float(epssm)
+    ww, t, t_ave = ww_ori.clone(), t_ori.clone(), t_ave_ori.clone()
+    mu, muave, muts, mudf = mu_ori.clone(), muave_ori.clone(), muts_ori.clone(), mudf_ori.clone()
+    _state_call("wrf_advance_mu_t", cg, {
+        "ww": ww, "ww1": ww_1, "u": u, "u_save": u_1, "v": v, "v_save": v_1, "mu": mu, "mut": mut, "muave": muave,
+        "muts": muts, "muu": muu, "muv": muv, "mudf": mudf, "t": t, "t_save": t_1, "t_2save": t_ave, "t_tend": ft,
+        "mu_tend": mu_tend, "dnw": dnw, "fnm": fnm, "fnp": fnp, "rdnw": rdnw, "msfuy": msfuy,
+        "msfvx_inv": msfvx_inv, "msftx": msftx, "msfty": msfty}, float(dts))
+    return ww, ww_1, t, t_ave, uam, vam, wwam, muave, muts, mudf, mu

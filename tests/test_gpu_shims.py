@@ -146,3 +146,56 @@ def test_relax_bdytend_shim_against_the_reference(var):
     with pytest.raises(ValueError):
         wrf_boundary.relax_bdytend(field, tend, *bdy, var, 5, 1, 4, 1.0, [0.0, 1.0, 2.0, 3.0, 0.0],
                                    wrf_boundary.GCX, *idx)
+
+
+def _c(a):
+    return torch.tensor(np.asarray(a), dtype=torch.float32, device="cuda").contiguous()
+
+
+@pytest.mark.parametrize("step", [0, 1])
+def test_calc_p_rho_shim_with_the_solver_arguments(step):
+    """calc_p_rho called with the reference's argument list against the
+    reference's own outputs (tests/golden/prho_adj_ref64.npz); at a later
+    step the caller's pm1 is updated in place, as in the reference."""
+    from helpers import load_npz
+
+    P = load_npz("prho_adj_ref64.npz")
+    nz, n = P["p"].shape[0], P["p"].shape[1]
+    one1 = torch.ones(nz, device="cuda")
+    t = {k: _c(P[k]) for k in ("al", "p", "ph", "alt", "t_2", "t_1", "c2a", "pm1", "mu", "mut", "rdnw")}
+    pm1_in = t["pm1"]
+    al, p, pm1 = wrf_dynamics.calc_p_rho(t["al"], t["p"], t["ph"], t["alt"], t["t_2"], t["t_1"], t["c2a"], pm1_in,
+                                         t["mu"], t["mut"], one1, one1 * 0, one1, one1 * 0, one1, one1 * 0, one1,
+                                         one1 * 0, one1, 300.0, t["rdnw"], one1, float(P["smdiv"]), True, step,
+                                         5, n - 5, 5, n - 5, 0, nz, 0, n, 0, n, 0, nz, 5, n - 5, 5, n - 5, 0, nz)
+    assert (pm1 is pm1_in) == (step != 0)
+    for nm, mine in (("al", al), ("p", p), ("pm1", pm1)):
+        assert rel_l2(mine.cpu().numpy(), P[f"s{step}_{nm}_new"]) < 1e-6, nm
+
+
+def test_advance_mu_t_shim_with_the_solver_arguments():
+    """advance_mu_t called with the reference's argument list (as
+    solver.py:1380-1393 calls it) against the reference's own outputs
+    (tests/golden/mut_adj_ref64.npz)."""
+    from helpers import load_npz
+
+    T = load_npz("mut_adj_ref64.npz")
+    nz, n = T["ww"].shape[0], T["ww"].shape[1]
+    one1 = torch.ones(nz, device="cuda")
+    t = {k: _c(T[k]) for k in T if not k.startswith(("cot_", "grad_", "fd_")) and not k.endswith("_new")
+         and np.asarray(T[k]).ndim > 0}
+    out = wrf_dynamics.advance_mu_t(t["ww"], t["ww_1"], t["u"], t["u_1"], t["v"], t["v_1"], t["mu"], t["mut"],
+                                    t["muave"], t["muts"], t["muu"], t["muv"], t["mudf"], one1, one1 * 0, one1,
+                                    one1 * 0, one1, one1 * 0, one1, one1 * 0, None, None, None, t["t"], t["t_1"],
+                                    t["t_ave"], t["ft"], t["mu_tend"], 1.0 / float(T["dx"]), 1.0 / float(T["dy"]),
+                                    float(T["dts"]), float(T["epssm"]), t["dnw"], t["fnm"], t["fnp"], t["rdnw"],
+                                    t["msfuy"], t["msfuy"], t["msfvx_inv"], t["msfvx_inv"], t["msfvx_inv"],
+                                    t["msftx"], t["msfty"], 1,
+                                    5, n - 5, 5, n - 5, 0, nz, 0, n, 0, n, 0, nz, 5, n - 5, 5, n - 5, 0, nz)
+    ww, ww_1, tt, t_ave, uam, vam, wwam, muave, muts, mudf, mu = out
+    assert ww_1 is t["ww_1"] and uam is None
+    for nm, mine in (("ww", ww), ("t", tt), ("t_ave", t_ave), ("muave", muave), ("muts", muts), ("mudf", mudf),
+                     ("mu", mu)):
+        assert rel_l2(mine.cpu().numpy(), T[f"{nm}_new"]) < 1e-6, nm
+    # the inputs are left as they were (the reference clones them)
+    assert torch.equal(t["ww"], _c(T["ww"])) and torch.equal(t["mu"], _c(T["mu"]))
