@@ -84,7 +84,7 @@ def test_small_two_steps_vs_reference_fp64(small):
     assert it.status() == {"nan_p": 0, "step": SMALL["nsteps"], "wait_timeouts": 0}
 
 
-def test_small_one_step_north_star_tolerance(small):
+def test_small_one_step_within_1e5_relative_l2(small):
     """After one step, relative L2 against the fp64 reference within 1e-5 for
     every field whose own fp32 reference error is below 1e-5 (the reference
     itself misses 1e-5 on v, w, mu, p, al, ww, qc, qi, h_diabatic)."""
