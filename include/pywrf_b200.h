@@ -205,6 +205,19 @@ int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream)
  * of a saved operand), so the product is checked against finite differences
  * of its forward. */
 int wrf_advance_uv_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float dts, void* stream);
+/* wrf_dynamics.py:3641-3796 advance_w on the state table, in place, with
+ * the solver's arguments: w, rw_tend, ww, w_save, u, v, muave, muts, mut,
+ * t_2ave (T_2SAVE), t_2 (T), t_1 (T_SAVE), ph, ph_1 (PH_SAVE), phb, ph_tend,
+ * ht, c2a, cqw, alt, a, alpha, gamma, msftx, msfty, fnm, fnp, rdnw, rdn and
+ * the grid's epssm, cf1..cf3 (top_lid 0); updates t_2save, w and ph. */
+int wrf_advance_w(const WrfGrid* g, const WrfState* s, float dts, void* stream);
+/* Its adjoint: sbar's W, PH, T_2SAVE hold the cotangents of the updated
+ * fields and are rewritten to those of the inputs; those of the other 20
+ * operands above (u, v, ht included, through the lower boundary) are
+ * accumulated (+=).  work: caller-owned scratch of ny*nx floats.  The
+ * reference's autograd cannot run backward through its in-place sweeps. */
+int wrf_advance_w_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float dts, float* work,
+                      void* stream);
 /* wrf_dynamics.py:3528-3638 advance_mu_t on the state table, in place, with
  * the solver's arguments (solver.py:1380-1393): ww (WW), ww_1 (WW1), u,
  * u_1 (U_SAVE), v, v_1 (V_SAVE), mu, mut, muave, muts, muu, muv, mudf, t,

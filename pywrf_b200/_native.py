@@ -98,6 +98,10 @@ def lib() -> ctypes.CDLL:
     L.wrf_set_kernel_form.argtypes = [ctypes.c_int]
     L.wrf_advect_momentum.restype = ip
     L.wrf_advect_momentum.argtypes = [ctypes.POINTER(WrfGridC), ctypes.c_int] + [vp] * 10 + [ctypes.c_int, vp]
+    L.wrf_advance_w.restype = ip
+    L.wrf_advance_w.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_float, vp]
+    L.wrf_advance_w_adj.restype = ip
+    L.wrf_advance_w_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, vp, vp]
     L.wrf_advance_mu_t.restype = ip
     L.wrf_advance_mu_t.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_float, vp]
     L.wrf_advance_mu_t_adj.restype = ip

@@ -24,6 +24,9 @@ operators keeps no tape of the forward's intermediates.
   gradients with respect to its 18 array inputs, either of the operator
   (default) or as the reference's autograd gives them (``ref_no_grad``: its
   mu / muts / mudf / muave update runs under ``torch.no_grad()``).
+* :class:`AdvanceW` -- advance_w (pywrf/wrf_dynamics.py:3641-3796): the
+  vertically implicit w / phi update with its terrain lower boundary and
+  Rayleigh damping; gradients with respect to its 23 array inputs.
 * :class:`RelaxBdytend` -- ``tendency + relax(field)`` toward the lateral
   boundary values (pywrf/wrf_boundary.py:52-147); gradients with respect to
   the field and the incoming tendency (the boundary arrays are data).
@@ -196,6 +199,61 @@ def advance_uv(inputs: dict, data: dict, dts, emdiv, cf1, cf2, cf3, rdx, rdy):
     ``inputs`` maps UV_INPUTS, ``data`` UV_DATA to tensors; returns (u', v')."""
     return AdvanceUV.apply((dts, emdiv, cf1, cf2, cf3, rdx, rdy), *[inputs[k] for k in UV_INPUTS],
                            *[data[k] for k in UV_DATA])
+
+
+AW_INPUTS = ("w", "rw_tend", "ww", "w_save", "u", "v", "muave", "muts", "mut", "t_2ave", "t_2", "t_1", "ph", "ph_1",
+             "phb", "ph_tend", "ht", "c2a", "cqw", "alt", "a", "alpha", "gamma")
+AW_DATA = ("msftx", "msfty", "fnm", "fnp", "rdnw", "rdn")
+AW_OUTPUTS = ("t_2ave", "w", "ph")
+_AW_FIELD = {"t_2ave": "t_2save", "t_2": "t", "t_1": "t_save", "ph_1": "ph_save"}
+
+
+class AdvanceW(torch.autograd.Function):
+    """(t_2ave', w', ph') = advance_w(...); the tensors follow AW_INPUTS then
+    AW_DATA, ``scal`` = (dts, epssm, cf1, cf2, cf3, rdx, rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, *tensors):
+        dts, epssm, cf1, cf2, cf3, rdx, rdy = (float(x) for x in scal)
+        named = dict(zip(AW_INPUTS + AW_DATA, tensors))
+        cg = scalar_grid(named["w"].shape, rdx, rdy)
+        cg.epssm, cg.cf1, cg.cf2, cg.cf3 = epssm, cf1, cf2, cf3
+        outs = {k: named[k].detach().clone() for k in AW_OUTPUTS}
+        tab = _table({_AW_FIELD.get(k, k): v for k, v in {**named, **outs}.items()})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(outs["w"].device):
+            rc = N.lib().wrf_advance_w(ctypes.byref(cg), tab, dts, stream)
+        N.check(rc, "wrf_advance_w")
+        ctx.save_for_backward(*tensors)
+        ctx.cg, ctx.dts = cg, dts
+        return tuple(outs[k] for k in AW_OUTPUTS)
+
+    @staticmethod
+    def backward(ctx, *gouts):
+        tensors = ctx.saved_tensors
+        named = dict(zip(AW_INPUTS + AW_DATA, tensors))
+        bars = {}
+        for k, gk in zip(AW_OUTPUTS, gouts):
+            bars[k] = torch.zeros_like(named[k]) if gk is None else gk.contiguous().clone()
+        for k in AW_INPUTS:
+            if k not in bars:
+                bars[k] = torch.zeros_like(named[k])
+        work = torch.empty_like(named["ht"])
+        tab = _table({_AW_FIELD.get(k, k): v for k, v in named.items()})
+        btab = _table({_AW_FIELD.get(k, k): v for k, v in bars.items()})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(work.device):
+            rc = N.lib().wrf_advance_w_adj(ctypes.byref(ctx.cg), tab, btab, ctx.dts, _ptr(work), stream)
+        N.check(rc, "wrf_advance_w_adj")
+        return (None,) + tuple(bars[k] for k in AW_INPUTS) + (None,) * len(AW_DATA)
+
+
+def advance_w(inputs: dict, data: dict, dts, epssm, cf1, cf2, cf3, rdx=1.0 / 9000.0, rdy=1.0 / 9000.0):
+    """Differentiable advance_w on the GPU: ``inputs`` maps AW_INPUTS, ``data``
+    AW_DATA to tensors; returns a dict of AW_OUTPUTS."""
+    outs = AdvanceW.apply((dts, epssm, cf1, cf2, cf3, rdx, rdy), *[inputs[k] for k in AW_INPUTS],
+                          *[data[k] for k in AW_DATA])
+    return dict(zip(AW_OUTPUTS, outs))
 
 
 MUT_INPUTS = ("ww", "ww_1", "u", "u_1", "v", "v_1", "t", "t_1", "t_ave", "ft", "mu", "mut", "muave", "muts", "muu",

@@ -86,6 +86,23 @@
 //                        input of the same name and nothing to dmdt, mut or
 //                        mu_tend).
 //
+//   k_advance_w / k_advance_w_adj_col / k_advance_w_adj_bc  advance_w
+//                        (wrf_dynamics.py:3641-3796) on the columns [ids+1,
+//                        ide-2) x [jds+1, jde-2): t_2ave, the right-hand side
+//                        rhs = ph + msfty R / mut (R from ph_tend, w and the
+//                        vertical phi fluxes wdwn), the explicit w x(k), the
+//                        lower boundary x(0) from the terrain slope and the
+//                        near-surface winds, the implicit solve with a, alpha,
+//                        gamma, the Rayleigh damping of the upper levels and
+//                        the phi update.  The adjoint runs each column's
+//                        chain backwards in one thread (forward values
+//                        recomputed into local arrays; the solve transposed
+//                        as in k_vsolve_w_adj; the damping weight's sin^2
+//                        differentiated in ph_1 and phb through hk and htop)
+//                        and leaves the cotangent of x(0) in a work array, from
+//                        which a second kernel gathers those of u, v (levels
+//                        0..2) and ht.
+//
 //   k_relax_field / k_relax_field_adj  relax_bdytend (wrf_boundary.py:52-147)
 //                        on one field, and its adjoint with respect to the
 //                        field: at a relaxation point P of distance b,
@@ -836,6 +853,335 @@ int launch_advance_mu_t_adj(const Grid& g, const S& s, const S& b, float dts, in
   k_advance_mu_t_adj_pt<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, dts, work);
   k_advance_mu_t_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, dts, ref_no_grad, work);
   return 3;
+}
+
+// ------------------------------------------------------------ advance_w
+// state-table operands (solver.py advance_w call): w W, rw_tend RW_TEND, ww WW,
+// w_save W_SAVE, u U, v V, muave MUAVE, muts MUTS, mut MUT, t_2ave T_2SAVE,
+// t_2 T, t_1 T_SAVE, ph PH, ph_1 PH_SAVE, phb PHB, ph_tend PH_TEND, ht HT,
+// c2a C2A, cqw CQW, alt ALT, a A, alpha ALPHA, gamma GAMMA, with msftx, msfty,
+// fnm, fnp, rdnw, rdn
+
+namespace {
+
+constexpr float kAwHdepth = 5000.0f;
+
+// one column's forward values
+struct AwCol {
+  float t2a[kMaxNz], wd[kMaxNz], R[kMaxNz], rhs[kMaxNz], P[kMaxNz], x[kMaxNz], y[kMaxNz], z[kMaxNz], d[kMaxNz],
+      wf[kMaxNz], hk[kMaxNz];
+  float hbot;
+};
+
+__device__ float aw_bc(const Grid& g, const S& s, int j, int i) {
+  const int nx = g.nx;
+  const size_t lev = (size_t)g.ny * nx, c = (size_t)j * nx + i;
+  const float* ht = s[WF_HT];
+  const float* u = s[WF_U];
+  const float* v = s[WF_V];
+  auto cv = [&](size_t cc) { return g.cf1 * v[cc] + g.cf2 * v[lev + cc] + g.cf3 * v[2 * lev + cc]; };
+  auto cu = [&](size_t cc) { return g.cf1 * u[cc] + g.cf2 * u[lev + cc] + g.cf3 * u[2 * lev + cc]; };
+  return s[WF_MSFTY][c] * 0.5f * g.rdy * ((ht[c + nx] - ht[c]) * cv(c + nx) + (ht[c] - ht[c - nx]) * cv(c)) +
+         s[WF_MSFTX][c] * 0.5f * g.rdx * ((ht[c + 1] - ht[c]) * cu(c + 1) + (ht[c] - ht[c - 1]) * cu(c));
+}
+
+__device__ void aw_column(const Grid& g, const S& s, float dts, int j, int i, AwCol& m) {
+  const int ktf = g.nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
+  const float ep1 = (float)(1.0 + (double)g.epssm), em1 = (float)(1.0 - (double)g.epssm);
+  const float gf = (float)G, t0 = (float)T0;
+  const float muave = s[WF_MUAVE][c], muts = s[WF_MUTS][c], mut = s[WF_MUT][c], msfty = s[WF_MSFTY][c];
+  const float* rdnw = s[WF_RDNW];
+  const float* rdn = s[WF_RDN];
+  auto F = [&](int id, int k) { return s[id][k * lev + c]; };
+  for (int k = 0; k < ktf; ++k) {
+    const float tt = 0.5f * (ep1 * F(WF_T, k) + em1 * F(WF_T_2SAVE, k));
+    m.t2a[k] = (tt + muave * t0) / (muts * (t0 + F(WF_T_SAVE, k)));
+  }
+  m.wd[0] = 0.f;
+  for (int k = 1; k <= ktf; ++k)
+    m.wd[k] = 0.5f * (F(WF_WW, k) + F(WF_WW, k - 1)) * rdnw[k - 1] *
+              (F(WF_PH_SAVE, k) - F(WF_PH_SAVE, k - 1) + F(WF_PHB, k) - F(WF_PHB, k - 1));
+  m.rhs[0] = 0.f;
+  for (int k = 1; k <= ktf; ++k) {
+    float r = dts * (F(WF_PH_TEND, k) + 0.5f * gf * em1 * F(WF_W, k));
+    if (k < ktf) r = r - dts * (s[WF_FNM][k] * m.wd[k + 1] + s[WF_FNP][k] * m.wd[k]);
+    m.R[k] = r;
+    m.rhs[k] = F(WF_PH, k) + msfty * r / mut;
+  }
+  for (int k = 0; k < ktf; ++k)
+    m.P[k] = ep1 * (m.rhs[k + 1] - m.rhs[k]) + em1 * (F(WF_PH, k + 1) - F(WF_PH, k));
+  const float minv = 1.0f / msfty;
+  m.x[0] = aw_bc(g, s, j, i);
+  for (int k = 1; k < ktf; ++k) {
+    const float X1 = F(WF_C2A, k) * rdnw[k] / mut * m.P[k];
+    const float X2 = F(WF_C2A, k - 1) * rdnw[k - 1] / mut * m.P[k - 1];
+    m.x[k] = F(WF_W, k) + dts * F(WF_RW_TEND, k) + minv * F(WF_CQW, k) * (0.5f * dts * gf * rdn[k] * (X1 - X2)) +
+             dts * gf * minv *
+                 (rdn[k] * (F(WF_C2A, k) * F(WF_ALT, k) * m.t2a[k] - F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * m.t2a[k - 1]) -
+                  muave);
+  }
+  {
+    const int k = ktf;
+    const float rm = rdnw[k - 1];
+    m.x[k] = F(WF_W, k) + dts * F(WF_RW_TEND, k) +
+             minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f * F(WF_C2A, k - 1) * m.P[k - 1] -
+                     dts * gf * (2.0f * rm * F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * m.t2a[k - 1] + muave));
+  }
+  m.y[0] = m.x[0];
+  for (int k = 1; k <= ktf; ++k) m.y[k] = (m.x[k] - F(WF_A, k) * m.y[k - 1]) * F(WF_ALPHA, k);
+  m.z[ktf] = m.y[ktf];
+  for (int k = ktf - 1; k >= 1; --k) m.z[k] = m.y[k] - F(WF_GAMMA, k) * m.z[k + 1];
+  m.z[0] = m.y[0];
+  const float dampmag = (float)((double)dts * 0.2), hpi = (float)(0.5 * 3.14159265359);
+  m.hbot = (F(WF_PH_SAVE, ktf) + F(WF_PHB, ktf)) / gf - kAwHdepth;
+  m.wf[0] = m.z[0];
+  for (int k = 1; k <= ktf; ++k) {
+    m.hk[k] = (F(WF_PH_SAVE, k) + F(WF_PHB, k)) / gf;
+    float dw = 0.f;
+    if (m.hk[k] >= m.hbot) {
+      const float sn = sinf(hpi * (m.hk[k] - m.hbot) / kAwHdepth);
+      dw = dampmag * (sn * sn);
+    }
+    m.d[k] = dw;
+    m.wf[k] = (m.z[k] - dw * mut * F(WF_W_SAVE, k)) / (1.0f + dw);
+  }
+}
+
+}  // namespace
+
+__global__ void k_advance_w(Grid g, S s, float dts) {
+  WRF_COLUMN_INDEX(g, j, i);
+  if (!mut_in(g, j, i)) return;
+  const int ktf = g.nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
+  AwCol m;
+  aw_column(g, s, dts, j, i, m);
+  const float ep1 = (float)(1.0 + (double)g.epssm), gf = (float)G;
+  const float muts = s[WF_MUTS][c], msfty = s[WF_MSFTY][c];
+  for (int k = 0; k < ktf; ++k) s[WF_T_2SAVE][k * lev + c] = m.t2a[k];
+  s[WF_W][c] = m.wf[0];
+  for (int k = 1; k <= ktf; ++k) {
+    s[WF_W][k * lev + c] = m.wf[k];
+    s[WF_PH][k * lev + c] = m.rhs[k] + msfty * 0.5f * dts * gf * ep1 * m.wf[k] / muts;
+  }
+}
+
+__global__ void k_advance_w_adj_col(Grid g, S s, S b, float dts, float* work) {
+  WRF_COLUMN_INDEX(g, j, i);
+  if (!mut_in(g, j, i)) return;
+  const int ktf = g.nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
+  AwCol m;
+  aw_column(g, s, dts, j, i, m);
+  const float ep1 = (float)(1.0 + (double)g.epssm), em1 = (float)(1.0 - (double)g.epssm);
+  const float gf = (float)G, t0 = (float)T0;
+  const float muave = s[WF_MUAVE][c], muts = s[WF_MUTS][c], mut = s[WF_MUT][c], msfty = s[WF_MSFTY][c];
+  const float minv = 1.0f / msfty;
+  const float* rdnw = s[WF_RDNW];
+  const float* rdn = s[WF_RDN];
+  auto F = [&](int id, int k) { return s[id][k * lev + c]; };
+  auto B = [&](int id, int k) -> float& { return b[id][k * lev + c]; };
+  float wb[kMaxNz], pb_in[kMaxNz], tb[kMaxNz], zb[kMaxNz], yb[kMaxNz], xb[kMaxNz], Pb[kMaxNz], rhsb[kMaxNz],
+      wdb[kMaxNz], t2ab[kMaxNz], ph1b[kMaxNz], phbb[kMaxNz], wib[kMaxNz];
+  for (int k = 0; k <= ktf; ++k) {
+    wb[k] = B(WF_W, k);
+    pb_in[k] = 0.f;
+    tb[k] = B(WF_T_2SAVE, k);
+    zb[k] = yb[k] = xb[k] = Pb[k] = rhsb[k] = wdb[k] = t2ab[k] = ph1b[k] = phbb[k] = wib[k] = 0.f;
+  }
+  float mutb = 0.f, mutsb = 0.f, muaveb = 0.f;
+  // phi update: ph'(k) = rhs(k) + msfty 0.5 dts g (1+e) w'(k) / muts, k >= 1; ph'(0) = ph(0)
+  const float cph = msfty * 0.5f * dts * gf * ep1;
+  float wfb[kMaxNz];
+  wfb[0] = wb[0];
+  pb_in[0] = B(WF_PH, 0);
+  for (int k = 1; k <= ktf; ++k) {
+    const float pbk = B(WF_PH, k);
+    rhsb[k] += pbk;
+    wfb[k] = wb[k] + pbk * cph / muts;
+    mutsb += -pbk * cph * m.wf[k] / (muts * muts);
+  }
+  // damping: w'(k) = (z(k) - d mut w_save) / (1 + d)
+  const float dampmag = (float)((double)dts * 0.2), hpi = (float)(0.5 * 3.14159265359);
+  float hbotb = 0.f;
+  zb[0] = wfb[0];
+  for (int k = 1; k <= ktf; ++k) {
+    const float dk = m.d[k], ws = F(WF_W_SAVE, k), den = 1.0f + dk;
+    zb[k] = wfb[k] / den;
+    B(WF_W_SAVE, k) += -wfb[k] * dk * mut / den;
+    mutb += -wfb[k] * dk * ws / den;
+    if (m.hk[k] >= m.hbot) {
+      const float db = wfb[k] * (-mut * ws - m.wf[k]) / den;
+      const float th = hpi * (m.hk[k] - m.hbot) / kAwHdepth;
+      const float thb = db * dampmag * sinf(2.0f * th);
+      const float hkb = thb * hpi / kAwHdepth;
+      hbotb += -hkb;
+      ph1b[k] += hkb / gf;
+      phbb[k] += hkb / gf;
+    }
+  }
+  ph1b[ktf] += hbotb / gf;  // hbot = htop - hdepth, htop = (ph_1 + phb)(ktf) / g
+  phbb[ktf] += hbotb / gf;
+  // the implicit solve, transposed
+  for (int k = 1; k <= ktf - 1; ++k) {
+    yb[k] += zb[k];
+    B(WF_GAMMA, k) += -m.z[k + 1] * zb[k];
+    zb[k + 1] += -F(WF_GAMMA, k) * zb[k];
+  }
+  yb[ktf] += zb[ktf];
+  yb[0] += zb[0];
+  for (int k = ktf; k >= 1; --k) {
+    const float al = F(WF_ALPHA, k), ak = F(WF_A, k);
+    xb[k] = al * yb[k];
+    B(WF_A, k) += -m.y[k - 1] * al * yb[k];
+    B(WF_ALPHA, k) += (m.x[k] - ak * m.y[k - 1]) * yb[k];
+    yb[k - 1] += -ak * al * yb[k];
+  }
+  xb[0] = yb[0];
+  // explicit w
+  for (int k = 1; k < ktf; ++k) {
+    const float x_b = xb[k];
+    if (x_b == 0.f) continue;
+    wib[k] += x_b;
+    B(WF_RW_TEND, k) += dts * x_b;
+    const float X1 = F(WF_C2A, k) * rdnw[k] / mut * m.P[k];
+    const float X2 = F(WF_C2A, k - 1) * rdnw[k - 1] / mut * m.P[k - 1];
+    const float C1 = minv * F(WF_CQW, k) * 0.5f * dts * gf * rdn[k];
+    B(WF_CQW, k) += x_b * minv * 0.5f * dts * gf * rdn[k] * (X1 - X2);
+    const float X1b = x_b * C1, X2b = -x_b * C1;
+    B(WF_C2A, k) += X1b * rdnw[k] / mut * m.P[k];
+    mutb += -X1b * X1 / mut;
+    Pb[k] += X1b * F(WF_C2A, k) * rdnw[k] / mut;
+    B(WF_C2A, k - 1) += X2b * rdnw[k - 1] / mut * m.P[k - 1];
+    mutb += -X2b * X2 / mut;
+    Pb[k - 1] += X2b * F(WF_C2A, k - 1) * rdnw[k - 1] / mut;
+    const float Bx = dts * gf * minv * x_b;
+    B(WF_C2A, k) += Bx * rdn[k] * F(WF_ALT, k) * m.t2a[k];
+    B(WF_ALT, k) += Bx * rdn[k] * F(WF_C2A, k) * m.t2a[k];
+    t2ab[k] += Bx * rdn[k] * F(WF_C2A, k) * F(WF_ALT, k);
+    B(WF_C2A, k - 1) += -Bx * rdn[k] * F(WF_ALT, k - 1) * m.t2a[k - 1];
+    B(WF_ALT, k - 1) += -Bx * rdn[k] * F(WF_C2A, k - 1) * m.t2a[k - 1];
+    t2ab[k - 1] += -Bx * rdn[k] * F(WF_C2A, k - 1) * F(WF_ALT, k - 1);
+    muaveb += -Bx;
+  }
+  {
+    const int k = ktf;
+    const float x_b = xb[k], rm = rdnw[k - 1];
+    wib[k] += x_b;
+    B(WF_RW_TEND, k) += dts * x_b;
+    const float Ct = minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f);
+    const float term1 = Ct * F(WF_C2A, k - 1) * m.P[k - 1];
+    B(WF_C2A, k - 1) += x_b * Ct * m.P[k - 1];
+    Pb[k - 1] += x_b * Ct * F(WF_C2A, k - 1);
+    mutb += -x_b * term1 / mut;
+    const float Bt = -minv * dts * gf * x_b;
+    B(WF_C2A, k - 1) += Bt * 2.0f * rm * F(WF_ALT, k - 1) * m.t2a[k - 1];
+    B(WF_ALT, k - 1) += Bt * 2.0f * rm * F(WF_C2A, k - 1) * m.t2a[k - 1];
+    t2ab[k - 1] += Bt * 2.0f * rm * F(WF_C2A, k - 1) * F(WF_ALT, k - 1);
+    muaveb += Bt;
+  }
+  // P(k) = (1+e) (rhs(k+1) - rhs(k)) + (1-e) (ph(k+1) - ph(k)), rhs(0) = 0
+  for (int k = 0; k < ktf; ++k) {
+    rhsb[k + 1] += ep1 * Pb[k];
+    if (k >= 1) rhsb[k] += -ep1 * Pb[k];
+    pb_in[k + 1] += em1 * Pb[k];
+    pb_in[k] += -em1 * Pb[k];
+  }
+  // rhs(k) = ph(k) + msfty R(k) / mut
+  for (int k = 1; k <= ktf; ++k) {
+    pb_in[k] += rhsb[k];
+    const float Rb = rhsb[k] * msfty / mut;
+    mutb += -rhsb[k] * msfty * m.R[k] / (mut * mut);
+    B(WF_PH_TEND, k) += dts * Rb;
+    wib[k] += dts * 0.5f * gf * em1 * Rb;
+    if (k < ktf) {
+      wdb[k + 1] += -dts * s[WF_FNM][k] * Rb;
+      wdb[k] += -dts * s[WF_FNP][k] * Rb;
+    }
+  }
+  // wdwn(k) = (ww(k) + ww(k-1)) / 2 rdnw(k-1) (ph_1 + phb)(k) - (ph_1 + phb)(k-1)
+  for (int k = 1; k <= ktf; ++k) {
+    if (wdb[k] == 0.f) continue;
+    const float h = 0.5f * rdnw[k - 1];
+    const float dph = F(WF_PH_SAVE, k) - F(WF_PH_SAVE, k - 1) + F(WF_PHB, k) - F(WF_PHB, k - 1);
+    B(WF_WW, k) += wdb[k] * h * dph;
+    B(WF_WW, k - 1) += wdb[k] * h * dph;
+    const float dphb = wdb[k] * h * (F(WF_WW, k) + F(WF_WW, k - 1));
+    ph1b[k] += dphb;
+    ph1b[k - 1] += -dphb;
+    phbb[k] += dphb;
+    phbb[k - 1] += -dphb;
+  }
+  // t_2ave(k) = (0.5 ((1+e) t_2 + (1-e) t_2ave) + muave t0) / (muts (t0 + t_1)), k < ktf
+  for (int k = 0; k < ktf; ++k) {
+    const float T = tb[k] + t2ab[k];
+    const float t1 = F(WF_T_SAVE, k), Dm = muts * (t0 + t1);
+    const float ttb = T / Dm;
+    muaveb += T * t0 / Dm;
+    mutsb += -T * m.t2a[k] / muts;
+    B(WF_T_SAVE, k) += -T * m.t2a[k] / (t0 + t1);
+    B(WF_T, k) += ttb * 0.5f * ep1;
+    B(WF_T_2SAVE, k) = ttb * 0.5f * em1;
+  }
+  for (int k = 0; k <= ktf; ++k) {
+    B(WF_PH_SAVE, k) += ph1b[k];
+    B(WF_PHB, k) += phbb[k];
+    B(WF_PH, k) = pb_in[k];
+    B(WF_W, k) = wib[k];  // w(0) is replaced by the lower boundary value: wib[0] = 0
+  }
+  b[WF_MUT][c] += mutb;
+  b[WF_MUTS][c] += mutsb;
+  b[WF_MUAVE][c] += muaveb;
+  work[c] = xb[0];
+}
+
+__global__ void k_advance_w_adj_bc(Grid g, S s, S b, const float* work) {
+  WRF_POINT_INDEX(g, k, j, i);
+  if (k > 2) return;
+  const int nx = g.nx;
+  const size_t lev = (size_t)g.ny * nx, c = (size_t)j * nx + i, p = k * lev + c;
+  const float* ht = s[WF_HT];
+  auto Y = [&](int jj, int ii) {
+    if (jj < 0 || ii < 0 || jj >= g.ny || ii >= nx || !mut_in(g, jj, ii)) return 0.f;
+    return work[(size_t)jj * nx + ii] * s[WF_MSFTY][(size_t)jj * nx + ii];
+  };
+  auto Xx = [&](int jj, int ii) {
+    if (jj < 0 || ii < 0 || jj >= g.ny || ii >= nx || !mut_in(g, jj, ii)) return 0.f;
+    return work[(size_t)jj * nx + ii] * s[WF_MSFTX][(size_t)jj * nx + ii];
+  };
+  const float cfk = k == 0 ? g.cf1 : k == 1 ? g.cf2 : g.cf3;
+  const float ys = Y(j - 1, i), yc = Y(j, i), xw = Xx(j, i - 1), xc = Xx(j, i);
+  if (ys != 0.f || yc != 0.f) b[WF_V][p] += cfk * 0.5f * g.rdy * (ht[c] - ht[c - nx]) * (ys + yc);
+  if (xw != 0.f || xc != 0.f) b[WF_U][p] += cfk * 0.5f * g.rdx * (ht[c] - ht[c - 1]) * (xw + xc);
+  if (k == 0) {
+    const float* u = s[WF_U];
+    const float* v = s[WF_V];
+    auto cv = [&](size_t cc) { return g.cf1 * v[cc] + g.cf2 * v[lev + cc] + g.cf3 * v[2 * lev + cc]; };
+    auto cu = [&](size_t cc) { return g.cf1 * u[cc] + g.cf2 * u[lev + cc] + g.cf3 * u[2 * lev + cc]; };
+    const float yn = Y(j + 1, i), xe = Xx(j, i + 1);
+    float h = 0.f;
+    if (ys != 0.f) h += 0.5f * g.rdy * ys * cv(c);
+    if (yc != 0.f) h += 0.5f * g.rdy * yc * (cv(c) - cv(c + nx));
+    if (yn != 0.f) h += -0.5f * g.rdy * yn * cv(c + nx);
+    if (xw != 0.f) h += 0.5f * g.rdx * xw * cu(c);
+    if (xc != 0.f) h += 0.5f * g.rdx * xc * (cu(c) - cu(c + 1));
+    if (xe != 0.f) h += -0.5f * g.rdx * xe * cu(c + 1);
+    if (h != 0.f) b[WF_HT][c] += h;
+  }
+}
+
+int launch_advance_w(const Grid& g, const S& s, float dts, cudaStream_t st) {
+  const dim3 b2(32, 4);
+  k_advance_w<<<col_grid(g, b2), b2, 0, st>>>(g, s, dts);
+  return 1;
+}
+
+int launch_advance_w_adj(const Grid& g, const S& s, const S& b, float dts, float* work, cudaStream_t st) {
+  const dim3 b2(32, 4), b3(32, 4);
+  k_advance_w_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, dts, work);
+  k_advance_w_adj_bc<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, work);
+  return 2;
 }
 
 // stagger of a relaxed field: the bounds of relax_bdytend's zones and levels

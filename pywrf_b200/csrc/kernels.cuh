@@ -55,6 +55,8 @@ int launch_advect_scalar(const Grid& g, const S& s, const float* field, float* t
 int launch_advance_uv_adj(const Grid& g, const S& s, const S& b, float dts, cudaStream_t st);
 int launch_calc_p_rho(const Grid& g, const S& s, int step, cudaStream_t st);
 int launch_advance_mu_t(const Grid& g, const S& s, float dts, cudaStream_t st);
+int launch_advance_w(const Grid& g, const S& s, float dts, cudaStream_t st);
+int launch_advance_w_adj(const Grid& g, const S& s, const S& b, float dts, float* work, cudaStream_t st);
 int launch_advance_mu_t_adj(const Grid& g, const S& s, const S& b, float dts, int ref_no_grad, float* work,
                             cudaStream_t st);
 int launch_calc_p_rho_adj(const Grid& g, const S& s, const S& b, int step, cudaStream_t st);

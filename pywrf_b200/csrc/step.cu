@@ -555,6 +555,41 @@ constexpr int kMutCotangents[] = {WF_WW, WF_WW1, WF_U, WF_U_SAVE, WF_V, WF_V_SAV
                                   WF_MU_TEND};
 }  // namespace
 
+namespace {
+constexpr int kAwCotangents[] = {WF_W, WF_RW_TEND, WF_WW, WF_W_SAVE, WF_U, WF_V, WF_MUAVE, WF_MUTS, WF_MUT,
+                                 WF_T_2SAVE, WF_T, WF_T_SAVE, WF_PH, WF_PH_SAVE, WF_PHB, WF_PH_TEND, WF_HT, WF_C2A,
+                                 WF_CQW, WF_ALT, WF_A, WF_ALPHA, WF_GAMMA};
+constexpr int kAwOperands[] = {WF_W, WF_RW_TEND, WF_WW, WF_W_SAVE, WF_U, WF_V, WF_MUAVE, WF_MUTS, WF_MUT,
+                               WF_T_2SAVE, WF_T, WF_T_SAVE, WF_PH, WF_PH_SAVE, WF_PHB, WF_PH_TEND, WF_HT, WF_C2A,
+                               WF_CQW, WF_ALT, WF_A, WF_ALPHA, WF_GAMMA, WF_MSFTX, WF_MSFTY, WF_FNM, WF_FNP,
+                               WF_RDNW, WF_RDN};
+}  // namespace
+
+int wrf_advance_w(const WrfGrid* gin, const WrfState* sin, float dts, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s;
+  if ((rc = state_of(sin, kAwOperands, sizeof(kAwOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_advance_w(g, s, dts, static_cast<cudaStream_t>(stream));
+  return check_launch("advance_w");
+}
+
+int wrf_advance_w_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dts, float* work,
+                      void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!work) return fail(WRF_EINVAL, "advance_w_adj: null work array");
+  S s, b;
+  if ((rc = state_of(sin, kAwOperands, sizeof(kAwOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kAwCotangents, sizeof(kAwCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_advance_w_adj(g, s, b, dts, work, static_cast<cudaStream_t>(stream));
+  return check_launch("advance_w_adj");
+}
+
 int wrf_advance_mu_t(const WrfGrid* gin, const WrfState* sin, float dts, void* stream) {
   Grid g;
   int rc = make_grid(gin, g);

@@ -1,6 +1,6 @@
 """Drop-ins for ``pywrf.wrf_dynamics.advect_scalar``, ``advect_u``,
-``advect_v``, ``advect_w``, ``calc_coef_w``, ``calc_p_rho`` and
-``advance_mu_t`` (reference signatures).
+``advect_v``, ``advect_w``, ``calc_coef_w``, ``calc_p_rho``,
+``advance_mu_t`` and ``advance_w`` (reference signatures).
 
 ``advect_scalar(...)`` takes the arguments of the reference function
 (pywrf/wrf_dynamics.py:1841-1850), adds the flux-form advection of ``field``
@@ -200,3 +200,29 @@ def advance_mu_t(ww_ori, ww_1, u, u_1, v, v_1, mu_ori, mut, muave_ori, muts_ori,
         "mu_tend": mu_tend, "dnw": dnw, "fnm": fnm, "fnp": fnp, "rdnw": rdnw, "msfuy": msfuy,
         "msfvx_inv": msfvx_inv, "msftx": msftx, "msfty": msfty}, float(dts))
     return ww, ww_1, t, t_ave, uam, vam, wwam, muave, muts, mudf, mu
+
+
+def advance_w(w_ori, rw_tend, ww, w_save, u, v, mu1, mut, muave, muts, c1h, c2h, c1f, c2f, c3h, c4h, c3f, c4f,
+              t_2ave_ori, t_2, t_1, ph_ori, ph_1, phb, ph_tend, ht, c2a, cqw, alt, alb, a, alpha, gamma, rdx, rdy,
+              dts, t0, epssm, dnw, fnm, fnp, rdnw, rdn, cf1, cf2, cf3, msftx, msfty, top_lid, ids, ide, jds, jde,
+              kds, kde, ims, ime, jms, jme, kms, kme, its, ite, jts, jte, kts, kte):
+    """advance_w (pywrf/wrf_dynamics.py:3641-3796) on the GPU through
+    ``wrf_advance_w``: returns new (t_2ave, w, ph) like the reference.  mu1,
+    c1h..c4f, alb, dnw and top_lid are accepted and unused, as in the
+    reference; t0 must be the solver's 300."""
+    _frame("advance_w", w_ori.shape, ids, ide, jds, jde, its, ite, jts, jte, kts, kte)
+    if abs(float(t0) - 300.0) > 1e-9:
+        raise ValueError("advance_w: the kernels use the solver's t0 = 300")
+    nz, ny, nx = w_ori.shape
+    cg = make_cgrid(Grid.make(nx, ny, nz, 1.0 / float(rdx), 1.0 / float(rdy), 1.0),
+                    {"cf1": float(cf1), "cf2": float(cf2), "cf3": float(cf3), "cfn": 0.0, "cfn1": 0.0})
+    cg.dx, cg.dy = 1.0 / float(rdx), 1.0 / float(rdy)
+    cg.epssm = float(epssm)
+    cg.cf1, cg.cf2, cg.cf3 = float(cf1), float(cf2), float(cf3)
+    w, ph, t_2ave = w_ori.clone(), ph_ori.clone(), t_2ave_ori.clone()
+    _state_call("wrf_advance_w", cg, {
+        "w": w, "rw_tend": rw_tend, "ww": ww, "w_save": w_save, "u": u, "v": v, "muave": muave, "muts": muts,
+        "mut": mut, "t_2save": t_2ave, "t": t_2, "t_save": t_1, "ph": ph, "ph_save": ph_1, "phb": phb,
+        "ph_tend": ph_tend, "ht": ht, "c2a": c2a, "cqw": cqw, "alt": alt, "a": a, "alpha": alpha, "gamma": gamma,
+        "msftx": msftx, "msfty": msfty, "fnm": fnm, "fnp": fnp, "rdnw": rdnw, "rdn": rdn}, float(dts))
+    return t_2ave, w, ph

@@ -38,6 +38,12 @@ the returned tendency with torch autograd, and writes next to this script:
   to the inputs of the same name and give mut, mu_tend and the divergence
   nothing) and, for the operator itself, central differences of the float64
   forward along 3 seeded directions per input (``mut_direction``);
+* ``advw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.advance_w``
+  (wrf_dynamics.py:3641-3796) w.r.t. its 23 array inputs: central
+  differences of the float64 forward of L = sum(w' cot_w + ph' cot_ph +
+  t_2ave' cot_t2a) along 3 seeded directions per input (``aw_direction``);
+  the reference's autograd cannot run backward through its in-place
+  tridiagonal sweeps; the upper levels lie in the Rayleigh damping layer;
 * ``coefw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_coef_w``
   (wrf_dynamics.py:3316-3388): the reference's autograd cannot differentiate
   it (the recurrence updates ``gamma`` in place between its reads, and
@@ -285,6 +291,86 @@ def advance_mu_t(dyn, g) -> None:
     print("wrote mut_adj_ref64.npz")
 
 
+AW3 = ("w", "rw_tend", "ww", "w_save", "u", "v", "t_2ave", "t_2", "t_1", "ph", "ph_1", "phb", "ph_tend", "c2a",
+       "cqw", "alt", "a", "alpha", "gamma")
+AW2 = ("muave", "muts", "mut", "ht")
+AW_OUT = ("w", "ph", "t_2ave")
+
+
+def aw_direction(n: int, r: int, shape) -> np.ndarray:
+    """Direction r of input n (AW3 + AW2) of the advance_w finite
+    differences (regenerated by the tests, not stored)."""
+    return np.random.default_rng(10000 + 100 * n + r).standard_normal(shape)
+
+
+def advance_w(dyn, g) -> None:
+    """advance_w: central differences (advw_adj_ref64.npz)."""
+    import torch
+
+    rng = np.random.default_rng(18)
+    sh, s2 = (NZ, N, N), (N, N)
+    kk = np.arange(NZ, dtype=np.float64)[:, None, None]
+    d = {
+        "w": rng.standard_normal(sh), "rw_tend": 0.1 * rng.standard_normal(sh), "ww": 5.0 * rng.standard_normal(sh),
+        "w_save": rng.standard_normal(sh), "u": 10.0 + 3.0 * rng.standard_normal(sh),
+        "v": 3.0 * rng.standard_normal(sh), "t_2ave": 100.0 * rng.standard_normal(sh),
+        "t_2": 100.0 * rng.standard_normal(sh), "t_1": 2.0 + 5.0 * rng.standard_normal(sh),
+        "ph": 50.0 * rng.standard_normal(sh), "ph_1": 50.0 * rng.standard_normal(sh),
+        "phb": 9.81 * 1800.0 * kk + 100.0 * rng.standard_normal(sh), "ph_tend": 10.0 * rng.standard_normal(sh),
+        "c2a": 1.6e5 + 1.0e4 * rng.standard_normal(sh), "cqw": 1.0 + 0.01 * rng.standard_normal(sh),
+        "alt": 1.0 + 0.05 * rng.standard_normal(sh), "a": -0.2 * rng.random(sh), "alpha": 0.6 + 0.3 * rng.random(sh),
+        "gamma": -0.3 * rng.random(sh),
+        "muave": 100.0 * rng.standard_normal(s2), "muts": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "mut": 8.0e4 + 1.0e3 * rng.standard_normal(s2), "ht": 800.0 * rng.random(s2),
+        "msftx": 1.0 + 0.02 * rng.random(s2), "msfty": 1.0 + 0.02 * rng.random(s2),
+        "fnm": 0.45 + 0.1 * rng.random(NZ), "rdnw": -(10.0 + rng.random(NZ)), "rdn": -(10.0 + rng.random(NZ)),
+        "cot_w": rng.standard_normal(sh), "cot_ph": rng.standard_normal(sh), "cot_t2a": rng.standard_normal(sh),
+    }
+    d["fnp"] = 1.0 - d["fnm"]
+    d = {k: v.astype(np.float32) for k, v in d.items()}
+    sc = {"dts": 11.25, "epssm": 0.1, "cf1": 1.5, "cf2": -0.625, "cf3": 0.125}
+    save = dict(d)
+    save.update({k: np.array(v) for k, v in sc.items()})
+    save["dx"], save["dy"] = np.array(g.dx), np.array(g.dy)
+    one1 = torch.ones(NZ, dtype=torch.float64)
+    ids, ide, jds, jde = 5, N - 5, 5, N - 5
+
+    def run(x):
+        t2a, w, ph = dyn.advance_w(x["w"], x["rw_tend"], x["ww"], x["w_save"], x["u"], x["v"], x["muave"] * 0,
+                                   x["mut"], x["muave"], x["muts"], one1, one1 * 0, one1, one1 * 0, one1, one1 * 0,
+                                   one1, one1 * 0, x["t_2ave"], x["t_2"], x["t_1"], x["ph"], x["ph_1"], x["phb"],
+                                   x["ph_tend"], x["ht"], x["c2a"], x["cqw"], x["alt"], x["alt"], x["a"], x["alpha"],
+                                   x["gamma"], 1.0 / g.dx, 1.0 / g.dy, sc["dts"], 300.0, sc["epssm"], 1.0 / x["rdnw"],
+                                   x["fnm"], x["fnp"], x["rdnw"], x["rdn"], sc["cf1"], sc["cf2"], sc["cf3"],
+                                   x["msftx"], x["msfty"], False,
+                                   ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+        return {"w": w, "ph": ph, "t_2ave": t2a}
+
+    def loss(x):
+        o = run(x)
+        return float((o["w"] * x["cot_w"]).sum() + (o["ph"] * x["cot_ph"]).sum() + (o["t_2ave"] * x["cot_t2a"]).sum())
+
+    base = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
+    with torch.no_grad():
+        outs = run(base)
+        for o_ in AW_OUT:
+            save[f"{o_}_new"] = outs[o_].numpy()
+        for n_, name in enumerate(AW3 + AW2):
+            # L is linear in all but these inputs: there a large step is exact
+            # and keeps the cancellation in L (~1e8) out of the difference
+            rel = 1e-4 if name in ("t_1", "ph_1", "phb", "muts", "mut", "a", "alpha", "gamma") else 1e-1
+            eps = rel * float(base[name].abs().max())
+            save[f"fd_eps_{name}"] = np.array(eps)
+            for r in range(3):
+                dirn = torch.tensor(aw_direction(n_, r, d[name].shape))
+                xp, xm = dict(base), dict(base)
+                xp[name] = base[name] + eps * dirn
+                xm[name] = base[name] - eps * dirn
+                save[f"fd_{name}_{r}"] = np.array((loss(xp) - loss(xm)) / (2 * eps))
+    np.savez_compressed(os.path.join(HERE, "advw_adj_ref64.npz"), **save)
+    print("wrote advw_adj_ref64.npz")
+
+
 def mom_direction(n: int, r: int, shape) -> np.ndarray:
     """Direction r of input n (field, ru, rv, rom) of the advect_w finite
     differences (regenerated by the tests, not stored)."""
@@ -372,7 +458,7 @@ def momentum(dyn, g) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default=None)
-    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv", "calc_p_rho", "advance_mu_t"), default=None,
+    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv", "calc_p_rho", "advance_mu_t", "advance_w"), default=None,
                     help="write one fixture only")
     a = ap.parse_args()
     if a.reference:
@@ -394,6 +480,9 @@ def main() -> None:
         return
     if a.only == "advance_mu_t":
         advance_mu_t(dyn, g)
+        return
+    if a.only == "advance_w":
+        advance_w(dyn, g)
         return
     if a.only is not None:
         raise SystemExit("--only: scalar, relax and coefw are written together (no --only)")
@@ -489,6 +578,7 @@ def main() -> None:
     advance_uv(dyn, importlib_bdy(), g)
     calc_p_rho(dyn, g)
     advance_mu_t(dyn, g)
+    advance_w(dyn, g)
 
 
 def importlib_bdy():

@@ -105,8 +105,12 @@ def test_null_arguments_of_function_entry_points_are_rejected():
     assert rc == N.WRF_EINVAL
     rc = L.wrf_advance_mu_t(ctypes.byref(_cgrid()), None, ctypes.c_float(1.0), None)
     assert rc == N.WRF_EINVAL
+    rc = L.wrf_advance_w(ctypes.byref(_cgrid()), None, ctypes.c_float(1.0), None)
+    assert rc == N.WRF_EINVAL
     tab = (ctypes.c_void_p * L.wrf_field_count())()
     rc = L.wrf_advance_mu_t_adj(ctypes.byref(_cgrid()), tab, tab, ctypes.c_float(1.0), 0, None, None)
+    assert rc == N.WRF_EINVAL
+    rc = L.wrf_advance_w_adj(ctypes.byref(_cgrid()), tab, tab, ctypes.c_float(1.0), None, None)
     assert rc == N.WRF_EINVAL
     rc = L.wrf_calc_p_rho_adj(ctypes.byref(_cgrid()), (ctypes.c_void_p * L.wrf_field_count())(), None, 1, None)
     assert rc == N.WRF_EINVAL

@@ -333,3 +333,32 @@ def test_advance_mu_t_and_its_adjoint(ref_no_grad):
                 an = float((gr * _mut_dir(n, r, gr.shape)).sum())
                 fd = float(T[f"fd_{k}_{r}"])
                 assert abs(an - fd) <= 1e-4 * abs(fd), (k, r, an, fd)
+
+
+def _aw_dir(n, r, shape):
+    # the directions of make_golden_adjoint.aw_direction
+    return np.random.default_rng(10000 + 100 * n + r).standard_normal(shape)
+
+
+def test_advance_w_and_its_adjoint_against_the_reference():
+    """advance_w: t_2ave, w, ph against the reference's, and the adjoint's
+    directional derivatives against central differences of the reference's
+    float64 forward (tests/golden/advw_adj_ref64.npz; the upper levels lie in
+    the Rayleigh damping layer)."""
+    A = load_npz("advw_adj_ref64.npz")
+    inputs = {k: _cuda(A[k]).requires_grad_(True) for k in adjoint.AW_INPUTS}
+    data = {k: _cuda(A[k]) for k in adjoint.AW_DATA}
+    outs = adjoint.advance_w(inputs, data, float(A["dts"]), float(A["epssm"]), float(A["cf1"]), float(A["cf2"]),
+                             float(A["cf3"]), 1.0 / float(A["dx"]), 1.0 / float(A["dy"]))
+    for k in adjoint.AW_OUTPUTS:
+        assert rel_l2(outs[k].detach().cpu().numpy(), A[f"{k}_new"]) < 1e-6, k
+    cot = {"w": "cot_w", "ph": "cot_ph", "t_2ave": "cot_t2a"}
+    sum((outs[k] * _cuda(A[cot[k]])).sum() for k in adjoint.AW_OUTPUTS).backward()
+    names = ("w", "rw_tend", "ww", "w_save", "u", "v", "t_2ave", "t_2", "t_1", "ph", "ph_1", "phb", "ph_tend",
+             "c2a", "cqw", "alt", "a", "alpha", "gamma", "muave", "muts", "mut", "ht")
+    for n, k in enumerate(names):
+        gr = inputs[k].grad.double().cpu().numpy()
+        for r in range(3):
+            an = float((gr * _aw_dir(n, r, gr.shape)).sum())
+            fd = float(A[f"fd_{k}_{r}"])
+            assert abs(an - fd) <= 1e-4 * abs(fd), (k, r, an, fd)

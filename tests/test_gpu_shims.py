@@ -199,3 +199,26 @@ def test_advance_mu_t_shim_with_the_solver_arguments():
         assert rel_l2(mine.cpu().numpy(), T[f"{nm}_new"]) < 1e-6, nm
     # the inputs are left as they were (the reference clones them)
     assert torch.equal(t["ww"], _c(T["ww"])) and torch.equal(t["mu"], _c(T["mu"]))
+
+
+def test_advance_w_shim_with_the_solver_arguments():
+    """advance_w called with the reference's argument list against the
+    reference's own outputs (tests/golden/advw_adj_ref64.npz)."""
+    from helpers import load_npz
+
+    A = load_npz("advw_adj_ref64.npz")
+    nz, n = A["w"].shape[0], A["w"].shape[1]
+    one1 = torch.ones(nz, device="cuda")
+    t = {k: _c(A[k]) for k in A if not k.startswith(("cot_", "fd_")) and not k.endswith("_new")
+         and np.asarray(A[k]).ndim > 0}
+    t2a, w, ph = wrf_dynamics.advance_w(t["w"], t["rw_tend"], t["ww"], t["w_save"], t["u"], t["v"], t["muave"] * 0,
+                                        t["mut"], t["muave"], t["muts"], one1, one1 * 0, one1, one1 * 0, one1,
+                                        one1 * 0, one1, one1 * 0, t["t_2ave"], t["t_2"], t["t_1"], t["ph"],
+                                        t["ph_1"], t["phb"], t["ph_tend"], t["ht"], t["c2a"], t["cqw"], t["alt"],
+                                        t["alt"], t["a"], t["alpha"], t["gamma"], 1.0 / float(A["dx"]),
+                                        1.0 / float(A["dy"]), float(A["dts"]), 300.0, float(A["epssm"]),
+                                        1.0 / t["rdnw"], t["fnm"], t["fnp"], t["rdnw"], t["rdn"], float(A["cf1"]),
+                                        float(A["cf2"]), float(A["cf3"]), t["msftx"], t["msfty"], False,
+                                        5, n - 5, 5, n - 5, 0, nz, 0, n, 0, n, 0, nz, 5, n - 5, 5, n - 5, 0, nz)
+    for nm, mine in (("t_2ave", t2a), ("w", w), ("ph", ph)):
+        assert rel_l2(mine.cpu().numpy(), A[f"{nm}_new"]) < 1e-6, nm

@@ -296,3 +296,54 @@ def test_advance_mu_t_fixture_pinned_by_the_oracle():
         fd = (loss(xp) - loss(xm)) / (2 * eps)
         ref = float(T[f"fd_{name}_0"])
         assert abs(fd - ref) <= 1e-6 * abs(ref) + 1e-9, (name, fd, ref)
+
+
+AWZ = load_npz("advw_adj_ref64.npz")
+AW3 = ("w", "rw_tend", "ww", "w_save", "u", "v", "t_2ave", "t_2", "t_1", "ph", "ph_1", "phb", "ph_tend", "c2a",
+       "cqw", "alt", "a", "alpha", "gamma")
+AW2 = ("muave", "muts", "mut", "ht")
+AW_OUT = ("w", "ph", "t_2ave")
+_AW_ST = {"t_2ave": "t_2save", "t_2": "t", "t_1": "t_save", "ph_1": "ph_save"}
+
+
+def _aw_dir(n, r, shape):
+    # the directions of make_golden_adjoint.aw_direction
+    return np.random.default_rng(10000 + 100 * n + r).standard_normal(shape)
+
+
+def _advance_w(g, x):
+    st = {_AW_ST.get(k, k): np.array(v, np.float64) for k, v in x.items()}
+    for k in ("msftx", "msfty", "fnm", "fnp", "rdnw", "rdn"):
+        st[k] = AWZ[k].astype(np.float64)
+    OD.advance_w(g, st, float(AWZ["dts"]), float(AWZ["epssm"]), float(AWZ["cf1"]), float(AWZ["cf2"]),
+                 float(AWZ["cf3"]))
+    return {o: st[_AW_ST.get(o, o)] for o in AW_OUT}
+
+
+def test_advance_w_fixture_pinned_by_the_oracle():
+    """advance_w: the oracle reproduces the reference's w, ph, t_2ave on the
+    fixture, and its central differences equal the fixture's (of the
+    reference's float64 forward)."""
+    g = _grid()
+    base = {k: AWZ[k].astype(np.float64) for k in AW3 + AW2}
+    outs = _advance_w(g, base)
+    for o in AW_OUT:
+        ref = AWZ[f"{o}_new"]
+        assert np.abs(outs[o] - ref).max() <= 1e-12 * np.abs(ref).max(), o
+    cot = {"w": AWZ["cot_w"], "ph": AWZ["cot_ph"], "t_2ave": AWZ["cot_t2a"]}
+
+    def loss(x):
+        out = _advance_w(g, x)
+        return sum(float((out[o] * cot[o].astype(np.float64)).sum()) for o in AW_OUT)
+
+    for n, name in enumerate(AW3 + AW2):
+        d = _aw_dir(n, 0, base[name].shape)
+        eps = float(AWZ[f"fd_eps_{name}"])  # the fixture's step
+        xp, xm = dict(base), dict(base)
+        xp[name] = base[name] + eps * d
+        xm[name] = base[name] - eps * d
+        fd = (loss(xp) - loss(xm)) / (2 * eps)
+        ref = float(AWZ[f"fd_{name}_0"])
+        # the two float64 forwards round differently (~1e-13 relative), which
+        # the finite difference magnifies by |L| / (eps |dL|)
+        assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-9, (name, fd, ref)
