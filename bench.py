@@ -341,9 +341,10 @@ def run_ours(a):
                 "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan,
                 "surrogate": sur,
                 "adjoint": {"unavailable": "no whole-step adjoint yet: hand-written reverse-mode kernels exist for "
-                                           "advect_scalar, advect_u/v/w, relax_bdytend, advance_uv, advance_mu_t, calc_p_rho, "
-                                           "calc_coef_w and the implicit w solve (pywrf_b200.adjoint), not for "
-                                           "the step they compose"}}
+                                           "advect_scalar, advect_u/v/w, relax_bdytend and the acoustic substep's "
+                                           "advance_uv, advance_mu_t, calc_coef_w, advance_w (implicit solve "
+                                           "included) and calc_p_rho (pywrf_b200.adjoint), not yet for the "
+                                           "forces, moisture, WSM6 or the step they compose"}}
         print(json.dumps(line), flush=True)
     it._graph = None
     if world > 1:
