@@ -33,6 +33,10 @@ operators keeps no tape of the forward's intermediates.
 * :class:`CoefW` -- calc_coef_w (pywrf/wrf_dynamics.py:3316-3388): the
   implicit solve's coefficients a, alpha, gamma from mut, cqw, c2a;
   gradients with respect to those three.
+* :func:`rollout` -- truncated backpropagation through ``n_steps`` of a
+  step made of these operators with per-step (or per-segment) checkpointing:
+  only each segment's input state is kept, and the backward pass recomputes
+  the segment's forward once before back-propagating through it.
 * :class:`VSolveW` -- the vertically implicit w solve of advance_w
   (pywrf/wrf_dynamics.py:3761-3767); gradients with respect to the
   right-hand side and the coefficients a, alpha, gamma (the transposed solve).
@@ -40,8 +44,10 @@ operators keeps no tape of the forward's intermediates.
 from __future__ import annotations
 
 import ctypes
+from typing import Callable, Sequence
 
 import torch
+from torch.utils.checkpoint import checkpoint
 
 from . import _native as N
 from .config import Grid
@@ -475,3 +481,34 @@ class CoefW(torch.autograd.Function):
 def coef_w(mut, cqw, c2a, rdn, rdnw, dts, epssm=0.1, top_lid=False, rdx=1.0 / 9000.0, rdy=1.0 / 9000.0):
     """Differentiable calc_coef_w: returns (a, alpha, gamma)."""
     return CoefW.apply(mut, cqw, c2a, rdn, rdnw, dts, epssm, top_lid, rdx, rdy)
+
+
+def rollout(step: Callable[..., Sequence[torch.Tensor]], state: Sequence[torch.Tensor], n_steps: int,
+            every: int = 1) -> tuple[torch.Tensor, ...]:
+    """Apply ``state = step(*state)`` ``n_steps`` times, differentiably, with
+    checkpoints every ``every`` steps: the forward keeps only the state at
+    the start of each segment (plus whatever ``step`` closes over, e.g.
+    learnable parameters, which receive their gradients as usual); the
+    backward recomputes each segment's forward once, with its operators'
+    hand-written adjoints recording what they need, and back-propagates
+    through it.  Peak memory is then one segment's intermediates plus
+    n_steps / every states, instead of every intermediate of every step.
+    ``every=0`` keeps the whole forward (no recomputation)."""
+    if n_steps < 0 or every < 0:
+        raise ValueError("n_steps and every must be >= 0")
+    state = tuple(state)
+
+    def segment(k, *xs):
+        for _ in range(k):
+            xs = tuple(step(*xs))
+        return xs
+
+    done = 0
+    while done < n_steps:
+        k = n_steps - done if every == 0 else min(every, n_steps - done)
+        if every == 0 or not torch.is_grad_enabled():
+            state = segment(k, *state)
+        else:
+            state = tuple(checkpoint(segment, k, *state, use_reentrant=False))
+        done += k
+    return state

@@ -61,3 +61,60 @@ def test_grid_validation():
         Grid.make(20, 28, 16, 9000.0, 9000.0, 45.0)
     with pytest.raises(ValueError):
         Grid.make(28, 28, 8, 9000.0, 9000.0, 45.0)
+
+
+def test_rollout_checkpointing_gives_the_taped_gradient_with_bounded_memory():
+    """pywrf_b200.adjoint.rollout: truncated backpropagation through n steps
+    of a nonlinear step with a learnable bias (the shape of the config-3
+    problem) gives the same gradients with per-step and per-segment
+    checkpoints as the fully taped rollout, runs each step's forward once
+    more in the backward, and keeps only the segments' input states for the
+    backward (the taped rollout keeps every saved operand of every step)."""
+    import torch
+
+    from pywrf_b200.adjoint import rollout
+
+    g = torch.Generator().manual_seed(5)
+    x0 = torch.randn(6, 8, 8, generator=g, dtype=torch.float64)
+    y0 = torch.randn(6, 8, 8, generator=g, dtype=torch.float64)
+    target = torch.randn(6, 8, 8, generator=g, dtype=torch.float64)
+    calls = {"n": 0}
+
+    def make_step(bias):
+        def step(x, y):
+            calls["n"] += 1
+            lap = torch.roll(x, 1, -1) + torch.roll(x, -1, -1) + torch.roll(x, 1, -2) + torch.roll(x, -1, -2) - 4 * x
+            t = torch.tanh(y) * torch.sin(x)
+            x1 = x + 0.1 * lap + 0.05 * t * torch.exp(-0.1 * x * x) + bias
+            y1 = y - 0.05 * x1 * torch.tanh(y * x1)
+            return x1, y1
+        return step
+
+    n = 12
+    grads, kept = {}, {}
+    for every in (0, 1, 4):
+        bias = torch.zeros(6, 8, 8, dtype=torch.float64, requires_grad=True)
+        xs = x0.clone().requires_grad_(True)
+        calls["n"] = 0
+        count = {"n": 0}
+
+        def pack(t):
+            count["n"] += t.numel()
+            return t
+
+        with torch.autograd.graph.saved_tensors_hooks(pack, lambda t: t):
+            x, y = rollout(make_step(bias), (xs, y0), n, every=every)
+        kept[every] = count["n"]
+        assert calls["n"] == n
+        loss = ((x[:3] - target[:3]) ** 2).mean() + ((y[:3] - target[:3]) ** 2).mean()
+        loss.backward()
+        assert calls["n"] == (n if every == 0 else 2 * n)  # one recomputation per step
+        grads[every] = (bias.grad.clone(), xs.grad.clone())
+    for every in (1, 4):
+        for a, b in zip(grads[every], grads[0]):
+            assert torch.allclose(a, b, rtol=1e-12, atol=1e-14)
+    # elements held for the backward: every saved operand of every step when
+    # taped, the two input states per segment when checkpointed
+    state = x0.numel()
+    assert kept[1] == 2 * state * n and kept[4] == 2 * state * (n // 4)
+    assert kept[0] > 4 * kept[1]
