@@ -33,13 +33,13 @@ operators keeps no tape of the forward's intermediates.
 * :class:`CoefW` -- calc_coef_w (pywrf/wrf_dynamics.py:3316-3388): the
   implicit solve's coefficients a, alpha, gamma from mut, cqw, c2a;
   gradients with respect to those three.
+* :class:`VSolveW` -- the vertically implicit w solve of advance_w
+  (pywrf/wrf_dynamics.py:3761-3767); gradients with respect to the
+  right-hand side and the coefficients a, alpha, gamma (the transposed solve).
 * :func:`rollout` -- truncated backpropagation through ``n_steps`` of a
   step made of these operators with per-step (or per-segment) checkpointing:
   only each segment's input state is kept, and the backward pass recomputes
   the segment's forward once before back-propagating through it.
-* :class:`VSolveW` -- the vertically implicit w solve of advance_w
-  (pywrf/wrf_dynamics.py:3761-3767); gradients with respect to the
-  right-hand side and the coefficients a, alpha, gamma (the transposed solve).
 """
 from __future__ import annotations
 
@@ -60,6 +60,14 @@ def _ptr(t: torch.Tensor) -> ctypes.c_void_p:
     return ctypes.c_void_p(t.data_ptr())
 
 
+def _cuda_only(*ts) -> None:
+    """Refuse anything but contiguous float32 CUDA tensors before any
+    library or stream call (None entries are optional operands)."""
+    for t in ts:
+        if t is not None:
+            _ptr(t)
+
+
 def scalar_grid(shape, rdx: float, rdy: float):
     """The C grid record of the solver's 5-cell frame for a field of ``shape``."""
     nz, ny, nx = shape
@@ -75,6 +83,7 @@ class AdvectScalar(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, field, tendency, ru, rv, rom, msftx, fnm, fnp, rdnw, rdx: float, rdy: float):
+        _cuda_only(field, tendency, ru, rv, rom, msftx, fnm, fnp, rdnw)
         cg = scalar_grid(field.shape, rdx, rdy)
         out = tendency.detach().clone()
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -112,6 +121,7 @@ class AdvectMomentum(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, component: int, field, tendency, ru, rv, rom, msf, msf2, fzm, fzp, rdz, rdx: float, rdy: float):
+        _cuda_only(field, tendency, ru, rv, rom, msf, msf2, fzm, fzp, rdz)
         if component not in (0, 1, 2):
             raise ValueError("component must be 0 (u), 1 (v) or 2 (w)")
         if component == 1 and msf2 is None:
@@ -170,6 +180,7 @@ class AdvanceUV(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        _cuda_only(*tensors)
         dts, emdiv, cf1, cf2, cf3, rdx, rdy = (float(x) for x in scal)
         named = dict(zip(UV_INPUTS + UV_DATA, tensors))
         cg = scalar_grid(named["u"].shape, rdx, rdy)
@@ -220,6 +231,7 @@ class AdvanceW(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        _cuda_only(*tensors)
         dts, epssm, cf1, cf2, cf3, rdx, rdy = (float(x) for x in scal)
         named = dict(zip(AW_INPUTS + AW_DATA, tensors))
         cg = scalar_grid(named["w"].shape, rdx, rdy)
@@ -276,6 +288,7 @@ class AdvanceMuT(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        _cuda_only(*tensors)
         dts, epssm, rdx, rdy = (float(x) for x in scal[:4])
         named = dict(zip(MUT_INPUTS + MUT_DATA, tensors))
         cg = scalar_grid(named["ww"].shape, rdx, rdy)
@@ -330,6 +343,7 @@ class CalcPRho(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        _cuda_only(*tensors)
         smdiv, step, rdx, rdy = float(scal[0]), int(scal[1]), float(scal[2]), float(scal[3])
         named = dict(zip(PRHO_INPUTS + ("rdnw",), tensors))
         cg = scalar_grid(named["p"].shape, rdx, rdy)
@@ -376,6 +390,7 @@ class RelaxBdytend(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, field, tendency, variable: str, dtbc: float, *bdy8):
+        _cuda_only(field, tendency, *bdy8)
         nz, ny, nx = field.shape
         cg = scalar_grid(field.shape, 1.0 / 9000.0, 1.0 / 9000.0)
         out = tendency.detach().clone()
@@ -413,6 +428,7 @@ class VSolveW(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, x, a, alpha, gamma):
+        _cuda_only(x, a, alpha, gamma)
         nz = x.shape[0]
         ncol = x.numel() // nz
         w = torch.empty_like(x)
@@ -448,6 +464,7 @@ class CoefW(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, mut, cqw, c2a, rdn, rdnw, dts: float, epssm: float, top_lid: bool, rdx: float, rdy: float):
+        _cuda_only(mut, cqw, c2a, rdn, rdnw)
         cg = scalar_grid(cqw.shape, rdx, rdy)
         cg.epssm = float(epssm)
         cg.top_lid = int(bool(top_lid))

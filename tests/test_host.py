@@ -118,3 +118,38 @@ def test_rollout_checkpointing_gives_the_taped_gradient_with_bounded_memory():
     state = x0.numel()
     assert kept[1] == 2 * state * n and kept[4] == 2 * state * (n // 4)
     assert kept[0] > 4 * kept[1]
+
+
+def test_adjoint_operators_refuse_cpu_tensors():
+    """Every differentiable operator fails loudly on CPU tensors: there is no
+    CPU path (the check runs before any library call)."""
+    import pytest
+    import torch
+
+    from pywrf_b200 import adjoint
+
+    z3 = torch.zeros(12, 24, 24)
+    z2 = torch.zeros(24, 24)
+    z1 = torch.zeros(12)
+    with pytest.raises(TypeError):
+        adjoint.advect_scalar(z3, z3, z3, z3, z3, z2, z1, z1, z1, 1e-4, 1e-4)
+    with pytest.raises(TypeError):
+        adjoint.advect_momentum(0, z3, z3, z3, z3, z3, z2, None, z1, z1, z1, 1e-4, 1e-4)
+    with pytest.raises(TypeError):
+        adjoint.vsolve_w(z3, z3, z3, z3)
+    uv = {k: (z2 if k in ("mu", "muu", "muv", "mudf") else z3) for k in adjoint.UV_INPUTS}
+    uvd = {k: (z1 if k in ("fnm", "fnp", "rdnw") else z2) for k in adjoint.UV_DATA}
+    with pytest.raises(TypeError):
+        adjoint.advance_uv(uv, uvd, 1.0, 0.01, 1.5, -0.6, 0.1, 1e-4, 1e-4)
+    pr = {k: (z2 if k in ("mu", "mut") else z3) for k in adjoint.PRHO_INPUTS}
+    with pytest.raises(TypeError):
+        adjoint.calc_p_rho(pr, z1, 0.1, 1)
+    mt = {k: (z2 if k in ("mu", "mut", "muave", "muts", "muu", "muv", "mudf", "mu_tend") else z3)
+          for k in adjoint.MUT_INPUTS}
+    mtd = {k: (z1 if k in ("dnw", "fnm", "fnp", "rdnw") else z2) for k in adjoint.MUT_DATA}
+    with pytest.raises(TypeError):
+        adjoint.advance_mu_t(mt, mtd, 1.0, 0.1)
+    aw = {k: (z2 if k in ("muave", "muts", "mut", "ht") else z3) for k in adjoint.AW_INPUTS}
+    awd = {k: (z1 if k in ("fnm", "fnp", "rdnw", "rdn") else z2) for k in adjoint.AW_DATA}
+    with pytest.raises(TypeError):
+        adjoint.advance_w(aw, awd, 1.0, 0.1, 1.5, -0.6, 0.1)
