@@ -7,7 +7,10 @@ the reference), runs ``nsteps`` ARW time steps and returns the final
 ``{"u", "v", "w", "t", "ph", "mu", "moist"}`` tensors in the reference's
 halo-frame layout.  The step itself is :class:`Integrator.step`, one call of
 ``wrf_rk3_step`` (include/pywrf_b200.h), optionally replayed from a CUDA
-graph; nothing of it runs on the CPU.
+graph; nothing of it runs on the CPU.  Every ``bdy_interval`` steps the
+boundary arrays are reloaded from the next record of the boundary file, as
+the reference's loop does (:func:`bdy_schedule`); the boundary time within
+an interval is kept on the device.
 """
 from __future__ import annotations
 
@@ -20,7 +23,7 @@ import torch
 
 from . import _native as N
 from .config import Grid
-from .state import DeviceState, grid_from_inputs
+from .state import DeviceState, grid_from_inputs, ingest_bdy
 
 # run parameters of the reference configuration (pywrf/config_params.py:41-72)
 DEFAULTS = dict(dx=9000.0, dy=9000.0, dt=60.0, p_top=1000.0, soundsteps=4, bdy_interval=360, nsteps=720)
@@ -110,6 +113,41 @@ class Integrator:
         return {"nan_p": out[N.WRF_ST_NAN_P], "step": out[N.WRF_ST_STEP], "wait_timeouts": out[N.WRF_ST_WAIT]}
 
 
+def bdy_schedule(nsteps: int, bdy_interval: int) -> list[tuple[int | None, int]]:
+    """The lateral-boundary records the reference's time loop loads, as
+    segments ``(record, steps)``: before step t with ``t % bdy_interval == 1``
+    the reference reloads every boundary array from record ``t //
+    bdy_interval`` of the boundary file (pywrf/solver.py:457-703); the first
+    segment's record (0) is the one the state was built with (None: nothing
+    to load)."""
+    if nsteps < 0 or bdy_interval < 1:
+        raise ValueError("nsteps >= 0 and bdy_interval >= 1 are required")
+
+    def reload_at(t: int) -> bool:
+        return t > 1 and bdy_interval > 1 and t % bdy_interval == 1
+
+    segs: list[tuple[int | None, int]] = []
+    t = 1
+    while t <= nsteps:
+        end = t
+        while end < nsteps and not reload_at(end + 1):
+            end += 1
+        segs.append((t // bdy_interval if reload_at(t) else None, end - t + 1))
+        t = end + 1
+    return segs
+
+
+def run_with_boundary_records(it, g, bdy, nsteps: int, graph: bool = True) -> None:
+    """Advance ``it`` (an :class:`Integrator`) by ``nsteps`` steps, loading
+    the boundary record of each segment of :func:`bdy_schedule` into the
+    state's boundary arrays in place (same storage, so a captured graph
+    stays valid) before the segment's steps."""
+    for rec, n in bdy_schedule(nsteps, g.bdy_interval):
+        if rec is not None:
+            it.state.load(ingest_bdy(g, bdy, rec))
+        it.run(n, graph=graph)
+
+
 class WrfSolver:
     """Orchestrate one WRF run on the GPU (same call pattern as the reference:
     construct, then :meth:`solve`)."""
@@ -154,6 +192,7 @@ class WrfSolver:
     def prepare(self) -> Integrator:
         wrfinput, wrfbdy, _ = self._load_datasets()
         inputs, bdy = self._arrays(wrfinput), self._arrays(wrfbdy)
+        self._bdy = bdy
         p = self.params
         g = grid_from_inputs(inputs, p["dx"], p["dy"], p["dt"], p["p_top"], p["soundsteps"], p["bdy_interval"])
         state = DeviceState.from_inputs(g, inputs, bdy, device=self.device)
@@ -163,7 +202,7 @@ class WrfSolver:
     def solve(self):
         """Integrate ``nsteps`` steps; returns the final key fields."""
         it = self.prepare()
-        it.run(self.nsteps, graph=self.graph)
+        run_with_boundary_records(it, it.state.g, self._bdy, self.nsteps, graph=self.graph)
         st = it.status()
         if st["nan_p"]:
             raise FloatingPointError(f"NaN in the diagnosed pressure ({st['nan_p']} stage(s)) by step {st['step']}")

@@ -153,3 +153,66 @@ def test_adjoint_operators_refuse_cpu_tensors():
     awd = {k: (z1 if k in ("fnm", "fnp", "rdnw", "rdn") else z2) for k in adjoint.AW_DATA}
     with pytest.raises(TypeError):
         adjoint.advance_w(aw, awd, 1.0, 0.1, 1.5, -0.6, 0.1)
+
+
+def test_boundary_record_schedule_follows_the_reference_loop():
+    """bdy_schedule reproduces the reference's reload rule (pywrf/solver.py:
+    457-458: before step t with t % bdy_interval == 1, record
+    t // bdy_interval), and run_with_boundary_records loads each record into
+    the state in place before that step."""
+    from pywrf_b200.solver import bdy_schedule, run_with_boundary_records
+
+    for nsteps in (0, 1, 5, 359, 360, 361, 720, 721, 1000):
+        for bi in (1, 2, 7, 360):
+            # step by step as the reference's loop does it
+            want, cur = [], None
+            for t in range(1, nsteps + 1):
+                if t % bi == 1 and t > 1:
+                    cur = t // bi
+                    want.append((t, cur))
+            segs = bdy_schedule(nsteps, bi)
+            assert sum(n for _, n in segs) == nsteps
+            got, t = [], 1
+            for rec, n in segs:
+                if rec is not None:
+                    got.append((t, rec))
+                t += n
+            assert got == want, (nsteps, bi)
+
+    class FakeState:
+        def __init__(self):
+            self.loaded = []
+
+        def load(self, host):
+            self.loaded.append(sorted(host)[0])
+
+    class FakeIt:
+        def __init__(self):
+            self.state, self.steps, self.log = FakeState(), 0, []
+
+        def run(self, n, graph=True):
+            self.log.append((self.steps + 1, len(self.state.loaded)))
+            self.steps += n
+
+    import numpy as np
+
+    from pywrf_b200 import synthetic
+    from pywrf_b200.state import BDY_FIELDS, _BDY_WRF
+
+    spec = synthetic.CaseSpec(n=24, nz=12)
+    g = synthetic.grid_for(spec)
+    g = type(g)(**{**g.__dict__, "bdy_interval": 4})
+    bdy = {}
+    for fld in BDY_FIELDS:
+        W = _BDY_WRF[fld]
+        nk = g.nz if fld == "ph" else (1 if fld == "mu" else g.nz - 1)
+        nj = g.ny - 10 if fld == "v" else g.ny - 11
+        ni = g.nx - 10 if fld == "u" else g.nx - 11
+        for pre in ("B", "BT"):
+            for side, n_ in (("XS", nj), ("XE", nj), ("YS", ni), ("YE", ni)):
+                shape = (3, 5, n_) if fld == "mu" else (3, 5, nk, n_)
+                bdy[f"{W}_{pre}{side}"] = np.zeros(shape, np.float32)
+    it = FakeIt()
+    run_with_boundary_records(it, g, bdy, 10)
+    # steps 1-4 on record 0, record 1 loaded before step 5, record 2 before step 9
+    assert it.log == [(1, 0), (5, 1), (9, 2)] and it.steps == 10
