@@ -151,6 +151,7 @@ class OracleModel:
     def __init__(self, g, inputs, bdy, dtype=np.float32):
         self.g = g
         self.dtype = dtype
+        self.bdy_src = bdy
         self.st = ingest(g, inputs, bdy, dtype)
         self.step_count = 0
 
@@ -175,6 +176,11 @@ class OracleModel:
         bd = s["bdy"]
         if t_big_step % g.bdy_interval == 1:
             self.it_bdy = int(t_big_step / g.bdy_interval)
+            # solver.py:457-703: every boundary array from record it_bdy
+            # (record 0 at step 1 is the one ingested)
+            if t_big_step > 1:
+                s["bdy"] = ingest_bdy(g, self.bdy_src, self.it_bdy, self.dtype)
+                bd = s["bdy"]
         self.it_bdy = getattr(self, "it_bdy", 0)
         dt = g.dt
         dts = dt / g.soundsteps

@@ -11,6 +11,10 @@ Writes, next to this script:
   values per field after 3 steps of configuration 0 (64x64x41) in float64.
 * ``c1_ref64_summary.json``: the same after 1 step of the 240x240x41
   configuration with boundary tendencies.
+* ``small_bdyrec_ref64.npz``: u, v, t, ph, mu, qv after 4 steps of the
+  28x28x16 case with a boundary interval of 2 steps and three distinct
+  boundary records (``bdy_records``), so that step 3 runs on record 1 after
+  the reference's reload (solver.py:457-703), in float64.
 
 The reference is read from its source tree (default /root/reference); this
 script is the only producer of the fixtures and is never run by the tests.
@@ -54,14 +58,47 @@ def summary(res, nsample=64, seed=0):
     return out
 
 
+def bdy_records(bdy, n=3):
+    """Boundary data with ``n`` distinct records: record r scales the values
+    by 1 + 0.002 r and the tendencies by 1 + 0.5 r."""
+    out = {}
+    for k, v in bdy.items():
+        v = np.asarray(v)
+        ten = "_BT" in k
+        out[k] = np.stack([v[0] * ((1.0 + 0.5 * r) if ten else (1.0 + 0.002 * r)) for r in range(n)]).astype(v.dtype)
+    return out
+
+
+BDYREC = dict(nsteps=4, bdy_interval=2)
+
+
+def bdyrec_case():
+    import dataclasses
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = dataclasses.replace(synthetic.grid_for(spec), bdy_interval=BDYREC["bdy_interval"])
+    inp, bdy = synthetic.build(spec)
+    return g, inp, bdy_records(bdy)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("PYWRF_REFERENCE_ROOT", "/root/reference"))
     ap.add_argument("--skip-c1", action="store_true")
+    ap.add_argument("--only-bdyrec", action="store_true", help="write small_bdyrec_ref64.npz only")
     args = ap.parse_args()
     os.environ["PYWRF_REFERENCE_ROOT"] = args.reference
     import refharness
     refharness.REF_ROOT = args.reference
+
+    g, inp, bdy = bdyrec_case()
+    res = refharness.run_reference(g, inp, bdy, BDYREC["nsteps"], dtype="float64")
+    keep = {k: np.asarray(v, "float64") for k, v in pick(res).items() if k in ("u", "v", "t", "ph", "mu", "qv")}
+    np.savez_compressed(os.path.join(HERE, "small_bdyrec_ref64.npz"), meta=json.dumps(
+        {"case": SMALL, **BDYREC, "solver_sha256": refharness.SOLVER_SHA256}), **keep)
+    print("wrote small_bdyrec")
+    if args.only_bdyrec:
+        return
 
     spec = synthetic.CaseSpec(**SMALL)
     g = synthetic.grid_for(spec)

@@ -89,7 +89,7 @@ def load_reference(grid, dtype="float32", device="cpu"):
                 ime=n, jme=n, kde=nz, kte=nz, kpe=nz, kme=nz, dx=grid.dx, dy=grid.dy,
                 rdx=1.0 / grid.dx, rdy=1.0 / grid.dy, dxdy=grid.dx, dt=grid.dt,
                 time_step=int(grid.dt), p_top=grid.p_top, soundsteps=grid.soundsteps,
-                device=torch.device(device))
+                bdy_interval=grid.bdy_interval, device=torch.device(device))
     for k, v in over.items():
         setattr(cp, k, v)
     dyn = importlib.import_module("pywrf.wrf_dynamics")

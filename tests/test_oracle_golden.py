@@ -67,3 +67,36 @@ def test_golden_fixtures_are_self_consistent():
     for k in r64:
         assert np.isfinite(r64[k]).sum() > 0.9 * r64[k].size, k
         assert rel_l2(r32[k], r64[k]) < 1e-3, k
+
+
+def _bdy_records(bdy, n=3):
+    # the records of make_golden.bdy_records: record r scales the values by
+    # 1 + 0.002 r and the tendencies by 1 + 0.5 r
+    return {k: np.stack([np.asarray(v)[0] * ((1.0 + 0.5 * r) if "_BT" in k else (1.0 + 0.002 * r))
+                         for r in range(n)]).astype(np.asarray(v).dtype) for k, v in bdy.items()}
+
+
+def test_oracle64_reloads_boundary_records_as_the_reference():
+    """With a boundary interval of 2 steps and three distinct records, the
+    reference reloads every boundary array from record 1 before step 3
+    (solver.py:457-703); the oracle, doing the same, matches its fields after
+    4 steps, and a run that keeps record 0 does not."""
+    import dataclasses
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = dataclasses.replace(synthetic.grid_for(spec), bdy_interval=2)
+    inputs, bdy = synthetic.build(spec)
+    ref = load_npz("small_bdyrec_ref64.npz")
+    m = OracleModel(g, inputs, _bdy_records(bdy), np.float64)
+    m.run(4)
+    out = pick(lambda k: m.st[k])
+    # 4 float64 steps: 1e-9 .. 7e-8 (mu) from the reference's operation order
+    for k in ("u", "v", "t", "ph", "mu", "qv"):
+        assert rel_l2(out[k], ref[k]) < 1e-6, k
+    # the fixture sees the reload: the same run on record 0 throughout is off
+    # by 3e-3 .. 4e-2
+    same = {k: np.stack([np.asarray(v)[0]] * 3) for k, v in _bdy_records(bdy).items()}
+    m0 = OracleModel(g, inputs, same, np.float64)
+    m0.run(4)
+    for k in ("u", "mu"):
+        assert rel_l2(pick(lambda kk: m0.st[kk])[k], ref[k]) > 1e-3, k
