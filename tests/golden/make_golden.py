@@ -11,10 +11,11 @@ Writes, next to this script:
   values per field after 3 steps of configuration 0 (64x64x41) in float64.
 * ``c1_ref64_summary.json``: the same after 1 step of the 240x240x41
   configuration with boundary tendencies.
-* ``small_bdyrec_ref64.npz``: u, v, t, ph, mu, qv after 4 steps of the
-  28x28x16 case with a boundary interval of 2 steps and three distinct
-  boundary records (``bdy_records``), so that step 3 runs on record 1 after
-  the reference's reload (solver.py:457-703), in float64.
+* ``small_bdyrec_ref64.npz`` / ``small_bdyrec_ref32.npz``: u, v, t, ph, mu,
+  qv after 4 steps of the 28x28x16 case with a boundary interval of 2 steps
+  and three distinct boundary records (``bdy_records``), so that step 3 runs
+  on record 1 after the reference's reload (solver.py:457-703), in float64
+  and float32.
 
 The reference is read from its source tree (default /root/reference); this
 script is the only producer of the fixtures and is never run by the tests.
@@ -92,11 +93,12 @@ def main():
     refharness.REF_ROOT = args.reference
 
     g, inp, bdy = bdyrec_case()
-    res = refharness.run_reference(g, inp, bdy, BDYREC["nsteps"], dtype="float64")
-    keep = {k: np.asarray(v, "float64") for k, v in pick(res).items() if k in ("u", "v", "t", "ph", "mu", "qv")}
-    np.savez_compressed(os.path.join(HERE, "small_bdyrec_ref64.npz"), meta=json.dumps(
-        {"case": SMALL, **BDYREC, "solver_sha256": refharness.SOLVER_SHA256}), **keep)
-    print("wrote small_bdyrec")
+    for dt in ("float64", "float32"):
+        res = refharness.run_reference(g, inp, bdy, BDYREC["nsteps"], dtype=dt)
+        keep = {k: np.asarray(v, dt) for k, v in pick(res).items() if k in ("u", "v", "t", "ph", "mu", "qv")}
+        np.savez_compressed(os.path.join(HERE, f"small_bdyrec_ref{dt[-2:]}.npz"), meta=json.dumps(
+            {"case": SMALL, **BDYREC, "solver_sha256": refharness.SOLVER_SHA256}), **keep)
+        print("wrote small_bdyrec", dt)
     if args.only_bdyrec:
         return
 

@@ -100,3 +100,20 @@ def test_oracle64_reloads_boundary_records_as_the_reference():
     m0.run(4)
     for k in ("u", "mu"):
         assert rel_l2(pick(lambda kk: m0.st[kk])[k], ref[k]) > 1e-3, k
+
+
+def test_oracle32_reloads_boundary_records_within_reference_fp32_error():
+    """The float32 oracle on the boundary-record case stays within the
+    reference's own float32 error (against its float64 run)."""
+    import dataclasses
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = dataclasses.replace(synthetic.grid_for(spec), bdy_interval=2)
+    inputs, bdy = synthetic.build(spec)
+    r64, r32 = load_npz("small_bdyrec_ref64.npz"), load_npz("small_bdyrec_ref32.npz")
+    m = OracleModel(g, inputs, _bdy_records(bdy), np.float32)
+    m.run(4)
+    out = pick(lambda k: m.st[k])
+    for k in ("u", "v", "t", "ph", "mu", "qv"):
+        floor = rel_l2(r32[k], r64[k])
+        assert rel_l2(out[k], r64[k]) <= 2.5 * floor + 1e-9, (k, rel_l2(out[k], r64[k]), floor)
