@@ -148,10 +148,13 @@ def ingest_bdy(g, bdy, it, dtype=np.float32):
 class OracleModel:
     """Numpy state + one-RK3-step driver following pywrf/solver.py:709-1910."""
 
-    def __init__(self, g, inputs, bdy, dtype=np.float32):
+    def __init__(self, g, inputs, bdy, dtype=np.float32, theta_bias=None):
         self.g = g
         self.dtype = dtype
         self.bdy_src = bdy
+        # optional [nz, ny, nx] bias added to t_tend after rk_addtend_dry in
+        # every RK stage (the learnable parameter of the adjoint configuration)
+        self.theta_bias = None if theta_bias is None else np.asarray(theta_bias, dtype)
         self.st = ingest(g, inputs, bdy, dtype)
         self.step_count = 0
 
@@ -269,6 +272,8 @@ class OracleModel:
                              s["rv_tendf"], s["rw_tendf"], s["ph_tendf"], s["t_tendf"], s["u_save"], s["v_save"],
                              s["w_save"], s["ph_save"], s["t_save"], s["mu_tend"], s["mu_tendf"], rk_step,
                              s["h_diabatic"], s["mut"], s["msfty"], s["msfuy"], s["msfvx"], s["msfvx_inv"])
+            if self.theta_bias is not None:
+                s["t_tend"][...] = s["t_tend"] + self.theta_bias
             B.spec_bdytend(g, s["ru_tend"], bd["u"], "u")
             B.spec_bdytend(g, s["rv_tend"], bd["v"], "v")
             B.spec_bdytend(g, s["ph_tend"], bd["ph"], "h")

@@ -11,6 +11,12 @@ Writes, next to this script:
   values per field after 3 steps of configuration 0 (64x64x41) in float64.
 * ``c1_ref64_summary.json``: the same after 1 step of the 240x240x41
   configuration with boundary tendencies.
+* ``thbias_ref64.npz``: the adjoint configuration's check on the 28x28x16
+  case in float64 - a bias field added to the theta tendency after
+  rk_addtend_dry, the loss L = mean (theta - theta*)^2 + mean (qv - qv*)^2
+  over the lowest 10 levels of the mass points after 2 steps, against the
+  initial state of a second seed - with L at zero bias and its central
+  differences (eps 1e-3) in the bias at 16 seeded points.
 * ``small_bdyrec_ref64.npz`` / ``small_bdyrec_ref32.npz``: u, v, t, ph, mu,
   qv after 4 steps of the 28x28x16 case with a boundary interval of 2 steps
   and three distinct boundary records (``bdy_records``), so that step 3 runs
@@ -82,15 +88,65 @@ def bdyrec_case():
     return g, inp, bdy_records(bdy)
 
 
+THB = dict(nsteps=2, levels=10, npoints=16, eps=1e-3, point_seed=2024)
+
+
+def thbias_region(g, levels):
+    return (slice(0, levels), slice(g.jds, g.jde - 1), slice(g.ids, g.ide - 1))
+
+
+def thbias_points(g):
+    rng = np.random.default_rng(THB["point_seed"])
+    return np.stack([rng.integers(0, THB["levels"], THB["npoints"]), rng.integers(g.jds, g.jde - 1, THB["npoints"]),
+                     rng.integers(g.ids, g.ide - 1, THB["npoints"])], axis=1)
+
+
+def thbias_loss(t, qv, target, g):
+    R = thbias_region(g, THB["levels"])
+    return float(((t[R] - target["t"]) ** 2).mean() + ((qv[R] - target["qv"]) ** 2).mean())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("PYWRF_REFERENCE_ROOT", "/root/reference"))
     ap.add_argument("--skip-c1", action="store_true")
     ap.add_argument("--only-bdyrec", action="store_true", help="write small_bdyrec_ref64.npz only")
+    ap.add_argument("--only-thbias", action="store_true", help="write thbias_ref64.npz only")
     args = ap.parse_args()
     os.environ["PYWRF_REFERENCE_ROOT"] = args.reference
     import refharness
     refharness.REF_ROOT = args.reference
+
+    if args.only_thbias:
+        import dataclasses
+
+        spec = synthetic.CaseSpec(**SMALL)
+        g = synthetic.grid_for(spec)
+        inp, bdy = synthetic.build(spec)
+        inp2, bdy2 = synthetic.build(dataclasses.replace(spec, seed=spec.seed + 1))
+        t0 = refharness.run_reference(g, inp2, bdy2, 0, dtype="float64")
+        R = thbias_region(g, THB["levels"])
+        target = {"t": t0["t"][R], "qv": t0["moist"][1][R]}
+        nz, ny, nx = g.nz, g.ny, g.nx
+
+        def loss(bias):
+            r = refharness.run_reference(g, inp, bdy, THB["nsteps"], dtype="float64", theta_bias=bias)
+            return thbias_loss(r["t"], r["moist"][1], target, g)
+
+        zero = np.zeros((nz, ny, nx))
+        pts = thbias_points(g)
+        fd = []
+        for k, j, i in pts:
+            b = zero.copy()
+            b[k, j, i] = THB["eps"]
+            lp = loss(b)
+            b[k, j, i] = -THB["eps"]
+            fd.append((lp - loss(b)) / (2 * THB["eps"]))
+        np.savez_compressed(os.path.join(HERE, "thbias_ref64.npz"), meta=json.dumps({"case": SMALL, **THB}),
+                            loss0=np.array(loss(zero)), points=pts, fd=np.array(fd), target_t=target["t"],
+                            target_qv=target["qv"])
+        print("wrote thbias", fd[:4])
+        return
 
     g, inp, bdy = bdyrec_case()
     for dt in ("float64", "float32"):

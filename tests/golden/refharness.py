@@ -106,7 +106,7 @@ def _load_patched_solver():
     SOLVER_SHA256 = hashlib.sha256(src.encode()).hexdigest()
     lines = src.split("\n")
     out = []
-    n_print = n_max = 0
+    n_print = n_max = n_bias = 0
     for line in lines:
         s = line.strip()
         ind = line[: len(line) - len(line.lstrip())]
@@ -118,12 +118,19 @@ def _load_patched_solver():
             n_max += 1
         elif s.startswith("for t_big_step in range(1,721,1):"):
             out.append(ind + "for t_big_step in range(1, self.nsteps + 1):")
+        elif s == "# spec_bdy_dry":
+            # a learnable theta-tendency bias (the adjoint configuration's
+            # parameter), added after rk_addtend_dry when the solver has one
+            out.append(ind + 'if getattr(self, "theta_bias", None) is not None:')
+            out.append(ind + "    t_tend = t_tend + self.theta_bias")
+            out.append(line)
+            n_bias += 1
         elif s.startswith("# ---- final state: return the key fields ----"):
             out.append(ind + "_loc = dict(locals())")
             out.append(ind + "return {k: v for k, v in _loc.items() if isinstance(v, torch.Tensor)}")
         else:
             out.append(line)
-    assert n_print >= 10 and n_max >= 12, (n_print, n_max)
+    assert n_print >= 10 and n_max >= 12 and n_bias == 1, (n_print, n_max, n_bias)
     patched = "\n".join(out)
     assert "range(1, self.nsteps + 1)" in patched and "_loc = dict(locals())" in patched
     mod = types.ModuleType("pywrf_patched_solver")
@@ -132,9 +139,10 @@ def _load_patched_solver():
     return mod
 
 
-def run_reference(grid, inputs, bdy, nsteps, dtype="float32", device="cpu"):
+def run_reference(grid, inputs, bdy, nsteps, dtype="float32", device="cpu", theta_bias=None):
     """Run ``nsteps`` RK3 steps of the reference and return every tensor local
-    of ``solve`` as a numpy array."""
+    of ``solve`` as a numpy array; ``theta_bias`` (optional, [nz, ny, nx]) is
+    added to t_tend after rk_addtend_dry in every RK stage."""
     import torch
 
     _cp, _dyn, _phy, _bdy, solver = load_reference(grid, dtype=dtype, device=device)
@@ -148,6 +156,8 @@ def run_reference(grid, inputs, bdy, nsteps, dtype="float32", device="cpu"):
 
     s = _Solver()
     s.nsteps = nsteps
+    if theta_bias is not None:
+        s.theta_bias = torch.tensor(cast(np.asarray(theta_bias)))
     with torch.no_grad():
         res = s.solve()
     return {k: v.detach().cpu().numpy() for k, v in res.items()}

@@ -117,3 +117,32 @@ def test_oracle32_reloads_boundary_records_within_reference_fp32_error():
     for k in ("u", "v", "t", "ph", "mu", "qv"):
         floor = rel_l2(r32[k], r64[k])
         assert rel_l2(out[k], r64[k]) <= 2.5 * floor + 1e-9, (k, rel_l2(out[k], r64[k]), floor)
+
+
+def test_theta_bias_fixture_pinned_by_the_oracle(small_case):
+    """The adjoint configuration's check on the 28x28x16 case
+    (tests/golden/thbias_ref64.npz, from the reference with a bias added to
+    the theta tendency after rk_addtend_dry): the oracle reproduces the
+    reference's loss at zero bias, and its central differences in the bias at
+    an interior point and at a specified-row point (where spec_bdytend
+    overwrites the tendency: zero) equal the reference's."""
+    g, inputs, bdy = small_case
+    Z = load_npz("thbias_ref64.npz")
+    R = (slice(0, 10), slice(g.jds, g.jde - 1), slice(g.ids, g.ide - 1))
+
+    def loss(bias):
+        m = OracleModel(g, inputs, bdy, np.float64, theta_bias=bias)
+        m.run(2)
+        return float(((m.st["t"][R] - Z["target_t"]) ** 2).mean() + ((m.st["moist"][1][R] - Z["target_qv"]) ** 2).mean())
+
+    zero = np.zeros((g.nz, g.ny, g.nx))
+    assert abs(loss(zero) - float(Z["loss0"])) <= 1e-10 * abs(float(Z["loss0"]))
+    eps = 1e-3
+    for n in (0, 1):
+        k, j, i = (int(x) for x in Z["points"][n])
+        bp, bm = zero.copy(), zero.copy()
+        bp[k, j, i], bm[k, j, i] = eps, -eps
+        fd = (loss(bp) - loss(bm)) / (2 * eps)
+        ref = float(Z["fd"][n])
+        assert abs(fd - ref) <= 1e-4 * abs(ref) + 1e-12, (n, fd, ref)
+    assert float(Z["fd"][1]) == 0.0 and int(Z["points"][1][2]) == g.ide - 2
