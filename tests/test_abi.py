@@ -126,3 +126,20 @@ def test_kernel_form_switch():
     assert L.wrf_set_kernel_form(7) == N.WRF_EINVAL
     assert L.wrf_set_kernel_form(N.WRF_FORM_POINT) == N.WRF_FORM_FAST
     assert L.wrf_set_kernel_form(N.WRF_FORM_FAST) == N.WRF_FORM_POINT
+
+
+def test_header_is_plain_c():
+    """include/pywrf_b200.h compiles as C99 and as C++ (plain C types only)."""
+    import os
+    import shutil
+    import subprocess
+
+    import pytest
+
+    hdr = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "pywrf_b200.h")
+    for cc, lang, std in (("gcc", "c", "-std=c99"), ("g++", "c++", "-std=c++17")):
+        if shutil.which(cc) is None:
+            pytest.skip(f"{cc} not found")
+        r = subprocess.run([cc, "-fsyntax-only", "-Wall", "-Werror", "-x", lang, std, hdr], capture_output=True,
+                           text=True)
+        assert r.returncode == 0, r.stderr
