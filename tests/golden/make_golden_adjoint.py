@@ -44,6 +44,11 @@ the returned tendency with torch autograd, and writes next to this script:
   t_2ave' cot_t2a) along 3 seeded directions per input (``aw_direction``);
   the reference's autograd cannot run backward through its in-place
   tridiagonal sweeps; the upper levels lie in the Rayleigh damping layer;
+* ``forces_adj_ref64.npz`` -- the tendency terms rhs_ph, horizontal_pressure_
+  gradient, pg_buoy_w, coriolis and curvature (wrf_dynamics.py:2031-2620) on
+  one shared input set: per function, checksums of its outputs and central
+  differences of the float64 forward of L = sum(output cot) along 3 seeded
+  directions (``forces_direction``) in each differentiable input;
 * ``coefw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_coef_w``
   (wrf_dynamics.py:3316-3388): the reference's autograd cannot differentiate
   it (the recurrence updates ``gamma`` in place between its reads, and
@@ -371,6 +376,130 @@ def advance_w(dyn, g) -> None:
     print("wrote advw_adj_ref64.npz")
 
 
+FORCES = {  # function: (differentiable inputs, outputs)
+    "rhs_ph": (("u", "v", "ww", "ph", "phb", "w", "mut", "muu", "muv"), ("ph_tend",)),
+    "hpg": (("ph", "alt", "p", "pb", "al", "php", "cqu", "cqv", "muu", "muv", "mu"), ("ru_tend", "rv_tend")),
+    "pg_buoy_w": (("p", "cqw", "mu", "mub"), ("rw_tend", "cqw")),
+    "coriolis": (("ru", "rv", "rw"), ("ru_tend", "rv_tend", "rw_tend")),
+    "curvature": (("ru", "rv", "rw", "u", "v"), ("ru_tend", "rv_tend", "rw_tend")),
+}
+
+
+def forces_direction(f: int, n: int, r: int, shape) -> np.ndarray:
+    """Direction r of input n of function f (in FORCES order) of the
+    tendency-term finite differences (regenerated by the tests)."""
+    return np.random.default_rng(20000 + 1000 * f + 10 * n + r).standard_normal(shape)
+
+
+def forces_inputs(g) -> dict:
+    rng = np.random.default_rng(19)
+    sh, s2 = (NZ, N, N), (N, N)
+    kk = np.arange(NZ, dtype=np.float64)[:, None, None]
+    d = {
+        "u": 10.0 + 3.0 * rng.standard_normal(sh), "v": 3.0 * rng.standard_normal(sh), "w": rng.standard_normal(sh),
+        "ww": 5.0 * rng.standard_normal(sh), "ph": 50.0 * rng.standard_normal(sh),
+        "phb": 9.81 * 1800.0 * kk + 100.0 * rng.standard_normal(sh), "alt": 1.0 + 0.05 * rng.standard_normal(sh),
+        "p": 100.0 * rng.standard_normal(sh), "pb": 8.0e4 - 5.0e3 * kk + 100.0 * rng.standard_normal(sh),
+        "al": 0.01 * rng.standard_normal(sh), "php": 1.0e3 * (kk + 1.0) + 10.0 * rng.standard_normal(sh),
+        "cqu": 1.0 + 0.01 * rng.standard_normal(sh), "cqv": 1.0 + 0.01 * rng.standard_normal(sh),
+        "cqw": 0.01 * rng.standard_normal(sh), "ru": 8.0e5 + 2.0e5 * rng.standard_normal(sh),
+        "rv": 2.0e5 * rng.standard_normal(sh), "rw": 8.0e4 * rng.standard_normal(sh),
+        "mut": 8.0e4 + 1.0e3 * rng.standard_normal(s2), "muu": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "muv": 8.0e4 + 1.0e3 * rng.standard_normal(s2), "mu": 100.0 * rng.standard_normal(s2),
+        "mub": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "msfux": 1.0 + 0.02 * rng.random(s2), "msfuy": 1.0 + 0.02 * rng.random(s2),
+        "msfvx": 1.0 + 0.02 * rng.random(s2), "msfvy": 1.0 + 0.02 * rng.random(s2),
+        "msftx": 1.0 + 0.02 * rng.random(s2), "msfty": 1.0 + 0.02 * rng.random(s2),
+        "f": 1.0e-4 + 1.0e-5 * rng.standard_normal(s2), "e": 5.0e-5 + 1.0e-5 * rng.standard_normal(s2),
+        "sina": 0.01 * rng.standard_normal(s2), "cosa": 1.0 - 0.001 * rng.random(s2),
+        "clat": 30.0 + 5.0 * rng.standard_normal(s2),
+        "fnm": 0.45 + 0.1 * rng.random(NZ), "rdnw": -(10.0 + rng.random(NZ)), "rdn": -(10.0 + rng.random(NZ)),
+        "cot_ph_tend": rng.standard_normal(sh), "cot_ru_tend": rng.standard_normal(sh),
+        "cot_rv_tend": rng.standard_normal(sh), "cot_rw_tend": rng.standard_normal(sh),
+        "cot_cqw": rng.standard_normal(sh),
+    }
+    d["fnp"] = 1.0 - d["fnm"]
+    d["msfvx_inv"] = 1.0 / d["msfvx"]
+    return {k: v.astype(np.float32) for k, v in d.items()}
+
+
+FORCES_SC = {"cf1": 1.5, "cf2": -0.625, "cf3": 0.125, "cfn": 1.5, "cfn1": -0.5}
+
+
+def forces_call(dyn, g, name, x):
+    """Run one tendency term of the reference with the solver's argument list
+    (solver.py rhs_ph .. curvature calls); returns its outputs by name."""
+    import torch
+
+    one1 = torch.ones(NZ, dtype=torch.float64)
+    z3 = torch.zeros((NZ, N, N), dtype=torch.float64)
+    ids, ide, jds, jde = 5, N - 5, 5, N - 5
+    idx = (ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+    sc = FORCES_SC
+    if name == "rhs_ph":
+        pt = dyn.rhs_ph(z3.clone(), x["u"], x["v"], x["ww"], x["ph"], x["ph"], x["phb"], x["w"], x["mut"], x["muu"],
+                        x["muv"], one1, one1 * 0, x["fnm"], x["fnp"], x["rdnw"], sc["cfn"], sc["cfn1"], 1.0 / g.dx,
+                        1.0 / g.dy, x["msfux"], x["msfuy"], x["msfvx"], x["msfvx_inv"], x["msfvy"], x["msftx"],
+                        x["msfty"], True, *idx)
+        return {"ph_tend": pt}
+    if name == "hpg":
+        ru, rv = dyn.horizontal_pressure_gradient(z3.clone(), z3.clone(), x["ph"], x["alt"], x["p"], x["pb"], x["al"],
+                                                  x["php"], x["cqu"], x["cqv"], x["muu"], x["muv"], x["mu"], one1,
+                                                  one1 * 0, x["fnm"], x["fnp"], x["rdnw"], sc["cf1"], sc["cf2"],
+                                                  sc["cf3"], sc["cfn"], sc["cfn1"], 1.0 / g.dx, 1.0 / g.dy, x["msfux"],
+                                                  x["msfuy"], x["msfvx"], x["msfvy"], x["msftx"], x["msfty"], True,
+                                                  False, *idx)
+        return {"ru_tend": ru, "rv_tend": rv}
+    if name == "pg_buoy_w":
+        rw, cqw = dyn.pg_buoy_w(z3.clone(), x["p"], x["cqw"].clone(), x["mu"], x["mub"], one1, one1 * 0, x["rdnw"],
+                                x["rdn"], 9.81, x["msftx"], x["msfty"], *idx)
+        return {"rw_tend": rw, "cqw": cqw}
+    if name == "coriolis":
+        ru, rv, rw = dyn.coriolis(x["ru"], x["rv"], x["rw"], z3.clone(), z3.clone(), z3.clone(), x["msftx"], x["msfty"],
+                                  x["msfux"], x["msfuy"], x["msfvx"], x["msfvy"], x["f"], x["e"], x["sina"], x["cosa"],
+                                  x["fnm"], x["fnp"], *idx)
+        return {"ru_tend": ru, "rv_tend": rv, "rw_tend": rw}
+    ru, rv, rw = dyn.curvature(x["ru"], x["rv"], x["rw"], x["u"], x["v"], x["w"], z3.clone(), z3.clone(), z3.clone(),
+                               x["msfux"], x["msfuy"], x["msfvx"], x["msfvy"], x["msftx"], x["msfty"], x["clat"],
+                               x["fnm"], x["fnp"], 1.0 / g.dx, 1.0 / g.dy, *idx)
+    return {"ru_tend": ru, "rv_tend": rv, "rw_tend": rw}
+
+
+def forces(dyn, g) -> None:
+    """The five tendency terms: checksums and central differences
+    (forces_adj_ref64.npz)."""
+    import torch
+
+    d = forces_inputs(g)
+    save = dict(d)
+    save.update({k: np.array(v) for k, v in FORCES_SC.items()})
+    save["dx"], save["dy"] = np.array(g.dx), np.array(g.dy)
+    base = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
+    with torch.no_grad():
+        for fi, (name, (ins, outs)) in enumerate(FORCES.items()):
+            o0 = forces_call(dyn, g, name, base)
+            for o_ in outs:
+                a = o0[o_].numpy()
+                save[f"{name}_{o_}_sum"] = np.array(a.sum())
+                save[f"{name}_{o_}_l2"] = np.array(np.sqrt((a * a).sum()))
+
+            def loss(x):
+                oo = forces_call(dyn, g, name, x)
+                return float(sum((oo[o_] * x[f"cot_{o_}"]).sum() for o_ in outs))
+
+            for ni, inp in enumerate(ins):
+                eps = 1e-4 * float(base[inp].abs().max())
+                for r in range(3):
+                    dirn = torch.tensor(forces_direction(fi, ni, r, d[inp].shape))
+                    xp, xm = dict(base), dict(base)
+                    xp[inp] = base[inp] + eps * dirn
+                    xm[inp] = base[inp] - eps * dirn
+                    save[f"{name}_fd_{inp}_{r}"] = np.array((loss(xp) - loss(xm)) / (2 * eps))
+                save[f"{name}_fd_eps_{inp}"] = np.array(eps)
+    np.savez_compressed(os.path.join(HERE, "forces_adj_ref64.npz"), **save)
+    print("wrote forces_adj_ref64.npz")
+
+
 def mom_direction(n: int, r: int, shape) -> np.ndarray:
     """Direction r of input n (field, ru, rv, rom) of the advect_w finite
     differences (regenerated by the tests, not stored)."""
@@ -458,7 +587,8 @@ def momentum(dyn, g) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default=None)
-    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv", "calc_p_rho", "advance_mu_t", "advance_w"), default=None,
+    ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv", "calc_p_rho", "advance_mu_t", "advance_w",
+                             "forces"), default=None,
                     help="write one fixture only")
     a = ap.parse_args()
     if a.reference:
@@ -483,6 +613,9 @@ def main() -> None:
         return
     if a.only == "advance_w":
         advance_w(dyn, g)
+        return
+    if a.only == "forces":
+        forces(dyn, g)
         return
     if a.only is not None:
         raise SystemExit("--only: scalar, relax and coefw are written together (no --only)")
@@ -579,6 +712,7 @@ def main() -> None:
     calc_p_rho(dyn, g)
     advance_mu_t(dyn, g)
     advance_w(dyn, g)
+    forces(dyn, g)
 
 
 def importlib_bdy():

@@ -6,6 +6,7 @@ gradients' directional derivatives."""
 from __future__ import annotations
 
 import numpy as np
+import pytest
 
 from helpers import load_npz
 from oracle import boundary as OB
@@ -347,3 +348,79 @@ def test_advance_w_fixture_pinned_by_the_oracle():
         # the two float64 forwards round differently (~1e-13 relative), which
         # the finite difference magnifies by |L| / (eps |dL|)
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-9, (name, fd, ref)
+
+
+FZ = load_npz("forces_adj_ref64.npz")
+FORCES = {  # function: (differentiable inputs, outputs), as in make_golden_adjoint.FORCES
+    "rhs_ph": (("u", "v", "ww", "ph", "phb", "w", "mut", "muu", "muv"), ("ph_tend",)),
+    "hpg": (("ph", "alt", "p", "pb", "al", "php", "cqu", "cqv", "muu", "muv", "mu"), ("ru_tend", "rv_tend")),
+    "pg_buoy_w": (("p", "cqw", "mu", "mub"), ("rw_tend", "cqw")),
+    "coriolis": (("ru", "rv", "rw"), ("ru_tend", "rv_tend", "rw_tend")),
+    "curvature": (("ru", "rv", "rw", "u", "v"), ("ru_tend", "rv_tend", "rw_tend")),
+}
+
+
+def _forces_dir(f, n, r, shape):
+    # the directions of make_golden_adjoint.forces_direction
+    return np.random.default_rng(20000 + 1000 * f + 10 * n + r).standard_normal(shape)
+
+
+def _forces_oracle(g, name, x):
+    x = {k: np.array(v, np.float64) for k, v in x.items()}
+    z = lambda: np.zeros_like(x["u"])  # noqa: E731
+    sc = {k: float(FZ[k]) for k in ("cf1", "cf2", "cf3", "cfn", "cfn1")}
+    if name == "rhs_ph":
+        pt = z()
+        OD.rhs_ph(g, pt, x["u"], x["v"], x["ww"], x["ph"], x["phb"], x["w"], x["mut"], x["muu"], x["muv"], x["fnm"],
+                  x["fnp"], x["rdnw"], sc["cfn"], sc["cfn1"], x["msfux"], x["msfvy"], x["msfty"])
+        return {"ph_tend": pt}
+    if name == "hpg":
+        ru, rv = z(), z()
+        OD.horizontal_pressure_gradient(g, ru, rv, x["ph"], x["alt"], x["p"], x["pb"], x["al"], x["php"], x["cqu"],
+                                        x["cqv"], x["muu"], x["muv"], x["mu"], x["fnm"], x["fnp"], x["rdnw"],
+                                        sc["cf1"], sc["cf2"], sc["cf3"], x["msfux"], x["msfuy"], x["msfvx"],
+                                        x["msfvy"])
+        return {"ru_tend": ru, "rv_tend": rv}
+    if name == "pg_buoy_w":
+        rw, cqw = z(), x["cqw"].copy()
+        OD.pg_buoy_w(g, rw, x["p"], cqw, x["mu"], x["mub"], x["rdnw"], x["rdn"], x["msfty"])
+        return {"rw_tend": rw, "cqw": cqw}
+    ru, rv, rw = z(), z(), z()
+    if name == "coriolis":
+        OD.coriolis(g, x["ru"], x["rv"], x["rw"], ru, rv, rw, x["msftx"], x["msfty"], x["msfux"], x["msfuy"],
+                    x["msfvx"], x["msfvy"], x["f"], x["e"], x["sina"], x["cosa"], x["fnm"], x["fnp"])
+    else:
+        OD.curvature(g, x["ru"], x["rv"], x["rw"], x["u"], x["v"], ru, rv, rw, x["msfux"], x["msfuy"], x["msfvx"],
+                     x["msfvy"], x["msftx"], x["msfty"], x["fnm"], x["fnp"])
+    return {"ru_tend": ru, "rv_tend": rv, "rw_tend": rw}
+
+
+@pytest.mark.parametrize("name", list(FORCES))
+def test_tendency_terms_fixture_pinned_by_the_oracle(name):
+    """rhs_ph, horizontal_pressure_gradient, pg_buoy_w (with its in-place
+    cqw), coriolis, curvature: the oracle's outputs have the reference's
+    checksums on the fixture's inputs, and its central differences equal the
+    reference's along the fixture's first direction of every input."""
+    g = _grid()
+    fi = list(FORCES).index(name)
+    ins, outs = FORCES[name]
+    base = {k: FZ[k] for k in FZ if np.asarray(FZ[k]).ndim > 0 and not k.startswith(name)}
+    o0 = _forces_oracle(g, name, base)
+    for o in outs:
+        l2 = float(np.sqrt((o0[o] ** 2).sum()))
+        assert abs(l2 - float(FZ[f"{name}_{o}_l2"])) <= 1e-12 * l2, (o, l2)
+        assert abs(float(o0[o].sum()) - float(FZ[f"{name}_{o}_sum"])) <= 1e-12 * l2 * o0[o].size ** 0.5, o
+
+    def loss(x):
+        oo = _forces_oracle(g, name, x)
+        return sum(float((oo[o] * np.asarray(FZ[f"cot_{o}"], np.float64)).sum()) for o in outs)
+
+    for ni, inp in enumerate(ins):
+        d = _forces_dir(fi, ni, 0, np.asarray(base[inp]).shape)
+        eps = float(FZ[f"{name}_fd_eps_{inp}"])
+        xp, xm = dict(base), dict(base)
+        xp[inp] = np.asarray(base[inp], np.float64) + eps * d
+        xm[inp] = np.asarray(base[inp], np.float64) - eps * d
+        fd = (loss(xp) - loss(xm)) / (2 * eps)
+        ref = float(FZ[f"{name}_fd_{inp}_0"])
+        assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-9, (name, inp, fd, ref)
