@@ -49,6 +49,11 @@ the returned tendency with torch autograd, and writes next to this script:
   one shared input set: per function, checksums of its outputs and central
   differences of the float64 forward of L = sum(output cot) along 3 seeded
   directions (``forces_direction``) in each differentiable input;
+* ``subbdy_adj_ref64.npz`` -- the rest of the acoustic substep: sumflux
+  (wrf_dynamics.py:3799-3839) at its first and last iteration,
+  spec_bdyupdate of a 3-D ('t') and a 2-D ('m') field and spec_bdyupdate_ph
+  (wrf_boundary.py:244-355), in the form of ``forces_adj_ref64.npz``
+  (``subbdy_direction``);
 * ``coefw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_coef_w``
   (wrf_dynamics.py:3316-3388): the reference's autograd cannot differentiate
   it (the recurrence updates ``gamma`` in place between its reads, and
@@ -500,6 +505,105 @@ def forces(dyn, g) -> None:
     print("wrote forces_adj_ref64.npz")
 
 
+SUBBDY = {  # case: (differentiable inputs, outputs)
+    "sumflux1": (("u", "v", "ww", "u_save", "v_save", "ww1", "muu", "muv"), ("ru_m", "rv_m", "ww_m")),
+    "sumflux2": (("u", "v", "ww", "u_save", "v_save", "ww1", "muu", "muv", "ru_m", "rv_m", "ww_m"),
+                 ("ru_m", "rv_m", "ww_m")),
+    "spec_t": (("t", "t_tend"), ("t",)),
+    "spec_m": (("mu", "mu_tend"), ("mu",)),
+    "spec_ph": (("ph_save", "ph", "ph_tend", "mu_tend", "muts"), ("ph",)),
+}
+
+
+def subbdy_direction(f: int, n: int, r: int, shape) -> np.ndarray:
+    """Direction r of input n of case f (in SUBBDY order), regenerated by the tests."""
+    return np.random.default_rng(30000 + 1000 * f + 10 * n + r).standard_normal(shape)
+
+
+def subbdy_inputs() -> dict:
+    rng = np.random.default_rng(21)
+    sh, s2 = (NZ, N, N), (N, N)
+    d = {
+        "u": 10.0 + 3.0 * rng.standard_normal(sh), "v": 3.0 * rng.standard_normal(sh),
+        "ww": 5.0 * rng.standard_normal(sh), "u_save": 10.0 + 3.0 * rng.standard_normal(sh),
+        "v_save": 3.0 * rng.standard_normal(sh), "ww1": 5.0 * rng.standard_normal(sh),
+        "ru_m": 8.0e5 * rng.standard_normal(sh), "rv_m": 2.0e5 * rng.standard_normal(sh),
+        "ww_m": 5.0 * rng.standard_normal(sh), "t": 100.0 * rng.standard_normal(sh),
+        "t_tend": rng.standard_normal(sh), "ph": 50.0 * rng.standard_normal(sh),
+        "ph_save": 50.0 * rng.standard_normal(sh), "ph_tend": 10.0 * rng.standard_normal(sh),
+        "muu": 8.0e4 + 1.0e3 * rng.standard_normal(s2), "muv": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "mu": 100.0 * rng.standard_normal(s2), "mu_tend": rng.standard_normal(s2),
+        "muts": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "msfux": 1.0 + 0.02 * rng.random(s2), "msfuy": 1.0 + 0.02 * rng.random(s2),
+        "msfvx": 1.0 + 0.02 * rng.random(s2), "msfvy": 1.0 + 0.02 * rng.random(s2),
+        "cot_ru_m": rng.standard_normal(sh), "cot_rv_m": rng.standard_normal(sh), "cot_ww_m": rng.standard_normal(sh),
+        "cot_t": rng.standard_normal(sh), "cot_mu": rng.standard_normal(s2), "cot_ph": rng.standard_normal(sh),
+    }
+    d["msfvx_inv"] = 1.0 / d["msfvx"]
+    return {k: v.astype(np.float32) for k, v in d.items()}
+
+
+SUBBDY_DTS = 11.25
+
+
+def subbdy_call(dyn, bnd, g, name, x):
+    """Run one case with the solver's argument lists (solver.py:1394-1445)."""
+    import torch
+
+    one1 = torch.ones(NZ, dtype=torch.float64)
+    ids, ide, jds, jde = 5, N - 5, 5, N - 5
+    idx = (ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+    bidx = (ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+    bidx2 = (ids, ide, jds, jde, 0, 0, 0, N, 0, N, 0, 0, 0, N, 0, N, 0, 0, ids, ide, jds, jde, 0, 0)
+    if name.startswith("sumflux"):
+        it = 1 if name == "sumflux1" else 2
+        ru_m, rv_m, ww_m = dyn.sumflux(x["u"], x["v"], x["ww"], x["u_save"], x["v_save"], x["ww1"], x["muu"], x["muv"],
+                                       one1, one1 * 0, one1, one1 * 0, one1, one1 * 0, one1, one1 * 0,
+                                       x["ru_m"].clone(), x["rv_m"].clone(), x["ww_m"].clone(), 0.1, x["msfux"],
+                                       x["msfuy"], x["msfvx"], x["msfvx_inv"], x["msfvy"], it, 2, *idx)
+        return {"ru_m": ru_m, "rv_m": rv_m, "ww_m": ww_m}
+    if name == "spec_t":
+        return {"t": bnd.spec_bdyupdate(x["t"].clone(), x["t_tend"], SUBBDY_DTS, "t", 1, *bidx)}
+    if name == "spec_m":
+        return {"mu": bnd.spec_bdyupdate(x["mu"].clone(), x["mu_tend"], SUBBDY_DTS, "m", 1, *bidx2)}
+    return {"ph": bnd.spec_bdyupdate_ph(x["ph_save"], x["ph"].clone(), x["ph_tend"], x["mu_tend"], x["muts"], one1,
+                                        one1 * 0, SUBBDY_DTS, "h", 1, *bidx)}
+
+
+def subbdy(dyn, bnd, g) -> None:
+    """The rest of the acoustic substep: checksums and central differences
+    (subbdy_adj_ref64.npz)."""
+    import torch
+
+    d = subbdy_inputs()
+    save = dict(d)
+    save["dts"] = np.array(SUBBDY_DTS)
+    base = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
+    with torch.no_grad():
+        for fi, (name, (ins, outs)) in enumerate(SUBBDY.items()):
+            o0 = subbdy_call(dyn, bnd, g, name, base)
+            for o_ in outs:
+                a = o0[o_].numpy()
+                save[f"{name}_{o_}_sum"] = np.array(a.sum())
+                save[f"{name}_{o_}_l2"] = np.array(np.sqrt((a * a).sum()))
+
+            def loss(x):
+                oo = subbdy_call(dyn, bnd, g, name, x)
+                return float(sum((oo[o_] * x[f"cot_{o_}"]).sum() for o_ in outs))
+
+            for ni, inp in enumerate(ins):
+                eps = 1e-4 * float(base[inp].abs().max())
+                save[f"{name}_fd_eps_{inp}"] = np.array(eps)
+                for r in range(3):
+                    dirn = torch.tensor(subbdy_direction(fi, ni, r, d[inp].shape))
+                    xp, xm = dict(base), dict(base)
+                    xp[inp] = base[inp] + eps * dirn
+                    xm[inp] = base[inp] - eps * dirn
+                    save[f"{name}_fd_{inp}_{r}"] = np.array((loss(xp) - loss(xm)) / (2 * eps))
+    np.savez_compressed(os.path.join(HERE, "subbdy_adj_ref64.npz"), **save)
+    print("wrote subbdy_adj_ref64.npz")
+
+
 def mom_direction(n: int, r: int, shape) -> np.ndarray:
     """Direction r of input n (field, ru, rv, rom) of the advect_w finite
     differences (regenerated by the tests, not stored)."""
@@ -588,7 +692,7 @@ def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default=None)
     ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv", "calc_p_rho", "advance_mu_t", "advance_w",
-                             "forces"), default=None,
+                             "forces", "subbdy"), default=None,
                     help="write one fixture only")
     a = ap.parse_args()
     if a.reference:
@@ -616,6 +720,9 @@ def main() -> None:
         return
     if a.only == "forces":
         forces(dyn, g)
+        return
+    if a.only == "subbdy":
+        subbdy(dyn, importlib_bdy(), g)
         return
     if a.only is not None:
         raise SystemExit("--only: scalar, relax and coefw are written together (no --only)")
@@ -713,6 +820,7 @@ def main() -> None:
     advance_mu_t(dyn, g)
     advance_w(dyn, g)
     forces(dyn, g)
+    subbdy(dyn, importlib_bdy(), g)
 
 
 def importlib_bdy():

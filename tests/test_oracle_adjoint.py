@@ -424,3 +424,66 @@ def test_tendency_terms_fixture_pinned_by_the_oracle(name):
         fd = (loss(xp) - loss(xm)) / (2 * eps)
         ref = float(FZ[f"{name}_fd_{inp}_0"])
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-9, (name, inp, fd, ref)
+
+
+SZ = load_npz("subbdy_adj_ref64.npz")
+SUBBDY = {  # case: (differentiable inputs, outputs), as in make_golden_adjoint.SUBBDY
+    "sumflux1": (("u", "v", "ww", "u_save", "v_save", "ww1", "muu", "muv"), ("ru_m", "rv_m", "ww_m")),
+    "sumflux2": (("u", "v", "ww", "u_save", "v_save", "ww1", "muu", "muv", "ru_m", "rv_m", "ww_m"),
+                 ("ru_m", "rv_m", "ww_m")),
+    "spec_t": (("t", "t_tend"), ("t",)),
+    "spec_m": (("mu", "mu_tend"), ("mu",)),
+    "spec_ph": (("ph_save", "ph", "ph_tend", "mu_tend", "muts"), ("ph",)),
+}
+
+
+def _subbdy_dir(f, n, r, shape):
+    # the directions of make_golden_adjoint.subbdy_direction
+    return np.random.default_rng(30000 + 1000 * f + 10 * n + r).standard_normal(shape)
+
+
+def _subbdy_oracle(g, name, x):
+    x = {k: np.array(v, np.float64) for k, v in x.items()}
+    dts = float(SZ["dts"])
+    if name.startswith("sumflux"):
+        OD.sumflux(g, x, 1 if name == "sumflux1" else 2, 2)
+        return {k: x[k] for k in ("ru_m", "rv_m", "ww_m")}
+    if name == "spec_t":
+        OB.spec_bdyupdate(g, x["t"], x["t_tend"], dts, "t")
+        return {"t": x["t"]}
+    if name == "spec_m":
+        OB.spec_bdyupdate(g, x["mu"], x["mu_tend"], dts, "m")
+        return {"mu": x["mu"]}
+    OB.spec_bdyupdate_ph(g, x["ph_save"], x["ph"], x["ph_tend"], x["mu_tend"], x["muts"], dts)
+    return {"ph": x["ph"]}
+
+
+@pytest.mark.parametrize("name", list(SUBBDY))
+def test_substep_boundary_and_flux_sums_pinned_by_the_oracle(name):
+    """sumflux (first and last iteration), spec_bdyupdate ('t', 'm') and
+    spec_bdyupdate_ph: the oracle's outputs have the reference's checksums on
+    the fixture's inputs, and its central differences equal the reference's
+    along the fixture's first direction of every input."""
+    g = _grid()
+    fi = list(SUBBDY).index(name)
+    ins, outs = SUBBDY[name]
+    base = {k: SZ[k] for k in SZ if np.asarray(SZ[k]).ndim > 0 and not k.startswith(name)}
+    o0 = _subbdy_oracle(g, name, base)
+    for o in outs:
+        l2 = float(np.sqrt((o0[o] ** 2).sum()))
+        assert abs(l2 - float(SZ[f"{name}_{o}_l2"])) <= 1e-12 * l2, (o, l2)
+        assert abs(float(o0[o].sum()) - float(SZ[f"{name}_{o}_sum"])) <= 1e-12 * l2 * o0[o].size ** 0.5, o
+
+    def loss(x):
+        oo = _subbdy_oracle(g, name, x)
+        return sum(float((oo[o] * np.asarray(SZ[f"cot_{o}"], np.float64)).sum()) for o in outs)
+
+    for ni, inp in enumerate(ins):
+        d = _subbdy_dir(fi, ni, 0, np.asarray(base[inp]).shape)
+        eps = float(SZ[f"{name}_fd_eps_{inp}"])
+        xp, xm = dict(base), dict(base)
+        xp[inp] = np.asarray(base[inp], np.float64) + eps * d
+        xm[inp] = np.asarray(base[inp], np.float64) - eps * d
+        fd = (loss(xp) - loss(xm)) / (2 * eps)
+        ref = float(SZ[f"{name}_fd_{inp}_0"])
+        assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-9, (name, inp, fd, ref)
