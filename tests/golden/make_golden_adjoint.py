@@ -54,6 +54,10 @@ the returned tendency with torch autograd, and writes next to this script:
   spec_bdyupdate of a 3-D ('t') and a 2-D ('m') field and spec_bdyupdate_ph
   (wrf_boundary.py:244-355), in the form of ``forces_adj_ref64.npz``
   (``subbdy_direction``);
+* ``prep_adj_ref64.npz`` -- rk_step_prep's functions calculate_full,
+  calc_mu_uv, couple_momentum, calc_ww_cp, calc_cq, calc_alt, calc_php
+  (wrf_dynamics.py:30-163), in the form of ``forces_adj_ref64.npz``
+  (``prep_direction``);
 * ``coefw_adj_ref64.npz`` -- ``pywrf.wrf_dynamics.calc_coef_w``
   (wrf_dynamics.py:3316-3388): the reference's autograd cannot differentiate
   it (the recurrence updates ``gamma`` in place between its reads, and
@@ -604,6 +608,116 @@ def subbdy(dyn, bnd, g) -> None:
     print("wrote subbdy_adj_ref64.npz")
 
 
+PREP = {  # function: (differentiable inputs, outputs)
+    "calculate_full": (("mub", "mu"), ("mut",)),
+    "calc_mu_uv": (("mu", "mub"), ("muu", "muv")),
+    "couple_momentum": (("muu", "u", "muv", "v", "mut", "w"), ("ru", "rv", "rw")),
+    "calc_ww_cp": (("u", "v", "muu", "muv", "ww"), ("ww",)),
+    "calc_cq": (("moist",), ("cqu", "cqv", "cqw")),
+    "calc_alt": (("al", "alb"), ("alt",)),
+    "calc_php": (("ph", "phb"), ("php",)),
+}
+
+
+def prep_direction(f: int, n: int, r: int, shape) -> np.ndarray:
+    """Direction r of input n of function f (in PREP order), regenerated by the tests."""
+    return np.random.default_rng(40000 + 1000 * f + 10 * n + r).standard_normal(shape)
+
+
+def prep_inputs() -> dict:
+    rng = np.random.default_rng(22)
+    sh, s2 = (NZ, N, N), (N, N)
+    kk = np.arange(NZ, dtype=np.float64)[:, None, None]
+    moist = np.zeros((7,) + sh)
+    moist[1] = 0.01 * rng.random(sh)
+    moist[2:] = 1.0e-4 * rng.random((5,) + sh)
+    d = {
+        "u": 10.0 + 3.0 * rng.standard_normal(sh), "v": 3.0 * rng.standard_normal(sh), "w": rng.standard_normal(sh),
+        "ww": 5.0 * rng.standard_normal(sh), "ph": 50.0 * rng.standard_normal(sh),
+        "phb": 9.81 * 1800.0 * kk + 100.0 * rng.standard_normal(sh), "al": 0.01 * rng.standard_normal(sh),
+        "alb": 1.0 + 0.2 * rng.random(sh), "moist": moist,
+        "mu": 100.0 * rng.standard_normal(s2), "mub": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "mut": 8.0e4 + 1.0e3 * rng.standard_normal(s2), "muu": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "muv": 8.0e4 + 1.0e3 * rng.standard_normal(s2),
+        "msfu": 1.0 + 0.02 * rng.random(s2), "msfv": 1.0 + 0.02 * rng.random(s2), "msft": 1.0 + 0.02 * rng.random(s2),
+        "msftx": 1.0 + 0.02 * rng.random(s2), "msfty": 1.0 + 0.02 * rng.random(s2),
+        "msfux": 1.0 + 0.02 * rng.random(s2), "msfuy": 1.0 + 0.02 * rng.random(s2),
+        "msfvx": 1.0 + 0.02 * rng.random(s2), "msfvy": 1.0 + 0.02 * rng.random(s2),
+        "rdnw": -(10.0 + rng.random(NZ)),
+    }
+    d["msfvx_inv"] = 1.0 / d["msfvx"]
+    d["dnw"] = 1.0 / d["rdnw"]
+    for o_ in ("mut", "muu", "muv", "ru", "rv", "rw", "ww", "cqu", "cqv", "cqw", "alt", "php"):
+        d[f"cot_{o_}"] = rng.standard_normal(s2 if o_ in ("mut", "muu", "muv") else sh)
+    return {k: v.astype(np.float32) for k, v in d.items()}
+
+
+def prep_call(dyn, g, name, x):
+    """Run one of rk_step_prep's functions with the solver's argument list
+    (solver.py:736-778); returns its outputs by name."""
+    import torch
+
+    one1 = torch.ones(NZ, dtype=torch.float64)
+    z3 = lambda: torch.zeros((NZ, N, N), dtype=torch.float64)  # noqa: E731
+    z2 = lambda: torch.zeros((N, N), dtype=torch.float64)  # noqa: E731
+    ids, ide, jds, jde = 5, N - 5, 5, N - 5
+    idx = (ids, ide, jds, jde, 0, NZ, 0, N, 0, N, 0, NZ, ids, ide, jds, jde, 0, NZ)
+    if name == "calculate_full":
+        return {"mut": dyn.calculate_full(z2(), x["mub"], x["mu"], *idx)}
+    if name == "calc_mu_uv":
+        muu, muv = dyn.calc_mu_uv(x["mu"], x["mub"], z2(), z2(), *idx)
+        return {"muu": muu, "muv": muv}
+    if name == "couple_momentum":
+        ru, rv, rw = dyn.couple_momentum(x["muu"], z3(), x["u"], x["msfu"], x["muv"], z3(), x["v"], x["msfv"],
+                                         x["msfvx_inv"], x["mut"], z3(), x["w"], x["msft"], one1, one1 * 0, one1,
+                                         one1 * 0, *idx)
+        return {"ru": ru, "rv": rv, "rw": rw}
+    if name == "calc_ww_cp":
+        ww = dyn.calc_ww_cp(x["u"], x["v"], x["mu"], x["mub"], x["muu"], x["muv"], one1, one1 * 0, x["ww"].clone(),
+                            1.0 / g.dx, 1.0 / g.dy, x["msftx"], x["msfty"], x["msfux"], x["msfuy"], x["msfvx"],
+                            x["msfvx_inv"], x["msfvy"], x["dnw"], *idx)
+        return {"ww": ww}
+    if name == "calc_cq":
+        cqu, cqv, cqw = dyn.calc_cq(x["moist"], z3(), z3(), z3(), 7, *idx)
+        return {"cqu": cqu, "cqv": cqv, "cqw": cqw}
+    if name == "calc_alt":
+        return {"alt": dyn.calc_alt(z3(), x["al"], x["alb"], *idx)}
+    return {"php": dyn.calc_php(z3(), x["ph"], x["phb"], *idx)}
+
+
+def prep(dyn, g) -> None:
+    """rk_step_prep's functions: checksums and central differences
+    (prep_adj_ref64.npz)."""
+    import torch
+
+    d = prep_inputs()
+    save = dict(d)
+    base = {k: torch.tensor(v, dtype=torch.float64) for k, v in d.items()}
+    with torch.no_grad():
+        for fi, (name, (ins, outs)) in enumerate(PREP.items()):
+            o0 = prep_call(dyn, g, name, base)
+            for o_ in outs:
+                a = o0[o_].numpy()
+                save[f"{name}_{o_}_sum"] = np.array(a.sum())
+                save[f"{name}_{o_}_l2"] = np.array(np.sqrt((a * a).sum()))
+
+            def loss(x):
+                oo = prep_call(dyn, g, name, x)
+                return float(sum((oo[o_] * x[f"cot_{o_}"]).sum() for o_ in outs))
+
+            for ni, inp in enumerate(ins):
+                eps = 1e-4 * float(base[inp].abs().max())
+                save[f"{name}_fd_eps_{inp}"] = np.array(eps)
+                for r in range(3):
+                    dirn = torch.tensor(prep_direction(fi, ni, r, d[inp].shape))
+                    xp, xm = dict(base), dict(base)
+                    xp[inp] = base[inp] + eps * dirn
+                    xm[inp] = base[inp] - eps * dirn
+                    save[f"{name}_fd_{inp}_{r}"] = np.array((loss(xp) - loss(xm)) / (2 * eps))
+    np.savez_compressed(os.path.join(HERE, "prep_adj_ref64.npz"), **save)
+    print("wrote prep_adj_ref64.npz")
+
+
 def mom_direction(n: int, r: int, shape) -> np.ndarray:
     """Direction r of input n (field, ru, rv, rom) of the advect_w finite
     differences (regenerated by the tests, not stored)."""
@@ -692,7 +806,7 @@ def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default=None)
     ap.add_argument("--only", choices=("scalar", "relax", "coefw", "momentum", "advance_uv", "calc_p_rho", "advance_mu_t", "advance_w",
-                             "forces", "subbdy"), default=None,
+                             "forces", "subbdy", "prep"), default=None,
                     help="write one fixture only")
     a = ap.parse_args()
     if a.reference:
@@ -723,6 +837,9 @@ def main() -> None:
         return
     if a.only == "subbdy":
         subbdy(dyn, importlib_bdy(), g)
+        return
+    if a.only == "prep":
+        prep(dyn, g)
         return
     if a.only is not None:
         raise SystemExit("--only: scalar, relax and coefw are written together (no --only)")
@@ -821,6 +938,7 @@ def main() -> None:
     advance_w(dyn, g)
     forces(dyn, g)
     subbdy(dyn, importlib_bdy(), g)
+    prep(dyn, g)
 
 
 def importlib_bdy():

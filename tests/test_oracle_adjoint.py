@@ -487,3 +487,86 @@ def test_substep_boundary_and_flux_sums_pinned_by_the_oracle(name):
         fd = (loss(xp) - loss(xm)) / (2 * eps)
         ref = float(SZ[f"{name}_fd_{inp}_0"])
         assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-9, (name, inp, fd, ref)
+
+
+PZ = load_npz("prep_adj_ref64.npz")
+PREP = {  # function: (differentiable inputs, outputs), as in make_golden_adjoint.PREP
+    "calculate_full": (("mub", "mu"), ("mut",)),
+    "calc_mu_uv": (("mu", "mub"), ("muu", "muv")),
+    "couple_momentum": (("muu", "u", "muv", "v", "mut", "w"), ("ru", "rv", "rw")),
+    "calc_ww_cp": (("u", "v", "muu", "muv", "ww"), ("ww",)),
+    "calc_cq": (("moist",), ("cqu", "cqv", "cqw")),
+    "calc_alt": (("al", "alb"), ("alt",)),
+    "calc_php": (("ph", "phb"), ("php",)),
+}
+
+
+def _prep_dir(f, n, r, shape):
+    # the directions of make_golden_adjoint.prep_direction
+    return np.random.default_rng(40000 + 1000 * f + 10 * n + r).standard_normal(shape)
+
+
+def _prep_oracle(g, name, x):
+    x = {k: np.array(v, np.float64) for k, v in x.items()}
+    z3 = lambda: np.zeros_like(x["u"])  # noqa: E731
+    z2 = lambda: np.zeros_like(x["mu"])  # noqa: E731
+    if name == "calculate_full":
+        mut = z2()
+        OD.calculate_full(g, mut, x["mub"], x["mu"])
+        return {"mut": mut}
+    if name == "calc_mu_uv":
+        muu, muv = z2(), z2()
+        OD.calc_mu_uv(g, x["mu"], x["mub"], muu, muv)
+        return {"muu": muu, "muv": muv}
+    if name == "couple_momentum":
+        ru, rv, rw = z3(), z3(), z3()
+        OD.couple_momentum(g, x["muu"], ru, x["u"], x["msfu"], x["muv"], rv, x["v"], x["msfvx_inv"], x["mut"], rw,
+                           x["w"], x["msft"])
+        return {"ru": ru, "rv": rv, "rw": rw}
+    if name == "calc_ww_cp":
+        ww = x["ww"].copy()
+        OD.calc_ww_cp(g, x["u"], x["v"], x["muu"], x["muv"], np.ones(g.nz), ww, x["msftx"], x["msfuy"],
+                      x["msfvx_inv"], x["dnw"])
+        return {"ww": ww}
+    if name == "calc_cq":
+        cqu, cqv, cqw = z3(), z3(), z3()
+        OD.calc_cq(g, x["moist"], cqu, cqv, cqw)
+        return {"cqu": cqu, "cqv": cqv, "cqw": cqw}
+    if name == "calc_alt":
+        alt = z3()
+        OD.calc_alt(g, alt, x["al"], x["alb"])
+        return {"alt": alt}
+    php = z3()
+    OD.calc_php(g, php, x["ph"], x["phb"])
+    return {"php": php}
+
+
+@pytest.mark.parametrize("name", list(PREP))
+def test_rk_step_prep_functions_pinned_by_the_oracle(name):
+    """calculate_full, calc_mu_uv, couple_momentum, calc_ww_cp, calc_cq,
+    calc_alt, calc_php: the oracle's outputs have the reference's checksums
+    on the fixture's inputs, and its central differences equal the
+    reference's along the fixture's first direction of every input."""
+    g = _grid()
+    fi = list(PREP).index(name)
+    ins, outs = PREP[name]
+    base = {k: PZ[k] for k in PZ if np.asarray(PZ[k]).ndim > 0 and not k.startswith(name)}
+    o0 = _prep_oracle(g, name, base)
+    for o in outs:
+        l2 = float(np.sqrt((o0[o] ** 2).sum()))
+        assert abs(l2 - float(PZ[f"{name}_{o}_l2"])) <= 1e-12 * l2, (o, l2)
+        assert abs(float(o0[o].sum()) - float(PZ[f"{name}_{o}_sum"])) <= 1e-12 * l2 * o0[o].size ** 0.5, o
+
+    def loss(x):
+        oo = _prep_oracle(g, name, x)
+        return sum(float((oo[o] * np.asarray(PZ[f"cot_{o}"], np.float64)).sum()) for o in outs)
+
+    for ni, inp in enumerate(ins):
+        d = _prep_dir(fi, ni, 0, np.asarray(base[inp]).shape)
+        eps = float(PZ[f"{name}_fd_eps_{inp}"])
+        xp, xm = dict(base), dict(base)
+        xp[inp] = np.asarray(base[inp], np.float64) + eps * d
+        xm[inp] = np.asarray(base[inp], np.float64) - eps * d
+        fd = (loss(xp) - loss(xm)) / (2 * eps)
+        ref = float(PZ[f"{name}_fd_{inp}_0"])
+        assert abs(fd - ref) <= 1e-5 * abs(ref) + 1e-9, (name, inp, fd, ref)
