@@ -54,10 +54,9 @@ FALLBACK_HBM_GBS = 6650.0
 E2E_FIELDS = ("u", "v", "w", "t", "ph", "mu", "p", "al", "moist")
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
-# dominant kernel from one ncu --set full capture of this workload
-# (profiles/k_acoustic_col_and_tma_stencils_240x240x41.md): the stage-1
-# launch, 201.5 MB read + 74.0 MB written, against 321 MB algorithmic for that
-# launch
+# dominant kernel, from one ncu capture of this workload's step (the first
+# k_acoustic_col launch of a step, RK stage 1): a constant of that capture, not
+# a measurement of the run, and labelled so in the bench line
 NCU_TRAFFIC = {"k_acoustic_col": 275.5e6}
 
 
@@ -227,30 +226,58 @@ def run_ours(a):
     st = DeviceState.from_inputs(g, inputs, bdy, device=f"cuda:{local}")
     it = Integrator(st)
 
+    # The workload is a 1-h integration (spec.nsteps = 80 steps): its seeded
+    # boundary tendencies push the boundary state linearly away from the
+    # initial one, and the forced state is defined (and stable) over that
+    # hour, not indefinitely.  K timed steps therefore run as integrations of
+    # at most spec.nsteps steps, each from the initial state; the copy back to
+    # it lies between the timed segments.  NaN counts of every segment are
+    # accumulated on the device before each restore.
+    seg = max(1, spec.nsteps)
+    init = st.snapshot()
+    nan_acc = torch.zeros((), dtype=torch.int64, device=st["status"].device)
+
+    def restart():
+        nan_acc.add_(st["status"][N.WRF_ST_NAN_P].to(torch.int64))
+        st.restore(init)
+
     # one eager step: launch count, then the graph
     it.step()
     launches = N.lib().wrf_last_launch_count()
+    restart()
     it.capture()
-    for _ in range(a.warmup):
+    for w in range(a.warmup):
+        if w and w % seg == 0:
+            restart()
         it.replay()
     torch.cuda.synchronize()
+    restart()
 
     stream = it._graph_stream
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nseg = (a.steps + seg - 1) // seg
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nseg)]
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as cs:
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            for _ in range(a.steps):
-                it._graph.replay()
-            e1.record(stream)
+        done = 0
+        for e0, e1 in evs:
+            n = min(seg, a.steps - done)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                for _ in range(n):
+                    it._graph.replay()
+                e1.record(stream)
+            done += n
+            if done < a.steps:
+                with torch.cuda.stream(stream):
+                    restart()
         torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1)
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
     ms_max = max_over_ranks(ms)
     value = job_rate(a.steps, ms_max, world)
     clocks = cs.summary()
+    restart()
 
     # per-phase device time of eager steps (probe events on the launch stream)
     phase_ms: dict[str, float] = {}
@@ -273,7 +300,7 @@ def run_ours(a):
                 key = "sub." + key.split(".")[1] if key.count(".") else "sub.bc"
             phase_ms[key] = phase_ms.get(key, 0.0) + prev.elapsed_time(e) / a.phase_steps
             prev = e
-    nan = it.status()["nan_p"]
+    restart()
 
     # roofline of the dominant kernel, k_acoustic_col (the "sub.col" phases:
     # that kernel alone, 7 launches per step)
@@ -284,6 +311,8 @@ def run_ours(a):
     traffic = NCU_TRAFFIC.get("k_acoustic_col")
     roofline = {"kernel": "k_acoustic_col", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_kind,
+                "traffic_source": "ncu capture of the 240x240x41 step (first launch of the kernel in a step), "
+                                  "not measured in this run",
                 "algorithmic_bytes": ab["k_acoustic_col"], "kernel_ms": k_ms}
     step_bytes = 662 * 4 * g.nx * g.ny * g.nz
     step_ms = ms_max / a.steps
@@ -316,6 +345,9 @@ def run_ours(a):
         nbytes = sum(host[k].numel() * host[k].element_size() for k in E2E_FIELDS)
         e2e = {"value": job_rate(ke, e_ms, world), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": ke}
+        restart()
+    nan = int(nan_acc.item())
+    del init
 
     sur = None
     if world > 1:
@@ -345,10 +377,13 @@ def run_ours(a):
                                            "advance_uv, advance_mu_t, calc_coef_w, advance_w (implicit solve "
                                            "included) and calc_p_rho (pywrf_b200.adjoint), not yet for the "
                                            "forces, moisture, WSM6 or the step they compose"}}
+        line["valid"] = nan == 0
         print(json.dumps(line), flush=True)
     it._graph = None
     if world > 1:
         dist.destroy_process_group()
+    if nan:
+        raise SystemExit(f"NaN in the diagnosed pressure at {nan} point(s): the timed state is not a result")
 
 
 def hydrometeor_budget(st, g):

@@ -306,9 +306,10 @@ int wrf_wsm6(const WrfGrid* g, float* th, float* qv, float* qc, float* qr, float
  * its two intermediate fields live in a fixed file-scope device array of
  * 2 x 2,097,152 floats (16 MiB), enough for the block of a 240x240x41 grid.
  * Larger blocks, and delt >= 240 s (two time-split loops), return WRF_EINVAL.
- * The first call on a device looks up the array's address (make it before
- * any stream capture on that device); calls that overlap on the GPU share
- * the array and race. */
+ * The first call in each CUDA context looks up the array's address (make it
+ * before any stream capture on that device; after a device reset the next
+ * call looks it up again); calls that overlap on the GPU share the array and
+ * race. */
 int wrf_wsm6_noalloc(const WrfGrid* g, float* th, float* qv, float* qc, float* qr, float* qi, float* qs,
                      float* qg, const float* rho, const float* pii, const float* p, const float* dz8w,
                      float delt, float* rainnc, float* rainncv, float* snownc, float* snowncv,

@@ -15,6 +15,7 @@
 // Arithmetic is IEEE float32 in the reference's operation order; constant
 // sub-expressions the reference forms from python floats are formed in double
 // and rounded once, as the reference does.
+#include <cuda.h>
 #include <mutex>
 #include "kernels.cuh"
 #include "mlp.cuh"
@@ -1534,9 +1535,26 @@ int launch_wsm6(const Grid& g, float* const* f, float delt, cudaStream_t st) {
   return 1;
 }
 
-// The scratch's device address is looked up once per device, by the first
-// call on that device (cudaGetSymbolAddress, with the device current); that
-// first call should come before any stream capture on the device.
+// The scratch's device address is looked up by the first call in each CUDA
+// context (cudaGetSymbolAddress, with the context's device current) and kept
+// with that context's handle: after a device reset the new primary context
+// differs, and the address is looked up again.  The lookup should come before
+// any stream capture on the device.
+namespace {
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<CtxGetCurrentFn>(nullptr);
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+}  // namespace
+
 int launch_wsm6_noalloc(const Grid& g, float* const* f, float delt, cudaStream_t st, const char** err) {
   const int km = g.nz - 1;
   const int ncol = g.ide - 2 - (g.ids + 1), nrow = g.jde - 2 - (g.jds + 1);
@@ -1551,6 +1569,7 @@ int launch_wsm6_noalloc(const Grid& g, float* const* f, float delt, cudaStream_t
     return WRF_EINVAL;
   }
   constexpr int kMaxDev = 64;
+  static CUcontext owner[kMaxDev] = {};
   static float* scratch[kMaxDev] = {};
   static std::mutex setup;
   int dev = -1;
@@ -1558,17 +1577,26 @@ int launch_wsm6_noalloc(const Grid& g, float* const* f, float delt, cudaStream_t
     *err = "wrf_wsm6_noalloc: no current CUDA device (or device index >= 64)";
     return WRF_ECUDA;
   }
+  // the calling thread's current context (null before the runtime has bound
+  // the device's primary context to the thread: the symbol lookup binds it)
+  CUcontext ctx = nullptr;
+  const CtxGetCurrentFn get_ctx = ctx_get_current();
+  if (!get_ctx || get_ctx(&ctx) != CUDA_SUCCESS) {
+    *err = "wrf_wsm6_noalloc: cuCtxGetCurrent is not available from the driver";
+    return WRF_ECUDA;
+  }
   float* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(setup);
-    if (!scratch[dev]) {
+    if (!ctx || !scratch[dev] || owner[dev] != ctx) {
       void* ptr = nullptr;
       const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_wsm6_scratch);
-      if (rc != cudaSuccess || !ptr) {
+      if (rc != cudaSuccess || !ptr || (!ctx && (get_ctx(&ctx) != CUDA_SUCCESS || !ctx))) {
         *err = "wrf_wsm6_noalloc: cudaGetSymbolAddress of the scratch array failed";
         return WRF_ECUDA;
       }
       scratch[dev] = static_cast<float*>(ptr);
+      owner[dev] = ctx;
     }
     base = scratch[dev];
   }

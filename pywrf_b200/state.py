@@ -177,6 +177,16 @@ class DeviceState:
                 raise ValueError(f"{k}: shape {tuple(src.shape)} != {tuple(dst.shape)}")
             dst.copy_(src)
 
+    def snapshot(self) -> dict[str, torch.Tensor]:
+        """Device copies of every field (status words included)."""
+        return {k: v.clone() for k, v in self.t.items()}
+
+    def restore(self, snap: Mapping[str, torch.Tensor]) -> None:
+        """Copy a :meth:`snapshot` back in place: the storage, and with it
+        every pointer a captured step graph holds, stays the same."""
+        for k, v in snap.items():
+            self.t[k].copy_(v)
+
     def __getitem__(self, name: str) -> torch.Tensor:
         return self.t[name]
 

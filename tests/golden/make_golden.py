@@ -22,8 +22,16 @@ Writes, next to this script:
   and three distinct boundary records (``bdy_records``), so that step 3 runs
   on record 1 after the reference's reload (solver.py:457-703), in float64
   and float32.
+* ``c1_80_ref_sample.npz`` (``--only-c1-80``): the 240x240x41 workload after
+  80 steps (1 h) in float64 and float32.  A full state is ~170 MB, so the
+  fixture keeps, per compared field, the values of both runs at 16384 seeded
+  flat indices, the exact full-field norm and sum of the float64 run and the
+  exact full-field relative L2 of the float32 run against it (the
+  reference's own float32 error), and the dry-mass total (sum of mu + mub
+  over the mass points) of both runs and of the initial state.
 
-The reference is read from its source tree (default /root/reference); this
+The reference is read from the source tree named by ``--reference`` or the
+PYWRF_REFERENCE_ROOT environment variable (one of them is required); this
 script is the only producer of the fixtures and is never run by the tests.
 """
 from __future__ import annotations
@@ -78,6 +86,45 @@ def bdy_records(bdy, n=3):
 
 BDYREC = dict(nsteps=4, bdy_interval=2)
 
+LONG = dict(config=1, seed=0, nsteps=80, nsample=16384, sample_seed=80)
+
+
+def dry_mass(res, g):
+    """Sum of the column dry mass mu + mub over the mass points."""
+    R = (slice(g.jds, g.jde - 1), slice(g.ids, g.ide - 1))
+    return float((np.asarray(res["mu"], np.float64)[R] + np.asarray(res["mub"], np.float64)[R]).sum())
+
+
+def long_fixture(refharness):
+    spec = synthetic.spec_for_config(LONG["config"], seed=LONG["seed"])
+    g = synthetic.grid_for(spec)
+    inp, bdy = synthetic.build(spec)
+    r0 = refharness.run_reference(g, inp, bdy, 0, dtype="float64")
+    runs = {}
+    for dt in ("float64", "float32"):
+        res = refharness.run_reference(g, inp, bdy, LONG["nsteps"], dtype=dt)
+        runs[dt] = (pick(res), dry_mass(res, g))
+        print("ran", dt, flush=True)
+    f64, m64 = runs["float64"]
+    f32, m32 = runs["float32"]
+    rng = np.random.default_rng(LONG["sample_seed"])
+    out = {"mass0": np.array(dry_mass(r0, g)), "mass64": np.array(m64), "mass32": np.array(m32)}
+    for k in f64:
+        a64 = np.asarray(f64[k], np.float64)
+        a32 = np.asarray(f32[k], np.float64)
+        idx = rng.integers(0, a64.size, LONG["nsample"])
+        nrm = float(np.sqrt((a64 * a64).sum()))
+        out[f"{k}__idx"] = idx.astype(np.int64)
+        out[f"{k}__v64"] = a64.reshape(-1)[idx]
+        out[f"{k}__v32"] = a32.reshape(-1)[idx].astype(np.float32)
+        out[f"{k}__l2"] = np.array(nrm)
+        out[f"{k}__sum"] = np.array(float(a64.sum()))
+        out[f"{k}__floor"] = np.array(float(np.sqrt(((a32 - a64) ** 2).sum())) / (nrm if nrm > 0 else 1.0))
+        out[f"{k}__shape"] = np.array(a64.shape)
+    np.savez_compressed(os.path.join(HERE, "c1_80_ref_sample.npz"),
+                        meta=json.dumps({**LONG, "solver_sha256": refharness.SOLVER_SHA256}), **out)
+    print("wrote c1_80_ref_sample", {k[:-7]: float(v) for k, v in out.items() if k.endswith("__floor")})
+
 
 def bdyrec_case():
     import dataclasses
@@ -108,14 +155,21 @@ def thbias_loss(t, qv, target, g):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("PYWRF_REFERENCE_ROOT", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("PYWRF_REFERENCE_ROOT"))
     ap.add_argument("--skip-c1", action="store_true")
     ap.add_argument("--only-bdyrec", action="store_true", help="write small_bdyrec_ref64.npz only")
     ap.add_argument("--only-thbias", action="store_true", help="write thbias_ref64.npz only")
+    ap.add_argument("--only-c1-80", action="store_true", help="write c1_80_ref_sample.npz only")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("name the reference source tree with --reference or PYWRF_REFERENCE_ROOT")
     os.environ["PYWRF_REFERENCE_ROOT"] = args.reference
     import refharness
     refharness.REF_ROOT = args.reference
+
+    if args.only_c1_80:
+        long_fixture(refharness)
+        return
 
     if args.only_thbias:
         import dataclasses

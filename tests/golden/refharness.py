@@ -1,7 +1,8 @@
 """Run the reference PyWRF step on CPU from a synthetic state (fixture generation only).
 
-This module imports the reference package from a source tree (default
-``/root/reference``) and is used only to generate and check golden fixtures:
+This module imports the reference package from the source tree named by the
+PYWRF_REFERENCE_ROOT environment variable (or ``REF_ROOT`` set by the caller)
+and is used only to generate and check golden fixtures:
 nothing on the GPU path imports it.  What it does, following the reference's
 own structure:
 
@@ -28,7 +29,7 @@ import types
 
 import numpy as np
 
-REF_ROOT = os.environ.get("PYWRF_REFERENCE_ROOT", "/root/reference")
+REF_ROOT = os.environ.get("PYWRF_REFERENCE_ROOT")
 SOLVER_SHA256 = None  # filled on first load, reported with fixtures
 
 
@@ -66,6 +67,8 @@ def load_reference(grid, dtype="float32", device="cpu"):
     in one process."""
     import torch
 
+    if not REF_ROOT:
+        raise RuntimeError("set PYWRF_REFERENCE_ROOT to the reference's source tree")
     _install_stubs()
     for m in list(sys.modules):
         if m == "pywrf" or m.startswith("pywrf."):
