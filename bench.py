@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--phase-steps", type=int, default=3, help="eager steps timed per phase for the roofline")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the network (harvest, training, surrogate run)")
+    ap.add_argument("--no-config4", action="store_true", help="skip the 512x512x61 plain-step figure")
     ap.add_argument("--sur-seeds", type=int, default=5, help="integrations harvested for the network's training set")
     ap.add_argument("--sur-harvest-steps", type=int, default=80)
     ap.add_argument("--sur-epochs", type=int, default=200)
@@ -355,6 +356,10 @@ def run_ours(a):
     elif not a.no_surrogate:
         sur = run_surrogate(a, hbm)
 
+    big = None
+    if world == 1 and not a.no_config4:
+        big = run_config4(hbm)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         sec, sample = cpu_reference_step_time(a.config, 1, 0)
@@ -371,7 +376,7 @@ def run_ours(a):
                 "gpu_launches": launches * a.steps, "launches_per_step": launches,
                 "roofline": roofline, "step_roofline": whole, "phases_ms": phase_ms,
                 "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan,
-                "surrogate": sur,
+                "surrogate": sur, "config4": big,
                 "adjoint": {"unavailable": "no whole-step adjoint yet: hand-written reverse-mode kernels exist for "
                                            "advect_scalar, advect_u/v/w, relax_bdytend and the acoustic substep's "
                                            "advance_uv, advance_mu_t, calc_coef_w, advance_w (implicit solve "
@@ -384,6 +389,56 @@ def run_ours(a):
         dist.destroy_process_group()
     if nan:
         raise SystemExit(f"NaN in the diagnosed pressure at {nan} point(s): the timed state is not a result")
+
+
+def run_config4(hbm):
+    """The 512x512x61 workload (dt 30 s, one 36-step integration) with the
+    plain step: steps/s, grid-point updates/s, the step's ledger fraction of
+    the HBM peak, peak device memory and the NaN count."""
+    import torch
+    from pywrf_b200 import _native as N_
+    from pywrf_b200 import synthetic
+    from pywrf_b200.solver import Integrator
+    from pywrf_b200.state import DeviceState
+
+    spec = synthetic.spec_for_config(4)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats()
+    base = torch.cuda.memory_allocated()
+    st = DeviceState.from_inputs(g, inputs, bdy, device="cuda")
+    del inputs, bdy
+    it = Integrator(st)
+    init = st.snapshot()
+    it.capture()
+    for _ in range(3):
+        it.replay()
+    st.restore(init)
+    torch.cuda.synchronize()
+    stream = it._graph_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(spec.nsteps):
+            it._graph.replay()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / spec.nsteps
+    nan = it.status()["nan_p"]
+    n3 = g.nx * g.ny * g.nz
+    ledger = 662 * 4 * n3
+    peak = torch.cuda.max_memory_allocated() - base
+    it._graph = None
+    del init, st, it
+    torch.cuda.empty_cache()
+    return {"workload": f"{g.nx}x{g.ny}x{g.nz} synthetic moist ARW, plain WSM6, dt={spec.dt:g} s, "
+                        f"{spec.nsteps} steps from the initial state",
+            "steps_per_s": 1e3 / ms, "ms_per_step": ms, "grid_point_updates_per_s": 1e3 / ms * n3,
+            "step_roofline": {"ledger_bytes_per_step": ledger, "achieved_gbs": ledger / (ms / 1e3) / 1e9,
+                              "frac": ledger / (ms / 1e3) / 1e9 / hbm},
+            "peak_device_bytes": peak, "state_plus_snapshot": "the field table and one copy of it",
+            "nan_points": nan}
 
 
 def hydrometeor_budget(st, g):

@@ -60,3 +60,11 @@ def summary_errors(fields: dict[str, np.ndarray], summ: dict) -> dict[str, tuple
         l2 = float(np.sqrt((a * a).sum()))
         out[k] = (float(np.abs(a[idx] - v).max()) / scale, abs(l2 - s["l2"]) / max(s["l2"], 1e-30))
     return out
+
+
+def bdy_records(bdy, n=3):
+    """The boundary records of tests/golden/make_golden.py's boundary-record
+    case: record r scales the values by 1 + 0.002 r and the tendencies by
+    1 + 0.5 r."""
+    return {k: np.stack([np.asarray(v)[0] * ((1.0 + 0.5 * r) if "_BT" in k else (1.0 + 0.002 * r))
+                         for r in range(n)]).astype(np.asarray(v).dtype) for k, v in bdy.items()}

@@ -318,3 +318,55 @@ def test_advect_scalar_entry_point_matches_oracle(small):
     torch.cuda.synchronize()
     err, floor = rel_l2(tend.cpu().numpy(), ref64), rel_l2(ref32, ref64)
     assert err <= K_FLOOR * floor + 1e-9, (err, floor)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_boundary_record_reload_vs_reference_fp64(graph):
+    """Boundary interval of 2 steps and three distinct boundary records: the
+    reference reloads every boundary array from record 1 before step 3
+    (solver.py:457-703).  run_with_boundary_records does the same between
+    steps (in place, so the captured graph stays valid); after 4 steps the
+    fields are within 3x the reference's own fp32 error of its fp64 run."""
+    import dataclasses
+
+    from helpers import bdy_records
+    from pywrf_b200.solver import run_with_boundary_records
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = dataclasses.replace(synthetic.grid_for(spec), bdy_interval=2)
+    inputs, bdy = synthetic.build(spec)
+    recs = bdy_records(bdy)
+    st = DeviceState.from_inputs(g, inputs, recs, device="cuda")
+    it = Integrator(st)
+    run_with_boundary_records(it, g, recs, 4, graph=graph)
+    torch.cuda.synchronize()
+    r64, r32 = load_npz("small_bdyrec_ref64.npz"), load_npz("small_bdyrec_ref32.npz")
+    out = cuda_fields(st)
+    bad = []
+    for k in ("u", "v", "t", "ph", "mu", "qv"):
+        err, floor = rel_l2(out[k], r64[k]), rel_l2(r32[k], r64[k])
+        if not err <= K_FLOOR * floor + ABS_FLOOR:
+            bad.append((k, err, floor))
+    assert not bad, bad
+    assert it.status() == {"nan_p": 0, "step": 4, "wait_timeouts": 0}
+
+
+def test_61_levels_dt30_vs_oracle_fp64():
+    """The 512x512x61 workload's vertical grid and time step (nz = 61, dt =
+    30 s; WSM6 on 60 levels takes its 32-lane column segments) on a 28x28
+    horizontal grid: two steps within 3x the fp32 oracle's own error of the
+    fp64 oracle, field by field."""
+    spec = synthetic.CaseSpec(n=28, nz=61, dt=30.0, nsteps=2, bdy_tend_amp=1.0e-4, seed=7)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    st, it = cuda_run(g, inputs, bdy, 2, graph=True)
+    out = cuda_fields(st)
+    o64 = oracle_fields(g, inputs, bdy, np.float64, 2)
+    o32 = oracle_fields(g, inputs, bdy, np.float32, 2)
+    bad = []
+    for k in out:
+        err, floor = rel_l2(out[k], o64[k]), rel_l2(o32[k], o64[k])
+        if not err <= K_FLOOR * floor + ABS_FLOOR:
+            bad.append((k, err, floor))
+    assert not bad, bad
+    assert it.status() == {"nan_p": 0, "step": 2, "wait_timeouts": 0}
