@@ -169,13 +169,18 @@ class WrfSolver:
 
     def _load_datasets(self):
         """Open the input / boundary / reference WRF NetCDF files named by
-        PYWRF_DATA_DIR and PYWRF_RUN_NAME (pywrf/solver.py:22-46)."""
-        import xarray as xr   # I/O only; absent here unless installed
+        PYWRF_DATA_DIR and PYWRF_RUN_NAME (pywrf/solver.py:22-46): through
+        xarray when it is installed, else classic-format files through
+        :mod:`pywrf_b200.netcdf`."""
         data_dir = os.environ.get("PYWRF_DATA_DIR", "data")
         run = os.environ.get("PYWRF_RUN_NAME", "2024020106")
-        return (xr.open_dataset(os.path.join(data_dir, f"wrf_inout_step3_{run}")),
-                xr.open_dataset(os.path.join(data_dir, f"wrfbdy_d01_{run}")),
-                xr.open_dataset(os.path.join(data_dir, f"wrfout_d01_{run}")))
+        paths = [os.path.join(data_dir, f"{stem}_{run}") for stem in ("wrf_inout_step3", "wrfbdy_d01", "wrfout_d01")]
+        try:
+            import xarray as xr   # I/O only
+        except ImportError:
+            from .netcdf import open_dataset
+            return tuple(open_dataset(p) if os.path.exists(p) or i < 2 else None for i, p in enumerate(paths))
+        return tuple(xr.open_dataset(p) for p in paths)
 
     @staticmethod
     def _arrays(ds) -> Mapping[str, np.ndarray]:

@@ -3,8 +3,11 @@ same steps with the one-thread-per-point and cp.async forms (WRF_FORM_POINT,
 which also runs the boundary relaxation over every point instead of the
 boundary band): every field of the state must agree to the bit, since both
 forms perform the reference's operations in the same order.  Grids: 28x28x16 (partial tiles,
-boundary blocks only) and 108x108x41 (interior blocks on the branch-free
-paths, several level chunks per kernel)."""
+boundary blocks only), 108x108x41 (interior blocks on the branch-free
+paths, several level chunks per kernel) and 28x28x61 (four level slots per
+thread in the acoustic column kernels).  The fast form's acoustic column
+kernel stages its operands by tensor-map copies; the point form's loads them
+itself."""
 from __future__ import annotations
 
 import pytest
@@ -33,7 +36,8 @@ def _run(spec, form, nsteps):
     return st
 
 
-@pytest.mark.parametrize("n,nz,nsteps", [(28, 16, 2), (108, 41, 1)], ids=["28x28x16x2", "108x108x41x1"])
+@pytest.mark.parametrize("n,nz,nsteps", [(28, 16, 2), (108, 41, 1), (28, 61, 1)],
+                         ids=["28x28x16x2", "108x108x41x1", "28x28x61x1"])
 def test_tiled_kernels_equal_point_kernels_bitwise(n, nz, nsteps):
     if not torch.cuda.is_available():
         pytest.fail("this test needs a CUDA device")

@@ -216,3 +216,45 @@ def test_boundary_record_schedule_follows_the_reference_loop():
     run_with_boundary_records(it, g, bdy, 10)
     # steps 1-4 on record 0, record 1 loaded before step 5, record 2 before step 9
     assert it.log == [(1, 0), (5, 1), (9, 2)] and it.steps == 10
+
+
+def test_classic_netcdf_files_feed_the_solver_without_xarray(tmp_path, monkeypatch):
+    """The synthetic case written as the three WRF files in the classic
+    NetCDF format (pywrf_b200.netcdf.write_dataset) is read back by
+    WrfSolver._load_datasets when xarray is absent, array for array, and the
+    state ingested from the files equals the one ingested from the arrays."""
+    import sys
+
+    from pywrf_b200 import netcdf
+    from pywrf_b200.solver import WrfSolver
+
+    spec = synthetic.CaseSpec(**SMALL)
+    inputs, bdy = synthetic.build(spec)
+    run = "test"
+    netcdf.write_dataset(str(tmp_path / f"wrf_inout_step3_{run}"), inputs)
+    netcdf.write_dataset(str(tmp_path / f"wrfbdy_d01_{run}"), bdy)
+    monkeypatch.setenv("PYWRF_DATA_DIR", str(tmp_path))
+    monkeypatch.setenv("PYWRF_RUN_NAME", run)
+    monkeypatch.setitem(sys.modules, "xarray", None)   # import xarray raises ImportError
+    ds_in, ds_bdy, ds_ref = WrfSolver(device="cpu")._load_datasets()
+    assert ds_ref is None
+    for src, ds in ((inputs, ds_in), (bdy, ds_bdy)):
+        assert set(src) == set(ds)
+        for k, v in src.items():
+            assert ds[k].shape == v.shape and ds[k].dtype == np.float32, k
+            assert np.array_equal(ds[k], v), k
+    g = synthetic.grid_for(spec)
+    a, sa = ingest(g, inputs, bdy)
+    b, sb = ingest(g, WrfSolver._arrays(ds_in), WrfSolver._arrays(ds_bdy))
+    assert sa == sb and set(a) == set(b)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_netcdf4_files_are_refused_with_a_reason(tmp_path):
+    from pywrf_b200 import netcdf
+
+    p = tmp_path / "f.nc"
+    p.write_bytes(b"\x89HDF\r\n\x1a\n" + bytes(64))
+    with pytest.raises(ValueError, match="NetCDF-4"):
+        netcdf.open_dataset(str(p))
