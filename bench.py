@@ -6,20 +6,30 @@ One step = one complete ``wrf_rk3_step`` (three RK stages, 1+2+4 acoustic
 substeps, moisture transport, WSM6, boundary updates) over the 240x240x41
 state built by :mod:`pywrf_b200.synthetic` (the 240x240x41 / dt 45 s / 80-step
 workload with seeded boundary tendencies), replayed from one captured CUDA
-graph.  The timed region is bracketed by barrier + synchronize; the device
-time is measured with CUDA events on the replay stream and the maximum over
-ranks is reported.  Multi-GPU runs are independent replicas (different seeds,
-no data-path collective): the step is column-local but its lateral boundary
-is one domain, so ``value`` = N * K / max-rank time ("weak" scaling).
+graph.  The workload is a 1-h integration: K steps run as integrations of at
+most 80 steps, each from the initial state (its seeded boundary tendencies
+drive the forced boundary state unstable after ~175 steps); the restore lies
+between timed segments and the NaN count of every integration is kept, a NaN
+making the run exit non-zero.  The timed region is bracketed by barrier +
+synchronize; the device time is measured with CUDA events on the replay
+stream and the maximum over ranks is reported.  Multi-GPU runs are
+independent replicas (different seeds, no data-path collective): the step is
+column-local but its lateral boundary is one domain, so ``value`` = N * K /
+max-rank time ("weak" scaling).
 
 Extra keys of the JSON line:
   roofline      the dominant kernel's algorithmic bytes / CUDA-event duration
                 against the measured HBM copy bandwidth
+  step_roofline the whole step's 662-pass ledger against the same peak
   phases        per-phase device time of one eager step (probe events)
   e2e           the same metric through the public API with host buffers:
                 pinned H2D of the prognostic state, one step, D2H of it back
   cpu_baseline  the numpy oracle (a restatement of the reference's CPU path)
                 timed on this host for one step of the same workload
+  reference_cpu the unmodified reference's own CPU step, recorded where its
+                source lives (tests/golden/reference_cpu_timing.json)
+  config4       the 512x512x61 workload's plain step (36 steps): steps/s,
+                ledger fraction, peak device memory
   clocks        SM clock samples taken during the timed region
   surrogate     the per-column network in place of WSM6: trained on the GPU
                 on harvested WSM6 increments, then one unseen state run for
@@ -162,6 +172,23 @@ def cpu_reference_step_time(config: int, nsteps: int, warmup: int):
         m.step(m.step_count + 1)
     dt = (time.perf_counter() - t0) / nsteps
     return dt, f"{nsteps} RK3 step(s) of the {g.nx}x{g.ny}x{g.nz} workload, numpy fp32 oracle, 1 thread"
+
+
+def reference_cpu_record(grid_key: str):
+    """The unmodified reference's own CPU step on this workload, as timed by
+    tests/golden/time_reference_cpu.py where the reference's source lives (a
+    recorded measurement of another machine, not of this run)."""
+    p = os.path.join(ROOT, "tests", "golden", "reference_cpu_timing.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        w = d["workloads"][grid_key]
+    except (OSError, KeyError, ValueError):
+        return None
+    return {"value": w["steps_per_s"], "unit": UNIT, "cores": d["threads"], "kind": "reference",
+            "machine": f"{d['cpu']} ({d['logical_cpus']} logical CPUs), torch {d['torch']}, {d['dtype']}",
+            "sample": f"{w['timed_steps']} timed step(s) after {w['warmup_steps']} warm-up",
+            "recorded_in": "tests/golden/reference_cpu_timing.json (not measured in this run)"}
 
 
 def run_reference(a):
@@ -377,6 +404,7 @@ def run_ours(a):
                 "roofline": roofline, "step_roofline": whole, "phases_ms": phase_ms,
                 "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan,
                 "surrogate": sur, "config4": big,
+                "reference_cpu": reference_cpu_record(f"{g.nx}x{g.ny}x{g.nz}"),
                 "adjoint": {"unavailable": "no whole-step adjoint yet: hand-written reverse-mode kernels exist for "
                                            "advect_scalar, advect_u/v/w, relax_bdytend and the acoustic substep's "
                                            "advance_uv, advance_mu_t, calc_coef_w, advance_w (implicit solve "

@@ -196,6 +196,59 @@ int wrf_advect_scalar_adj(const WrfGrid* g, const float* field, const float* ru,
  * cqu, cqv, mudf, msfux, msfuy, msfvx, msfvx_inv, msfvy, fnm, fnp, rdnw and
  * the grid's emdiv, cf1..cf3 (spec_zone 1); fields it does not read may be
  * null.  Runs the kernel of the form wrf_set_kernel_form selects. */
+/* wrf_dynamics.py:2031-2620 the large-step tendency terms selected by the
+ * mask `terms` (1 rhs_ph, 2 horizontal_pressure_gradient, 4 pg_buoy_w, 8
+ * coriolis, 16 curvature) on the state table, with the solver's arguments:
+ * adds to ph_tend, ru_tend, rv_tend, rw_tend; pg_buoy_w also replaces cqw by
+ * 1 / (1 + cqw) on levels 1 .. nz-2 of the mass points (wrf_dynamics.py:2453).
+ * The step itself runs these terms fused in one tiled kernel. */
+int wrf_forces(const WrfGrid* g, const WrfState* s, int terms, void* stream);
+/* Its adjoint: sbar's PH_TEND, RU_TEND, RV_TEND, RW_TEND and CQW hold the
+ * cotangents of the updated fields and are rewritten to those of the inputs
+ * (the tendencies' pass through, except ph_tend's top level, which rhs_ph
+ * sets); the cotangents of u, v, w, ww, ph, phb, mut, muu, muv, alt, p, pb,
+ * al, php, cqu, cqv, mu, mub, ru, rv and rw are accumulated (+=), all
+ * required.  Accumulation order is not fixed (atomic adds). */
+int wrf_forces_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, int terms, void* stream);
+/* wrf_dynamics.py:3799-3839 sumflux on the state table, with the solver's
+ * arguments: u, v, ww, u_save, v_save, ww1, muu, muv, msfuy, msfvx_inv;
+ * updates ru_m, rv_m, ww_m (zeroed first at iteration 1, averaged at
+ * iteration nsub).  The step fuses it into its acoustic column kernel. */
+int wrf_sumflux(const WrfGrid* g, const WrfState* s, int iteration, int nsub, void* stream);
+/* Its adjoint: sbar's RU_M, RV_M, WW_M hold the cotangents of the updated
+ * sums and are rewritten to those of the incoming sums; those of u, v, ww,
+ * u_save, v_save, ww1, muu, muv are accumulated (+=). */
+int wrf_sumflux_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, int iteration, int nsub,
+                    void* stream);
+/* wrf_boundary.py:244-294 spec_bdyupdate: field += dt * tend on the
+ * specified rows of stagger var ('t', 'u', 'v': [nz][ny][nx] fields, levels
+ * below nz-1; 'm': [ny][nx]). */
+int wrf_spec_bdyupdate(const WrfGrid* g, float* field, const float* tend, float dt, char var, void* stream);
+/* Its adjoint: tend_bar += dt * field_bar on those rows (the field's own
+ * cotangent passes through). */
+int wrf_spec_bdyupdate_adj(const WrfGrid* g, const float* field_bar, float* tend_bar, float dt, char var,
+                           void* stream);
+/* wrf_boundary.py:297-355 spec_bdyupdate_ph on the state table (ph, ph_save,
+ * ph_tend, mu_tend, muts): the specified rows of ph with the mass
+ * re-weighting mu_old = muts - dt * mu_tend, all levels. */
+int wrf_spec_bdyupdate_ph(const WrfGrid* g, const WrfState* s, float dt, void* stream);
+/* Its adjoint: sbar's PH holds the cotangent of the updated ph and is
+ * rewritten to that of the incoming ph; those of ph_save, ph_tend, mu_tend
+ * and muts are accumulated (+=). */
+int wrf_spec_bdyupdate_ph_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float dt, void* stream);
+/* wrf_dynamics.py:30-159 rk_step_prep's functions selected by the mask ops
+ * (1 calculate_full, 2 calc_mu_uv, 4 couple_momentum, 8 calc_ww_cp, 16
+ * calc_cq, 32 calc_alt, 64 calc_php), in that order, on the state table with
+ * the solver's arguments (couple_momentum divides by msfu and msft, calc_cq
+ * sums all seven moisture slots; c1h, dnw, msftx, msfuy, msfvx_inv).  The
+ * step computes them fused in its prep kernels. */
+int wrf_prep(const WrfGrid* g, const WrfState* s, int ops, void* stream);
+/* Its adjoint: the cotangents of the outputs (mut, muu, muv, ru, rv, rw,
+ * ww levels 1 .. nz-2, cqu, cqv, cqw, alt, php) are read on each function's
+ * region and set to zero there (the functions overwrite them); those of the
+ * inputs (mu, mub, u, v, w, ww level 0, moist, al, alb, ph, phb, and muu,
+ * muv, mut where a later function reads them) are accumulated (+=). */
+int wrf_prep_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, int ops, void* stream);
 int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream);
 /* Its adjoint (reverse mode): sbar holds, under the same field ids, the
  * cotangents of the updated u and v (which are also those of the incoming

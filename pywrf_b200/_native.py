@@ -112,6 +112,26 @@ def lib() -> ctypes.CDLL:
     L.wrf_calc_p_rho_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_int, vp]
     L.wrf_advance_uv.restype = ip
     L.wrf_advance_uv.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_float, vp]
+    L.wrf_forces.restype = ip
+    L.wrf_forces.argtypes = [ctypes.POINTER(WrfGridC), vp, ip, vp]
+    L.wrf_forces_adj.restype = ip
+    L.wrf_forces_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ip, vp]
+    L.wrf_sumflux.restype = ip
+    L.wrf_sumflux.argtypes = [ctypes.POINTER(WrfGridC), vp, ip, ip, vp]
+    L.wrf_sumflux_adj.restype = ip
+    L.wrf_sumflux_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ip, ip, vp]
+    L.wrf_spec_bdyupdate.restype = ip
+    L.wrf_spec_bdyupdate.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, ctypes.c_char, vp]
+    L.wrf_spec_bdyupdate_adj.restype = ip
+    L.wrf_spec_bdyupdate_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, ctypes.c_char, vp]
+    L.wrf_spec_bdyupdate_ph.restype = ip
+    L.wrf_spec_bdyupdate_ph.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_float, vp]
+    L.wrf_spec_bdyupdate_ph_adj.restype = ip
+    L.wrf_spec_bdyupdate_ph_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, vp]
+    L.wrf_prep.restype = ip
+    L.wrf_prep.argtypes = [ctypes.POINTER(WrfGridC), vp, ip, vp]
+    L.wrf_prep_adj.restype = ip
+    L.wrf_prep_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ip, vp]
     L.wrf_advance_uv_adj.restype = ip
     L.wrf_advance_uv_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, vp]
     L.wrf_advect_momentum_adj.restype = ip

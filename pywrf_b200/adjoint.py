@@ -27,6 +27,17 @@ operators keeps no tape of the forward's intermediates.
 * :class:`AdvanceW` -- advance_w (pywrf/wrf_dynamics.py:3641-3796): the
   vertically implicit w / phi update with its terrain lower boundary and
   Rayleigh damping; gradients with respect to its 23 array inputs.
+* :class:`Forces` -- the large-step tendency terms rhs_ph,
+  horizontal_pressure_gradient, pg_buoy_w, coriolis and curvature
+  (pywrf/wrf_dynamics.py:2031-2620), any subset by a mask; gradients with
+  respect to the incoming tendencies, cqw (which pg_buoy_w overwrites) and the
+  21 state arrays they read.
+* :class:`Sumflux`, :class:`SpecUpdate`, :class:`SpecUpdatePh` -- sumflux
+  (pywrf/wrf_dynamics.py:3799-3839), spec_bdyupdate and spec_bdyupdate_ph
+  (pywrf/wrf_boundary.py:244-355), the rest of the acoustic substep.
+* :class:`Prep` -- rk_step_prep's functions calculate_full, calc_mu_uv,
+  couple_momentum, calc_ww_cp, calc_cq, calc_alt, calc_php
+  (pywrf/wrf_dynamics.py:30-159), any subset by a mask.
 * :class:`RelaxBdytend` -- ``tendency + relax(field)`` toward the lateral
   boundary values (pywrf/wrf_boundary.py:52-147); gradients with respect to
   the field and the incoming tendency (the boundary arrays are data).
@@ -216,6 +227,232 @@ def advance_uv(inputs: dict, data: dict, dts, emdiv, cf1, cf2, cf3, rdx, rdy):
     ``inputs`` maps UV_INPUTS, ``data`` UV_DATA to tensors; returns (u', v')."""
     return AdvanceUV.apply((dts, emdiv, cf1, cf2, cf3, rdx, rdy), *[inputs[k] for k in UV_INPUTS],
                            *[data[k] for k in UV_DATA])
+
+
+FORCES_OUTPUTS = ("ph_tend", "ru_tend", "rv_tend", "rw_tend", "cqw")
+FORCES_INPUTS = FORCES_OUTPUTS + ("u", "v", "w", "ww", "ph", "phb", "mut", "muu", "muv", "alt", "p", "pb", "al",
+                                  "php", "cqu", "cqv", "mu", "mub", "ru", "rv", "rw")
+FORCES_DATA = ("msfux", "msfuy", "msfvx", "msfvy", "msftx", "msfty", "f", "e", "sina", "cosa", "fnm", "fnp", "rdnw",
+               "rdn")
+FORCES_TERMS = {"rhs_ph": 1, "hpg": 2, "pg_buoy_w": 4, "coriolis": 8, "curvature": 16}
+
+
+class Forces(torch.autograd.Function):
+    """(ph_tend', ru_tend', rv_tend', rw_tend', cqw') = the tendency terms of
+    the mask ``terms`` (rhs_ph 1, horizontal_pressure_gradient 2, pg_buoy_w 4,
+    coriolis 8, curvature 16) added to the incoming tendencies; the tensors
+    follow FORCES_INPUTS then FORCES_DATA, ``scal`` = (terms, rdx, rdy, cf1,
+    cf2, cf3, cfn, cfn1)."""
+
+    @staticmethod
+    def forward(ctx, scal, *tensors):
+        _cuda_only(*tensors)
+        terms = int(scal[0])
+        rdx, rdy, cf1, cf2, cf3, cfn, cfn1 = (float(x) for x in scal[1:])
+        named = dict(zip(FORCES_INPUTS + FORCES_DATA, tensors))
+        cg = scalar_grid(named["u"].shape, rdx, rdy)
+        cg.cf1, cg.cf2, cg.cf3, cg.cfn, cg.cfn1 = cf1, cf2, cf3, cfn, cfn1
+        outs = {k: named[k].detach().clone() for k in FORCES_OUTPUTS}
+        tab = _table({**named, **outs})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(outs["ph_tend"].device):
+            rc = N.lib().wrf_forces(ctypes.byref(cg), tab, terms, stream)
+        N.check(rc, "wrf_forces")
+        ctx.save_for_backward(*tensors)
+        ctx.cg, ctx.terms = cg, terms
+        return tuple(outs[k] for k in FORCES_OUTPUTS)
+
+    @staticmethod
+    def backward(ctx, *gouts):
+        tensors = ctx.saved_tensors
+        named = dict(zip(FORCES_INPUTS + FORCES_DATA, tensors))
+        bars = {k: (torch.zeros_like(named[k]) if g is None else g.contiguous().clone())
+                for k, g in zip(FORCES_OUTPUTS, gouts)}
+        bars.update({k: torch.zeros_like(named[k]) for k in FORCES_INPUTS[len(FORCES_OUTPUTS):]})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(bars["u"].device):
+            rc = N.lib().wrf_forces_adj(ctypes.byref(ctx.cg), _table(named), _table(bars), ctx.terms, stream)
+        N.check(rc, "wrf_forces_adj")
+        return (None,) + tuple(bars[k] for k in FORCES_INPUTS) + (None,) * len(FORCES_DATA)
+
+
+def forces(inputs: dict, data: dict, terms, rdx, rdy, cf1, cf2, cf3, cfn, cfn1):
+    """Differentiable tendency terms on the GPU: ``inputs`` maps
+    FORCES_INPUTS, ``data`` FORCES_DATA to tensors; ``terms`` is a mask or a
+    sequence of FORCES_TERMS names; returns (ph_tend', ru_tend', rv_tend',
+    rw_tend', cqw')."""
+    if not isinstance(terms, int):
+        terms = sum(FORCES_TERMS[t] for t in terms)
+    return Forces.apply((terms, rdx, rdy, cf1, cf2, cf3, cfn, cfn1), *[inputs[k] for k in FORCES_INPUTS],
+                        *[data[k] for k in FORCES_DATA])
+
+
+SF_INPUTS = ("ru_m", "rv_m", "ww_m", "u", "v", "ww", "u_save", "v_save", "ww1", "muu", "muv")
+SF_DATA = ("msfuy", "msfvx_inv")
+
+
+class Sumflux(torch.autograd.Function):
+    """(ru_m', rv_m', ww_m') = sumflux at ``iteration`` of ``nsub``; the
+    tensors follow SF_INPUTS then SF_DATA, ``scal`` = (iteration, nsub, rdx,
+    rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, *tensors):
+        _cuda_only(*tensors)
+        iteration, nsub = int(scal[0]), int(scal[1])
+        named = dict(zip(SF_INPUTS + SF_DATA, tensors))
+        cg = scalar_grid(named["u"].shape, float(scal[2]), float(scal[3]))
+        outs = {k: named[k].detach().clone() for k in SF_INPUTS[:3]}
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(named["u"].device):
+            rc = N.lib().wrf_sumflux(ctypes.byref(cg), _table({**named, **outs}), iteration, nsub, stream)
+        N.check(rc, "wrf_sumflux")
+        ctx.save_for_backward(*tensors)
+        ctx.cg, ctx.it = cg, (iteration, nsub)
+        return tuple(outs[k] for k in SF_INPUTS[:3])
+
+    @staticmethod
+    def backward(ctx, *gouts):
+        named = dict(zip(SF_INPUTS + SF_DATA, ctx.saved_tensors))
+        bars = {k: (torch.zeros_like(named[k]) if g is None else g.contiguous().clone())
+                for k, g in zip(SF_INPUTS[:3], gouts)}
+        bars.update({k: torch.zeros_like(named[k]) for k in SF_INPUTS[3:]})
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(bars["u"].device):
+            rc = N.lib().wrf_sumflux_adj(ctypes.byref(ctx.cg), _table(named), _table(bars), ctx.it[0], ctx.it[1],
+                                         stream)
+        N.check(rc, "wrf_sumflux_adj")
+        return (None,) + tuple(bars[k] for k in SF_INPUTS) + (None,) * len(SF_DATA)
+
+
+def sumflux(inputs: dict, data: dict, iteration: int, nsub: int, rdx, rdy):
+    """Differentiable sumflux on the GPU; returns (ru_m', rv_m', ww_m')."""
+    return Sumflux.apply((iteration, nsub, rdx, rdy), *[inputs[k] for k in SF_INPUTS], *[data[k] for k in SF_DATA])
+
+
+class SpecUpdate(torch.autograd.Function):
+    """field' = spec_bdyupdate(field, tend, dt, var) (var 't', 'u', 'v' or
+    'm'); ``scal`` = (dt, var, rdx, rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, field, tend):
+        _cuda_only(field, tend)
+        dt, var = float(scal[0]), str(scal[1])
+        shape = field.shape if field.dim() == 3 else (12,) + tuple(field.shape)
+        cg = scalar_grid(shape, float(scal[2]), float(scal[3]))
+        out = field.detach().clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(field.device):
+            rc = N.lib().wrf_spec_bdyupdate(ctypes.byref(cg), _ptr(out), _ptr(tend), dt, var.encode(), stream)
+        N.check(rc, "wrf_spec_bdyupdate")
+        ctx.cg, ctx.dt, ctx.var = cg, dt, var
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        gout = gout.contiguous()
+        tb = torch.zeros_like(gout)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(gout.device):
+            rc = N.lib().wrf_spec_bdyupdate_adj(ctypes.byref(ctx.cg), _ptr(gout), _ptr(tb), ctx.dt, ctx.var.encode(),
+                                                stream)
+        N.check(rc, "wrf_spec_bdyupdate_adj")
+        return None, gout, tb
+
+
+def spec_bdyupdate(field, tend, dt, var: str, rdx, rdy):
+    """Differentiable spec_bdyupdate on the GPU."""
+    return SpecUpdate.apply((dt, var, rdx, rdy), field, tend)
+
+
+SPH_INPUTS = ("ph", "ph_save", "ph_tend", "mu_tend", "muts")
+
+
+class SpecUpdatePh(torch.autograd.Function):
+    """ph' = spec_bdyupdate_ph(ph_save, ph, ph_tend, mu_tend, muts, dt); the
+    tensors follow SPH_INPUTS, ``scal`` = (dt, rdx, rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, *tensors):
+        _cuda_only(*tensors)
+        named = dict(zip(SPH_INPUTS, tensors))
+        cg = scalar_grid(named["ph"].shape, float(scal[1]), float(scal[2]))
+        out = named["ph"].detach().clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(out.device):
+            rc = N.lib().wrf_spec_bdyupdate_ph(ctypes.byref(cg), _table({**named, "ph": out}), float(scal[0]), stream)
+        N.check(rc, "wrf_spec_bdyupdate_ph")
+        ctx.save_for_backward(*tensors)
+        ctx.cg, ctx.dt = cg, float(scal[0])
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        named = dict(zip(SPH_INPUTS, ctx.saved_tensors))
+        bars = {k: torch.zeros_like(named[k]) for k in SPH_INPUTS}
+        bars["ph"] = gout.contiguous().clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(gout.device):
+            rc = N.lib().wrf_spec_bdyupdate_ph_adj(ctypes.byref(ctx.cg), _table(named), _table(bars), ctx.dt, stream)
+        N.check(rc, "wrf_spec_bdyupdate_ph_adj")
+        return (None,) + tuple(bars[k] for k in SPH_INPUTS)
+
+
+def spec_bdyupdate_ph(inputs: dict, dt, rdx, rdy):
+    """Differentiable spec_bdyupdate_ph on the GPU; ``inputs`` maps SPH_INPUTS."""
+    return SpecUpdatePh.apply((dt, rdx, rdy), *[inputs[k] for k in SPH_INPUTS])
+
+
+PREP_FIELDS = ("mu", "mub", "mut", "muu", "muv", "u", "v", "w", "ru", "rv", "rw", "ww", "moist", "cqu", "cqv",
+               "cqw", "al", "alb", "alt", "ph", "phb", "php")
+PREP_OUTPUTS = ("mut", "muu", "muv", "ru", "rv", "rw", "ww", "cqu", "cqv", "cqw", "alt", "php")
+PREP_DATA = ("msfu", "msfvx_inv", "msft", "msftx", "msfuy", "dnw", "c1h")
+PREP_OPS = {"calculate_full": 1, "calc_mu_uv": 2, "couple_momentum": 4, "calc_ww_cp": 8, "calc_cq": 16,
+            "calc_alt": 32, "calc_php": 64}
+
+
+class Prep(torch.autograd.Function):
+    """PREP_OUTPUTS' = rk_step_prep's functions of the mask ``ops`` (the
+    others pass through); the tensors follow PREP_FIELDS then PREP_DATA,
+    ``scal`` = (ops, rdx, rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, *tensors):
+        _cuda_only(*tensors)
+        ops = int(scal[0])
+        named = dict(zip(PREP_FIELDS + PREP_DATA, tensors))
+        cg = scalar_grid(named["u"].shape, float(scal[1]), float(scal[2]))
+        outs = {k: named[k].detach().clone() for k in PREP_OUTPUTS}
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(named["u"].device):
+            rc = N.lib().wrf_prep(ctypes.byref(cg), _table({**named, **outs}), ops, stream)
+        N.check(rc, "wrf_prep")
+        ctx.save_for_backward(*tensors)
+        ctx.cg, ctx.ops = cg, ops
+        return tuple(outs[k] for k in PREP_OUTPUTS)
+
+    @staticmethod
+    def backward(ctx, *gouts):
+        named = dict(zip(PREP_FIELDS + PREP_DATA, ctx.saved_tensors))
+        bars = {k: torch.zeros_like(named[k]) for k in PREP_FIELDS}
+        for k, gr in zip(PREP_OUTPUTS, gouts):
+            if gr is not None:
+                bars[k] = gr.contiguous().clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(bars["u"].device):
+            rc = N.lib().wrf_prep_adj(ctypes.byref(ctx.cg), _table(named), _table(bars), ctx.ops, stream)
+        N.check(rc, "wrf_prep_adj")
+        return (None,) + tuple(bars[k] for k in PREP_FIELDS) + (None,) * len(PREP_DATA)
+
+
+def prep(fields: dict, data: dict, ops, rdx, rdy):
+    """Differentiable rk_step_prep functions on the GPU: ``fields`` maps
+    PREP_FIELDS, ``data`` PREP_DATA; ``ops`` a mask or PREP_OPS names; returns
+    a dict of PREP_OUTPUTS."""
+    if not isinstance(ops, int):
+        ops = sum(PREP_OPS[o] for o in ops)
+    outs = Prep.apply((ops, rdx, rdy), *[fields[k] for k in PREP_FIELDS], *[data[k] for k in PREP_DATA])
+    return dict(zip(PREP_OUTPUTS, outs))
 
 
 AW_INPUTS = ("w", "rw_tend", "ww", "w_save", "u", "v", "muave", "muts", "mut", "t_2ave", "t_2", "t_1", "ph", "ph_1",

@@ -217,6 +217,56 @@ __global__ void __launch_bounds__(kCwTX * kCwKT) k_coef_w(Grid g, S s, float dts
   }
 }
 
+// calc_coef_w with one thread per mass column (32 x 4 columns per block): the
+// coefficients of level k are formed as the recurrence reaches it, so nothing
+// waits on a block barrier and every level's loads and stores are coalesced
+// across the warp.  The same operations as k_coef_w, in the same order (the
+// divisions by mut^2 and the reciprocals in their correctly rounded forms).
+__global__ void __launch_bounds__(128) k_coef_w_col(Grid g, S s, float dts) {
+  const int i = g.ids + blockIdx.x * 32 + threadIdx.x, j = g.jds + blockIdx.y * 4 + threadIdx.y;
+  if (i >= g.ide - 1 || j >= g.jde - 1) return;
+  const int nz = g.nz;
+  const int c = g.i2(j, i);
+  const size_t lev = (size_t)g.ny * g.nx;
+  const double cofd = (0.5 * (double)dts * G * (1.0 + (double)g.epssm)) * (0.5 * (double)dts * G * (1.0 + (double)g.epssm));
+  const float cof = (float)cofd, cofm2 = (float)(-2.0 * cofd), cof2 = (float)(2.0 * cofd);
+  const float* cqw = s[WF_CQW];
+  const float* c2a = s[WF_C2A];
+  const float* rdn = s[WF_RDN];
+  const float* rdnw = s[WF_RDNW];
+  float* a = s[WF_A];
+  float* alpha = s[WF_ALPHA];
+  float* gamma = s[WF_GAMMA];
+  const float mut = s[WF_MUT][c];
+  const float mm = mut * mut, r_mm = __frcp_rn(mm);
+  gamma[c] = 0.f;
+  float gm = 0.f;
+  float c2m = __ldg(&c2a[c]);
+#pragma unroll 4
+  for (int k = 1; k < nz - 1; ++k) {
+    const size_t p = k * lev + c;
+    const float cw = __ldg(&cqw[p]), c2k = __ldg(&c2a[p]);
+    const float rk = __ldg(&rdn[k]), rwk = __ldg(&rdnw[k]), rwm = __ldg(&rdnw[k - 1]);
+    const float ak = k >= 2 ? divc(-cw * cof * rk * rwm * c2m, mm, r_mm) : 0.f;
+    const float bk = 1.0f + cw * cof * rk * (divc(rwk * c2k, mm, r_mm) + divc(rwm * c2m, mm, r_mm));
+    const float ck = divc(-cw * cof * rk * rwk * c2k, mm, r_mm);
+    const float al = __frcp_rn(bk - ak * gm);
+    gm = ck * al;
+    a[p] = ak;
+    alpha[p] = al;
+    gamma[p] = gm;
+    c2m = c2k;
+  }
+  const float lid = g.top_lid ? 0.f : 1.f;
+  const float rwt = __ldg(&rdnw[nz - 2]);
+  const float atop = divc(cofm2 * (rwt * rwt) * c2m * lid, mm, r_mm);
+  const float btop = 1.0f + divc(cof2 * (rwt * rwt) * c2m, mm, r_mm);
+  const size_t pt = (size_t)(nz - 1) * lev + c;
+  a[pt] = atop;
+  alpha[pt] = __frcp_rn(btop - atop * gm);
+  gamma[pt] = 0.f;
+}
+
 __global__ void k_advance_uv(Grid g, S s, float dts) {
   WRF_POINT_INDEX(g, k, j, i);
   const int nz = g.nz, ktf = nz - 1, nx = g.nx;
@@ -1074,7 +1124,12 @@ int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cu
   k_ssp2d<<<col_grid(g, b2), b2, 0, st>>>(g, s, rk_step);
   k_ssp3d<<<point_grid(g, b3), b3, 0, st>>>(g, s, rk_step);
   k_p_rho0<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  k_coef_w<<<dim3((g.ide - 1 - g.ids + kCwTX - 1) / kCwTX, g.jde - 1 - g.jds), kCwTX * kCwKT, 0, st>>>(g, s, dts);
+  if (kernel_form() == WRF_FORM_FAST) {
+    const dim3 bc(32, 4);
+    k_coef_w_col<<<dim3((g.ide - 1 - g.ids + 31) / 32, (g.jde - 1 - g.jds + 3) / 4), bc, 0, st>>>(g, s, dts);
+  } else {
+    k_coef_w<<<dim3((g.ide - 1 - g.ids + kCwTX - 1) / kCwTX, g.jde - 1 - g.jds), kCwTX * kCwKT, 0, st>>>(g, s, dts);
+  }
   return 4;
 }
 

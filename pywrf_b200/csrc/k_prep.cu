@@ -167,6 +167,50 @@ __global__ void __launch_bounds__(kWwTX * kWwKT) k_ww_cp(Grid g, S s) {
     for (int k = 1 + tk; k < ktf; k += kWwKT) ww[k * lev + c] = sww[k][tx];
 }
 
+// calc_ww_cp with one thread per mass column (32 x 4 columns per block): the
+// column's divergences stay in registers (the level loop is unrolled to the
+// 64-level limit and predicated), the column sum and the upward scan run in
+// the reference's order; neighbouring threads' columns make every level's
+// loads and stores coalesced.  Same operations as k_ww_cp (the divisions by
+// the map factors in their correctly rounded reciprocal form).
+__global__ void __launch_bounds__(128) k_ww_cp_col(Grid g, S s) {
+  const int i = g.ids + blockIdx.x * 32 + threadIdx.x, j = g.jds + blockIdx.y * 4 + threadIdx.y;
+  if (i >= g.ide - 1 || j >= g.jde - 1) return;
+  const int ktf = g.nz - 1;
+  const int c = g.i2(j, i), ce = c + 1, cn = c + g.nx;
+  const float* u = s[WF_U];
+  const float* v = s[WF_V];
+  const float* dnw = s[WF_DNW];
+  const float* c1h = s[WF_C1H];
+  const size_t lev = (size_t)g.ny * g.nx;
+  const float muu0 = s[WF_MUU][c], muu1 = s[WF_MUU][ce], mfu0 = s[WF_MSFUY][c], mfu1 = s[WF_MSFUY][ce];
+  const float muv0 = s[WF_MUV][c], muv1 = s[WF_MUV][cn], mfv0 = s[WF_MSFVX_INV][c], mfv1 = s[WF_MSFVX_INV][cn];
+  const float r_mfu0 = __frcp_rn(mfu0), r_mfu1 = __frcp_rn(mfu1);
+  const float msftx = s[WF_MSFTX][c];
+  const float rdx = g.rdx, rdy = g.rdy;
+  float sdv[kMaxNz];
+  float dmdt = 0.f;
+#pragma unroll
+  for (int k = 0; k < kMaxNz; ++k) {
+    if (k < ktf) {
+      const size_t p = k * lev + c;
+      const float fu1 = divc(muu1 * __ldg(&u[p + 1]), mfu1, r_mfu1), fu0 = divc(muu0 * __ldg(&u[p]), mfu0, r_mfu0);
+      const float fv1 = muv1 * __ldg(&v[p + g.nx]) * mfv1, fv0 = muv0 * __ldg(&v[p]) * mfv0;
+      sdv[k] = (msftx * __ldg(&dnw[k])) * (rdx * (fu1 - fu0) + rdy * (fv1 - fv0));
+      dmdt = dmdt + sdv[k];
+    }
+  }
+  float* ww = s[WF_WW];
+  float wk = ww[c];
+#pragma unroll
+  for (int k = 0; k < kMaxNz - 1; ++k) {
+    if (k < ktf - 1) {
+      wk = wk - (__ldg(&dnw[k]) * __ldg(&c1h[k])) * dmdt - sdv[k];
+      ww[(k + 1) * lev + c] = wk;
+    }
+  }
+}
+
 __global__ void k_diff_metrics(Grid g, S s) {
   WRF_POINT_INDEX(g, k, j, i);
   const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde, nz = g.nz, ktf = nz - 1;
@@ -515,7 +559,12 @@ int launch_prep(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b2(32, 8), b3(32, 4);
   k_rk_prep2d<<<col_grid(g, b2), b2, 0, st>>>(g, s);
   k_rk_prep3d<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  k_ww_cp<<<dim3((g.ide - 1 - g.ids + kWwTX - 1) / kWwTX, g.jde - 1 - g.jds), kWwTX * kWwKT, 0, st>>>(g, s);
+  if (kernel_form() == WRF_FORM_FAST) {
+    const dim3 bc(32, 4);
+    k_ww_cp_col<<<dim3((g.ide - 1 - g.ids + 31) / 32, (g.jde - 1 - g.jds + 3) / 4), bc, 0, st>>>(g, s);
+  } else {
+    k_ww_cp<<<dim3((g.ide - 1 - g.ids + kWwTX - 1) / kWwTX, g.jde - 1 - g.jds), kWwTX * kWwKT, 0, st>>>(g, s);
+  }
   return 3;
 }
 

@@ -289,7 +289,7 @@ __device__ __forceinline__ float d6(const float* a, size_t p, int st) {
   return 45.0f * (a[p + st] - a[p - st]) - 9.0f * (a[p + 2 * st] - a[p - 2 * st]) + (a[p + 3 * st] - a[p - 3 * st]);
 }
 
-__global__ void k_forces(Grid g, S s) {
+__global__ void k_forces(Grid g, S s, int terms) {
   WRF_POINT_INDEX(g, k, j, i);
   const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde, nz = g.nz, ktf = nz - 1, nx = g.nx;
   const size_t lev = (size_t)g.ny * nx;
@@ -304,7 +304,7 @@ __global__ void k_forces(Grid g, S s) {
   const float* fnm = s[WF_FNM];
   const float* fnp = s[WF_FNP];
   // ---------------- rhs_ph (wrf_dynamics.py:2031-2297)
-  if (mass && k >= 1) {
+  if ((terms & 1) && mass && k >= 1) {
     const float* ww = s[WF_WW];
     const float* u = s[WF_U];
     const float* v = s[WF_V];
@@ -373,7 +373,7 @@ __global__ void k_forces(Grid g, S s) {
     if (kk == nz - 1) return 0.f;
     return 0.5f * (fnm[kk] * (pp[kk * lev + cb] + pp[kk * lev + ca]) + fnp[kk] * (pp[(kk - 1) * lev + cb] + pp[(kk - 1) * lev + ca]));
   };
-  if (k < ktf && j >= jds && j < jde - 1 && i >= ids + 1 && i < ide - 1) {  // u
+  if ((terms & 2) && k < ktf && j >= jds && j < jde - 1 && i >= ids + 1 && i < ide - 1) {  // u
     const float r = s[WF_MSFUX][c] / s[WF_MSFUY][c];
     const size_t q = p, qm = p - 1;
     float dpx = r * 0.5f * rdx * s[WF_MUU][c] *
@@ -381,7 +381,7 @@ __global__ void k_forces(Grid g, S s) {
     dpx = dpx + r * rdx * (php[q] - php[qm]) * (rdnw[k] * (dpn(k + 1, c, c - 1) - dpn(k, c, c - 1)) - 0.5f * (mu[c - 1] + mu[c]));
     s[WF_RU_TEND][p] = s[WF_RU_TEND][p] - s[WF_CQU][p] * dpx;
   }
-  if (k < ktf && j >= jds + 1 && j < jde - 1 && i >= ids && i < ide - 1) {  // v
+  if ((terms & 2) && k < ktf && j >= jds + 1 && j < jde - 1 && i >= ids && i < ide - 1) {  // v
     const float r = s[WF_MSFVY][c] / s[WF_MSFVX][c];
     const size_t q = p, qm = p - nx;
     float dpy = r * 0.5f * rdy * s[WF_MUV][c] *
@@ -390,7 +390,7 @@ __global__ void k_forces(Grid g, S s) {
     s[WF_RV_TEND][p] = s[WF_RV_TEND][p] - s[WF_CQV][p] * dpy;
   }
   // ---------------- pg_buoy_w (wrf_dynamics.py:2424-2460); cqw becomes 1/(1+cqw)
-  if (mass && k >= 1 && k < nz - 1) {
+  if ((terms & 4) && mass && k >= 1 && k < nz - 1) {
     float* cqw = s[WF_CQW];
     const float rm = 1.0f / s[WF_MSFTY][c];
     const float mub = s[WF_MUB][c];
@@ -414,11 +414,12 @@ __global__ void k_forces(Grid g, S s) {
   const float* sina = s[WF_SINA];
   const float* cosa = s[WF_COSA];
   const float rr = (float)RERADIUS;
-  if (k < ktf && j >= jds && j < jde - 1 && i >= ids + 1 && i < ide - 1) {  // u
+  if ((terms & 24) && k < ktf && j >= jds && j < jde - 1 && i >= ids + 1 && i < ide - 1) {  // u
     const float rvs = rv[p + nx - 1] + rv[p + nx] + rv[p - 1] + rv[p];
     const float rws = rw[p + lev - 1] + rw[p - 1] + rw[p + lev] + rw[p];
     float t = s[WF_RU_TEND][p];
-    t = t + (s[WF_MSFUX][c] / s[WF_MSFUY][c]) * 0.5f * (f[c] + f[c - 1]) * 0.25f * rvs -
+    if (terms & 8)
+      t = t + (s[WF_MSFUX][c] / s[WF_MSFUY][c]) * 0.5f * (f[c] + f[c - 1]) * 0.25f * rvs -
         0.5f * (e[c] + e[c - 1]) * 0.5f * (cosa[c] + cosa[c - 1]) * 0.25f * rws;
     const float* u = s[WF_U];
     const float* v = s[WF_V];
@@ -426,38 +427,46 @@ __global__ void k_forces(Grid g, S s) {
       return 0.5f * (u[qq] + u[qq + 1]) * (s[WF_MSFVX][cc + nx] - s[WF_MSFVX][cc]) * rdy -
              0.5f * (v[qq] + v[qq + nx]) * (s[WF_MSFUY][cc + 1] - s[WF_MSFUY][cc]) * rdx;
     };
-    t = t + 0.5f * (vx(c, p) + vx(c - 1, p - 1)) * 0.25f * rvs - u[p] * rr * 0.25f * rws;
+    if (terms & 16) t = t + 0.5f * (vx(c, p) + vx(c - 1, p - 1)) * 0.25f * rvs - u[p] * rr * 0.25f * rws;
     s[WF_RU_TEND][p] = t;
   }
-  if (k < ktf && j >= jds + 1 && j < jde - 1 && i >= ids && i < ide - 1) {  // v
+  if ((terms & 24) && k < ktf && j >= jds + 1 && j < jde - 1 && i >= ids && i < ide - 1) {  // v
     const float r = s[WF_MSFVY][c] / s[WF_MSFVX][c];
     const float rus = ru[p] + ru[p + 1] + ru[p - nx] + ru[p - nx + 1];
     const float rws = rw[p + lev - nx] + rw[p - nx] + rw[p + lev] + rw[p];
     float t = s[WF_RV_TEND][p];
-    t = t - r * 0.5f * (f[c] + f[c - nx]) * 0.25f * rus + r * 0.5f * (e[c] + e[c - nx]) * 0.5f * (sina[c] + sina[c - nx]) * 0.25f * rws;
+    if (terms & 8) t = t - r * 0.5f * (f[c] + f[c - nx]) * 0.25f * rus + r * 0.5f * (e[c] + e[c - nx]) * 0.5f * (sina[c] + sina[c - nx]) * 0.25f * rws;
     const float* u = s[WF_U];
     const float* v = s[WF_V];
     auto vx = [&](int cc, size_t qq) {
       return 0.5f * (u[qq] + u[qq + 1]) * (s[WF_MSFVX][cc + nx] - s[WF_MSFVX][cc]) * rdy -
              0.5f * (v[qq] + v[qq + nx]) * (s[WF_MSFUY][cc + 1] - s[WF_MSFUY][cc]) * rdx;
     };
-    t = t - 0.5f * (vx(c, p) + vx(c - nx, p - nx)) * 0.25f * rus - r * v[p] * rr * 0.25f * rws;
+    if (terms & 16) t = t - 0.5f * (vx(c, p) + vx(c - nx, p - nx)) * 0.25f * rus - r * v[p] * rr * 0.25f * rws;
     s[WF_RV_TEND][p] = t;
   }
-  if (mass && k >= 1 && k < ktf) {  // w
+  if ((terms & 24) && mass && k >= 1 && k < ktf) {  // w
     const float fm = fnm[k], fp = fnp[k];
     const float A = fm * (ru[p] + ru[p + 1]) + fp * (ru[p - lev] + ru[p - lev + 1]);
     const float B = fm * (rv[p] + rv[p + nx]) + fp * (rv[p - lev] + rv[p - lev + nx]);
     const float rmt = s[WF_MSFTX][c] / s[WF_MSFTY][c];
     float t = s[WF_RW_TEND][p];
-    t = t + e[c] * (cosa[c] * 0.5f * A - rmt * sina[c] * 0.5f * B);
+    if (terms & 8) t = t + e[c] * (cosa[c] * 0.5f * A - rmt * sina[c] * 0.5f * B);
     const float* u = s[WF_U];
     const float* v = s[WF_V];
     const float Cu = fm * (u[p] + u[p + 1]) + fp * (u[p - lev] + u[p - lev + 1]);
     const float Cv = fm * (v[p] + v[p + nx]) + fp * (v[p - lev] + v[p - lev + nx]);
-    t = t + rr * (0.5f * A * 0.5f * Cu + rmt * 0.5f * B * 0.5f * Cv);
+    if (terms & 16) t = t + rr * (0.5f * A * 0.5f * Cu + rmt * 0.5f * B * 0.5f * Cv);
     s[WF_RW_TEND][p] = t;
   }
+}
+
+// the tendency terms selected by `terms` alone (1 rhs_ph, 2 the pressure
+// gradient, 4 pg_buoy_w, 8 coriolis, 16 curvature), with the point kernel
+int launch_forces_terms(const Grid& g, const S& s, int terms, cudaStream_t st) {
+  const dim3 b3(32, 4);
+  k_forces<<<point_grid(g, b3), b3, 0, st>>>(g, s, terms);
+  return 1;
 }
 
 // -------------------------------------------- tendency accumulation + spec rows
@@ -593,7 +602,7 @@ int launch_advect_forces(const Grid& g, const S& s, cudaStream_t st) {
   int n = launch_advect_mom_tma(g, s, 0, 3, st);
   if (n == 0) n = launch_advect_mom_point(g, s, 7, st);
   n += launch_advect_theta_tiled(g, s, st);
-  if (launch_forces_tma(g, s, st) == 0) k_forces<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  if (launch_forces_tma(g, s, st) == 0) k_forces<<<point_grid(g, b3), b3, 0, st>>>(g, s, 31);
   return n + 1;
 }
 

@@ -32,6 +32,26 @@ int launch_advect_forces(const Grid& g, const S& s, cudaStream_t st);
 // launched) when nx is not a multiple of 4, a map is refused or the point form
 // is selected
 int launch_forces_tma(const Grid& g, const S& s, cudaStream_t st);
+// the tendency terms selected by a mask (1 rhs_ph, 2 pressure gradient,
+// 4 pg_buoy_w, 8 coriolis, 16 curvature) with the point kernel (k_tend.cu),
+// and their adjoint (k_adjoint_forces.cu)
+int launch_forces_terms(const Grid& g, const S& s, int terms, cudaStream_t st);
+int launch_forces_adj(const Grid& g, const S& s, const S& b, int terms, cudaStream_t st);
+// sumflux, spec_bdyupdate (var 't', 'u', 'v' 3-D or 'm' 2-D) and
+// spec_bdyupdate_ph as stand-alone operators, and their adjoints
+// (k_adjoint_subbdy.cu)
+int launch_sumflux(const Grid& g, const S& s, int iteration, int nsub, cudaStream_t st);
+int launch_sumflux_adj(const Grid& g, const S& s, const S& b, int iteration, int nsub, cudaStream_t st);
+int launch_spec_update(const Grid& g, float* field, const float* tend, float dt, char var, bool two_d, cudaStream_t st);
+int launch_spec_update_adj(const Grid& g, const float* field_bar, float* tend_bar, float dt, char var, bool two_d,
+                           cudaStream_t st);
+int launch_spec_ph(const Grid& g, const S& s, float dt, cudaStream_t st);
+int launch_spec_ph_adj(const Grid& g, const S& s, const S& b, float dt, cudaStream_t st);
+// rk_step_prep's functions selected by a mask (1 calculate_full, 2
+// calc_mu_uv, 4 couple_momentum, 8 calc_ww_cp, 16 calc_cq, 32 calc_alt, 64
+// calc_php) and their adjoints (k_adjoint_prep.cu)
+int launch_prep_ops(const Grid& g, const S& s, int ops, cudaStream_t st);
+int launch_prep_ops_adj(const Grid& g, const S& s, const S& b, int ops, cudaStream_t st);
 // rk_addtend_dry + spec_bdytend (k_tend.cu)
 int launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st);
 // moisture advection with the time-averaged fluxes (k_tend.cu)

@@ -531,6 +531,32 @@ constexpr int kUvOperands[] = {WF_U, WF_V, WF_RU_TEND, WF_RV_TEND, WF_P, WF_PB, 
 constexpr int kUvCotangents[] = {WF_U, WF_V, WF_RU_TEND, WF_RV_TEND, WF_P, WF_PB, WF_PH, WF_PHP, WF_ALT, WF_AL,
                                  WF_MU, WF_MUU, WF_MUV, WF_CQU, WF_CQV, WF_MUDF};
 
+// the tendency terms' operands (rhs_ph, horizontal_pressure_gradient,
+// pg_buoy_w, coriolis, curvature) and the cotangents their adjoint reads or
+// accumulates
+constexpr int kForcesOperands[] = {WF_PH_TEND, WF_RU_TEND, WF_RV_TEND, WF_RW_TEND, WF_CQW, WF_U, WF_V, WF_W, WF_WW,
+                                   WF_PH, WF_PHB, WF_MUT, WF_MUU, WF_MUV, WF_ALT, WF_P, WF_PB, WF_AL, WF_PHP, WF_CQU,
+                                   WF_CQV, WF_MU, WF_MUB, WF_RU, WF_RV, WF_RW, WF_MSFUX, WF_MSFUY, WF_MSFVX, WF_MSFVY,
+                                   WF_MSFTX, WF_MSFTY, WF_F, WF_E, WF_SINA, WF_COSA, WF_FNM, WF_FNP, WF_RDNW, WF_RDN};
+constexpr int kForcesCotangents[] = {WF_PH_TEND, WF_RU_TEND, WF_RV_TEND, WF_RW_TEND, WF_CQW, WF_U, WF_V, WF_W,
+                                     WF_WW, WF_PH, WF_PHB, WF_MUT, WF_MUU, WF_MUV, WF_ALT, WF_P, WF_PB, WF_AL,
+                                     WF_PHP, WF_CQU, WF_CQV, WF_MU, WF_MUB, WF_RU, WF_RV, WF_RW};
+
+// sumflux and spec_bdyupdate_ph operands and cotangents
+constexpr int kSumfluxOperands[] = {WF_U, WF_V, WF_WW, WF_U_SAVE, WF_V_SAVE, WF_WW1, WF_MUU, WF_MUV, WF_RU_M,
+                                    WF_RV_M, WF_WW_M, WF_MSFUY, WF_MSFVX_INV};
+constexpr int kSumfluxCotangents[] = {WF_U, WF_V, WF_WW, WF_U_SAVE, WF_V_SAVE, WF_WW1, WF_MUU, WF_MUV, WF_RU_M,
+                                      WF_RV_M, WF_WW_M};
+constexpr int kSpecPhOperands[] = {WF_PH, WF_PH_SAVE, WF_PH_TEND, WF_MU_TEND, WF_MUTS};
+
+// rk_step_prep's operands and the cotangents its adjoint reads or accumulates
+constexpr int kPrepOperands[] = {WF_MU, WF_MUB, WF_MUT, WF_MUU, WF_MUV, WF_U, WF_V, WF_W, WF_RU, WF_RV, WF_RW,
+                                 WF_WW, WF_MOIST, WF_CQU, WF_CQV, WF_CQW, WF_AL, WF_ALB, WF_ALT, WF_PH, WF_PHB,
+                                 WF_PHP, WF_MSFU, WF_MSFVX_INV, WF_MSFT, WF_MSFTX, WF_MSFUY, WF_DNW, WF_C1H};
+constexpr int kPrepCotangents[] = {WF_MU, WF_MUB, WF_MUT, WF_MUU, WF_MUV, WF_U, WF_V, WF_W, WF_RU, WF_RV, WF_RW,
+                                   WF_WW, WF_MOIST, WF_CQU, WF_CQV, WF_CQW, WF_AL, WF_ALB, WF_ALT, WF_PH, WF_PHB,
+                                   WF_PHP};
+
 int state_of(const WrfState* in, const int* ids, int n, S& s) {
   if (!in) return fail(WRF_EINVAL, "null state");
   s = S{};
@@ -649,6 +675,128 @@ int wrf_advance_uv(const WrfGrid* gin, const WrfState* sin, float dts, void* str
   cudaGetLastError();
   launch_advance_uv(g, s, dts, static_cast<cudaStream_t>(stream));
   return check_launch("advance_uv");
+}
+
+int wrf_forces(const WrfGrid* gin, const WrfState* sin, int terms, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (terms < 1 || terms > 31) return fail(WRF_EINVAL, "forces: terms is a mask of 1 .. 31");
+  S s;
+  if ((rc = state_of(sin, kForcesOperands, sizeof(kForcesOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_forces_terms(g, s, terms, static_cast<cudaStream_t>(stream));
+  return check_launch("forces");
+}
+
+int wrf_forces_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, int terms, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (terms < 1 || terms > 31) return fail(WRF_EINVAL, "forces_adj: terms is a mask of 1 .. 31");
+  S s, b;
+  if ((rc = state_of(sin, kForcesOperands, sizeof(kForcesOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kForcesCotangents, sizeof(kForcesCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_forces_adj(g, s, b, terms, static_cast<cudaStream_t>(stream));
+  return check_launch("forces_adj");
+}
+
+int wrf_sumflux(const WrfGrid* gin, const WrfState* sin, int iteration, int nsub, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (nsub < 1 || iteration < 1 || iteration > nsub) return fail(WRF_EINVAL, "sumflux: needs 1 <= iteration <= nsub");
+  S s;
+  if ((rc = state_of(sin, kSumfluxOperands, sizeof(kSumfluxOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_sumflux(g, s, iteration, nsub, static_cast<cudaStream_t>(stream));
+  return check_launch("sumflux");
+}
+
+int wrf_sumflux_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, int iteration, int nsub,
+                    void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (nsub < 1 || iteration < 1 || iteration > nsub) return fail(WRF_EINVAL, "sumflux_adj: needs 1 <= iteration <= nsub");
+  S s, b;
+  if ((rc = state_of(sin, kSumfluxOperands, sizeof(kSumfluxOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kSumfluxCotangents, sizeof(kSumfluxCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_sumflux_adj(g, s, b, iteration, nsub, static_cast<cudaStream_t>(stream));
+  return check_launch("sumflux_adj");
+}
+
+int wrf_spec_bdyupdate(const WrfGrid* gin, float* field, const float* tend, float dt, char var, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!field || !tend) return fail(WRF_EINVAL, "null argument");
+  if (var != 't' && var != 'u' && var != 'v' && var != 'm') return fail(WRF_EINVAL, "spec_bdyupdate: var is t, u, v or m");
+  cudaGetLastError();
+  launch_spec_update(g, field, tend, dt, var, var == 'm', static_cast<cudaStream_t>(stream));
+  return check_launch("spec_bdyupdate");
+}
+
+int wrf_spec_bdyupdate_adj(const WrfGrid* gin, const float* field_bar, float* tend_bar, float dt, char var,
+                           void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!field_bar || !tend_bar) return fail(WRF_EINVAL, "null argument");
+  if (var != 't' && var != 'u' && var != 'v' && var != 'm') return fail(WRF_EINVAL, "spec_bdyupdate_adj: var is t, u, v or m");
+  cudaGetLastError();
+  launch_spec_update_adj(g, field_bar, tend_bar, dt, var, var == 'm', static_cast<cudaStream_t>(stream));
+  return check_launch("spec_bdyupdate_adj");
+}
+
+int wrf_spec_bdyupdate_ph(const WrfGrid* gin, const WrfState* sin, float dt, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s;
+  if ((rc = state_of(sin, kSpecPhOperands, sizeof(kSpecPhOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_spec_ph(g, s, dt, static_cast<cudaStream_t>(stream));
+  return check_launch("spec_bdyupdate_ph");
+}
+
+int wrf_spec_bdyupdate_ph_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dt, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s, b;
+  if ((rc = state_of(sin, kSpecPhOperands, sizeof(kSpecPhOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kSpecPhOperands, sizeof(kSpecPhOperands) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_spec_ph_adj(g, s, b, dt, static_cast<cudaStream_t>(stream));
+  return check_launch("spec_bdyupdate_ph_adj");
+}
+
+int wrf_prep(const WrfGrid* gin, const WrfState* sin, int ops, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (ops < 1 || ops > 127) return fail(WRF_EINVAL, "prep: ops is a mask of 1 .. 127");
+  S s;
+  if ((rc = state_of(sin, kPrepOperands, sizeof(kPrepOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_prep_ops(g, s, ops, static_cast<cudaStream_t>(stream));
+  return check_launch("prep");
+}
+
+int wrf_prep_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, int ops, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (ops < 1 || ops > 127) return fail(WRF_EINVAL, "prep_adj: ops is a mask of 1 .. 127");
+  S s, b;
+  if ((rc = state_of(sin, kPrepOperands, sizeof(kPrepOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kPrepCotangents, sizeof(kPrepCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_prep_ops_adj(g, s, b, ops, static_cast<cudaStream_t>(stream));
+  return check_launch("prep_adj");
 }
 
 int wrf_advance_uv_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dts, void* stream) {

@@ -362,3 +362,145 @@ def test_advance_w_and_its_adjoint_against_the_reference():
             an = float((gr * _aw_dir(n, r, gr.shape)).sum())
             fd = float(A[f"fd_{k}_{r}"])
             assert abs(an - fd) <= 1e-4 * abs(fd), (k, r, an, fd)
+
+
+FORCES_FIX = {  # function: (differentiable inputs, outputs), as in tests/golden/make_golden_adjoint.py
+    "rhs_ph": (("u", "v", "ww", "ph", "phb", "w", "mut", "muu", "muv"), ("ph_tend",)),
+    "hpg": (("ph", "alt", "p", "pb", "al", "php", "cqu", "cqv", "muu", "muv", "mu"), ("ru_tend", "rv_tend")),
+    "pg_buoy_w": (("p", "cqw", "mu", "mub"), ("rw_tend", "cqw")),
+    "coriolis": (("ru", "rv", "rw"), ("ru_tend", "rv_tend", "rw_tend")),
+    "curvature": (("ru", "rv", "rw", "u", "v"), ("ru_tend", "rv_tend", "rw_tend")),
+}
+
+
+@pytest.mark.parametrize("name", list(FORCES_FIX))
+def test_tendency_terms_and_their_adjoint_against_the_reference(name):
+    """rhs_ph, horizontal_pressure_gradient, pg_buoy_w (with its in-place
+    cqw), coriolis and curvature one at a time through
+    pywrf_b200.adjoint.forces: the outputs' norms and sums against the
+    reference's on the fixture's inputs, and the adjoint's directional
+    derivatives in every differentiable input against the reference's
+    float64 central differences along three seeded directions
+    (tests/golden/forces_adj_ref64.npz)."""
+    F = load_npz("forces_adj_ref64.npz")
+    fi = list(FORCES_FIX).index(name)
+    ins, outs = FORCES_FIX[name]
+    z = np.zeros_like(F["u"])
+    inputs = {k: _cuda(z if k.endswith("_tend") else F[k]).requires_grad_(True) for k in adjoint.FORCES_INPUTS}
+    data = {k: _cuda(F[k]) for k in adjoint.FORCES_DATA}
+    sc = {k: float(F[k]) for k in ("cf1", "cf2", "cf3", "cfn", "cfn1")}
+    res = dict(zip(adjoint.FORCES_OUTPUTS, adjoint.forces(inputs, data, [name], 1.0 / float(F["dx"]),
+                                                          1.0 / float(F["dy"]), sc["cf1"], sc["cf2"], sc["cf3"],
+                                                          sc["cfn"], sc["cfn1"])))
+    for o in outs:
+        a = res[o].detach().double().cpu().numpy()
+        l2 = float(np.sqrt((a * a).sum()))
+        ref_l2 = float(F[f"{name}_{o}_l2"])
+        assert abs(l2 - ref_l2) <= 1e-5 * ref_l2, (o, l2, ref_l2)
+        assert abs(float(a.sum()) - float(F[f"{name}_{o}_sum"])) <= 1e-5 * ref_l2 * a.size ** 0.5, o
+    loss = sum((res[o] * _cuda(F[f"cot_{o}"])).sum() for o in outs)
+    loss.backward()
+    for n, inp in enumerate(ins):
+        gr = inputs[inp].grad.double().cpu().numpy()
+        for r in range(3):
+            d = np.random.default_rng(20000 + 1000 * fi + 10 * n + r).standard_normal(gr.shape)
+            an = float((gr * d).sum())
+            scale = float(np.abs(gr * d).sum())
+            fd = float(F[f"{name}_fd_{inp}_{r}"])
+            # fp32 partial products against the reference's float64 differences
+            assert abs(an - fd) <= 1e-4 * abs(fd) + 1e-6 * scale, (inp, r, an, fd, scale)
+
+
+SUBBDY_FIX = {  # case: (differentiable inputs, outputs), as in tests/golden/make_golden_adjoint.py
+    "sumflux1": (("u", "v", "ww", "u_save", "v_save", "ww1", "muu", "muv"), ("ru_m", "rv_m", "ww_m")),
+    "sumflux2": (("u", "v", "ww", "u_save", "v_save", "ww1", "muu", "muv", "ru_m", "rv_m", "ww_m"),
+                 ("ru_m", "rv_m", "ww_m")),
+    "spec_t": (("t", "t_tend"), ("t",)),
+    "spec_m": (("mu", "mu_tend"), ("mu",)),
+    "spec_ph": (("ph_save", "ph", "ph_tend", "mu_tend", "muts"), ("ph",)),
+}
+
+
+@pytest.mark.parametrize("name", list(SUBBDY_FIX))
+def test_substep_flux_sums_and_specified_rows_against_the_reference(name):
+    """sumflux at the first and the last of two iterations, spec_bdyupdate of
+    't' and 'm' and spec_bdyupdate_ph: the outputs' norms and sums against the
+    reference's, and the adjoints' directional derivatives in every
+    differentiable input against the reference's float64 central differences
+    (tests/golden/subbdy_adj_ref64.npz)."""
+    Z = load_npz("subbdy_adj_ref64.npz")
+    fi = list(SUBBDY_FIX).index(name)
+    ins, outs = SUBBDY_FIX[name]
+    x = {k: _cuda(Z[k]).requires_grad_(True) for k in ("u", "v", "ww", "u_save", "v_save", "ww1", "muu", "muv", "ru_m",
+                                                       "rv_m", "ww_m", "t", "t_tend", "mu", "mu_tend", "ph", "ph_save",
+                                                       "ph_tend", "muts")}
+    dts, rdx = float(Z["dts"]), 1.0 / 9000.0
+    if name.startswith("sumflux"):
+        res = dict(zip(("ru_m", "rv_m", "ww_m"),
+                       adjoint.sumflux(x, {k: _cuda(Z[k]) for k in adjoint.SF_DATA}, 1 if name == "sumflux1" else 2,
+                                       2, rdx, rdx)))
+    elif name == "spec_t":
+        res = {"t": adjoint.spec_bdyupdate(x["t"], x["t_tend"], dts, "t", rdx, rdx)}
+    elif name == "spec_m":
+        res = {"mu": adjoint.spec_bdyupdate(x["mu"], x["mu_tend"], dts, "m", rdx, rdx)}
+    else:
+        res = {"ph": adjoint.spec_bdyupdate_ph(x, dts, rdx, rdx)}
+    for o in outs:
+        a = res[o].detach().double().cpu().numpy()
+        l2 = float(np.sqrt((a * a).sum()))
+        ref_l2 = float(Z[f"{name}_{o}_l2"])
+        assert abs(l2 - ref_l2) <= 1e-6 * ref_l2, (o, l2, ref_l2)
+        assert abs(float(a.sum()) - float(Z[f"{name}_{o}_sum"])) <= 1e-6 * ref_l2 * a.size ** 0.5, o
+    sum((res[o] * _cuda(Z[f"cot_{o}"])).sum() for o in outs).backward()
+    for n, inp in enumerate(ins):
+        gr = x[inp].grad.double().cpu().numpy()
+        for r in range(3):
+            d = np.random.default_rng(30000 + 1000 * fi + 10 * n + r).standard_normal(gr.shape)
+            an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
+            fd = float(Z[f"{name}_fd_{inp}_{r}"])
+            assert abs(an - fd) <= 1e-4 * abs(fd) + 1e-6 * scale, (inp, r, an, fd, scale)
+
+
+PREP_FIX = {  # function: (differentiable inputs, outputs), as in tests/golden/make_golden_adjoint.py
+    "calculate_full": (("mub", "mu"), ("mut",)),
+    "calc_mu_uv": (("mu", "mub"), ("muu", "muv")),
+    "couple_momentum": (("muu", "u", "muv", "v", "mut", "w"), ("ru", "rv", "rw")),
+    "calc_ww_cp": (("u", "v", "muu", "muv", "ww"), ("ww",)),
+    "calc_cq": (("moist",), ("cqu", "cqv", "cqw")),
+    "calc_alt": (("al", "alb"), ("alt",)),
+    "calc_php": (("ph", "phb"), ("php",)),
+}
+
+
+@pytest.mark.parametrize("name", list(PREP_FIX))
+def test_rk_step_prep_functions_and_their_adjoint_against_the_reference(name):
+    """rk_step_prep's functions one at a time through pywrf_b200.adjoint.prep:
+    the outputs' norms and sums against the reference's on the fixture's
+    inputs (outputs start from zero, as the fixture's calls pass), and the
+    adjoints' directional derivatives in every differentiable input against
+    the reference's float64 central differences
+    (tests/golden/prep_adj_ref64.npz)."""
+    Z = load_npz("prep_adj_ref64.npz")
+    fi = list(PREP_FIX).index(name)
+    ins, outs = PREP_FIX[name]
+    fields = {}
+    for k in adjoint.PREP_FIELDS:
+        src = Z[k] if (k in Z and k not in outs) or k == "ww" else np.zeros_like(Z["ww"] if k not in ("mut", "muu", "muv") else Z["mu"])
+        fields[k] = _cuda(src).requires_grad_(True)
+    data = {k: _cuda(Z[k]) for k in adjoint.PREP_DATA if k != "c1h"}
+    data["c1h"] = _cuda(np.ones(Z["ww"].shape[0], np.float32))
+    res = adjoint.prep(fields, data, [name], 1.0 / 9000.0, 1.0 / 9000.0)
+    for o in outs:
+        a = res[o].detach().double().cpu().numpy()
+        l2 = float(np.sqrt((a * a).sum()))
+        ref_l2 = float(Z[f"{name}_{o}_l2"])
+        assert abs(l2 - ref_l2) <= 2e-6 * ref_l2, (o, l2, ref_l2)
+        assert abs(float(a.sum()) - float(Z[f"{name}_{o}_sum"])) <= 2e-6 * ref_l2 * a.size ** 0.5, o
+    sum((res[o] * _cuda(Z[f"cot_{o}"])).sum() for o in outs).backward()
+    for n, inp in enumerate(ins):
+        gr = fields[inp].grad.double().cpu().numpy()
+        for r in range(3):
+            d = np.random.default_rng(40000 + 1000 * fi + 10 * n + r).standard_normal(gr.shape)
+            an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
+            fd = float(Z[f"{name}_fd_{inp}_{r}"])
+            assert abs(an - fd) <= 1e-4 * abs(fd) + 1e-6 * scale, (inp, r, an, fd, scale)
