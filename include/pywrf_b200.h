@@ -249,6 +249,17 @@ int wrf_prep(const WrfGrid* g, const WrfState* s, int ops, void* stream);
  * inputs (mu, mub, u, v, w, ww level 0, moist, al, alb, ph, phb, and muu,
  * muv, mut where a later function reads them) are accumulated (+=). */
 int wrf_prep_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, int ops, void* stream);
+/* wrf_dynamics.py:164-278 set_physical_bc3d (two_d 0, [nz][ny][nx]) /
+ * set_physical_bc2d (two_d 1, [ny][nx]) of one field for the stagger letter
+ * var, in place: the reference's open-boundary halo copies, x sides first. */
+int wrf_halo(const WrfGrid* g, float* field, char var, int two_d, void* stream);
+/* Its adjoint: the cotangent of the copied field is added (+=) into in_bar,
+ * the cotangent of the field before the copies (a separate array). */
+int wrf_halo_adj(const WrfGrid* g, const float* field_bar, float* in_bar, char var, int two_d, void* stream);
+/* wrf_boundary.py:358-400 zero_grad_bdy of w (all levels), in place. */
+int wrf_zero_grad_w(const WrfGrid* g, float* w, void* stream);
+/* Its adjoint: w_bar is added (+=) into in_bar (a separate array). */
+int wrf_zero_grad_w_adj(const WrfGrid* g, const float* w_bar, float* in_bar, void* stream);
 int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream);
 /* Its adjoint (reverse mode): sbar holds, under the same field ids, the
  * cotangents of the updated u and v (which are also those of the incoming

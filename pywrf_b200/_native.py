@@ -132,6 +132,14 @@ def lib() -> ctypes.CDLL:
     L.wrf_prep.argtypes = [ctypes.POINTER(WrfGridC), vp, ip, vp]
     L.wrf_prep_adj.restype = ip
     L.wrf_prep_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ip, vp]
+    L.wrf_halo.restype = ip
+    L.wrf_halo.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_char, ip, vp]
+    L.wrf_halo_adj.restype = ip
+    L.wrf_halo_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_char, ip, vp]
+    L.wrf_zero_grad_w.restype = ip
+    L.wrf_zero_grad_w.argtypes = [ctypes.POINTER(WrfGridC), vp, vp]
+    L.wrf_zero_grad_w_adj.restype = ip
+    L.wrf_zero_grad_w_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp]
     L.wrf_advance_uv_adj.restype = ip
     L.wrf_advance_uv_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, vp]
     L.wrf_advect_momentum_adj.restype = ip

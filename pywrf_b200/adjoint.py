@@ -455,6 +455,73 @@ def prep(fields: dict, data: dict, ops, rdx, rdy):
     return dict(zip(PREP_OUTPUTS, outs))
 
 
+class Halo(torch.autograd.Function):
+    """field' = set_physical_bc3d / set_physical_bc2d(field, var) (the open
+    halo copies); ``scal`` = (var, rdx, rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, field):
+        _cuda_only(field)
+        var = str(scal[0])
+        two_d = field.dim() == 2
+        shape = (12,) + tuple(field.shape) if two_d else field.shape
+        cg = scalar_grid(shape, float(scal[1]), float(scal[2]))
+        out = field.detach().clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(field.device):
+            rc = N.lib().wrf_halo(ctypes.byref(cg), _ptr(out), var.encode(), int(two_d), stream)
+        N.check(rc, "wrf_halo")
+        ctx.cg, ctx.var, ctx.two_d = cg, var, two_d
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        gout = gout.contiguous()
+        gin = torch.zeros_like(gout)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(gout.device):
+            rc = N.lib().wrf_halo_adj(ctypes.byref(ctx.cg), _ptr(gout), _ptr(gin), ctx.var.encode(), int(ctx.two_d),
+                                      stream)
+        N.check(rc, "wrf_halo_adj")
+        return None, gin
+
+
+def halo(field, var: str, rdx=1.0 / 9000.0, rdy=1.0 / 9000.0):
+    """Differentiable open-boundary halo copy of a [nz, ny, nx] or [ny, nx] field."""
+    return Halo.apply((var, rdx, rdy), field)
+
+
+class ZeroGradW(torch.autograd.Function):
+    """w' = zero_grad_bdy(w, 'w'); ``scal`` = (rdx, rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, w):
+        _cuda_only(w)
+        cg = scalar_grid(w.shape, float(scal[0]), float(scal[1]))
+        out = w.detach().clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(w.device):
+            rc = N.lib().wrf_zero_grad_w(ctypes.byref(cg), _ptr(out), stream)
+        N.check(rc, "wrf_zero_grad_w")
+        ctx.cg = cg
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        gout = gout.contiguous()
+        gin = torch.zeros_like(gout)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(gout.device):
+            rc = N.lib().wrf_zero_grad_w_adj(ctypes.byref(ctx.cg), _ptr(gout), _ptr(gin), stream)
+        N.check(rc, "wrf_zero_grad_w_adj")
+        return None, gin
+
+
+def zero_grad_w(w, rdx=1.0 / 9000.0, rdy=1.0 / 9000.0):
+    """Differentiable zero_grad_bdy of w."""
+    return ZeroGradW.apply((rdx, rdy), w)
+
+
 AW_INPUTS = ("w", "rw_tend", "ww", "w_save", "u", "v", "muave", "muts", "mut", "t_2ave", "t_2", "t_1", "ph", "ph_1",
              "phb", "ph_tend", "ht", "c2a", "cqw", "alt", "a", "alpha", "gamma")
 AW_DATA = ("msftx", "msfty", "fnm", "fnp", "rdnw", "rdn")
@@ -766,3 +833,56 @@ def rollout(step: Callable[..., Sequence[torch.Tensor]], state: Sequence[torch.T
             state = tuple(checkpoint(segment, k, *state, use_reentrant=False))
         done += k
     return state
+
+
+# the fields one acoustic substep reads (state) and the constant arrays it
+# takes as data
+SUBSTEP_STATE = ("u", "v", "ru_tend", "rv_tend", "p", "pb", "ph", "php", "alt", "al", "mu", "muu", "muv", "cqu", "cqv",
+                 "mudf", "ww", "ww1", "u_save", "v_save", "t", "t_save", "t_2save", "t_tend", "mut", "muave", "muts",
+                 "mu_tend", "w", "rw_tend", "w_save", "ph_save", "phb", "ph_tend", "ht", "c2a", "cqw", "a", "alpha",
+                 "gamma", "ru_m", "rv_m", "ww_m", "pm1")
+SUBSTEP_DATA = ("msfux", "msfuy", "msfvx", "msfvx_inv", "msfvy", "msftx", "msfty", "fnm", "fnp", "rdnw", "rdn", "dnw")
+
+
+def acoustic_substep(st: dict, data: dict, iteration: int, nsub: int, dts: float, *, epssm: float, emdiv: float,
+                     smdiv: float, cf1: float, cf2: float, cf3: float, rdx: float, rdy: float) -> dict:
+    """One acoustic substep composed from the operators above, in the
+    reference's order (pywrf/solver.py:1394-1445): advance_uv with the
+    specified-row update of u and v, advance_mu_t, spec_bdyupdate of t, mu
+    and muts, advance_w, sumflux, spec_bdyupdate_ph, zero_grad_bdy of w,
+    calc_p_rho and the halo copies of ph, al, p, muts, mu and mudf.  ``st``
+    maps SUBSTEP_STATE, ``data`` SUBSTEP_DATA to tensors; returns the state
+    after the substep (a new dict).  Differentiable end to end: every piece
+    is a hand-written reverse kernel, and the chain keeps only the operators'
+    inputs."""
+    s = dict(st)
+    u, v = advance_uv({k: s[k] for k in UV_INPUTS}, {k: data[k] for k in UV_DATA}, dts, emdiv, cf1, cf2, cf3, rdx,
+                      rdy)
+    s["u"], s["v"] = u, v
+    mt_in = {"ww": s["ww"], "ww_1": s["ww1"], "u": u, "u_1": s["u_save"], "v": v, "v_1": s["v_save"], "t": s["t"],
+             "t_1": s["t_save"], "t_ave": s["t_2save"], "ft": s["t_tend"], "mu": s["mu"], "mut": s["mut"],
+             "muave": s["muave"], "muts": s["muts"], "muu": s["muu"], "muv": s["muv"], "mudf": s["mudf"],
+             "mu_tend": s["mu_tend"]}
+    mt = advance_mu_t(mt_in, {k: data[k] for k in MUT_DATA}, dts, epssm, rdx, rdy)
+    s.update(ww=mt["ww"], t=mt["t"], t_2save=mt["t_ave"], muave=mt["muave"], muts=mt["muts"], mudf=mt["mudf"],
+             mu=mt["mu"])
+    s["t"] = spec_bdyupdate(s["t"], s["t_tend"], dts, "t", rdx, rdy)
+    s["mu"] = spec_bdyupdate(s["mu"], s["mu_tend"], dts, "m", rdx, rdy)
+    s["muts"] = spec_bdyupdate(s["muts"], s["mu_tend"], dts, "m", rdx, rdy)
+    aw_in = {k: s[k] for k in AW_INPUTS if k not in ("t_2ave", "t_2", "t_1", "ph_1")}
+    aw_in.update(t_2ave=s["t_2save"], t_2=s["t"], t_1=s["t_save"], ph_1=s["ph_save"])
+    aw = advance_w(aw_in, {k: data[k] for k in AW_DATA}, dts, epssm, cf1, cf2, cf3, rdx, rdy)
+    s.update(t_2save=aw["t_2ave"], w=aw["w"], ph=aw["ph"])
+    s["ru_m"], s["rv_m"], s["ww_m"] = sumflux({k: s[k] for k in SF_INPUTS}, {k: data[k] for k in SF_DATA},
+                                              iteration, nsub, rdx, rdy)
+    s["ph"] = spec_bdyupdate_ph({k: s[k] for k in SPH_INPUTS}, dts, rdx, rdy)
+    s["w"] = zero_grad_w(s["w"], rdx, rdy)
+    pr_in = {"al": s["al"], "p": s["p"], "ph": s["ph"], "alt": s["alt"], "t_2": s["t"], "t_1": s["t_save"],
+             "c2a": s["c2a"], "pm1": s["pm1"], "mu": s["mu"], "mut": s["muts"]}
+    s["al"], s["p"], s["pm1"] = calc_p_rho(pr_in, data["rdnw"], smdiv, iteration, rdx, rdy)
+    s["ph"] = halo(s["ph"], "w", rdx, rdy)
+    s["al"] = halo(s["al"], "p", rdx, rdy)
+    s["p"] = halo(s["p"], "p", rdx, rdy)
+    for k in ("muts", "mu", "mudf"):
+        s[k] = halo(s[k], "t", rdx, rdy)
+    return s

@@ -799,6 +799,55 @@ int wrf_prep_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, 
   return check_launch("prep_adj");
 }
 
+namespace {
+bool halo_var(char v) {
+  return v == 'u' || v == 'v' || v == 'w' || v == 't' || v == 'p' || v == 'd' || v == 'e' || v == 'f' || v == 'x' ||
+         v == 'y' || v == 'r' || v == 'U' || v == 'V';
+}
+}  // namespace
+
+int wrf_halo(const WrfGrid* gin, float* field, char var, int two_d, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!field) return fail(WRF_EINVAL, "null argument");
+  if (!halo_var(var)) return fail(WRF_EINVAL, "halo: unknown stagger letter");
+  cudaGetLastError();
+  launch_halo(g, field, var, two_d != 0, static_cast<cudaStream_t>(stream));
+  return check_launch("halo");
+}
+
+int wrf_halo_adj(const WrfGrid* gin, const float* field_bar, float* in_bar, char var, int two_d, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!field_bar || !in_bar || field_bar == in_bar) return fail(WRF_EINVAL, "halo_adj: two distinct arrays needed");
+  if (!halo_var(var)) return fail(WRF_EINVAL, "halo_adj: unknown stagger letter");
+  cudaGetLastError();
+  launch_halo_adj(g, field_bar, in_bar, var, two_d != 0, static_cast<cudaStream_t>(stream));
+  return check_launch("halo_adj");
+}
+
+int wrf_zero_grad_w(const WrfGrid* gin, float* w, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!w) return fail(WRF_EINVAL, "null argument");
+  cudaGetLastError();
+  launch_zero_grad_w(g, w, static_cast<cudaStream_t>(stream));
+  return check_launch("zero_grad_w");
+}
+
+int wrf_zero_grad_w_adj(const WrfGrid* gin, const float* w_bar, float* in_bar, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!w_bar || !in_bar || w_bar == in_bar) return fail(WRF_EINVAL, "zero_grad_w_adj: two distinct arrays needed");
+  cudaGetLastError();
+  launch_zero_grad_w_adj(g, w_bar, in_bar, static_cast<cudaStream_t>(stream));
+  return check_launch("zero_grad_w_adj");
+}
+
 int wrf_advance_uv_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dts, void* stream) {
   Grid g;
   int rc = make_grid(gin, g);

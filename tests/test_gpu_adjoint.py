@@ -504,3 +504,105 @@ def test_rk_step_prep_functions_and_their_adjoint_against_the_reference(name):
             an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
             fd = float(Z[f"{name}_fd_{inp}_{r}"])
             assert abs(an - fd) <= 1e-4 * abs(fd) + 1e-6 * scale, (inp, r, an, fd, scale)
+
+
+def _oracle_substep(g, s, iteration, nsub, dts):
+    """One acoustic substep of the oracle (its model loop, solver.py:1394-1445)
+    on the state dict ``s``, in place."""
+    from oracle import boundary as OB
+    from oracle import dynamics as OD
+
+    OD.advance_uv(g, s["u"], s["ru_tend"], s["v"], s["rv_tend"], s["p"], s["pb"], s["ph"], s["php"], s["alt"],
+                  s["al"], s["mu"], s["muu"], s["cqu"], s["muv"], s["cqv"], s["mudf"], s["msfux"], s["msfuy"],
+                  s["msfvx"], s["msfvx_inv"], s["msfvy"], dts, s["cf1"], s["cf2"], s["cf3"], s["fnm"], s["fnp"],
+                  g.emdiv, s["rdnw"])
+    OB.spec_bdyupdate(g, s["u"], s["ru_tend"], dts, "u")
+    OB.spec_bdyupdate(g, s["v"], s["rv_tend"], dts, "v")
+    OD.advance_mu_t(g, s, dts, g.epssm, iteration)
+    OB.spec_bdyupdate(g, s["t"], s["t_tend"], dts, "t")
+    OB.spec_bdyupdate(g, s["mu"], s["mu_tend"], dts, "m")
+    OB.spec_bdyupdate(g, s["muts"], s["mu_tend"], dts, "m")
+    OD.advance_w(g, s, dts, g.epssm, s["cf1"], s["cf2"], s["cf3"])
+    OD.sumflux(g, s, iteration, nsub)
+    OB.spec_bdyupdate_ph(g, s["ph_save"], s["ph"], s["ph_tend"], s["mu_tend"], s["muts"], dts)
+    OB.zero_grad_bdy(g, s["w"], "w")
+    s["pm1"] = OD.calc_p_rho(g, s["al"], s["p"], s["ph"], s["alt"], s["t"], s["t_save"], s["c2a"], s["pm1"], s["mu"],
+                             s["muts"], s["rdnw"], g.smdiv, iteration)
+    OD.set_physical_bc3d(g, s["ph"], "w")
+    OD.set_physical_bc3d(g, s["al"], "p")
+    OD.set_physical_bc3d(g, s["p"], "p")
+    for k in ("muts", "mu", "mudf"):
+        OD.set_physical_bc2d(g, s[k], "t")
+
+
+SUB_OUT = ("u", "v", "w", "ph", "t", "mu", "muts", "p", "al", "ww", "ru_m", "rv_m", "ww_m", "t_2save", "pm1", "mudf",
+           "muave")
+
+
+def test_composed_acoustic_substep_and_its_adjoint_against_the_oracle():
+    """pywrf_b200.adjoint.acoustic_substep (the substep composed from the
+    operators' Functions) on the small case's state just before stage 2's
+    substeps: every output within 3x the float32 oracle's own error of the
+    float64 oracle's substep, and the gradient of a seeded linear functional
+    of 17 outputs, in 14 inputs, against float64 central differences of the
+    oracle's substep along seeded directions (the outputs' error allowance:
+    3x the float32 oracle's own error plus 2e-6)."""
+    import copy
+
+    from helpers import SMALL
+    from oracle.model import OracleModel
+    from pywrf_b200 import synthetic
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    snap = {}
+
+    def probe(name, m):
+        if name == "s2.acprep" and not snap:
+            snap.update(copy.deepcopy(m.st))
+
+    m = OracleModel(g, inputs, bdy, np.float64)
+    m.run(1)
+    m.step(2, probe)
+    dts = g.dt / g.soundsteps
+    it, nsub = 1, g.soundsteps // 2
+
+    def oracle_run(dtype, pert=None):
+        s = {k: (np.array(v, dtype) if isinstance(v, np.ndarray) else v) for k, v in snap.items()}
+        if pert:
+            for k, d in pert.items():
+                s[k] = s[k] + d
+        _oracle_substep(g, s, it, nsub, dts)
+        return s
+
+    o64, o32 = oracle_run(np.float64), oracle_run(np.float32)
+    st = {k: _cuda(snap[k]).requires_grad_(True) for k in adjoint.SUBSTEP_STATE}
+    data = {k: _cuda(snap[k]) for k in adjoint.SUBSTEP_DATA}
+    sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=float(snap["cf1"]), cf2=float(snap["cf2"]),
+              cf3=float(snap["cf3"]), rdx=g.rdx, rdy=g.rdy)
+    out = adjoint.acoustic_substep(st, data, it, nsub, dts, **sc)
+    bad = []
+    for k in SUB_OUT:
+        c = out[k].detach().double().cpu().numpy()
+        err, floor = rel_l2(c, o64[k]), rel_l2(o32[k], o64[k])
+        # the stand-alone operators round like the fused step's kernels, not
+        # like numpy: a 2e-6 allowance on top of 3x the oracle's own error
+        if not err <= 3.0 * floor + 2e-6:
+            bad.append((k, err, floor))
+    assert not bad, bad
+    rng = np.random.default_rng(77)
+    cot = {k: rng.standard_normal(np.shape(snap[k])) for k in SUB_OUT}
+    sum((out[k].double() * torch.tensor(cot[k], device="cuda")).sum() for k in SUB_OUT).backward()
+
+    def loss(pert):
+        s = oracle_run(np.float64, pert)
+        return sum(float((s[k] * cot[k]).sum()) for k in SUB_OUT)
+
+    for name in ("u", "v", "t", "ph", "w", "mu", "muts", "p", "al", "ww", "ru_tend", "t_tend", "ph_tend", "c2a"):
+        gr = st[name].grad.double().cpu().numpy()
+        d = rng.standard_normal(gr.shape)
+        eps = 1e-6 * float(np.abs(snap[name]).max() or 1.0)
+        fd = (loss({name: eps * d}) - loss({name: -eps * d})) / (2 * eps)
+        an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
+        assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
