@@ -144,7 +144,10 @@ __global__ void k_spec_ph_adj(Grid g, S s, S bar, float dt) {
   const float P = bar[WF_PH][p];
   bar[WF_PH][p] = P * mu_old / mt;
   bar[WF_PH_TEND][p] += dt / mt * P;
-  bar[WF_PH_SAVE][p] += (mu_old / mt - 1.0f) * P;
+  // d/d ph_save = mu_old / mt - 1 = -dt mu_tend / mt, formed without the
+  // cancellation of the difference (which float32 would round to a few
+  // significant digits)
+  bar[WF_PH_SAVE][p] += -(dt * s[WF_MU_TEND][c]) / mt * P;
   const float mob = (ph + ps) / mt * P;
   const float mtb = -(ph * mu_old + dt * pt + ps * mu_old) / (mt * mt) * P;
   atomicAdd(&bar[WF_MUTS][c], mob + mtb);
