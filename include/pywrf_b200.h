@@ -260,6 +260,23 @@ int wrf_halo_adj(const WrfGrid* g, const float* field_bar, float* in_bar, char v
 int wrf_zero_grad_w(const WrfGrid* g, float* w, void* stream);
 /* Its adjoint: w_bar is added (+=) into in_bar (a separate array). */
 int wrf_zero_grad_w_adj(const WrfGrid* g, const float* w_bar, float* in_bar, void* stream);
+/* wrf_dynamics.py:3152-3266 small_step_prep on the state table (without the
+ * calc_p_rho / calc_coef_w the step runs after it): mu_1, muts, muus, muvs,
+ * mu_save, mu, the _1 and _save copies, the perturbation forms of u, v, t,
+ * w, ph, c2a and ww1, at RK stage rk_step. */
+int wrf_small_step_prep(const WrfGrid* g, const WrfState* s, int rk_step, void* stream);
+/* Its adjoint: sbar holds the cotangents of the updated fields and is
+ * rewritten to those of the incoming state (overwritten fields get zero);
+ * work: caller-owned scratch of 3 * ny * nx floats (the column masses the
+ * forward formed). */
+int wrf_small_step_prep_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, int rk_step, float* work,
+                            void* stream);
+/* wrf_dynamics.py:3844-3930 calc_mu_uv_1 then small_step_finish on the state
+ * table (back from the perturbation form; h_diabatic enters at rk_step 3). */
+int wrf_small_step_finish(const WrfGrid* g, const WrfState* s, float dts, int nsub, int rk_step, void* stream);
+/* Its adjoint: as wrf_small_step_prep_adj; work: 2 * ny * nx floats. */
+int wrf_small_step_finish_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float dts, int nsub,
+                              int rk_step, float* work, void* stream);
 int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream);
 /* Its adjoint (reverse mode): sbar holds, under the same field ids, the
  * cotangents of the updated u and v (which are also those of the incoming

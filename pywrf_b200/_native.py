@@ -140,6 +140,14 @@ def lib() -> ctypes.CDLL:
     L.wrf_zero_grad_w.argtypes = [ctypes.POINTER(WrfGridC), vp, vp]
     L.wrf_zero_grad_w_adj.restype = ip
     L.wrf_zero_grad_w_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp]
+    L.wrf_small_step_prep.restype = ip
+    L.wrf_small_step_prep.argtypes = [ctypes.POINTER(WrfGridC), vp, ip, vp]
+    L.wrf_small_step_prep_adj.restype = ip
+    L.wrf_small_step_prep_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ip, vp, vp]
+    L.wrf_small_step_finish.restype = ip
+    L.wrf_small_step_finish.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_float, ip, ip, vp]
+    L.wrf_small_step_finish_adj.restype = ip
+    L.wrf_small_step_finish_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, ip, ip, vp, vp]
     L.wrf_advance_uv_adj.restype = ip
     L.wrf_advance_uv_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, vp]
     L.wrf_advect_momentum_adj.restype = ip

@@ -886,3 +886,134 @@ def acoustic_substep(st: dict, data: dict, iteration: int, nsub: int, dts: float
     for k in ("muts", "mu", "mudf"):
         s[k] = halo(s[k], "t", rdx, rdy)
     return s
+
+
+class _TableOp(torch.autograd.Function):
+    """A state-table operator with a hand-written adjoint: ``op`` names the
+    fields it reads (``op.fields``, the updated ones ``op.outputs`` among
+    them), its constant arrays (``op.data``), and runs the forward
+    (``op.fwd(cg, table, stream)``) and the reverse product
+    (``op.adj(cg, table, bar_table, stream)``, which rewrites the outputs'
+    cotangents to the inputs' and accumulates the rest)."""
+
+    @staticmethod
+    def forward(ctx, op, cg, *tensors):
+        _cuda_only(*tensors)
+        named = dict(zip(op.fields + op.data, tensors))
+        outs = {k: named[k].detach().clone() for k in op.outputs}
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(tensors[0].device):
+            N.check(op.fwd(cg, _table({**named, **outs}), stream), op.name)
+        ctx.save_for_backward(*tensors)
+        ctx.op, ctx.cg = op, cg
+        return tuple(outs[k] for k in op.outputs)
+
+    @staticmethod
+    def backward(ctx, *gouts):
+        op = ctx.op
+        named = dict(zip(op.fields + op.data, ctx.saved_tensors))
+        bars = {k: torch.zeros_like(named[k]) for k in op.fields}
+        for k, gr in zip(op.outputs, gouts):
+            if gr is not None:
+                bars[k] = gr.contiguous().clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(ctx.saved_tensors[0].device):
+            N.check(op.adj(ctx.cg, _table(named), _table(bars), stream), op.name + "_adj")
+        return (None, None) + tuple(bars[k] for k in op.fields) + (None,) * len(op.data)
+
+
+class _SmallStepPrep:
+    name = "wrf_small_step_prep"
+    fields = ("mu", "mu_1", "mub", "mudf", "muts", "mu_save", "muu", "muv", "muus", "muvs", "mut", "u", "u_1",
+              "u_save", "v", "v_1", "v_save", "t", "t_1", "t_save", "w", "w_1", "w_save", "ph", "ph_1", "ph_save",
+              "ww", "ww1", "c2a", "pb", "p", "alt")
+    outputs = ("mu", "mu_1", "mudf", "muts", "mu_save", "muus", "muvs", "u", "u_1", "u_save", "v", "v_1", "v_save",
+               "t", "t_1", "t_save", "w", "w_1", "w_save", "ph", "ph_1", "ph_save", "ww1", "c2a")
+    data = ("msfuy", "msfvx_inv", "msfty")
+
+    def __init__(self, rk_step, ny, nx, device):
+        self.rk_step = rk_step
+        self.work = torch.empty(3 * ny * nx, dtype=torch.float32, device=device)
+
+    def fwd(self, cg, tab, stream):
+        return N.lib().wrf_small_step_prep(ctypes.byref(cg), tab, self.rk_step, stream)
+
+    def adj(self, cg, tab, btab, stream):
+        return N.lib().wrf_small_step_prep_adj(ctypes.byref(cg), tab, btab, self.rk_step,
+                                               ctypes.c_void_p(self.work.data_ptr()), stream)
+
+
+class _SmallStepFinish:
+    name = "wrf_small_step_finish"
+    fields = ("u", "u_save", "v", "v_save", "w", "w_save", "ph", "ph_save", "ww", "ww1", "t", "t_save", "h_diabatic",
+              "mu", "mu_save", "mut", "muts", "muu", "muv", "muus", "muvs")
+    outputs = ("u", "v", "w", "ph", "ww", "t", "mu", "muus", "muvs")
+    data = ("msfuy", "msfvx", "msfty")
+
+    def __init__(self, dts, nsub, rk_step, ny, nx, device):
+        self.dts, self.nsub, self.rk_step = dts, nsub, rk_step
+        self.work = torch.empty(2 * ny * nx, dtype=torch.float32, device=device)
+
+    def fwd(self, cg, tab, stream):
+        return N.lib().wrf_small_step_finish(ctypes.byref(cg), tab, self.dts, self.nsub, self.rk_step, stream)
+
+    def adj(self, cg, tab, btab, stream):
+        return N.lib().wrf_small_step_finish_adj(ctypes.byref(cg), tab, btab, self.dts, self.nsub, self.rk_step,
+                                                 ctypes.c_void_p(self.work.data_ptr()), stream)
+
+
+def small_step_prep(st: dict, data: dict, rk_step: int, rdx, rdy) -> dict:
+    """Differentiable small_step_prep (pywrf/wrf_dynamics.py:3152-3266):
+    returns ``st`` with the fields it updates replaced."""
+    nz, ny, nx = st["u"].shape
+    op = _SmallStepPrep(rk_step, ny, nx, st["u"].device)
+    cg = scalar_grid(st["u"].shape, rdx, rdy)
+    outs = _TableOp.apply(op, cg, *[st[k] for k in op.fields], *[data[k] for k in op.data])
+    return {**st, **dict(zip(op.outputs, outs))}
+
+
+def small_step_finish(st: dict, data: dict, dts: float, nsub: int, rk_step: int, rdx, rdy) -> dict:
+    """Differentiable calc_mu_uv_1 + small_step_finish
+    (pywrf/wrf_dynamics.py:3844-3930): returns ``st`` with the fields they
+    update replaced."""
+    nz, ny, nx = st["u"].shape
+    op = _SmallStepFinish(dts, nsub, rk_step, ny, nx, st["u"].device)
+    cg = scalar_grid(st["u"].shape, rdx, rdy)
+    outs = _TableOp.apply(op, cg, *[st[k] for k in op.fields], *[data[k] for k in op.data])
+    return {**st, **dict(zip(op.outputs, outs))}
+
+
+# the fields the acoustic part of an RK stage reads (state) and its constant
+# arrays (data)
+STAGE_STATE = SUBSTEP_STATE + ("h_diabatic", "mu_1", "mu_save", "mub", "muus", "muvs", "ph_1", "t_1", "u_1", "v_1",
+                               "w_1")
+STAGE_DATA = SUBSTEP_DATA
+
+
+def acoustic_stage(st: dict, data: dict, rk_step: int, nsub: int, dts: float, *, epssm: float, emdiv: float,
+                   smdiv: float, cf1: float, cf2: float, cf3: float, rdx: float, rdy: float,
+                   top_lid: bool = False) -> dict:
+    """The acoustic part of one RK stage composed from the operators'
+    Functions, in the reference's order (pywrf/solver.py:1258-1492):
+    small_step_prep, calc_p_rho at step 0, calc_coef_w, the halo copies that
+    follow them, ``nsub`` substeps (:func:`acoustic_substep`), calc_mu_uv_1
+    with small_step_finish, and at the last stage the halo copies of the
+    averaged fluxes and column masses.  ``st`` maps every field these read;
+    returns the state after the stage."""
+    s = small_step_prep(st, data, rk_step, rdx, rdy)
+    pr = {"al": s["al"], "p": s["p"], "ph": s["ph"], "alt": s["alt"], "t_2": s["t"], "t_1": s["t_save"],
+          "c2a": s["c2a"], "pm1": s["pm1"], "mu": s["mu"], "mut": s["muts"]}
+    s["al"], s["p"], s["pm1"] = calc_p_rho(pr, data["rdnw"], smdiv, 0, rdx, rdy)
+    s["a"], s["alpha"], s["gamma"] = coef_w(s["mut"], s["cqw"], s["c2a"], data["rdn"], data["rdnw"], dts, epssm,
+                                            top_lid, rdx, rdy)
+    for k, var in (("ru_tend", "u"), ("rv_tend", "v"), ("ph", "w"), ("al", "p"), ("p", "p"), ("t_1", "t"),
+                   ("t_save", "t"), ("mu_1", "t"), ("mu", "t"), ("mudf", "t")):
+        s[k] = halo(s[k], var, rdx, rdy)
+    sc = dict(epssm=epssm, emdiv=emdiv, smdiv=smdiv, cf1=cf1, cf2=cf2, cf3=cf3, rdx=rdx, rdy=rdy)
+    for it in range(1, nsub + 1):
+        s = acoustic_substep(s, data, it, nsub, dts, **sc)
+    s = small_step_finish(s, data, dts, nsub, rk_step, rdx, rdy)
+    if rk_step == 3:
+        for k, var in (("ru_m", "u"), ("rv_m", "v"), ("ww_m", "w"), ("mut", "t"), ("muts", "t")):
+            s[k] = halo(s[k], var, rdx, rdy)
+    return s

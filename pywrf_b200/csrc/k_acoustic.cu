@@ -1133,6 +1133,14 @@ int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cu
   return 4;
 }
 
+// small_step_prep alone (the step's k_ssp2d and k_ssp3d)
+int launch_ssp_only(const Grid& g, const S& s, int rk_step, cudaStream_t st) {
+  const dim3 b2(32, 8), b3(32, 4);
+  k_ssp2d<<<col_grid(g, b2), b2, 0, st>>>(g, s, rk_step);
+  k_ssp3d<<<point_grid(g, b3), b3, 0, st>>>(g, s, rk_step);
+  return 2;
+}
+
 int launch_coef_w(const Grid& g, const float* mut, const float* cqw, const float* c2a, const float* rdn,
                   const float* rdnw, float dts, float* a, float* alpha, float* gamma, cudaStream_t st) {
   S s{};

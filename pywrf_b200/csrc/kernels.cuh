@@ -116,6 +116,13 @@ int launch_small_step_prep(const Grid& g, const S& s, int rk_step, float dts, cu
 int launch_advance_uv(const Grid& g, const S& s, float dts, cudaStream_t st);
 int launch_acoustic_col(const Grid& g, const S& s, float dts, int iteration, int nsub, cudaStream_t st);
 int launch_small_step_finish(const Grid& g, const S& s, float dts, int nsub, int rk_step, cudaStream_t st);
+// small_step_prep without the calc_p_rho / calc_coef_w that follow it in the
+// step (k_acoustic.cu), and the adjoints of small_step_prep and of
+// calc_mu_uv_1 + small_step_finish (k_adjoint_ssp.cu)
+int launch_ssp_only(const Grid& g, const S& s, int rk_step, cudaStream_t st);
+int launch_small_step_prep_adj(const Grid& g, const S& s, const S& b, int rk_step, float* work, cudaStream_t st);
+int launch_small_step_finish_adj(const Grid& g, const S& s, const S& b, float dts, int nsub, int rk_step, float* work,
+                                 cudaStream_t st);
 
 // moisture (k_moist.cu)
 int launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st);

@@ -557,6 +557,22 @@ constexpr int kPrepCotangents[] = {WF_MU, WF_MUB, WF_MUT, WF_MUU, WF_MUV, WF_U, 
                                    WF_WW, WF_MOIST, WF_CQU, WF_CQV, WF_CQW, WF_AL, WF_ALB, WF_ALT, WF_PH, WF_PHB,
                                    WF_PHP};
 
+// small_step_prep and calc_mu_uv_1 + small_step_finish operands and cotangents
+constexpr int kSspOperands[] = {WF_MU, WF_MU_1, WF_MUB, WF_MUDF, WF_MUTS, WF_MU_SAVE, WF_MUU, WF_MUV, WF_MUUS,
+                                WF_MUVS, WF_MUT, WF_U, WF_U_1, WF_U_SAVE, WF_V, WF_V_1, WF_V_SAVE, WF_T, WF_T_1,
+                                WF_T_SAVE, WF_W, WF_W_1, WF_W_SAVE, WF_PH, WF_PH_1, WF_PH_SAVE, WF_WW, WF_WW1,
+                                WF_C2A, WF_PB, WF_P, WF_ALT, WF_MSFUY, WF_MSFVX_INV, WF_MSFTY};
+constexpr int kSspCotangents[] = {WF_MU, WF_MU_1, WF_MUB, WF_MUDF, WF_MUTS, WF_MU_SAVE, WF_MUU, WF_MUV, WF_MUUS,
+                                  WF_MUVS, WF_MUT, WF_U, WF_U_1, WF_U_SAVE, WF_V, WF_V_1, WF_V_SAVE, WF_T, WF_T_1,
+                                  WF_T_SAVE, WF_W, WF_W_1, WF_W_SAVE, WF_PH, WF_PH_1, WF_PH_SAVE, WF_WW, WF_WW1,
+                                  WF_C2A, WF_PB, WF_P, WF_ALT};
+constexpr int kSsfOperands[] = {WF_U, WF_U_SAVE, WF_V, WF_V_SAVE, WF_W, WF_W_SAVE, WF_PH, WF_PH_SAVE, WF_WW, WF_WW1,
+                                WF_T, WF_T_SAVE, WF_H_DIABATIC, WF_MU, WF_MU_SAVE, WF_MUT, WF_MUTS, WF_MUU, WF_MUV,
+                                WF_MUUS, WF_MUVS, WF_MSFUY, WF_MSFVX, WF_MSFTY};
+constexpr int kSsfCotangents[] = {WF_U, WF_U_SAVE, WF_V, WF_V_SAVE, WF_W, WF_W_SAVE, WF_PH, WF_PH_SAVE, WF_WW, WF_WW1,
+                                  WF_T, WF_T_SAVE, WF_H_DIABATIC, WF_MU, WF_MU_SAVE, WF_MUT, WF_MUTS, WF_MUU, WF_MUV,
+                                  WF_MUUS, WF_MUVS};
+
 int state_of(const WrfState* in, const int* ids, int n, S& s) {
   if (!in) return fail(WRF_EINVAL, "null state");
   s = S{};
@@ -846,6 +862,60 @@ int wrf_zero_grad_w_adj(const WrfGrid* gin, const float* w_bar, float* in_bar, v
   cudaGetLastError();
   launch_zero_grad_w_adj(g, w_bar, in_bar, static_cast<cudaStream_t>(stream));
   return check_launch("zero_grad_w_adj");
+}
+
+int wrf_small_step_prep(const WrfGrid* gin, const WrfState* sin, int rk_step, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (rk_step < 1 || rk_step > 3) return fail(WRF_EINVAL, "small_step_prep: rk_step is 1, 2 or 3");
+  S s;
+  if ((rc = state_of(sin, kSspOperands, sizeof(kSspOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_ssp_only(g, s, rk_step, static_cast<cudaStream_t>(stream));
+  return check_launch("small_step_prep");
+}
+
+int wrf_small_step_prep_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, int rk_step, float* work,
+                            void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (rk_step < 1 || rk_step > 3) return fail(WRF_EINVAL, "small_step_prep_adj: rk_step is 1, 2 or 3");
+  if (!work) return fail(WRF_EINVAL, "small_step_prep_adj: work (3 ny*nx floats) is required");
+  S s, b;
+  if ((rc = state_of(sin, kSspOperands, sizeof(kSspOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kSspCotangents, sizeof(kSspCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_small_step_prep_adj(g, s, b, rk_step, work, static_cast<cudaStream_t>(stream));
+  return check_launch("small_step_prep_adj");
+}
+
+int wrf_small_step_finish(const WrfGrid* gin, const WrfState* sin, float dts, int nsub, int rk_step, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (rk_step < 1 || rk_step > 3 || nsub < 1) return fail(WRF_EINVAL, "small_step_finish: rk_step 1..3, nsub >= 1");
+  S s;
+  if ((rc = state_of(sin, kSsfOperands, sizeof(kSsfOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_small_step_finish(g, s, dts, nsub, rk_step, static_cast<cudaStream_t>(stream));
+  return check_launch("small_step_finish");
+}
+
+int wrf_small_step_finish_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dts, int nsub,
+                              int rk_step, float* work, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (rk_step < 1 || rk_step > 3 || nsub < 1) return fail(WRF_EINVAL, "small_step_finish_adj: rk_step 1..3, nsub >= 1");
+  if (!work) return fail(WRF_EINVAL, "small_step_finish_adj: work (2 ny*nx floats) is required");
+  S s, b;
+  if ((rc = state_of(sin, kSsfOperands, sizeof(kSsfOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kSsfCotangents, sizeof(kSsfCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_small_step_finish_adj(g, s, b, dts, nsub, rk_step, work, static_cast<cudaStream_t>(stream));
+  return check_launch("small_step_finish_adj");
 }
 
 int wrf_advance_uv_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dts, void* stream) {

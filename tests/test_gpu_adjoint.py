@@ -606,3 +606,101 @@ def test_composed_acoustic_substep_and_its_adjoint_against_the_oracle():
         fd = (loss({name: eps * d}) - loss({name: -eps * d})) / (2 * eps)
         an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
         assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
+
+
+def _oracle_acoustic_stage(g, s, rk_step, nsub, dts):
+    """The acoustic part of one RK stage of the oracle (its model loop,
+    solver.py:1258-1492) on the state dict ``s``, in place."""
+    from oracle import dynamics as OD
+
+    OD.small_step_prep(g, s, rk_step)
+    s["pm1"] = OD.calc_p_rho(g, s["al"], s["p"], s["ph"], s["alt"], s["t"], s["t_save"], s["c2a"], s["pm1"], s["mu"],
+                             s["muts"], s["rdnw"], g.smdiv, 0)
+    OD.calc_coef_w(g, s["a"], s["alpha"], s["gamma"], s["mut"], s["cqw"], s["rdn"], s["rdnw"], s["c2a"], dts, g.epssm,
+                   g.top_lid)
+    for k, var in (("ru_tend", "u"), ("rv_tend", "v"), ("ph", "w"), ("al", "p"), ("p", "p"), ("t_1", "t"),
+                   ("t_save", "t")):
+        OD.set_physical_bc3d(g, s[k], var)
+    for k in ("mu_1", "mu", "mudf"):
+        OD.set_physical_bc2d(g, s[k], "t")
+    for it in range(1, nsub + 1):
+        _oracle_substep(g, s, it, nsub, dts)
+    OD.calc_mu_uv_1(g, s["muts"], s["muus"], s["muvs"])
+    OD.small_step_finish(g, s, nsub, dts, rk_step)
+    if rk_step == 3:
+        for k, var in (("ru_m", "u"), ("rv_m", "v"), ("ww_m", "w")):
+            OD.set_physical_bc3d(g, s[k], var)
+        OD.set_physical_bc2d(g, s["mut"], "t")
+        OD.set_physical_bc2d(g, s["muts"], "t")
+
+
+STAGE_OUT = ("u", "v", "w", "ph", "t", "mu", "muts", "p", "al", "ww", "ru_m", "rv_m", "ww_m", "t_2save", "pm1")
+
+
+@pytest.mark.parametrize("rk_step", [2, 3])
+def test_composed_acoustic_stage_and_its_adjoint_against_the_oracle(rk_step):
+    """pywrf_b200.adjoint.acoustic_stage (small_step_prep, calc_p_rho,
+    calc_coef_w, the substeps, calc_mu_uv_1 and small_step_finish composed
+    from their Functions) on the small case's state after the tendencies of
+    step 2, stage 2 (2 substeps) and stage 3 (4 substeps): the outputs
+    against the float64 oracle (3x the float32 oracle's own error plus 2e-6),
+    and the gradient of a seeded linear functional of 15 outputs in 12
+    inputs against float64 central differences of the oracle's stage."""
+    import copy
+
+    from helpers import SMALL
+    from oracle.model import OracleModel
+    from pywrf_b200 import synthetic
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    snap = {}
+    tag = f"s{rk_step}.tend"
+
+    def probe(name, m):
+        if name == tag and not snap:
+            snap.update(copy.deepcopy(m.st))
+
+    m = OracleModel(g, inputs, bdy, np.float64)
+    m.run(1)
+    m.step(2, probe)
+    dts = g.dt / g.soundsteps
+    nsub = g.soundsteps // 2 if rk_step == 2 else g.soundsteps
+
+    def oracle_run(dtype, pert=None):
+        s = {k: (np.array(v, dtype) if isinstance(v, np.ndarray) else v) for k, v in snap.items()}
+        if pert:
+            for k, d in pert.items():
+                s[k] = s[k] + d
+        _oracle_acoustic_stage(g, s, rk_step, nsub, dts)
+        return s
+
+    o64, o32 = oracle_run(np.float64), oracle_run(np.float32)
+    st = {k: _cuda(snap[k]).requires_grad_(True) for k in adjoint.STAGE_STATE}
+    data = {k: _cuda(snap[k]) for k in adjoint.STAGE_DATA}
+    sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=float(snap["cf1"]), cf2=float(snap["cf2"]),
+              cf3=float(snap["cf3"]), rdx=g.rdx, rdy=g.rdy)
+    out = adjoint.acoustic_stage(st, data, rk_step, nsub, dts, **sc)
+    bad = []
+    for k in STAGE_OUT:
+        c = out[k].detach().double().cpu().numpy()
+        err, floor = rel_l2(c, o64[k]), rel_l2(o32[k], o64[k])
+        if not err <= 3.0 * floor + 2e-6:
+            bad.append((k, err, floor))
+    assert not bad, bad
+    rng = np.random.default_rng(78)
+    cot = {k: rng.standard_normal(np.shape(snap[k])) for k in STAGE_OUT}
+    sum((out[k].double() * torch.tensor(cot[k], device="cuda")).sum() for k in STAGE_OUT).backward()
+
+    def loss(pert):
+        s = oracle_run(np.float64, pert)
+        return sum(float((s[k] * cot[k]).sum()) for k in STAGE_OUT)
+
+    for name in ("u", "v", "t", "ph", "w", "mu", "mu_1", "p", "ww", "ru_tend", "t_tend", "ph_tend"):
+        gr = st[name].grad.double().cpu().numpy()
+        d = rng.standard_normal(gr.shape)
+        eps = 1e-6 * float(np.abs(snap[name]).max() or 1.0)
+        fd = (loss({name: eps * d}) - loss({name: -eps * d})) / (2 * eps)
+        an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
+        assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
