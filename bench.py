@@ -82,6 +82,7 @@ def parse():
     ap.add_argument("--phase-steps", type=int, default=3, help="eager steps timed per phase for the roofline")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the network (harvest, training, surrogate run)")
     ap.add_argument("--no-config4", action="store_true", help="skip the 512x512x61 plain-step figure")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the composed acoustic-stage forward + adjoint")
     ap.add_argument("--sur-seeds", type=int, default=5, help="integrations harvested for the network's training set")
     ap.add_argument("--sur-harvest-steps", type=int, default=80)
     ap.add_argument("--sur-epochs", type=int, default=200)
@@ -386,6 +387,10 @@ def run_ours(a):
     big = None
     if world == 1 and not a.no_config4:
         big = run_config4(hbm)
+    adj = {"unavailable": "no whole-step adjoint: the moisture update, the first stage's diffusion, the end-of-step "
+                          "boundary updates and WSM6 have no reverse kernels yet"}
+    if world == 1 and not a.no_adjoint:
+        adj["acoustic_stage"] = run_adjoint_stage(st, it, phase_ms)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -405,11 +410,7 @@ def run_ours(a):
                 "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan,
                 "surrogate": sur, "config4": big,
                 "reference_cpu": reference_cpu_record(f"{g.nx}x{g.ny}x{g.nz}"),
-                "adjoint": {"unavailable": "no whole-step adjoint yet: hand-written reverse-mode kernels exist for "
-                                           "advect_scalar, advect_u/v/w, relax_bdytend and the acoustic substep's "
-                                           "advance_uv, advance_mu_t, calc_coef_w, advance_w (implicit solve "
-                                           "included) and calc_p_rho (pywrf_b200.adjoint), not yet for the "
-                                           "forces, moisture, WSM6 or the step they compose"}}
+                "adjoint": adj}
         line["valid"] = nan == 0
         print(json.dumps(line), flush=True)
     it._graph = None
@@ -417,6 +418,71 @@ def run_ours(a):
         dist.destroy_process_group()
     if nan:
         raise SystemExit(f"NaN in the diagnosed pressure at {nan} point(s): the timed state is not a result")
+
+
+def run_adjoint_stage(st, it, phase_ms, reps=5):
+    """Forward + reverse pass of the acoustic part of RK stage 3 (4
+    substeps) composed from the hand-written operator adjoints
+    (pywrf_b200.adjoint.acoustic_stage) on the 240x240x41 state after the
+    tendencies of a step, timed with CUDA events (3 warm-up passes): stages
+    per second, beside the fused forward's time for the same part of a step
+    (stage 3's share of the acoustic phases in the step's probe timing)."""
+    import torch
+    from pywrf_b200 import _native as N_
+    from pywrf_b200 import adjoint as A
+
+    g = st.g
+    L = N_.lib()
+    h = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    gp = ctypes.byref(st.cgrid)
+    # a state after one step and the first stage's tendencies of the next
+    it.step()
+    for fn, args in (("wrf_step_begin", ()), ("wrf_rk_prep", (1,)), ("wrf_diff_stage1", ()), ("wrf_tend_stage", (1,))):
+        N_.check(getattr(L, fn)(gp, st.ptr, *args, h), fn)
+    torch.cuda.synchronize()
+    state = {k: st[k].detach().clone().requires_grad_(True) for k in A.STAGE_STATE}
+    data = {k: st[k] for k in A.STAGE_DATA}
+    sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=st.scal["cf1"], cf2=st.scal["cf2"],
+              cf3=st.scal["cf3"], rdx=g.rdx, rdy=g.rdy)
+    dts = g.dt / g.soundsteps
+    gen = torch.Generator(device=st["u"].device).manual_seed(5)
+    outs = ("u", "v", "w", "ph", "t", "mu", "p", "al", "ww", "ru_m", "rv_m", "ww_m")
+    cot = {k: torch.randn(st[k].shape, generator=gen, device=st[k].device) for k in outs}
+
+    def one():
+        for v in state.values():
+            v.grad = None
+        o = A.acoustic_stage(state, data, 3, g.soundsteps, dts, **sc)
+        sum((o[k] * cot[k]).sum() for k in outs).backward()
+
+    def fwd():
+        with torch.no_grad():
+            A.acoustic_stage(state, data, 3, g.soundsteps, dts, **sc)
+
+    res = {}
+    for name, fn in (("fwd_adj", one), ("fwd_composed", fwd)):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        res[name] = e0.elapsed_time(e1) / reps
+    # stage 3's share of the step's acoustic phases: a third of the prep and
+    # finish, four of the seven substeps
+    fused = (phase_ms.get("acprep", 0.0) + phase_ms.get("acfinish", 0.0)) / 3.0 + \
+        sum(phase_ms.get(k, 0.0) for k in ("sub.uv", "sub.col", "sub.bc")) * 4.0 / 7.0
+    return {"what": "acoustic part of RK stage 3 (small_step_prep, calc_p_rho, calc_coef_w, 4 substeps, "
+                    "small_step_finish) composed from the operator adjoints, 240x240x41",
+            "fwd_adj_ms": res["fwd_adj"], "fwd_adj_stages_per_s": 1e3 / res["fwd_adj"],
+            "fwd_composed_ms": res["fwd_composed"],
+            "fused_step_forward_ms_per_stage": fused,
+            "reference_autograd": "not comparable: the reference's autograd cannot run backward through its "
+                                  "acoustic solve (in-place updates of saved operands in calc_coef_w, advance_uv, "
+                                  "advance_w)"}
 
 
 def run_config4(hbm):
