@@ -148,10 +148,15 @@ __global__ void k_spec_ph_adj(Grid g, S s, S bar, float dt) {
   // cancellation of the difference (which float32 would round to a few
   // significant digits)
   bar[WF_PH_SAVE][p] += -(dt * s[WF_MU_TEND][c]) / mt * P;
-  const float mob = (ph + ps) / mt * P;
-  const float mtb = -(ph * mu_old + dt * pt + ps * mu_old) / (mt * mt) * P;
-  atomicAdd(&bar[WF_MUTS][c], mob + mtb);
-  atomicAdd(&bar[WF_MU_TEND][c], -dt * mob);
+  // with mu_old = muts - dt mu_tend the update is ph + ph_save mu_old / muts
+  // - ph_save + (dt ph_tend - ph dt mu_tend) / muts ... in sum:
+  //   d/d mu_tend = -dt (ph + ph_save) / muts
+  //   d/d muts    = dt ((ph + ph_save) mu_tend - ph_tend) / muts^2
+  // (the second formed directly: the sum of the partial derivatives through
+  // mu_old and through muts cancels to a few digits in float32)
+  const float mtn = s[WF_MU_TEND][c];
+  atomicAdd(&bar[WF_MUTS][c], dt * ((ph + ps) * mtn - pt) / (mt * mt) * P);
+  atomicAdd(&bar[WF_MU_TEND][c], -dt * (ph + ps) / mt * P);
 }
 
 }  // namespace
