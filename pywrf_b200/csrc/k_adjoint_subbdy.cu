@@ -148,8 +148,8 @@ __global__ void k_spec_ph_adj(Grid g, S s, S bar, float dt) {
   // cancellation of the difference (which float32 would round to a few
   // significant digits)
   bar[WF_PH_SAVE][p] += -(dt * s[WF_MU_TEND][c]) / mt * P;
-  // with mu_old = muts - dt mu_tend the update is ph + ph_save mu_old / muts
-  // - ph_save + (dt ph_tend - ph dt mu_tend) / muts ... in sum:
+  // with mu_old = muts - dt mu_tend the update is
+  //   ph - dt ((ph + ph_save) mu_tend - ph_tend) / muts, so
   //   d/d mu_tend = -dt (ph + ph_save) / muts
   //   d/d muts    = dt ((ph + ph_save) mu_tend - ph_tend) / muts^2
   // (the second formed directly: the sum of the partial derivatives through
