@@ -277,6 +277,22 @@ int wrf_small_step_finish(const WrfGrid* g, const WrfState* s, float dts, int ns
 /* Its adjoint: as wrf_small_step_prep_adj; work: 2 * ny * nx floats. */
 int wrf_small_step_finish_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float dts, int nsub,
                               int rk_step, float* work, void* stream);
+/* wrf_dynamics.py:3100-3148 rk_addtend_dry on the state table: at rk_step 1
+ * the physics tendencies take the saved fields first; every stage adds them
+ * (divided by the map factor) to ru/rv/rw/ph/t_tend, theta also mut
+ * h_diabatic / msfty, and mu_tend += mu_tendf. */
+int wrf_addtend(const WrfGrid* g, const WrfState* s, int rk_step, void* stream);
+/* Its adjoint: the tendencies' cotangents pass through; those of the
+ * updated physics tendencies are rewritten to the incoming ones'; the saved
+ * fields, mut and h_diabatic accumulate (+=). */
+int wrf_addtend_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, int rk_step, void* stream);
+/* wrf_boundary.py:189-241 spec_bdytend: the specified rows of tend take the
+ * boundary tendency (x sides [nk][ny][5], y sides [nk][5][nx]; var 'u', 'v',
+ * 't' below level nz-1, 'h' all levels, 'm' 2-D). */
+int wrf_spec_bdytend(const WrfGrid* g, float* tend, const float* txs, const float* txe, const float* tys,
+                     const float* tye, char var, void* stream);
+/* Its adjoint: sets those rows of tend_bar to zero (in place). */
+int wrf_spec_bdytend_adj(const WrfGrid* g, float* tend_bar, char var, void* stream);
 int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream);
 /* Its adjoint (reverse mode): sbar holds, under the same field ids, the
  * cotangents of the updated u and v (which are also those of the incoming

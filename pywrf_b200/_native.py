@@ -148,6 +148,14 @@ def lib() -> ctypes.CDLL:
     L.wrf_small_step_finish.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_float, ip, ip, vp]
     L.wrf_small_step_finish_adj.restype = ip
     L.wrf_small_step_finish_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, ip, ip, vp, vp]
+    L.wrf_addtend.restype = ip
+    L.wrf_addtend.argtypes = [ctypes.POINTER(WrfGridC), vp, ip, vp]
+    L.wrf_addtend_adj.restype = ip
+    L.wrf_addtend_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ip, vp]
+    L.wrf_spec_bdytend.restype = ip
+    L.wrf_spec_bdytend.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp, vp, vp, ctypes.c_char, vp]
+    L.wrf_spec_bdytend_adj.restype = ip
+    L.wrf_spec_bdytend_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_char, vp]
     L.wrf_advance_uv_adj.restype = ip
     L.wrf_advance_uv_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, vp]
     L.wrf_advect_momentum_adj.restype = ip

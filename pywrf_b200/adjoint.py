@@ -1017,3 +1017,113 @@ def acoustic_stage(st: dict, data: dict, rk_step: int, nsub: int, dts: float, *,
         for k, var in (("ru_m", "u"), ("rv_m", "v"), ("ww_m", "w"), ("mut", "t"), ("muts", "t")):
             s[k] = halo(s[k], var, rdx, rdy)
     return s
+
+
+class _Addtend:
+    name = "wrf_addtend"
+    fields = ("ru_tend", "rv_tend", "rw_tend", "ph_tend", "t_tend", "mu_tend", "ru_tendf", "rv_tendf", "rw_tendf",
+              "ph_tendf", "t_tendf", "mu_tendf", "u_save", "v_save", "w_save", "ph_save", "t_save", "h_diabatic", "mut")
+    outputs = ("ru_tend", "rv_tend", "rw_tend", "ph_tend", "t_tend", "mu_tend", "ru_tendf", "rv_tendf", "rw_tendf",
+               "ph_tendf", "t_tendf")
+    data = ("msfty", "msfuy", "msfvx", "msfvx_inv")
+
+    def __init__(self, rk_step):
+        self.rk_step = rk_step
+
+    def fwd(self, cg, tab, stream):
+        return N.lib().wrf_addtend(ctypes.byref(cg), tab, self.rk_step, stream)
+
+    def adj(self, cg, tab, btab, stream):
+        return N.lib().wrf_addtend_adj(ctypes.byref(cg), tab, btab, self.rk_step, stream)
+
+
+def addtend(st: dict, data: dict, rk_step: int, rdx, rdy) -> dict:
+    """Differentiable rk_addtend_dry (pywrf/wrf_dynamics.py:3100-3148):
+    returns ``st`` with the tendencies (and at stage 1 the physics
+    tendencies) replaced."""
+    op = _Addtend(rk_step)
+    cg = scalar_grid(st["ru_tend"].shape, rdx, rdy)
+    outs = _TableOp.apply(op, cg, *[st[k] for k in op.fields], *[data[k] for k in op.data])
+    return {**st, **dict(zip(op.outputs, outs))}
+
+
+class SpecBdytend(torch.autograd.Function):
+    """tend' = spec_bdytend(tend, boundary tendencies, var): the specified
+    rows take the boundary file's tendency (data); ``scal`` = (var, rdx,
+    rdy), then the x-start, x-end, y-start, y-end boundary tendencies."""
+
+    @staticmethod
+    def forward(ctx, scal, tend, txs, txe, tys, tye):
+        _cuda_only(tend, txs, txe, tys, tye)
+        var = str(scal[0])
+        shape = (12,) + tuple(tend.shape) if tend.dim() == 2 else tend.shape
+        cg = scalar_grid(shape, float(scal[1]), float(scal[2]))
+        out = tend.detach().clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(tend.device):
+            rc = N.lib().wrf_spec_bdytend(ctypes.byref(cg), _ptr(out), _ptr(txs), _ptr(txe), _ptr(tys), _ptr(tye),
+                                          var.encode(), stream)
+        N.check(rc, "wrf_spec_bdytend")
+        ctx.cg, ctx.var = cg, var
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        gin = gout.contiguous().clone()
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(gin.device):
+            rc = N.lib().wrf_spec_bdytend_adj(ctypes.byref(ctx.cg), _ptr(gin), ctx.var.encode(), stream)
+        N.check(rc, "wrf_spec_bdytend_adj")
+        return None, gin, None, None, None, None
+
+
+def spec_bdytend(tend, bt: dict, var: str, rdx, rdy):
+    """Differentiable spec_bdytend; ``bt`` maps txs txe tys tye to the
+    variable's boundary tendencies (solver layout)."""
+    return SpecBdytend.apply((var, rdx, rdy), tend, bt["txs"], bt["txe"], bt["tys"], bt["tye"])
+
+
+# the fields the dynamics part of RK stage 2 or 3 reads (state) beyond the
+# acoustic stage's
+DYN_STATE = tuple(dict.fromkeys(STAGE_STATE + PREP_FIELDS + FORCES_INPUTS + _Addtend.fields + ("moist",)))
+DYN_DATA = tuple(dict.fromkeys(STAGE_DATA + PREP_DATA + FORCES_DATA + _Addtend.data + ("msfux", "msfvx")))
+
+
+def dynamics_stage(st: dict, data: dict, bt: dict, rk_step: int, nsub: int, dts: float, *, epssm: float,
+                   emdiv: float, smdiv: float, cf1: float, cf2: float, cf3: float, cfn: float, cfn1: float,
+                   rdx: float, rdy: float) -> dict:
+    """The dynamics of RK stage 2 or 3 composed from the operators'
+    Functions, in the reference's order (pywrf/solver.py:736-1492):
+    rk_step_prep and its halo copies, the advection of u, v, w and theta, the
+    tendency terms, rk_addtend_dry, spec_bdytend of u, v, ph, t, mu, and the
+    acoustic part (:func:`acoustic_stage`).  (The first stage also has the
+    diffusion and boundary relaxation, which have no Functions yet.)  ``bt``
+    maps 'u', 'v', 'h', 't', 'm' to dicts of their boundary tendencies
+    (txs txe tys tye); returns the state after the acoustic steps."""
+    if rk_step not in (2, 3):
+        raise ValueError("dynamics_stage composes RK stages 2 and 3")
+    s = dict(st)
+    s.update(prep({k: s[k] for k in PREP_FIELDS}, {k: data[k] for k in PREP_DATA}, 127, rdx, rdy))
+    for k, var in (("ru", "u"), ("rv", "v"), ("rw", "w"), ("ww", "w"), ("php", "w"), ("alt", "t"), ("p", "p"),
+                   ("muu", "u"), ("muv", "v"), ("mut", "t"), ("al", "p"), ("ph", "w")):
+        s[k] = halo(s[k], var, rdx, rdy)
+    for k in ("ru_tend", "rv_tend", "rw_tend", "t_tend", "ph_tend", "u_save", "v_save", "w_save", "ph_save",
+              "t_save", "mu_tend", "mu_save"):
+        s[k] = torch.zeros_like(st[k])
+    z = lambda k: s[k]  # noqa: E731
+    s["ru_tend"] = advect_momentum(0, s["u"], z("ru_tend"), s["ru"], s["rv"], s["ww"], data["msfux"], None,
+                                   data["fnm"], data["fnp"], data["rdnw"], rdx, rdy)
+    s["rv_tend"] = advect_momentum(1, s["v"], z("rv_tend"), s["ru"], s["rv"], s["ww"], data["msfvy"], data["msfvx"],
+                                   data["fnm"], data["fnp"], data["rdnw"], rdx, rdy)
+    s["rw_tend"] = advect_momentum(2, s["w"], z("rw_tend"), s["ru"], s["rv"], s["ww"], data["msftx"], None,
+                                   data["fnm"], data["fnp"], data["rdn"], rdx, rdy)
+    s["t_tend"] = advect_scalar(s["t"], z("t_tend"), s["ru"], s["rv"], s["ww"], data["msftx"], data["fnm"],
+                                data["fnp"], data["rdnw"], rdx, rdy)
+    outs = forces({k: s[k] for k in FORCES_INPUTS}, {k: data[k] for k in FORCES_DATA}, 31, rdx, rdy, cf1, cf2, cf3,
+                  cfn, cfn1)
+    s.update(dict(zip(FORCES_OUTPUTS, outs)))
+    s = addtend(s, data, rk_step, rdx, rdy)
+    for k, var in (("ru_tend", "u"), ("rv_tend", "v"), ("ph_tend", "h"), ("t_tend", "t"), ("mu_tend", "m")):
+        s[k] = spec_bdytend(s[k], bt[var], var, rdx, rdy)
+    return acoustic_stage(s, data, rk_step, nsub, dts, epssm=epssm, emdiv=emdiv, smdiv=smdiv, cf1=cf1, cf2=cf2,
+                          cf3=cf3, rdx=rdx, rdy=rdy)

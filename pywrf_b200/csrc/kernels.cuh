@@ -52,6 +52,13 @@ int launch_spec_ph_adj(const Grid& g, const S& s, const S& b, float dt, cudaStre
 // calc_php) and their adjoints (k_adjoint_prep.cu)
 int launch_prep_ops(const Grid& g, const S& s, int ops, cudaStream_t st);
 int launch_prep_ops_adj(const Grid& g, const S& s, const S& b, int ops, cudaStream_t st);
+// rk_addtend_dry and spec_bdytend as stand-alone operators, and their
+// adjoints (k_adjoint_tend.cu); bt4: the x-start, x-end, y-start, y-end
+// boundary tendencies of the variable
+int launch_addtend_op(const Grid& g, const S& s, int rk_step, cudaStream_t st);
+int launch_addtend_op_adj(const Grid& g, const S& s, const S& b, int rk_step, cudaStream_t st);
+int launch_spec_tend(const Grid& g, float* tend, const float* const* bt4, char var, cudaStream_t st);
+int launch_spec_tend_adj(const Grid& g, float* tend_bar, char var, cudaStream_t st);
 // rk_addtend_dry + spec_bdytend (k_tend.cu)
 int launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st);
 // moisture advection with the time-averaged fluxes (k_tend.cu)

@@ -573,6 +573,15 @@ constexpr int kSsfCotangents[] = {WF_U, WF_U_SAVE, WF_V, WF_V_SAVE, WF_W, WF_W_S
                                   WF_T, WF_T_SAVE, WF_H_DIABATIC, WF_MU, WF_MU_SAVE, WF_MUT, WF_MUTS, WF_MUU, WF_MUV,
                                   WF_MUUS, WF_MUVS};
 
+// rk_addtend_dry's operands and cotangents
+constexpr int kAddtendOperands[] = {WF_RU_TEND, WF_RV_TEND, WF_RW_TEND, WF_PH_TEND, WF_T_TEND, WF_MU_TEND,
+                                    WF_RU_TENDF, WF_RV_TENDF, WF_RW_TENDF, WF_PH_TENDF, WF_T_TENDF, WF_MU_TENDF,
+                                    WF_U_SAVE, WF_V_SAVE, WF_W_SAVE, WF_PH_SAVE, WF_T_SAVE, WF_H_DIABATIC, WF_MUT,
+                                    WF_MSFTY, WF_MSFUY, WF_MSFVX, WF_MSFVX_INV};
+constexpr int kAddtendCotangents[] = {WF_RU_TEND, WF_RV_TEND, WF_RW_TEND, WF_PH_TEND, WF_T_TEND, WF_MU_TEND,
+                                      WF_RU_TENDF, WF_RV_TENDF, WF_RW_TENDF, WF_PH_TENDF, WF_T_TENDF, WF_MU_TENDF,
+                                      WF_U_SAVE, WF_V_SAVE, WF_W_SAVE, WF_PH_SAVE, WF_T_SAVE, WF_H_DIABATIC, WF_MUT};
+
 int state_of(const WrfState* in, const int* ids, int n, S& s) {
   if (!in) return fail(WRF_EINVAL, "null state");
   s = S{};
@@ -916,6 +925,57 @@ int wrf_small_step_finish_adj(const WrfGrid* gin, const WrfState* sin, const Wrf
   cudaGetLastError();
   launch_small_step_finish_adj(g, s, b, dts, nsub, rk_step, work, static_cast<cudaStream_t>(stream));
   return check_launch("small_step_finish_adj");
+}
+
+int wrf_addtend(const WrfGrid* gin, const WrfState* sin, int rk_step, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (rk_step < 1 || rk_step > 3) return fail(WRF_EINVAL, "addtend: rk_step is 1, 2 or 3");
+  S s;
+  if ((rc = state_of(sin, kAddtendOperands, sizeof(kAddtendOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_addtend_op(g, s, rk_step, static_cast<cudaStream_t>(stream));
+  return check_launch("addtend");
+}
+
+int wrf_addtend_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, int rk_step, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (rk_step < 1 || rk_step > 3) return fail(WRF_EINVAL, "addtend_adj: rk_step is 1, 2 or 3");
+  S s, b;
+  if ((rc = state_of(sin, kAddtendOperands, sizeof(kAddtendOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kAddtendCotangents, sizeof(kAddtendCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_addtend_op_adj(g, s, b, rk_step, static_cast<cudaStream_t>(stream));
+  return check_launch("addtend_adj");
+}
+
+int wrf_spec_bdytend(const WrfGrid* gin, float* tend, const float* txs, const float* txe, const float* tys,
+                     const float* tye, char var, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!tend || !txs || !txe || !tys || !tye) return fail(WRF_EINVAL, "null argument");
+  if (var != 'u' && var != 'v' && var != 't' && var != 'h' && var != 'm')
+    return fail(WRF_EINVAL, "spec_bdytend: var is u, v, t, h or m");
+  const float* bt4[4] = {txs, txe, tys, tye};
+  cudaGetLastError();
+  launch_spec_tend(g, tend, bt4, var, static_cast<cudaStream_t>(stream));
+  return check_launch("spec_bdytend");
+}
+
+int wrf_spec_bdytend_adj(const WrfGrid* gin, float* tend_bar, char var, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!tend_bar) return fail(WRF_EINVAL, "null argument");
+  if (var != 'u' && var != 'v' && var != 't' && var != 'h' && var != 'm')
+    return fail(WRF_EINVAL, "spec_bdytend_adj: var is u, v, t, h or m");
+  cudaGetLastError();
+  launch_spec_tend_adj(g, tend_bar, var, static_cast<cudaStream_t>(stream));
+  return check_launch("spec_bdytend_adj");
 }
 
 int wrf_advance_uv_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dts, void* stream) {

@@ -704,3 +704,136 @@ def test_composed_acoustic_stage_and_its_adjoint_against_the_oracle(rk_step):
         fd = (loss({name: eps * d}) - loss({name: -eps * d})) / (2 * eps)
         an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
         assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
+
+
+def _oracle_dynamics_stage(g, s, rk_step, nsub, dts):
+    """The dynamics of RK stage 2 or 3 of the oracle (its model loop,
+    solver.py:736-1492, without the first stage's diffusion) on ``s``."""
+    from oracle import boundary as OB
+    from oracle import dynamics as OD
+
+    OD.calculate_full(g, s["mut"], s["mub"], s["mu"])
+    OD.calc_mu_uv(g, s["mu"], s["mub"], s["muu"], s["muv"])
+    OD.couple_momentum(g, s["muu"], s["ru"], s["u"], s["msfu"], s["muv"], s["rv"], s["v"], s["msfvx_inv"], s["mut"],
+                       s["rw"], s["w"], s["msft"])
+    OD.calc_ww_cp(g, s["u"], s["v"], s["muu"], s["muv"], s["c1h"], s["ww"], s["msftx"], s["msfuy"], s["msfvx_inv"],
+                  s["dnw"])
+    OD.calc_cq(g, s["moist"], s["cqu"], s["cqv"], s["cqw"])
+    OD.calc_alt(g, s["alt"], s["al"], s["alb"])
+    OD.calc_php(g, s["php"], s["ph"], s["phb"])
+    for nm, var in (("ru", "u"), ("rv", "v"), ("rw", "w"), ("ww", "w"), ("php", "w"), ("alt", "t"), ("p", "p")):
+        OD.set_physical_bc3d(g, s[nm], var)
+    OD.set_physical_bc2d(g, s["muu"], "u")
+    OD.set_physical_bc2d(g, s["muv"], "v")
+    OD.set_physical_bc2d(g, s["mut"], "t")
+    OD.set_physical_bc3d(g, s["al"], "p")
+    OD.set_physical_bc3d(g, s["ph"], "w")
+    for nm in ("ru_tend", "rv_tend", "rw_tend", "t_tend", "ph_tend", "u_save", "v_save", "w_save", "ph_save", "t_save"):
+        s[nm] = np.zeros_like(s[nm])
+    s["mu_tend"] = np.zeros_like(s["mu_tend"])
+    s["mu_save"] = np.zeros_like(s["mu_save"])
+    OD.advect_u(g, s["u"], s["ru_tend"], s["ru"], s["rv"], s["ww"], s["msfux"], s["fnm"], s["fnp"], s["rdnw"])
+    OD.advect_v(g, s["v"], s["rv_tend"], s["ru"], s["rv"], s["ww"], s["msfvx"], s["msfvy"], s["fnm"], s["fnp"], s["rdnw"])
+    OD.advect_w(g, s["w"], s["rw_tend"], s["ru"], s["rv"], s["ww"], s["msftx"], s["fnm"], s["fnp"], s["rdn"])
+    OD.advect_scalar(g, s["t"], s["t_tend"], s["ru"], s["rv"], s["ww"], s["msftx"], s["fnm"], s["fnp"], s["rdnw"])
+    OD.rhs_ph(g, s["ph_tend"], s["u"], s["v"], s["ww"], s["ph"], s["phb"], s["w"], s["mut"], s["muu"], s["muv"],
+              s["fnm"], s["fnp"], s["rdnw"], s["cfn"], s["cfn1"], s["msfux"], s["msfvy"], s["msfty"])
+    OD.horizontal_pressure_gradient(g, s["ru_tend"], s["rv_tend"], s["ph"], s["alt"], s["p"], s["pb"], s["al"],
+                                    s["php"], s["cqu"], s["cqv"], s["muu"], s["muv"], s["mu"], s["fnm"], s["fnp"],
+                                    s["rdnw"], s["cf1"], s["cf2"], s["cf3"], s["msfux"], s["msfuy"], s["msfvx"],
+                                    s["msfvy"])
+    OD.pg_buoy_w(g, s["rw_tend"], s["p"], s["cqw"], s["mu"], s["mub"], s["rdnw"], s["rdn"], s["msfty"])
+    OD.coriolis(g, s["ru"], s["rv"], s["rw"], s["ru_tend"], s["rv_tend"], s["rw_tend"], s["msftx"], s["msfty"],
+                s["msfux"], s["msfuy"], s["msfvx"], s["msfvy"], s["f"], s["e"], s["sina"], s["cosa"], s["fnm"],
+                s["fnp"])
+    OD.curvature(g, s["ru"], s["rv"], s["rw"], s["u"], s["v"], s["ru_tend"], s["rv_tend"], s["rw_tend"], s["msfux"],
+                 s["msfuy"], s["msfvx"], s["msfvy"], s["msftx"], s["msfty"], s["fnm"], s["fnp"])
+    OD.rk_addtend_dry(g, s["ru_tend"], s["rv_tend"], s["rw_tend"], s["ph_tend"], s["t_tend"], s["ru_tendf"],
+                      s["rv_tendf"], s["rw_tendf"], s["ph_tendf"], s["t_tendf"], s["u_save"], s["v_save"],
+                      s["w_save"], s["ph_save"], s["t_save"], s["mu_tend"], s["mu_tendf"], rk_step, s["h_diabatic"],
+                      s["mut"], s["msfty"], s["msfuy"], s["msfvx"], s["msfvx_inv"])
+    bd = s["bdy"]
+    OB.spec_bdytend(g, s["ru_tend"], bd["u"], "u")
+    OB.spec_bdytend(g, s["rv_tend"], bd["v"], "v")
+    OB.spec_bdytend(g, s["ph_tend"], bd["ph"], "h")
+    OB.spec_bdytend(g, s["t_tend"], bd["t"], "t")
+    OB.spec_bdytend(g, s["mu_tend"][None], bd["mu"], "m")
+    _oracle_acoustic_stage(g, s, rk_step, nsub, dts)
+
+
+@pytest.mark.parametrize("rk_step", [2, 3])
+def test_composed_dynamics_stage_and_its_adjoint_against_the_oracle(rk_step):
+    """pywrf_b200.adjoint.dynamics_stage (rk_step_prep, the advection of u, v,
+    w, theta, the tendency terms, rk_addtend_dry, spec_bdytend and the
+    acoustic part, composed from their Functions) from the small case's state
+    at the start of stage 2 / 3 of step 2: the outputs against the float64
+    oracle (3x the float32 oracle's own error plus 2e-6) and the gradient of a
+    seeded linear functional of 15 outputs in 10 inputs against float64
+    central differences of the oracle's stage."""
+    import copy
+
+    from helpers import SMALL
+    from oracle.model import OracleModel
+    from pywrf_b200 import synthetic
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    snap = {}
+    tag = f"s{rk_step - 1}.moist"
+
+    def probe(name, m):
+        if name == tag and not snap:
+            snap.update(copy.deepcopy(m.st))
+
+    m = OracleModel(g, inputs, bdy, np.float64)
+    m.run(1)
+    m.step(2, probe)
+    dts = g.dt / g.soundsteps
+    nsub = g.soundsteps // 2 if rk_step == 2 else g.soundsteps
+
+    def cast(v, dtype):
+        if isinstance(v, np.ndarray):
+            return np.array(v, dtype)
+        if isinstance(v, dict):
+            return {k: cast(x, dtype) for k, x in v.items()}
+        return v
+
+    def oracle_run(dtype, pert=None):
+        s = {k: cast(v, dtype) for k, v in snap.items()}
+        if pert:
+            for k, d in pert.items():
+                s[k] = s[k] + d
+        _oracle_dynamics_stage(g, s, rk_step, nsub, dts)
+        return s
+
+    o64, o32 = oracle_run(np.float64), oracle_run(np.float32)
+    st = {k: _cuda(snap[k]).requires_grad_(True) for k in adjoint.DYN_STATE}
+    data = {k: _cuda(snap[k]) for k in adjoint.DYN_DATA}
+    bname = {"u": "u", "v": "v", "h": "ph", "t": "t", "m": "mu"}
+    bt = {v: {s_: _cuda(snap["bdy"][f][s_]) for s_ in ("txs", "txe", "tys", "tye")} for v, f in bname.items()}
+    sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=float(snap["cf1"]), cf2=float(snap["cf2"]),
+              cf3=float(snap["cf3"]), cfn=float(snap["cfn"]), cfn1=float(snap["cfn1"]), rdx=g.rdx, rdy=g.rdy)
+    out = adjoint.dynamics_stage(st, data, bt, rk_step, nsub, dts, **sc)
+    bad = []
+    for k in STAGE_OUT:
+        c = out[k].detach().double().cpu().numpy()
+        err, floor = rel_l2(c, o64[k]), rel_l2(o32[k], o64[k])
+        if not err <= 3.0 * floor + 2e-6:
+            bad.append((k, err, floor))
+    assert not bad, bad
+    rng = np.random.default_rng(79)
+    cot = {k: rng.standard_normal(np.shape(snap[k])) for k in STAGE_OUT}
+    sum((out[k].double() * torch.tensor(cot[k], device="cuda")).sum() for k in STAGE_OUT).backward()
+
+    def loss(pert):
+        s = oracle_run(np.float64, pert)
+        return sum(float((s[k] * cot[k]).sum()) for k in STAGE_OUT)
+
+    for name in ("u", "v", "t", "ph", "w", "mu", "mu_1", "p", "moist", "ru_tendf"):
+        gr = st[name].grad.double().cpu().numpy()
+        d = rng.standard_normal(gr.shape)
+        eps = 1e-6 * float(np.abs(snap[name]).max() or 1.0)
+        fd = (loss({name: eps * d}) - loss({name: -eps * d})) / (2 * eps)
+        an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
+        assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
