@@ -293,6 +293,18 @@ int wrf_spec_bdytend(const WrfGrid* g, float* tend, const float* txs, const floa
                      const float* tye, char var, void* stream);
 /* Its adjoint: sets those rows of tend_bar to zero (in place). */
 int wrf_spec_bdytend_adj(const WrfGrid* g, float* tend_bar, char var, void* stream);
+/* wrf_dynamics.py:4055-4164, wrf_boundary.py:470-508 the moisture update of
+ * an RK stage on the state table: rk_update_scalar of qv .. qg (moist_old,
+ * moist_tend, advect_tend, mu_1, mu, mub, msfty), flow_dep_bdy of qc .. qg
+ * (ru_m, rv_m) and calc_p_rho_phi (al, p from ph, t, qv, alb, pb, mu, muts);
+ * NaN in the diagnosed p is counted in the status words. */
+int wrf_moist_update(const WrfGrid* g, const WrfState* s, int rk_step, float dt_rk, void* stream);
+/* Its adjoint: the cotangents of moist (and at rk_step 1 moist_old), al and
+ * p are rewritten to those of the incoming values; those of moist_tend,
+ * advect_tend, mu_1, mu, mub, alb, muts, ph, pb, t (and moist_old after the
+ * first stage) are accumulated; work: nz * ny * nx floats. */
+int wrf_moist_update_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, int rk_step, float dt_rk,
+                         float* work, void* stream);
 int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream);
 /* Its adjoint (reverse mode): sbar holds, under the same field ids, the
  * cotangents of the updated u and v (which are also those of the incoming

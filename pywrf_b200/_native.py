@@ -156,6 +156,10 @@ def lib() -> ctypes.CDLL:
     L.wrf_spec_bdytend.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp, vp, vp, ctypes.c_char, vp]
     L.wrf_spec_bdytend_adj.restype = ip
     L.wrf_spec_bdytend_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_char, vp]
+    L.wrf_moist_update.restype = ip
+    L.wrf_moist_update.argtypes = [ctypes.POINTER(WrfGridC), vp, ip, ctypes.c_float, vp]
+    L.wrf_moist_update_adj.restype = ip
+    L.wrf_moist_update_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ip, ctypes.c_float, vp, vp]
     L.wrf_advance_uv_adj.restype = ip
     L.wrf_advance_uv_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, vp]
     L.wrf_advect_momentum_adj.restype = ip

@@ -1127,3 +1127,62 @@ def dynamics_stage(st: dict, data: dict, bt: dict, rk_step: int, nsub: int, dts:
         s[k] = spec_bdytend(s[k], bt[var], var, rdx, rdy)
     return acoustic_stage(s, data, rk_step, nsub, dts, epssm=epssm, emdiv=emdiv, smdiv=smdiv, cf1=cf1, cf2=cf2,
                           cf3=cf3, rdx=rdx, rdy=rdy)
+
+
+class _MoistUpdate:
+    name = "wrf_moist_update"
+    fields = ("moist", "moist_old", "moist_tend", "advect_tend", "mu", "mu_1", "mub", "al", "alb", "muts", "ph", "p",
+              "pb", "t")
+    outputs = ("moist", "moist_old", "al", "p")
+    data = ("msfty", "ru_m", "rv_m", "rdnw")
+
+    def __init__(self, rk_step, dt_rk, like):
+        self.rk_step, self.dt_rk = rk_step, float(dt_rk)
+        self.work = torch.empty(like.numel(), dtype=torch.float32, device=like.device)
+        self.status = torch.zeros(16, dtype=torch.int32, device=like.device)
+
+    def fwd(self, cg, tab, stream):
+        tab[N.field_names().index("status")] = self.status.data_ptr()
+        return N.lib().wrf_moist_update(ctypes.byref(cg), tab, self.rk_step, self.dt_rk, stream)
+
+    def adj(self, cg, tab, btab, stream):
+        tab[N.field_names().index("status")] = self.status.data_ptr()
+        return N.lib().wrf_moist_update_adj(ctypes.byref(cg), tab, btab, self.rk_step, self.dt_rk,
+                                            ctypes.c_void_p(self.work.data_ptr()), stream)
+
+
+def moist_stage(st: dict, data: dict, rk_step: int, dt_rk: float, rdx, rdy) -> dict:
+    """The moisture part of an RK stage after its acoustic steps, composed
+    from the operators' Functions (pywrf/solver.py:1548-1712, without the
+    first stage's moisture diffusion and qv relaxation): advection of qv ..
+    qg by the averaged fluxes, rk_update_scalar, flow_dep_bdy of qc .. qg,
+    calc_p_rho_phi and, before the last stage, the halo copies."""
+    s = dict(st)
+    moist = s["moist"]
+    adv = [torch.zeros_like(moist[0])]
+    for im in range(1, 7):
+        adv.append(advect_scalar(moist[im], torch.zeros_like(moist[im]), s["ru_m"], s["rv_m"], s["ww_m"],
+                                 data["msftx"], data["fnm"], data["fnp"], data["rdnw"], rdx, rdy))
+    s["advect_tend"] = torch.stack(adv)
+    op = _MoistUpdate(rk_step, dt_rk, moist[0])
+    cg = scalar_grid(s["u"].shape, rdx, rdy)
+    dd = {"msfty": data["msfty"], "ru_m": s["ru_m"].detach(), "rv_m": s["rv_m"].detach(), "rdnw": data["rdnw"]}
+    outs = _TableOp.apply(op, cg, *[s[k] for k in op.fields], *[dd[k] for k in op.data])
+    s.update(dict(zip(op.outputs, outs)))
+    if rk_step < 3:
+        for k, var in (("u", "U"), ("v", "V"), ("w", "w"), ("t", "p"), ("ph", "w"), ("mu", "t")):
+            s[k] = halo(s[k], var, rdx, rdy)
+        m = s["moist"]
+        s["moist"] = torch.stack([m[0]] + [halo(m[im], "p", rdx, rdy) for im in range(1, 7)])
+    return s
+
+
+RK_STATE = tuple(dict.fromkeys(DYN_STATE + _MoistUpdate.fields + ("ru_m", "rv_m", "ww_m")))
+RK_DATA = tuple(dict.fromkeys(DYN_DATA + ("msftx", "fnm", "fnp", "rdnw")))
+
+
+def rk_stage(st: dict, data: dict, bt: dict, rk_step: int, nsub: int, dts: float, dt_rk: float, **sc) -> dict:
+    """RK stage 2 or 3 of the step, composed: :func:`dynamics_stage` then
+    :func:`moist_stage`; ``sc`` as for :func:`dynamics_stage`."""
+    s = dynamics_stage(st, data, bt, rk_step, nsub, dts, **sc)
+    return moist_stage(s, data, rk_step, dt_rk, sc["rdx"], sc["rdy"])

@@ -582,6 +582,14 @@ constexpr int kAddtendCotangents[] = {WF_RU_TEND, WF_RV_TEND, WF_RW_TEND, WF_PH_
                                       WF_RU_TENDF, WF_RV_TENDF, WF_RW_TENDF, WF_PH_TENDF, WF_T_TENDF, WF_MU_TENDF,
                                       WF_U_SAVE, WF_V_SAVE, WF_W_SAVE, WF_PH_SAVE, WF_T_SAVE, WF_H_DIABATIC, WF_MUT};
 
+// the moisture update's operands (rk_update_scalar, flow_dep_bdy,
+// calc_p_rho_phi) and cotangents
+constexpr int kMoistOperands[] = {WF_MOIST, WF_MOIST_OLD, WF_MOIST_TEND, WF_ADVECT_TEND, WF_MU, WF_MU_1, WF_MUB,
+                                  WF_MSFTY, WF_RU_M, WF_RV_M, WF_AL, WF_ALB, WF_MUTS, WF_PH, WF_P, WF_PB, WF_T,
+                                  WF_RDNW, WF_STATUS};
+constexpr int kMoistCotangents[] = {WF_MOIST, WF_MOIST_OLD, WF_MOIST_TEND, WF_ADVECT_TEND, WF_MU, WF_MU_1, WF_MUB,
+                                    WF_AL, WF_ALB, WF_MUTS, WF_PH, WF_P, WF_PB, WF_T};
+
 int state_of(const WrfState* in, const int* ids, int n, S& s) {
   if (!in) return fail(WRF_EINVAL, "null state");
   s = S{};
@@ -976,6 +984,33 @@ int wrf_spec_bdytend_adj(const WrfGrid* gin, float* tend_bar, char var, void* st
   cudaGetLastError();
   launch_spec_tend_adj(g, tend_bar, var, static_cast<cudaStream_t>(stream));
   return check_launch("spec_bdytend_adj");
+}
+
+int wrf_moist_update(const WrfGrid* gin, const WrfState* sin, int rk_step, float dt_rk, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (rk_step < 1 || rk_step > 3) return fail(WRF_EINVAL, "moist_update: rk_step is 1, 2 or 3");
+  S s;
+  if ((rc = state_of(sin, kMoistOperands, sizeof(kMoistOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_moist(g, s, rk_step, dt_rk, static_cast<cudaStream_t>(stream));
+  return check_launch("moist_update");
+}
+
+int wrf_moist_update_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, int rk_step, float dt_rk,
+                         float* work, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (rk_step < 1 || rk_step > 3) return fail(WRF_EINVAL, "moist_update_adj: rk_step is 1, 2 or 3");
+  if (!work) return fail(WRF_EINVAL, "moist_update_adj: work (nz*ny*nx floats) is required");
+  S s, b;
+  if ((rc = state_of(sin, kMoistOperands, sizeof(kMoistOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kMoistCotangents, sizeof(kMoistCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_moist_adj(g, s, b, rk_step, dt_rk, work, static_cast<cudaStream_t>(stream));
+  return check_launch("moist_update_adj");
 }
 
 int wrf_advance_uv_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float dts, void* stream) {

@@ -837,3 +837,110 @@ def test_composed_dynamics_stage_and_its_adjoint_against_the_oracle(rk_step):
         fd = (loss({name: eps * d}) - loss({name: -eps * d})) / (2 * eps)
         an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
         assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
+
+
+def _oracle_rk_stage(g, s, rk_step, nsub, dts, dt_rk):
+    """RK stage 2 or 3 of the oracle: the dynamics, then the moisture part
+    (its model loop, solver.py:1548-1712)."""
+    from oracle import boundary as OB
+    from oracle import dynamics as OD
+
+    _oracle_dynamics_stage(g, s, rk_step, nsub, dts)
+    s["advect_tend"] = s["advect_tend"].copy()
+    for im in range(1, 7):
+        s["advect_tend"][im][0:g.nz, g.jts:g.jte, g.its:g.ite] = 0.0
+        OD.advect_scalar(g, s["moist"][im], s["advect_tend"][im], s["ru_m"], s["rv_m"], s["ww_m"], s["msftx"],
+                         s["fnm"], s["fnp"], s["rdnw"])
+    OD.rk_update_scalar(g, s["moist_old"], s["moist"], s["moist_tend"], s["advect_tend"], s["msfty"], s["mu_1"],
+                        s["mu"], s["mub"], rk_step, dt_rk)
+    for im in range(2, 7):
+        OB.flow_dep_bdy(g, s["moist"][im], s["ru_m"], s["rv_m"])
+    OD.calc_p_rho_phi(g, s["moist"][1], s["al"], s["alb"], s["mu"], s["muts"], s["ph"], s["p"], s["pb"], s["t"],
+                      s["rdnw"])
+    if rk_step < 3:
+        for nm, var in (("u", "U"), ("v", "V"), ("w", "w"), ("t", "p"), ("ph", "w")):
+            OD.set_physical_bc3d(g, s[nm], var)
+        OD.set_physical_bc2d(g, s["mu"], "t")
+        for im in range(1, 7):
+            OD.set_physical_bc3d(g, s["moist"][im], "p")
+
+
+RK_OUT = STAGE_OUT + ("moist",)
+
+
+@pytest.mark.parametrize("rk_step", [2, 3])
+def test_composed_rk_stage_and_its_adjoint_against_the_oracle(rk_step):
+    """pywrf_b200.adjoint.rk_stage (dynamics_stage, then the moisture
+    advection, rk_update_scalar, flow_dep_bdy and calc_p_rho_phi) from the
+    small case's state at the start of stage 2 / 3 of step 2: the outputs
+    (moisture included) against the float64 oracle (3x the float32 oracle's
+    own error plus 2e-6), and the gradient of a seeded linear functional of
+    16 outputs in 8 inputs against float64 central differences of the
+    oracle's stage."""
+    import copy
+
+    from helpers import SMALL
+    from oracle.model import OracleModel
+    from pywrf_b200 import synthetic
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    snap = {}
+    tag = f"s{rk_step - 1}.moist"
+
+    def probe(name, m):
+        if name == tag and not snap:
+            snap.update(copy.deepcopy(m.st))
+
+    m = OracleModel(g, inputs, bdy, np.float64)
+    m.run(1)
+    m.step(2, probe)
+    dts = g.dt / g.soundsteps
+    nsub, dt_rk = (g.soundsteps // 2, 0.5 * g.dt) if rk_step == 2 else (g.soundsteps, g.dt)
+
+    def cast(v, dtype):
+        if isinstance(v, np.ndarray):
+            return np.array(v, dtype)
+        if isinstance(v, dict):
+            return {k: cast(x, dtype) for k, x in v.items()}
+        return v
+
+    def oracle_run(dtype, pert=None):
+        s = {k: cast(v, dtype) for k, v in snap.items()}
+        if pert:
+            for k, d in pert.items():
+                s[k] = s[k] + d
+        _oracle_rk_stage(g, s, rk_step, nsub, dts, dt_rk)
+        return s
+
+    o64, o32 = oracle_run(np.float64), oracle_run(np.float32)
+    st = {k: _cuda(snap[k]).requires_grad_(True) for k in adjoint.RK_STATE}
+    data = {k: _cuda(snap[k]) for k in adjoint.RK_DATA}
+    bname = {"u": "u", "v": "v", "h": "ph", "t": "t", "m": "mu"}
+    bt = {v: {s_: _cuda(snap["bdy"][f][s_]) for s_ in ("txs", "txe", "tys", "tye")} for v, f in bname.items()}
+    sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=float(snap["cf1"]), cf2=float(snap["cf2"]),
+              cf3=float(snap["cf3"]), cfn=float(snap["cfn"]), cfn1=float(snap["cfn1"]), rdx=g.rdx, rdy=g.rdy)
+    out = adjoint.rk_stage(st, data, bt, rk_step, nsub, dts, dt_rk, **sc)
+    bad = []
+    for k in RK_OUT:
+        c = out[k].detach().double().cpu().numpy()
+        err, floor = rel_l2(c, o64[k]), rel_l2(o32[k], o64[k])
+        if not err <= 3.0 * floor + 2e-6:
+            bad.append((k, err, floor))
+    assert not bad, bad
+    rng = np.random.default_rng(80)
+    cot = {k: rng.standard_normal(np.shape(snap[k])) for k in RK_OUT}
+    sum((out[k].double() * torch.tensor(cot[k], device="cuda")).sum() for k in RK_OUT).backward()
+
+    def loss(pert):
+        s = oracle_run(np.float64, pert)
+        return sum(float((s[k] * cot[k]).sum()) for k in RK_OUT)
+
+    for name in ("u", "t", "ph", "w", "mu", "p", "moist", "moist_tend"):
+        gr = st[name].grad.double().cpu().numpy()
+        d = rng.standard_normal(gr.shape)
+        eps = 1e-6 * float(np.abs(snap[name]).max() or 1.0)
+        fd = (loss({name: eps * d}) - loss({name: -eps * d})) / (2 * eps)
+        an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
+        assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
