@@ -293,6 +293,45 @@ int wrf_spec_bdytend(const WrfGrid* g, float* tend, const float* txs, const floa
                      const float* tye, char var, void* stream);
 /* Its adjoint: sets those rows of tend_bar to zero (in place). */
 int wrf_spec_bdytend_adj(const WrfGrid* g, float* tend_bar, char var, void* stream);
+/* wrf_dynamics.py:491-536, 539-813, 816-995 the first stage's eddy
+ * viscosities on the state table: compute_diff_metrics (rdzw, zx, zy from
+ * ph, phb) with their halo copies, cal_deform_and_div's defor11, defor22,
+ * defor12 (from u, v) and the 2-D Smagorinsky calculate_km_kh (xkmh, xkhh);
+ * rdzw, zx, zy and the defor fields are scratch the call overwrites. */
+int wrf_eddy_viscosity(const WrfGrid* g, const WrfState* s, void* stream);
+/* Its adjoint: the cotangents of xkmh and xkhh are rewritten to those of
+ * their incoming values (which reach the output only where the region's
+ * formula does not apply); u, v and ph accumulate.  The scratch fields are
+ * recomputed from s; work: 6 * nz * ny * nx floats. */
+int wrf_eddy_viscosity_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, float* work, void* stream);
+/* wrf_dynamics.py:2623-2838 horizontal_diffusion of u ('u'), v ('v'), w
+ * ('w') or a mass-point scalar ('m'; with base, horizontal_diffusion_3dmp at
+ * :2841-2915, the diffusion of field - base): tend += the diffusion of
+ * field with column mass mut and eddy viscosity xk; s supplies the map
+ * factors (msfux, msfuy, msfvx, msfvy, msftx, msfty, msfvx_inv). */
+int wrf_horizontal_diffusion(const WrfGrid* g, const WrfState* s, char var, const float* field, const float* base,
+                             const float* mut, const float* xk, float* tend, void* stream);
+/* Its adjoint: field_bar, mut_bar and xk_bar accumulate (each may be null
+ * when not wanted); tend_bar passes through unchanged. */
+int wrf_horizontal_diffusion_adj(const WrfGrid* g, const WrfState* s, char var, const float* field,
+                                 const float* base, const float* mut, const float* xk, const float* tend_bar,
+                                 float* field_bar, float* mut_bar, float* xk_bar, void* stream);
+/* wrf_boundary.py:408-414 mass_weight: out = field * mut on levels below nk
+ * of the mass points (other points of out are left as they are). */
+int wrf_mass_weight(const WrfGrid* g, const float* field, const float* mut, float* out, int nk, void* stream);
+/* Its adjoint: field_bar and mut_bar accumulate. */
+int wrf_mass_weight_adj(const WrfGrid* g, const float* field, const float* mut, const float* out_bar,
+                        float* field_bar, float* mut_bar, int nk, void* stream);
+/* wrf_boundary.py:511-587, wrf_dynamics.py:4218-4324 the end-of-step
+ * lateral boundaries on the state table: spec_bdy_final of u, v, t, ph and
+ * qv (the specified rows take msf (bdy + dtbc bdy_tend) / mu with mu = muus,
+ * muvs or muts; dtbc is DSCAL[0]) then set_w_surface (w at the lowest
+ * level from the lowest three levels of u and v and the terrain ht). */
+int wrf_bdy_final(const WrfGrid* g, const WrfState* s, void* stream);
+/* Its adjoint: the cotangents of u, v, t, ph, qv and w are rewritten to
+ * those of their incoming values; muus, muvs and muts accumulate (the
+ * boundary arrays and ht are data). */
+int wrf_bdy_final_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, void* stream);
 /* wrf_dynamics.py:4055-4164, wrf_boundary.py:470-508 the moisture update of
  * an RK stage on the state table: rk_update_scalar of qv .. qg (moist_old,
  * moist_tend, advect_tend, mu_1, mu, mub, msfty), flow_dep_bdy of qc .. qg

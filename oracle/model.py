@@ -148,9 +148,12 @@ def ingest_bdy(g, bdy, it, dtype=np.float32):
 class OracleModel:
     """Numpy state + one-RK3-step driver following pywrf/solver.py:709-1910."""
 
-    def __init__(self, g, inputs, bdy, dtype=np.float32, theta_bias=None):
+    def __init__(self, g, inputs, bdy, dtype=np.float32, theta_bias=None, microphysics=True):
         self.g = g
         self.dtype = dtype
+        # False: the step of a model without microphysics (no moist physics
+        # prep, WSM6 or finish; the equation of state after them still runs)
+        self.microphysics = microphysics
         self.bdy_src = bdy
         # optional [nz, ny, nx] bias added to t_tend after rk_addtend_dry in
         # every RK stage (the learnable parameter of the adjoint configuration)
@@ -359,11 +362,13 @@ class OracleModel:
                     D.set_physical_bc3d(g, s["moist"][im], "p")
             probe(tag + ".moist", self)
         # microphysics (solver.py:1714-1766)
-        P.moist_physics_prep_em(g, s)
-        mo = s["moist"]
-        P.wsm6(g, s["th_phy"], mo[1], mo[2], mo[3], mo[4], mo[5], mo[6], s["rho"], s["pi_phy"], s["p_phy"], s["dz8w"],
-               float(dt), s["rainnc"], s["rainncv"], s["snownc"], s["snowncv"], s["graupelnc"], s["graupelncv"], s["sr"])
-        P.moist_physics_finish_em(g, s, dt)
+        if self.microphysics:
+            P.moist_physics_prep_em(g, s)
+            mo = s["moist"]
+            P.wsm6(g, s["th_phy"], mo[1], mo[2], mo[3], mo[4], mo[5], mo[6], s["rho"], s["pi_phy"], s["p_phy"],
+                   s["dz8w"], float(dt), s["rainnc"], s["rainncv"], s["snownc"], s["snowncv"], s["graupelnc"],
+                   s["graupelncv"], s["sr"])
+            P.moist_physics_finish_em(g, s, dt)
         D.calc_p_rho_phi(g, s["moist"][1], s["al"], s["alb"], s["mu"], s["muts"], s["ph"], s["p"], s["pb"], s["t"], s["rdnw"])
         probe("mp", self)
         # end-of-step boundaries (solver.py:1776-1910)

@@ -156,6 +156,23 @@ def lib() -> ctypes.CDLL:
     L.wrf_spec_bdytend.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp, vp, vp, ctypes.c_char, vp]
     L.wrf_spec_bdytend_adj.restype = ip
     L.wrf_spec_bdytend_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_char, vp]
+    L.wrf_eddy_viscosity.restype = ip
+    L.wrf_eddy_viscosity.argtypes = [ctypes.POINTER(WrfGridC), vp, vp]
+    L.wrf_eddy_viscosity_adj.restype = ip
+    L.wrf_eddy_viscosity_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp, vp]
+    L.wrf_horizontal_diffusion.restype = ip
+    L.wrf_horizontal_diffusion.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_char, vp, vp, vp, vp, vp, vp]
+    L.wrf_horizontal_diffusion_adj.restype = ip
+    L.wrf_horizontal_diffusion_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, ctypes.c_char, vp, vp, vp, vp, vp, vp,
+                                               vp, vp, vp]
+    L.wrf_mass_weight.restype = ip
+    L.wrf_mass_weight.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp, ip, vp]
+    L.wrf_mass_weight_adj.restype = ip
+    L.wrf_mass_weight_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp, vp, vp, ip, vp]
+    L.wrf_bdy_final.restype = ip
+    L.wrf_bdy_final.argtypes = [ctypes.POINTER(WrfGridC), vp, vp]
+    L.wrf_bdy_final_adj.restype = ip
+    L.wrf_bdy_final_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp]
     L.wrf_moist_update.restype = ip
     L.wrf_moist_update.argtypes = [ctypes.POINTER(WrfGridC), vp, ip, ctypes.c_float, vp]
     L.wrf_moist_update_adj.restype = ip

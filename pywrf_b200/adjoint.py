@@ -1083,30 +1083,191 @@ def spec_bdytend(tend, bt: dict, var: str, rdx, rdy):
     return SpecBdytend.apply((var, rdx, rdy), tend, bt["txs"], bt["txe"], bt["tys"], bt["tye"])
 
 
-# the fields the dynamics part of RK stage 2 or 3 reads (state) beyond the
-# acoustic stage's
-DYN_STATE = tuple(dict.fromkeys(STAGE_STATE + PREP_FIELDS + FORCES_INPUTS + _Addtend.fields + ("moist",)))
-DYN_DATA = tuple(dict.fromkeys(STAGE_DATA + PREP_DATA + FORCES_DATA + _Addtend.data + ("msfux", "msfvx")))
+HDIFF_DATA = ("msfux", "msfuy", "msfvx", "msfvy", "msftx", "msfty", "msfvx_inv")
+
+
+class HorizontalDiffusion(torch.autograd.Function):
+    """tend' = tend + horizontal_diffusion(field) (pywrf/wrf_dynamics.py:
+    2623-2915): ``scal`` = (var, rdx, rdy) with var 'u', 'v', 'w' or 'm' (a
+    mass-point scalar; with ``base``, the diffusion of field - base as
+    horizontal_diffusion_3dmp forms it), then the field, the incoming
+    tendency, the column mass, the eddy viscosity, ``base`` (data, or None)
+    and the seven map factors of HDIFF_DATA; gradients with respect to the
+    field, the tendency, the mass and the viscosity."""
+
+    @staticmethod
+    def forward(ctx, scal, field, tend, mut, xk, base, *maps):
+        _cuda_only(field, tend, mut, xk, base, *maps)
+        var = str(scal[0])
+        cg = scalar_grid(field.shape, float(scal[1]), float(scal[2]))
+        out = tend.detach().clone()
+        tab = _table(dict(zip(HDIFF_DATA, maps)))
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        bp = None if base is None else _ptr(base)
+        with torch.cuda.device(field.device):
+            rc = N.lib().wrf_horizontal_diffusion(ctypes.byref(cg), tab, var.encode(), _ptr(field), bp, _ptr(mut),
+                                                  _ptr(xk), _ptr(out), stream)
+        N.check(rc, "wrf_horizontal_diffusion")
+        ctx.cg, ctx.var, ctx.has_base = cg, var, base is not None
+        ctx.save_for_backward(field, mut, xk, *(() if base is None else (base,)), *maps)
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        saved = ctx.saved_tensors
+        field, mut, xk = saved[:3]
+        base = saved[3] if ctx.has_base else None
+        maps = saved[4:] if ctx.has_base else saved[3:]
+        gout = gout.contiguous()
+        fb, mb, kb = torch.zeros_like(field), torch.zeros_like(mut), torch.zeros_like(xk)
+        tab = _table(dict(zip(HDIFF_DATA, maps)))
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        bp = None if base is None else _ptr(base)
+        with torch.cuda.device(field.device):
+            rc = N.lib().wrf_horizontal_diffusion_adj(ctypes.byref(ctx.cg), tab, ctx.var.encode(), _ptr(field), bp,
+                                                      _ptr(mut), _ptr(xk), _ptr(gout), _ptr(fb), _ptr(mb), _ptr(kb),
+                                                      stream)
+        N.check(rc, "wrf_horizontal_diffusion_adj")
+        return (None, fb, gout, mb, kb, None) + (None,) * len(HDIFF_DATA)
+
+
+def horizontal_diffusion(var: str, field, tend, mut, xk, data: dict, rdx, rdy, base=None):
+    """Differentiable ``tend + horizontal_diffusion(field)``; ``data`` maps
+    the map factors of HDIFF_DATA."""
+    return HorizontalDiffusion.apply((var, rdx, rdy), field, tend, mut, xk, base, *[data[k] for k in HDIFF_DATA])
+
+
+class MassWeight(torch.autograd.Function):
+    """out = field * mut on levels below nk of the mass points, zero elsewhere
+    (mass_weight, pywrf/wrf_boundary.py:408-414); ``scal`` = (nk, rdx, rdy)."""
+
+    @staticmethod
+    def forward(ctx, scal, field, mut):
+        _cuda_only(field, mut)
+        nk = int(scal[0])
+        cg = scalar_grid(field.shape, float(scal[1]), float(scal[2]))
+        out = torch.zeros_like(field)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(field.device):
+            N.check(N.lib().wrf_mass_weight(ctypes.byref(cg), _ptr(field), _ptr(mut), _ptr(out), nk, stream),
+                    "wrf_mass_weight")
+        ctx.cg, ctx.nk = cg, nk
+        ctx.save_for_backward(field, mut)
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        field, mut = ctx.saved_tensors
+        gout = gout.contiguous()
+        fb, mb = torch.zeros_like(field), torch.zeros_like(mut)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        with torch.cuda.device(field.device):
+            rc = N.lib().wrf_mass_weight_adj(ctypes.byref(ctx.cg), _ptr(field), _ptr(mut), _ptr(gout), _ptr(fb),
+                                             _ptr(mb), ctx.nk, stream)
+        N.check(rc, "wrf_mass_weight_adj")
+        return None, fb, mb
+
+
+def mass_weight(field, mut, nk: int, rdx, rdy):
+    """Differentiable mass_weight on levels below ``nk``."""
+    return MassWeight.apply((nk, rdx, rdy), field, mut)
+
+
+class _EddyViscosity:
+    name = "wrf_eddy_viscosity"
+    fields = ("u", "v", "ph", "xkmh", "xkhh")
+    outputs = ("xkmh", "xkhh")
+    data = ("phb", "msfux", "msfuy", "msfvx", "msfvy", "msftx", "msfty", "fnm", "fnp", "dn", "dnw")
+    scratch = ("rdzw", "zx", "zy", "defor11", "defor22", "defor12")
+
+    def __init__(self, like):
+        n3 = like.numel()
+        self.buf = torch.empty(len(self.scratch) * n3, dtype=torch.float32, device=like.device)
+        self.views = [self.buf[q * n3:(q + 1) * n3] for q in range(len(self.scratch))]
+        self.work = torch.empty(6 * n3, dtype=torch.float32, device=like.device)
+
+    def _scratch(self, tab):
+        names = N.field_names()
+        for k, v in zip(self.scratch, self.views):
+            tab[names.index(k)] = v.data_ptr()
+
+    def fwd(self, cg, tab, stream):
+        self._scratch(tab)
+        return N.lib().wrf_eddy_viscosity(ctypes.byref(cg), tab, stream)
+
+    def adj(self, cg, tab, btab, stream):
+        self._scratch(tab)
+        return N.lib().wrf_eddy_viscosity_adj(ctypes.byref(cg), tab, btab, ctypes.c_void_p(self.work.data_ptr()),
+                                              stream)
+
+
+def eddy_viscosity(st: dict, data: dict, rdx, rdy, cf1: float, cf2: float, cf3: float):
+    """Differentiable first-stage eddy viscosities (compute_diff_metrics,
+    cal_deform_and_div, calculate_km_kh: pywrf/wrf_dynamics.py:491-995) from
+    u, v and ph; returns (xkmh, xkhh).  ``st`` also maps the incoming xkmh
+    and xkhh (which survive outside the formula's region)."""
+    op = _EddyViscosity(st["u"])
+    cg = scalar_grid(st["u"].shape, rdx, rdy)
+    cg.cf1, cg.cf2, cg.cf3 = float(cf1), float(cf2), float(cf3)
+    return _TableOp.apply(op, cg, *[st[k] for k in op.fields], *[data[k] for k in op.data])
+
+
+# the fields the dynamics part of an RK stage reads (state) beyond the
+# acoustic stage's, and its constant arrays (data)
+DYN_STATE = tuple(dict.fromkeys(STAGE_STATE + PREP_FIELDS + FORCES_INPUTS + _Addtend.fields +
+                                ("moist", "xkmh", "xkhh", "moist_tend")))
+DYN_DATA = tuple(dict.fromkeys(STAGE_DATA + PREP_DATA + FORCES_DATA + _Addtend.data + _EddyViscosity.data +
+                               HDIFF_DATA + ("t_init",)))
+
+
+def _first_stage_diffusion(s: dict, data: dict, bdy: dict, dtbc: float, rdx, rdy) -> dict:
+    """The first stage's horizontal diffusion of u, v, w and theta into the
+    physics tendencies and the lateral relaxation into the saved fields
+    (pywrf/solver.py:1112-1203)."""
+    hd = {k: data[k] for k in HDIFF_DATA}
+    for name in ("u", "v", "w"):
+        s[f"r{name}_tendf"] = horizontal_diffusion(name, s[name], s[f"r{name}_tendf"], s["mut"], s["xkmh"], hd,
+                                                   rdx, rdy)
+    s["t_tendf"] = horizontal_diffusion("m", s["t"], s["t_tendf"], s["mut"], s["xkhh"], hd, rdx, rdy,
+                                        base=data["t_init"])
+    nz = s["u"].shape[0]
+    s["u_save"] = relax_bdytend(s["ru"], s["u_save"], "u", dtbc, bdy["u"])
+    s["v_save"] = relax_bdytend(s["rv"], s["v_save"], "v", dtbc, bdy["v"])
+    s["ph_save"] = relax_bdytend(mass_weight(s["ph"], s["mut"], nz, rdx, rdy), s["ph_save"], "h", dtbc, bdy["h"])
+    s["t_save"] = relax_bdytend(mass_weight(s["t"], s["mut"], nz, rdx, rdy), s["t_save"], "t", dtbc, bdy["t"])
+    s["mu_tend"] = relax_bdytend(s["mu"][None], s["mu_tend"][None], "m", dtbc, bdy["m"])[0]
+    return s
 
 
 def dynamics_stage(st: dict, data: dict, bt: dict, rk_step: int, nsub: int, dts: float, *, epssm: float,
                    emdiv: float, smdiv: float, cf1: float, cf2: float, cf3: float, cfn: float, cfn1: float,
-                   rdx: float, rdy: float) -> dict:
-    """The dynamics of RK stage 2 or 3 composed from the operators'
-    Functions, in the reference's order (pywrf/solver.py:736-1492):
-    rk_step_prep and its halo copies, the advection of u, v, w and theta, the
-    tendency terms, rk_addtend_dry, spec_bdytend of u, v, ph, t, mu, and the
-    acoustic part (:func:`acoustic_stage`).  (The first stage also has the
-    diffusion and boundary relaxation, which have no Functions yet.)  ``bt``
-    maps 'u', 'v', 'h', 't', 'm' to dicts of their boundary tendencies
-    (txs txe tys tye); returns the state after the acoustic steps."""
-    if rk_step not in (2, 3):
-        raise ValueError("dynamics_stage composes RK stages 2 and 3")
+                   rdx: float, rdy: float, dtbc: float | None = None, theta_bias=None) -> dict:
+    """The dynamics of one RK stage composed from the operators' Functions,
+    in the reference's order (pywrf/solver.py:736-1492): rk_step_prep and
+    its halo copies; at the first stage the physics tendencies from zero, the
+    eddy viscosities and their halo copies; the advection of u, v, w and
+    theta, the tendency terms; at the first stage the horizontal diffusion
+    and the lateral relaxation; rk_addtend_dry (then ``theta_bias``, when
+    given, added to t_tend); spec_bdytend of u, v, ph, t, mu; and the
+    acoustic part (:func:`acoustic_stage`).  ``bt`` maps 'u', 'v', 'h', 't',
+    'm' to dicts of their boundary arrays (txs txe tys tye; at the first
+    stage also xs xe ys ye, with ``dtbc`` the boundary time); returns the
+    state after the acoustic steps."""
+    if rk_step not in (1, 2, 3):
+        raise ValueError("rk_step is 1, 2 or 3")
+    if rk_step == 1 and dtbc is None:
+        raise ValueError("the first stage's relaxation needs dtbc")
     s = dict(st)
     s.update(prep({k: s[k] for k in PREP_FIELDS}, {k: data[k] for k in PREP_DATA}, 127, rdx, rdy))
     for k, var in (("ru", "u"), ("rv", "v"), ("rw", "w"), ("ww", "w"), ("php", "w"), ("alt", "t"), ("p", "p"),
                    ("muu", "u"), ("muv", "v"), ("mut", "t"), ("al", "p"), ("ph", "w")):
         s[k] = halo(s[k], var, rdx, rdy)
+    if rk_step == 1:
+        for k in ("ru_tendf", "rv_tendf", "rw_tendf", "ph_tendf", "t_tendf", "mu_tendf", "moist_tend"):
+            s[k] = torch.zeros_like(st[k])
+        s["xkmh"], s["xkhh"] = eddy_viscosity(s, data, rdx, rdy, cf1, cf2, cf3)
+        s["xkmh"] = halo(s["xkmh"], "t", rdx, rdy)
+        s["xkhh"] = halo(s["xkhh"], "t", rdx, rdy)
     for k in ("ru_tend", "rv_tend", "rw_tend", "t_tend", "ph_tend", "u_save", "v_save", "w_save", "ph_save",
               "t_save", "mu_tend", "mu_save"):
         s[k] = torch.zeros_like(st[k])
@@ -1122,7 +1283,11 @@ def dynamics_stage(st: dict, data: dict, bt: dict, rk_step: int, nsub: int, dts:
     outs = forces({k: s[k] for k in FORCES_INPUTS}, {k: data[k] for k in FORCES_DATA}, 31, rdx, rdy, cf1, cf2, cf3,
                   cfn, cfn1)
     s.update(dict(zip(FORCES_OUTPUTS, outs)))
+    if rk_step == 1:
+        s = _first_stage_diffusion(s, data, bt, dtbc, rdx, rdy)
     s = addtend(s, data, rk_step, rdx, rdy)
+    if theta_bias is not None:
+        s["t_tend"] = s["t_tend"] + theta_bias
     for k, var in (("ru_tend", "u"), ("rv_tend", "v"), ("ph_tend", "h"), ("t_tend", "t"), ("mu_tend", "m")):
         s[k] = spec_bdytend(s[k], bt[var], var, rdx, rdy)
     return acoustic_stage(s, data, rk_step, nsub, dts, epssm=epssm, emdiv=emdiv, smdiv=smdiv, cf1=cf1, cf2=cf2,
@@ -1151,11 +1316,14 @@ class _MoistUpdate:
                                             ctypes.c_void_p(self.work.data_ptr()), stream)
 
 
-def moist_stage(st: dict, data: dict, rk_step: int, dt_rk: float, rdx, rdy) -> dict:
+def moist_stage(st: dict, data: dict, rk_step: int, dt_rk: float, rdx, rdy, bt: dict | None = None,
+                dtbc: float | None = None) -> dict:
     """The moisture part of an RK stage after its acoustic steps, composed
-    from the operators' Functions (pywrf/solver.py:1548-1712, without the
-    first stage's moisture diffusion and qv relaxation): advection of qv ..
-    qg by the averaged fluxes, rk_update_scalar, flow_dep_bdy of qc .. qg,
+    from the operators' Functions (pywrf/solver.py:1548-1712): advection of
+    qv .. qg by the averaged fluxes; at the first stage the horizontal
+    diffusion of each species (mass muts, viscosity xkhh), and the relaxation
+    and specified tendency of qv (``bt['q']``: its eight boundary arrays,
+    ``dtbc`` the boundary time); rk_update_scalar, flow_dep_bdy of qc .. qg,
     calc_p_rho_phi and, before the last stage, the halo copies."""
     s = dict(st)
     moist = s["moist"]
@@ -1164,6 +1332,17 @@ def moist_stage(st: dict, data: dict, rk_step: int, dt_rk: float, rdx, rdy) -> d
         adv.append(advect_scalar(moist[im], torch.zeros_like(moist[im]), s["ru_m"], s["rv_m"], s["ww_m"],
                                  data["msftx"], data["fnm"], data["fnp"], data["rdnw"], rdx, rdy))
     s["advect_tend"] = torch.stack(adv)
+    if rk_step == 1:
+        if bt is None or dtbc is None:
+            raise ValueError("the first stage's qv relaxation needs its boundary arrays and dtbc")
+        hd = {k: data[k] for k in HDIFF_DATA}
+        mt = s["moist_tend"]
+        tends = [mt[0]] + [horizontal_diffusion("m", moist[im], mt[im], s["muts"], s["xkhh"], hd, rdx, rdy)
+                           for im in range(1, 7)]
+        nz = moist.shape[1]
+        rq = mass_weight(moist[1], s["mut"], nz - 1, rdx, rdy)
+        tends[1] = spec_bdytend(relax_bdytend(rq, tends[1], "t", dtbc, bt["q"]), bt["q"], "t", rdx, rdy)
+        s["moist_tend"] = torch.stack(tends)
     op = _MoistUpdate(rk_step, dt_rk, moist[0])
     cg = scalar_grid(s["u"].shape, rdx, rdy)
     dd = {"msfty": data["msfty"], "ru_m": s["ru_m"].detach(), "rv_m": s["rv_m"].detach(), "rdnw": data["rdnw"]}
@@ -1182,7 +1361,87 @@ RK_DATA = tuple(dict.fromkeys(DYN_DATA + ("msftx", "fnm", "fnp", "rdnw")))
 
 
 def rk_stage(st: dict, data: dict, bt: dict, rk_step: int, nsub: int, dts: float, dt_rk: float, **sc) -> dict:
-    """RK stage 2 or 3 of the step, composed: :func:`dynamics_stage` then
-    :func:`moist_stage`; ``sc`` as for :func:`dynamics_stage`."""
+    """One RK stage of the step, composed: :func:`dynamics_stage` then
+    :func:`moist_stage`; ``sc`` as for :func:`dynamics_stage` (at the first
+    stage ``bt`` also holds 'q', qv's boundary arrays)."""
     s = dynamics_stage(st, data, bt, rk_step, nsub, dts, **sc)
-    return moist_stage(s, data, rk_step, dt_rk, sc["rdx"], sc["rdy"])
+    return moist_stage(s, data, rk_step, dt_rk, sc["rdx"], sc["rdy"], bt, sc.get("dtbc"))
+
+
+BDY_FINAL_ARRAYS = tuple(f"{v}_{n}" for v in ("u", "v", "t", "ph", "qv")
+                         for n in ("bxs", "bxe", "bys", "bye", "btxs", "btxe", "btys", "btye"))
+
+
+class _BdyFinal:
+    name = "wrf_bdy_final"
+    fields = ("u", "v", "t", "ph", "moist", "w", "muus", "muvs", "muts")
+    outputs = ("u", "v", "t", "ph", "moist", "w")
+    data = ("msfuy", "msfvx", "msftx", "msfty", "ht", "dscal") + BDY_FINAL_ARRAYS
+
+    def fwd(self, cg, tab, stream):
+        return N.lib().wrf_bdy_final(ctypes.byref(cg), tab, stream)
+
+    def adj(self, cg, tab, btab, stream):
+        return N.lib().wrf_bdy_final_adj(ctypes.byref(cg), tab, btab, stream)
+
+
+def boundary_arrays(bdy: dict) -> dict:
+    """The state table's boundary-array fields (u_bxs .. qv_btye) from
+    per-variable dicts in the solver layout ('u', 'v', 't', 'ph', 'qv' each
+    mapping xs xe ys ye txs txe tys tye)."""
+    out = {}
+    for v in ("u", "v", "t", "ph", "qv"):
+        for n, key in (("bxs", "xs"), ("bxe", "xe"), ("bys", "ys"), ("bye", "ye"), ("btxs", "txs"),
+                       ("btxe", "txe"), ("btys", "tys"), ("btye", "tye")):
+            out[f"{v}_{n}"] = bdy[v][key]
+    return out
+
+
+def step_end(st: dict, data: dict, bdy: dict, dtbc: float, *, cf1: float, cf2: float, cf3: float, rdx: float,
+             rdy: float) -> dict:
+    """The end of a step after its microphysics, composed
+    (pywrf/solver.py:1776-1910): the halo copies of u_1, u, v_1, v, w_1, w,
+    t_1, t, ph_1, ph, mu_1, mu and qv .. qg, spec_bdy_final of u, v, t, ph,
+    qv and set_w_surface.  ``bdy`` maps 'u', 'v', 't', 'ph', 'qv' to their
+    boundary arrays (xs .. tye)."""
+    s = dict(st)
+    for k, var in (("u_1", "U"), ("u", "U"), ("v_1", "V"), ("v", "V"), ("w_1", "w"), ("w", "w"), ("t_1", "p"),
+                   ("t", "p"), ("ph_1", "w"), ("ph", "w"), ("mu_1", "t"), ("mu", "t")):
+        s[k] = halo(s[k], var, rdx, rdy)
+    m = s["moist"]
+    s["moist"] = torch.stack([m[0]] + [halo(m[im], "p", rdx, rdy) for im in range(1, 7)])
+    op = _BdyFinal()
+    cg = scalar_grid(s["u"].shape, rdx, rdy)
+    cg.cf1, cg.cf2, cg.cf3 = float(cf1), float(cf2), float(cf3)
+    dscal = torch.zeros(16, dtype=torch.float32, device=s["u"].device)
+    dscal[0] = float(dtbc)
+    dd = {**{k: data[k] for k in ("msfuy", "msfvx", "msftx", "msfty", "ht")}, "dscal": dscal,
+          **boundary_arrays(bdy)}
+    outs = _TableOp.apply(op, cg, *[s[k] for k in op.fields], *[dd[k] for k in op.data])
+    s.update(dict(zip(op.outputs, outs)))
+    return s
+
+
+STEP_DATA = tuple(dict.fromkeys(RK_DATA + ("msfuy", "msfvx", "msftx", "msfty", "ht")))
+
+
+def step(st: dict, data: dict, bdy: dict, dtbc: float, *, dt: float, soundsteps: int, microphysics=None,
+         theta_bias=None, **sc) -> dict:
+    """One time step composed from the operators' Functions
+    (pywrf/solver.py:709-1910): the three RK stages (:func:`rk_stage`), then
+    ``microphysics`` (a differentiable callable on the state dict, or None
+    for none: the step of a model without microphysics), then
+    :func:`step_end`.  ``bdy`` maps 'u', 'v', 'ph', 't', 'mu', 'qv' to their
+    boundary arrays (xs .. tye); ``sc`` holds epssm, emdiv, smdiv, cf1, cf2,
+    cf3, cfn, cfn1, rdx, rdy; ``theta_bias`` is added to t_tend in every
+    stage."""
+    bt = {"u": bdy["u"], "v": bdy["v"], "h": bdy["ph"], "t": bdy["t"], "m": bdy["mu"], "q": bdy["qv"]}
+    s = dict(st)
+    for rk in (1, 2, 3):
+        nsub = {1: 1, 2: soundsteps // 2, 3: soundsteps}[rk]
+        dts = dt / 3.0 if rk == 1 else dt / soundsteps
+        dt_rk = {1: dt / 3.0, 2: 0.5 * dt, 3: dt}[rk]
+        s = rk_stage(s, data, bt, rk, nsub, dts, dt_rk, dtbc=dtbc, theta_bias=theta_bias, **sc)
+    if microphysics is not None:
+        s = microphysics(s)
+    return step_end(s, data, bdy, dtbc, cf1=sc["cf1"], cf2=sc["cf2"], cf3=sc["cf3"], rdx=sc["rdx"], rdy=sc["rdy"])

@@ -568,12 +568,18 @@ int launch_prep(const Grid& g, const S& s, cudaStream_t st) {
   return 3;
 }
 
-int launch_km(const Grid& g, const S& s, cudaStream_t st) {
+int launch_deform(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_deform<<<point_grid(g, b3), b3, 0, st>>>(g, s);
   k_defor12_bc<<<point_grid(g, b3), b3, 0, st>>>(g, s);
+  return 2;
+}
+
+int launch_km(const Grid& g, const S& s, cudaStream_t st) {
+  const dim3 b3(32, 4);
+  const int n = launch_deform(g, s, st);
   k_km<<<point_grid(g, b3), b3, 0, st>>>(g, s);
-  return 3;
+  return n + 1;
 }
 
 int launch_diff_metrics(const Grid& g, const S& s, cudaStream_t st) {

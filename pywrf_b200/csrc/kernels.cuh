@@ -18,7 +18,9 @@ int set_kernel_form(int form);  // returns the previous form
 int launch_prep(const Grid& g, const S& s, cudaStream_t st);
 // compute_diff_metrics (k_prep.cu)
 int launch_diff_metrics(const Grid& g, const S& s, cudaStream_t st);
-// cal_deform_and_div + calculate_km_kh (k_prep.cu)
+// cal_deform_and_div (defor11/22/12 and defor12's boundary copies) alone,
+// and with calculate_km_kh (k_prep.cu)
+int launch_deform(const Grid& g, const S& s, cudaStream_t st);
 int launch_km(const Grid& g, const S& s, cudaStream_t st);
 // horizontal_diffusion u/v/w/theta + relax_bdytend u/v/ph/t/mu (k_prep.cu)
 int launch_hdiff_relax(const Grid& g, const S& s, cudaStream_t st);
@@ -59,6 +61,19 @@ int launch_addtend_op(const Grid& g, const S& s, int rk_step, cudaStream_t st);
 int launch_addtend_op_adj(const Grid& g, const S& s, const S& b, int rk_step, cudaStream_t st);
 int launch_spec_tend(const Grid& g, float* tend, const float* const* bt4, char var, cudaStream_t st);
 int launch_spec_tend_adj(const Grid& g, float* tend_bar, char var, cudaStream_t st);
+// the first stage's horizontal diffusion of one field ('u', 'v', 'w', or
+// 'm' for a mass-point scalar, about base when given), the eddy viscosities
+// and mass_weight as stand-alone operators with their adjoints
+// (k_adjoint_diff.cu)
+int launch_hdiff_op(const Grid& g, const S& s, char var, const float* f, const float* base, const float* mut,
+                    const float* K, float* tend, cudaStream_t st);
+int launch_hdiff_op_adj(const Grid& g, const S& s, char var, const float* f, const float* base, const float* mut,
+                        const float* K, const float* tbar, float* fbar, float* mutbar, float* Kbar, cudaStream_t st);
+int launch_km_op(const Grid& g, const S& s, cudaStream_t st);
+int launch_km_op_adj(const Grid& g, const S& s, const S& b, float* work, cudaStream_t st);
+int launch_mass_weight(const Grid& g, const float* f, const float* mut, float* out, int nk, cudaStream_t st);
+int launch_mass_weight_adj(const Grid& g, const float* f, const float* mut, const float* ob, float* fb, float* mb,
+                           int nk, cudaStream_t st);
 // rk_addtend_dry + spec_bdytend (k_tend.cu)
 int launch_addtend(const Grid& g, const S& s, int rk_step, cudaStream_t st);
 // moisture advection with the time-averaged fluxes (k_tend.cu)
@@ -137,6 +152,10 @@ int launch_moist(const Grid& g, const S& s, int rk_step, float dt_rk, cudaStream
 // its adjoint (k_adjoint_moist.cu); work: nz*ny*nx floats
 int launch_moist_adj(const Grid& g, const S& s, const S& b, int rk_step, float dt_rk, float* work, cudaStream_t st);
 int launch_bdy_final(const Grid& g, const S& s, cudaStream_t st);
+// spec_bdy_final + set_w_surface as a stand-alone operator and its adjoint
+// (k_adjoint_end.cu)
+int launch_bdy_final_op(const Grid& g, const S& s, cudaStream_t st);
+int launch_bdy_final_op_adj(const Grid& g, const S& s, const S& b, cudaStream_t st);
 
 // microphysics (k_wsm6.cu)
 int launch_physics(const Grid& g, const S& s, cudaStream_t st);

@@ -573,6 +573,27 @@ constexpr int kSsfCotangents[] = {WF_U, WF_U_SAVE, WF_V, WF_V_SAVE, WF_W, WF_W_S
                                   WF_T, WF_T_SAVE, WF_H_DIABATIC, WF_MU, WF_MU_SAVE, WF_MUT, WF_MUTS, WF_MUU, WF_MUV,
                                   WF_MUUS, WF_MUVS};
 
+// the eddy viscosities' operands (metrics, deformations, calculate_km_kh;
+// rdzw, zx, zy and the defor fields are scratch) and cotangents
+constexpr int kKmOperands[] = {WF_U, WF_V, WF_PH, WF_PHB, WF_XKMH, WF_XKHH, WF_RDZW, WF_ZX, WF_ZY, WF_DEFOR11,
+                               WF_DEFOR22, WF_DEFOR12, WF_MSFUX, WF_MSFUY, WF_MSFVX, WF_MSFVY, WF_MSFTX, WF_MSFTY,
+                               WF_FNM, WF_FNP, WF_DN, WF_DNW};
+constexpr int kKmCotangents[] = {WF_U, WF_V, WF_PH, WF_XKMH, WF_XKHH};
+// horizontal_diffusion's map factors
+constexpr int kHdiffOperands[] = {WF_MSFUX, WF_MSFUY, WF_MSFVX, WF_MSFVY, WF_MSFTX, WF_MSFTY, WF_MSFVX_INV};
+
+// the end-of-step boundaries' operands (spec_bdy_final of u, v, t, ph, qv;
+// set_w_surface) and cotangents
+constexpr int kBdyFinalOperands[] = {
+    WF_U, WF_V, WF_T, WF_PH, WF_MOIST, WF_W, WF_MUUS, WF_MUVS, WF_MUTS, WF_MSFUY, WF_MSFVX, WF_MSFTX, WF_MSFTY,
+    WF_HT, WF_DSCAL, WF_U_BXS, WF_U_BXS + 1, WF_U_BXS + 2, WF_U_BXS + 3, WF_U_BXS + 4, WF_U_BXS + 5, WF_U_BXS + 6,
+    WF_U_BXS + 7, WF_V_BXS, WF_V_BXS + 1, WF_V_BXS + 2, WF_V_BXS + 3, WF_V_BXS + 4, WF_V_BXS + 5, WF_V_BXS + 6,
+    WF_V_BXS + 7, WF_T_BXS, WF_T_BXS + 1, WF_T_BXS + 2, WF_T_BXS + 3, WF_T_BXS + 4, WF_T_BXS + 5, WF_T_BXS + 6,
+    WF_T_BXS + 7, WF_PH_BXS, WF_PH_BXS + 1, WF_PH_BXS + 2, WF_PH_BXS + 3, WF_PH_BXS + 4, WF_PH_BXS + 5,
+    WF_PH_BXS + 6, WF_PH_BXS + 7, WF_QV_BXS, WF_QV_BXS + 1, WF_QV_BXS + 2, WF_QV_BXS + 3, WF_QV_BXS + 4,
+    WF_QV_BXS + 5, WF_QV_BXS + 6, WF_QV_BXS + 7};
+constexpr int kBdyFinalCotangents[] = {WF_U, WF_V, WF_T, WF_PH, WF_MOIST, WF_W, WF_MUUS, WF_MUVS, WF_MUTS};
+
 // rk_addtend_dry's operands and cotangents
 constexpr int kAddtendOperands[] = {WF_RU_TEND, WF_RV_TEND, WF_RW_TEND, WF_PH_TEND, WF_T_TEND, WF_MU_TEND,
                                     WF_RU_TENDF, WF_RV_TENDF, WF_RW_TENDF, WF_PH_TENDF, WF_T_TENDF, WF_MU_TENDF,
@@ -984,6 +1005,117 @@ int wrf_spec_bdytend_adj(const WrfGrid* gin, float* tend_bar, char var, void* st
   cudaGetLastError();
   launch_spec_tend_adj(g, tend_bar, var, static_cast<cudaStream_t>(stream));
   return check_launch("spec_bdytend_adj");
+}
+
+int wrf_eddy_viscosity(const WrfGrid* gin, const WrfState* sin, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s;
+  if ((rc = state_of(sin, kKmOperands, sizeof(kKmOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_km_op(g, s, static_cast<cudaStream_t>(stream));
+  return check_launch("eddy_viscosity");
+}
+
+int wrf_eddy_viscosity_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, float* work,
+                           void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!work) return fail(WRF_EINVAL, "eddy_viscosity_adj: work (6*nz*ny*nx floats) is required");
+  S s, b;
+  if ((rc = state_of(sin, kKmOperands, sizeof(kKmOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kKmCotangents, sizeof(kKmCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_km_op_adj(g, s, b, work, static_cast<cudaStream_t>(stream));
+  return check_launch("eddy_viscosity_adj");
+}
+
+namespace {
+int hdiff_args(const Grid& g, char var, const float* field, const float* mut, const float* xk, const void* out) {
+  (void)g;
+  if (var != 'u' && var != 'v' && var != 'w' && var != 'm')
+    return fail(WRF_EINVAL, "horizontal_diffusion: var is u, v, w or m");
+  if (!field || !mut || !xk || !out) return fail(WRF_EINVAL, "null argument");
+  return 0;
+}
+}  // namespace
+
+int wrf_horizontal_diffusion(const WrfGrid* gin, const WrfState* sin, char var, const float* field, const float* base,
+                             const float* mut, const float* xk, float* tend, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if ((rc = hdiff_args(g, var, field, mut, xk, tend))) return rc;
+  if (base && var != 'm') return fail(WRF_EINVAL, "horizontal_diffusion: base is for a mass-point scalar");
+  S s;
+  if ((rc = state_of(sin, kHdiffOperands, sizeof(kHdiffOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_hdiff_op(g, s, var, field, base, mut, xk, tend, static_cast<cudaStream_t>(stream));
+  return check_launch("horizontal_diffusion");
+}
+
+int wrf_horizontal_diffusion_adj(const WrfGrid* gin, const WrfState* sin, char var, const float* field,
+                                 const float* base, const float* mut, const float* xk, const float* tend_bar,
+                                 float* field_bar, float* mut_bar, float* xk_bar, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if ((rc = hdiff_args(g, var, field, mut, xk, tend_bar))) return rc;
+  if (base && var != 'm') return fail(WRF_EINVAL, "horizontal_diffusion_adj: base is for a mass-point scalar");
+  S s;
+  if ((rc = state_of(sin, kHdiffOperands, sizeof(kHdiffOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_hdiff_op_adj(g, s, var, field, base, mut, xk, tend_bar, field_bar, mut_bar, xk_bar,
+                      static_cast<cudaStream_t>(stream));
+  return check_launch("horizontal_diffusion_adj");
+}
+
+int wrf_mass_weight(const WrfGrid* gin, const float* field, const float* mut, float* out, int nk, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!field || !mut || !out) return fail(WRF_EINVAL, "null argument");
+  if (nk < 1 || nk > g.nz) return fail(WRF_EINVAL, "mass_weight: 1 <= nk <= nz");
+  cudaGetLastError();
+  launch_mass_weight(g, field, mut, out, nk, static_cast<cudaStream_t>(stream));
+  return check_launch("mass_weight");
+}
+
+int wrf_mass_weight_adj(const WrfGrid* gin, const float* field, const float* mut, const float* out_bar,
+                        float* field_bar, float* mut_bar, int nk, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!field || !mut || !out_bar || !field_bar || !mut_bar) return fail(WRF_EINVAL, "null argument");
+  if (nk < 1 || nk > g.nz) return fail(WRF_EINVAL, "mass_weight_adj: 1 <= nk <= nz");
+  cudaGetLastError();
+  launch_mass_weight_adj(g, field, mut, out_bar, field_bar, mut_bar, nk, static_cast<cudaStream_t>(stream));
+  return check_launch("mass_weight_adj");
+}
+
+int wrf_bdy_final(const WrfGrid* gin, const WrfState* sin, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s;
+  if ((rc = state_of(sin, kBdyFinalOperands, sizeof(kBdyFinalOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_bdy_final_op(g, s, static_cast<cudaStream_t>(stream));
+  return check_launch("bdy_final");
+}
+
+int wrf_bdy_final_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* sbar, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s, b;
+  if ((rc = state_of(sin, kBdyFinalOperands, sizeof(kBdyFinalOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(sbar, kBdyFinalCotangents, sizeof(kBdyFinalCotangents) / sizeof(int), b))) return rc;
+  cudaGetLastError();
+  launch_bdy_final_op_adj(g, s, b, static_cast<cudaStream_t>(stream));
+  return check_launch("bdy_final_adj");
 }
 
 int wrf_moist_update(const WrfGrid* gin, const WrfState* sin, int rk_step, float dt_rk, void* stream) {

@@ -706,9 +706,10 @@ def test_composed_acoustic_stage_and_its_adjoint_against_the_oracle(rk_step):
         assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
 
 
-def _oracle_dynamics_stage(g, s, rk_step, nsub, dts):
-    """The dynamics of RK stage 2 or 3 of the oracle (its model loop,
-    solver.py:736-1492, without the first stage's diffusion) on ``s``."""
+def _oracle_dynamics_stage(g, s, rk_step, nsub, dts, dtbc=None):
+    """The dynamics of one RK stage of the oracle (its model loop,
+    solver.py:736-1492) on ``s``; the first stage needs the boundary time
+    ``dtbc``."""
     from oracle import boundary as OB
     from oracle import dynamics as OD
 
@@ -728,6 +729,20 @@ def _oracle_dynamics_stage(g, s, rk_step, nsub, dts):
     OD.set_physical_bc2d(g, s["mut"], "t")
     OD.set_physical_bc3d(g, s["al"], "p")
     OD.set_physical_bc3d(g, s["ph"], "w")
+    if rk_step == 1:
+        for nm in ("ru_tendf", "rv_tendf", "rw_tendf", "ph_tendf", "t_tendf", "mu_tendf", "moist_tend"):
+            s[nm] = np.zeros_like(s[nm])
+        for nm in ("z", "rdz", "rdzw", "zx", "zy", "defor11", "defor22", "defor12", "xkmh", "xkhh"):
+            s[nm] = s[nm].copy()
+        OD.compute_diff_metrics(g, s["ph"], s["phb"], s["z"], s["rdz"], s["rdzw"], s["zx"], s["zy"])
+        for nm, var in (("rdzw", "w"), ("rdz", "w"), ("z", "w"), ("zx", "e"), ("zy", "f")):
+            OD.set_physical_bc3d(g, s[nm], var)
+        OD.cal_deform_and_div(g, s["u"], s["v"], s["defor11"], s["defor22"], s["defor12"], s["msfux"], s["msfuy"],
+                              s["msfvx"], s["msfvy"], s["msftx"], s["msfty"], s["dn"], s["dnw"], s["rdzw"], s["fnm"],
+                              s["fnp"], s["cf1"], s["cf2"], s["cf3"], s["zx"], s["zy"])
+        OD.calculate_km_kh(g, s["xkmh"], s["xkhh"], s["defor11"], s["defor22"], s["defor12"], s["msftx"], s["msfty"])
+        OD.set_physical_bc3d(g, s["xkmh"], "t")
+        OD.set_physical_bc3d(g, s["xkhh"], "t")
     for nm in ("ru_tend", "rv_tend", "rw_tend", "t_tend", "ph_tend", "u_save", "v_save", "w_save", "ph_save", "t_save"):
         s[nm] = np.zeros_like(s[nm])
     s["mu_tend"] = np.zeros_like(s["mu_tend"])
@@ -748,11 +763,26 @@ def _oracle_dynamics_stage(g, s, rk_step, nsub, dts):
                 s["fnp"])
     OD.curvature(g, s["ru"], s["rv"], s["rw"], s["u"], s["v"], s["ru_tend"], s["rv_tend"], s["rw_tend"], s["msfux"],
                  s["msfuy"], s["msfvx"], s["msfvy"], s["msftx"], s["msfty"], s["fnm"], s["fnp"])
+    bd = s["bdy"]
+    if rk_step == 1:
+        mp = (s["msfux"], s["msfuy"], s["msfvx"], s["msfvx_inv"], s["msfvy"], s["msftx"], s["msfty"])
+        for name in ("u", "v", "w"):
+            OD.horizontal_diffusion(g, name, s[name], s[f"r{name}_tendf"], s["mut"], *mp, s["xkmh"])
+        OD.horizontal_diffusion(g, "m", s["t"], s["t_tendf"], s["mut"], *mp, s["xkhh"], base=s["t_init"])
+        fcx, gcx = s["fcx"], s["gcx"]
+        OB.relax_bdytend(g, s["ru"], s["u_save"], bd["u"], "u", dtbc, fcx, gcx)
+        OB.relax_bdytend(g, s["rv"], s["v_save"], bd["v"], "v", dtbc, fcx, gcx)
+        mw = (slice(0, g.nz), slice(g.jds, g.jde - 1), slice(g.ids, g.ide - 1))
+        s["rfield"] = s["rfield"].copy()
+        OB.mass_weight(s["ph"], s["mut"], s["rfield"], *mw)
+        OB.relax_bdytend(g, s["rfield"], s["ph_save"], bd["ph"], "h", dtbc, fcx, gcx)
+        OB.mass_weight(s["t"], s["mut"], s["rfield"], *mw)
+        OB.relax_bdytend(g, s["rfield"], s["t_save"], bd["t"], "t", dtbc, fcx, gcx)
+        OB.relax_bdytend(g, s["mu"][None], s["mu_tend"][None], bd["mu"], "m", dtbc, fcx, gcx)
     OD.rk_addtend_dry(g, s["ru_tend"], s["rv_tend"], s["rw_tend"], s["ph_tend"], s["t_tend"], s["ru_tendf"],
                       s["rv_tendf"], s["rw_tendf"], s["ph_tendf"], s["t_tendf"], s["u_save"], s["v_save"],
                       s["w_save"], s["ph_save"], s["t_save"], s["mu_tend"], s["mu_tendf"], rk_step, s["h_diabatic"],
                       s["mut"], s["msfty"], s["msfuy"], s["msfvx"], s["msfvx_inv"])
-    bd = s["bdy"]
     OB.spec_bdytend(g, s["ru_tend"], bd["u"], "u")
     OB.spec_bdytend(g, s["rv_tend"], bd["v"], "v")
     OB.spec_bdytend(g, s["ph_tend"], bd["ph"], "h")
@@ -839,44 +869,10 @@ def test_composed_dynamics_stage_and_its_adjoint_against_the_oracle(rk_step):
         assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
 
 
-def _oracle_rk_stage(g, s, rk_step, nsub, dts, dt_rk):
-    """RK stage 2 or 3 of the oracle: the dynamics, then the moisture part
-    (its model loop, solver.py:1548-1712)."""
-    from oracle import boundary as OB
-    from oracle import dynamics as OD
-
-    _oracle_dynamics_stage(g, s, rk_step, nsub, dts)
-    s["advect_tend"] = s["advect_tend"].copy()
-    for im in range(1, 7):
-        s["advect_tend"][im][0:g.nz, g.jts:g.jte, g.its:g.ite] = 0.0
-        OD.advect_scalar(g, s["moist"][im], s["advect_tend"][im], s["ru_m"], s["rv_m"], s["ww_m"], s["msftx"],
-                         s["fnm"], s["fnp"], s["rdnw"])
-    OD.rk_update_scalar(g, s["moist_old"], s["moist"], s["moist_tend"], s["advect_tend"], s["msfty"], s["mu_1"],
-                        s["mu"], s["mub"], rk_step, dt_rk)
-    for im in range(2, 7):
-        OB.flow_dep_bdy(g, s["moist"][im], s["ru_m"], s["rv_m"])
-    OD.calc_p_rho_phi(g, s["moist"][1], s["al"], s["alb"], s["mu"], s["muts"], s["ph"], s["p"], s["pb"], s["t"],
-                      s["rdnw"])
-    if rk_step < 3:
-        for nm, var in (("u", "U"), ("v", "V"), ("w", "w"), ("t", "p"), ("ph", "w")):
-            OD.set_physical_bc3d(g, s[nm], var)
-        OD.set_physical_bc2d(g, s["mu"], "t")
-        for im in range(1, 7):
-            OD.set_physical_bc3d(g, s["moist"][im], "p")
-
-
-RK_OUT = STAGE_OUT + ("moist",)
-
-
-@pytest.mark.parametrize("rk_step", [2, 3])
-def test_composed_rk_stage_and_its_adjoint_against_the_oracle(rk_step):
-    """pywrf_b200.adjoint.rk_stage (dynamics_stage, then the moisture
-    advection, rk_update_scalar, flow_dep_bdy and calc_p_rho_phi) from the
-    small case's state at the start of stage 2 / 3 of step 2: the outputs
-    (moisture included) against the float64 oracle (3x the float32 oracle's
-    own error plus 2e-6), and the gradient of a seeded linear functional of
-    16 outputs in 8 inputs against float64 central differences of the
-    oracle's stage."""
+def _stage_start(rk_step):
+    """The small case's float64 oracle state at the start of RK stage
+    ``rk_step`` of step 2, with the stage's (nsub, dts, dt_rk) and the
+    boundary time dtbc of step 2 (pywrf/solver.py:713-734)."""
     import copy
 
     from helpers import SMALL
@@ -895,32 +891,100 @@ def test_composed_rk_stage_and_its_adjoint_against_the_oracle(rk_step):
 
     m = OracleModel(g, inputs, bdy, np.float64)
     m.run(1)
-    m.step(2, probe)
+    if rk_step == 1:
+        snap.update(copy.deepcopy(m.st))
+    else:
+        m.step(2, probe)
     dts = g.dt / g.soundsteps
-    nsub, dt_rk = (g.soundsteps // 2, 0.5 * g.dt) if rk_step == 2 else (g.soundsteps, g.dt)
+    nsub, dt_rk = {1: (1, g.dt / 3.0), 2: (g.soundsteps // 2, 0.5 * g.dt), 3: (g.soundsteps, g.dt)}[rk_step]
+    if rk_step == 1:
+        dts = g.dt / 3.0
+    assert 2 % g.bdy_interval != 1  # no boundary record is loaded at step 2
+    dtbc = g.dt * (2 - m.it_bdy * g.bdy_interval)
+    return g, snap, nsub, dts, dt_rk, dtbc
 
-    def cast(v, dtype):
-        if isinstance(v, np.ndarray):
-            return np.array(v, dtype)
-        if isinstance(v, dict):
-            return {k: cast(x, dtype) for k, x in v.items()}
-        return v
+
+def _cast(v, dtype):
+    if isinstance(v, np.ndarray):
+        return np.array(v, dtype)
+    if isinstance(v, dict):
+        return {k: _cast(x, dtype) for k, x in v.items()}
+    return v
+
+
+def _stage_bdy(snap, with_values):
+    """The boundary arrays a composed stage takes, by stagger letter."""
+    names = ("txs", "txe", "tys", "tye") + (("xs", "xe", "ys", "ye") if with_values else ())
+    letters = {"u": "u", "v": "v", "h": "ph", "t": "t", "m": "mu", "q": "qv"}
+    return {v: {s_: _cuda(snap["bdy"][f][s_]) for s_ in names} for v, f in letters.items()}
+
+
+def _oracle_rk_stage(g, s, rk_step, nsub, dts, dt_rk, dtbc=None):
+    """One RK stage of the oracle: the dynamics, then the moisture part (its
+    model loop, solver.py:1548-1712)."""
+    from oracle import boundary as OB
+    from oracle import dynamics as OD
+
+    _oracle_dynamics_stage(g, s, rk_step, nsub, dts, dtbc)
+    s["advect_tend"] = s["advect_tend"].copy()
+    for im in range(1, 7):
+        s["advect_tend"][im][0:g.nz, g.jts:g.jte, g.its:g.ite] = 0.0
+        OD.advect_scalar(g, s["moist"][im], s["advect_tend"][im], s["ru_m"], s["rv_m"], s["ww_m"], s["msftx"],
+                         s["fnm"], s["fnp"], s["rdnw"])
+        if rk_step == 1:
+            OD.horizontal_diffusion(g, "m", s["moist"][im], s["moist_tend"][im], s["muts"], s["msfux"], s["msfuy"],
+                                    s["msfvx"], s["msfvx_inv"], s["msfvy"], s["msftx"], s["msfty"], s["xkhh"])
+    if rk_step == 1:
+        rq = np.zeros_like(s["t"])
+        OB.mass_weight(s["moist"][1], s["mut"], rq, slice(0, g.nz - 1), slice(g.jds, g.jde - 1),
+                       slice(g.ids, g.ide - 1))
+        OB.relax_bdytend(g, rq, s["moist_tend"][1], s["bdy"]["qv"], "q", dtbc, s["fcx"], s["gcx"])
+        OB.spec_bdytend(g, s["moist_tend"][1], s["bdy"]["qv"], "q")
+    OD.rk_update_scalar(g, s["moist_old"], s["moist"], s["moist_tend"], s["advect_tend"], s["msfty"], s["mu_1"],
+                        s["mu"], s["mub"], rk_step, dt_rk)
+    for im in range(2, 7):
+        OB.flow_dep_bdy(g, s["moist"][im], s["ru_m"], s["rv_m"])
+    OD.calc_p_rho_phi(g, s["moist"][1], s["al"], s["alb"], s["mu"], s["muts"], s["ph"], s["p"], s["pb"], s["t"],
+                      s["rdnw"])
+    if rk_step < 3:
+        for nm, var in (("u", "U"), ("v", "V"), ("w", "w"), ("t", "p"), ("ph", "w")):
+            OD.set_physical_bc3d(g, s[nm], var)
+        OD.set_physical_bc2d(g, s["mu"], "t")
+        for im in range(1, 7):
+            OD.set_physical_bc3d(g, s["moist"][im], "p")
+
+
+RK_OUT = STAGE_OUT + ("moist",)
+
+
+@pytest.mark.parametrize("rk_step", [1, 2, 3])
+def test_composed_rk_stage_and_its_adjoint_against_the_oracle(rk_step):
+    """pywrf_b200.adjoint.rk_stage (dynamics_stage -- at the first stage with
+    the eddy viscosities, the horizontal diffusion and the relaxation --
+    then the moisture advection, at the first stage the moisture diffusion
+    and qv's relaxation, rk_update_scalar, flow_dep_bdy and calc_p_rho_phi)
+    from the small case's state at the start of stage 1 / 2 / 3 of step 2:
+    the outputs (moisture included) against the float64 oracle (3x the
+    float32 oracle's own error plus 2e-6), and the gradient of a seeded
+    linear functional of 16 outputs in 8 inputs against float64 central
+    differences of the oracle's stage."""
+    g, snap, nsub, dts, dt_rk, dtbc = _stage_start(rk_step)
 
     def oracle_run(dtype, pert=None):
-        s = {k: cast(v, dtype) for k, v in snap.items()}
+        s = {k: _cast(v, dtype) for k, v in snap.items()}
         if pert:
             for k, d in pert.items():
                 s[k] = s[k] + d
-        _oracle_rk_stage(g, s, rk_step, nsub, dts, dt_rk)
+        _oracle_rk_stage(g, s, rk_step, nsub, dts, dt_rk, dtbc)
         return s
 
     o64, o32 = oracle_run(np.float64), oracle_run(np.float32)
     st = {k: _cuda(snap[k]).requires_grad_(True) for k in adjoint.RK_STATE}
     data = {k: _cuda(snap[k]) for k in adjoint.RK_DATA}
-    bname = {"u": "u", "v": "v", "h": "ph", "t": "t", "m": "mu"}
-    bt = {v: {s_: _cuda(snap["bdy"][f][s_]) for s_ in ("txs", "txe", "tys", "tye")} for v, f in bname.items()}
+    bt = _stage_bdy(snap, rk_step == 1)
     sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=float(snap["cf1"]), cf2=float(snap["cf2"]),
-              cf3=float(snap["cf3"]), cfn=float(snap["cfn"]), cfn1=float(snap["cfn1"]), rdx=g.rdx, rdy=g.rdy)
+              cf3=float(snap["cf3"]), cfn=float(snap["cfn"]), cfn1=float(snap["cfn1"]), rdx=g.rdx, rdy=g.rdy,
+              dtbc=dtbc)
     out = adjoint.rk_stage(st, data, bt, rk_step, nsub, dts, dt_rk, **sc)
     bad = []
     for k in RK_OUT:
@@ -929,7 +993,7 @@ def test_composed_rk_stage_and_its_adjoint_against_the_oracle(rk_step):
         if not err <= 3.0 * floor + 2e-6:
             bad.append((k, err, floor))
     assert not bad, bad
-    rng = np.random.default_rng(80)
+    rng = np.random.default_rng(80 + rk_step)
     cot = {k: rng.standard_normal(np.shape(snap[k])) for k in RK_OUT}
     sum((out[k].double() * torch.tensor(cot[k], device="cuda")).sum() for k in RK_OUT).backward()
 
@@ -937,10 +1001,188 @@ def test_composed_rk_stage_and_its_adjoint_against_the_oracle(rk_step):
         s = oracle_run(np.float64, pert)
         return sum(float((s[k] * cot[k]).sum()) for k in RK_OUT)
 
-    for name in ("u", "t", "ph", "w", "mu", "p", "moist", "moist_tend"):
+    for name in ("u", "v", "t", "ph", "w", "mu", "p", "moist") + (("moist_tend",) if rk_step > 1 else ()):
         gr = st[name].grad.double().cpu().numpy()
         d = rng.standard_normal(gr.shape)
         eps = 1e-6 * float(np.abs(snap[name]).max() or 1.0)
         fd = (loss({name: eps * d}) - loss({name: -eps * d})) / (2 * eps)
+        an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
+        assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
+
+
+def test_first_stage_viscosity_and_diffusion_operators_against_the_oracle():
+    """pywrf_b200.adjoint.eddy_viscosity (compute_diff_metrics,
+    cal_deform_and_div, calculate_km_kh), the halo copies of xkmh / xkhh and
+    horizontal_diffusion of u, v, w, theta (about t_init) and qc from the
+    small case's state at the start of step 2: the outputs against the
+    float64 oracle (3x the float32 oracle's own error plus 2e-6), and the
+    gradient of a seeded linear functional of the outputs in u, v, w, ph, t,
+    mut, muts and qc against float64 central differences of the oracle."""
+    from oracle import dynamics as OD
+
+    g, snap, *_ = _stage_start(1)
+    outs = ("xkmh", "xkhh", "ru_tendf", "rv_tendf", "rw_tendf", "t_tendf", "qc_tend")
+    mp_names = ("msfux", "msfuy", "msfvx", "msfvx_inv", "msfvy", "msftx", "msfty")
+
+    def oracle(dtype, pert=None):
+        s = {k: _cast(v, dtype) for k, v in snap.items() if k != "bdy"}
+        if pert:
+            for k, d in pert.items():
+                s[k] = s[k] + d
+        OD.compute_diff_metrics(g, s["ph"], s["phb"], s["z"], s["rdz"], s["rdzw"], s["zx"], s["zy"])
+        for nm, var in (("rdzw", "w"), ("rdz", "w"), ("z", "w"), ("zx", "e"), ("zy", "f")):
+            OD.set_physical_bc3d(g, s[nm], var)
+        OD.cal_deform_and_div(g, s["u"], s["v"], s["defor11"], s["defor22"], s["defor12"], s["msfux"], s["msfuy"],
+                              s["msfvx"], s["msfvy"], s["msftx"], s["msfty"], s["dn"], s["dnw"], s["rdzw"], s["fnm"],
+                              s["fnp"], s["cf1"], s["cf2"], s["cf3"], s["zx"], s["zy"])
+        OD.calculate_km_kh(g, s["xkmh"], s["xkhh"], s["defor11"], s["defor22"], s["defor12"], s["msftx"], s["msfty"])
+        OD.set_physical_bc3d(g, s["xkmh"], "t")
+        OD.set_physical_bc3d(g, s["xkhh"], "t")
+        mp = [s[k] for k in mp_names]
+        r = {"xkmh": s["xkmh"], "xkhh": s["xkhh"]}
+        for name in ("u", "v", "w"):
+            r[f"r{name}_tendf"] = np.zeros_like(s[name])
+            OD.horizontal_diffusion(g, name, s[name], r[f"r{name}_tendf"], s["mut"], *mp, s["xkmh"])
+        r["t_tendf"] = np.zeros_like(s["t"])
+        OD.horizontal_diffusion(g, "m", s["t"], r["t_tendf"], s["mut"], *mp, s["xkhh"], base=s["t_init"])
+        r["qc_tend"] = np.zeros_like(s["t"])
+        OD.horizontal_diffusion(g, "m", s["moist"][2], r["qc_tend"], s["muts"], *mp, s["xkhh"])
+        return r
+
+    o64, o32 = oracle(np.float64), oracle(np.float32)
+    st = {k: _cuda(snap[k]).requires_grad_(True) for k in ("u", "v", "w", "ph", "t", "mut", "muts", "xkmh", "xkhh")}
+    qc = _cuda(snap["moist"][2]).requires_grad_(True)
+    data = {k: _cuda(snap[k]) for k in adjoint.DYN_DATA}
+    rdx, rdy = g.rdx, g.rdy
+    xkmh, xkhh = adjoint.eddy_viscosity(st, data, rdx, rdy, float(snap["cf1"]), float(snap["cf2"]),
+                                        float(snap["cf3"]))
+    xkmh, xkhh = adjoint.halo(xkmh, "t", rdx, rdy), adjoint.halo(xkhh, "t", rdx, rdy)
+    hd = {k: data[k] for k in adjoint.HDIFF_DATA}
+    z = lambda: torch.zeros_like(st["u"])  # noqa: E731
+    out = {"xkmh": xkmh, "xkhh": xkhh}
+    for name in ("u", "v", "w"):
+        out[f"r{name}_tendf"] = adjoint.horizontal_diffusion(name, st[name], z(), st["mut"], xkmh, hd, rdx, rdy)
+    out["t_tendf"] = adjoint.horizontal_diffusion("m", st["t"], z(), st["mut"], xkhh, hd, rdx, rdy,
+                                                  base=data["t_init"])
+    out["qc_tend"] = adjoint.horizontal_diffusion("m", qc, z(), st["muts"], xkhh, hd, rdx, rdy)
+    bad = []
+    for k in outs:
+        c = out[k].detach().double().cpu().numpy()
+        err, floor = rel_l2(c, o64[k]), rel_l2(o32[k], o64[k])
+        if not err <= 3.0 * floor + 2e-6:
+            bad.append((k, err, floor))
+    assert not bad, bad
+    rng = np.random.default_rng(91)
+    cot = {k: rng.standard_normal(o64[k].shape) for k in outs}
+    sum((out[k].double() * torch.tensor(cot[k], device="cuda")).sum() for k in outs).backward()
+
+    def loss(pert):
+        r = oracle(np.float64, pert)
+        return sum(float((r[k] * cot[k]).sum()) for k in outs)
+
+    grads = {k: st[k].grad for k in ("u", "v", "w", "ph", "t", "mut", "muts")}
+    qpert = lambda d: np.concatenate([np.zeros((2,) + d.shape), d[None], np.zeros((4,) + d.shape)])  # noqa: E731
+    for name, gr in list(grads.items()) + [("qc", qc.grad)]:
+        gr = gr.double().cpu().numpy()
+        d = rng.standard_normal(gr.shape)
+        base = snap["moist"][2] if name == "qc" else snap[name]
+        eps = 1e-6 * float(np.abs(base).max() or 1.0)
+        key, dd = ("moist", qpert(d)) if name == "qc" else (name, d)
+        fd = (loss({key: eps * dd}) - loss({key: -eps * dd})) / (2 * eps)
+        an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
+        assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
+
+
+STEP_OUT = ("u", "v", "w", "ph", "t", "mu", "muts", "p", "al", "ww", "ru_m", "rv_m", "ww_m", "moist", "u_1", "t_1",
+            "ph_1", "mu_1")
+
+
+def _dry_start():
+    """The small case after one full oracle step (float64), the model's
+    scalars and its boundary arrays (solver layout)."""
+    import copy
+
+    from helpers import SMALL
+    from oracle.model import OracleModel
+    from pywrf_b200 import synthetic
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    m = OracleModel(g, inputs, bdy, np.float64)
+    m.run(1)
+    return g, inputs, bdy, copy.deepcopy(m.st)
+
+
+def _dry_oracle(g, inputs, bdy, snap, dtype, nsteps, pert=None, bias=None):
+    from oracle.model import OracleModel
+
+    m = OracleModel(g, inputs, bdy, dtype, theta_bias=bias, microphysics=False)
+    m.st = {k: _cast(v, dtype) for k, v in snap.items()}
+    if pert:
+        for k, d in pert.items():
+            m.st[k] = m.st[k] + d
+    m.step_count = 1
+    m.run(nsteps)
+    return m.st
+
+
+@pytest.mark.parametrize("nsteps", [1, 2])
+def test_composed_step_without_microphysics_and_its_adjoint_against_the_oracle(nsteps):
+    """pywrf_b200.adjoint.step (the three RK stages and the end-of-step
+    boundaries, composed from the operators' Functions) without
+    microphysics, run through adjoint.rollout (one step per checkpoint
+    segment) from the small case's state after its first step: the state
+    after 1 and 2 steps against the float64 oracle's steps without
+    microphysics (3x the float32 oracle's own error plus 2e-6), and the
+    gradient of a seeded linear functional of 18 outputs with respect to 7
+    inputs and a theta-tendency bias against float64 central differences of
+    the oracle."""
+    g, inputs, bdy, snap = _dry_start()
+    o64 = _dry_oracle(g, inputs, bdy, snap, np.float64, nsteps)
+    o32 = _dry_oracle(g, inputs, bdy, snap, np.float32, nsteps)
+    names = tuple(dict.fromkeys(adjoint.RK_STATE + ("u_1", "w_1", "ph_1", "mu_1", "t_1", "v_1")))
+    st = {k: _cuda(snap[k]).requires_grad_(True) for k in names}
+    data = {k: _cuda(snap[k]) for k in adjoint.STEP_DATA}
+    bd = {f: {k: _cuda(v) for k, v in snap["bdy"][f].items()} for f in ("u", "v", "ph", "t", "mu", "qv")}
+    bias = torch.zeros_like(st["t"], requires_grad=True)
+    sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=float(snap["cf1"]), cf2=float(snap["cf2"]),
+              cf3=float(snap["cf3"]), cfn=float(snap["cfn"]), cfn1=float(snap["cfn1"]), rdx=g.rdx, rdy=g.rdy)
+    assert 2 % g.bdy_interval != 1 and 3 % g.bdy_interval != 1  # one boundary record throughout
+
+    def one(*xs):
+        n = int(round(float(xs[-1].item())))
+        dtbc = g.dt * n  # boundary record 0 for every step here
+        s = adjoint.step(dict(zip(names, xs[:-1])), data, bd, dtbc, dt=g.dt, soundsteps=g.soundsteps,
+                         theta_bias=bias, **sc)
+        return tuple(s[k] for k in names) + (xs[-1] + 1,)
+
+    state = tuple(st[k] for k in names) + (torch.tensor(2.0, device="cuda"),)
+    outs = adjoint.rollout(one, state, nsteps, every=1)
+    out = dict(zip(names, outs))
+    bad = []
+    for k in STEP_OUT:
+        c = out[k].detach().double().cpu().numpy()
+        err, floor = rel_l2(c, o64[k]), rel_l2(o32[k], o64[k])
+        if not err <= 3.0 * floor + 2e-6:
+            bad.append((k, err, floor))
+    assert not bad, bad
+    rng = np.random.default_rng(97 + nsteps)
+    cot = {k: rng.standard_normal(np.shape(snap[k])) for k in STEP_OUT}
+    sum((out[k].double() * torch.tensor(cot[k], device="cuda")).sum() for k in STEP_OUT).backward()
+
+    def loss(pert=None, b=None):
+        s = _dry_oracle(g, inputs, bdy, snap, np.float64, nsteps, pert, b)
+        return sum(float((s[k] * cot[k]).sum()) for k in STEP_OUT)
+
+    for name in ("u", "v", "t", "ph", "w", "mu", "moist", "bias"):
+        gr = (bias.grad if name == "bias" else st[name].grad).double().cpu().numpy()
+        d = rng.standard_normal(gr.shape)
+        if name == "bias":
+            eps = 1e-6
+            fd = (loss(b=eps * d) - loss(b=-eps * d)) / (2 * eps)
+        else:
+            eps = 1e-6 * float(np.abs(snap[name]).max() or 1.0)
+            fd = (loss({name: eps * d}) - loss({name: -eps * d})) / (2 * eps)
         an, scale = float((gr * d).sum()), float(np.abs(gr * d).sum())
         assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (name, an, fd, scale)
