@@ -387,9 +387,11 @@ def run_ours(a):
     big = None
     if world == 1 and not a.no_config4:
         big = run_config4(hbm)
-    adj = {"unavailable": "no whole-step adjoint: the moisture update, the first stage's diffusion, the end-of-step "
-                          "boundary updates and WSM6 have no reverse kernels yet"}
-    if world == 1 and not a.no_adjoint:
+    adj = None
+    if world > 1:
+        adj = {"unavailable": "measured at one GPU only"}
+    elif not a.no_adjoint:
+        adj = run_adjoint_step(st, it, ms_max / a.steps)
         adj["acoustic_stage"] = run_adjoint_stage(st, it, phase_ms)
 
     cpu = None
@@ -418,6 +420,67 @@ def run_ours(a):
         dist.destroy_process_group()
     if nan:
         raise SystemExit(f"NaN in the diagnosed pressure at {nan} point(s): the timed state is not a result")
+
+
+def run_adjoint_step(st, it, fused_step_ms, reps=3):
+    """Forward + reverse pass of one whole step -- the three RK stages, the
+    microphysics (WSM6's reverse by forward-mode tangents) and the
+    end-of-step boundaries -- composed from the hand-written operator
+    adjoints (pywrf_b200.adjoint.step) on the 240x240x41 state after one
+    step, timed with CUDA events (2 warm-up passes): the fwd+adj steps per
+    second of the adjoint configuration's unit of work, the same without the
+    microphysics, and the composed forward alone, beside the fused forward
+    step."""
+    import torch
+    from pywrf_b200 import adjoint as A
+
+    g = st.g
+    it.step()
+    torch.cuda.synchronize()
+    names = tuple(dict.fromkeys(A.RK_STATE + ("u_1", "w_1", "ph_1", "mu_1", "t_1", "v_1")))
+    data = {k: st[k] for k in dict.fromkeys(A.STEP_DATA + A._Microphysics.data)}
+    keys = (("bxs", "xs"), ("bxe", "xe"), ("bys", "ys"), ("bye", "ye"), ("btxs", "txs"), ("btxe", "txe"),
+            ("btys", "tys"), ("btye", "tye"))
+    bd = {f: {key: st[f"{f}_{n}"] for n, key in keys} for f in ("u", "v", "ph", "t", "mu", "qv")}
+    sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=st.scal["cf1"], cf2=st.scal["cf2"],
+              cf3=st.scal["cf3"], cfn=st.scal["cfn"], cfn1=st.scal["cfn1"], rdx=g.rdx, rdy=g.rdy)
+    state = {k: st[k].detach().clone().requires_grad_(True) for k in names}
+    mp = lambda s: A.microphysics(s, data, g.dt, g.rdx, g.rdy)  # noqa: E731
+    gen = torch.Generator(device=st["u"].device).manual_seed(7)
+    outs = ("u", "v", "w", "ph", "t", "mu", "p", "al", "moist")
+    cot = {k: torch.randn(st[k].shape, generator=gen, device=st[k].device) for k in outs}
+
+    def run(micro, backward):
+        for v in state.values():
+            v.grad = None
+        if backward:
+            o = A.step(state, data, bd, 2.0 * g.dt, dt=g.dt, soundsteps=g.soundsteps, microphysics=micro, **sc)
+            sum((o[k] * cot[k]).sum() for k in outs).backward()
+        else:
+            with torch.no_grad():
+                A.step(state, data, bd, 2.0 * g.dt, dt=g.dt, soundsteps=g.soundsteps, microphysics=micro, **sc)
+
+    res = {}
+    for name, micro, bwd in (("fwd_adj", mp, True), ("fwd_adj_dry", None, True), ("fwd_composed", mp, False)):
+        for _ in range(2):
+            run(micro, bwd)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            run(micro, bwd)
+        e1.record()
+        torch.cuda.synchronize()
+        res[name] = e0.elapsed_time(e1) / reps
+    peak = torch.cuda.max_memory_allocated() / 2**30
+    return {"what": "one whole step (3 RK stages, WSM6 microphysics, end-of-step boundaries) forward and reverse, "
+                    "composed from the operator adjoints, 240x240x41",
+            "fwd_adj_ms": res["fwd_adj"], "fwd_adj_steps_per_s": 1e3 / res["fwd_adj"],
+            "fwd_adj_ms_without_microphysics": res["fwd_adj_dry"], "fwd_composed_ms": res["fwd_composed"],
+            "fused_forward_step_ms": fused_step_ms, "peak_gib": peak,
+            "reference_autograd": "not comparable: the reference's autograd cannot run backward through its "
+                                  "acoustic solve (in-place updates of saved operands in calc_coef_w, advance_uv, "
+                                  "advance_w)"}
 
 
 def run_adjoint_stage(st, it, phase_ms, reps=5):

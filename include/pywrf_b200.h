@@ -20,6 +20,8 @@
 #ifndef PYWRF_B200_H
 #define PYWRF_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -332,6 +334,27 @@ int wrf_bdy_final(const WrfGrid* g, const WrfState* s, void* stream);
  * those of their incoming values; muus, muvs and muts accumulate (the
  * boundary arrays and ht are data). */
 int wrf_bdy_final_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, void* stream);
+/* solver.py:1714-1766 the step's microphysics on the state table:
+ * moist_physics_prep_em, wsm6 on the solver's column block,
+ * moist_physics_finish_em and calc_p_rho_phi (wrf_physics.py:27-91,
+ * 137-1214, 2106-2137; wrf_dynamics.py:4124-4164).  The table needs t,
+ * moist, al, alb, p, pb, ph, phb, mu, muts, rdnw, h_diabatic, qv_diabatic,
+ * qc_diabatic, the precipitation accumulators and the wsm_t / wsm_qr0s
+ * scratch; the grid's dt is the step's. */
+int wrf_microphysics_op(const WrfGrid* g, const WrfState* s, void* stream);
+/* The number of floats of work wrf_microphysics_adj needs for the grid. */
+int wrf_microphysics_adj_work(const WrfGrid* g, size_t* floats);
+/* Its adjoint.  s holds the block's inputs (t, moist, al, alb, p, pb, ph,
+ * phb, mu, muts, rdnw), post the same fields after the block; sbar the
+ * cotangents of the outputs t, moist, al, p and h_diabatic, rewritten to
+ * those of the inputs, while ph, mu, muts, alb and pb accumulate.  The
+ * equation of state is reversed exactly; prep + WSM6 + finish by
+ * forward-mode tangents of a per-column restatement of the scheme (the
+ * derivative of the branch taken), assembled into the reverse product
+ * column by column.  values (optional: t, moist, h_diabatic) receives that
+ * restatement's own outputs, for checking it against the forward. */
+int wrf_microphysics_adj(const WrfGrid* g, const WrfState* s, const WrfState* post, const WrfState* sbar,
+                         float* work, size_t work_floats, const WrfState* values, void* stream);
 /* wrf_dynamics.py:4055-4164, wrf_boundary.py:470-508 the moisture update of
  * an RK stage on the state table: rk_update_scalar of qv .. qg (moist_old,
  * moist_tend, advect_tend, mu_1, mu, mub, msfty), flow_dep_bdy of qc .. qg
@@ -411,8 +434,9 @@ int wrf_advect_momentum_adj(const WrfGrid* g, int component, const float* field,
  * toward bdy + dtbc * bdy_tend over the zone rows 1..3.  bdy8: device arrays
  * xs xe ys ye (values) and txs txe tys tye (tendencies) in the solver's
  * permuted layout ([nz][ny][5] and [nz][5][nx]); variable: the reference's
- * stagger letter ('u', 'v', 'h' / 'm' for all nz levels, else nz - 1), with
- * the weights fcx / gcx the solver passes (solver.py:440-441). */
+ * stagger letter ('u', 'v', 'h' for all nz levels, 'm' for the 2-D mu
+ * (one level), else nz - 1), with the weights fcx / gcx the solver passes
+ * (solver.py:440-441). */
 int wrf_relax_bdytend(const WrfGrid* g, const float* field, float* tend, const float* const* bdy8,
                       char variable, float dtbc, void* stream);
 /* its adjoint w.r.t. the field: field_bar += d(tend)/d(field)^T tend_bar (the

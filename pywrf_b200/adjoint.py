@@ -696,7 +696,9 @@ class RelaxBdytend(torch.autograd.Function):
     def forward(ctx, field, tendency, variable: str, dtbc: float, *bdy8):
         _cuda_only(field, tendency, *bdy8)
         nz, ny, nx = field.shape
-        cg = scalar_grid(field.shape, 1.0 / 9000.0, 1.0 / 9000.0)
+        # 'm' (mu) is 2-D: its [1, ny, nx] field rides on a grid record of
+        # the frame's minimum depth, and the library relaxes one level
+        cg = scalar_grid((12, ny, nx) if variable == "m" else field.shape, 1.0 / 9000.0, 1.0 / 9000.0)
         out = tendency.detach().clone()
         arr = (ctypes.c_void_p * 8)(*[_ptr(b).value for b in bdy8])
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -911,13 +913,14 @@ class _TableOp(torch.autograd.Function):
     @staticmethod
     def backward(ctx, *gouts):
         op = ctx.op
-        named = dict(zip(op.fields + op.data, ctx.saved_tensors))
+        saved = ctx.saved_tensors  # read once (checkpoint unpacks each saved tensor once)
+        named = dict(zip(op.fields + op.data, saved))
         bars = {k: torch.zeros_like(named[k]) for k in op.fields}
         for k, gr in zip(op.outputs, gouts):
             if gr is not None:
                 bars[k] = gr.contiguous().clone()
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-        with torch.cuda.device(ctx.saved_tensors[0].device):
+        with torch.cuda.device(saved[0].device):
             N.check(op.adj(ctx.cg, _table(named), _table(bars), stream), op.name + "_adj")
         return (None, None) + tuple(bars[k] for k in op.fields) + (None,) * len(op.data)
 
@@ -1420,6 +1423,72 @@ def step_end(st: dict, data: dict, bdy: dict, dtbc: float, *, cf1: float, cf2: f
     outs = _TableOp.apply(op, cg, *[s[k] for k in op.fields], *[dd[k] for k in op.data])
     s.update(dict(zip(op.outputs, outs)))
     return s
+
+
+class _Microphysics:
+    """The step's microphysics (moist_physics_prep_em, WSM6,
+    moist_physics_finish_em, calc_p_rho_phi) as a table operator; the
+    precipitation accumulators and the diagnostic tendencies it also writes
+    go to scratch (they do not feed back into the state)."""
+    name = "wrf_microphysics_op"
+    fields = ("t", "moist", "al", "p", "ph", "h_diabatic", "mu", "muts")
+    outputs = ("t", "moist", "al", "p", "h_diabatic")
+    data = ("alb", "pb", "phb", "rdnw")
+    scratch3 = ("qv_diabatic", "qc_diabatic", "wsm_t", "wsm_qr0s")
+    scratch2 = ("rainnc", "rainncv", "snownc", "snowncv", "graupelnc", "graupelncv", "sr")
+
+    def __init__(self, like):
+        nz, ny, nx = like.shape
+        dev = like.device
+        self.s3 = {k: torch.zeros(nz, ny, nx, dtype=torch.float32, device=dev) for k in self.scratch3}
+        self.s2 = {k: torch.zeros(ny, nx, dtype=torch.float32, device=dev) for k in self.scratch2}
+        self.dbar = {k: torch.zeros(nz, ny, nx, dtype=torch.float32, device=dev) for k in ("alb", "pb")}
+
+    def _scratch(self, tab):
+        names = N.field_names()
+        for k, v in {**self.s3, **self.s2}.items():
+            tab[names.index(k)] = v.data_ptr()
+
+    def fwd(self, cg, tab, stream):
+        self._scratch(tab)
+        return N.lib().wrf_microphysics_op(ctypes.byref(cg), tab, stream)
+
+    def adj(self, cg, tab, btab, stream):
+        names = N.field_names()
+        # the state after the block, recomputed from clones of the inputs it
+        # updates (the other fields are the same tensors)
+        ptab = (ctypes.c_void_p * len(names))()
+        for q in range(len(names)):
+            ptab[q] = tab[q]
+        clones = {k: self._saved[k].detach().clone() for k in self.outputs}
+        for k, v in clones.items():
+            ptab[names.index(k)] = v.data_ptr()
+        self._scratch(ptab)
+        rc = N.lib().wrf_microphysics_op(ctypes.byref(cg), ptab, stream)
+        if rc:
+            return rc
+        for k, v in self.dbar.items():
+            btab[names.index(k)] = v.data_ptr()
+        n = ctypes.c_size_t(0)
+        rc = N.lib().wrf_microphysics_adj_work(ctypes.byref(cg), ctypes.byref(n))
+        if rc:
+            return rc
+        work = torch.empty(int(n.value), dtype=torch.float32, device=clones["t"].device)
+        return N.lib().wrf_microphysics_adj(ctypes.byref(cg), tab, ptab, btab, ctypes.c_void_p(work.data_ptr()), n,
+                                            None, stream)
+
+
+def microphysics(st: dict, data: dict, dt: float, rdx, rdy) -> dict:
+    """Differentiable microphysics of the step (pywrf/solver.py:1714-1766):
+    returns ``st`` with t, moist, al, p and h_diabatic replaced.  Its reverse
+    is the equation of state's exact reverse, then prep + WSM6 + finish by
+    forward-mode tangents of a per-column restatement of the scheme."""
+    op = _Microphysics(st["t"])
+    cg = scalar_grid(st["t"].shape, rdx, rdy)
+    cg.dt = float(dt)
+    op._saved = {k: st[k] for k in op.outputs}
+    outs = _TableOp.apply(op, cg, *[st[k] for k in op.fields], *[data[k] for k in op.data])
+    return {**st, **dict(zip(op.outputs, outs))}
 
 
 STEP_DATA = tuple(dict.fromkeys(RK_DATA + ("msfuy", "msfvx", "msftx", "msfty", "ht")))

@@ -1230,13 +1230,17 @@ int launch_relax_field(const Grid& g, const float* field, float* tend, const flo
   S s{};
   for (int q = 0; q < 8; ++q) s.f[q] = const_cast<float*>(bdy8[q]);
   const dim3 b3(32, 4);
-  k_relax_field<<<point_grid(g, b3), b3, 0, st>>>(g, s, relax_shape(g, var), field, tend, dtbc);
+  Grid g2 = g;
+  if (var == 'm') g2.nz = 1;  // mu is 2-D
+  k_relax_field<<<point_grid(g2, b3), b3, 0, st>>>(g2, s, relax_shape(g2, var), field, tend, dtbc);
   return 1;
 }
 
 int launch_relax_field_adj(const Grid& g, const float* tbar, float* fbar, char var, cudaStream_t st) {
   const dim3 b3(32, 4);
-  k_relax_field_adj<<<point_grid(g, b3), b3, 0, st>>>(g, relax_shape(g, var), tbar, fbar);
+  Grid g2 = g;
+  if (var == 'm') g2.nz = 1;
+  k_relax_field_adj<<<point_grid(g2, b3), b3, 0, st>>>(g2, relax_shape(g2, var), tbar, fbar);
   return 1;
 }
 

@@ -160,6 +160,14 @@ __global__ void k_moist_update_adj(Grid g, S s, S b, int rk_step, float dt) {
 
 }  // namespace
 
+// calc_p_rho_phi's reverse alone, with the state's own qv (the equation of
+// state after the microphysics)
+int launch_eos_adj(const Grid& g, const S& s, const S& b, cudaStream_t st) {
+  const dim3 b3(32, 4);
+  k_eos_adj<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, s[WF_MOIST] + g.n3());
+  return 1;
+}
+
 // work: caller-owned scratch of nz * ny * nx floats
 int launch_moist_adj(const Grid& g, const S& s, const S& b, int rk_step, float dt_rk, float* work, cudaStream_t st) {
   const dim3 b3(32, 4);

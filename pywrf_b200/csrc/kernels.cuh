@@ -151,6 +151,16 @@ int launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st);
 int launch_moist(const Grid& g, const S& s, int rk_step, float dt_rk, cudaStream_t st);
 // its adjoint (k_adjoint_moist.cu); work: nz*ny*nx floats
 int launch_moist_adj(const Grid& g, const S& s, const S& b, int rk_step, float dt_rk, float* work, cudaStream_t st);
+// calc_p_rho_phi's reverse with the state's own qv (k_adjoint_moist.cu)
+int launch_eos_adj(const Grid& g, const S& s, const S& b, cudaStream_t st);
+// the microphysics block's reverse (the equation of state after it, then
+// prep + WSM6 + finish by forward-mode tangents; k_adjoint_wsm6.cu): s holds
+// the block's inputs, post the state after it; work holds
+// microphysics_adj_work_floats(g) floats; values (optional) receives the
+// tangent code's own outputs
+size_t microphysics_adj_work_floats(const Grid& g);
+int launch_physics_adj(const Grid& g, const S& s, const S& post, const S& b, float* work, float dt, cudaStream_t st,
+                       const S* values);
 int launch_bdy_final(const Grid& g, const S& s, cudaStream_t st);
 // spec_bdy_final + set_w_surface as a stand-alone operator and its adjoint
 // (k_adjoint_end.cu)

@@ -594,6 +594,15 @@ constexpr int kBdyFinalOperands[] = {
     WF_QV_BXS + 5, WF_QV_BXS + 6, WF_QV_BXS + 7};
 constexpr int kBdyFinalCotangents[] = {WF_U, WF_V, WF_T, WF_PH, WF_MOIST, WF_W, WF_MUUS, WF_MUVS, WF_MUTS};
 
+// the microphysics block's operands (moist_physics_prep_em, WSM6,
+// moist_physics_finish_em, calc_p_rho_phi), those its reverse reads, and
+// the cotangents
+constexpr int kMpOperands[] = {WF_T, WF_MOIST, WF_AL, WF_ALB, WF_P, WF_PB, WF_PH, WF_PHB, WF_MU, WF_MUTS, WF_RDNW,
+                               WF_H_DIABATIC, WF_QV_DIABATIC, WF_QC_DIABATIC, WF_RAINNC, WF_RAINNCV, WF_SNOWNC,
+                               WF_SNOWNCV, WF_GRAUPELNC, WF_GRAUPELNCV, WF_SR, WF_WSM_T, WF_WSM_QR0S};
+constexpr int kMpAdjOperands[] = {WF_T, WF_MOIST, WF_AL, WF_ALB, WF_P, WF_PB, WF_PH, WF_PHB, WF_MU, WF_MUTS, WF_RDNW};
+constexpr int kMpCotangents[] = {WF_T, WF_MOIST, WF_AL, WF_ALB, WF_P, WF_PB, WF_PH, WF_MU, WF_MUTS, WF_H_DIABATIC};
+
 // rk_addtend_dry's operands and cotangents
 constexpr int kAddtendOperands[] = {WF_RU_TEND, WF_RV_TEND, WF_RW_TEND, WF_PH_TEND, WF_T_TEND, WF_MU_TEND,
                                     WF_RU_TENDF, WF_RV_TENDF, WF_RW_TENDF, WF_PH_TENDF, WF_T_TENDF, WF_MU_TENDF,
@@ -1116,6 +1125,44 @@ int wrf_bdy_final_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* s
   cudaGetLastError();
   launch_bdy_final_op_adj(g, s, b, static_cast<cudaStream_t>(stream));
   return check_launch("bdy_final_adj");
+}
+
+int wrf_microphysics_op(const WrfGrid* gin, const WrfState* sin, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s;
+  if ((rc = state_of(sin, kMpOperands, sizeof(kMpOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_physics(g, s, static_cast<cudaStream_t>(stream));
+  return check_launch("microphysics_op");
+}
+
+int wrf_microphysics_adj_work(const WrfGrid* gin, size_t* floats) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!floats) return fail(WRF_EINVAL, "null argument");
+  *floats = microphysics_adj_work_floats(g);
+  return WRF_OK;
+}
+
+int wrf_microphysics_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* spost, const WrfState* sbar,
+                         float* work, size_t work_floats, const WrfState* values, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!work || work_floats < microphysics_adj_work_floats(g))
+    return fail(WRF_EINVAL, "microphysics_adj: work smaller than wrf_microphysics_adj_work gives");
+  S s, post, b, vo;
+  if ((rc = state_of(sin, kMpAdjOperands, sizeof(kMpAdjOperands) / sizeof(int), s))) return rc;
+  if ((rc = state_of(spost, kMpAdjOperands, sizeof(kMpAdjOperands) / sizeof(int), post))) return rc;
+  if ((rc = state_of(sbar, kMpCotangents, sizeof(kMpCotangents) / sizeof(int), b))) return rc;
+  const int kVals[] = {WF_T, WF_MOIST, WF_H_DIABATIC};
+  if (values && (rc = state_of(values, kVals, 3, vo))) return rc;
+  cudaGetLastError();
+  launch_physics_adj(g, s, post, b, work, g.dt, static_cast<cudaStream_t>(stream), values ? &vo : nullptr);
+  return check_launch("microphysics_adj");
 }
 
 int wrf_moist_update(const WrfGrid* gin, const WrfState* sin, int rk_step, float dt_rk, void* stream) {
