@@ -157,14 +157,22 @@ __device__ void fall_interfaces(const Col<T>& C, int km, float dt) {
 
 // the piecewise-constant overlap remap of the departure cells' mass (array
 // qa, the top cell's zeroed) onto the grid (wrf_physics.py:1339-1357, the
-// last layers 3800 m deep), written into array out
+// last layers 3800 m deep), written into array out.  A pair of cells whose
+// overlap is not positive contributes the constant 0 (value and
+// derivatives), so the pairs are screened on the values first: only the
+// few overlapping departure cells of a level enter the dual arithmetic.
 template <class T>
 __device__ void remap(const Col<T>& C, int km, int qa, int out) {
+  float za[kMaxNz + 1];
+  for (int k = 0; k <= km; ++k) za[k] = val(C(A_ZA, k));
   for (int k = 0; k < km; ++k) {
     const T zlo = C(A_ZI, k);
     const T zhi = k < km - 1 ? C(A_ZI, k + 1) : C(A_ZI, km - 1) + 3800.0f;
+    const float zlov = val(zlo), zhiv = val(zhi);
     T acc = cst<T>(0.f);
     for (int ka = 0; ka < km; ++ka) {
+      const float alov = za[ka], ahiv = ka < km - 1 ? za[ka + 1] : za[km - 1] + 3800.0f;
+      if (!(vmin(zhiv, ahiv) - vmax(zlov, alov) > 0.0f)) continue;
       const T alo = C(A_ZA, ka);
       const T ahi = ka < km - 1 ? C(A_ZA, ka + 1) : C(A_ZA, km - 1) + 3800.0f;
       const T ov = vmax(0.0f, vmin(zhi, ahi) - vmax(zlo, alo));

@@ -1349,10 +1349,13 @@ def test_theta_bias_gradient_of_two_steps_against_the_reference():
     tt = torch.tensor(Z["target_t"], device="cuda")
     tq = torch.tensor(Z["target_qv"], device="cuda")
     loss = ((out["t"][R].double() - tt) ** 2).mean() + ((out["moist"][1][R].double() - tq) ** 2).mean()
-    assert abs(float(loss) - float(Z["loss0"])) <= 1e-4 * abs(float(Z["loss0"])), (float(loss), float(Z["loss0"]))
+    l0 = float(loss.detach())
+    assert abs(l0 - float(Z["loss0"])) <= 1e-4 * abs(float(Z["loss0"])), (l0, float(Z["loss0"]))
     loss.backward()
     gr = bias.grad.double().cpu().numpy()
     got = np.array([gr[k, j, i] for k, j, i in Z["points"]])
     fd = np.asarray(Z["fd"], np.float64)
     tol = 1e-2 * np.abs(fd) + 1e-3 * np.abs(fd).max()
+    print("theta-bias gradient: loss %.9g (reference %.9g); max |adjoint - reference| / max |reference| = %.3g"
+          % (l0, float(Z["loss0"]), float(np.abs(got - fd).max() / np.abs(fd).max())))
     assert np.all(np.abs(got - fd) <= tol), list(zip(got, fd))
