@@ -191,13 +191,6 @@ int wrf_advect_scalar_adj(const WrfGrid* g, const float* field, const float* ru,
                           const float* rom, const float* msftx, const float* fzm, const float* fzp,
                           const float* rdzw, const float* tend_bar, float* field_bar, float* ru_bar,
                           float* rv_bar, float* rom_bar, void* stream);
-/* wrf_dynamics.py:3391-3525 advance_uv followed by spec_bdyupdate of u and
- * v (wrf_boundary.py:244-290), as the acoustic substep calls them
- * (solver.py:1350-1377): u and v of the state table are updated in place
- * from the table's ru_tend, rv_tend, p, pb, ph, php, alt, al, mu, muu, muv,
- * cqu, cqv, mudf, msfux, msfuy, msfvx, msfvx_inv, msfvy, fnm, fnp, rdnw and
- * the grid's emdiv, cf1..cf3 (spec_zone 1); fields it does not read may be
- * null.  Runs the kernel of the form wrf_set_kernel_form selects. */
 /* wrf_dynamics.py:2031-2620 the large-step tendency terms selected by the
  * mask `terms` (1 rhs_ph, 2 horizontal_pressure_gradient, 4 pg_buoy_w, 8
  * coriolis, 16 curvature) on the state table, with the solver's arguments:
@@ -355,6 +348,10 @@ int wrf_microphysics_adj_work(const WrfGrid* g, size_t* floats);
  * restatement's own outputs, for checking it against the forward. */
 int wrf_microphysics_adj(const WrfGrid* g, const WrfState* s, const WrfState* post, const WrfState* sbar,
                          float* work, size_t work_floats, const WrfState* values, void* stream);
+/* wrf_dynamics.py:4124-4164 calc_p_rho_phi on the state table: al and p on
+ * the mass points below the top level from ph, t, qv (moist slot 1), alb,
+ * pb, mu, muts, rdnw; NaN in p is counted in the status words. */
+int wrf_calc_p_rho_phi(const WrfGrid* g, const WrfState* s, void* stream);
 /* wrf_dynamics.py:4055-4164, wrf_boundary.py:470-508 the moisture update of
  * an RK stage on the state table: rk_update_scalar of qv .. qg (moist_old,
  * moist_tend, advect_tend, mu_1, mu, mub, msfty), flow_dep_bdy of qc .. qg
@@ -367,6 +364,13 @@ int wrf_moist_update(const WrfGrid* g, const WrfState* s, int rk_step, float dt_
  * first stage) are accumulated; work: nz * ny * nx floats. */
 int wrf_moist_update_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar, int rk_step, float dt_rk,
                          float* work, void* stream);
+/* wrf_dynamics.py:3391-3525 advance_uv followed by spec_bdyupdate of u and
+ * v (wrf_boundary.py:244-290), as the acoustic substep calls them
+ * (solver.py:1350-1377): u and v of the state table are updated in place
+ * from the table's ru_tend, rv_tend, p, pb, ph, php, alt, al, mu, muu, muv,
+ * cqu, cqv, mudf, msfux, msfuy, msfvx, msfvx_inv, msfvy, fnm, fnp, rdnw and
+ * the grid's emdiv, cf1..cf3 (spec_zone 1); fields it does not read may be
+ * null.  Runs the kernel of the form wrf_set_kernel_form selects. */
 int wrf_advance_uv(const WrfGrid* g, const WrfState* s, float dts, void* stream);
 /* Its adjoint (reverse mode): sbar holds, under the same field ids, the
  * cotangents of the updated u and v (which are also those of the incoming

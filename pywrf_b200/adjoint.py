@@ -47,6 +47,19 @@ operators keeps no tape of the forward's intermediates.
 * :class:`VSolveW` -- the vertically implicit w solve of advance_w
   (pywrf/wrf_dynamics.py:3761-3767); gradients with respect to the
   right-hand side and the coefficients a, alpha, gamma (the transposed solve).
+* :class:`HorizontalDiffusion`, :func:`eddy_viscosity`, :class:`MassWeight`
+  -- the first RK stage's diffusion (pywrf/wrf_dynamics.py:2623-2915), the
+  eddy viscosities (compute_diff_metrics, cal_deform_and_div,
+  calculate_km_kh: :491-995) and mass_weight (pywrf/wrf_boundary.py:408).
+* :func:`addtend`, :class:`SpecBdytend`, the moisture update
+  (rk_update_scalar, flow_dep_bdy, calc_p_rho_phi), :func:`microphysics`
+  (moist_physics_prep_em, WSM6, moist_physics_finish_em, calc_p_rho_phi;
+  WSM6's reverse by forward-mode tangents of a per-column restatement) and
+  :func:`step_end` (halo copies, spec_bdy_final, set_w_surface).
+* Composed in the reference's order: :func:`acoustic_substep`,
+  :func:`acoustic_stage`, :func:`dynamics_stage`, :func:`moist_stage`,
+  :func:`rk_stage` and :func:`step` (one whole time step,
+  pywrf/solver.py:709-1910, with an optional theta-tendency bias).
 * :func:`rollout` -- truncated backpropagation through ``n_steps`` of a
   step made of these operators with per-step (or per-segment) checkpointing:
   only each segment's input state is kept, and the backward pass recomputes

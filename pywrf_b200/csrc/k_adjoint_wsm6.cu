@@ -68,6 +68,17 @@ __device__ T vt_of(int kind, const T& q, const T& den, const T& denfac, const T&
   return val(q) <= 0.f ? cst<T>(0.f) : pv * rb * denfac;
 }
 
+// whether any directional derivative of x is nonzero (always true for a
+// plain float, whose value path is the point of running the code)
+__device__ __forceinline__ bool live(float) { return true; }
+template <int N>
+__device__ __forceinline__ bool live(const Dual<N>& x) {
+  bool any = false;
+#pragma unroll
+  for (int n = 0; n < N; ++n) any |= x.d[n] != 0.f;
+  return any;
+}
+
 template <class T>
 struct Slope3 {
   T rs[3], rb[3], r2[3], r3[3];
@@ -205,6 +216,14 @@ __device__ T nislfv(const Col<T>& C, int km, int kind, int r1, int r2, float dt,
   for (int k = 0; k < km; ++k) allold = allold + C(r1, k);
   if (kind == 1)
     for (int k = 0; k < km; ++k) allold = allold + C(r2, k);
+  if (!(val(allold) > 0.f)) {
+    // nothing to fall: the scheme's result is zero (value and derivatives)
+    for (int k = 0; k < km; ++k) {
+      C(r1, k) = cst<T>(0.f);
+      if (kind == 1) C(r2, k) = cst<T>(0.f);
+    }
+    return cst<T>(0.f);
+  }
   C(A_ZI, 0) = cst<T>(0.f);
   for (int k = 0; k < km; ++k) C(A_ZI, k + 1) = C(A_ZI, k) + C(A_DELZ, k);
   for (int k = 0; k < km; ++k) {
@@ -513,7 +532,7 @@ __device__ void point_processes(T& t, T& q, T& qc, T& qi, T& qr, T& qs, T& qg, c
 // A_T (temperature), A_Q, A_QC, A_QI, A_QR, A_QS, A_QG, A_DEN, A_P and
 // A_DELZ hold the inputs and receive the results
 template <class T>
-__device__ void wsm6_column(const Col<T>& C, int km, float delt) {
+__device__ void wsm6_column(const Col<T>& C, int km, float delt, bool skip_dead = false) {
   for (int k = 0; k < km; ++k) {
     const T q = C(A_Q, k), t = C(A_T, k);
     C(A_CPM, k) = val(q) >= F(QMIN) ? F(CPV) * q + (1.0f - q) * F(CPD) : cst<T>(F(CPD * (1.0 - QMIN) + CPV * QMIN));
@@ -603,6 +622,14 @@ __device__ void wsm6_column(const Col<T>& C, int km, float delt) {
       T t = C(A_T, k), q = C(A_Q, k), qc = C(A_QC, k), qr = C(A_QR, k), qs = C(A_QS, k), qg = C(A_QG, k);
       const T den = C(A_DEN, k);
       T qi = vmax(C(A_R1, k) / den, 0.0f);
+      // a level whose every operand has zero tangents keeps zero tangents
+      // through the processes; its values are not needed when only the
+      // derivatives are wanted
+      if (skip_dead && !(live(t) || live(q) || live(qc) || live(qr) || live(qs) || live(qg) || live(den) ||
+                         live(qi) || live(C(A_P, k)) || live(C(A_DENFAC, k)) || live(C(A_CPM, k)) ||
+                         live(C(A_XL, k)) || live(C(A_QS0, k)) || live(C(A_QS1, k)) || live(C(A_RH0, k)) ||
+                         live(C(A_RH1, k)) || live(C(A_SR3, k)) || live(C(A_SRS, k))))
+        continue;
       Slope3<T> sl0;
       sl0.r3[0] = C(A_SR3, k);
       sl0.rs[0] = C(A_SRS, k);
@@ -684,7 +711,8 @@ __global__ void __launch_bounds__(64) k_mp_tangent(Grid g, S s, S yb, S b, int p
     C(A_DELZ, k) = zhi - zlo;
     for (int m = 1; m < 7; ++m) C(slot_of[m - 1], k) = seed(m * km + k, s[WF_MOIST][m * n3 + p]);
   }
-  wsm6_column(C, km, dt);
+  // (pass 0 with values wanted runs every level for its values)
+  wsm6_column(C, km, dt, !(vo[WF_T] && pass == 0));
   // moist_physics_finish_em and the reverse products
   float acc[N];
 #pragma unroll

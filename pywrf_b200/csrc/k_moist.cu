@@ -222,6 +222,13 @@ int launch_moist(const Grid& g, const S& s, int rk_step, float dt_rk, cudaStream
   return 2;
 }
 
+// calc_p_rho_phi alone (al and p from ph, t, qv; NaN in p counted)
+int launch_eos(const Grid& g, const S& s, cudaStream_t st) {
+  const dim3 b3(32, 4);
+  k_eos_flowdep<<<point_grid(g, b3), b3, 0, st>>>(g, s, 0);
+  return 1;
+}
+
 int launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st) {
   const dim3 b3(32, 4);
   k_hdiff_moist<<<point_grid(g, b3), b3, 0, st>>>(g, s);

@@ -148,6 +148,8 @@ int launch_small_step_finish_adj(const Grid& g, const S& s, const S& b, float dt
 
 // moisture (k_moist.cu)
 int launch_hdiff_moist(const Grid& g, const S& s, cudaStream_t st);
+// calc_p_rho_phi alone (k_moist.cu)
+int launch_eos(const Grid& g, const S& s, cudaStream_t st);
 int launch_moist(const Grid& g, const S& s, int rk_step, float dt_rk, cudaStream_t st);
 // its adjoint (k_adjoint_moist.cu); work: nz*ny*nx floats
 int launch_moist_adj(const Grid& g, const S& s, const S& b, int rk_step, float dt_rk, float* work, cudaStream_t st);

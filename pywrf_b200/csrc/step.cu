@@ -603,6 +603,10 @@ constexpr int kMpOperands[] = {WF_T, WF_MOIST, WF_AL, WF_ALB, WF_P, WF_PB, WF_PH
 constexpr int kMpAdjOperands[] = {WF_T, WF_MOIST, WF_AL, WF_ALB, WF_P, WF_PB, WF_PH, WF_PHB, WF_MU, WF_MUTS, WF_RDNW};
 constexpr int kMpCotangents[] = {WF_T, WF_MOIST, WF_AL, WF_ALB, WF_P, WF_PB, WF_PH, WF_MU, WF_MUTS, WF_H_DIABATIC};
 
+// calc_p_rho_phi's operands
+constexpr int kEosOperands[] = {WF_AL, WF_ALB, WF_MU, WF_MUTS, WF_PH, WF_P, WF_PB, WF_T, WF_MOIST, WF_RDNW,
+                                WF_STATUS};
+
 // rk_addtend_dry's operands and cotangents
 constexpr int kAddtendOperands[] = {WF_RU_TEND, WF_RV_TEND, WF_RW_TEND, WF_PH_TEND, WF_T_TEND, WF_MU_TEND,
                                     WF_RU_TENDF, WF_RV_TENDF, WF_RW_TENDF, WF_PH_TENDF, WF_T_TENDF, WF_MU_TENDF,
@@ -1163,6 +1167,17 @@ int wrf_microphysics_adj(const WrfGrid* gin, const WrfState* sin, const WrfState
   cudaGetLastError();
   launch_physics_adj(g, s, post, b, work, g.dt, static_cast<cudaStream_t>(stream), values ? &vo : nullptr);
   return check_launch("microphysics_adj");
+}
+
+int wrf_calc_p_rho_phi(const WrfGrid* gin, const WrfState* sin, void* stream) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  S s;
+  if ((rc = state_of(sin, kEosOperands, sizeof(kEosOperands) / sizeof(int), s))) return rc;
+  cudaGetLastError();
+  launch_eos(g, s, static_cast<cudaStream_t>(stream));
+  return check_launch("calc_p_rho_phi");
 }
 
 int wrf_moist_update(const WrfGrid* gin, const WrfState* sin, int rk_step, float dt_rk, void* stream) {

@@ -1,4 +1,5 @@
-"""Drop-in for the WSM6 entry of ``pywrf.wrf_physics`` (reference signature).
+"""Drop-ins for ``pywrf.wrf_physics.wsm6`` and ``microphysics_driver``
+(reference signatures).
 
 ``wsm6(...)`` takes the arguments of the reference function
 (pywrf/wrf_physics.py:137-151) and runs the scheme on the GPU through
@@ -72,3 +73,21 @@ def wsm6(th, q, qc, qr, qi, qs, qg, den, pii, p, delz, delt, g, cpd, cpv, rd, rv
                               ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     N.check(rc, "wrf_wsm6")
     return th, q, qc, qr, qi, qs, qg, rain, rainncv, snow, snowncv, graupel, graupelncv, sr, refl_10cm
+
+
+def microphysics_driver(th, rho, pi_phy, p, ht, dz8w, p8w, dt, dx, dy, qv_curr, qc_curr, qr_curr, qi_curr, qs_curr,
+                        qg_curr, rainnc, rainncv, snownc, snowncv, sr, refl_10cm, diagflag, do_radar_ref, graupelnc,
+                        graupelncv, has_reqc, has_reqi, has_reqs, re_cloud, re_ice, re_snow, ids, ide, jds, jde, kds,
+                        kde, ims, ime, jms, jme, kms, kme, its, ite, jts, jte, kts, kte):
+    """microphysics_driver (pywrf/wrf_physics.py:94-135): WSM6 with the
+    driver's constants, on the GPU through :func:`wsm6`; returns what the
+    reference returns (th, qv .. qg, the precipitation accumulators, sr,
+    refl_10cm).  ht, p8w, dx and dy are accepted and unused, as in the
+    reference."""
+    c = _CONSTANTS
+    return wsm6(th, qv_curr, qc_curr, qr_curr, qi_curr, qs_curr, qg_curr, rho, pi_phy, p, dz8w, dt, c["g"], c["cpd"],
+                c["cpv"], c["rd"], c["rv"], c["t0c"], c["ep1"], c["ep2"], c["qmin"], c["xls"], c["xlv0"], c["xlf0"],
+                c["den0"], c["denr"], c["cliq"], c["cice"], c["psat"], rainnc, rainncv, snownc, snowncv, sr,
+                refl_10cm, diagflag, do_radar_ref, graupelnc, graupelncv, has_reqc, has_reqi, has_reqs, re_cloud,
+                re_ice, re_snow, ids, ide, jds, jde, kds, kde, ims, ime, jms, jme, kms, kme, its, ite, jts, jte, kts,
+                kte)
