@@ -35,7 +35,10 @@ Extra keys of the JSON line:
                 on harvested WSM6 increments, then one unseen state run for
                 1 h with the plain and the surrogate step (speed, hydrometeor
                 mass and precipitation errors, tensor-core roofline)
-  adjoint       unavailable: operator adjoints only (no whole-step adjoint)
+  adjoint       one whole step forward + reverse (WSM6 included) composed
+                from the hand-written operator adjoints, with and without the
+                microphysics, beside the fused forward step; and the acoustic
+                part of RK stage 3 alone
 ``--impl reference`` times that CPU path alone (rank 0; other ranks exit).
 """
 from __future__ import annotations

@@ -569,7 +569,15 @@ __device__ float nislfv_w(const Seg<SEG, NS>& g, const float (&den)[NS], const f
   bool any = false;
 #pragma unroll
   for (int s = 0; s < NS; ++s) any |= (g.k(s) < km && rq[s] > 0.f);
-  const bool ok = g.bits(__ballot_sync(kFull, any)) != 0u;
+  const unsigned wb = __ballot_sync(kFull, any);
+  const bool ok = g.bits(wb) != 0u;
+  // no mass in any column of the warp: the result is zero, as the full
+  // path would store it
+  if (wb == 0u) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) rq[s] = 0.f;
+    return 0.f;
+  }
   float www[NS], dza[NS], qa[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) www[s] = ww0[s];
@@ -608,7 +616,20 @@ __device__ void nislfv6_w(const Seg<SEG, NS>& g, const float (&den)[NS], const f
   bool any = false;
 #pragma unroll
   for (int s = 0; s < NS; ++s) any |= (g.k(s) < km && (rq[s] > 0.f || rq2[s] > 0.f));
-  const bool ok = g.bits(__ballot_sync(kFull, any)) != 0u;
+  const unsigned wb = __ballot_sync(kFull, any);
+  const bool ok = g.bits(wb) != 0u;
+  // no mass in any column of the warp: the results are zero, as the full
+  // path would store them
+  if (wb == 0u) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      rq[s] = 0.f;
+      rq2[s] = 0.f;
+    }
+    *p1 = 0.f;
+    *p2 = 0.f;
+    return;
+  }
   float www[NS], dza[NS], qa[NS], qa2[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) www[s] = ww0[s];
