@@ -657,7 +657,7 @@ __device__ void wsm6_column(const Col<T>& C, int km, float delt, bool skip_dead 
 // the outputs' values.
 template <int N>
 __global__ void __launch_bounds__(64) k_mp_tangent(Grid g, S s, S yb, S b, int pass, float dt, Dual<N>* ws,
-                                                   int ncol, S vo) {
+                                                   int ncol, S vo, int* quiet) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   const int wi = g.ide - 1 - (g.ids + 1), wj = g.jde - 1 - (g.jds + 1);
   if (col >= ncol || col >= wi * wj) return;
@@ -681,6 +681,41 @@ __global__ void __launch_bounds__(64) k_mp_tangent(Grid g, S s, S yb, S b, int p
         vo[WF_H_DIABATIC][p] = 0.f;
       }
     }
+    return;
+  }
+  // A quiet column -- no cloud, rain, ice, snow or graupel at any level, and
+  // qv below both saturation mixing ratios everywhere -- takes no
+  // process at all: every rate is zero, nothing falls, the saturation
+  // adjustment condenses nothing, and its reverse product is theta's and
+  // qv's cotangents passed through, zero for the hydrometeors (their
+  // results are constants: the zero of the empty sedimentation and the
+  // final zeroing of cloud and ice) and for h_diabatic.  Found at pass 0
+  // on the value path (unless the values are wanted), remembered per column.
+  if (pass == 0) {
+    bool q0 = !vo[WF_T];
+    for (int k = 0; k < km && q0; ++k) {
+      const size_t p = k * lev + c2;
+      for (int m = 2; m < 7; ++m) q0 = q0 && !(s[WF_MOIST][m * n3 + p] > 0.f);
+      const float th = s[WF_T][p] + (float)T0;
+      const float pfull = s[WF_P][p] + s[WF_PB][p];
+      const float t = th * wpow(pfull / (float)P0, F(RCP));
+      float qs0, qs1;
+      fpvs(t, pfull, qs0, qs1);
+      const float qv = s[WF_MOIST][n3 + p];
+      q0 = q0 && qv < qs0 && qv < qs1;
+    }
+    quiet[col] = q0 ? 1 : 0;
+    if (q0) {
+      for (int k = 0; k < km; ++k) {
+        const size_t p = k * lev + c2;
+        b[WF_T][p] = yb[WF_T][p];
+        b[WF_MOIST][n3 + p] = yb[WF_MOIST][n3 + p];
+        for (int m = 2; m < 7; ++m) b[WF_MOIST][m * n3 + p] = 0.f;
+        b[WF_H_DIABATIC][p] = 0.f;
+      }
+      return;
+    }
+  } else if (quiet[col]) {
     return;
   }
   using T = Dual<N>;
@@ -761,7 +796,7 @@ constexpr int kMpDirections = 8;
 
 size_t microphysics_adj_work_floats(const Grid& g) {
   const size_t ncol = (size_t)(g.ide - 1 - (g.ids + 1)) * (g.jde - 1 - (g.jds + 1));
-  return 9 * g.n3() + (size_t)mpt::A_COUNT * g.nz * ncol * (kMpDirections + 1);
+  return 9 * g.n3() + (size_t)mpt::A_COUNT * g.nz * ncol * (kMpDirections + 1) + ncol;
 }
 
 int launch_physics_adj(const Grid& g, const S& s, const S& post, const S& b, float* work, float dt, cudaStream_t st,
@@ -778,11 +813,12 @@ int launch_physics_adj(const Grid& g, const S& s, const S& post, const S& b, flo
   cudaMemcpyAsync(yb.f[WF_H_DIABATIC], b[WF_H_DIABATIC], n3 * sizeof(float), cudaMemcpyDeviceToDevice, st);
   auto* ws = reinterpret_cast<Dual<kMpDirections>*>(work + 9 * n3);
   const int km = g.nz - 1, ncol = (g.ide - 1 - (g.ids + 1)) * (g.jde - 1 - (g.jds + 1));
+  int* quiet = reinterpret_cast<int*>(work + 9 * n3 + (size_t)mpt::A_COUNT * g.nz * ncol * (kMpDirections + 1));
   const int nin = 9 * km + g.nz, passes = (nin + kMpDirections - 1) / kMpDirections;
   S vo{};
   if (values) vo = *values;
   for (int pass = 0; pass < passes; ++pass) {
-    mpt::k_mp_tangent<kMpDirections><<<(ncol + 63) / 64, 64, 0, st>>>(g, s, yb, b, pass, dt, ws, ncol, vo);
+    mpt::k_mp_tangent<kMpDirections><<<(ncol + 63) / 64, 64, 0, st>>>(g, s, yb, b, pass, dt, ws, ncol, vo, quiet);
     ++n;
   }
   return n;
