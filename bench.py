@@ -389,7 +389,7 @@ def run_ours(a):
 
     big = None
     if world == 1 and not a.no_config4:
-        big = run_config4(hbm)
+        big = run_config4(hbm, with_adjoint=not a.no_adjoint)
     adj = None
     if world > 1:
         adj = {"unavailable": "measured at one GPU only"}
@@ -551,10 +551,11 @@ def run_adjoint_stage(st, it, phase_ms, reps=5):
                                   "advance_w)"}
 
 
-def run_config4(hbm):
+def run_config4(hbm, with_adjoint=True):
     """The 512x512x61 workload (dt 30 s, one 36-step integration) with the
     plain step: steps/s, grid-point updates/s, the step's ledger fraction of
-    the HBM peak, peak device memory and the NaN count."""
+    the HBM peak, peak device memory and the NaN count; with_adjoint adds
+    the forward + reverse of whole steps at that size (config4_adjoint)."""
     import torch
     from pywrf_b200 import _native as N_
     from pywrf_b200 import synthetic
@@ -590,6 +591,12 @@ def run_config4(hbm):
     ledger = 662 * 4 * n3
     peak = torch.cuda.max_memory_allocated() - base
     it._graph = None
+    adj = None
+    if with_adjoint:
+        st.restore(init)
+        it.step()
+        torch.cuda.synchronize()
+        adj = config4_adjoint(st, g, base)
     del init, st, it
     torch.cuda.empty_cache()
     return {"workload": f"{g.nx}x{g.ny}x{g.nz} synthetic moist ARW, plain WSM6, dt={spec.dt:g} s, "
@@ -598,7 +605,61 @@ def run_config4(hbm):
             "step_roofline": {"ledger_bytes_per_step": ledger, "achieved_gbs": ledger / (ms / 1e3) / 1e9,
                               "frac": ledger / (ms / 1e3) / 1e9 / hbm},
             "peak_device_bytes": peak, "state_plus_snapshot": "the field table and one copy of it",
-            "nan_points": nan}
+            "nan_points": nan, "adjoint": adj}
+
+
+def config4_adjoint(st, g, base, nsteps=2):
+    """Forward + reverse of ``nsteps`` whole steps (plain WSM6) at the
+    config-4 size under adjoint.rollout with one checkpoint per step (the
+    forward keeps each step's input state; the backward recomputes a step and
+    runs its operators' adjoints), from the state after one step: seconds
+    per step and the peak device memory of the pass (a 1-step pass first as
+    warm-up)."""
+    import torch
+    from pywrf_b200 import adjoint as A
+
+    names = tuple(dict.fromkeys(A.RK_STATE + ("u_1", "w_1", "ph_1", "mu_1", "t_1", "v_1")))
+    data = {k: st[k] for k in dict.fromkeys(A.STEP_DATA + A._Microphysics.data)}
+    keys = (("bxs", "xs"), ("bxe", "xe"), ("bys", "ys"), ("bye", "ye"), ("btxs", "txs"), ("btxe", "txe"),
+            ("btys", "tys"), ("btye", "tye"))
+    bd = {f: {key: st[f"{f}_{n}"] for n, key in keys} for f in ("u", "v", "ph", "t", "mu", "qv")}
+    sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=st.scal["cf1"], cf2=st.scal["cf2"],
+              cf3=st.scal["cf3"], cfn=st.scal["cfn"], cfn1=st.scal["cfn1"], rdx=g.rdx, rdy=g.rdy)
+    bias = torch.zeros_like(st["t"], requires_grad=True)
+    mp = lambda s: A.microphysics(s, data, g.dt, g.rdx, g.rdy)  # noqa: E731
+
+    def one(*xs):
+        n = int(round(float(xs[-1].item())))
+        s = A.step(dict(zip(names, xs[:-1])), data, bd, g.dt * n, dt=g.dt, soundsteps=g.soundsteps,
+                   microphysics=mp, theta_bias=bias, **sc)
+        return tuple(s[k] for k in names) + (xs[-1] + 1,)
+
+    def run(k):
+        bias.grad = None
+        x0 = tuple(st[k2].detach().clone() for k2 in names) + (torch.tensor(2.0, device=st["u"].device),)
+        outs = A.rollout(one, x0, k, every=1)
+        o = dict(zip(names, outs))
+        ((o["t"][:10].double() ** 2).mean() + (o["moist"][1][:10].double() ** 2).mean()).backward()
+
+    try:
+        run(1)
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run(nsteps)
+        e1.record()
+        torch.cuda.synchronize()
+    except torch.cuda.OutOfMemoryError as e:  # reported, not fatal to the bench
+        torch.cuda.empty_cache()
+        return {"unavailable": f"out of device memory: {str(e).splitlines()[0]}"}
+    sec = e0.elapsed_time(e1) / 1e3 / nsteps
+    return {"what": f"{nsteps} whole steps (plain WSM6) forward and reverse under rollout, one checkpoint per "
+                    "step, theta-bias gradient of a lowest-10-level loss",
+            "seconds_per_step": sec, "fwd_adj_steps_per_s": 1.0 / sec,
+            "peak_device_bytes": torch.cuda.max_memory_allocated() - base,
+            "surrogate_form": "not composed: the network's reverse is built for its training, not wired into "
+                              "the differentiable step"}
 
 
 def hydrometeor_budget(st, g):

@@ -4,7 +4,7 @@ tests/golden/make_golden.py from the unmodified reference step).
 An fp64 oracle must reproduce the fp64 reference to rounding (1e-10 relative
 L2); the fp32 oracle must stay within the reference's own fp32 error (its
 fp32 run against its fp64 run), so that the oracle can stand in for the
-reference when the CUDA kernels are judged.
+reference when the CUDA kernels are checked.
 """
 from __future__ import annotations
 
