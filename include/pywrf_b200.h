@@ -341,13 +341,22 @@ int wrf_microphysics_adj_work(const WrfGrid* g, size_t* floats);
  * phb, mu, muts, rdnw), post the same fields after the block; sbar the
  * cotangents of the outputs t, moist, al, p and h_diabatic, rewritten to
  * those of the inputs, while ph, mu, muts, alb and pb accumulate.  The
- * equation of state is reversed exactly; prep + WSM6 + finish by
- * forward-mode tangents of a per-column restatement of the scheme (the
- * derivative of the branch taken), assembled into the reverse product
- * column by column.  values (optional: t, moist, h_diabatic) receives that
- * restatement's own outputs, for checking it against the forward. */
+ * equation of state is reversed exactly; prep + WSM6 + finish by reverse
+ * mode over a per-column restatement of the scheme (the derivative of the
+ * branch taken): each column runs once on taped scalars and one reverse
+ * sweep of its tape gives its inputs' cotangents; a column whose tape
+ * outgrows the capacity takes forward-mode tangents of the same
+ * restatement instead.  values (optional: t, moist, h_diabatic) receives
+ * that restatement's own outputs, for checking it against the forward. */
 int wrf_microphysics_adj(const WrfGrid* g, const WrfState* s, const WrfState* post, const WrfState* sbar,
                          float* work, size_t work_floats, const WrfState* values, void* stream);
+/* The tape capacity of wrf_microphysics_adj in entries per column, for the
+ * whole library (0 restores the default, 640 entries per level plus the
+ * inputs, at most 65535); *previous (optional) receives the setting it
+ * replaces.  A capacity below the column's input count sends every column
+ * to the tangents.  Call wrf_microphysics_adj_work again after changing
+ * it. */
+int wrf_set_microphysics_tape_capacity(int entries, int* previous);
 /* wrf_dynamics.py:4124-4164 calc_p_rho_phi on the state table: al and p on
  * the mass points below the top level from ph, t, qv (moist slot 1), alb,
  * pb, mu, muts, rdnw; NaN in p is counted in the status words. */

@@ -179,6 +179,8 @@ def lib() -> ctypes.CDLL:
     L.wrf_microphysics_adj_work.argtypes = [ctypes.POINTER(WrfGridC), ctypes.POINTER(ctypes.c_size_t)]
     L.wrf_microphysics_adj.restype = ip
     L.wrf_microphysics_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, vp, vp, ctypes.c_size_t, vp, vp]
+    L.wrf_set_microphysics_tape_capacity.restype = ip
+    L.wrf_set_microphysics_tape_capacity.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.wrf_calc_p_rho_phi.restype = ip
     L.wrf_calc_p_rho_phi.argtypes = [ctypes.POINTER(WrfGridC), vp, vp]
     L.wrf_moist_update.restype = ip

@@ -1,24 +1,32 @@
 // Adjoint of the step's microphysics (moist_physics_prep_em, WSM6 and
-// moist_physics_finish_em: wrf_physics.py:27-91, 137-1214, 2106-2137) by
-// forward-mode tangents.
+// moist_physics_finish_em: wrf_physics.py:27-91, 137-1214, 2106-2137).
 //
 // Every output of the block in a column (theta, qv .. qg, h_diabatic) is a
 // function of that column's inputs only (t, qv .. qg, al, p below the top
 // level and ph on every level; alb, pb and phb are data), so its reverse
-// product is assembled column by column from Jacobian columns: one pass
-// evaluates the column once in Dual<N> arithmetic with N of its inputs
-// seeded, and the cotangent of each seeded input is the dot product of the
-// outputs' cotangents with their N tangents.  ceil(n_inputs / N) passes
-// cover the column.  The column is restated here as plain per-column code
-// (one thread per column, column arrays in a global workspace) in the order
-// of the reference's statements: the instantaneous processes, the source and
-// sink rates with their limiters, the saturation adjustment, and the
-// semi-Lagrangian sedimentation (nislfv_rain_plm / _plm6,
-// wrf_physics.py:1216-1583) with its interface fall speeds, departure cells
-// and overlap remap.  The derivative is that of the branch taken.
+// product is formed column by column, one thread per column.  The column is
+// restated here as plain per-column code templated on its scalar type
+// (column arrays in a global workspace) in the order of the reference's
+// statements: the instantaneous processes, the source and sink rates with
+// their limiters, the saturation adjustment, and the semi-Lagrangian
+// sedimentation (nislfv_rain_plm / _plm6, wrf_physics.py:1216-1583) with its
+// interface fall speeds, departure cells and overlap remap.  The derivative
+// is that of the branch taken.
+//
+// The reverse product is taken in reverse mode: the column runs once on
+// taped scalars (tape.cuh), the outputs' cotangents seed the adjoints of
+// their entries, and one reverse sweep yields every input's cotangent.
+// Columns are taped in chunks that bound the tape's memory.  A column whose
+// tape outgrows the capacity is finished by forward-mode tangents instead:
+// the same code on Dual<N> numbers with N inputs seeded per pass, the
+// cotangent of each seeded input the dot product of the outputs' cotangents
+// with their tangents, ceil(n_inputs / N) passes per column.
 #include "dual.cuh"
 #include "kernels.cuh"
+#include "tape.cuh"
 #include "wsm6_const.cuh"
+
+#include <algorithm>
 
 namespace wrf {
 namespace mpt {
@@ -78,6 +86,7 @@ __device__ __forceinline__ bool live(const Dual<N>& x) {
   for (int n = 0; n < N; ++n) any |= x.d[n] != 0.f;
   return any;
 }
+__device__ __forceinline__ bool live(const Tv& x) { return x.id >= 0; }
 
 template <class T>
 struct Slope3 {
@@ -646,36 +655,141 @@ __device__ void wsm6_column(const Col<T>& C, int km, float delt, bool skip_dead 
   }
 }
 
-// one pass of the tangent over the columns of moist_physics_prep_em's block
-// ([jds+1, jde-1) x [ids+1, ide-1)): the inputs with indices [pass N, pass N
-// + N) of each column are seeded (t, qv, qc, qr, qi, qs, qg, al, p at
-// levels < km as 9 km indices, then ph at levels < km + 1), and their
-// cotangents are formed from the outputs' cotangents yb (theta, qv .. qg,
-// h_diabatic).  Columns outside WSM6's block ([jds+1, jde-2) x [ids+1,
-// ide-2)) only take the prep and finish: their t and q pass through and
-// h_diabatic is set to zero.  vo (when its T is not null, pass 0) receives
-// the outputs' values.
-template <int N>
-__global__ void __launch_bounds__(64) k_mp_tangent(Grid g, S s, S yb, S b, int pass, float dt, Dual<N>* ws,
-                                                   int ncol, S vo, int* quiet) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+// the columns of moist_physics_prep_em's block ([jds+1, jde-1) x [ids+1,
+// ide-1)), numbered row by row; WSM6 runs on [jds+1, jde-2) x [ids+1,
+// ide-2) of them (run), the others only take the prep and finish
+struct ColPos {
+  int c2;
+  bool run;
+};
+__device__ __forceinline__ bool col_pos(const Grid& g, int col, ColPos& o) {
   const int wi = g.ide - 1 - (g.ids + 1), wj = g.jde - 1 - (g.jds + 1);
-  if (col >= ncol || col >= wi * wj) return;
+  if (col >= wi * wj) return false;
   const int j = g.jds + 1 + col / wi, i = g.ids + 1 + col % wi;
-  const bool run = j < g.jde - 2 && i < g.ide - 2;
+  o.c2 = g.i2(j, i);
+  o.run = j < g.jde - 2 && i < g.ide - 2;
+  return true;
+}
+
+// the column's inputs are numbered t, qv, qc, qr, qi, qs, qg, al, p at
+// levels < km (9 km indices: field f at level k is f km + k), then ph at
+// levels < km + 1
+__host__ __device__ __forceinline__ int mp_inputs(const Grid& g) { return 9 * (g.nz - 1) + g.nz; }
+
+// moist_physics_prep_em (wrf_physics.py:27-91): theta, Exner function,
+// temperature, density, pressure and layer depths of the column and its
+// moisture into the column arrays; in(idx, value) makes input idx
+template <class T, class In>
+__device__ void prep_column(const Grid& g, const S& s, const Col<T>& C, int c2, In in) {
   const int km = g.nz - 1;
   const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
-  const int c2 = g.i2(j, i);
-  const int nin = 9 * km + g.nz, j0 = pass * N;
-  if (j0 >= nin) return;
-  if (!run) {
-    if (pass != 0) return;
+  const int slot_of[6] = {A_Q, A_QC, A_QR, A_QI, A_QS, A_QG};
+  for (int k = 0; k < km; ++k) {
+    const size_t p = k * lev + c2;
+    const T tin = in(k, s[WF_T][p]);
+    C(A_TIN, k) = tin;
+    const T th = tin + (float)T0;
+    C(A_TH, k) = th;
+    const T pfull = in(8 * km + k, s[WF_P][p]) + s[WF_PB][p];
+    const T pii = vpow(pfull / (float)P0, F(RCP));
+    C(A_PII, k) = pii;
+    C(A_T, k) = th * pii;
+    C(A_DEN, k) = 1.0f / (in(7 * km + k, s[WF_AL][p]) + s[WF_ALB][p]);
+    C(A_P, k) = pfull;
+    const T zlo = (in(9 * km + k, s[WF_PH][p]) + s[WF_PHB][p]) / (float)G;
+    const T zhi = (in(9 * km + k + 1, s[WF_PH][p + lev]) + s[WF_PHB][p + lev]) / (float)G;
+    C(A_DELZ, k) = zhi - zlo;
+    for (int m = 1; m < 7; ++m) C(slot_of[m - 1], k) = in(m * km + k, s[WF_MOIST][m * n3 + p]);
+  }
+}
+
+// moist_physics_finish_em (wrf_physics.py:2106-2137) at level k: theta's
+// new value replaces A_TIN, h_diabatic replaces A_TH
+template <class T>
+__device__ __forceinline__ void finish_level(const Col<T>& C, int k, float dt) {
+  const T mpten = C(A_T, k) / C(A_PII, k) - C(A_TH, k);
+  C(A_TIN, k) = C(A_TIN, k) + mpten;
+  C(A_TH, k) = mpten / dt;
+}
+
+// the array holding moist species m (1 qv .. 6 qg) in the column
+__device__ __forceinline__ int moist_slot(int m) {
+  const int slot_of[6] = {A_Q, A_QC, A_QR, A_QI, A_QS, A_QG};
+  return slot_of[m - 1];
+}
+
+// a column that takes no process at all: no cloud, rain, ice, snow or
+// graupel at any level, and qv below both saturation mixing ratios
+// everywhere.  Every rate is zero, nothing falls, the saturation adjustment
+// condenses nothing, and its reverse product is theta's and qv's
+// cotangents passed through, zero for the hydrometeors (their results are
+// constants: the zero of the empty sedimentation and the final zeroing of
+// cloud and ice) and for h_diabatic.
+__device__ bool quiet_column(const Grid& g, const S& s, int c2) {
+  const int km = g.nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
+  for (int k = 0; k < km; ++k) {
+    const size_t p = k * lev + c2;
+    for (int m = 2; m < 7; ++m)
+      if (s[WF_MOIST][m * n3 + p] > 0.f) return false;
+    const float th = s[WF_T][p] + (float)T0;
+    const float pfull = s[WF_P][p] + s[WF_PB][p];
+    const float t = th * wpow(pfull / (float)P0, F(RCP));
+    float qs0, qs1;
+    fpvs(t, pfull, qs0, qs1);
+    const float qv = s[WF_MOIST][n3 + p];
+    if (!(qv < qs0 && qv < qs1)) return false;
+  }
+  return true;
+}
+
+// the cotangent v of input idx into the cotangent table: assigned for t and
+// the moisture (the block overwrites them), added for al, p and ph
+__device__ __forceinline__ void put_input_cot(const Grid& g, const S& b, int c2, int idx, float v) {
+  const int km = g.nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
+  if (idx >= 9 * km) {
+    b[WF_PH][(size_t)(idx - 9 * km) * lev + c2] += v;
+    return;
+  }
+  const int f = idx / km, k = idx - f * km;
+  const size_t p = k * lev + c2;
+  if (f == 0) b[WF_T][p] = v;
+  else if (f < 7) b[WF_MOIST][f * n3 + p] = v;
+  else if (f == 7) b[WF_AL][p] += v;
+  else b[WF_P][p] += v;
+}
+
+// the taped forward over the columns [c0, c0 + nc) (lane l of the launch
+// takes column c0 + l; tape and column arrays interleaved with the
+// context's stride): the column runs once on taped scalars and the
+// outputs' cotangents yb (theta, qv .. qg, h_diabatic) seed their entries'
+// adjoints.  Columns outside WSM6's block pass t and q through and set
+// h_diabatic to zero; quiet columns pass theta's and qv's cotangents
+// through (unless the values are wanted); both are done here.  vo (when
+// its T is not null) receives the outputs' values.  used[col] receives the
+// entries the column's tape took (0 when none) and done[col] whether its
+// cotangents are (or, after k_mp_tape_rev, will be) written: not when the
+// tape outgrew the capacity.
+__global__ void __launch_bounds__(kTapeBlock) k_mp_tape(Grid g, S s, S yb, S b, float dt, Tv* ws, TapeCtx tc,
+                                                        int c0, int nc, S vo, int* done, int* used) {
+  if (threadIdx.x == 0) g_tape = tc;
+  __syncthreads();
+  const int lane = tape_lane(), col = c0 + lane;
+  ColPos cp;
+  if (lane >= nc || !col_pos(g, col, cp)) return;
+  const int km = g.nz - 1, c2 = cp.c2;
+  const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
+  const bool want = vo[WF_T] != nullptr;
+  used[col] = 0;
+  done[col] = 1;
+  if (!cp.run) {
     for (int k = 0; k < km; ++k) {
       const size_t p = k * lev + c2;
       b[WF_T][p] = yb[WF_T][p];
       for (int m = 1; m < 7; ++m) b[WF_MOIST][m * n3 + p] = yb[WF_MOIST][m * n3 + p];
       b[WF_H_DIABATIC][p] = 0.f;
-      if (vo[WF_T]) {
+      if (want) {
         vo[WF_T][p] = s[WF_T][p];
         for (int m = 1; m < 7; ++m) vo[WF_MOIST][m * n3 + p] = s[WF_MOIST][m * n3 + p];
         vo[WF_H_DIABATIC][p] = 0.f;
@@ -683,127 +797,164 @@ __global__ void __launch_bounds__(64) k_mp_tangent(Grid g, S s, S yb, S b, int p
     }
     return;
   }
-  // A quiet column -- no cloud, rain, ice, snow or graupel at any level, and
-  // qv below both saturation mixing ratios everywhere -- takes no
-  // process at all: every rate is zero, nothing falls, the saturation
-  // adjustment condenses nothing, and its reverse product is theta's and
-  // qv's cotangents passed through, zero for the hydrometeors (their
-  // results are constants: the zero of the empty sedimentation and the
-  // final zeroing of cloud and ice) and for h_diabatic.  Found at pass 0
-  // on the value path (unless the values are wanted), remembered per column.
-  if (pass == 0) {
-    bool q0 = !vo[WF_T];
-    for (int k = 0; k < km && q0; ++k) {
+  if (!want && quiet_column(g, s, c2)) {
+    for (int k = 0; k < km; ++k) {
       const size_t p = k * lev + c2;
-      for (int m = 2; m < 7; ++m) q0 = q0 && !(s[WF_MOIST][m * n3 + p] > 0.f);
-      const float th = s[WF_T][p] + (float)T0;
-      const float pfull = s[WF_P][p] + s[WF_PB][p];
-      const float t = th * wpow(pfull / (float)P0, F(RCP));
-      float qs0, qs1;
-      fpvs(t, pfull, qs0, qs1);
-      const float qv = s[WF_MOIST][n3 + p];
-      q0 = q0 && qv < qs0 && qv < qs1;
+      b[WF_T][p] = yb[WF_T][p];
+      b[WF_MOIST][n3 + p] = yb[WF_MOIST][n3 + p];
+      for (int m = 2; m < 7; ++m) b[WF_MOIST][m * n3 + p] = 0.f;
+      b[WF_H_DIABATIC][p] = 0.f;
     }
-    quiet[col] = q0 ? 1 : 0;
-    if (q0) {
-      for (int k = 0; k < km; ++k) {
-        const size_t p = k * lev + c2;
-        b[WF_T][p] = yb[WF_T][p];
-        b[WF_MOIST][n3 + p] = yb[WF_MOIST][n3 + p];
-        for (int m = 2; m < 7; ++m) b[WF_MOIST][m * n3 + p] = 0.f;
-        b[WF_H_DIABATIC][p] = 0.f;
-      }
-      return;
-    }
-  } else if (quiet[col]) {
     return;
   }
+  const Col<Tv> C{ws + lane, tc.stride, km + 1};
+  tape_reserve(mp_inputs(g));
+  prep_column(g, s, C, c2, [](int idx, float v) { return Tv{v, idx}; });
+  wsm6_column(C, km, dt);
+  for (int k = 0; k < km; ++k) finish_level(C, k, dt);
+  const int n = g_tape_n[threadIdx.x];
+  used[col] = n;
+  if (want)
+    for (int k = 0; k < km; ++k) {
+      const size_t p = k * lev + c2;
+      vo[WF_T][p] = C(A_TIN, k).v;
+      vo[WF_H_DIABATIC][p] = C(A_TH, k).v;
+      for (int m = 1; m < 7; ++m) vo[WF_MOIST][m * n3 + p] = C(moist_slot(m), k).v;
+    }
+  for (int k = 0; k < km; ++k) b[WF_H_DIABATIC][k * lev + c2] = 0.f;
+  if (n > tc.cap) {
+    done[col] = 0;
+    return;
+  }
+  const size_t st = tc.stride;
+  auto seed = [&](const Tv& y, float w) {
+    if (y.id >= 0 && w != 0.f) tc.adj[(size_t)y.id * st + lane] += w;
+  };
+  for (int k = 0; k < km; ++k) {
+    const size_t p = k * lev + c2;
+    seed(C(A_TIN, k), yb[WF_T][p]);
+    seed(C(A_TH, k), yb[WF_H_DIABATIC][p]);
+    for (int m = 1; m < 7; ++m) seed(C(moist_slot(m), k), yb[WF_MOIST][m * n3 + p]);
+  }
+}
+
+// the reverse sweep of the tapes k_mp_tape left (same chunk and lanes):
+// the inputs' cotangents from the adjoints of entries [0, n_inputs)
+__global__ void __launch_bounds__(128) k_mp_tape_rev(Grid g, S b, TapeCtx tc, int c0, int nc, const int* used) {
+  const int lane = blockIdx.x * blockDim.x + threadIdx.x, col = c0 + lane;
+  ColPos cp;
+  if (lane >= nc || !col_pos(g, col, cp)) return;
+  const int n = used[col];
+  if (n == 0 || n > tc.cap) return;
+  const int nin = mp_inputs(g);
+  tape_sweep<8>(tc, lane, nin, n);
+  for (int idx = 0; idx < nin; ++idx) put_input_cot(g, b, cp.c2, idx, __ldcg(tc.adj + (size_t)idx * tc.stride + lane));
+}
+
+// one pass of forward-mode tangents over the columns that the tape left
+// undone: the inputs with indices [pass N, pass N + N) of each column are
+// seeded and their cotangents formed from the outputs' cotangents yb
+template <int N>
+__global__ void __launch_bounds__(64) k_mp_tangent(Grid g, S s, S yb, S b, int pass, float dt, Dual<N>* ws,
+                                                   int ncol, const int* done) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  ColPos cp;
+  if (col >= ncol || !col_pos(g, col, cp) || done[col] || !cp.run) return;
+  const int nin = mp_inputs(g), j0 = pass * N;
+  if (j0 >= nin) return;
+  const int km = g.nz - 1, c2 = cp.c2;
+  const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
   using T = Dual<N>;
   const Col<T> C{ws + col, ncol, km + 1};
-  auto seed = [&](int idx, float v) {
+  prep_column(g, s, C, c2, [&](int idx, float v) {
     T x = dconst<N>(v);
     const int d = idx - j0;
     if (d >= 0 && d < N) x.d[d] = 1.f;
     return x;
-  };
-  // moist_physics_prep_em: theta, Exner function, temperature, density,
-  // pressure and layer depths of the column
-  const int slot_of[6] = {A_Q, A_QC, A_QR, A_QI, A_QS, A_QG};
-  for (int k = 0; k < km; ++k) {
-    const size_t p = k * lev + c2;
-    const T tin = seed(k, s[WF_T][p]);
-    C(A_TIN, k) = tin;
-    const T th = tin + (float)T0;
-    C(A_TH, k) = th;
-    const T pfull = seed(8 * km + k, s[WF_P][p]) + s[WF_PB][p];
-    const T pii = vpow(pfull / (float)P0, F(RCP));
-    C(A_PII, k) = pii;
-    C(A_T, k) = th * pii;
-    C(A_DEN, k) = 1.0f / (seed(7 * km + k, s[WF_AL][p]) + s[WF_ALB][p]);
-    C(A_P, k) = pfull;
-    const T zlo = (seed(9 * km + k, s[WF_PH][p]) + s[WF_PHB][p]) / (float)G;
-    const T zhi = (seed(9 * km + k + 1, s[WF_PH][p + lev]) + s[WF_PHB][p + lev]) / (float)G;
-    C(A_DELZ, k) = zhi - zlo;
-    for (int m = 1; m < 7; ++m) C(slot_of[m - 1], k) = seed(m * km + k, s[WF_MOIST][m * n3 + p]);
-  }
-  // (pass 0 with values wanted runs every level for its values)
-  wsm6_column(C, km, dt, !(vo[WF_T] && pass == 0));
-  // moist_physics_finish_em and the reverse products
+  });
+  wsm6_column(C, km, dt, true);
   float acc[N];
 #pragma unroll
   for (int n = 0; n < N; ++n) acc[n] = 0.f;
   for (int k = 0; k < km; ++k) {
+    finish_level(C, k, dt);
     const size_t p = k * lev + c2;
-    const T mpten = C(A_T, k) / C(A_PII, k) - C(A_TH, k);
-    const T tnew = C(A_TIN, k) + mpten;
-    const T h = mpten / dt;
+    const T tnew = C(A_TIN, k), h = C(A_TH, k);
     const float yt = yb[WF_T][p], yh = yb[WF_H_DIABATIC][p];
 #pragma unroll
     for (int n = 0; n < N; ++n) acc[n] += yt * tnew.d[n] + yh * h.d[n];
     for (int m = 1; m < 7; ++m) {
-      const T qo = C(slot_of[m - 1], k);
+      const T qo = C(moist_slot(m), k);
       const float y = yb[WF_MOIST][m * n3 + p];
 #pragma unroll
       for (int n = 0; n < N; ++n) acc[n] += y * qo.d[n];
-      if (vo[WF_T] && pass == 0) vo[WF_MOIST][m * n3 + p] = qo.v;
     }
-    if (vo[WF_T] && pass == 0) {
-      vo[WF_T][p] = tnew.v;
-      vo[WF_H_DIABATIC][p] = h.v;
-    }
-    if (pass == 0) b[WF_H_DIABATIC][p] = 0.f;
   }
 #pragma unroll
-  for (int n = 0; n < N; ++n) {
-    const int idx = j0 + n;
-    if (idx >= nin) break;
-    if (idx >= 9 * km) {
-      b[WF_PH][(size_t)(idx - 9 * km) * lev + c2] += acc[n];
-      continue;
-    }
-    const int f = idx / km, k = idx - f * km;
-    const size_t p = k * lev + c2;
-    if (f == 0) b[WF_T][p] = acc[n];
-    else if (f < 7) b[WF_MOIST][f * n3 + p] = acc[n];
-    else if (f == 7) b[WF_AL][p] += acc[n];
-    else b[WF_P][p] += acc[n];
-  }
+  for (int n = 0; n < N; ++n)
+    if (j0 + n < nin) put_input_cot(g, b, c2, j0 + n, acc[n]);
 }
 
 }  // namespace mpt
 
-constexpr int kMpDirections = 8;
+namespace {
 
-size_t microphysics_adj_work_floats(const Grid& g) {
-  const size_t ncol = (size_t)(g.ide - 1 - (g.ids + 1)) * (g.jde - 1 - (g.jds + 1));
-  return 9 * g.n3() + (size_t)mpt::A_COUNT * g.nz * ncol * (kMpDirections + 1) + ncol;
+constexpr int kMpDirections = 8;
+// entries a column's tape may take per level by default, and the memory
+// the tapes of one chunk of columns may take
+constexpr int kTapeEntriesPerLevel = 640;
+constexpr size_t kTapeChunkBytes = size_t(16) << 30;
+// the capacity set through set_microphysics_tape_capacity (0: default)
+int g_tape_capacity = 0;
+
+// the adjoint's workspace, in floats: the outputs' cotangents (9 n3), the
+// per-column done flags and tape sizes, then one region shared by the
+// chunk's tapes and column arrays and (afterwards) the tangent passes'
+// column arrays
+struct MpAdjWork {
+  size_t done, used, region, tangent, dd, ab, adj, cols, total;
+  int ncol, width, cap;
+};
+
+MpAdjWork mp_adj_work(const Grid& g) {
+  MpAdjWork w;
+  const int km = g.nz - 1;
+  w.ncol = (g.ide - 1 - (g.ids + 1)) * (g.jde - 1 - (g.jds + 1));
+  w.cap = g_tape_capacity > 0 ? std::min(kTapeMaxEntries, g_tape_capacity)
+                              : std::min(kTapeMaxEntries, kTapeEntriesPerLevel * km + mpt::mp_inputs(g));
+  const size_t per_col = (size_t)w.cap * 16 + (size_t)mpt::A_COUNT * (km + 1) * 8;
+  const size_t fit = std::max<size_t>(64, kTapeChunkBytes / per_col / 64 * 64);
+  w.width = (int)std::min<size_t>(fit, ((size_t)w.ncol + 63) / 64 * 64);
+  w.done = 9 * g.n3();
+  w.used = w.done + w.ncol;
+  w.region = (w.used + w.ncol + 3) / 4 * 4;
+  w.tangent = (size_t)mpt::A_COUNT * g.nz * w.ncol * (kMpDirections + 1);
+  const size_t ent = (size_t)w.cap * w.width;
+  w.dd = w.region;
+  w.ab = w.dd + 2 * ent;
+  w.adj = w.ab + ent;
+  w.cols = w.adj + ent;
+  const size_t tape = 4 * ent + 2 * (size_t)mpt::A_COUNT * (km + 1) * w.width;
+  w.total = w.region + std::max(w.tangent, tape);
+  return w;
+}
+
+}  // namespace
+
+size_t microphysics_adj_work_floats(const Grid& g) { return mp_adj_work(g).total; }
+
+int set_microphysics_tape_capacity(int entries) {
+  const int prev = g_tape_capacity;
+  g_tape_capacity = entries;
+  return prev;
 }
 
 int launch_physics_adj(const Grid& g, const S& s, const S& post, const S& b, float* work, float dt, cudaStream_t st,
                        const S* values) {
   const size_t n3 = g.n3();
+  const MpAdjWork w = mp_adj_work(g);
   int n = launch_eos_adj(g, post, b, st);
-  // the outputs' cotangents, kept while the passes write the inputs'
+  // the outputs' cotangents, kept while the kernels write the inputs'
   S yb{};
   yb.f[WF_T] = work;
   yb.f[WF_MOIST] = work + n3;
@@ -811,14 +962,29 @@ int launch_physics_adj(const Grid& g, const S& s, const S& post, const S& b, flo
   cudaMemcpyAsync(yb.f[WF_T], b[WF_T], n3 * sizeof(float), cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(yb.f[WF_MOIST], b[WF_MOIST], 7 * n3 * sizeof(float), cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(yb.f[WF_H_DIABATIC], b[WF_H_DIABATIC], n3 * sizeof(float), cudaMemcpyDeviceToDevice, st);
-  auto* ws = reinterpret_cast<Dual<kMpDirections>*>(work + 9 * n3);
-  const int km = g.nz - 1, ncol = (g.ide - 1 - (g.ids + 1)) * (g.jde - 1 - (g.jds + 1));
-  int* quiet = reinterpret_cast<int*>(work + 9 * n3 + (size_t)mpt::A_COUNT * g.nz * ncol * (kMpDirections + 1));
-  const int nin = 9 * km + g.nz, passes = (nin + kMpDirections - 1) / kMpDirections;
+  int* done = reinterpret_cast<int*>(work + w.done);
+  int* used = reinterpret_cast<int*>(work + w.used);
   S vo{};
   if (values) vo = *values;
+  TapeCtx tc;
+  tc.dd = reinterpret_cast<float2*>(work + w.dd);
+  tc.ab = reinterpret_cast<unsigned*>(work + w.ab);
+  tc.adj = work + w.adj;
+  tc.stride = w.width;
+  tc.cap = w.cap;
+  auto* cols = reinterpret_cast<Tv*>(work + w.cols);
+  for (int c0 = 0; c0 < w.ncol; c0 += w.width) {
+    const int nc = std::min(w.width, w.ncol - c0);
+    mpt::k_mp_tape<<<(nc + kTapeBlock - 1) / kTapeBlock, kTapeBlock, 0, st>>>(g, s, yb, b, dt, cols, tc, c0, nc, vo,
+                                                                               done, used);
+    mpt::k_mp_tape_rev<<<(nc + 127) / 128, 128, 0, st>>>(g, b, tc, c0, nc, used);
+    n += 2;
+  }
+  // the columns whose tape outgrew the capacity, by tangent passes
+  auto* ws = reinterpret_cast<Dual<kMpDirections>*>(work + w.region);
+  const int passes = (mpt::mp_inputs(g) + kMpDirections - 1) / kMpDirections;
   for (int pass = 0; pass < passes; ++pass) {
-    mpt::k_mp_tangent<kMpDirections><<<(ncol + 63) / 64, 64, 0, st>>>(g, s, yb, b, pass, dt, ws, ncol, vo, quiet);
+    mpt::k_mp_tangent<kMpDirections><<<(w.ncol + 63) / 64, 64, 0, st>>>(g, s, yb, b, pass, dt, ws, w.ncol, done);
     ++n;
   }
   return n;

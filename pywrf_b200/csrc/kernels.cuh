@@ -156,11 +156,15 @@ int launch_moist_adj(const Grid& g, const S& s, const S& b, int rk_step, float d
 // calc_p_rho_phi's reverse with the state's own qv (k_adjoint_moist.cu)
 int launch_eos_adj(const Grid& g, const S& s, const S& b, cudaStream_t st);
 // the microphysics block's reverse (the equation of state after it, then
-// prep + WSM6 + finish by forward-mode tangents; k_adjoint_wsm6.cu): s holds
-// the block's inputs, post the state after it; work holds
+// prep + WSM6 + finish by a per-column tape, forward-mode tangents for the
+// columns whose tape outgrows its capacity; k_adjoint_wsm6.cu): s holds the
+// block's inputs, post the state after it; work holds
 // microphysics_adj_work_floats(g) floats; values (optional) receives the
-// tangent code's own outputs
+// taped code's own outputs
 size_t microphysics_adj_work_floats(const Grid& g);
+// the tape capacity in entries per column (0: the default, which grows with
+// the levels); returns the previous setting
+int set_microphysics_tape_capacity(int entries);
 int launch_physics_adj(const Grid& g, const S& s, const S& post, const S& b, float* work, float dt, cudaStream_t st,
                        const S* values);
 int launch_bdy_final(const Grid& g, const S& s, cudaStream_t st);

@@ -1169,6 +1169,13 @@ int wrf_microphysics_adj(const WrfGrid* gin, const WrfState* sin, const WrfState
   return check_launch("microphysics_adj");
 }
 
+int wrf_set_microphysics_tape_capacity(int entries, int* previous) {
+  if (entries < 0) return fail(WRF_EINVAL, "microphysics tape capacity: negative");
+  const int prev = set_microphysics_tape_capacity(entries);
+  if (previous) *previous = prev;
+  return WRF_OK;
+}
+
 int wrf_calc_p_rho_phi(const WrfGrid* gin, const WrfState* sin, void* stream) {
   Grid g;
   int rc = make_grid(gin, g);

@@ -1216,7 +1216,7 @@ MP_OUT = ("t", "moist", "al", "p", "h_diabatic")
 def test_microphysics_adjoint_against_the_oracle():
     """pywrf_b200.adjoint.microphysics (the step's microphysics forward and
     its reverse: the equation of state's exact reverse, then prep + WSM6 +
-    finish by forward-mode tangents of a per-column restatement of the
+    finish by reverse mode over a per-column tape of a restatement of the
     scheme) from the small case's state before the microphysics of step 2:
     the outputs against the float64 oracle (3x the float32 oracle's own
     error plus 2e-6), the restatement's own outputs against the forward's,
@@ -1262,7 +1262,7 @@ def test_microphysics_adjoint_against_the_oracle():
         if not err <= 3.0 * floor + 2e-6:
             bad.append((k, err, floor))
     assert not bad, bad
-    # the tangent code's own outputs (its value path) against the forward's
+    # the taped code's own outputs (its value path) against the forward's
     from pywrf_b200 import _native as N
 
     cg = adjoint.scalar_grid(st["t"].shape, g.rdx, g.rdy)
@@ -1307,6 +1307,82 @@ def test_microphysics_adjoint_against_the_oracle():
         if not abs(an - fd) <= 2e-3 * abs(fd) + 1e-5 * scale:
             bad.append((name, an, fd, scale))
     assert not bad, bad
+
+
+def _microphysics_state_before_step2():
+    import copy
+
+    from helpers import SMALL
+    from oracle.model import OracleModel
+    from pywrf_b200 import synthetic
+
+    spec = synthetic.CaseSpec(**SMALL)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+    snap = {}
+
+    def probe(name, m):
+        if name == "s3.moist" and not snap:
+            snap.update(copy.deepcopy(m.st))
+
+    m = OracleModel(g, inputs, bdy, np.float64)
+    m.run(1)
+    m.step(2, probe)
+    return g, snap
+
+
+def test_microphysics_adjoint_tape_and_tangent_columns_agree():
+    """wrf_microphysics_adj with the tape capacity at its default (every
+    column taped), at 1 (every column by forward-mode tangents) and at 4500
+    and 6500 entries (on this 16-level case, whose columns take 3800 to
+    8600 entries, the columns whose tape outgrows the capacity go to the
+    tangents and the rest are taped, in one call): the input cotangents agree to float32 summation order (relative
+    L2 1e-5 per field), and the setting is restored."""
+    from pywrf_b200 import _native as N
+
+    g, snap = _microphysics_state_before_step2()
+    names = adjoint._Microphysics.fields
+    st = {k: _cuda(snap[k]) for k in names}
+    data = {k: _cuda(snap[k]) for k in adjoint._Microphysics.data}
+    out = adjoint.microphysics(st, data, g.dt, g.rdx, g.rdy)
+    cg = adjoint.scalar_grid(st["t"].shape, g.rdx, g.rdy)
+    cg.dt = float(g.dt)
+    tab = adjoint._table({**st, **data})
+    post = adjoint._table({**st, **data, **{k: out[k].detach() for k in ("t", "moist", "al", "p")}})
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    seeds = {k: torch.randn(st[k].shape, generator=gen, device="cuda") for k in MP_OUT}
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def reverse(capacity):
+        prev = ctypes.c_int(-1)
+        N.check(N.lib().wrf_set_microphysics_tape_capacity(capacity, ctypes.byref(prev)), "capacity")
+        try:
+            bars = {k: torch.zeros_like(st[k]) for k in ("t", "moist", "al", "p", "ph", "mu", "muts", "h_diabatic")}
+            bars.update({k: torch.zeros_like(st["t"]) for k in ("alb", "pb")})
+            for k in MP_OUT:
+                bars[k].copy_(seeds[k])
+            n = ctypes.c_size_t(0)
+            N.check(N.lib().wrf_microphysics_adj_work(ctypes.byref(cg), ctypes.byref(n)), "work")
+            work = torch.empty(int(n.value), dtype=torch.float32, device="cuda")
+            N.check(N.lib().wrf_microphysics_adj(ctypes.byref(cg), tab, post, adjoint._table(bars),
+                                                 ctypes.c_void_p(work.data_ptr()), n, None, stream), "adj")
+            torch.cuda.synchronize()
+            return {k: v.double().cpu().numpy() for k, v in bars.items()}
+        finally:
+            back = ctypes.c_int(-1)
+            N.check(N.lib().wrf_set_microphysics_tape_capacity(prev.value, ctypes.byref(back)), "restore")
+            assert back.value == capacity
+
+    taped = reverse(0)
+    bad = []
+    for cap in (1, 4500, 6500):
+        other = reverse(cap)
+        for k in ("t", "moist", "al", "p", "ph", "mu", "muts"):
+            e = rel_l2(other[k], taped[k])
+            if not e <= 1e-5:
+                bad.append((k, cap, e))
+    assert not bad, bad
+    assert float(np.abs(taped["moist"][3]).max()) > 0.0
 
 
 def test_theta_bias_gradient_of_two_steps_against_the_reference():
