@@ -427,7 +427,7 @@ def run_ours(a):
 
 def run_adjoint_step(st, it, fused_step_ms, reps=3):
     """Forward + reverse pass of one whole step -- the three RK stages, the
-    microphysics (WSM6's reverse by forward-mode tangents) and the
+    microphysics (WSM6's reverse over a per-column tape) and the
     end-of-step boundaries -- composed from the hand-written operator
     adjoints (pywrf_b200.adjoint.step) on the 240x240x41 state after one
     step, timed with CUDA events (2 warm-up passes): the fwd+adj steps per

@@ -54,7 +54,7 @@ operators keeps no tape of the forward's intermediates.
 * :func:`addtend`, :class:`SpecBdytend`, the moisture update
   (rk_update_scalar, flow_dep_bdy, calc_p_rho_phi), :func:`microphysics`
   (moist_physics_prep_em, WSM6, moist_physics_finish_em, calc_p_rho_phi;
-  WSM6's reverse by forward-mode tangents of a per-column restatement) and
+  WSM6's reverse in reverse mode over a per-column tape of a restatement) and
   :func:`step_end` (halo copies, spec_bdy_final, set_w_surface).
 * Composed in the reference's order: :func:`acoustic_substep`,
   :func:`acoustic_stage`, :func:`dynamics_stage`, :func:`moist_stage`,
@@ -1494,8 +1494,11 @@ class _Microphysics:
 def microphysics(st: dict, data: dict, dt: float, rdx, rdy) -> dict:
     """Differentiable microphysics of the step (pywrf/solver.py:1714-1766):
     returns ``st`` with t, moist, al, p and h_diabatic replaced.  Its reverse
-    is the equation of state's exact reverse, then prep + WSM6 + finish by
-    forward-mode tangents of a per-column restatement of the scheme."""
+    is the equation of state's exact reverse, then prep + WSM6 + finish in
+    reverse mode: each column of a restatement of the scheme runs once on
+    taped scalars and one reverse sweep of its tape gives its inputs'
+    cotangents (forward-mode tangents for a column whose tape outgrows the
+    capacity)."""
     op = _Microphysics(st["t"])
     cg = scalar_grid(st["t"].shape, rdx, rdy)
     cg.dt = float(dt)

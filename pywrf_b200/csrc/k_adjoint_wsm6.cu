@@ -826,9 +826,8 @@ __global__ void __launch_bounds__(kTapeBlock) k_mp_tape(Grid g, S s, S yb, S b, 
     done[col] = 0;
     return;
   }
-  const size_t st = tc.stride;
   auto seed = [&](const Tv& y, float w) {
-    if (y.id >= 0 && w != 0.f) tc.adj[(size_t)y.id * st + lane] += w;
+    if (y.id >= 0 && w != 0.f) *tc.adj(y.id, lane) += w;
   };
   for (int k = 0; k < km; ++k) {
     const size_t p = k * lev + c2;
@@ -840,15 +839,18 @@ __global__ void __launch_bounds__(kTapeBlock) k_mp_tape(Grid g, S s, S yb, S b, 
 
 // the reverse sweep of the tapes k_mp_tape left (same chunk and lanes):
 // the inputs' cotangents from the adjoints of entries [0, n_inputs)
-__global__ void __launch_bounds__(128) k_mp_tape_rev(Grid g, S b, TapeCtx tc, int c0, int nc, const int* used) {
+constexpr int kSweepBlock = 128, kSweepWindow = 16, kSweepRing = 64;
+__global__ void __launch_bounds__(kSweepBlock) k_mp_tape_rev(Grid g, S b, TapeCtx tc, int c0, int nc,
+                                                             const int* used) {
+  __shared__ float acc[kSweepRing * kSweepBlock];
   const int lane = blockIdx.x * blockDim.x + threadIdx.x, col = c0 + lane;
   ColPos cp;
   if (lane >= nc || !col_pos(g, col, cp)) return;
   const int n = used[col];
   if (n == 0 || n > tc.cap) return;
   const int nin = mp_inputs(g);
-  tape_sweep<8>(tc, lane, nin, n);
-  for (int idx = 0; idx < nin; ++idx) put_input_cot(g, b, cp.c2, idx, __ldcg(tc.adj + (size_t)idx * tc.stride + lane));
+  tape_sweep<kSweepWindow, kSweepRing, kSweepBlock>(tc, lane, nin, n, acc);
+  for (int idx = 0; idx < nin; ++idx) put_input_cot(g, b, cp.c2, idx, __ldcg(tc.adj(idx, lane)));
 }
 
 // one pass of forward-mode tangents over the columns that the tape left
@@ -912,7 +914,7 @@ int g_tape_capacity = 0;
 // chunk's tapes and column arrays and (afterwards) the tangent passes'
 // column arrays
 struct MpAdjWork {
-  size_t done, used, region, tangent, dd, ab, adj, cols, total;
+  size_t done, used, region, tangent, rec, cols, total;
   int ncol, width, cap;
 };
 
@@ -930,10 +932,8 @@ MpAdjWork mp_adj_work(const Grid& g) {
   w.region = (w.used + w.ncol + 3) / 4 * 4;
   w.tangent = (size_t)mpt::A_COUNT * g.nz * w.ncol * (kMpDirections + 1);
   const size_t ent = (size_t)w.cap * w.width;
-  w.dd = w.region;
-  w.ab = w.dd + 2 * ent;
-  w.adj = w.ab + ent;
-  w.cols = w.adj + ent;
+  w.rec = w.region;
+  w.cols = w.rec + 4 * ent;
   const size_t tape = 4 * ent + 2 * (size_t)mpt::A_COUNT * (km + 1) * w.width;
   w.total = w.region + std::max(w.tangent, tape);
   return w;
@@ -967,9 +967,7 @@ int launch_physics_adj(const Grid& g, const S& s, const S& post, const S& b, flo
   S vo{};
   if (values) vo = *values;
   TapeCtx tc;
-  tc.dd = reinterpret_cast<float2*>(work + w.dd);
-  tc.ab = reinterpret_cast<unsigned*>(work + w.ab);
-  tc.adj = work + w.adj;
+  tc.rec = reinterpret_cast<TapeRec*>(work + w.rec);
   tc.stride = w.width;
   tc.cap = w.cap;
   auto* cols = reinterpret_cast<Tv*>(work + w.cols);
@@ -977,7 +975,8 @@ int launch_physics_adj(const Grid& g, const S& s, const S& post, const S& b, flo
     const int nc = std::min(w.width, w.ncol - c0);
     mpt::k_mp_tape<<<(nc + kTapeBlock - 1) / kTapeBlock, kTapeBlock, 0, st>>>(g, s, yb, b, dt, cols, tc, c0, nc, vo,
                                                                                done, used);
-    mpt::k_mp_tape_rev<<<(nc + 127) / 128, 128, 0, st>>>(g, b, tc, c0, nc, used);
+    mpt::k_mp_tape_rev<<<(nc + mpt::kSweepBlock - 1) / mpt::kSweepBlock, mpt::kSweepBlock, 0, st>>>(g, b, tc, c0, nc,
+                                                                                                    used);
     n += 2;
   }
   // the columns whose tape outgrew the capacity, by tangent passes

@@ -13,13 +13,17 @@
 //
 // A thread's tape lives in global memory, interleaved across the threads of
 // a launch (entry n of lane t at n * stride + t), so that threads running
-// the same operation store and load neighbouring words: the two operand
-// indices packed in 16 bits each (0xffff for none), the two partials, and
-// the entry's adjoint (zeroed when the entry is recorded).  The per-thread
-// entry count sits in shared memory (blocks of at most kTapeBlock threads)
-// beside the launch's tape context.  Entries past the capacity are counted
-// but not stored; the caller compares the count with the capacity and
-// treats such a thread's tape as unusable.
+// the same operation store and load neighbouring records.  An entry is one
+// 16-byte record -- the two operand indices packed in 16 bits each (0xffff
+// for none), the two partials, and the entry's adjoint (zeroed when the
+// entry is recorded) -- written by one vector store and read back by one
+// vector load: the lanes of a warp are mostly at different entries, so
+// each access touches one cache line per lane, and one access per entry
+// keeps that cost down.  The per-thread entry count sits in shared memory
+// (blocks of at most kTapeBlock threads) beside the launch's tape context.
+// Entries past the capacity are counted but not stored; the caller
+// compares the count with the capacity and treats such a thread's tape as
+// unusable.
 #pragma once
 #include "dual.cuh"
 
@@ -28,11 +32,17 @@ namespace wrf {
 constexpr int kTapeBlock = 64;
 constexpr int kTapeMaxEntries = 0xffff;  // operand indices fit in 16 bits
 
+// an entry: x the packed operand indices, y and z the partials (float
+// bits), w the adjoint
+using TapeRec = uint4;
+
 struct TapeCtx {
-  unsigned* ab;  // packed operand indices of entry n of lane t at [n * stride + t]
-  float2* dd;    // partials
-  float* adj;    // adjoints
+  TapeRec* rec;  // entry n of lane t at rec[n * stride + t]
   int stride, cap;
+  // the adjoint of entry n of lane
+  __device__ __forceinline__ float* adj(size_t n, size_t lane) const {
+    return reinterpret_cast<float*>(rec + n * stride + lane) + 3;
+  }
 };
 
 // the block's tape context and the per-thread entry counts
@@ -51,12 +61,9 @@ __device__ __forceinline__ int tape_rec(int a, int b, float da, float db) {
   const int t = threadIdx.x;
   const int n = g_tape_n[t];
   g_tape_n[t] = n + 1;
-  if (n < g_tape.cap) {
-    const size_t q = (size_t)n * g_tape.stride + tape_lane();
-    g_tape.ab[q] = (unsigned)(a & 0xffff) | ((unsigned)(b & 0xffff) << 16);
-    g_tape.dd[q] = make_float2(da, db);
-    g_tape.adj[q] = 0.f;
-  }
+  if (n < g_tape.cap)
+    g_tape.rec[(size_t)n * g_tape.stride + tape_lane()] =
+        make_uint4((unsigned)(a & 0xffff) | ((unsigned)(b & 0xffff) << 16), __float_as_uint(da), __float_as_uint(db), 0u);
   return n;
 }
 
@@ -65,7 +72,7 @@ __device__ __forceinline__ int tape_rec(int a, int b, float da, float db) {
 __device__ __forceinline__ void tape_reserve(int n) {
   const int t = threadIdx.x;
   const int m = n < g_tape.cap ? n : g_tape.cap;
-  for (int k = 0; k < m; ++k) g_tape.adj[(size_t)k * g_tape.stride + tape_lane()] = 0.f;
+  for (int k = 0; k < m; ++k) g_tape.rec[(size_t)k * g_tape.stride + tape_lane()] = make_uint4(0xffffffffu, 0u, 0u, 0u);
   g_tape_n[t] = n;
 }
 
@@ -126,73 +133,65 @@ struct Lift<Tv> {
   __device__ static Tv c(float x) { return Tv{x, -1}; }
 };
 
-// one contribution c to the adjoint of entry a (0xffff: none) during the
-// sweep's step t, after the load of step t + D: to the window's
-// accumulator of a's step when it lies inside the window (steps t + 1 ..
-// t + D), else a fire-and-forget reduction in memory
-template <int D>
-__device__ __forceinline__ void tape_give(const TapeCtx& tc, size_t lane, int n0, int n, int t, unsigned a, float c,
-                                          float (&acc)[D]) {
-  if (a == 0xffffu || c == 0.f) return;
-  const int ta = n - 1 - (int)a;
-  if ((int)a >= n0 && ta <= t + D) {
-    const int slot = ta & (D - 1);
-#pragma unroll
-    for (int u = 0; u < D; ++u) acc[u] += slot == u ? c : 0.f;
-  } else {
-    atomicAdd(tc.adj + (size_t)a * tc.stride + lane, c);
-  }
-}
-
 // the reverse sweep of lane's entries [n0, n) (n within the capacity):
-// adj[a] += da adj[e], adj[b] += db adj[e] from the last entry down.  The
-// sweep is software-pipelined over a window of D entries held in
-// registers: entry e's record and adjoint are loaded D steps before they
-// are used, a contribution to an entry inside the window goes to the
-// window's accumulator registers (kept apart from the loaded values, so
-// that no contribution waits for a load in flight), and one to an entry
-// below the window is a fire-and-forget reduction in memory, which the
-// entry's own load (issued later in program order) sees.  The window's
-// slot of step t (entry n - 1 - t) is t mod D.
-template <int D>
-__device__ __forceinline__ void tape_sweep(const TapeCtx& tc, size_t lane, int n0, int n) {
-  static_assert((D & (D - 1)) == 0, "window of a power of two");
+// adj[a] += da adj[e], adj[b] += db adj[e] from the last entry down, by
+// the threads of a block of B threads.  Entry e's record (operands,
+// partials and the adjoint it holds in memory) is loaded D steps before it
+// is used, into a window of registers.  A contribution to one of the next
+// A - 1 entries goes to the thread's ring of A accumulators in shared
+// memory (acc[slot * B + thread], conflict-free across the warp; the slot
+// of step t, entry n - 1 - t, is t mod A), read and cleared when its step
+// comes; one to an entry further down is a fire-and-forget reduction into
+// the entry's record, which the record's own load (issued at least A - D
+// steps later in program order) sees.
+template <int D, int A, int B>
+__device__ __forceinline__ void tape_sweep(const TapeCtx& tc, size_t lane, int n0, int n, float* acc) {
+  static_assert((D & (D - 1)) == 0 && (A & (A - 1)) == 0 && A > D, "windows of powers of two");
   const size_t st = tc.stride;
   const int steps = n - n0;
-  float w[D], acc[D];
+  float* my = acc + threadIdx.x;
+#pragma unroll 4
+  for (int u = 0; u < A; ++u) my[u * B] = 0.f;
+  float w[D];
   unsigned ab[D];
   float2 dd[D];
 #pragma unroll
   for (int u = 0; u < D; ++u) {
-    acc[u] = 0.f;
     w[u] = 0.f;
     ab[u] = 0xffffffffu;
     dd[u] = make_float2(0.f, 0.f);
     if (u < steps) {
-      const size_t q = (size_t)(n - 1 - u) * st + lane;
-      w[u] = __ldcg(tc.adj + q);
-      ab[u] = __ldcs(tc.ab + q);
-      dd[u] = __ldcs(tc.dd + q);
+      const uint4 r = __ldcg(tc.rec + (size_t)(n - 1 - u) * st + lane);
+      ab[u] = r.x;
+      dd[u] = make_float2(__uint_as_float(r.y), __uint_as_float(r.z));
+      w[u] = __uint_as_float(r.w);
     }
   }
+  auto give = [&](int t, unsigned a, float c) {
+    if (a == 0xffffu || c == 0.f) return;
+    const int ta = n - 1 - (int)a;
+    if ((int)a >= n0 && ta < t + A) my[(ta & (A - 1)) * B] += c;
+    else atomicAdd(tc.adj(a, lane), c);
+  };
   for (int t0 = 0; t0 < steps; t0 += D) {
 #pragma unroll
     for (int u = 0; u < D; ++u) {
       const int t = t0 + u;
       if (t < steps) {
-        const float wv = w[u] + acc[u];
+        float* slot = my + (t & (A - 1)) * B;
+        const float wv = w[u] + *slot;
+        *slot = 0.f;
         const unsigned abv = ab[u];
         const float2 ddv = dd[u];
-        acc[u] = 0.f;
         if (t + D < steps) {
-          const size_t q = (size_t)(n - 1 - t - D) * st + lane;
-          w[u] = __ldcg(tc.adj + q);
-          ab[u] = __ldcs(tc.ab + q);
-          dd[u] = __ldcs(tc.dd + q);
+          const uint4 r = __ldcg(tc.rec + (size_t)(n - 1 - t - D) * st + lane);
+          ab[u] = r.x;
+          dd[u] = make_float2(__uint_as_float(r.y), __uint_as_float(r.z));
+          w[u] = __uint_as_float(r.w);
         }
         if (wv != 0.f) {
-          tape_give<D>(tc, lane, n0, n, t, abv & 0xffffu, ddv.x * wv, acc);
-          tape_give<D>(tc, lane, n0, n, t, abv >> 16, ddv.y * wv, acc);
+          give(t, abv & 0xffffu, ddv.x * wv);
+          give(t, abv >> 16, ddv.y * wv);
         }
       }
     }
