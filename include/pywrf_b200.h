@@ -438,11 +438,15 @@ int wrf_calc_p_rho_adj(const WrfGrid* g, const WrfState* s, const WrfState* sbar
  * autograd through wrf_dynamics.py:1112-1331 (advect_u) and 1332-1534
  * (advect_v); its advect_w (1535-1823) cannot be differentiated by its
  * autograd (an in-place update of a saved operand), the product is the
- * same transpose of the linearised operator. */
+ * same transpose of the linearised operator.  work: device scratch of at
+ * least wrf_advect_momentum_adj_work floats (work_floats, checked). */
 int wrf_advect_momentum_adj(const WrfGrid* g, int component, const float* field, const float* ru,
                             const float* rv, const float* rom, const float* msf, const float* msf2,
                             const float* fzm, const float* fzp, const float* rdz, const float* tend_bar,
-                            float* field_bar, float* ru_bar, float* rv_bar, float* rom_bar, void* stream);
+                            float* field_bar, float* ru_bar, float* rv_bar, float* rom_bar, float* work,
+                            size_t work_floats, void* stream);
+/* The number of floats of work wrf_advect_momentum_adj needs for the grid. */
+int wrf_advect_momentum_adj_work(const WrfGrid* g, size_t* floats);
 /* wrf_boundary.py:52-147 relax_bdytend on one field: tend += the relaxation
  * toward bdy + dtbc * bdy_tend over the zone rows 1..3.  bdy8: device arrays
  * xs xe ys ye (values) and txs txe tys tye (tendencies) in the solver's

@@ -190,7 +190,9 @@ def lib() -> ctypes.CDLL:
     L.wrf_advance_uv_adj.restype = ip
     L.wrf_advance_uv_adj.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.c_float, vp]
     L.wrf_advect_momentum_adj.restype = ip
-    L.wrf_advect_momentum_adj.argtypes = [ctypes.POINTER(WrfGridC), ctypes.c_int] + [vp] * 14 + [vp]
+    L.wrf_advect_momentum_adj.argtypes = [ctypes.POINTER(WrfGridC), ctypes.c_int] + [vp] * 15 + [ctypes.c_size_t, vp]
+    L.wrf_advect_momentum_adj_work.restype = ip
+    L.wrf_advect_momentum_adj_work.argtypes = [ctypes.POINTER(WrfGridC), ctypes.POINTER(ctypes.c_size_t)]
     L.wrf_advect_scalar_adj.restype = ip
     L.wrf_advect_scalar_adj.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 13 + [vp]
     L.wrf_relax_bdytend.restype = ip

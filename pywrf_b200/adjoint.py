@@ -123,7 +123,7 @@ class AdvectScalar(torch.autograd.Function):
     def backward(ctx, gout):
         field, ru, rv, rom, msftx, fnm, fnp, rdnw = ctx.saved_tensors
         gout = gout.contiguous()
-        qb, rub, rvb, romb = (torch.zeros_like(field) for _ in range(4))
+        qb, rub, rvb, romb = _zeros(field, field, field, field)
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(field.device):
             rc = N.lib().wrf_advect_scalar_adj(ctypes.byref(ctx.cg), _ptr(field), _ptr(ru), _ptr(rv), _ptr(rom),
@@ -167,13 +167,16 @@ class AdvectMomentum(torch.autograd.Function):
     def backward(ctx, gout):
         field, ru, rv, rom, msf, msf2, fzm, fzp, rdz = ctx.saved_tensors
         gout = gout.contiguous()
-        qb, rub, rvb, romb = (torch.zeros_like(field) for _ in range(4))
+        qb, rub, rvb, romb = _zeros(field, field, field, field)
         m2 = _ptr(msf2) if ctx.has_msf2 else None
+        n = ctypes.c_size_t(0)
+        N.check(N.lib().wrf_advect_momentum_adj_work(ctypes.byref(ctx.cg), ctypes.byref(n)), "work")
+        work = torch.empty(int(n.value), dtype=torch.float32, device=field.device)
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(field.device):
             rc = N.lib().wrf_advect_momentum_adj(ctypes.byref(ctx.cg), ctx.component, _ptr(field), _ptr(ru), _ptr(rv),
                                                  _ptr(rom), _ptr(msf), m2, _ptr(fzm), _ptr(fzp), _ptr(rdz), _ptr(gout),
-                                                 _ptr(qb), _ptr(rub), _ptr(rvb), _ptr(romb), stream)
+                                                 _ptr(qb), _ptr(rub), _ptr(rvb), _ptr(romb), _ptr(work), n, stream)
         N.check(rc, "wrf_advect_momentum_adj")
         return None, qb, gout, rub, rvb, romb, None, None, None, None, None, None, None
 
@@ -196,6 +199,33 @@ def _table(named: dict):
     for k, t in named.items():
         arr[names.index(k)] = _ptr(t).value
     return arr
+
+
+def _zeros(*likes):
+    """Zero float32 tensors shaped like ``likes``, carved (at 256-byte
+    aligned offsets) from one buffer that a single fill clears: one launch
+    instead of one per cotangent buffer."""
+    if not likes:
+        return []
+    sizes = [(t.numel() + 63) // 64 * 64 for t in likes]
+    buf = torch.zeros(sum(sizes), dtype=torch.float32, device=likes[0].device)
+    out, o = [], 0
+    for t, n in zip(likes, sizes):
+        out.append(buf[o:o + t.numel()].view(t.shape))
+        o += n
+    return out
+
+
+def _bars(named: dict, fields, grads: dict) -> dict:
+    """Cotangent buffers for ``fields``: a clone of the incoming gradient
+    where ``grads`` holds one (the adjoint rewrites it in place), zeros from
+    one shared buffer for the rest."""
+    rest = [k for k in fields if grads.get(k) is None]
+    bars = dict(zip(rest, _zeros(*[named[k] for k in rest])))
+    for k in fields:
+        if k not in bars:
+            bars[k] = grads[k].contiguous().clone()
+    return bars
 
 
 class AdvanceUV(torch.autograd.Function):
@@ -223,9 +253,9 @@ class AdvanceUV(torch.autograd.Function):
     def backward(ctx, gu, gv):
         tensors = ctx.saved_tensors
         named = dict(zip(UV_INPUTS + UV_DATA, tensors))
-        gu = torch.zeros_like(named["u"]) if gu is None else gu.contiguous()
-        gv = torch.zeros_like(named["v"]) if gv is None else gv.contiguous()
-        bars = {k: torch.zeros_like(named[k]) for k in UV_INPUTS[2:]}
+        bars = _bars(named, UV_INPUTS[2:] + tuple(k for k, gk in (("u", gu), ("v", gv)) if gk is None), {})
+        gu = bars["u"] if gu is None else gu.contiguous()
+        gv = bars["v"] if gv is None else gv.contiguous()
         tab = _table(named)
         btab = _table({"u": gu, "v": gv, **bars})
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -279,9 +309,7 @@ class Forces(torch.autograd.Function):
     def backward(ctx, *gouts):
         tensors = ctx.saved_tensors
         named = dict(zip(FORCES_INPUTS + FORCES_DATA, tensors))
-        bars = {k: (torch.zeros_like(named[k]) if g is None else g.contiguous().clone())
-                for k, g in zip(FORCES_OUTPUTS, gouts)}
-        bars.update({k: torch.zeros_like(named[k]) for k in FORCES_INPUTS[len(FORCES_OUTPUTS):]})
+        bars = _bars(named, FORCES_INPUTS, dict(zip(FORCES_OUTPUTS, gouts)))
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(bars["u"].device):
             rc = N.lib().wrf_forces_adj(ctypes.byref(ctx.cg), _table(named), _table(bars), ctx.terms, stream)
@@ -327,9 +355,7 @@ class Sumflux(torch.autograd.Function):
     @staticmethod
     def backward(ctx, *gouts):
         named = dict(zip(SF_INPUTS + SF_DATA, ctx.saved_tensors))
-        bars = {k: (torch.zeros_like(named[k]) if g is None else g.contiguous().clone())
-                for k, g in zip(SF_INPUTS[:3], gouts)}
-        bars.update({k: torch.zeros_like(named[k]) for k in SF_INPUTS[3:]})
+        bars = _bars(named, SF_INPUTS, dict(zip(SF_INPUTS[:3], gouts)))
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(bars["u"].device):
             rc = N.lib().wrf_sumflux_adj(ctypes.byref(ctx.cg), _table(named), _table(bars), ctx.it[0], ctx.it[1],
@@ -402,8 +428,7 @@ class SpecUpdatePh(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gout):
         named = dict(zip(SPH_INPUTS, ctx.saved_tensors))
-        bars = {k: torch.zeros_like(named[k]) for k in SPH_INPUTS}
-        bars["ph"] = gout.contiguous().clone()
+        bars = _bars(named, SPH_INPUTS, {"ph": gout})
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(gout.device):
             rc = N.lib().wrf_spec_bdyupdate_ph_adj(ctypes.byref(ctx.cg), _table(named), _table(bars), ctx.dt, stream)
@@ -447,10 +472,7 @@ class Prep(torch.autograd.Function):
     @staticmethod
     def backward(ctx, *gouts):
         named = dict(zip(PREP_FIELDS + PREP_DATA, ctx.saved_tensors))
-        bars = {k: torch.zeros_like(named[k]) for k in PREP_FIELDS}
-        for k, gr in zip(PREP_OUTPUTS, gouts):
-            if gr is not None:
-                bars[k] = gr.contiguous().clone()
+        bars = _bars(named, PREP_FIELDS, dict(zip(PREP_OUTPUTS, gouts)))
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(bars["u"].device):
             rc = N.lib().wrf_prep_adj(ctypes.byref(ctx.cg), _table(named), _table(bars), ctx.ops, stream)
@@ -567,12 +589,7 @@ class AdvanceW(torch.autograd.Function):
     def backward(ctx, *gouts):
         tensors = ctx.saved_tensors
         named = dict(zip(AW_INPUTS + AW_DATA, tensors))
-        bars = {}
-        for k, gk in zip(AW_OUTPUTS, gouts):
-            bars[k] = torch.zeros_like(named[k]) if gk is None else gk.contiguous().clone()
-        for k in AW_INPUTS:
-            if k not in bars:
-                bars[k] = torch.zeros_like(named[k])
+        bars = _bars(named, tuple(dict.fromkeys(AW_OUTPUTS + AW_INPUTS)), dict(zip(AW_OUTPUTS, gouts)))
         work = torch.empty_like(named["ht"])
         tab = _table({_AW_FIELD.get(k, k): v for k, v in named.items()})
         btab = _table({_AW_FIELD.get(k, k): v for k, v in bars.items()})
@@ -624,12 +641,7 @@ class AdvanceMuT(torch.autograd.Function):
     def backward(ctx, *gouts):
         tensors = ctx.saved_tensors
         named = dict(zip(MUT_INPUTS + MUT_DATA, tensors))
-        bars = {}
-        for k, gk in zip(MUT_OUTPUTS, gouts):
-            bars[k] = torch.zeros_like(named[k]) if gk is None else gk.contiguous().clone()
-        for k in MUT_INPUTS:
-            if k not in bars:
-                bars[k] = torch.zeros_like(named[k])
+        bars = _bars(named, tuple(dict.fromkeys(MUT_OUTPUTS + MUT_INPUTS)), dict(zip(MUT_OUTPUTS, gouts)))
         work = torch.empty_like(named["ww"])
         tab = _table({_MUT_FIELD.get(k, k): v for k, v in named.items()})
         btab = _table({_MUT_FIELD.get(k, k): v for k, v in bars.items()})
@@ -679,10 +691,9 @@ class CalcPRho(torch.autograd.Function):
     def backward(ctx, gal, gp, gpm1):
         tensors = ctx.saved_tensors
         named = dict(zip(PRHO_INPUTS + ("rdnw",), tensors))
-        out_b = {}
-        for k, gk in (("al", gal), ("p", gp), ("pm1", gpm1)):
-            out_b[k] = torch.zeros_like(named[k]) if gk is None else gk.contiguous().clone()
-        bars = {k: torch.zeros_like(named[k]) for k in PRHO_INPUTS if k not in out_b}
+        allb = _bars(named, tuple(dict.fromkeys(("al", "p", "pm1") + PRHO_INPUTS)), {"al": gal, "p": gp, "pm1": gpm1})
+        out_b = {k: allb[k] for k in ("al", "p", "pm1")}
+        bars = {k: v for k, v in allb.items() if k not in out_b}
         tab = _table({_PRHO_FIELD.get(k, k): v for k, v in named.items()})
         btab = _table({_PRHO_FIELD.get(k, k): v for k, v in {**out_b, **bars}.items()})
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -764,7 +775,7 @@ class VSolveW(torch.autograd.Function):
         nz = x.shape[0]
         ncol = x.numel() // nz
         gw = gw.contiguous()
-        gx, ga, gal, gg = (torch.zeros_like(x) for _ in range(4))
+        gx, ga, gal, gg = _zeros(x, x, x, x)
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(x.device):
             rc = N.lib().wrf_vsolve_w_adj(ncol, nz, _ptr(x), _ptr(a), _ptr(alpha), _ptr(gamma), _ptr(gw), _ptr(gx),
@@ -800,11 +811,10 @@ class CoefW(torch.autograd.Function):
     @staticmethod
     def backward(ctx, ga, galpha, ggamma):
         mut, cqw, c2a, rdn, rdnw = ctx.saved_tensors
-        z = torch.zeros_like(cqw)
+        z, mb, cb, c2b = _zeros(cqw, mut, cqw, c2a)
         ga = z if ga is None else ga.contiguous()
         galpha = z if galpha is None else galpha.contiguous()
         ggamma = z if ggamma is None else ggamma.contiguous()
-        mb, cb, c2b = torch.zeros_like(mut), torch.zeros_like(cqw), torch.zeros_like(c2a)
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(cqw.device):
             rc = N.lib().wrf_coef_w_adj(ctypes.byref(ctx.cg), _ptr(mut), _ptr(cqw), _ptr(c2a), _ptr(rdn), _ptr(rdnw),
@@ -928,10 +938,7 @@ class _TableOp(torch.autograd.Function):
         op = ctx.op
         saved = ctx.saved_tensors  # read once (checkpoint unpacks each saved tensor once)
         named = dict(zip(op.fields + op.data, saved))
-        bars = {k: torch.zeros_like(named[k]) for k in op.fields}
-        for k, gr in zip(op.outputs, gouts):
-            if gr is not None:
-                bars[k] = gr.contiguous().clone()
+        bars = _bars(named, op.fields, dict(zip(op.outputs, gouts)))
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(saved[0].device):
             N.check(op.adj(ctx.cg, _table(named), _table(bars), stream), op.name + "_adj")
@@ -1135,7 +1142,7 @@ class HorizontalDiffusion(torch.autograd.Function):
         base = saved[3] if ctx.has_base else None
         maps = saved[4:] if ctx.has_base else saved[3:]
         gout = gout.contiguous()
-        fb, mb, kb = torch.zeros_like(field), torch.zeros_like(mut), torch.zeros_like(xk)
+        fb, mb, kb = _zeros(field, mut, xk)
         tab = _table(dict(zip(HDIFF_DATA, maps)))
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         bp = None if base is None else _ptr(base)
@@ -1175,7 +1182,7 @@ class MassWeight(torch.autograd.Function):
     def backward(ctx, gout):
         field, mut = ctx.saved_tensors
         gout = gout.contiguous()
-        fb, mb = torch.zeros_like(field), torch.zeros_like(mut)
+        fb, mb = _zeros(field, mut)
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(field.device):
             rc = N.lib().wrf_mass_weight_adj(ctypes.byref(ctx.cg), _ptr(field), _ptr(mut), _ptr(gout), _ptr(fb),

@@ -18,7 +18,8 @@
 // touch it), so results do not depend on scheduling; tend's own cotangent is
 // tbar unchanged (the caller passes it through).
 //
-//   k_advect_mom_adj<C>  adjoint of advect_u (C = 0, wrf_dynamics.py:1112-1331),
+//   k_advect_mom_faces<C> + k_advect_mom_gather<C>
+//                        adjoint of advect_u (C = 0, wrf_dynamics.py:1112-1331),
 //                        advect_v (1, :1332-1534) and advect_w (2, :1535-1823),
 //                        forward k_advect / k_advect_mom_tma, with respect to
 //                        the advected component and ru, rv, rom.  Every face
@@ -29,8 +30,10 @@
 //                        component for fixed upwind choices (the sign of V, or
 //                        of the component itself at advect_u's / advect_v's
 //                        outermost faces).  face_lin<C, D> lists both linear
-//                        forms of a face; the kernel gathers, per point, over
-//                        the faces whose lists hold it:
+//                        forms of a face.  k_advect_mom_faces<C> forms each
+//                        face once and stores its contributions by stencil
+//                        slot, k_advect_mom_gather<C> sums, per point, the
+//                        slots that address it:
 //   qbar(m) += sum_f Fbar(f) V(f) dPhi_f/dq(m),  rbar(n) += sum_f Fbar(f) Phi(f) dV_f/dr(n)
 //                        with Fbar(f) from the tendency cotangent of the cells
 //                        either side of f (one writer per output element).
@@ -1603,88 +1606,126 @@ __device__ float fbar(const Grid& g, const MomAdjArgs& a, const float* tbar, int
   return v;
 }
 
-// the field cotangent at m = (k, j, i) from the faces of direction D
-template <int C, int D>
-__device__ float gather_q(const Grid& g, const MomAdjArgs& a, const float* tbar, int k, int j, int i, size_t m) {
-  const float* r = D == 0 ? a.rv : D == 1 ? a.ru : a.rom;
-  float acc = 0.f;
-  for (int o = -2; o <= 3; ++o) {
-    const int kf = D == 2 ? k + o : k, jf = D == 0 ? j + o : j, f = D == 1 ? i + o : i;
-    const float fb = fbar<C, D>(g, a, tbar, kf, jf, f);
-    if (fb == 0.f) continue;
-    FaceLin L;
-    if (!face_lin<C, D>(g, a, kf, jf, f, L)) continue;
-    float w = 0.f;
-    for (int n = 0; n < L.nq; ++n)
-      if (L.qi[n] == m) w += L.qc[n];
-    if (w == 0.f) continue;
-    float v = 0.f;
-    for (int n = 0; n < L.nr; ++n) v += L.rc[n] * r[L.ri[n]];
-    acc += fb * v * w;
-  }
-  return acc;
+// The two passes of the momentum adjoint.  Pass 1 (one thread per point,
+// taken as the face index of each direction D) forms every face once: its
+// cotangent Fbar, velocity V and face value Phi, then the face's
+// contributions Fbar V dPhi/dq to the field at its stencil offsets o in
+// [-3, 2] along D, stored in slot o + 3 of the face (Q, 6 slots per
+// direction), and Fbar Phi dV/dr to the velocity points p - d (R, one slot
+// per distance d of the component's velocity forms: d in {0, 1} for u,
+// {0, nx} for v, {0, lev, 2 lev} for w).  Pass 2 gathers each point's
+// cotangents from the slots that address it, in a fixed order (one writer
+// per output element, no atomics).
+template <int C>
+__device__ __forceinline__ int r_slot(size_t d, size_t nx, size_t lev) {
+  if (C == 0) return (int)d;
+  if (C == 1) return d == 0 ? 0 : 1;
+  return d == 0 ? 0 : (d == lev ? 1 : 2);
+}
+template <int C>
+__device__ __forceinline__ size_t r_dist(int s, size_t nx, size_t lev) {
+  if (C == 0) return (size_t)s;
+  if (C == 1) return s == 0 ? 0 : nx;
+  return (size_t)s * lev;
+}
+template <int C>
+__host__ __device__ constexpr int r_slots() {
+  return C == 2 ? 3 : 2;
 }
 
-// the cotangent of the D-direction velocity (ru, rv, rom) at n = (k, j, i):
-// the faces whose velocity holds n lie at offsets 0 / +1 in each direction,
-// and advect_w's horizontal faces at the top level also read levels
-// ktf-1 and ktf-2
 template <int C, int D>
-__device__ float gather_r(const Grid& g, const MomAdjArgs& a, const float* tbar, int k, int j, int i, size_t n) {
-  const int ktf = g.nz - 1;
-  float acc = 0.f;
-  const int nk = (C == 2 && D != 2 && k != ktf && k + 1 != ktf) ? 3 : 2;
-  for (int dk = 0; dk < nk; ++dk) {
-    const int kf = dk < 2 ? k + dk : ktf;
-    for (int dj = 0; dj < 2; ++dj)
-      for (int di = 0; di < 2; ++di) {
-        const float fb = fbar<C, D>(g, a, tbar, kf, j + dj, i + di);
-        if (fb == 0.f) continue;
-        FaceLin L;
-        if (!face_lin<C, D>(g, a, kf, j + dj, i + di, L)) continue;
-        float w = 0.f;
-        for (int e = 0; e < L.nr; ++e)
-          if (L.ri[e] == n) w += L.rc[e];
-        if (w == 0.f) continue;
-        float phi = 0.f;
-        for (int e = 0; e < L.nq; ++e) phi += L.qc[e] * a.q[L.qi[e]];
-        acc += fb * phi * w;
-      }
+__device__ __forceinline__ void face_pass(const Grid& g, const MomAdjArgs& a, const float* tbar, int k, int j, int i,
+                                          size_t p, size_t n3, float* Q, float* R) {
+  const size_t lev = (size_t)g.ny * g.nx, nx = g.nx;
+  float q6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, r3[3] = {0.f, 0.f, 0.f};
+  const float fb = fbar<C, D>(g, a, tbar, k, j, i);
+  FaceLin L;
+  if (fb != 0.f && face_lin<C, D>(g, a, k, j, i, L)) {
+    const float* r = D == 0 ? a.rv : D == 1 ? a.ru : a.rom;
+    const long long st = D == 0 ? (long long)nx : D == 1 ? 1 : (long long)lev;
+    float v = 0.f, phi = 0.f;
+    for (int n = 0; n < L.nr; ++n) v += L.rc[n] * r[L.ri[n]];
+    for (int n = 0; n < L.nq; ++n) phi += L.qc[n] * a.q[L.qi[n]];
+    const float gv = fb * v, gp = fb * phi;
+    for (int n = 0; n < L.nq; ++n) {
+      const int slot = (int)(((long long)L.qi[n] - (long long)p) / st) + 3;
+#pragma unroll
+      for (int s = 0; s < 6; ++s) q6[s] += slot == s ? gv * L.qc[n] : 0.f;
+    }
+    for (int n = 0; n < L.nr; ++n) {
+      const int slot = r_slot<C>(p - L.ri[n], nx, lev);
+#pragma unroll
+      for (int s = 0; s < 3; ++s) r3[s] += slot == s ? gp * L.rc[n] : 0.f;
+    }
   }
-  return acc;
+#pragma unroll
+  for (int s = 0; s < 6; ++s) Q[(size_t)(D * 6 + s) * n3 + p] = q6[s];
+#pragma unroll
+  for (int s = 0; s < r_slots<C>(); ++s) R[(size_t)(D * 3 + s) * n3 + p] = r3[s];
 }
 
 }  // namespace
 
 template <int C>
-__global__ void k_advect_mom_adj(Grid g, MomAdjArgs a, const float* tbar, float* qbar, float* rubar, float* rvbar,
-                                 float* rombar) {
+__global__ void k_advect_mom_faces(Grid g, MomAdjArgs a, const float* tbar, float* Q, float* R) {
   WRF_POINT_INDEX(g, k, j, i);
-  const size_t m = ((size_t)k * g.ny + j) * g.nx + i;
-  const float aq = gather_q<C, 0>(g, a, tbar, k, j, i, m) + gather_q<C, 1>(g, a, tbar, k, j, i, m) +
-                   gather_q<C, 2>(g, a, tbar, k, j, i, m);
-  if (aq != 0.f) qbar[m] += aq;
-  const float arv = gather_r<C, 0>(g, a, tbar, k, j, i, m);
-  if (arv != 0.f) rvbar[m] += arv;
-  const float aru = gather_r<C, 1>(g, a, tbar, k, j, i, m);
-  if (aru != 0.f) rubar[m] += aru;
-  const float arom = gather_r<C, 2>(g, a, tbar, k, j, i, m);
-  if (arom != 0.f) rombar[m] += arom;
+  const size_t n3 = g.n3(), p = ((size_t)k * g.ny + j) * g.nx + i;
+  face_pass<C, 0>(g, a, tbar, k, j, i, p, n3, Q, R);
+  face_pass<C, 1>(g, a, tbar, k, j, i, p, n3, Q, R);
+  face_pass<C, 2>(g, a, tbar, k, j, i, p, n3, Q, R);
 }
+
+template <int C>
+__global__ void k_advect_mom_gather(Grid g, const float* Q, const float* R, float* qbar, float* rubar, float* rvbar,
+                                    float* rombar) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const size_t n3 = g.n3(), lev = (size_t)g.ny * g.nx, nx = g.nx;
+  const size_t m = ((size_t)k * g.ny + j) * g.nx + i;
+  float aq = 0.f;
+#pragma unroll
+  for (int D = 0; D < 3; ++D) {
+    const long long st = D == 0 ? (long long)nx : D == 1 ? 1 : (long long)lev;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+      const long long f = (long long)m - (long long)(s - 3) * st;
+      if (f >= 0 && f < (long long)n3) aq += Q[(size_t)(D * 6 + s) * n3 + (size_t)f];
+    }
+  }
+  if (aq != 0.f) qbar[m] += aq;
+  float ar[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int D = 0; D < 3; ++D)
+#pragma unroll
+    for (int s = 0; s < r_slots<C>(); ++s) {
+      const size_t f = m + r_dist<C>(s, nx, lev);
+      if (f < n3) ar[D] += R[(size_t)(D * 3 + s) * n3 + f];
+    }
+  if (ar[0] != 0.f) rvbar[m] += ar[0];
+  if (ar[1] != 0.f) rubar[m] += ar[1];
+  if (ar[2] != 0.f) rombar[m] += ar[2];
+}
+
+size_t advect_mom_adj_work_floats(const Grid& g) { return (size_t)(18 + 9) * g.n3(); }
 
 int launch_advect_mom_adj(const Grid& g, int component, const float* q, const float* ru, const float* rv,
                           const float* rom, const float* msf, const float* msf2, const float* fzm, const float* fzp,
                           const float* rdz, const float* tbar, float* qbar, float* rubar, float* rvbar,
-                          float* rombar, cudaStream_t st) {
+                          float* rombar, float* work, cudaStream_t st) {
   const dim3 b3(32, 4);
   const MomAdjArgs a{q, ru, rv, rom, msf, msf2, fzm, fzp, rdz};
-  if (component == 0)
-    k_advect_mom_adj<0><<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, qbar, rubar, rvbar, rombar);
-  else if (component == 1)
-    k_advect_mom_adj<1><<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, qbar, rubar, rvbar, rombar);
-  else
-    k_advect_mom_adj<2><<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, qbar, rubar, rvbar, rombar);
-  return 1;
+  float* Q = work;
+  float* R = work + 18 * g.n3();
+  if (component == 0) {
+    k_advect_mom_faces<0><<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, Q, R);
+    k_advect_mom_gather<0><<<point_grid(g, b3), b3, 0, st>>>(g, Q, R, qbar, rubar, rvbar, rombar);
+  } else if (component == 1) {
+    k_advect_mom_faces<1><<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, Q, R);
+    k_advect_mom_gather<1><<<point_grid(g, b3), b3, 0, st>>>(g, Q, R, qbar, rubar, rvbar, rombar);
+  } else {
+    k_advect_mom_faces<2><<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, Q, R);
+    k_advect_mom_gather<2><<<point_grid(g, b3), b3, 0, st>>>(g, Q, R, qbar, rubar, rvbar, rombar);
+  }
+  return 2;
 }
 
 int launch_advect_scalar_adj(const Grid& g, const float* q, const float* ru, const float* rv, const float* rom,

@@ -905,7 +905,7 @@ constexpr int kMpDirections = 8;
 // entries a column's tape may take per level by default, and the memory
 // the tapes of one chunk of columns may take
 constexpr int kTapeEntriesPerLevel = 640;
-constexpr size_t kTapeChunkBytes = size_t(16) << 30;
+constexpr size_t kTapeChunkBytes = size_t(24) << 30;
 // the capacity set through set_microphysics_tape_capacity (0: default)
 int g_tape_capacity = 0;
 

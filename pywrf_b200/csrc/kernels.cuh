@@ -102,10 +102,12 @@ int launch_advance_w_adj(const Grid& g, const S& s, const S& b, float dts, float
 int launch_advance_mu_t_adj(const Grid& g, const S& s, const S& b, float dts, int ref_no_grad, float* work,
                             cudaStream_t st);
 int launch_calc_p_rho_adj(const Grid& g, const S& s, const S& b, int step, cudaStream_t st);
+// work: advect_mom_adj_work_floats(g) floats (the faces' stencil slots)
+size_t advect_mom_adj_work_floats(const Grid& g);
 int launch_advect_mom_adj(const Grid& g, int component, const float* q, const float* ru, const float* rv,
                           const float* rom, const float* msf, const float* msf2, const float* fzm, const float* fzp,
                           const float* rdz, const float* tbar, float* qbar, float* rubar, float* rvbar,
-                          float* rombar, cudaStream_t st);
+                          float* rombar, float* work, cudaStream_t st);
 int launch_advect_scalar_adj(const Grid& g, const float* q, const float* ru, const float* rv, const float* rom,
                              const float* msftx, const float* fnm, const float* fnp, const float* rdnw,
                              const float* tbar, float* qbar, float* rubar, float* rvbar, float* rombar,

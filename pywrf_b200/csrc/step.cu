@@ -1229,18 +1229,29 @@ int wrf_advance_uv_adj(const WrfGrid* gin, const WrfState* sin, const WrfState* 
 int wrf_advect_momentum_adj(const WrfGrid* gin, int component, const float* field, const float* ru, const float* rv,
                             const float* rom, const float* msf, const float* msf2, const float* fzm, const float* fzp,
                             const float* rdz, const float* tend_bar, float* field_bar, float* ru_bar, float* rv_bar,
-                            float* rom_bar, void* stream) {
+                            float* rom_bar, float* work, size_t work_floats, void* stream) {
   Grid g;
   int rc = make_grid(gin, g);
   if (rc) return rc;
   if (component < 0 || component > 2) return fail(WRF_EINVAL, "advect_momentum_adj: component 0..2");
   if (!field || !ru || !rv || !rom || !msf || (component == 1 && !msf2) || !fzm || !fzp || !rdz || !tend_bar ||
-      !field_bar || !ru_bar || !rv_bar || !rom_bar)
+      !field_bar || !ru_bar || !rv_bar || !rom_bar || !work)
     return fail(WRF_EINVAL, "null argument");
+  if (work_floats < advect_mom_adj_work_floats(g))
+    return fail(WRF_EINVAL, "advect_momentum_adj: work smaller than wrf_advect_momentum_adj_work gives");
   cudaGetLastError();
   launch_advect_mom_adj(g, component, field, ru, rv, rom, msf, msf2, fzm, fzp, rdz, tend_bar, field_bar, ru_bar,
-                        rv_bar, rom_bar, static_cast<cudaStream_t>(stream));
+                        rv_bar, rom_bar, work, static_cast<cudaStream_t>(stream));
   return check_launch("advect_momentum_adj");
+}
+
+int wrf_advect_momentum_adj_work(const WrfGrid* gin, size_t* floats) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!floats) return fail(WRF_EINVAL, "null argument");
+  *floats = advect_mom_adj_work_floats(g);
+  return WRF_OK;
 }
 
 int wrf_relax_bdytend(const WrfGrid* gin, const float* field, float* tend, const float* const* bdy8, char variable,

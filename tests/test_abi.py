@@ -95,9 +95,9 @@ def test_null_arguments_of_function_entry_points_are_rejected():
     assert rc == N.WRF_EINVAL
     rc = L.wrf_advect_momentum(ctypes.byref(_cgrid()), 0, *([None] * 10), 0, None)
     assert rc == N.WRF_EINVAL
-    rc = L.wrf_advect_momentum_adj(ctypes.byref(_cgrid()), 1, *([None] * 14), None)
+    rc = L.wrf_advect_momentum_adj(ctypes.byref(_cgrid()), 1, *([None] * 15), 0, None)
     assert rc == N.WRF_EINVAL
-    rc = L.wrf_advect_momentum_adj(ctypes.byref(_cgrid()), 3, *([None] * 14), None)
+    rc = L.wrf_advect_momentum_adj(ctypes.byref(_cgrid()), 3, *([None] * 15), 0, None)
     assert rc == N.WRF_EINVAL
     rc = L.wrf_advance_uv(ctypes.byref(_cgrid()), None, ctypes.c_float(1.0), None)
     assert rc == N.WRF_EINVAL
