@@ -11,15 +11,15 @@
 // reverse sweep walks the thread's entries backwards and accumulates the
 // adjoints of the operands.
 //
-// A thread's tape lives in global memory, interleaved across the threads of
-// a launch (entry n of lane t at n * stride + t), so that threads running
-// the same operation store and load neighbouring records.  An entry is one
-// 16-byte record -- the two operand indices packed in 16 bits each (0xffff
-// for none), the two partials, and the entry's adjoint (zeroed when the
-// entry is recorded) -- written by one vector store and read back by one
-// vector load: the lanes of a warp are mostly at different entries, so
-// each access touches one cache line per lane, and one access per entry
-// keeps that cost down.  The per-thread entry count sits in shared memory
+// A thread's tape lives in global memory, contiguous per thread (entry n of
+// lane t at t * cap + n): the lanes of a warp are mostly at different
+// entries, so a warp's accesses fall on different cache lines whatever the
+// layout, and a contiguous tape lets the consecutive entries a thread
+// writes, then reads back in reverse, share lines and DRAM bursts.  An
+// entry is one 16-byte record -- the two operand indices packed in 16 bits
+// each (0xffff for none), the two partials, and the entry's adjoint (zeroed
+// when the entry is recorded) -- written by one vector store and read back
+// by one vector load.  The per-thread entry count sits in shared memory
 // (blocks of at most kTapeBlock threads) beside the launch's tape context.
 // Entries past the capacity are counted but not stored; the caller
 // compares the count with the capacity and treats such a thread's tape as
@@ -37,11 +37,13 @@ constexpr int kTapeMaxEntries = 0xffff;  // operand indices fit in 16 bits
 using TapeRec = uint4;
 
 struct TapeCtx {
-  TapeRec* rec;  // entry n of lane t at rec[n * stride + t]
-  int stride, cap;
+  TapeRec* rec;  // entry n of lane t at rec[t * cap + n]
+  int stride;    // the interleave stride of the caller's column arrays (lanes)
+  int cap;
+  __device__ __forceinline__ TapeRec* at(size_t n, size_t lane) const { return rec + lane * (size_t)cap + n; }
   // the adjoint of entry n of lane
   __device__ __forceinline__ float* adj(size_t n, size_t lane) const {
-    return reinterpret_cast<float*>(rec + n * stride + lane) + 3;
+    return reinterpret_cast<float*>(at(n, lane)) + 3;
   }
 };
 
@@ -62,7 +64,7 @@ __device__ __forceinline__ int tape_rec(int a, int b, float da, float db) {
   const int n = g_tape_n[t];
   g_tape_n[t] = n + 1;
   if (n < g_tape.cap)
-    g_tape.rec[(size_t)n * g_tape.stride + tape_lane()] =
+    *g_tape.at(n, tape_lane()) =
         make_uint4((unsigned)(a & 0xffff) | ((unsigned)(b & 0xffff) << 16), __float_as_uint(da), __float_as_uint(db), 0u);
   return n;
 }
@@ -72,7 +74,7 @@ __device__ __forceinline__ int tape_rec(int a, int b, float da, float db) {
 __device__ __forceinline__ void tape_reserve(int n) {
   const int t = threadIdx.x;
   const int m = n < g_tape.cap ? n : g_tape.cap;
-  for (int k = 0; k < m; ++k) g_tape.rec[(size_t)k * g_tape.stride + tape_lane()] = make_uint4(0xffffffffu, 0u, 0u, 0u);
+  for (int k = 0; k < m; ++k) *g_tape.at(k, tape_lane()) = make_uint4(0xffffffffu, 0u, 0u, 0u);
   g_tape_n[t] = n;
 }
 
@@ -147,8 +149,8 @@ struct Lift<Tv> {
 template <int D, int A, int B>
 __device__ __forceinline__ void tape_sweep(const TapeCtx& tc, size_t lane, int n0, int n, float* acc) {
   static_assert((D & (D - 1)) == 0 && (A & (A - 1)) == 0 && A > D, "windows of powers of two");
-  const size_t st = tc.stride;
   const int steps = n - n0;
+  const TapeRec* mine = tc.at(0, lane);
   float* my = acc + threadIdx.x;
 #pragma unroll 4
   for (int u = 0; u < A; ++u) my[u * B] = 0.f;
@@ -161,7 +163,7 @@ __device__ __forceinline__ void tape_sweep(const TapeCtx& tc, size_t lane, int n
     ab[u] = 0xffffffffu;
     dd[u] = make_float2(0.f, 0.f);
     if (u < steps) {
-      const uint4 r = __ldcg(tc.rec + (size_t)(n - 1 - u) * st + lane);
+      const uint4 r = __ldcg(mine + (n - 1 - u));
       ab[u] = r.x;
       dd[u] = make_float2(__uint_as_float(r.y), __uint_as_float(r.z));
       w[u] = __uint_as_float(r.w);
@@ -184,7 +186,7 @@ __device__ __forceinline__ void tape_sweep(const TapeCtx& tc, size_t lane, int n
         const unsigned abv = ab[u];
         const float2 ddv = dd[u];
         if (t + D < steps) {
-          const uint4 r = __ldcg(tc.rec + (size_t)(n - 1 - t - D) * st + lane);
+          const uint4 r = __ldcg(mine + (n - 1 - t - D));
           ab[u] = r.x;
           dd[u] = make_float2(__uint_as_float(r.y), __uint_as_float(r.z));
           w[u] = __uint_as_float(r.w);
