@@ -431,9 +431,10 @@ def run_adjoint_step(st, it, fused_step_ms, reps=3):
     end-of-step boundaries -- composed from the hand-written operator
     adjoints (pywrf_b200.adjoint.step) on the 240x240x41 state after one
     step, timed with CUDA events (2 warm-up passes): the fwd+adj steps per
-    second of the adjoint configuration's unit of work, the same without the
-    microphysics, and the composed forward alone, beside the fused forward
-    step."""
+    second of the adjoint configuration's unit of work (eagerly, and
+    captured once in a CUDA graph by adjoint.capture and replayed), the same
+    without the microphysics, and the composed forward alone, beside the
+    fused forward step."""
     import torch
     from pywrf_b200 import adjoint as A
 
@@ -475,10 +476,22 @@ def run_adjoint_step(st, it, fused_step_ms, reps=3):
         e1.record()
         torch.cuda.synchronize()
         res[name] = e0.elapsed_time(e1) / reps
+    # the same pass with microphysics, captured once in a CUDA graph and replayed
+    graph = A.capture(lambda: run(mp, True))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    res["fwd_adj_graph"] = e0.elapsed_time(e1) / reps
+    del graph
     peak = torch.cuda.max_memory_allocated() / 2**30
     return {"what": "one whole step (3 RK stages, WSM6 microphysics, end-of-step boundaries) forward and reverse, "
                     "composed from the operator adjoints, 240x240x41",
             "fwd_adj_ms": res["fwd_adj"], "fwd_adj_steps_per_s": 1e3 / res["fwd_adj"],
+            "fwd_adj_ms_graph": res["fwd_adj_graph"], "fwd_adj_steps_per_s_graph": 1e3 / res["fwd_adj_graph"],
             "fwd_adj_ms_without_microphysics": res["fwd_adj_dry"], "fwd_composed_ms": res["fwd_composed"],
             "fused_forward_step_ms": fused_step_ms, "peak_gib": peak,
             "reference_autograd": "not comparable: the reference's autograd cannot run backward through its "

@@ -829,6 +829,29 @@ def coef_w(mut, cqw, c2a, rdn, rdnw, dts, epssm=0.1, top_lid=False, rdx=1.0 / 90
     return CoefW.apply(mut, cqw, c2a, rdn, rdnw, dts, epssm, top_lid, rdx, rdy)
 
 
+def capture(run: Callable[[], object], warmup: int = 2) -> torch.cuda.CUDAGraph:
+    """Capture ``run`` -- a forward and its backward through these
+    Functions, with fixed input tensors and cotangent seeds -- in a CUDA
+    graph, after ``warmup`` eager runs on a side stream; ``graph.replay()``
+    then re-runs every kernel of the pass with no host work between them.
+    Every Function launches on the current stream, reads its scalars from
+    the host arguments (no device-to-host read inside a step) and takes its
+    scratch from torch's allocator (the graph's private pool during
+    capture), so a whole step forward + reverse is capturable.  The
+    gradients that ``run`` leaves (``.grad`` of the leaves) live in the
+    graph's pool and are rewritten by each replay."""
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(warmup):
+            run()
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        run()
+    return graph
+
+
 def rollout(step: Callable[..., Sequence[torch.Tensor]], state: Sequence[torch.Tensor], n_steps: int,
             every: int = 1) -> tuple[torch.Tensor, ...]:
     """Apply ``state = step(*state)`` ``n_steps`` times, differentiably, with
@@ -1437,7 +1460,7 @@ def step_end(st: dict, data: dict, bdy: dict, dtbc: float, *, cf1: float, cf2: f
     cg = scalar_grid(s["u"].shape, rdx, rdy)
     cg.cf1, cg.cf2, cg.cf3 = float(cf1), float(cf2), float(cf3)
     dscal = torch.zeros(16, dtype=torch.float32, device=s["u"].device)
-    dscal[0] = float(dtbc)
+    dscal[:1].fill_(float(dtbc))  # a fill launch, not a host copy: the step stays capturable in a CUDA graph
     dd = {**{k: data[k] for k in ("msfuy", "msfvx", "msftx", "msfty", "ht")}, "dscal": dscal,
           **boundary_arrays(bdy)}
     outs = _TableOp.apply(op, cg, *[s[k] for k in op.fields], *[dd[k] for k in op.data])

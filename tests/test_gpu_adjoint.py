@@ -1116,6 +1116,59 @@ def _dry_start():
     return g, inputs, bdy, copy.deepcopy(m.st)
 
 
+def test_whole_step_forward_and_reverse_replay_from_a_cuda_graph():
+    """adjoint.capture: one whole step with WSM6 (adjoint.step with the
+    microphysics), forward and reverse for seeded cotangents, captured once
+    in a CUDA graph from the small case's state after its first step; two
+    replays give the eager pass's gradients (relative L2 1e-5 per input:
+    the scatter kernels' atomics may add in another order), and a replay
+    after the inputs are changed in place follows the new inputs."""
+    g, inputs, bdy, snap = _dry_start()
+    names = tuple(dict.fromkeys(adjoint.RK_STATE + ("u_1", "w_1", "ph_1", "mu_1", "t_1", "v_1")))
+    st = {k: _cuda(snap[k]).requires_grad_(True) for k in names}
+    data = {k: _cuda(snap[k]) for k in dict.fromkeys(adjoint.STEP_DATA + adjoint._Microphysics.data)}
+    bd = {f: {k: _cuda(v) for k, v in snap["bdy"][f].items()} for f in ("u", "v", "ph", "t", "mu", "qv")}
+    sc = dict(epssm=g.epssm, emdiv=g.emdiv, smdiv=g.smdiv, cf1=float(snap["cf1"]), cf2=float(snap["cf2"]),
+              cf3=float(snap["cf3"]), cfn=float(snap["cfn"]), cfn1=float(snap["cfn1"]), rdx=g.rdx, rdy=g.rdy)
+    mp = lambda s: adjoint.microphysics(s, data, g.dt, g.rdx, g.rdy)  # noqa: E731
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    cot = {k: torch.randn(st[k].shape, generator=gen, device="cuda") for k in STEP_OUT}
+    grads = {}
+
+    def run():
+        for v in st.values():
+            v.grad = None
+        o = adjoint.step(st, data, bd, 2.0 * g.dt, dt=g.dt, soundsteps=g.soundsteps, microphysics=mp, **sc)
+        sum((o[k] * cot[k]).sum() for k in STEP_OUT).backward()
+        grads.clear()
+        grads.update({k: v.grad for k, v in st.items() if v.grad is not None})
+
+    def eager():
+        run()
+        torch.cuda.synchronize()
+        return {k: v.detach().clone() for k, v in grads.items()}
+
+    ref = eager()
+    graph = adjoint.capture(run)
+    captured = dict(grads)
+    for _ in range(2):
+        graph.replay()
+    torch.cuda.synchronize()
+    bad = [(k, rel_l2(captured[k].cpu().numpy(), ref[k].cpu().numpy())) for k in ref]
+    assert not [b for b in bad if not b[1] <= 1e-5], bad
+    # the replay reads the inputs' current values
+    with torch.no_grad():
+        st["t"].mul_(1.001)
+        st["u"].add_(0.01)
+    ref2 = eager()
+    graph.replay()
+    torch.cuda.synchronize()
+    bad = [(k, rel_l2(captured[k].cpu().numpy(), ref2[k].cpu().numpy())) for k in ref2]
+    assert not [b for b in bad if not b[1] <= 1e-5], bad
+    assert any(rel_l2(ref2[k].cpu().numpy(), ref[k].cpu().numpy()) > 1e-4 for k in ref)
+    del graph
+
+
 def _dry_oracle(g, inputs, bdy, snap, dtype, nsteps, pert=None, bias=None):
     from oracle.model import OracleModel
 
