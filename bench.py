@@ -22,8 +22,9 @@ Extra keys of the JSON line:
                 against the measured HBM copy bandwidth
   step_roofline the whole step's 662-pass ledger against the same peak
   phases        per-phase device time of one eager step (probe events)
-  e2e           the same metric through the public API with host buffers:
-                pinned H2D of the prognostic state, one step, D2H of it back
+  e2e           the same metric through the public API with host buffers
+                (Integrator.run_host): every step the pinned H2D of the
+                prognostic state, the step, the D2H of it back
   cpu_baseline  the numpy oracle (a restatement of the reference's CPU path)
                 timed on this host for one step of the same workload
   reference_cpu the unmodified reference's own CPU step, recorded where its
@@ -364,12 +365,9 @@ def run_ours(a):
         barrier()
         torch.cuda.synchronize()
         h0.record(cur)
-        for _ in range(ke):
-            for k in E2E_FIELDS:
-                st[k].copy_(host[k], non_blocking=True)
-            it.run(1)  # the public stepping call: one replay of the captured step
-            for k in E2E_FIELDS:
-                host[k].copy_(st[k], non_blocking=True)
+        # the public host-driven call: every step copies the fields in from the
+        # pinned host buffers, replays the captured step and copies them back
+        it.run_host(host, ke)
         h1.record(cur)
         torch.cuda.synchronize()
         barrier()

@@ -104,6 +104,53 @@ class Integrator:
             else:
                 self.step()
 
+    def run_host(self, host: Mapping[str, torch.Tensor], nsteps: int, chunk_bytes: int = 16 << 20) -> None:
+        """``nsteps`` steps for a caller that keeps fields of the state in
+        pinned host memory (``host``: name -> pinned tensor of the field's
+        shape): every step copies them into the device state, runs the
+        step (graph replay) and copies them back, so that after the call
+        ``host`` holds the state after ``nsteps`` steps.  The copies run on
+        two side streams in chunks of about ``chunk_bytes`` (slices along
+        the first dimension): a chunk's copy back to the host and the next
+        step's copy of it to the device follow each other while the other
+        chunks are still in flight, so the two directions of the link
+        overlap.  Returns with the current stream ordered after the last
+        copy back."""
+        st = self.state
+        pieces = []
+        for k, h in host.items():
+            d = st[k]
+            if h.shape != d.shape or h.dtype != d.dtype or h.device.type != "cpu" or not h.is_pinned():
+                raise ValueError(f"run_host: {k} must be a pinned host tensor shaped like the field")
+            row = d[0].numel() * d.element_size() if d.dim() > 1 else d.numel() * d.element_size()
+            rows = max(1, chunk_bytes // max(1, row)) if d.dim() > 1 else d.shape[0]
+            for a in range(0, d.shape[0], rows):
+                pieces.append((d[a:a + rows], h[a:a + rows]))
+        with torch.cuda.device(st.device):
+            main = torch.cuda.current_stream()
+            h2d, d2h = torch.cuda.Stream(), torch.cuda.Stream()
+            h2d.wait_stream(main)
+            with torch.cuda.stream(h2d):
+                for dv, hv in pieces:
+                    dv.copy_(hv, non_blocking=True)
+            for n in range(nsteps):
+                main.wait_stream(h2d)
+                self.replay()
+                d2h.wait_stream(main)
+                back = []
+                for dv, hv in pieces:
+                    with torch.cuda.stream(d2h):
+                        hv.copy_(dv, non_blocking=True)
+                    e = torch.cuda.Event()
+                    e.record(d2h)
+                    back.append(e)
+                if n + 1 < nsteps:
+                    for (dv, hv), e in zip(pieces, back):
+                        h2d.wait_event(e)
+                        with torch.cuda.stream(h2d):
+                            dv.copy_(hv, non_blocking=True)
+            main.wait_stream(d2h)
+
     def status(self) -> dict[str, int]:
         out = (ctypes.c_int * 16)()
         with torch.cuda.device(self.state.device):
