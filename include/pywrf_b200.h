@@ -186,11 +186,14 @@ int wrf_advect_momentum(const WrfGrid* g, int component, const float* field, flo
  * the updated tendency, accumulates (+=) the cotangents of field, ru, rv and
  * rom.  The cotangent of the incoming tendency is tend_bar itself.  The
  * reference obtains this product from torch autograd through
- * wrf_dynamics.py:1841-2028. */
+ * wrf_dynamics.py:1841-2028.  work: device scratch of at least
+ * wrf_advect_scalar_adj_work floats (work_floats, checked). */
 int wrf_advect_scalar_adj(const WrfGrid* g, const float* field, const float* ru, const float* rv,
                           const float* rom, const float* msftx, const float* fzm, const float* fzp,
                           const float* rdzw, const float* tend_bar, float* field_bar, float* ru_bar,
-                          float* rv_bar, float* rom_bar, void* stream);
+                          float* rv_bar, float* rom_bar, float* work, size_t work_floats, void* stream);
+/* The number of floats of work wrf_advect_scalar_adj needs for the grid. */
+int wrf_advect_scalar_adj_work(const WrfGrid* g, size_t* floats);
 /* wrf_dynamics.py:2031-2620 the large-step tendency terms selected by the
  * mask `terms` (1 rhs_ph, 2 horizontal_pressure_gradient, 4 pg_buoy_w, 8
  * coriolis, 16 curvature) on the state table, with the solver's arguments:

@@ -194,7 +194,9 @@ def lib() -> ctypes.CDLL:
     L.wrf_advect_momentum_adj_work.restype = ip
     L.wrf_advect_momentum_adj_work.argtypes = [ctypes.POINTER(WrfGridC), ctypes.POINTER(ctypes.c_size_t)]
     L.wrf_advect_scalar_adj.restype = ip
-    L.wrf_advect_scalar_adj.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 13 + [vp]
+    L.wrf_advect_scalar_adj.argtypes = [ctypes.POINTER(WrfGridC)] + [vp] * 14 + [ctypes.c_size_t, vp]
+    L.wrf_advect_scalar_adj_work.restype = ip
+    L.wrf_advect_scalar_adj_work.argtypes = [ctypes.POINTER(WrfGridC), ctypes.POINTER(ctypes.c_size_t)]
     L.wrf_relax_bdytend.restype = ip
     L.wrf_relax_bdytend.argtypes = [ctypes.POINTER(WrfGridC), vp, vp, ctypes.POINTER(ctypes.c_void_p), ctypes.c_char,
                                     ctypes.c_float, vp]

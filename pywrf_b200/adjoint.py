@@ -124,11 +124,14 @@ class AdvectScalar(torch.autograd.Function):
         field, ru, rv, rom, msftx, fnm, fnp, rdnw = ctx.saved_tensors
         gout = gout.contiguous()
         qb, rub, rvb, romb = _zeros(field, field, field, field)
+        n = ctypes.c_size_t(0)
+        N.check(N.lib().wrf_advect_scalar_adj_work(ctypes.byref(ctx.cg), ctypes.byref(n)), "work")
+        work = torch.empty(int(n.value), dtype=torch.float32, device=field.device)
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         with torch.cuda.device(field.device):
             rc = N.lib().wrf_advect_scalar_adj(ctypes.byref(ctx.cg), _ptr(field), _ptr(ru), _ptr(rv), _ptr(rom),
                                                _ptr(msftx), _ptr(fnm), _ptr(fnp), _ptr(rdnw), _ptr(gout), _ptr(qb),
-                                               _ptr(rub), _ptr(rvb), _ptr(romb), stream)
+                                               _ptr(rub), _ptr(rvb), _ptr(romb), _ptr(work), n, stream)
         N.check(rc, "wrf_advect_scalar_adj")
         return qb, gout, rub, rvb, romb, None, None, None, None, None, None
 

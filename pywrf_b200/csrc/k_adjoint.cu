@@ -1,6 +1,7 @@
 // Hand-written adjoints of step operators (reverse mode, one cotangent per call).
 //
-//   k_advect_scalar_adj  adjoint of advect_scalar (wrf_dynamics.py:1841-2028,
+//   k_advect_scalar_faces + k_advect_scalar_gather
+//                        adjoint of advect_scalar (wrf_dynamics.py:1841-2028,
 //                        forward: k_advect_scalar / k_advect_tiled) with
 //                        respect to the advected field and the three mass
 //                        fluxes ru, rv, rom.
@@ -14,9 +15,11 @@
 //   Fbar(f)  = a(cell above f) tbar(cell above) - a(cell below f) tbar(cell below)
 //   qbar(m) += sum over faces f whose stencil holds m of Fbar(f) r(f) dPhi_f/dq(m)
 //   rbar(f) += Fbar(f) Phi(f)
-// Each output element is written by one thread (a gather over the faces that
-// touch it), so results do not depend on scheduling; tend's own cotangent is
-// tbar unchanged (the caller passes it through).
+// The faces pass forms each face once (its rbar, and its field terms stored
+// by stencil offset in 18 slot arrays of caller work); the gather pass sums,
+// per point, the slots that address it in a fixed order.  Each output
+// element is written by one thread, so results do not depend on scheduling;
+// tend's own cotangent is tbar unchanged (the caller passes it through).
 //
 //   k_advect_mom_faces<C> + k_advect_mom_gather<C>
 //                        adjoint of advect_u (C = 0, wrf_dynamics.py:1112-1331),
@@ -183,137 +186,139 @@ struct AdvArgs0 {
   const float *q, *ru, *rv, *rom, *msftx, *fnm, *fnp, *rdnw;
 };
 
-}  // namespace
-
-__global__ void k_advect_scalar_adj(Grid g, AdvArgs0 a, const float* tbar, float* qbar, float* rubar, float* rvbar,
-                                    float* rombar) {
-  WRF_POINT_INDEX(g, k, j, i);
-  const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde, nz = g.nz, ktf = nz - 1, nx = g.nx;
-  const size_t lev = (size_t)g.ny * nx;
-  const int c = g.i2(j, i);
-  const size_t p = (size_t)k * lev + c;
-  // the update set and the per-cell coefficients of each direction
-  auto inset = [&](int kk, int jj, int ii) {
-    return kk >= 0 && kk < ktf && ii >= ids && ii < ide - 1 && jj >= jds && jj < jde - 1;
-  };
-  auto tb = [&](int kk, int jj, int ii) { return tbar[(size_t)kk * lev + (size_t)jj * nx + ii]; };
-  auto ay = [&](int kk, int jj, int ii) {
-    return (inset(kk, jj, ii) && jj >= jds + 1 && jj < jde - 2) ? a.msftx[(size_t)jj * nx + ii] * g.rdy : 0.f;
-  };
-  auto ax = [&](int kk, int jj, int ii) {
-    return (inset(kk, jj, ii) && ii >= ids + 1 && ii < ide - 2) ? a.msftx[(size_t)jj * nx + ii] * g.rdx : 0.f;
-  };
-  auto az = [&](int kk, int jj, int ii) { return inset(kk, jj, ii) ? a.rdnw[kk] : 0.f; };
-  // face cotangents
-  auto fby = [&](int kk, int jf, int ii) {
+// The face cotangent Fbar of advect_scalar's faces and the cell coefficients
+// it is formed from: every mass cell of the update set subtracts coef
+// (F(upper face) - F(lower face)) in each direction
+struct ScalarFaces {
+  const Grid& g;
+  const AdvArgs0& a;
+  const float* tbar;
+  size_t lev;
+  __device__ bool inset(int kk, int jj, int ii) const {
+    return kk >= 0 && kk < g.nz - 1 && ii >= g.ids && ii < g.ide - 1 && jj >= g.jds && jj < g.jde - 1;
+  }
+  __device__ float tb(int kk, int jj, int ii) const { return tbar[(size_t)kk * lev + (size_t)jj * g.nx + ii]; }
+  __device__ float ay(int kk, int jj, int ii) const {
+    return (inset(kk, jj, ii) && jj >= g.jds + 1 && jj < g.jde - 2) ? a.msftx[(size_t)jj * g.nx + ii] * g.rdy : 0.f;
+  }
+  __device__ float ax(int kk, int jj, int ii) const {
+    return (inset(kk, jj, ii) && ii >= g.ids + 1 && ii < g.ide - 2) ? a.msftx[(size_t)jj * g.nx + ii] * g.rdx : 0.f;
+  }
+  __device__ float az(int kk, int jj, int ii) const { return inset(kk, jj, ii) ? a.rdnw[kk] : 0.f; }
+  __device__ float fby(int kk, int jf, int ii) const {
     float v = 0.f;
     if (jf < g.ny) { const float cf = ay(kk, jf, ii); if (cf != 0.f) v += cf * tb(kk, jf, ii); }
     if (jf >= 1) { const float cf = ay(kk, jf - 1, ii); if (cf != 0.f) v -= cf * tb(kk, jf - 1, ii); }
     return v;
-  };
-  auto fbx = [&](int kk, int jj, int f) {
+  }
+  __device__ float fbx(int kk, int jj, int f) const {
     float v = 0.f;
-    if (f < nx) { const float cf = ax(kk, jj, f); if (cf != 0.f) v += cf * tb(kk, jj, f); }
+    if (f < g.nx) { const float cf = ax(kk, jj, f); if (cf != 0.f) v += cf * tb(kk, jj, f); }
     if (f >= 1) { const float cf = ax(kk, jj, f - 1); if (cf != 0.f) v -= cf * tb(kk, jj, f - 1); }
     return v;
-  };
-  auto fbz = [&](int kf, int jj, int ii) {
+  }
+  __device__ float fbz(int kf, int jj, int ii) const {
     float v = 0.f;
-    if (kf < nz) { const float cf = az(kf, jj, ii); if (cf != 0.f) v += cf * tb(kf, jj, ii); }
+    if (kf < g.nz) { const float cf = az(kf, jj, ii); if (cf != 0.f) v += cf * tb(kf, jj, ii); }
     if (kf >= 1) { const float cf = az(kf - 1, jj, ii); if (cf != 0.f) v -= cf * tb(kf - 1, jj, ii); }
     return v;
-  };
+  }
+};
+
+// one face's contributions Fbar r dPhi/dq(f + o) to the slots o + 3 of
+// direction D (ord 5: o in [-3, 2], 3: [-2, 1], 2: the two-point average,
+// 1: the fnm / fnp average of the vertical faces next to the ends)
+__device__ __forceinline__ void scalar_slots(float* Q, size_t n3, int D, size_t p, int ord, float fbr, float s,
+                                             float c0, float cm1) {
+#pragma unroll
+  for (int o = -3; o <= 2; ++o) {
+    float w = 0.f;
+    if (ord == 5) w = w5(o, s);
+    else if (ord == 3) w = w3(o, s);
+    else if (ord == 2) w = (o == 0 || o == -1) ? 0.5f : 0.f;
+    else if (ord == 1) w = o == 0 ? c0 : (o == -1 ? cm1 : 0.f);
+    Q[(size_t)(D * 6 + o + 3) * n3 + p] = fbr * w;
+  }
+}
+
+}  // namespace
+
+// Pass 1 of advect_scalar's reverse: one thread per point p, taken as the y
+// face jf = j, the x face f = i and the vertical face kf = k.  Each face's
+// cotangent Fbar (from the cells either side), velocity r and upwind sign
+// give its contributions to the field at its stencil offsets (slots, as in
+// the momentum reverse) and its own velocity cotangent rbar = Fbar Phi,
+// which only this thread writes.
+__global__ void k_advect_scalar_faces(Grid g, AdvArgs0 a, const float* tbar, float* Q, float* rubar, float* rvbar,
+                                      float* rombar) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const int ids = g.ids, ide = g.ide, jds = g.jds, jde = g.jde, nz = g.nz, ktf = nz - 1, nx = g.nx;
+  const size_t lev = (size_t)g.ny * nx, n3 = g.n3();
+  const size_t p = (size_t)k * lev + (size_t)j * nx + i;
+  const ScalarFaces F{g, a, tbar, lev};
   const float* q = a.q;
-
-  // --- field cotangent: gather over the faces whose stencil holds (k, j, i)
-  float acc = 0.f;
-  for (int jf = j - 2; jf <= j + 3; ++jf) {
-    if (jf < 0 || jf >= g.ny) continue;
-    const int ord = horder(jf, jds, jde);
-    if (!ord) continue;
-    const float fb = fby(k, jf, i);
-    if (fb == 0.f) continue;
-    const float r = a.rv[(size_t)k * lev + (size_t)jf * nx + i];
-    const int o = j - jf;
-    const float w = ord == 5 ? w5(o, sgnf(r)) : ord == 3 ? w3(o, sgnf(r)) : ((o == 0 || o == -1) ? 0.5f : 0.f);
-    acc += fb * r * w;
-  }
-  for (int f = i - 2; f <= i + 3; ++f) {
-    if (f < 0 || f >= nx) continue;
-    const int ord = horder(f, ids, ide);
-    if (!ord) continue;
-    const float fb = fbx(k, j, f);
-    if (fb == 0.f) continue;
-    const size_t row = (size_t)k * lev + (size_t)j * nx;
-    const float r = a.ru[row + f];
-    const float rs = f == ide - 3 ? a.ru[row + ide - 2] : r;  // the reference's sign source of that face
-    const int o = i - f;
-    const float w = ord == 5 ? w5(o, sgnf(rs)) : ord == 3 ? w3(o, sgnf(rs)) : ((o == 0 || o == -1) ? 0.5f : 0.f);
-    acc += fb * r * w;
-  }
-  for (int kf = k - 2; kf <= k + 3; ++kf) {
-    if (kf < 0 || kf >= nz) continue;
-    const int ord = vorder(kf, ktf);
-    if (!ord) continue;
-    const float fb = fbz(kf, j, i);
-    if (fb == 0.f) continue;
-    const float r = a.rom[(size_t)kf * lev + c];
-    const int o = k - kf;
-    float w;
-    if (ord == 5) w = w5(o, sgnf(-r));
-    else if (ord == 3) w = w3(o, sgnf(-r));
-    else w = o == 0 ? a.fnm[kf] : (o == -1 ? a.fnp[kf] : 0.f);
-    acc += fb * r * w;
-  }
-  if (acc != 0.f) qbar[p] += acc;
-
-  // --- flux cotangents of the faces owned by this point: rbar = Fbar Phi
-  auto Q = [&](size_t base, int off, int st) { return q[base + (size_t)((long long)off * st)]; };
+  auto Qv = [&](size_t base, int off, int st) { return q[base + (size_t)((long long)off * st)]; };
   {  // y face jf = j at (k, i)
     const int ord = horder(j, jds, jde);
-    if (ord && k < nz) {
-      const float fb = fby(k, j, i);
-      if (fb != 0.f) {
-        const float r = a.rv[p];
-        const size_t b = p;
-        float phi;
-        if (ord == 5) phi = flux5(Q(b, -3, nx), Q(b, -2, nx), Q(b, -1, nx), Q(b, 0, nx), Q(b, 1, nx), Q(b, 2, nx), r);
-        else if (ord == 3) phi = flux3(Q(b, -2, nx), Q(b, -1, nx), Q(b, 0, nx), Q(b, 1, nx), r);
-        else phi = 0.5f * (Q(b, 0, nx) + Q(b, -1, nx));
-        rvbar[p] += fb * phi;
-      }
+    const float fb = ord ? F.fby(k, j, i) : 0.f;
+    const float r = a.rv[p];
+    scalar_slots(Q, n3, 0, p, fb != 0.f ? ord : 0, fb * r, sgnf(r), 0.f, 0.f);
+    if (fb != 0.f) {
+      float phi;
+      if (ord == 5) phi = flux5(Qv(p, -3, nx), Qv(p, -2, nx), Qv(p, -1, nx), Qv(p, 0, nx), Qv(p, 1, nx), Qv(p, 2, nx), r);
+      else if (ord == 3) phi = flux3(Qv(p, -2, nx), Qv(p, -1, nx), Qv(p, 0, nx), Qv(p, 1, nx), r);
+      else phi = 0.5f * (Qv(p, 0, nx) + Qv(p, -1, nx));
+      rvbar[p] += fb * phi;
     }
   }
   {  // x face f = i at (k, j)
     const int ord = horder(i, ids, ide);
-    if (ord) {
-      const float fb = fbx(k, j, i);
-      if (fb != 0.f) {
-        const size_t row = (size_t)k * lev + (size_t)j * nx;
-        const float rs = i == ide - 3 ? a.ru[row + ide - 2] : a.ru[p];
-        float phi;
-        if (ord == 5) phi = flux5(Q(p, -3, 1), Q(p, -2, 1), Q(p, -1, 1), Q(p, 0, 1), Q(p, 1, 1), Q(p, 2, 1), rs);
-        else if (ord == 3) phi = flux3(Q(p, -2, 1), Q(p, -1, 1), Q(p, 0, 1), Q(p, 1, 1), rs);
-        else phi = 0.5f * (Q(p, 0, 1) + Q(p, -1, 1));
-        rubar[p] += fb * phi;
-      }
+    const float fb = ord ? F.fbx(k, j, i) : 0.f;
+    const size_t row = (size_t)k * lev + (size_t)j * nx;
+    const float r = a.ru[p];
+    const float rs = (i == ide - 3 && ord) ? a.ru[row + ide - 2] : r;  // the reference's sign source of that face
+    scalar_slots(Q, n3, 1, p, fb != 0.f ? ord : 0, fb * r, sgnf(rs), 0.f, 0.f);
+    if (fb != 0.f) {
+      float phi;
+      if (ord == 5) phi = flux5(Qv(p, -3, 1), Qv(p, -2, 1), Qv(p, -1, 1), Qv(p, 0, 1), Qv(p, 1, 1), Qv(p, 2, 1), rs);
+      else if (ord == 3) phi = flux3(Qv(p, -2, 1), Qv(p, -1, 1), Qv(p, 0, 1), Qv(p, 1, 1), rs);
+      else phi = 0.5f * (Qv(p, 0, 1) + Qv(p, -1, 1));
+      rubar[p] += fb * phi;
     }
   }
   {  // vertical face kf = k at (j, i)
     const int ord = vorder(k, ktf);
-    if (ord) {
-      const float fb = fbz(k, j, i);
-      if (fb != 0.f) {
-        const float r = a.rom[p];
-        const int st = (int)lev;
-        float phi;
-        if (ord == 5) phi = flux5(Q(p, -3, st), Q(p, -2, st), Q(p, -1, st), Q(p, 0, st), Q(p, 1, st), Q(p, 2, st), -r);
-        else if (ord == 3) phi = flux3(Q(p, -2, st), Q(p, -1, st), Q(p, 0, st), Q(p, 1, st), -r);
-        else phi = a.fnm[k] * Q(p, 0, st) + a.fnp[k] * Q(p, -1, st);
-        rombar[p] += fb * phi;
-      }
+    const float fb = ord ? F.fbz(k, j, i) : 0.f;
+    const float r = a.rom[p];
+    scalar_slots(Q, n3, 2, p, fb != 0.f ? ord : 0, fb * r, sgnf(-r), ord == 1 ? a.fnm[k] : 0.f,
+                 ord == 1 ? a.fnp[k] : 0.f);
+    if (fb != 0.f) {
+      const int st = (int)lev;
+      float phi;
+      if (ord == 5) phi = flux5(Qv(p, -3, st), Qv(p, -2, st), Qv(p, -1, st), Qv(p, 0, st), Qv(p, 1, st), Qv(p, 2, st), -r);
+      else if (ord == 3) phi = flux3(Qv(p, -2, st), Qv(p, -1, st), Qv(p, 0, st), Qv(p, 1, st), -r);
+      else phi = a.fnm[k] * Qv(p, 0, st) + a.fnp[k] * Qv(p, -1, st);
+      rombar[p] += fb * phi;
     }
   }
+}
+
+// Pass 2: the field cotangent of each point, summed in a fixed order over
+// the slots of the faces whose stencils hold it (faces on the point's own
+// line in each direction)
+__global__ void k_advect_scalar_gather(Grid g, const float* Q, float* qbar) {
+  WRF_POINT_INDEX(g, k, j, i);
+  const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3();
+  const size_t m = (size_t)k * lev + (size_t)j * g.nx + i;
+  float aq = 0.f;
+#pragma unroll
+  for (int s = 0; s < 6; ++s) {
+    const int o = s - 3;
+    if (j - o >= 0 && j - o < g.ny) aq += Q[(size_t)(0 * 6 + s) * n3 + (m - (long long)o * g.nx)];
+    if (i - o >= 0 && i - o < g.nx) aq += Q[(size_t)(1 * 6 + s) * n3 + (m - o)];
+    if (k - o >= 0 && k - o < g.nz) aq += Q[(size_t)(2 * 6 + s) * n3 + (m - (long long)o * lev)];
+  }
+  if (aq != 0.f) qbar[m] += aq;
 }
 
 // ------------------------------------------------------------ advance_uv
@@ -1728,14 +1733,17 @@ int launch_advect_mom_adj(const Grid& g, int component, const float* q, const fl
   return 2;
 }
 
+size_t advect_scalar_adj_work_floats(const Grid& g) { return (size_t)18 * g.n3(); }
+
 int launch_advect_scalar_adj(const Grid& g, const float* q, const float* ru, const float* rv, const float* rom,
                              const float* msftx, const float* fnm, const float* fnp, const float* rdnw,
-                             const float* tbar, float* qbar, float* rubar, float* rvbar, float* rombar,
+                             const float* tbar, float* qbar, float* rubar, float* rvbar, float* rombar, float* work,
                              cudaStream_t st) {
   const dim3 b3(32, 4);
   AdvArgs0 a{q, ru, rv, rom, msftx, fnm, fnp, rdnw};
-  k_advect_scalar_adj<<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, qbar, rubar, rvbar, rombar);
-  return 1;
+  k_advect_scalar_faces<<<point_grid(g, b3), b3, 0, st>>>(g, a, tbar, work, rubar, rvbar, rombar);
+  k_advect_scalar_gather<<<point_grid(g, b3), b3, 0, st>>>(g, work, qbar);
+  return 2;
 }
 
 }  // namespace wrf

@@ -108,9 +108,11 @@ int launch_advect_mom_adj(const Grid& g, int component, const float* q, const fl
                           const float* rom, const float* msf, const float* msf2, const float* fzm, const float* fzp,
                           const float* rdz, const float* tbar, float* qbar, float* rubar, float* rvbar,
                           float* rombar, float* work, cudaStream_t st);
+// work: advect_scalar_adj_work_floats(g) floats (the faces' stencil slots)
+size_t advect_scalar_adj_work_floats(const Grid& g);
 int launch_advect_scalar_adj(const Grid& g, const float* q, const float* ru, const float* rv, const float* rom,
                              const float* msftx, const float* fnm, const float* fnp, const float* rdnw,
-                             const float* tbar, float* qbar, float* rubar, float* rvbar, float* rombar,
+                             const float* tbar, float* qbar, float* rubar, float* rvbar, float* rombar, float* work,
                              cudaStream_t st);
 
 // relax_bdytend on one field (bdy8: xs xe ys ye txs txe tys tye device

@@ -509,17 +509,28 @@ int wrf_advect_momentum(const WrfGrid* gin, int component, const float* field, f
 int wrf_advect_scalar_adj(const WrfGrid* gin, const float* field, const float* ru, const float* rv, const float* rom,
                           const float* msftx, const float* fzm, const float* fzp, const float* rdzw,
                           const float* tend_bar, float* field_bar, float* ru_bar, float* rv_bar, float* rom_bar,
-                          void* stream) {
+                          float* work, size_t work_floats, void* stream) {
   Grid g;
   int rc = make_grid(gin, g);
   if (rc) return rc;
   if (!field || !ru || !rv || !rom || !msftx || !fzm || !fzp || !rdzw || !tend_bar || !field_bar || !ru_bar ||
-      !rv_bar || !rom_bar)
+      !rv_bar || !rom_bar || !work)
     return fail(WRF_EINVAL, "null argument");
+  if (work_floats < advect_scalar_adj_work_floats(g))
+    return fail(WRF_EINVAL, "advect_scalar_adj: work smaller than wrf_advect_scalar_adj_work gives");
   cudaGetLastError();
   launch_advect_scalar_adj(g, field, ru, rv, rom, msftx, fzm, fzp, rdzw, tend_bar, field_bar, ru_bar, rv_bar, rom_bar,
-                           static_cast<cudaStream_t>(stream));
+                           work, static_cast<cudaStream_t>(stream));
   return check_launch("advect_scalar_adj");
+}
+
+int wrf_advect_scalar_adj_work(const WrfGrid* gin, size_t* floats) {
+  Grid g;
+  int rc = make_grid(gin, g);
+  if (rc) return rc;
+  if (!floats) return fail(WRF_EINVAL, "null argument");
+  *floats = advect_scalar_adj_work_floats(g);
+  return WRF_OK;
 }
 
 namespace {
