@@ -354,7 +354,7 @@ int wrf_microphysics_adj_work(const WrfGrid* g, size_t* floats);
 int wrf_microphysics_adj(const WrfGrid* g, const WrfState* s, const WrfState* post, const WrfState* sbar,
                          float* work, size_t work_floats, const WrfState* values, void* stream);
 /* The tape capacity of wrf_microphysics_adj in entries per column, for the
- * whole library (0 restores the default, 640 entries per level plus the
+ * whole library (0 restores the default, 480 entries per level plus the
  * inputs, at most 65535); *previous (optional) receives the setting it
  * replaces.  A capacity below the column's input count sends every column
  * to the tangents.  Call wrf_microphysics_adj_work again after changing

@@ -809,7 +809,7 @@ __global__ void __launch_bounds__(kTapeBlock) k_mp_tape(Grid g, S s, S yb, S b, 
   }
   const Col<Tv> C{ws + lane, tc.stride, km + 1};
   tape_reserve(mp_inputs(g));
-  prep_column(g, s, C, c2, [](int idx, float v) { return Tv{v, idx}; });
+  prep_column(g, s, C, c2, [](int idx, float v) { return Tv{v, idx, 1.f}; });
   wsm6_column(C, km, dt);
   for (int k = 0; k < km; ++k) finish_level(C, k, dt);
   const int n = g_tape_n[threadIdx.x];
@@ -827,7 +827,7 @@ __global__ void __launch_bounds__(kTapeBlock) k_mp_tape(Grid g, S s, S yb, S b, 
     return;
   }
   auto seed = [&](const Tv& y, float w) {
-    if (y.id >= 0 && w != 0.f) *tc.adj(y.id, lane) += w;
+    if (y.id >= 0 && w != 0.f) *tc.adj(y.id, lane) += w * y.s;
   };
   for (int k = 0; k < km; ++k) {
     const size_t p = k * lev + c2;
@@ -904,7 +904,7 @@ namespace {
 constexpr int kMpDirections = 8;
 // entries a column's tape may take per level by default, and the memory
 // the tapes of one chunk of columns may take
-constexpr int kTapeEntriesPerLevel = 640;
+constexpr int kTapeEntriesPerLevel = 480;
 constexpr size_t kTapeChunkBytes = size_t(24) << 30;
 // the capacity set through set_microphysics_tape_capacity (0: default)
 int g_tape_capacity = 0;
@@ -924,7 +924,7 @@ MpAdjWork mp_adj_work(const Grid& g) {
   w.ncol = (g.ide - 1 - (g.ids + 1)) * (g.jde - 1 - (g.jds + 1));
   w.cap = g_tape_capacity > 0 ? std::min(kTapeMaxEntries, g_tape_capacity)
                               : std::min(kTapeMaxEntries, kTapeEntriesPerLevel * km + mpt::mp_inputs(g));
-  const size_t per_col = (size_t)w.cap * 16 + (size_t)mpt::A_COUNT * (km + 1) * 8;
+  const size_t per_col = (size_t)w.cap * 16 + (size_t)mpt::A_COUNT * (km + 1) * sizeof(Tv);
   const size_t fit = std::max<size_t>(64, kTapeChunkBytes / per_col / 64 * 64);
   w.width = (int)std::min<size_t>(fit, ((size_t)w.ncol + 63) / 64 * 64);
   w.done = 9 * g.n3();
@@ -934,7 +934,7 @@ MpAdjWork mp_adj_work(const Grid& g) {
   const size_t ent = (size_t)w.cap * w.width;
   w.rec = w.region;
   w.cols = w.rec + 4 * ent;
-  const size_t tape = 4 * ent + 2 * (size_t)mpt::A_COUNT * (km + 1) * w.width;
+  const size_t tape = 4 * ent + sizeof(Tv) / sizeof(float) * (size_t)mpt::A_COUNT * (km + 1) * w.width;
   w.total = w.region + std::max(w.tangent, tape);
   return w;
 }

@@ -6,8 +6,9 @@
 // the partial derivatives with respect to them -- to the calling thread's
 // tape; selections (vmin, vmax, sel, the branches of the code) append
 // nothing: the result is the chosen operand itself, so the derivative is
-// that of the branch taken.  Adding a constant appends nothing either (the
-// result keeps its operand's entry).  After the forward code has run, the
+// that of the branch taken.  A value is carried as a multiple of its entry,
+// so adding a constant, scaling by one and negating append nothing either
+// (the multiple enters the partials of the next entry that uses it).  After the forward code has run, the
 // reverse sweep walks the thread's entries backwards and accumulates the
 // adjoints of the operands.
 //
@@ -51,9 +52,13 @@ struct TapeCtx {
 __shared__ TapeCtx g_tape;
 __shared__ int g_tape_n[kTapeBlock];
 
+// a taped value: v the value, id the entry it is a multiple of (-1: a
+// constant) and s that multiple, so that scaling by a constant, negation
+// and adding a constant record nothing
 struct Tv {
   float v;
   int id;
+  float s;
 };
 
 __device__ __forceinline__ int tape_lane() { return blockIdx.x * blockDim.x + threadIdx.x; }
@@ -70,7 +75,7 @@ __device__ __forceinline__ int tape_rec(int a, int b, float da, float db) {
 }
 
 // reserve entries [0, n) for the independent variables (the inputs of the
-// taped code): Tv{value, index} with index < n then names input index
+// taped code): Tv{value, index, 1} with index < n then names input index
 __device__ __forceinline__ void tape_reserve(int n) {
   const int t = threadIdx.x;
   const int m = n < g_tape.cap ? n : g_tape.cap;
@@ -80,59 +85,74 @@ __device__ __forceinline__ void tape_reserve(int n) {
 
 __device__ __forceinline__ float val(const Tv& x) { return x.v; }
 
+// a new entry with operands a and b (partials with respect to the values)
+__device__ __forceinline__ Tv tape_op(float v, const Tv& a, float da, const Tv& b, float db) {
+  return Tv{v, tape_rec(a.id, b.id, da * a.s, db * b.s), 1.f};
+}
+__device__ __forceinline__ Tv tape_op1(float v, const Tv& x, float dx) {
+  return Tv{v, tape_rec(x.id, -1, dx * x.s, 0.f), 1.f};
+}
+
 __device__ __forceinline__ Tv operator+(const Tv& a, const Tv& b) {
-  return Tv{a.v + b.v, tape_rec(a.id, b.id, 1.f, 1.f)};
+  if (b.id < 0) return Tv{a.v + b.v, a.id, a.s};
+  if (a.id < 0) return Tv{a.v + b.v, b.id, b.s};
+  return tape_op(a.v + b.v, a, 1.f, b, 1.f);
 }
 __device__ __forceinline__ Tv operator-(const Tv& a, const Tv& b) {
-  return Tv{a.v - b.v, tape_rec(a.id, b.id, 1.f, -1.f)};
+  if (b.id < 0) return Tv{a.v - b.v, a.id, a.s};
+  if (a.id < 0) return Tv{a.v - b.v, b.id, -b.s};
+  return tape_op(a.v - b.v, a, 1.f, b, -1.f);
 }
-__device__ __forceinline__ Tv operator-(const Tv& a) { return Tv{-a.v, tape_rec(a.id, -1, -1.f, 0.f)}; }
+__device__ __forceinline__ Tv operator-(const Tv& a) { return Tv{-a.v, a.id, -a.s}; }
 __device__ __forceinline__ Tv operator*(const Tv& a, const Tv& b) {
-  return Tv{a.v * b.v, tape_rec(a.id, b.id, b.v, a.v)};
+  if (b.id < 0) return Tv{a.v * b.v, a.id, a.s * b.v};
+  if (a.id < 0) return Tv{a.v * b.v, b.id, b.s * a.v};
+  return tape_op(a.v * b.v, a, b.v, b, a.v);
 }
 __device__ __forceinline__ Tv operator/(const Tv& a, const Tv& b) {
   const float r = a.v / b.v;
+  if (b.id < 0) return Tv{r, a.id, a.s / b.v};
   const float ib = 1.0f / b.v;
-  return Tv{r, tape_rec(a.id, b.id, ib, -r * ib)};
+  return tape_op(r, a, ib, b, -r * ib);
 }
-__device__ __forceinline__ Tv operator+(const Tv& a, float b) { return Tv{a.v + b, a.id}; }
-__device__ __forceinline__ Tv operator+(float a, const Tv& b) { return Tv{a + b.v, b.id}; }
-__device__ __forceinline__ Tv operator-(const Tv& a, float b) { return Tv{a.v - b, a.id}; }
-__device__ __forceinline__ Tv operator-(float a, const Tv& b) { return Tv{a - b.v, tape_rec(b.id, -1, -1.f, 0.f)}; }
-__device__ __forceinline__ Tv operator*(const Tv& a, float b) { return Tv{a.v * b, tape_rec(a.id, -1, b, 0.f)}; }
-__device__ __forceinline__ Tv operator*(float a, const Tv& b) { return Tv{a * b.v, tape_rec(b.id, -1, a, 0.f)}; }
-__device__ __forceinline__ Tv operator/(const Tv& a, float b) { return Tv{a.v / b, tape_rec(a.id, -1, 1.0f / b, 0.f)}; }
+__device__ __forceinline__ Tv operator+(const Tv& a, float b) { return Tv{a.v + b, a.id, a.s}; }
+__device__ __forceinline__ Tv operator+(float a, const Tv& b) { return Tv{a + b.v, b.id, b.s}; }
+__device__ __forceinline__ Tv operator-(const Tv& a, float b) { return Tv{a.v - b, a.id, a.s}; }
+__device__ __forceinline__ Tv operator-(float a, const Tv& b) { return Tv{a - b.v, b.id, -b.s}; }
+__device__ __forceinline__ Tv operator*(const Tv& a, float b) { return Tv{a.v * b, a.id, a.s * b}; }
+__device__ __forceinline__ Tv operator*(float a, const Tv& b) { return Tv{a * b.v, b.id, b.s * a}; }
+__device__ __forceinline__ Tv operator/(const Tv& a, float b) { return Tv{a.v / b, a.id, a.s / b}; }
 __device__ __forceinline__ Tv operator/(float a, const Tv& b) {
   const float r = a / b.v;
-  return Tv{r, tape_rec(b.id, -1, -r / b.v, 0.f)};
+  return tape_op1(r, b, -r / b.v);
 }
 
 // elementary functions: the value by the library's float function, the
 // partial from its closed form (as in the dual numbers)
 __device__ __forceinline__ Tv vsqrt(const Tv& x) {
   const float v = sqrtf(x.v);
-  return Tv{v, tape_rec(x.id, -1, v > 0.f ? 0.5f / v : 0.f, 0.f)};
+  return tape_op1(v, x, v > 0.f ? 0.5f / v : 0.f);
 }
 __device__ __forceinline__ Tv vexp(const Tv& x) {
   const float v = wexp(x.v);
-  return Tv{v, tape_rec(x.id, -1, v, 0.f)};
+  return tape_op1(v, x, v);
 }
-__device__ __forceinline__ Tv vlog(const Tv& x) { return Tv{wlog(x.v), tape_rec(x.id, -1, 1.0f / x.v, 0.f)}; }
+__device__ __forceinline__ Tv vlog(const Tv& x) { return tape_op1(wlog(x.v), x, 1.0f / x.v); }
 __device__ __forceinline__ Tv vpow(const Tv& x, float e) {
   const float v = wpow(x.v, e);
-  return Tv{v, tape_rec(x.id, -1, x.v != 0.f ? e * v / x.v : 0.f, 0.f)};
+  return tape_op1(v, x, x.v != 0.f ? e * v / x.v : 0.f);
 }
 __device__ __forceinline__ Tv vabs(const Tv& x) { return x.v < 0.f ? -x : x; }
 __device__ __forceinline__ Tv vmin(const Tv& a, const Tv& b) { return b.v < a.v ? b : a; }
 __device__ __forceinline__ Tv vmax(const Tv& a, const Tv& b) { return b.v > a.v ? b : a; }
-__device__ __forceinline__ Tv vmin(const Tv& a, float b) { return b < a.v ? Tv{b, -1} : a; }
-__device__ __forceinline__ Tv vmax(const Tv& a, float b) { return b > a.v ? Tv{b, -1} : a; }
-__device__ __forceinline__ Tv vmin(float a, const Tv& b) { return b.v < a ? b : Tv{a, -1}; }
-__device__ __forceinline__ Tv vmax(float a, const Tv& b) { return b.v > a ? b : Tv{a, -1}; }
+__device__ __forceinline__ Tv vmin(const Tv& a, float b) { return b < a.v ? Tv{b, -1, 0.f} : a; }
+__device__ __forceinline__ Tv vmax(const Tv& a, float b) { return b > a.v ? Tv{b, -1, 0.f} : a; }
+__device__ __forceinline__ Tv vmin(float a, const Tv& b) { return b.v < a ? b : Tv{a, -1, 0.f}; }
+__device__ __forceinline__ Tv vmax(float a, const Tv& b) { return b.v > a ? b : Tv{a, -1, 0.f}; }
 
 template <>
 struct Lift<Tv> {
-  __device__ static Tv c(float x) { return Tv{x, -1}; }
+  __device__ static Tv c(float x) { return Tv{x, -1, 0.f}; }
 };
 
 // the reverse sweep of lane's entries [n0, n) (n within the capacity):

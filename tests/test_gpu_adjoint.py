@@ -1386,9 +1386,9 @@ def _microphysics_state_before_step2():
 
 def test_microphysics_adjoint_tape_and_tangent_columns_agree():
     """wrf_microphysics_adj with the tape capacity at its default (every
-    column taped), at 1 (every column by forward-mode tangents) and at 4500
-    and 6500 entries (on this 16-level case, whose columns take 3800 to
-    8600 entries, the columns whose tape outgrows the capacity go to the
+    column taped), at 1 (every column by forward-mode tangents) and at 3000
+    and 4500 entries (on this 16-level case, whose columns take 2 800 to
+    5 600 entries, the columns whose tape outgrows the capacity go to the
     tangents and the rest are taped, in one call): the input cotangents agree to float32 summation order (relative
     L2 1e-5 per field), and the setting is restored."""
     from pywrf_b200 import _native as N
@@ -1428,7 +1428,7 @@ def test_microphysics_adjoint_tape_and_tangent_columns_agree():
 
     taped = reverse(0)
     bad = []
-    for cap in (1, 4500, 6500):
+    for cap in (1, 3000, 4500):
         other = reverse(cap)
         for k in ("t", "moist", "al", "p", "ph", "mu", "muts"):
             e = rel_l2(other[k], taped[k])
