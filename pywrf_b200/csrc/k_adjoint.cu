@@ -92,7 +92,7 @@
 //                        input of the same name and nothing to dmdt, mut or
 //                        mu_tend).
 //
-//   k_advance_w / k_advance_w_adj_col / k_advance_w_adj_bc  advance_w
+//   k_advance_w / k_advance_w_adj_lp / k_advance_w_adj_bc  advance_w
 //                        (wrf_dynamics.py:3641-3796) on the columns [ids+1,
 //                        ide-2) x [jds+1, jde-2): t_2ave, the right-hand side
 //                        rhs = ph + msfty R / mut (R from ph_tend, w and the
@@ -101,9 +101,11 @@
 //                        near-surface winds, the implicit solve with a, alpha,
 //                        gamma, the Rayleigh damping of the upper levels and
 //                        the phi update.  The adjoint runs each column's
-//                        chain backwards in one thread (forward values
-//                        recomputed into local arrays; the solve transposed
-//                        as in k_vsolve_w_adj; the damping weight's sin^2
+//                        chain backwards over a block's level groups (forward
+//                        values recomputed into shared column arrays, the
+//                        per-level parts on all threads in gather form, the
+//                        solve transposed as in k_vsolve_w_adj on one thread
+//                        per column; the damping weight's sin^2
 //                        differentiated in ph_1 and phb through hk and htop)
 //                        and leaves the cotangent of x(0) in a work array, from
 //                        which a second kernel gathers those of u, v (levels
@@ -975,173 +977,347 @@ __global__ void k_advance_w(Grid g, S s, float dts) {
   }
 }
 
-__global__ void k_advance_w_adj_col(Grid g, S s, S b, float dts, float* work) {
-  WRF_COLUMN_INDEX(g, j, i);
-  if (!mut_in(g, j, i)) return;
-  const int ktf = g.nz - 1;
-  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
-  AwCol m;
-  aw_column(g, s, dts, j, i, m);
+// advance_w's reverse with a column's levels spread over the threads of a
+// block: 32 adjacent columns of one row (threadIdx.x) x kAwGroups level
+// groups (threadIdx.y; group y takes levels y, y + kAwGroups, ...).  The
+// per-level parts of the forward recomputation and of the reverse run on
+// all threads, each written in gather form (a level's thread forms every
+// contribution that lands on its level, from its own level's terms and
+// from the neighbouring levels' terms), so every cotangent element has one
+// writer; the three vertical recurrences (the forward's two sweeps of the
+// implicit solve, the transposed sweeps) run on the threads of group 0,
+// one per column, through the column arrays in shared memory
+// ([array][level][column]: a warp's lanes read neighbouring words).  The
+// column sums (mut, muts, muave, and the damping top's height) are reduced
+// across the groups at the end.
+constexpr int kAwGroups = 8, kAwLevels = kMaxNz / kAwGroups;
+constexpr int kAwArrays = 12;  // t2a, wd, R, rhs, P, x, y, z, zb (then xb), yb, Pb, rhsb
+
+size_t advance_w_adj_smem(const Grid& g) { return ((size_t)kAwArrays * g.nz * 32 + 4 * kAwGroups * 32) * sizeof(float); }
+
+__global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_adj_lp(Grid g, S s, S b, float dts, float* work) {
+  extern __shared__ float awsm[];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.x * 32 + tx, j = blockIdx.y;
+  const bool on = i < g.nx && j < g.ny && mut_in(g, j, i);
+  const int nz = g.nz, ktf = nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + (on ? i : 0);
+  auto A = [&](int arr, int k) -> float& { return awsm[((size_t)arr * nz + k) * 32 + tx]; };
+  float* red = awsm + (size_t)kAwArrays * nz * 32;  // [4][kAwGroups][32]
+  enum { T2A, WD, RR, RHS, PP, XX, YY, ZZ, ZB, YB, PB, RHSB };
   const float ep1 = (float)(1.0 + (double)g.epssm), em1 = (float)(1.0 - (double)g.epssm);
   const float gf = (float)G, t0 = (float)T0;
-  const float muave = s[WF_MUAVE][c], muts = s[WF_MUTS][c], mut = s[WF_MUT][c], msfty = s[WF_MSFTY][c];
+  float muave = 0.f, muts = 1.f, mut = 1.f, msfty = 1.f;
+  if (on) muave = s[WF_MUAVE][c], muts = s[WF_MUTS][c], mut = s[WF_MUT][c], msfty = s[WF_MSFTY][c];
   const float minv = 1.0f / msfty;
   const float* rdnw = s[WF_RDNW];
   const float* rdn = s[WF_RDN];
   auto F = [&](int id, int k) { return s[id][k * lev + c]; };
   auto B = [&](int id, int k) -> float& { return b[id][k * lev + c]; };
-  float wb[kMaxNz], pb_in[kMaxNz], tb[kMaxNz], zb[kMaxNz], yb[kMaxNz], xb[kMaxNz], Pb[kMaxNz], rhsb[kMaxNz],
-      wdb[kMaxNz], t2ab[kMaxNz], ph1b[kMaxNz], phbb[kMaxNz], wib[kMaxNz];
-  for (int k = 0; k <= ktf; ++k) {
-    wb[k] = B(WF_W, k);
-    pb_in[k] = 0.f;
-    tb[k] = B(WF_T_2SAVE, k);
-    zb[k] = yb[k] = xb[k] = Pb[k] = rhsb[k] = wdb[k] = t2ab[k] = ph1b[k] = phbb[k] = wib[k] = 0.f;
+  // ---- forward recomputation (aw_column)
+  if (on)
+#pragma unroll
+    for (int l = 0; l < kAwLevels; ++l) {
+      const int k = ty + kAwGroups * l;
+      if (k < ktf) {
+        const float tt = 0.5f * (ep1 * F(WF_T, k) + em1 * F(WF_T_2SAVE, k));
+        A(T2A, k) = (tt + muave * t0) / (muts * (t0 + F(WF_T_SAVE, k)));
+      }
+      if (k == 0) A(WD, 0) = 0.f;
+      if (k >= 1 && k <= ktf)
+        A(WD, k) = 0.5f * (F(WF_WW, k) + F(WF_WW, k - 1)) * rdnw[k - 1] *
+                   (F(WF_PH_SAVE, k) - F(WF_PH_SAVE, k - 1) + F(WF_PHB, k) - F(WF_PHB, k - 1));
+    }
+  __syncthreads();
+  if (on)
+#pragma unroll
+    for (int l = 0; l < kAwLevels; ++l) {
+      const int k = ty + kAwGroups * l;
+      if (k == 0) A(RHS, 0) = 0.f;
+      if (k >= 1 && k <= ktf) {
+        float r = dts * (F(WF_PH_TEND, k) + 0.5f * gf * em1 * F(WF_W, k));
+        if (k < ktf) r = r - dts * (s[WF_FNM][k] * A(WD, k + 1) + s[WF_FNP][k] * A(WD, k));
+        A(RR, k) = r;
+        A(RHS, k) = F(WF_PH, k) + msfty * r / mut;
+      }
+    }
+  __syncthreads();
+  if (on)
+#pragma unroll
+    for (int l = 0; l < kAwLevels; ++l) {
+      const int k = ty + kAwGroups * l;
+      if (k < ktf) A(PP, k) = ep1 * (A(RHS, k + 1) - A(RHS, k)) + em1 * (F(WF_PH, k + 1) - F(WF_PH, k));
+    }
+  __syncthreads();
+  if (on)
+#pragma unroll
+    for (int l = 0; l < kAwLevels; ++l) {
+      const int k = ty + kAwGroups * l;
+      if (k == 0) A(XX, 0) = aw_bc(g, s, j, i);
+      if (k >= 1 && k < ktf) {
+        const float X1 = F(WF_C2A, k) * rdnw[k] / mut * A(PP, k);
+        const float X2 = F(WF_C2A, k - 1) * rdnw[k - 1] / mut * A(PP, k - 1);
+        A(XX, k) = F(WF_W, k) + dts * F(WF_RW_TEND, k) + minv * F(WF_CQW, k) * (0.5f * dts * gf * rdn[k] * (X1 - X2)) +
+                   dts * gf * minv *
+                       (rdn[k] * (F(WF_C2A, k) * F(WF_ALT, k) * A(T2A, k) -
+                                  F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * A(T2A, k - 1)) -
+                        muave);
+      }
+      if (k == ktf) {
+        const float rm = rdnw[k - 1];
+        A(XX, k) = F(WF_W, k) + dts * F(WF_RW_TEND, k) +
+                   minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f * F(WF_C2A, k - 1) * A(PP, k - 1) -
+                           dts * gf * (2.0f * rm * F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * A(T2A, k - 1) + muave));
+      }
+    }
+  __syncthreads();
+  if (on && ty == 0) {  // the implicit solve's two sweeps
+    A(YY, 0) = A(XX, 0);
+    for (int k = 1; k <= ktf; ++k) A(YY, k) = (A(XX, k) - F(WF_A, k) * A(YY, k - 1)) * F(WF_ALPHA, k);
+    A(ZZ, ktf) = A(YY, ktf);
+    for (int k = ktf - 1; k >= 1; --k) A(ZZ, k) = A(YY, k) - F(WF_GAMMA, k) * A(ZZ, k + 1);
+    A(ZZ, 0) = A(YY, 0);
   }
-  float mutb = 0.f, mutsb = 0.f, muaveb = 0.f;
-  // phi update: ph'(k) = rhs(k) + msfty 0.5 dts g (1+e) w'(k) / muts, k >= 1; ph'(0) = ph(0)
-  const float cph = msfty * 0.5f * dts * gf * ep1;
-  float wfb[kMaxNz];
-  wfb[0] = wb[0];
-  pb_in[0] = B(WF_PH, 0);
-  for (int k = 1; k <= ktf; ++k) {
-    const float pbk = B(WF_PH, k);
-    rhsb[k] += pbk;
-    wfb[k] = wb[k] + pbk * cph / muts;
-    mutsb += -pbk * cph * m.wf[k] / (muts * muts);
-  }
-  // damping: w'(k) = (z(k) - d mut w_save) / (1 + d)
+  __syncthreads();
+  // ---- reverse
   const float dampmag = (float)((double)dts * 0.2), hpi = (float)(0.5 * 3.14159265359);
-  float hbotb = 0.f;
-  zb[0] = wfb[0];
-  for (int k = 1; k <= ktf; ++k) {
-    const float dk = m.d[k], ws = F(WF_W_SAVE, k), den = 1.0f + dk;
-    zb[k] = wfb[k] / den;
-    B(WF_W_SAVE, k) += -wfb[k] * dk * mut / den;
-    mutb += -wfb[k] * dk * ws / den;
-    if (m.hk[k] >= m.hbot) {
-      const float db = wfb[k] * (-mut * ws - m.wf[k]) / den;
-      const float th = hpi * (m.hk[k] - m.hbot) / kAwHdepth;
-      const float thb = db * dampmag * sinf(2.0f * th);
-      const float hkb = thb * hpi / kAwHdepth;
-      hbotb += -hkb;
-      ph1b[k] += hkb / gf;
-      phbb[k] += hkb / gf;
+  const float cph = msfty * 0.5f * dts * gf * ep1;
+  float mutb = 0.f, mutsb = 0.f, muaveb = 0.f, hbotb = 0.f;
+  float ph1b[kAwLevels], phbb[kAwLevels], wib[kAwLevels], pbin[kAwLevels];
+#pragma unroll
+  for (int l = 0; l < kAwLevels; ++l) ph1b[l] = phbb[l] = wib[l] = pbin[l] = 0.f;
+  // phi update and damping, per level
+  if (on) {
+    const float hbot = (F(WF_PH_SAVE, ktf) + F(WF_PHB, ktf)) / gf - kAwHdepth;
+#pragma unroll
+    for (int l = 0; l < kAwLevels; ++l) {
+      const int k = ty + kAwGroups * l;
+      if (k == 0) A(ZB, 0) = B(WF_W, 0);
+      if (k >= 1 && k <= ktf) {
+        const float hk = (F(WF_PH_SAVE, k) + F(WF_PHB, k)) / gf;
+        float dk = 0.f;
+        if (hk >= hbot) {
+          const float sn = sinf(hpi * (hk - hbot) / kAwHdepth);
+          dk = dampmag * (sn * sn);
+        }
+        const float ws = F(WF_W_SAVE, k), den = 1.0f + dk;
+        const float wf = (A(ZZ, k) - dk * mut * ws) / den;
+        const float pbk = B(WF_PH, k);
+        const float wfb = B(WF_W, k) + pbk * cph / muts;
+        mutsb += -pbk * cph * wf / (muts * muts);
+        A(ZB, k) = wfb / den;
+        B(WF_W_SAVE, k) += -wfb * dk * mut / den;
+        mutb += -wfb * dk * ws / den;
+        if (hk >= hbot) {
+          const float db = wfb * (-mut * ws - wf) / den;
+          const float th = hpi * (hk - hbot) / kAwHdepth;
+          const float thb = db * dampmag * sinf(2.0f * th);
+          const float hkb = thb * hpi / kAwHdepth;
+          hbotb += -hkb;
+          ph1b[l] += hkb / gf;
+          phbb[l] += hkb / gf;
+        }
+      }
     }
   }
-  ph1b[ktf] += hbotb / gf;  // hbot = htop - hdepth, htop = (ph_1 + phb)(ktf) / g
-  phbb[ktf] += hbotb / gf;
-  // the implicit solve, transposed
-  for (int k = 1; k <= ktf - 1; ++k) {
-    yb[k] += zb[k];
-    B(WF_GAMMA, k) += -m.z[k + 1] * zb[k];
-    zb[k + 1] += -F(WF_GAMMA, k) * zb[k];
+  red[(3 * kAwGroups + ty) * 32 + tx] = hbotb;
+  __syncthreads();
+  if (on && ty == 0) {  // hbot = htop - hdepth, htop = (ph_1 + phb)(ktf) / g: the top level's thread adds it below
+    float hb = 0.f;
+    for (int y = 0; y < kAwGroups; ++y) hb += red[(3 * kAwGroups + y) * 32 + tx];
+    red[(3 * kAwGroups) * 32 + tx] = hb;
+    // the transposed solve: z = y - gamma z(k+1) backwards, y = (x - a y(k-1)) alpha forwards
+    float carry = 0.f;
+    for (int k = 1; k <= ktf - 1; ++k) {
+      const float zbk = A(ZB, k) + carry;
+      A(YB, k) = zbk;
+      B(WF_GAMMA, k) += -A(ZZ, k + 1) * zbk;
+      carry = -F(WF_GAMMA, k) * zbk;
+    }
+    A(YB, ktf) = A(ZB, ktf) + carry;
+    A(YB, 0) = A(ZB, 0);
+    float yc = 0.f;
+    for (int k = ktf; k >= 1; --k) {
+      const float ybk = A(YB, k) + yc;
+      const float al = F(WF_ALPHA, k), ak = F(WF_A, k);
+      A(ZB, k) = al * ybk;  // xb
+      B(WF_A, k) += -A(YY, k - 1) * al * ybk;
+      B(WF_ALPHA, k) += (A(XX, k) - ak * A(YY, k - 1)) * ybk;
+      yc = -ak * al * ybk;
+    }
+    A(ZB, 0) = A(YB, 0) + yc;  // xb(0)
   }
-  yb[ktf] += zb[ktf];
-  yb[0] += zb[0];
-  for (int k = ktf; k >= 1; --k) {
-    const float al = F(WF_ALPHA, k), ak = F(WF_A, k);
-    xb[k] = al * yb[k];
-    B(WF_A, k) += -m.y[k - 1] * al * yb[k];
-    B(WF_ALPHA, k) += (m.x[k] - ak * m.y[k - 1]) * yb[k];
-    yb[k - 1] += -ak * al * yb[k];
-  }
-  xb[0] = yb[0];
-  // explicit w
-  for (int k = 1; k < ktf; ++k) {
-    const float x_b = xb[k];
-    if (x_b == 0.f) continue;
-    wib[k] += x_b;
-    B(WF_RW_TEND, k) += dts * x_b;
-    const float X1 = F(WF_C2A, k) * rdnw[k] / mut * m.P[k];
-    const float X2 = F(WF_C2A, k - 1) * rdnw[k - 1] / mut * m.P[k - 1];
-    const float C1 = minv * F(WF_CQW, k) * 0.5f * dts * gf * rdn[k];
-    B(WF_CQW, k) += x_b * minv * 0.5f * dts * gf * rdn[k] * (X1 - X2);
-    const float X1b = x_b * C1, X2b = -x_b * C1;
-    B(WF_C2A, k) += X1b * rdnw[k] / mut * m.P[k];
-    mutb += -X1b * X1 / mut;
-    Pb[k] += X1b * F(WF_C2A, k) * rdnw[k] / mut;
-    B(WF_C2A, k - 1) += X2b * rdnw[k - 1] / mut * m.P[k - 1];
-    mutb += -X2b * X2 / mut;
-    Pb[k - 1] += X2b * F(WF_C2A, k - 1) * rdnw[k - 1] / mut;
-    const float Bx = dts * gf * minv * x_b;
-    B(WF_C2A, k) += Bx * rdn[k] * F(WF_ALT, k) * m.t2a[k];
-    B(WF_ALT, k) += Bx * rdn[k] * F(WF_C2A, k) * m.t2a[k];
-    t2ab[k] += Bx * rdn[k] * F(WF_C2A, k) * F(WF_ALT, k);
-    B(WF_C2A, k - 1) += -Bx * rdn[k] * F(WF_ALT, k - 1) * m.t2a[k - 1];
-    B(WF_ALT, k - 1) += -Bx * rdn[k] * F(WF_C2A, k - 1) * m.t2a[k - 1];
-    t2ab[k - 1] += -Bx * rdn[k] * F(WF_C2A, k - 1) * F(WF_ALT, k - 1);
-    muaveb += -Bx;
-  }
-  {
-    const int k = ktf;
-    const float x_b = xb[k], rm = rdnw[k - 1];
-    wib[k] += x_b;
-    B(WF_RW_TEND, k) += dts * x_b;
-    const float Ct = minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f);
-    const float term1 = Ct * F(WF_C2A, k - 1) * m.P[k - 1];
-    B(WF_C2A, k - 1) += x_b * Ct * m.P[k - 1];
-    Pb[k - 1] += x_b * Ct * F(WF_C2A, k - 1);
-    mutb += -x_b * term1 / mut;
-    const float Bt = -minv * dts * gf * x_b;
-    B(WF_C2A, k - 1) += Bt * 2.0f * rm * F(WF_ALT, k - 1) * m.t2a[k - 1];
-    B(WF_ALT, k - 1) += Bt * 2.0f * rm * F(WF_C2A, k - 1) * m.t2a[k - 1];
-    t2ab[k - 1] += Bt * 2.0f * rm * F(WF_C2A, k - 1) * F(WF_ALT, k - 1);
-    muaveb += Bt;
-  }
-  // P(k) = (1+e) (rhs(k+1) - rhs(k)) + (1-e) (ph(k+1) - ph(k)), rhs(0) = 0
-  for (int k = 0; k < ktf; ++k) {
-    rhsb[k + 1] += ep1 * Pb[k];
-    if (k >= 1) rhsb[k] += -ep1 * Pb[k];
-    pb_in[k + 1] += em1 * Pb[k];
-    pb_in[k] += -em1 * Pb[k];
-  }
-  // rhs(k) = ph(k) + msfty R(k) / mut
-  for (int k = 1; k <= ktf; ++k) {
-    pb_in[k] += rhsb[k];
-    const float Rb = rhsb[k] * msfty / mut;
-    mutb += -rhsb[k] * msfty * m.R[k] / (mut * mut);
-    B(WF_PH_TEND, k) += dts * Rb;
-    wib[k] += dts * 0.5f * gf * em1 * Rb;
-    if (k < ktf) {
-      wdb[k + 1] += -dts * s[WF_FNM][k] * Rb;
-      wdb[k] += -dts * s[WF_FNP][k] * Rb;
+  __syncthreads();
+  // explicit w (and t_2ave's reverse), per level in gather form
+  if (on) {
+    const float hbt = red[(3 * kAwGroups) * 32 + tx];
+#pragma unroll
+    for (int l = 0; l < kAwLevels; ++l) {
+      const int k = ty + kAwGroups * l;
+      if (k > ktf) continue;
+      if (k == ktf) {
+        ph1b[l] += hbt / gf;
+        phbb[l] += hbt / gf;
+      }
+      float c2ab = 0.f, altb = 0.f, pbk = 0.f, t2ab = 0.f;
+      if (k >= 1 && k < ktf) {  // the level's own terms
+        const float x_b = A(ZB, k);
+        if (x_b != 0.f) {
+          wib[l] += x_b;
+          B(WF_RW_TEND, k) += dts * x_b;
+          const float X1 = F(WF_C2A, k) * rdnw[k] / mut * A(PP, k);
+          const float X2 = F(WF_C2A, k - 1) * rdnw[k - 1] / mut * A(PP, k - 1);
+          const float C1 = minv * F(WF_CQW, k) * 0.5f * dts * gf * rdn[k];
+          B(WF_CQW, k) += x_b * minv * 0.5f * dts * gf * rdn[k] * (X1 - X2);
+          const float X1b = x_b * C1, X2b = -x_b * C1;
+          c2ab += X1b * rdnw[k] / mut * A(PP, k);
+          mutb += -X1b * X1 / mut;
+          pbk += X1b * F(WF_C2A, k) * rdnw[k] / mut;
+          mutb += -X2b * X2 / mut;
+          const float Bx = dts * gf * minv * x_b;
+          c2ab += Bx * rdn[k] * F(WF_ALT, k) * A(T2A, k);
+          altb += Bx * rdn[k] * F(WF_C2A, k) * A(T2A, k);
+          t2ab += Bx * rdn[k] * F(WF_C2A, k) * F(WF_ALT, k);
+          muaveb += -Bx;
+        }
+      }
+      if (k + 1 >= 1 && k + 1 < ktf) {  // level k + 1's terms on level k
+        const float x_b = A(ZB, k + 1);
+        if (x_b != 0.f) {
+          const float C1 = minv * F(WF_CQW, k + 1) * 0.5f * dts * gf * rdn[k + 1];
+          const float X2b = -x_b * C1;
+          c2ab += X2b * rdnw[k] / mut * A(PP, k);
+          pbk += X2b * F(WF_C2A, k) * rdnw[k] / mut;
+          const float Bx = dts * gf * minv * x_b;
+          c2ab += -Bx * rdn[k + 1] * F(WF_ALT, k) * A(T2A, k);
+          altb += -Bx * rdn[k + 1] * F(WF_C2A, k) * A(T2A, k);
+          t2ab += -Bx * rdn[k + 1] * F(WF_C2A, k) * F(WF_ALT, k);
+        }
+      }
+      if (k == ktf) {  // the top level's own terms
+        const float x_b = A(ZB, k), rm = rdnw[k - 1];
+        wib[l] += x_b;
+        B(WF_RW_TEND, k) += dts * x_b;
+        const float Ct = minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f);
+        const float term1 = Ct * F(WF_C2A, k - 1) * A(PP, k - 1);
+        mutb += -x_b * term1 / mut;
+        muaveb += -minv * dts * gf * x_b;
+      }
+      if (k == ktf - 1) {  // the top level's terms on the level below it
+        const float x_b = A(ZB, ktf), rm = rdnw[ktf - 1];
+        const float Ct = minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f);
+        c2ab += x_b * Ct * A(PP, k);
+        pbk += x_b * Ct * F(WF_C2A, k);
+        const float Bt = -minv * dts * gf * x_b;
+        c2ab += Bt * 2.0f * rm * F(WF_ALT, k) * A(T2A, k);
+        altb += Bt * 2.0f * rm * F(WF_C2A, k) * A(T2A, k);
+        t2ab += Bt * 2.0f * rm * F(WF_C2A, k) * F(WF_ALT, k);
+      }
+      if (c2ab != 0.f) B(WF_C2A, k) += c2ab;
+      if (altb != 0.f) B(WF_ALT, k) += altb;
+      if (k < ktf) {
+        A(PB, k) = pbk;
+        // t_2ave(k) = (0.5 ((1+e) t_2 + (1-e) t_2ave) + muave t0) / (muts (t0 + t_1))
+        const float T = B(WF_T_2SAVE, k) + t2ab;
+        const float t1 = F(WF_T_SAVE, k), Dm = muts * (t0 + t1);
+        const float ttb = T / Dm;
+        muaveb += T * t0 / Dm;
+        mutsb += -T * A(T2A, k) / muts;
+        B(WF_T_SAVE, k) += -T * A(T2A, k) / (t0 + t1);
+        B(WF_T, k) += ttb * 0.5f * ep1;
+        B(WF_T_2SAVE, k) = ttb * 0.5f * em1;
+      }
     }
   }
-  // wdwn(k) = (ww(k) + ww(k-1)) / 2 rdnw(k-1) (ph_1 + phb)(k) - (ph_1 + phb)(k-1)
-  for (int k = 1; k <= ktf; ++k) {
-    if (wdb[k] == 0.f) continue;
-    const float h = 0.5f * rdnw[k - 1];
-    const float dph = F(WF_PH_SAVE, k) - F(WF_PH_SAVE, k - 1) + F(WF_PHB, k) - F(WF_PHB, k - 1);
-    B(WF_WW, k) += wdb[k] * h * dph;
-    B(WF_WW, k - 1) += wdb[k] * h * dph;
-    const float dphb = wdb[k] * h * (F(WF_WW, k) + F(WF_WW, k - 1));
-    ph1b[k] += dphb;
-    ph1b[k - 1] += -dphb;
-    phbb[k] += dphb;
-    phbb[k - 1] += -dphb;
+  __syncthreads();
+  // P(k) = (1+e) (rhs(k+1) - rhs(k)) + (1-e) (ph(k+1) - ph(k)) and
+  // rhs(k) = ph(k) + msfty R(k) / mut, per level
+  if (on)
+#pragma unroll
+    for (int l = 0; l < kAwLevels; ++l) {
+      const int k = ty + kAwGroups * l;
+      if (k > ktf) continue;
+      float rhsb = 0.f, pb = k == 0 ? B(WF_PH, 0) : 0.f;
+      if (k >= 1) {
+        rhsb += B(WF_PH, k) + ep1 * A(PB, k - 1);
+        pb += em1 * A(PB, k - 1);
+      }
+      if (k < ktf) {
+        if (k >= 1) rhsb += -ep1 * A(PB, k);
+        pb += -em1 * A(PB, k);
+      }
+      if (k >= 1) {
+        pb += rhsb;
+        const float Rb = rhsb * msfty / mut;
+        mutb += -rhsb * msfty * A(RR, k) / (mut * mut);
+        B(WF_PH_TEND, k) += dts * Rb;
+        wib[l] += dts * 0.5f * gf * em1 * Rb;
+      }
+      A(RHSB, k) = rhsb;
+      pbin[l] = pb;
+    }
+  __syncthreads();
+  // wdwn(k) = (ww(k) + ww(k-1)) / 2 rdnw(k-1) (ph_1 + phb)(k) - (ph_1 + phb)(k-1),
+  // then the level's results
+  if (on) {
+    const float* fnm = s[WF_FNM];
+    const float* fnp = s[WF_FNP];
+    auto wdb = [&](int kk) {  // wdwn's cotangent at level kk (1 .. ktf)
+      float v = 0.f;
+      if (kk - 1 >= 1 && kk - 1 < ktf) v += -dts * fnm[kk - 1] * (A(RHSB, kk - 1) * msfty / mut);
+      if (kk >= 1 && kk < ktf) v += -dts * fnp[kk] * (A(RHSB, kk) * msfty / mut);
+      return v;
+    };
+#pragma unroll
+    for (int l = 0; l < kAwLevels; ++l) {
+      const int k = ty + kAwGroups * l;
+      if (k > ktf) continue;
+      float wwb = 0.f;
+      if (k >= 1) {
+        const float w = wdb(k);
+        if (w != 0.f) {
+          const float h = 0.5f * rdnw[k - 1];
+          const float dph = F(WF_PH_SAVE, k) - F(WF_PH_SAVE, k - 1) + F(WF_PHB, k) - F(WF_PHB, k - 1);
+          wwb += w * h * dph;
+          const float dphb = w * h * (F(WF_WW, k) + F(WF_WW, k - 1));
+          ph1b[l] += dphb;
+          phbb[l] += dphb;
+        }
+      }
+      if (k + 1 <= ktf) {
+        const float w = wdb(k + 1);
+        if (w != 0.f) {
+          const float h = 0.5f * rdnw[k];
+          const float dph = F(WF_PH_SAVE, k + 1) - F(WF_PH_SAVE, k) + F(WF_PHB, k + 1) - F(WF_PHB, k);
+          wwb += w * h * dph;
+          const float dphb = w * h * (F(WF_WW, k + 1) + F(WF_WW, k));
+          ph1b[l] += -dphb;
+          phbb[l] += -dphb;
+        }
+      }
+      if (wwb != 0.f) B(WF_WW, k) += wwb;
+      B(WF_PH_SAVE, k) += ph1b[l];
+      B(WF_PHB, k) += phbb[l];
+      B(WF_PH, k) = pbin[l];
+      B(WF_W, k) = wib[l];  // w(0) is replaced by the lower boundary value: wib = 0 there
+    }
   }
-  // t_2ave(k) = (0.5 ((1+e) t_2 + (1-e) t_2ave) + muave t0) / (muts (t0 + t_1)), k < ktf
-  for (int k = 0; k < ktf; ++k) {
-    const float T = tb[k] + t2ab[k];
-    const float t1 = F(WF_T_SAVE, k), Dm = muts * (t0 + t1);
-    const float ttb = T / Dm;
-    muaveb += T * t0 / Dm;
-    mutsb += -T * m.t2a[k] / muts;
-    B(WF_T_SAVE, k) += -T * m.t2a[k] / (t0 + t1);
-    B(WF_T, k) += ttb * 0.5f * ep1;
-    B(WF_T_2SAVE, k) = ttb * 0.5f * em1;
+  red[(0 * kAwGroups + ty) * 32 + tx] = mutb;
+  red[(1 * kAwGroups + ty) * 32 + tx] = mutsb;
+  red[(2 * kAwGroups + ty) * 32 + tx] = muaveb;
+  __syncthreads();
+  if (on && ty == 0) {
+    float m0 = 0.f, m1 = 0.f, m2 = 0.f;
+    for (int y = 0; y < kAwGroups; ++y) {
+      m0 += red[(0 * kAwGroups + y) * 32 + tx];
+      m1 += red[(1 * kAwGroups + y) * 32 + tx];
+      m2 += red[(2 * kAwGroups + y) * 32 + tx];
+    }
+    b[WF_MUT][c] += m0;
+    b[WF_MUTS][c] += m1;
+    b[WF_MUAVE][c] += m2;
+    work[c] = A(ZB, 0);
   }
-  for (int k = 0; k <= ktf; ++k) {
-    B(WF_PH_SAVE, k) += ph1b[k];
-    B(WF_PHB, k) += phbb[k];
-    B(WF_PH, k) = pb_in[k];
-    B(WF_W, k) = wib[k];  // w(0) is replaced by the lower boundary value: wib[0] = 0
-  }
-  b[WF_MUT][c] += mutb;
-  b[WF_MUTS][c] += mutsb;
-  b[WF_MUAVE][c] += muaveb;
-  work[c] = xb[0];
 }
 
 __global__ void k_advance_w_adj_bc(Grid g, S s, S b, const float* work) {
@@ -1186,8 +1362,14 @@ int launch_advance_w(const Grid& g, const S& s, float dts, cudaStream_t st) {
 }
 
 int launch_advance_w_adj(const Grid& g, const S& s, const S& b, float dts, float* work, cudaStream_t st) {
-  const dim3 b2(32, 4), b3(32, 4);
-  k_advance_w_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, dts, work);
+  const dim3 bl(32, kAwGroups), b3(32, 4);
+  const size_t smem = advance_w_adj_smem(g);
+  static size_t granted = 48 * 1024;
+  if (smem > granted) {
+    cudaFuncSetAttribute(k_advance_w_adj_lp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    granted = smem;
+  }
+  k_advance_w_adj_lp<<<dim3((g.nx + 31) / 32, g.ny), bl, smem, st>>>(g, s, b, dts, work);
   k_advance_w_adj_bc<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, work);
   return 2;
 }
