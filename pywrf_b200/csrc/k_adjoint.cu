@@ -1005,6 +1005,7 @@ __global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_adj_lp(Grid g, S s
   auto A = [&](int arr, int k) -> float& { return awsm[((size_t)arr * nz + k) * 32 + tx]; };
   float* red = awsm + (size_t)kAwArrays * nz * 32;  // [4][kAwGroups][32]
   enum { T2A, WD, RR, RHS, PP, XX, YY, ZZ, ZB, YB, PB, RHSB };
+  enum { CA = RHS, CAL = RHSB, CG = PB };
   const float ep1 = (float)(1.0 + (double)g.epssm), em1 = (float)(1.0 - (double)g.epssm);
   const float gf = (float)G, t0 = (float)T0;
   float muave = 0.f, muts = 1.f, mut = 1.f, msfty = 1.f;
@@ -1069,13 +1070,20 @@ __global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_adj_lp(Grid g, S s
                    minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f * F(WF_C2A, k - 1) * A(PP, k - 1) -
                            dts * gf * (2.0f * rm * F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * A(T2A, k - 1) + muave));
       }
+      // the solve's coefficients, staged for the sweeps (in arrays free until
+      // the reverse writes them: rhs is done, Pb and rhsb come later)
+      if (k >= 1 && k <= ktf) {
+        A(CA, k) = F(WF_A, k);
+        A(CAL, k) = F(WF_ALPHA, k);
+        A(CG, k) = F(WF_GAMMA, k);
+      }
     }
   __syncthreads();
   if (on && ty == 0) {  // the implicit solve's two sweeps
     A(YY, 0) = A(XX, 0);
-    for (int k = 1; k <= ktf; ++k) A(YY, k) = (A(XX, k) - F(WF_A, k) * A(YY, k - 1)) * F(WF_ALPHA, k);
+    for (int k = 1; k <= ktf; ++k) A(YY, k) = (A(XX, k) - A(CA, k) * A(YY, k - 1)) * A(CAL, k);
     A(ZZ, ktf) = A(YY, ktf);
-    for (int k = ktf - 1; k >= 1; --k) A(ZZ, k) = A(YY, k) - F(WF_GAMMA, k) * A(ZZ, k + 1);
+    for (int k = ktf - 1; k >= 1; --k) A(ZZ, k) = A(YY, k) - A(CG, k) * A(ZZ, k + 1);
     A(ZZ, 0) = A(YY, 0);
   }
   __syncthreads();
@@ -1126,23 +1134,24 @@ __global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_adj_lp(Grid g, S s
     float hb = 0.f;
     for (int y = 0; y < kAwGroups; ++y) hb += red[(3 * kAwGroups + y) * 32 + tx];
     red[(3 * kAwGroups) * 32 + tx] = hb;
-    // the transposed solve: z = y - gamma z(k+1) backwards, y = (x - a y(k-1)) alpha forwards
+    // the transposed solve: z = y - gamma z(k+1) backwards, y = (x - a y(k-1))
+    // alpha forwards; the coefficients' cotangents are formed per level after
+    // it from the sweeps' values kept in shared memory (zb in wd's array)
     float carry = 0.f;
     for (int k = 1; k <= ktf - 1; ++k) {
       const float zbk = A(ZB, k) + carry;
       A(YB, k) = zbk;
-      B(WF_GAMMA, k) += -A(ZZ, k + 1) * zbk;
-      carry = -F(WF_GAMMA, k) * zbk;
+      A(WD, k) = zbk;
+      carry = -A(CG, k) * zbk;
     }
     A(YB, ktf) = A(ZB, ktf) + carry;
     A(YB, 0) = A(ZB, 0);
     float yc = 0.f;
     for (int k = ktf; k >= 1; --k) {
       const float ybk = A(YB, k) + yc;
-      const float al = F(WF_ALPHA, k), ak = F(WF_A, k);
+      const float al = A(CAL, k), ak = A(CA, k);
       A(ZB, k) = al * ybk;  // xb
-      B(WF_A, k) += -A(YY, k - 1) * al * ybk;
-      B(WF_ALPHA, k) += (A(XX, k) - ak * A(YY, k - 1)) * ybk;
+      A(YB, k) = ybk;
       yc = -ak * al * ybk;
     }
     A(ZB, 0) = A(YB, 0) + yc;  // xb(0)
@@ -1158,6 +1167,12 @@ __global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_adj_lp(Grid g, S s
       if (k == ktf) {
         ph1b[l] += hbt / gf;
         phbb[l] += hbt / gf;
+      }
+      if (k >= 1) {  // the solve's coefficients
+        const float ybk = A(YB, k), al = A(CAL, k);
+        if (k <= ktf - 1) B(WF_GAMMA, k) += -A(ZZ, k + 1) * A(WD, k);
+        B(WF_A, k) += -A(YY, k - 1) * al * ybk;
+        B(WF_ALPHA, k) += (A(XX, k) - A(CA, k) * A(YY, k - 1)) * ybk;
       }
       float c2ab = 0.f, altb = 0.f, pbk = 0.f, t2ab = 0.f;
       if (k >= 1 && k < ktf) {  // the level's own terms
