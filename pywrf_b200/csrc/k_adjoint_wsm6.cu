@@ -541,7 +541,7 @@ __device__ void point_processes(T& t, T& q, T& qc, T& qi, T& qr, T& qs, T& qg, c
 // A_T (temperature), A_Q, A_QC, A_QI, A_QR, A_QS, A_QG, A_DEN, A_P and
 // A_DELZ hold the inputs and receive the results
 template <class T>
-__device__ void wsm6_column(const Col<T>& C, int km, float delt, bool skip_dead = false) {
+__device__ void wsm6_column(const Col<T>& C, int km, float delt, bool skip_dead = false, bool stop_at_points = false) {
   for (int k = 0; k < km; ++k) {
     const T q = C(A_Q, k), t = C(A_T, k);
     C(A_CPM, k) = val(q) >= F(QMIN) ? F(CPV) * q + (1.0f - q) * F(CPD) : cst<T>(F(CPD * (1.0 - QMIN) + CPV * QMIN));
@@ -627,14 +627,20 @@ __device__ void wsm6_column(const Col<T>& C, int km, float delt, bool skip_dead 
       C(A_R1, k) = den * qi;
     }
     nislfv(C, km, 2, A_R1, -1, dtcld, 0);
+    if (stop_at_points) {
+      // (one time-split loop only) the point processes' inputs stay in the
+      // column arrays, cloud ice from its sedimented mass in A_QI
+      for (int k = 0; k < km; ++k) C(A_QI, k) = vmax(C(A_R1, k) / C(A_DEN, k), 0.0f);
+      return;
+    }
     for (int k = 0; k < km; ++k) {
       T t = C(A_T, k), q = C(A_Q, k), qc = C(A_QC, k), qr = C(A_QR, k), qs = C(A_QS, k), qg = C(A_QG, k);
       const T den = C(A_DEN, k);
       T qi = vmax(C(A_R1, k) / den, 0.0f);
       // a level whose every operand has zero tangents keeps zero tangents
       // through the processes; its values are not needed when only the
-      // derivatives are wanted
-      if (skip_dead && !(live(t) || live(q) || live(qc) || live(qr) || live(qs) || live(qg) || live(den) ||
+      // derivatives are wanted and no later time-split loop reads them
+      if (skip_dead && it == nloop - 1 && !(live(t) || live(q) || live(qc) || live(qr) || live(qs) || live(qg) || live(den) ||
                          live(qi) || live(C(A_P, k)) || live(C(A_DENFAC, k)) || live(C(A_CPM, k)) ||
                          live(C(A_XL, k)) || live(C(A_QS0, k)) || live(C(A_QS1, k)) || live(C(A_RH0, k)) ||
                          live(C(A_RH1, k)) || live(C(A_SR3, k)) || live(C(A_SRS, k))))
@@ -772,7 +778,7 @@ __device__ __forceinline__ void put_input_cot(const Grid& g, const S& b, int c2,
 // cotangents are (or, after k_mp_tape_rev, will be) written: not when the
 // tape outgrew the capacity.
 __global__ void __launch_bounds__(kTapeBlock) k_mp_tape(Grid g, S s, S yb, S b, float dt, Tv* ws, TapeCtx tc,
-                                                        int c0, int nc, S vo, int* done, int* used) {
+                                                        int c0, int nc, S vo, int* done, int* used, bool split) {
   if (threadIdx.x == 0) g_tape = tc;
   __syncthreads();
   const int lane = tape_lane(), col = c0 + lane;
@@ -810,6 +816,16 @@ __global__ void __launch_bounds__(kTapeBlock) k_mp_tape(Grid g, S s, S yb, S b, 
   const Col<Tv> C{ws + lane, tc.stride, km + 1};
   tape_reserve(mp_inputs(g));
   prep_column(g, s, C, c2, [](int idx, float v) { return Tv{v, idx, 1.f}; });
+  if (split) {
+    // the point processes and finish are reversed per level by
+    // k_mp_points_adj, which seeds this tape's entries
+    wsm6_column(C, km, dt, false, true);
+    const int n = g_tape_n[threadIdx.x];
+    used[col] = n;
+    for (int k = 0; k < km; ++k) b[WF_H_DIABATIC][k * lev + c2] = 0.f;
+    if (n > tc.cap) done[col] = 0;
+    return;
+  }
   wsm6_column(C, km, dt);
   for (int k = 0; k < km; ++k) finish_level(C, k, dt);
   const int n = g_tape_n[threadIdx.x];
@@ -835,6 +851,87 @@ __global__ void __launch_bounds__(kTapeBlock) k_mp_tape(Grid g, S s, S yb, S b, 
     seed(C(A_TH, k), yb[WF_H_DIABATIC][p]);
     for (int m = 1; m < 7; ++m) seed(C(moist_slot(m), k), yb[WF_MOIST][m * n3 + p]);
   }
+}
+
+// The point processes and finish of one level of a column taped in split
+// mode, reversed by forward-mode tangents: one thread per (column, level)
+// reads the level's inputs from the column arrays k_mp_tape left (their
+// values, and the tape entries they are multiples of), evaluates the level
+// in Dual<N> arithmetic with N inputs seeded per pass, forms the inputs'
+// cotangents from the outputs' (yb: theta, qv .. qg, h_diabatic) and adds
+// them into the adjoints of those entries of the column's tape, which
+// k_mp_tape_rev then sweeps.  The level's processes read no other level, so
+// the chain a thread runs is one level's, not the column's.  vo (when its T
+// is not null) receives the level's output values.
+constexpr int kPointInputs = 21;
+template <int N>
+__global__ void __launch_bounds__(128) k_mp_points_adj(Grid g, S yb, Tv* ws, TapeCtx tc, int c0, int nc, S vo,
+                                                       const int* done, const int* used, float dt) {
+  const int km = g.nz - 1;
+  // neighbouring threads take neighbouring columns at one level: their
+  // column-array reads coalesce, and their branches mostly agree
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = (int)(t / nc), lane = (int)(t - (long long)k * nc);
+  if (k >= km) return;
+  const int col = c0 + lane;
+  const int n = used[col];
+  if (!done[col] || n == 0 || n > tc.cap) return;
+  ColPos cp;
+  col_pos(g, col, cp);
+  const Col<Tv> C{ws + lane, tc.stride, km + 1};
+  const int arr[kPointInputs] = {A_T,  A_Q,   A_QC,  A_QI,  A_QR,  A_QS,  A_QG,  A_DEN, A_P,  A_DENFAC, A_CPM,
+                                 A_XL, A_QS0, A_QS1, A_RH0, A_RH1, A_SR3, A_SRS, A_TIN, A_TH, A_PII};
+  Tv in[kPointInputs];
+#pragma unroll
+  for (int q = 0; q < kPointInputs; ++q) in[q] = C(arr[q], k);
+  const size_t lev = (size_t)g.ny * g.nx, n3 = g.n3(), p = k * lev + cp.c2;
+  const float yt = yb[WF_T][p], yh = yb[WF_H_DIABATIC][p];
+  float ym[7];
+#pragma unroll
+  for (int m = 1; m < 7; ++m) ym[m] = yb[WF_MOIST][m * n3 + p];
+  float cot[kPointInputs];
+#pragma unroll
+  for (int q = 0; q < kPointInputs; ++q) cot[q] = 0.f;
+  // the time-split loop's step (one loop: dt itself up to the split step)
+  const float loops = fmaxf(dt / F(DTCLDCR), 1.0f);
+  const float dtcld = dt <= F(DTCLDCR) ? dt : dt / loops;
+  using D = Dual<N>;
+  for (int j0 = 0; j0 < kPointInputs; j0 += N) {
+    D x[kPointInputs];
+#pragma unroll
+    for (int q = 0; q < kPointInputs; ++q) {
+      x[q] = dconst<N>(in[q].v);
+#pragma unroll
+      for (int d = 0; d < N; ++d)
+        if (q == j0 + d) x[q].d[d] = 1.f;
+    }
+    D tt = x[0], qv = x[1], qc = x[2], qi = x[3], qr = x[4], qs = x[5], qg = x[6];
+    Slope3<D> sl0;
+    sl0.r3[0] = x[16];
+    sl0.rs[0] = x[17];
+    point_processes(tt, qv, qc, qi, qr, qs, qg, x[7], x[8], x[9], x[10], x[11], x[12], x[13], x[14], x[15], sl0, dtcld);
+    // moist_physics_finish_em at the level
+    const D mpten = tt / x[20] - x[19];
+    const D tnew = x[18] + mpten;
+    const D h = mpten / dt;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const float v = yt * tnew.d[d] + yh * h.d[d] + ym[1] * qv.d[d] + ym[2] * qc.d[d] + ym[3] * qr.d[d] +
+                      ym[4] * qi.d[d] + ym[5] * qs.d[d] + ym[6] * qg.d[d];
+#pragma unroll
+      for (int q = 0; q < kPointInputs; ++q)
+        if (q == j0 + d) cot[q] += v;
+    }
+    if (j0 == 0 && vo[WF_T]) {
+      vo[WF_T][p] = tnew.v;
+      vo[WF_H_DIABATIC][p] = h.v;
+      const float mv[7] = {0.f, qv.v, qc.v, qr.v, qi.v, qs.v, qg.v};
+      for (int m = 1; m < 7; ++m) vo[WF_MOIST][m * n3 + p] = mv[m];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kPointInputs; ++q)
+    if (in[q].id >= 0 && cot[q] != 0.f) atomicAdd(tc.adj(in[q].id, lane), cot[q] * in[q].s);
 }
 
 // the reverse sweep of the tapes k_mp_tape left (same chunk and lanes):
@@ -902,9 +999,10 @@ __global__ void __launch_bounds__(64) k_mp_tangent(Grid g, S s, S yb, S b, int p
 namespace {
 
 constexpr int kMpDirections = 8;
-// entries a column's tape may take per level by default, and the memory
-// the tapes of one chunk of columns may take
-constexpr int kTapeEntriesPerLevel = 480;
+// entries a column's tape may take per level by default (per time-split
+// loop of the whole column; of the column-coupled part in split mode), and
+// the memory the tapes of one chunk of columns may take
+constexpr int kTapeEntriesPerLevel = 480, kTapeSplitPerLevel = 256;
 constexpr size_t kTapeChunkBytes = size_t(24) << 30;
 // the capacity set through set_microphysics_tape_capacity (0: default)
 int g_tape_capacity = 0;
@@ -922,8 +1020,12 @@ MpAdjWork mp_adj_work(const Grid& g) {
   MpAdjWork w;
   const int km = g.nz - 1;
   w.ncol = (g.ide - 1 - (g.ids + 1)) * (g.jde - 1 - (g.jds + 1));
+  // the tape holds the column-coupled part in split mode (one time-split
+  // loop), the whole column once per loop otherwise
+  const int nloop = (int)fmaxf(g.dt / F(mp::DTCLDCR), 1.0f);
+  const int per_level = nloop == 1 ? kTapeSplitPerLevel : kTapeEntriesPerLevel * nloop;
   w.cap = g_tape_capacity > 0 ? std::min(kTapeMaxEntries, g_tape_capacity)
-                              : std::min(kTapeMaxEntries, kTapeEntriesPerLevel * km + mpt::mp_inputs(g));
+                              : std::min(kTapeMaxEntries, per_level * km + mpt::mp_inputs(g));
   const size_t per_col = (size_t)w.cap * 16 + (size_t)mpt::A_COUNT * (km + 1) * sizeof(Tv);
   const size_t fit = std::max<size_t>(64, kTapeChunkBytes / per_col / 64 * 64);
   w.width = (int)std::min<size_t>(fit, ((size_t)w.ncol + 63) / 64 * 64);
@@ -971,10 +1073,18 @@ int launch_physics_adj(const Grid& g, const S& s, const S& post, const S& b, flo
   tc.stride = w.width;
   tc.cap = w.cap;
   auto* cols = reinterpret_cast<Tv*>(work + w.cols);
+  // one time-split loop: the point processes are reversed per level
+  const bool split = (int)fmaxf(dt / F(mp::DTCLDCR), 1.0f) == 1;
+  const int km = g.nz - 1;
   for (int c0 = 0; c0 < w.ncol; c0 += w.width) {
     const int nc = std::min(w.width, w.ncol - c0);
     mpt::k_mp_tape<<<(nc + kTapeBlock - 1) / kTapeBlock, kTapeBlock, 0, st>>>(g, s, yb, b, dt, cols, tc, c0, nc, vo,
-                                                                               done, used);
+                                                                               done, used, split);
+    if (split) {
+      const long long nt = (long long)nc * km;
+      mpt::k_mp_points_adj<4><<<(unsigned)((nt + 127) / 128), 128, 0, st>>>(g, yb, cols, tc, c0, nc, vo, done, used, dt);
+      ++n;
+    }
     mpt::k_mp_tape_rev<<<(nc + mpt::kSweepBlock - 1) / mpt::kSweepBlock, mpt::kSweepBlock, 0, st>>>(g, b, tc, c0, nc,
                                                                                                     used);
     n += 2;

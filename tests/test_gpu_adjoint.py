@@ -1384,22 +1384,28 @@ def _microphysics_state_before_step2():
     return g, snap
 
 
-def test_microphysics_adjoint_tape_and_tangent_columns_agree():
+@pytest.mark.parametrize("dt, mixed", [(None, (1400, 2000)), (150.0, ()), (250.0, (5000,))])
+def test_microphysics_adjoint_tape_and_tangent_columns_agree(dt, mixed):
     """wrf_microphysics_adj with the tape capacity at its default (every
-    column taped), at 1 (every column by forward-mode tangents) and at 3000
-    and 4500 entries (on this 16-level case, whose columns take 2 800 to
-    5 600 entries, the columns whose tape outgrows the capacity go to the
-    tangents and the rest are taped, in one call): the input cotangents agree to float32 summation order (relative
-    L2 1e-5 per field), and the setting is restored."""
+    column taped) against capacity 1 (every column by forward-mode
+    tangents) and, where listed, capacities that send only the columns with
+    the longest tapes to the tangents (a mix in one call), at the case's dt
+    of 45 s (one time-split loop: the tape stops before the point
+    processes, which are reversed per level; its columns take 1 400 to
+    2 600 entries here), 150 s (one loop of 120 s, the same split) and 250 s
+    (two loops: the whole column on the tape twice): the input cotangents
+    agree to float32 summation order (relative L2 1e-5 per field), and the
+    setting is restored."""
     from pywrf_b200 import _native as N
 
     g, snap = _microphysics_state_before_step2()
+    dt = float(g.dt if dt is None else dt)
     names = adjoint._Microphysics.fields
     st = {k: _cuda(snap[k]) for k in names}
     data = {k: _cuda(snap[k]) for k in adjoint._Microphysics.data}
-    out = adjoint.microphysics(st, data, g.dt, g.rdx, g.rdy)
+    out = adjoint.microphysics(st, data, dt, g.rdx, g.rdy)
     cg = adjoint.scalar_grid(st["t"].shape, g.rdx, g.rdy)
-    cg.dt = float(g.dt)
+    cg.dt = dt
     tab = adjoint._table({**st, **data})
     post = adjoint._table({**st, **data, **{k: out[k].detach() for k in ("t", "moist", "al", "p")}})
     gen = torch.Generator(device="cuda").manual_seed(5)
@@ -1428,7 +1434,7 @@ def test_microphysics_adjoint_tape_and_tangent_columns_agree():
 
     taped = reverse(0)
     bad = []
-    for cap in (1, 3000, 4500):
+    for cap in (1,) + tuple(mixed):
         other = reverse(cap)
         for k in ("t", "moist", "al", "p", "ph", "mu", "muts"):
             e = rel_l2(other[k], taped[k])
