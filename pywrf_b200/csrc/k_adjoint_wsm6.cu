@@ -16,6 +16,10 @@
 // The reverse product is taken in reverse mode: the column runs once on
 // taped scalars (tape.cuh), the outputs' cotangents seed the adjoints of
 // their entries, and one reverse sweep yields every input's cotangent.
+// With one time-split loop (split mode) the tape stops before the point
+// processes: those read only their own level, so each level's are reversed
+// on a thread of its own by forward-mode tangents and added into the
+// adjoints of the tape entries its inputs come from, before the sweep.
 // Columns are taped in chunks that bound the tape's memory.  A column whose
 // tape outgrows the capacity is finished by forward-mode tangents instead:
 // the same code on Dual<N> numbers with N inputs seeded per pass, the
