@@ -92,7 +92,7 @@
 //                        input of the same name and nothing to dmdt, mut or
 //                        mu_tend).
 //
-//   k_advance_w / k_advance_w_adj_lp / k_advance_w_adj_bc  advance_w
+//   k_advance_w_lp / k_advance_w_adj_lp / k_advance_w_adj_bc  advance_w
 //                        (wrf_dynamics.py:3641-3796) on the columns [ids+1,
 //                        ide-2) x [jds+1, jde-2): t_2ave, the right-hand side
 //                        rhs = ph + msfty R / mut (R from ph_tend, w and the
@@ -877,11 +877,6 @@ namespace {
 constexpr float kAwHdepth = 5000.0f;
 
 // one column's forward values
-struct AwCol {
-  float t2a[kMaxNz], wd[kMaxNz], R[kMaxNz], rhs[kMaxNz], P[kMaxNz], x[kMaxNz], y[kMaxNz], z[kMaxNz], d[kMaxNz],
-      wf[kMaxNz], hk[kMaxNz];
-  float hbot;
-};
 
 __device__ float aw_bc(const Grid& g, const S& s, int j, int i) {
   const int nx = g.nx;
@@ -895,87 +890,8 @@ __device__ float aw_bc(const Grid& g, const S& s, int j, int i) {
          s[WF_MSFTX][c] * 0.5f * g.rdx * ((ht[c + 1] - ht[c]) * cu(c + 1) + (ht[c] - ht[c - 1]) * cu(c));
 }
 
-__device__ void aw_column(const Grid& g, const S& s, float dts, int j, int i, AwCol& m) {
-  const int ktf = g.nz - 1;
-  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
-  const float ep1 = (float)(1.0 + (double)g.epssm), em1 = (float)(1.0 - (double)g.epssm);
-  const float gf = (float)G, t0 = (float)T0;
-  const float muave = s[WF_MUAVE][c], muts = s[WF_MUTS][c], mut = s[WF_MUT][c], msfty = s[WF_MSFTY][c];
-  const float* rdnw = s[WF_RDNW];
-  const float* rdn = s[WF_RDN];
-  auto F = [&](int id, int k) { return s[id][k * lev + c]; };
-  for (int k = 0; k < ktf; ++k) {
-    const float tt = 0.5f * (ep1 * F(WF_T, k) + em1 * F(WF_T_2SAVE, k));
-    m.t2a[k] = (tt + muave * t0) / (muts * (t0 + F(WF_T_SAVE, k)));
-  }
-  m.wd[0] = 0.f;
-  for (int k = 1; k <= ktf; ++k)
-    m.wd[k] = 0.5f * (F(WF_WW, k) + F(WF_WW, k - 1)) * rdnw[k - 1] *
-              (F(WF_PH_SAVE, k) - F(WF_PH_SAVE, k - 1) + F(WF_PHB, k) - F(WF_PHB, k - 1));
-  m.rhs[0] = 0.f;
-  for (int k = 1; k <= ktf; ++k) {
-    float r = dts * (F(WF_PH_TEND, k) + 0.5f * gf * em1 * F(WF_W, k));
-    if (k < ktf) r = r - dts * (s[WF_FNM][k] * m.wd[k + 1] + s[WF_FNP][k] * m.wd[k]);
-    m.R[k] = r;
-    m.rhs[k] = F(WF_PH, k) + msfty * r / mut;
-  }
-  for (int k = 0; k < ktf; ++k)
-    m.P[k] = ep1 * (m.rhs[k + 1] - m.rhs[k]) + em1 * (F(WF_PH, k + 1) - F(WF_PH, k));
-  const float minv = 1.0f / msfty;
-  m.x[0] = aw_bc(g, s, j, i);
-  for (int k = 1; k < ktf; ++k) {
-    const float X1 = F(WF_C2A, k) * rdnw[k] / mut * m.P[k];
-    const float X2 = F(WF_C2A, k - 1) * rdnw[k - 1] / mut * m.P[k - 1];
-    m.x[k] = F(WF_W, k) + dts * F(WF_RW_TEND, k) + minv * F(WF_CQW, k) * (0.5f * dts * gf * rdn[k] * (X1 - X2)) +
-             dts * gf * minv *
-                 (rdn[k] * (F(WF_C2A, k) * F(WF_ALT, k) * m.t2a[k] - F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * m.t2a[k - 1]) -
-                  muave);
-  }
-  {
-    const int k = ktf;
-    const float rm = rdnw[k - 1];
-    m.x[k] = F(WF_W, k) + dts * F(WF_RW_TEND, k) +
-             minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f * F(WF_C2A, k - 1) * m.P[k - 1] -
-                     dts * gf * (2.0f * rm * F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * m.t2a[k - 1] + muave));
-  }
-  m.y[0] = m.x[0];
-  for (int k = 1; k <= ktf; ++k) m.y[k] = (m.x[k] - F(WF_A, k) * m.y[k - 1]) * F(WF_ALPHA, k);
-  m.z[ktf] = m.y[ktf];
-  for (int k = ktf - 1; k >= 1; --k) m.z[k] = m.y[k] - F(WF_GAMMA, k) * m.z[k + 1];
-  m.z[0] = m.y[0];
-  const float dampmag = (float)((double)dts * 0.2), hpi = (float)(0.5 * 3.14159265359);
-  m.hbot = (F(WF_PH_SAVE, ktf) + F(WF_PHB, ktf)) / gf - kAwHdepth;
-  m.wf[0] = m.z[0];
-  for (int k = 1; k <= ktf; ++k) {
-    m.hk[k] = (F(WF_PH_SAVE, k) + F(WF_PHB, k)) / gf;
-    float dw = 0.f;
-    if (m.hk[k] >= m.hbot) {
-      const float sn = sinf(hpi * (m.hk[k] - m.hbot) / kAwHdepth);
-      dw = dampmag * (sn * sn);
-    }
-    m.d[k] = dw;
-    m.wf[k] = (m.z[k] - dw * mut * F(WF_W_SAVE, k)) / (1.0f + dw);
-  }
-}
 
 }  // namespace
-
-__global__ void k_advance_w(Grid g, S s, float dts) {
-  WRF_COLUMN_INDEX(g, j, i);
-  if (!mut_in(g, j, i)) return;
-  const int ktf = g.nz - 1;
-  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
-  AwCol m;
-  aw_column(g, s, dts, j, i, m);
-  const float ep1 = (float)(1.0 + (double)g.epssm), gf = (float)G;
-  const float muts = s[WF_MUTS][c], msfty = s[WF_MSFTY][c];
-  for (int k = 0; k < ktf; ++k) s[WF_T_2SAVE][k * lev + c] = m.t2a[k];
-  s[WF_W][c] = m.wf[0];
-  for (int k = 1; k <= ktf; ++k) {
-    s[WF_W][k * lev + c] = m.wf[k];
-    s[WF_PH][k * lev + c] = m.rhs[k] + msfty * 0.5f * dts * gf * ep1 * m.wf[k] / muts;
-  }
-}
 
 // advance_w's reverse with a column's levels spread over the threads of a
 // block: 32 adjacent columns of one row (threadIdx.x) x kAwGroups level
@@ -995,6 +911,100 @@ constexpr int kAwArrays = 12;  // t2a, wd, R, rhs, P, x, y, z, zb (then xb), yb,
 
 size_t advance_w_adj_smem(const Grid& g) { return ((size_t)kAwArrays * g.nz * 32 + 4 * kAwGroups * 32) * sizeof(float); }
 
+// the forward recomputation of advance_w over a block's level groups, in
+// the reference's order: t_2ave, wdwn, R, rhs, P and the explicit w x in
+// the column arrays, then the solve's two sweeps (y, z) on group 0, the
+// solve's coefficients staged first; ends with the block synchronised
+struct AwLp {
+  const Grid& g;
+  const S& s;
+  float* sm;
+  int nz, ktf, tx, ty;
+  bool on;
+  size_t lev, c;
+  int j, i;
+  float dts, ep1, em1, gf, t0, muave, muts, mut, msfty, minv;
+  enum { T2A, WD, RR, RHS, PP, XX, YY, ZZ, ZB, YB, PB, RHSB };
+  enum { CA = RHS, CAL = RHSB, CG = PB };
+  __device__ float& A(int arr, int k) const { return sm[((size_t)arr * nz + k) * 32 + tx]; }
+  __device__ float F(int id, int k) const { return s[id][k * lev + c]; }
+  __device__ void forward() const {
+    const float* rdnw = s[WF_RDNW];
+    const float* rdn = s[WF_RDN];
+    if (on)
+  #pragma unroll
+      for (int l = 0; l < kAwLevels; ++l) {
+        const int k = ty + kAwGroups * l;
+        if (k < ktf) {
+          const float tt = 0.5f * (ep1 * F(WF_T, k) + em1 * F(WF_T_2SAVE, k));
+          A(T2A, k) = (tt + muave * t0) / (muts * (t0 + F(WF_T_SAVE, k)));
+        }
+        if (k == 0) A(WD, 0) = 0.f;
+        if (k >= 1 && k <= ktf)
+          A(WD, k) = 0.5f * (F(WF_WW, k) + F(WF_WW, k - 1)) * rdnw[k - 1] *
+                     (F(WF_PH_SAVE, k) - F(WF_PH_SAVE, k - 1) + F(WF_PHB, k) - F(WF_PHB, k - 1));
+      }
+    __syncthreads();
+    if (on)
+  #pragma unroll
+      for (int l = 0; l < kAwLevels; ++l) {
+        const int k = ty + kAwGroups * l;
+        if (k == 0) A(RHS, 0) = 0.f;
+        if (k >= 1 && k <= ktf) {
+          float r = dts * (F(WF_PH_TEND, k) + 0.5f * gf * em1 * F(WF_W, k));
+          if (k < ktf) r = r - dts * (s[WF_FNM][k] * A(WD, k + 1) + s[WF_FNP][k] * A(WD, k));
+          A(RR, k) = r;
+          A(RHS, k) = F(WF_PH, k) + msfty * r / mut;
+        }
+      }
+    __syncthreads();
+    if (on)
+  #pragma unroll
+      for (int l = 0; l < kAwLevels; ++l) {
+        const int k = ty + kAwGroups * l;
+        if (k < ktf) A(PP, k) = ep1 * (A(RHS, k + 1) - A(RHS, k)) + em1 * (F(WF_PH, k + 1) - F(WF_PH, k));
+      }
+    __syncthreads();
+    if (on)
+  #pragma unroll
+      for (int l = 0; l < kAwLevels; ++l) {
+        const int k = ty + kAwGroups * l;
+        if (k == 0) A(XX, 0) = aw_bc(g, s, j, i);
+        if (k >= 1 && k < ktf) {
+          const float X1 = F(WF_C2A, k) * rdnw[k] / mut * A(PP, k);
+          const float X2 = F(WF_C2A, k - 1) * rdnw[k - 1] / mut * A(PP, k - 1);
+          A(XX, k) = F(WF_W, k) + dts * F(WF_RW_TEND, k) + minv * F(WF_CQW, k) * (0.5f * dts * gf * rdn[k] * (X1 - X2)) +
+                     dts * gf * minv *
+                         (rdn[k] * (F(WF_C2A, k) * F(WF_ALT, k) * A(T2A, k) -
+                                    F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * A(T2A, k - 1)) -
+                          muave);
+        }
+        if (k == ktf) {
+          const float rm = rdnw[k - 1];
+          A(XX, k) = F(WF_W, k) + dts * F(WF_RW_TEND, k) +
+                     minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f * F(WF_C2A, k - 1) * A(PP, k - 1) -
+                             dts * gf * (2.0f * rm * F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * A(T2A, k - 1) + muave));
+        }
+        // the solve's coefficients, staged for the sweeps (in arrays free until
+        // the reverse writes them: rhs is done, Pb and rhsb come later)
+        if (k >= 1 && k <= ktf) {
+          A(CA, k) = F(WF_A, k);
+          A(CAL, k) = F(WF_ALPHA, k);
+          A(CG, k) = F(WF_GAMMA, k);
+        }
+      }
+    __syncthreads();
+    if (on && ty == 0) {  // the implicit solve's two sweeps
+      A(YY, 0) = A(XX, 0);
+      for (int k = 1; k <= ktf; ++k) A(YY, k) = (A(XX, k) - A(CA, k) * A(YY, k - 1)) * A(CAL, k);
+      A(ZZ, ktf) = A(YY, ktf);
+      for (int k = ktf - 1; k >= 1; --k) A(ZZ, k) = A(YY, k) - A(CG, k) * A(ZZ, k + 1);
+      A(ZZ, 0) = A(YY, 0);
+    }
+    __syncthreads();
+  }
+};
+
 __global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_adj_lp(Grid g, S s, S b, float dts, float* work) {
   extern __shared__ float awsm[];
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -1002,10 +1012,7 @@ __global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_adj_lp(Grid g, S s
   const bool on = i < g.nx && j < g.ny && mut_in(g, j, i);
   const int nz = g.nz, ktf = nz - 1;
   const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + (on ? i : 0);
-  auto A = [&](int arr, int k) -> float& { return awsm[((size_t)arr * nz + k) * 32 + tx]; };
   float* red = awsm + (size_t)kAwArrays * nz * 32;  // [4][kAwGroups][32]
-  enum { T2A, WD, RR, RHS, PP, XX, YY, ZZ, ZB, YB, PB, RHSB };
-  enum { CA = RHS, CAL = RHSB, CG = PB };
   const float ep1 = (float)(1.0 + (double)g.epssm), em1 = (float)(1.0 - (double)g.epssm);
   const float gf = (float)G, t0 = (float)T0;
   float muave = 0.f, muts = 1.f, mut = 1.f, msfty = 1.f;
@@ -1013,80 +1020,14 @@ __global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_adj_lp(Grid g, S s
   const float minv = 1.0f / msfty;
   const float* rdnw = s[WF_RDNW];
   const float* rdn = s[WF_RDN];
+  const AwLp L{g, s, awsm, nz, ktf, tx, ty, on, lev, c, j, i, dts, ep1, em1, gf, t0, muave, muts, mut, msfty, minv};
+  auto A = [&](int arr, int k) -> float& { return L.A(arr, k); };
   auto F = [&](int id, int k) { return s[id][k * lev + c]; };
   auto B = [&](int id, int k) -> float& { return b[id][k * lev + c]; };
-  // ---- forward recomputation (aw_column)
-  if (on)
-#pragma unroll
-    for (int l = 0; l < kAwLevels; ++l) {
-      const int k = ty + kAwGroups * l;
-      if (k < ktf) {
-        const float tt = 0.5f * (ep1 * F(WF_T, k) + em1 * F(WF_T_2SAVE, k));
-        A(T2A, k) = (tt + muave * t0) / (muts * (t0 + F(WF_T_SAVE, k)));
-      }
-      if (k == 0) A(WD, 0) = 0.f;
-      if (k >= 1 && k <= ktf)
-        A(WD, k) = 0.5f * (F(WF_WW, k) + F(WF_WW, k - 1)) * rdnw[k - 1] *
-                   (F(WF_PH_SAVE, k) - F(WF_PH_SAVE, k - 1) + F(WF_PHB, k) - F(WF_PHB, k - 1));
-    }
-  __syncthreads();
-  if (on)
-#pragma unroll
-    for (int l = 0; l < kAwLevels; ++l) {
-      const int k = ty + kAwGroups * l;
-      if (k == 0) A(RHS, 0) = 0.f;
-      if (k >= 1 && k <= ktf) {
-        float r = dts * (F(WF_PH_TEND, k) + 0.5f * gf * em1 * F(WF_W, k));
-        if (k < ktf) r = r - dts * (s[WF_FNM][k] * A(WD, k + 1) + s[WF_FNP][k] * A(WD, k));
-        A(RR, k) = r;
-        A(RHS, k) = F(WF_PH, k) + msfty * r / mut;
-      }
-    }
-  __syncthreads();
-  if (on)
-#pragma unroll
-    for (int l = 0; l < kAwLevels; ++l) {
-      const int k = ty + kAwGroups * l;
-      if (k < ktf) A(PP, k) = ep1 * (A(RHS, k + 1) - A(RHS, k)) + em1 * (F(WF_PH, k + 1) - F(WF_PH, k));
-    }
-  __syncthreads();
-  if (on)
-#pragma unroll
-    for (int l = 0; l < kAwLevels; ++l) {
-      const int k = ty + kAwGroups * l;
-      if (k == 0) A(XX, 0) = aw_bc(g, s, j, i);
-      if (k >= 1 && k < ktf) {
-        const float X1 = F(WF_C2A, k) * rdnw[k] / mut * A(PP, k);
-        const float X2 = F(WF_C2A, k - 1) * rdnw[k - 1] / mut * A(PP, k - 1);
-        A(XX, k) = F(WF_W, k) + dts * F(WF_RW_TEND, k) + minv * F(WF_CQW, k) * (0.5f * dts * gf * rdn[k] * (X1 - X2)) +
-                   dts * gf * minv *
-                       (rdn[k] * (F(WF_C2A, k) * F(WF_ALT, k) * A(T2A, k) -
-                                  F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * A(T2A, k - 1)) -
-                        muave);
-      }
-      if (k == ktf) {
-        const float rm = rdnw[k - 1];
-        A(XX, k) = F(WF_W, k) + dts * F(WF_RW_TEND, k) +
-                   minv * (-0.5f * dts * gf / mut * (rm * rm) * 2.0f * F(WF_C2A, k - 1) * A(PP, k - 1) -
-                           dts * gf * (2.0f * rm * F(WF_C2A, k - 1) * F(WF_ALT, k - 1) * A(T2A, k - 1) + muave));
-      }
-      // the solve's coefficients, staged for the sweeps (in arrays free until
-      // the reverse writes them: rhs is done, Pb and rhsb come later)
-      if (k >= 1 && k <= ktf) {
-        A(CA, k) = F(WF_A, k);
-        A(CAL, k) = F(WF_ALPHA, k);
-        A(CG, k) = F(WF_GAMMA, k);
-      }
-    }
-  __syncthreads();
-  if (on && ty == 0) {  // the implicit solve's two sweeps
-    A(YY, 0) = A(XX, 0);
-    for (int k = 1; k <= ktf; ++k) A(YY, k) = (A(XX, k) - A(CA, k) * A(YY, k - 1)) * A(CAL, k);
-    A(ZZ, ktf) = A(YY, ktf);
-    for (int k = ktf - 1; k >= 1; --k) A(ZZ, k) = A(YY, k) - A(CG, k) * A(ZZ, k + 1);
-    A(ZZ, 0) = A(YY, 0);
-  }
-  __syncthreads();
+  enum { T2A = AwLp::T2A, WD = AwLp::WD, RR = AwLp::RR, PP = AwLp::PP, XX = AwLp::XX, YY = AwLp::YY,
+         ZZ = AwLp::ZZ, ZB = AwLp::ZB, YB = AwLp::YB, PB = AwLp::PB, RHSB = AwLp::RHSB, CA = AwLp::CA,
+         CAL = AwLp::CAL, CG = AwLp::CG };
+  L.forward();
   // ---- reverse
   const float dampmag = (float)((double)dts * 0.2), hpi = (float)(0.5 * 3.14159265359);
   const float cph = msfty * 0.5f * dts * gf * ep1;
@@ -1335,6 +1276,48 @@ __global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_adj_lp(Grid g, S s
   }
 }
 
+// advance_w forward over a block's level groups (the stand-alone operator;
+// in the step k_acoustic_col does this work): the recomputation above, then
+// per level the Rayleigh damping, w and the phi update
+__global__ void __launch_bounds__(32 * kAwGroups) k_advance_w_lp(Grid g, S s, float dts) {
+  extern __shared__ float awsm[];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.x * 32 + tx, j = blockIdx.y;
+  const bool on = i < g.nx && j < g.ny && mut_in(g, j, i);
+  const int nz = g.nz, ktf = nz - 1;
+  const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + (on ? i : 0);
+  const float ep1 = (float)(1.0 + (double)g.epssm), em1 = (float)(1.0 - (double)g.epssm);
+  const float gf = (float)G, t0 = (float)T0;
+  float muave = 0.f, muts = 1.f, mut = 1.f, msfty = 1.f;
+  if (on) muave = s[WF_MUAVE][c], muts = s[WF_MUTS][c], mut = s[WF_MUT][c], msfty = s[WF_MSFTY][c];
+  const AwLp L{g, s, awsm, nz, ktf, tx, ty, on, lev, c, j, i, dts, ep1, em1, gf, t0, muave, muts, mut, msfty,
+               1.0f / msfty};
+  L.forward();
+  if (!on) return;
+  const float dampmag = (float)((double)dts * 0.2), hpi = (float)(0.5 * 3.14159265359);
+  const float hbot = (L.F(WF_PH_SAVE, ktf) + L.F(WF_PHB, ktf)) / gf - kAwHdepth;
+#pragma unroll
+  for (int l = 0; l < kAwLevels; ++l) {
+    const int k = ty + kAwGroups * l;
+    if (k > ktf) continue;
+    if (k < ktf) s[WF_T_2SAVE][k * lev + c] = L.A(AwLp::T2A, k);
+    if (k == 0) {
+      s[WF_W][c] = L.A(AwLp::ZZ, 0);
+      continue;
+    }
+    const float hk = (L.F(WF_PH_SAVE, k) + L.F(WF_PHB, k)) / gf;
+    float dw = 0.f;
+    if (hk >= hbot) {
+      const float sn = sinf(hpi * (hk - hbot) / kAwHdepth);
+      dw = dampmag * (sn * sn);
+    }
+    const float wf = (L.A(AwLp::ZZ, k) - dw * mut * L.F(WF_W_SAVE, k)) / (1.0f + dw);
+    const float rhs = L.F(WF_PH, k) + msfty * L.A(AwLp::RR, k) / mut;
+    s[WF_W][k * lev + c] = wf;
+    s[WF_PH][k * lev + c] = rhs + msfty * 0.5f * dts * gf * ep1 * wf / muts;
+  }
+}
+
 __global__ void k_advance_w_adj_bc(Grid g, S s, S b, const float* work) {
   WRF_POINT_INDEX(g, k, j, i);
   if (k > 2) return;
@@ -1371,8 +1354,13 @@ __global__ void k_advance_w_adj_bc(Grid g, S s, S b, const float* work) {
 }
 
 int launch_advance_w(const Grid& g, const S& s, float dts, cudaStream_t st) {
-  const dim3 b2(32, 4);
-  k_advance_w<<<col_grid(g, b2), b2, 0, st>>>(g, s, dts);
+  const size_t smem = advance_w_adj_smem(g);
+  static size_t granted = 48 * 1024;
+  if (smem > granted) {
+    cudaFuncSetAttribute(k_advance_w_lp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    granted = smem;
+  }
+  k_advance_w_lp<<<dim3((g.nx + 31) / 32, g.ny), dim3(32, kAwGroups), smem, st>>>(g, s, dts);
   return 1;
 }
 
