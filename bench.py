@@ -29,6 +29,10 @@ Extra keys of the JSON line:
                 timed on this host for one step of the same workload
   reference_cpu the unmodified reference's own CPU step, recorded where its
                 source lives (tests/golden/reference_cpu_timing.json)
+  reference_gpu the unmodified reference's own PyTorch step on a B200,
+                recorded by tests/golden/time_reference_gpu.py
+                (tests/golden/reference_gpu_timing.json), with this run's
+                value and e2e as ratios to it
   config4       the 512x512x61 workload's plain step (36 steps): steps/s,
                 ledger fraction, peak device memory
   clocks        SM clock samples taken during the timed region
@@ -194,6 +198,26 @@ def reference_cpu_record(grid_key: str):
             "machine": f"{d['cpu']} ({d['logical_cpus']} logical CPUs), torch {d['torch']}, {d['dtype']}",
             "sample": f"{w['timed_steps']} timed step(s) after {w['warmup_steps']} warm-up",
             "recorded_in": "tests/golden/reference_cpu_timing.json (not measured in this run)"}
+
+
+def reference_gpu_record(grid_key: str, value: float, e2e: float | None):
+    """The unmodified reference's own PyTorch step on a B200 on this
+    workload, as timed by tests/golden/time_reference_gpu.py (its solver
+    loop on cuda:0, float32; a recorded measurement, not of this run), with
+    the ratios of this run's device-resident and end-to-end figures to it."""
+    p = os.path.join(ROOT, "tests", "golden", "reference_gpu_timing.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        w = d["workloads"][grid_key]
+    except (OSError, KeyError, ValueError):
+        return None
+    return {"value": w["steps_per_s"], "unit": UNIT, "device": d["device"],
+            "machine": f"torch {d['torch']}, {d['dtype']}",
+            "sample": f"{w['timed_steps']} timed step(s) after {w['warmup_steps']} warm-up",
+            "recorded_in": "tests/golden/reference_gpu_timing.json (not measured in this run)",
+            "value_ratio": value / w["steps_per_s"],
+            "e2e_ratio": (e2e / w["steps_per_s"]) if e2e else None}
 
 
 def run_reference(a):
@@ -413,6 +437,8 @@ def run_ours(a):
                 "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan,
                 "surrogate": sur, "config4": big,
                 "reference_cpu": reference_cpu_record(f"{g.nx}x{g.ny}x{g.nz}"),
+                "reference_gpu": reference_gpu_record(f"{g.nx}x{g.ny}x{g.nz}", value,
+                                                      e2e["value"] if e2e else None),
                 "adjoint": adj}
         line["valid"] = nan == 0
         print(json.dumps(line), flush=True)
