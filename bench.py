@@ -25,8 +25,11 @@ Extra keys of the JSON line:
   e2e           the same metric through the public API with host buffers
                 (Integrator.run_host): every step the pinned H2D of the
                 prognostic state, the step, the D2H of it back
-  cpu_baseline  the numpy oracle (a restatement of the reference's CPU path)
-                timed on this host for one step of the same workload
+  cpu_baseline  the unmodified reference (installed offline in
+                baseline/_ref) on this host's CPU threads, one step of the
+                same workload; where the install is absent, the numpy oracle
+  cpu_baseline_port  the numpy oracle (a restatement of the reference's
+                algorithm) on one host thread, one step
   reference_cpu the unmodified reference's own CPU step, recorded where its
                 source lives (tests/golden/reference_cpu_timing.json)
   reference_gpu the unmodified reference's own PyTorch step on a B200,
@@ -183,6 +186,44 @@ def cpu_reference_step_time(config: int, nsteps: int, warmup: int):
     return dt, f"{nsteps} RK3 step(s) of the {g.nx}x{g.ny}x{g.nz} workload, numpy fp32 oracle, 1 thread"
 
 
+REF_INSTALL = os.path.join(ROOT, "baseline", "_ref")
+
+
+def reference_host_step_time(config: int, nsteps: int, warmup: int):
+    """Seconds per step of the unmodified reference -- installed offline in
+    baseline/_ref, run through its own solver loop by
+    tests/golden/refharness.py (float32, torch on the CPU with all host
+    threads) -- on the same workload: the difference of a solve of
+    ``warmup`` steps and one of ``warmup + nsteps`` steps, after a
+    first-touch solve.  Returns (seconds, threads, sample) or None when the
+    install is absent."""
+    if not os.path.isfile(os.path.join(REF_INSTALL, "pywrf", "solver.py")):
+        return None
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import refharness
+    from pywrf_b200 import synthetic
+    refharness.REF_ROOT = REF_INSTALL
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    spec = synthetic.spec_for_config(config)
+    g = synthetic.grid_for(spec)
+    inputs, bdy = synthetic.build(spec)
+
+    def solve(n):
+        t0 = time.perf_counter()
+        refharness.run_reference(g, inputs, bdy, n, dtype="float32", device="cpu")
+        return time.perf_counter() - t0
+
+    w = max(1, warmup)
+    solve(1)
+    t_w = solve(w)
+    t_wk = solve(w + nsteps)
+    sec = (t_wk - t_w) / nsteps
+    return sec, threads, (f"{nsteps} RK3 step(s) of the {g.nx}x{g.ny}x{g.nz} workload after {w} warm-up, the "
+                          f"unmodified reference (baseline/_ref, float32) on {threads} host threads")
+
+
 def reference_cpu_record(grid_key: str):
     """The unmodified reference's own CPU step on this workload, as timed by
     tests/golden/time_reference_cpu.py where the reference's source lives (a
@@ -227,13 +268,19 @@ def run_reference(a):
     # bounded sample: each oracle step of this workload is tens of seconds of
     # CPU work, so at most 1 warm-up and 2 timed steps are run
     k, w = max(1, min(a.steps, 2)), min(a.warmup, 1)
-    sec, sample = cpu_reference_step_time(a.config, k, w)
+    ref = reference_host_step_time(a.config, k, w)
+    if ref is not None:
+        sec, cores, sample = ref
+        kind = "reference"
+    else:  # the reference's install is absent: its algorithm by the numpy port
+        sec, sample = cpu_reference_step_time(a.config, k, w)
+        cores, kind = 1, "port"
     v = 1.0 / sec
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": k, "warmup": w,
             "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "parallelism": "replicas"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -419,10 +466,16 @@ def run_ours(a):
         adj = run_adjoint_step(st, it, ms_max / a.steps)
         adj["acoustic_stage"] = run_adjoint_stage(st, it, phase_ms)
 
-    cpu = None
+    cpu = cpu_port = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         sec, sample = cpu_reference_step_time(a.config, 1, 0)
-        cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
+        cpu_port = {"value": 1.0 / sec, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
+        ref = reference_host_step_time(a.config, 1, 1)
+        if ref is not None:
+            sec, cores, sample = ref
+            cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample}
+        else:
+            cpu = cpu_port
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -434,7 +487,7 @@ def run_ours(a):
                            "grid_point_updates_per_s": value * g.nx * g.ny * g.nz},
                 "gpu_launches": launches * a.steps, "launches_per_step": launches,
                 "roofline": roofline, "step_roofline": whole, "phases_ms": phase_ms,
-                "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "nan_points": nan,
+                "e2e": e2e, "cpu_baseline": cpu, "cpu_baseline_port": cpu_port, "clocks": clocks, "nan_points": nan,
                 "surrogate": sur, "config4": big,
                 "reference_cpu": reference_cpu_record(f"{g.nx}x{g.ny}x{g.nz}"),
                 "reference_gpu": reference_gpu_record(f"{g.nx}x{g.ny}x{g.nz}", value,
