@@ -1,16 +1,16 @@
 // Reverse-mode differentiation of scalar device code by a per-thread tape.
 //
-// Tv carries a float value and the index of the tape entry that produced it
-// (-1 for a constant).  Every arithmetic operation or elementary function on
-// a Tv appends one entry -- the indices of its (at most two) operands and
-// the partial derivatives with respect to them -- to the calling thread's
-// tape; selections (vmin, vmax, sel, the branches of the code) append
-// nothing: the result is the chosen operand itself, so the derivative is
-// that of the branch taken.  A value is carried as a multiple of its entry,
-// so adding a constant, scaling by one and negating append nothing either
-// (the multiple enters the partials of the next entry that uses it).  After the forward code has run, the
-// reverse sweep walks the thread's entries backwards and accumulates the
-// adjoints of the operands.
+// Tv carries a float value, the index of a tape entry (-1 for a constant)
+// and the multiple of that entry's value it is.  Every arithmetic operation
+// or elementary function of taped operands appends one entry -- the indices
+// of its (at most two) operands and the partial derivatives with respect to
+// them -- to the calling thread's tape; selections (vmin, vmax, sel, the
+// branches of the code) append nothing: the result is the chosen operand
+// itself, so the derivative is that of the branch taken.  Adding a
+// constant, scaling by one and negating append nothing either: the multiple
+// changes and enters the partials of the next entry that uses the value.
+// After the forward code has run, the reverse sweep walks the thread's
+// entries backwards and accumulates the adjoints of the operands.
 //
 // A thread's tape lives in global memory, contiguous per thread (entry n of
 // lane t at t * cap + n): the lanes of a warp are mostly at different
