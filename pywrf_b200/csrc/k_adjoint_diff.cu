@@ -152,60 +152,77 @@ __device__ void diff_point(const Grid& g, const S& s, int var, const float* f, c
   o.mr[1] = m1[c] * m2[c] * g.rdy;
 }
 
+// a thread takes one column's levels [z0, z0 + kHdiffLevels) of the
+// diffusion region: the column's coefficients once, then its levels
+constexpr int kHdiffLevels = 8;
 __global__ void k_hdiff_op(Grid g, S s, int var, const float* f, const float* base, const float* mut, const float* K,
                            float* tend) {
-  WRF_POINT_INDEX(g, k, j, i);
-  if (!diff_region(g, var, k, j, i)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z0 = blockIdx.z * kHdiffLevels;
+  if (i >= g.nx || j >= g.ny || !diff_region(g, var, g.nz - 2, j, i)) return;
   const int c = g.i2(j, i);
-  const size_t p = (size_t)k * g.ny * g.nx + c;
   Coef cf[4];
   diff_coefs(g, s, var, c, cf);
-  DiffPoint o;
-  diff_point(g, s, var, f, base, mut, K, k, c, p, cf, o);
-  tend[p] = tend[p] + (o.mr[0] * (o.kx[1] * o.d[1] - o.kx[0] * o.d[0]) + o.mr[1] * (o.kx[3] * o.d[3] - o.kx[2] * o.d[2]));
+  for (int k = z0; k < z0 + kHdiffLevels && k < g.nz; ++k) {
+    if (!diff_region(g, var, k, j, i)) continue;
+    const size_t p = (size_t)k * g.ny * g.nx + c;
+    DiffPoint o;
+    diff_point(g, s, var, f, base, mut, K, k, c, p, cf, o);
+    tend[p] = tend[p] + (o.mr[0] * (o.kx[1] * o.d[1] - o.kx[0] * o.d[0]) + o.mr[1] * (o.kx[3] * o.d[3] - o.kx[2] * o.d[2]));
+  }
 }
 
+// its reverse, over the same level ranges: the field's and the viscosity's
+// cotangents scattered with atomics, the column mass's summed over the
+// thread's levels first
 __global__ void k_hdiff_op_adj(Grid g, S s, int var, const float* f, const float* base, const float* mut,
                                const float* K, const float* tbar, float* fbar, float* mutbar, float* Kbar) {
-  WRF_POINT_INDEX(g, k, j, i);
-  if (!diff_region(g, var, k, j, i)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z0 = blockIdx.z * kHdiffLevels;
+  if (i >= g.nx || j >= g.ny || !diff_region(g, var, g.nz - 2, j, i)) return;
   const int nx = g.nx;
   const size_t lev = (size_t)g.ny * nx;
   const int c = g.i2(j, i);
-  const size_t p = (size_t)k * lev + c;
-  const float T = tbar[p];
-  if (T == 0.f) return;
   Coef cf[4];
   diff_coefs(g, s, var, c, cf);
-  DiffPoint o;
-  diff_point(g, s, var, f, base, mut, K, k, c, p, cf, o);
-  // d/d(differences): +-mr * k..
-  const float gx0 = -o.mr[0] * o.kx[0] * T, gx1 = o.mr[0] * o.kx[1] * T;
-  const float gy0 = -o.mr[1] * o.kx[2] * T, gy1 = o.mr[1] * o.kx[3] * T;
-  // dxm = c - xm, dxp = xp - c, dym = c - ym, dyp = yp - c (base is data)
-  if (fbar) {
-    acc(fbar, p, gx0 - gx1 + gy0 - gy1);
-    acc(fbar, p - 1, -gx0);
-    acc(fbar, p + 1, gx1);
-    acc(fbar, p - nx, -gy0);
-    acc(fbar, p + nx, gy1);
-  }
-  // d/d k.. then into the averages
+  float wm[4] = {0.f, 0.f, 0.f, 0.f};  // the mass averages' cotangents, per edge
   const float sgn[4] = {-1.f, 1.f, -1.f, 1.f};
-  for (int e = 0; e < 4; ++e) {
-    const float mr = e < 2 ? o.mr[0] : o.mr[1];
-    const float kb = sgn[e] * mr * o.d[e] * T;  // cotangent of k..
-    const float base_c = cf[e].ratio * cf[e].rd * kb;
-    if (mutbar && cf[e].nm) {
-      const float wmb = base_c * o.kavg[e] * cf[e].wm;
-      for (int q = 0; q < cf[e].nm; ++q) acc(mutbar, c + cf[e].mj[q] * nx + cf[e].mi[q], wmb);
+  for (int k = z0; k < z0 + kHdiffLevels && k < g.nz; ++k) {
+    if (!diff_region(g, var, k, j, i)) continue;
+    const size_t p = (size_t)k * lev + c;
+    const float T = tbar[p];
+    if (T == 0.f) continue;
+    DiffPoint o;
+    diff_point(g, s, var, f, base, mut, K, k, c, p, cf, o);
+    // d/d(differences): +-mr * k..
+    const float gx0 = -o.mr[0] * o.kx[0] * T, gx1 = o.mr[0] * o.kx[1] * T;
+    const float gy0 = -o.mr[1] * o.kx[2] * T, gy1 = o.mr[1] * o.kx[3] * T;
+    // dxm = c - xm, dxp = xp - c, dym = c - ym, dyp = yp - c (base is data)
+    if (fbar) {
+      acc(fbar, p, gx0 - gx1 + gy0 - gy1);
+      acc(fbar, p - 1, -gx0);
+      acc(fbar, p + 1, gx1);
+      acc(fbar, p - nx, -gy0);
+      acc(fbar, p + nx, gy1);
     }
-    if (Kbar) {
-      const float wkb = base_c * o.mavg[e] * cf[e].wk;
-      for (int q = 0; q < cf[e].nk; ++q)
-        acc(Kbar, p + (long)cf[e].kk[q] * (long)lev + cf[e].kj[q] * nx + cf[e].ki[q], wkb);
+    // d/d k.. then into the averages
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const float mr = e < 2 ? o.mr[0] : o.mr[1];
+      const float kb = sgn[e] * mr * o.d[e] * T;  // cotangent of k..
+      const float base_c = cf[e].ratio * cf[e].rd * kb;
+      if (cf[e].nm) wm[e] += base_c * o.kavg[e] * cf[e].wm;
+      if (Kbar) {
+        const float wkb = base_c * o.mavg[e] * cf[e].wk;
+        for (int q = 0; q < cf[e].nk; ++q)
+          acc(Kbar, p + (long)cf[e].kk[q] * (long)lev + cf[e].kj[q] * nx + cf[e].ki[q], wkb);
+      }
     }
   }
+  if (mutbar)
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      for (int q = 0; q < cf[e].nm; ++q) acc(mutbar, c + cf[e].mj[q] * nx + cf[e].mi[q], wm[e]);
 }
 
 // ---- the eddy viscosities ----
@@ -458,16 +475,16 @@ __global__ void k_mass_weight_adj(Grid g, const float* f, const float* mut, cons
 int launch_hdiff_op(const Grid& g, const S& s, char var, const float* f, const float* base, const float* mut,
                     const float* K, float* tend, cudaStream_t st) {
   const int v = var == 'u' ? DV_U : (var == 'v' ? DV_V : (var == 'w' ? DV_W : DV_M));
-  const dim3 b3(32, 4);
-  k_hdiff_op<<<point_grid(g, b3), b3, 0, st>>>(g, s, v, f, base, mut, K, tend);
+  const dim3 b3(32, 4), grid((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + kHdiffLevels - 1) / kHdiffLevels);
+  k_hdiff_op<<<grid, b3, 0, st>>>(g, s, v, f, base, mut, K, tend);
   return 1;
 }
 
 int launch_hdiff_op_adj(const Grid& g, const S& s, char var, const float* f, const float* base, const float* mut,
                         const float* K, const float* tbar, float* fbar, float* mutbar, float* Kbar, cudaStream_t st) {
   const int v = var == 'u' ? DV_U : (var == 'v' ? DV_V : (var == 'w' ? DV_W : DV_M));
-  const dim3 b3(32, 4);
-  k_hdiff_op_adj<<<point_grid(g, b3), b3, 0, st>>>(g, s, v, f, base, mut, K, tbar, fbar, mutbar, Kbar);
+  const dim3 b3(32, 4), grid((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + kHdiffLevels - 1) / kHdiffLevels);
+  k_hdiff_op_adj<<<grid, b3, 0, st>>>(g, s, v, f, base, mut, K, tbar, fbar, mutbar, Kbar);
   return 1;
 }
 
