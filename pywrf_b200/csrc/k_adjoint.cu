@@ -53,7 +53,8 @@
 //                        difference to it, dpn the vertical pressure average
 //                        of the two columns); v likewise in y.  The point
 //                        kernel gathers the 3-D cotangents from the u and v
-//                        points whose stencils hold the point, the column
+//                        points whose stencils hold the point (forming of
+//                        each only the factors that reach the point), the column
 //                        kernel sums the 2-D ones (muu, muv, mu, mudf) over
 //                        the levels.  The cotangents of u and v pass through
 //                        (du'/du = 1).
@@ -366,6 +367,7 @@ struct UvTerm {
   float ub, dpb, A, B, Cf, C, D;
 };
 
+template <bool kB = true, bool kD = true>
 __device__ UvTerm uv_term(const Grid& g, const S& s, const S& b, float dts, int V, int k, int j, int i) {
   const size_t lev = (size_t)g.ny * g.nx;
   const size_t c = (size_t)j * g.nx + i, p = k * lev + c, no = V ? (size_t)g.nx : 1;
@@ -382,11 +384,15 @@ __device__ UvTerm uv_term(const Grid& g, const S& s, const S& b, float dts, int 
   t.ub = b[V ? WF_V : WF_U][p];
   t.dpb = -dts * s[V ? WF_CQV : WF_CQU][p] * t.ub;
   t.A = r * 0.5f * rd * s[V ? WF_MUV : WF_MUU][c];
-  t.B = ((ph[p + lev] - ph[p + lev - no]) + (ph[p] - ph[p - no])) + (alt[p] + alt[p - no]) * (pp[p] - pp[p - no]) +
-        (al[p] + al[p - no]) * (pb[p] - pb[p - no]);
+  t.B = 0.f;
+  if (kB)
+    t.B = ((ph[p + lev] - ph[p + lev - no]) + (ph[p] - ph[p - no])) + (alt[p] + alt[p - no]) * (pp[p] - pp[p - no]) +
+          (al[p] + al[p - no]) * (pb[p] - pb[p - no]);
   t.Cf = r * rd;
   t.C = t.Cf * (php[p] - php[p - no]);
-  t.D = s[WF_RDNW][k] * (uv_dpn(g, s, k + 1, c, c - no) - uv_dpn(g, s, k, c, c - no)) - 0.5f * (mu[c - no] + mu[c]);
+  t.D = 0.f;
+  if (kD)
+    t.D = s[WF_RDNW][k] * (uv_dpn(g, s, k + 1, c, c - no) - uv_dpn(g, s, k, c, c - no)) - 0.5f * (mu[c - no] + mu[c]);
   return t;
 }
 
@@ -412,7 +418,10 @@ __global__ void k_advance_uv_adj(Grid g, S s, S b, float dts) {
       const float sg = e == 0 ? 1.f : -1.f;
       for (int kP = k - 2; kP <= k + 1; ++kP) {
         if (kP < 0 || kP >= ktf) continue;
-        const UvTerm t = uv_term(g, s, b, dts, V, kP, jP, iP);
+        // B enters the gathered cotangents only through A (and the own
+        // point's cqu / cqv, below), D only at kP == k
+        const UvTerm t = kP == k ? uv_term<false, true>(g, s, b, dts, V, kP, jP, iP)
+                                 : uv_term<false, false>(g, s, b, dts, V, kP, jP, iP);
         if (t.dpb == 0.f) continue;
         const float Bb = t.dpb * t.A, Db = t.dpb * t.C;
         const size_t P = (size_t)kP * lev + (size_t)jP * nx + iP;
@@ -461,8 +470,10 @@ __global__ void k_advance_uv_adj_col(Grid g, S s, S b, float dts) {
       const size_t cP = (size_t)jP * nx + iP;
       const float sg = e == 0 ? 1.f : -1.f;
       const float em = V ? ev * s[WF_MSFVX_INV][cP] : eu / s[WF_MSFUY][cP];
+#pragma unroll 4
       for (int k = 0; k < ktf; ++k) {
-        const UvTerm t = uv_term(g, s, b, dts, V, k, jP, iP);
+        const UvTerm t = e == 0 ? uv_term<true, false>(g, s, b, dts, V, k, jP, iP)
+                                : uv_term<false, false>(g, s, b, dts, V, k, jP, iP);
         if (e == 0) {
           const float r = V ? s[WF_MSFVY][cP] / s[WF_MSFVX][cP] : s[WF_MSFUX][cP] / s[WF_MSFUY][cP];
           const float d = t.dpb * (r * 0.5f * (V ? g.rdy : g.rdx)) * t.B;

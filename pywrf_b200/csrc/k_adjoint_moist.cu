@@ -113,7 +113,9 @@ __global__ void k_flowdep_adj(Grid g, S s, S b) {
   }
 }
 
-// rk_update_scalar's reverse, all six species
+// rk_update_scalar's reverse, all six species.  The arrays may alias as far
+// as the compiler knows, so the six species' loads are all written before
+// the first store and issue together.
 __global__ void k_moist_update_adj(Grid g, S s, S b, int rk_step, float dt) {
   WRF_POINT_INDEX(g, k, j, i);
   const size_t n3 = g.n3();
@@ -121,41 +123,65 @@ __global__ void k_moist_update_adj(Grid g, S s, S b, int rk_step, float dt) {
   const size_t p = (size_t)k * g.ny * g.nx + c;
   const MoistRegions r = moist_regions(g, k, j, i);
   const bool first = rk_step == 1;
-  const float muold = r.full ? s[WF_MU_1][c] + s[WF_MUB][c] : 0.f;
-  const float munew = r.full ? s[WF_MU][c] + s[WF_MUB][c] : 1.f;
-  const float msfty = r.full ? s[WF_MSFTY][c] : 0.f;
-  float mu1b = 0.f, mub_b = 0.f, mub2 = 0.f;
+  float* qb = b[WF_MOIST];
+  float* qob = b[WF_MOIST_OLD];
+  if (!r.full) {
+    // outside the updated region only the first stage's copy moist_old =
+    // moist passes its cotangent back
+    if (!first) return;
+    float qv[6], qo[6];
+#pragma unroll
+    for (int m = 1; m < 7; ++m) {
+      qv[m - 1] = qb[(size_t)m * n3 + p];
+      qo[m - 1] = qob[(size_t)m * n3 + p];
+    }
+#pragma unroll
+    for (int m = 1; m < 7; ++m) {
+      qob[(size_t)m * n3 + p] = 0.f;
+      qb[(size_t)m * n3 + p] = qv[m - 1] + qo[m - 1];
+    }
+    return;
+  }
+  const float muold = s[WF_MU_1][c] + s[WF_MUB][c];
+  const float munew = s[WF_MU][c] + s[WF_MUB][c];
+  const float msfty = s[WF_MSFTY][c];
+  float Q[6], QO[6], qo[6], adv[6], mt[6], advb[6], mtb[6];
+#pragma unroll
   for (int m = 1; m < 7; ++m) {
     const size_t o = (size_t)m * n3 + p;
-    float* qb = b[WF_MOIST];
-    float* qob = b[WF_MOIST_OLD];
+    Q[m - 1] = qb[o];
+    QO[m - 1] = qob[o];
+    qo[m - 1] = first ? s[WF_MOIST][o] : s[WF_MOIST_OLD][o];
+    adv[m - 1] = r.inner ? s[WF_ADVECT_TEND][o] : 0.f;
+    advb[m - 1] = r.inner ? b[WF_ADVECT_TEND][o] : 0.f;
+    mt[m - 1] = s[WF_MOIST_TEND][o];
+    mtb[m - 1] = b[WF_MOIST_TEND][o];
+  }
+  float mu1b = 0.f, mub2 = 0.f;
+#pragma unroll
+  for (int m = 1; m < 7; ++m) {
+    const size_t o = (size_t)m * n3 + p;
+    const float q = Q[m - 1];
     // at the first stage moist_old became a copy of the incoming moist
-    float qin_b = first ? qob[o] : 0.f;
-    if (first) qob[o] = 0.f;
-    if (!r.full) {
-      qb[o] += qin_b;
-      continue;
+    float qin_b = first ? QO[m - 1] : 0.f;
+    const float tend = (r.inner ? adv[m - 1] * msfty : 0.f) + mt[m - 1];
+    const float Tb = dt / munew * q;
+    if (r.inner) b[WF_ADVECT_TEND][o] = advb[m - 1] + Tb * msfty;
+    b[WF_MOIST_TEND][o] = mtb[m - 1] + Tb;
+    const float qob_v = muold / munew * q;
+    if (first) {
+      qin_b += qob_v;
+      qob[o] = 0.f;
+    } else {
+      qob[o] = QO[m - 1] + qob_v;
     }
-    const float Q = qb[o];
-    const float qo = first ? s[WF_MOIST][o] : s[WF_MOIST_OLD][o];
-    float tend = r.inner ? s[WF_ADVECT_TEND][o] * msfty : 0.f;
-    tend = tend + s[WF_MOIST_TEND][o];
-    const float Tb = dt / munew * Q;
-    if (r.inner) b[WF_ADVECT_TEND][o] += Tb * msfty;
-    b[WF_MOIST_TEND][o] += Tb;
-    const float qob_v = muold / munew * Q;
-    if (first) qin_b += qob_v;
-    else qob[o] += qob_v;
-    mu1b += qo * Q / munew;
-    mub2 += -(muold * qo + dt * tend) / (munew * munew) * Q;
+    mu1b += qo[m - 1] * q / munew;
+    mub2 += -(muold * qo[m - 1] + dt * tend) / (munew * munew) * q;
     qb[o] = qin_b;  // the updated value replaced the incoming one
   }
-  if (r.full) {
-    mub_b = mu1b + mub2;
-    acc(b[WF_MU_1], c, mu1b);
-    acc(b[WF_MU], c, mub2);
-    acc(b[WF_MUB], c, mub_b);
-  }
+  acc(b[WF_MU_1], c, mu1b);
+  acc(b[WF_MU], c, mub2);
+  acc(b[WF_MUB], c, mu1b + mub2);
 }
 
 }  // namespace
