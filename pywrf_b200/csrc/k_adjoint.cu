@@ -652,11 +652,14 @@ struct MutCol {
   float dmdt;
 };
 
+constexpr int kMutChunk = 8;  // levels whose loads a column kernel issues together
+
 __device__ void mut_column(const Grid& g, const S& s, int j, int i, MutCol& m) {
   const int ktf = g.nz - 1;
   const size_t lev = (size_t)g.ny * g.nx, c = (size_t)j * g.nx + i;
   const float* dnw = s[WF_DNW];
   m.dmdt = 0.f;
+#pragma unroll 8
   for (int k = 0; k < ktf; ++k) {
     m.dv[k] = mut_dvdxi(g, s, k, j, i);
     m.dmdt = m.dmdt + dnw[k] * m.dv[k];
@@ -664,6 +667,7 @@ __device__ void mut_column(const Grid& g, const S& s, int j, int i, MutCol& m) {
   const float mt = s[WF_MU_TEND][c], msfty = s[WF_MSFTY][c];
   float W = s[WF_WW][c];
   m.wwp[0] = W - s[WF_WW1][c];
+#pragma unroll 8
   for (int k = 1; k < ktf; ++k) {
     W = W - dnw[k - 1] * (m.dmdt + m.dv[k - 1] + mt) / msfty;
     m.wwp[k] = W - s[WF_WW1][k * lev + c];
@@ -678,6 +682,7 @@ __device__ void mut_ww_bar(const Grid& g, const S& s, const S& b, float dts, int
   const float dm = dts * s[WF_MSFTY][c];
   const float* rdnw = s[WF_RDNW];
   const float* t1 = s[WF_T_SAVE];
+#pragma unroll 8
   for (int k = 0; k < ktf; ++k) {
     wdb[k] = 0.f;
     if (k >= 1) wdb[k] = -dm * rdnw[k - 1] * b[WF_T][(k - 1) * lev + c] + dm * rdnw[k] * b[WF_T][k * lev + c];
@@ -717,14 +722,30 @@ __global__ void k_advance_mu_t(Grid g, S s, float dts) {
     if (k < 1 || k >= ktf) return 0.f;
     return m.wwp[k] * (s[WF_FNM][k] * t1[k * lev + c] + s[WF_FNP][k] * t1[(k - 1) * lev + c]);
   };
-  for (int k = 0; k < ktf; ++k) {
-    const size_t p = k * lev + c;
-    const float tk = s[WF_T][p];
-    s[WF_T_2SAVE][p] = tk;
-    const float t1v = tk + msfty * dts * s[WF_T_TEND][p];
-    const float h = 0.5f * rdy * (v[p + nx] * (t1[p + nx] + t1[p]) - v[p] * (t1[p] + t1[p - nx])) +
-                    0.5f * rdx * (u[p + 1] * (t1[p + 1] + t1[p]) - u[p] * (t1[p] + t1[p - 1]));
-    s[WF_T][p] = t1v - dts * msfty * (msftx * h + s[WF_RDNW][k] * (wdtn(k + 1) - wdtn(k)));
+  // kMutChunk levels at a time, every load of the block before its stores
+  for (int k0 = 0; k0 < ktf; k0 += kMutChunk) {
+    float tk[kMutChunk], tt[kMutChunk], h[kMutChunk], rd[kMutChunk], wd[kMutChunk + 1];
+#pragma unroll
+    for (int q = 0; q <= kMutChunk; ++q) wd[q] = wdtn(k0 + q);
+#pragma unroll
+    for (int q = 0; q < kMutChunk; ++q) {
+      const int k = k0 + q;
+      const size_t p = (size_t)(k < ktf ? k : 0) * lev + c;
+      tk[q] = s[WF_T][p];
+      tt[q] = s[WF_T_TEND][p];
+      h[q] = 0.5f * rdy * (v[p + nx] * (t1[p + nx] + t1[p]) - v[p] * (t1[p] + t1[p - nx])) +
+             0.5f * rdx * (u[p + 1] * (t1[p + 1] + t1[p]) - u[p] * (t1[p] + t1[p - 1]));
+      rd[q] = s[WF_RDNW][k < ktf ? k : 0];
+    }
+#pragma unroll
+    for (int q = 0; q < kMutChunk; ++q) {
+      const int k = k0 + q;
+      if (k >= ktf) break;
+      const size_t p = k * lev + c;
+      s[WF_T_2SAVE][p] = tk[q];
+      const float t1v = tk[q] + msfty * dts * tt[q];
+      s[WF_T][p] = t1v - dts * msfty * (msftx * h[q] + rd[q] * (wd[q + 1] - wd[q]));
+    }
   }
 }
 
@@ -739,13 +760,24 @@ __global__ void k_advance_mu_t_adj_dv(Grid g, S s, S b, float dts, int ref_no_gr
   mut_ww_bar(g, s, b, dts, j, i, m, wdb, wwb);
   const float msfty = s[WF_MSFTY][c];
   float S_ = 0.f, qsum = 0.f;
+#pragma unroll 8
   for (int k = ktf - 1; k >= 1; --k) {
     S_ += wwb[k];
     qb[k - 1] = -s[WF_DNW][k - 1] / msfty * S_;
     qsum += qb[k - 1];
   }
   const float dmdtb = qsum + (ref_no_grad ? 0.f : dts * mut_mu_bar(g, b, c) + b[WF_MUDF][c]);
-  for (int k = 0; k < ktf; ++k) work[k * lev + c] = (k <= ktf - 2 ? qb[k] : 0.f) + s[WF_DNW][k] * dmdtb;
+  for (int k0 = 0; k0 < ktf; k0 += kMutChunk) {  // dnw loaded before the block's stores
+    float dn[kMutChunk];
+#pragma unroll
+    for (int q = 0; q < kMutChunk; ++q) dn[q] = s[WF_DNW][k0 + q < ktf ? k0 + q : 0];
+#pragma unroll
+    for (int q = 0; q < kMutChunk; ++q) {
+      const int k = k0 + q;
+      if (k >= ktf) break;
+      work[k * lev + c] = (k <= ktf - 2 ? qb[k] : 0.f) + dn[q] * dmdtb;
+    }
+  }
 }
 
 __global__ void k_advance_mu_t_adj_pt(Grid g, S s, S b, float dts, const float* work) {
@@ -802,6 +834,7 @@ __global__ void k_advance_mu_t_adj_col(Grid g, S s, S b, float dts, int ref_no_g
       const float mw = w ? s[WF_MSFTX][c - 1] * s[WF_MSFTY][c - 1] : 0.f;
       const float mo = o ? s[WF_MSFTX][c] * s[WF_MSFTY][c] : 0.f;
       const float ms = sth ? s[WF_MSFTX][c - nx] * s[WF_MSFTY][c - nx] : 0.f;
+#pragma unroll 8
       for (int k = 0; k < ktf; ++k) {
         const size_t p = k * lev + c;
         float ub = 0.f, vb = 0.f;
@@ -824,26 +857,57 @@ __global__ void k_advance_mu_t_adj_col(Grid g, S s, S b, float dts, int ref_no_g
   const float msfty = s[WF_MSFTY][c];
   // ww, ww_1 (the scan passes every ww' cotangent down to ww(0))
   float wsum = 0.f, qsum = 0.f, S_ = 0.f;
+#pragma unroll 8
   for (int k = ktf - 1; k >= 1; --k) {
     S_ += wwb[k];
     qsum += -s[WF_DNW][k - 1] / msfty * S_;
   }
-  for (int k = 0; k < ktf; ++k) {
-    wsum += wwb[k];
-    b[WF_WW1][k * lev + c] += -wwb[k];
-    if (k >= 1) b[WF_WW][k * lev + c] = 0.f;
+  // (the arrays may alias as far as the compiler knows: each block of
+  // kMutChunk levels loads everything it reads before its first store, so
+  // the loads issue together)
+  for (int k0 = 0; k0 < ktf; k0 += kMutChunk) {
+    float w1[kMutChunk];
+#pragma unroll
+    for (int q = 0; q < kMutChunk; ++q) w1[q] = k0 + q < ktf ? b[WF_WW1][(k0 + q) * lev + c] : 0.f;
+#pragma unroll
+    for (int q = 0; q < kMutChunk; ++q) {
+      const int k = k0 + q;
+      if (k >= ktf) break;
+      wsum += wwb[k];
+      b[WF_WW1][k * lev + c] = w1[q] - wwb[k];
+      if (k >= 1) b[WF_WW][k * lev + c] = 0.f;
+    }
   }
   b[WF_WW][c] = wsum;
-  // theta: t_ave = t, ft, the vertical fluxes' t_1
-  for (int k = 0; k < ktf; ++k) {
-    const size_t p = k * lev + c;
-    const float tb = b[WF_T][p];
-    b[WF_T_TEND][p] += msfty * dts * tb;
-    b[WF_T][p] = tb + b[WF_T_2SAVE][p];
-    b[WF_T_2SAVE][p] = 0.f;
-    if (k >= 1) {
-      b[WF_T_SAVE][p] += wdb[k] * m.wwp[k] * s[WF_FNM][k];
-      b[WF_T_SAVE][p - lev] += wdb[k] * m.wwp[k] * s[WF_FNP][k];
+  // theta: t_ave = t, ft, the vertical fluxes' t_1 (t_1(k) takes level k's
+  // fnm term, then level k + 1's fnp term)
+  const float* fnm = s[WF_FNM];
+  const float* fnp = s[WF_FNP];
+  for (int k0 = 0; k0 < ktf; k0 += kMutChunk) {
+    float tb[kMutChunk], tt[kMutChunk], t2s[kMutChunk], tsv[kMutChunk], fm[kMutChunk], fp[kMutChunk];
+#pragma unroll
+    for (int q = 0; q < kMutChunk; ++q) {
+      const int k = k0 + q;
+      const size_t p = (size_t)(k < ktf ? k : 0) * lev + c;
+      tb[q] = k < ktf ? b[WF_T][p] : 0.f;
+      tt[q] = k < ktf ? b[WF_T_TEND][p] : 0.f;
+      t2s[q] = k < ktf ? b[WF_T_2SAVE][p] : 0.f;
+      tsv[q] = k < ktf ? b[WF_T_SAVE][p] : 0.f;
+      fm[q] = k >= 1 && k < ktf ? fnm[k] : 0.f;
+      fp[q] = k + 1 < ktf ? fnp[k + 1] : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < kMutChunk; ++q) {
+      const int k = k0 + q;
+      if (k >= ktf) break;
+      const size_t p = k * lev + c;
+      b[WF_T_TEND][p] = tt[q] + msfty * dts * tb[q];
+      b[WF_T][p] = tb[q] + t2s[q];
+      b[WF_T_2SAVE][p] = 0.f;
+      float x = tsv[q];
+      if (k >= 1) x += wdb[k] * m.wwp[k] * fm[q];
+      if (k + 1 < ktf) x += wdb[k + 1] * m.wwp[k + 1] * fp[q];
+      b[WF_T_SAVE][p] = x;
     }
   }
   // the mu update

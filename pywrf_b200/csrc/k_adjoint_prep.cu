@@ -245,34 +245,64 @@ __global__ void k_ww_cp_op_adj(Grid g, S s, S b) {
   const float* dnw = s[WF_DNW];
   const float* c1h = s[WF_C1H];
   float* wwb = b[WF_WW];
-  float Sk[kMaxNz];
+  // the arrays may alias as far as the compiler knows: the column's loads
+  // are written before its stores (in blocks of kChunk levels below), so
+  // they issue together
+  constexpr int kChunk = 8;
+  float Wk[kMaxNz], Sk[kMaxNz];
+#pragma unroll 8
+  for (int k = 0; k < ktf; ++k) Wk[k] = wwb[k * lev + c];
   float run = 0.f, sumw = 0.f, dmb = 0.f;
+#pragma unroll 8
   for (int k = ktf - 2; k >= 0; --k) {  // S(k) = W(k+1) + S(k+1)
-    const float W = wwb[(k + 1) * lev + c];
-    wwb[(k + 1) * lev + c] = 0.f;
+    const float W = Wk[k + 1];
     run = run + W;
     Sk[k] = run;
     sumw = sumw + W;
     dmb = dmb - (dnw[k] * c1h[k]) * run;
   }
-  wwb[c] += sumw;
   const float msftx = s[WF_MSFTX][c];
   const float* u = s[WF_U];
   const float* v = s[WF_V];
-  for (int k = 0; k < ktf; ++k) {
-    const float D = dmb - (k < ktf - 1 ? Sk[k] : 0.f);
-    const float E = msftx * dnw[k] * D;
-    const size_t p = k * lev + c;
-    const float fu1b = g.rdx * E, fv1b = g.rdy * E;
-    acc(b[WF_U], p + 1, s[WF_MUU][c + 1] / s[WF_MSFUY][c + 1] * fu1b);
-    acc(b[WF_MUU], c + 1, u[p + 1] / s[WF_MSFUY][c + 1] * fu1b);
-    acc(b[WF_U], p, -s[WF_MUU][c] / s[WF_MSFUY][c] * fu1b);
-    acc(b[WF_MUU], c, -u[p] / s[WF_MSFUY][c] * fu1b);
-    acc(b[WF_V], p + nx, s[WF_MUV][c + nx] * s[WF_MSFVX_INV][c + nx] * fv1b);
-    acc(b[WF_MUV], c + nx, v[p + nx] * s[WF_MSFVX_INV][c + nx] * fv1b);
-    acc(b[WF_V], p, -s[WF_MUV][c] * s[WF_MSFVX_INV][c] * fv1b);
-    acc(b[WF_MUV], c, -v[p] * s[WF_MSFVX_INV][c] * fv1b);
+  const float muu0 = s[WF_MUU][c], muu1 = s[WF_MUU][c + 1], mfu0 = s[WF_MSFUY][c], mfu1 = s[WF_MSFUY][c + 1];
+  const float muv0 = s[WF_MUV][c], muv1 = s[WF_MUV][c + nx], mfv0 = s[WF_MSFVX_INV][c],
+              mfv1 = s[WF_MSFVX_INV][c + nx];
+  for (int k = 1; k < ktf; ++k) wwb[k * lev + c] = 0.f;
+  wwb[c] = Wk[0] + sumw;
+  float amuu0 = 0.f, amuu1 = 0.f, amuv0 = 0.f, amuv1 = 0.f;
+  for (int k0 = 0; k0 < ktf; k0 += kChunk) {
+    float u0[kChunk], u1[kChunk], v0[kChunk], v1[kChunk], dn[kChunk];
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) {
+      const size_t p = (size_t)(k0 + q < ktf ? k0 + q : 0) * lev + c;
+      u0[q] = u[p];
+      u1[q] = u[p + 1];
+      v0[q] = v[p];
+      v1[q] = v[p + nx];
+      dn[q] = dnw[k0 + q < ktf ? k0 + q : 0];
+    }
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) {
+      const int k = k0 + q;
+      if (k >= ktf) break;
+      const float D = dmb - (k < ktf - 1 ? Sk[k] : 0.f);
+      const float E = msftx * dn[q] * D;
+      const size_t p = k * lev + c;
+      const float fu1b = g.rdx * E, fv1b = g.rdy * E;
+      acc(b[WF_U], p + 1, muu1 / mfu1 * fu1b);
+      amuu1 += u1[q] / mfu1 * fu1b;
+      acc(b[WF_U], p, -muu0 / mfu0 * fu1b);
+      amuu0 += -u0[q] / mfu0 * fu1b;
+      acc(b[WF_V], p + nx, muv1 * mfv1 * fv1b);
+      amuv1 += v1[q] * mfv1 * fv1b;
+      acc(b[WF_V], p, -muv0 * mfv0 * fv1b);
+      amuv0 += -v0[q] * mfv0 * fv1b;
+    }
   }
+  acc(b[WF_MUU], c + 1, amuu1);
+  acc(b[WF_MUU], c, amuu0);
+  acc(b[WF_MUV], c + nx, amuv1);
+  acc(b[WF_MUV], c, amuv0);
 }
 
 }  // namespace
