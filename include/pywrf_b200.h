@@ -310,7 +310,8 @@ int wrf_eddy_viscosity_adj(const WrfGrid* g, const WrfState* s, const WrfState* 
 int wrf_horizontal_diffusion(const WrfGrid* g, const WrfState* s, char var, const float* field, const float* base,
                              const float* mut, const float* xk, float* tend, void* stream);
 /* Its adjoint: field_bar, mut_bar and xk_bar accumulate (each may be null
- * when not wanted); tend_bar passes through unchanged. */
+ * when not wanted; they must not overlap each other, tend_bar or the
+ * operands); tend_bar passes through unchanged. */
 int wrf_horizontal_diffusion_adj(const WrfGrid* g, const WrfState* s, char var, const float* field,
                                  const float* base, const float* mut, const float* xk, const float* tend_bar,
                                  float* field_bar, float* mut_bar, float* xk_bar, void* stream);
@@ -481,8 +482,9 @@ int wrf_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const flo
  * top_lid from the grid */
 int wrf_coef_w(const WrfGrid* g, const float* mut, const float* cqw, const float* c2a, const float* rdn,
                const float* rdnw, float dts, float* a, float* alpha, float* gamma, void* stream);
-/* its adjoint w.r.t. mut, cqw and c2a (accumulates into the *_bar outputs);
- * the reference obtains it from torch autograd */
+/* its adjoint w.r.t. mut, cqw and c2a (accumulates into the *_bar outputs,
+ * which must not overlap the inputs or each other); the reference obtains
+ * it from torch autograd */
 int wrf_coef_w_adj(const WrfGrid* g, const float* mut, const float* cqw, const float* c2a, const float* rdn,
                    const float* rdnw, float dts, const float* a_bar, const float* alpha_bar,
                    const float* gamma_bar, float* mut_bar, float* cqw_bar, float* c2a_bar, void* stream);

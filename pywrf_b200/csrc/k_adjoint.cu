@@ -457,21 +457,28 @@ __global__ void k_advance_uv_adj(Grid g, S s, S b, float dts) {
   if (ap != 0.f) b[WF_P][m] += ap;
 }
 
-__global__ void k_advance_uv_adj_col(Grid g, S s, S b, float dts) {
-  WRF_COLUMN_INDEX(g, j, i);
+// the column sums by kColLevels level groups (threadIdx.y, levels ty,
+// ty + kColLevels, ...) of 32 columns of a row, added up in a fixed order
+constexpr int kColLevels = 8;
+
+__global__ void __launch_bounds__(32 * kColLevels) k_advance_uv_adj_col(Grid g, S s, S b, float dts) {
+  __shared__ float red[4][kColLevels][32];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.x * 32 + tx, j = blockIdx.y;
   const int ktf = g.nz - 1, nx = g.nx;
-  const size_t c = (size_t)j * nx + i;
+  const bool on = i < nx;
+  const size_t c = (size_t)j * nx + (on ? i : 0);
   const float eu = (float)(-(double)g.emdiv * g.dxd), ev = (float)(-(double)g.emdiv * g.dyd);
   float amuu = 0.f, amuv = 0.f, amu = 0.f, amudf = 0.f;
   for (int V = 0; V < 2; ++V)
     for (int e = 0; e < 2; ++e) {
       const int jP = j + V * e, iP = i + (1 - V) * e;
-      if (jP >= g.ny || iP >= nx || !uv_in(g, V, jP, iP)) continue;
+      if (!on || jP >= g.ny || iP >= nx || !uv_in(g, V, jP, iP)) continue;
       const size_t cP = (size_t)jP * nx + iP;
       const float sg = e == 0 ? 1.f : -1.f;
       const float em = V ? ev * s[WF_MSFVX_INV][cP] : eu / s[WF_MSFUY][cP];
-#pragma unroll 4
-      for (int k = 0; k < ktf; ++k) {
+#pragma unroll 2
+      for (int k = ty; k < ktf; k += kColLevels) {
         const UvTerm t = e == 0 ? uv_term<true, false>(g, s, b, dts, V, k, jP, iP)
                                 : uv_term<false, false>(g, s, b, dts, V, k, jP, iP);
         if (e == 0) {
@@ -484,6 +491,20 @@ __global__ void k_advance_uv_adj_col(Grid g, S s, S b, float dts) {
         amudf += sg * t.ub * em;
       }
     }
+  red[0][ty][tx] = amuu;
+  red[1][ty][tx] = amuv;
+  red[2][ty][tx] = amu;
+  red[3][ty][tx] = amudf;
+  __syncthreads();
+  if (ty != 0 || !on) return;
+  amuu = amuv = amu = amudf = 0.f;
+#pragma unroll
+  for (int y = 0; y < kColLevels; ++y) {
+    amuu += red[0][y][tx];
+    amuv += red[1][y][tx];
+    amu += red[2][y][tx];
+    amudf += red[3][y][tx];
+  }
   if (amuu != 0.f) b[WF_MUU][c] += amuu;
   if (amuv != 0.f) b[WF_MUV][c] += amuv;
   if (amu != 0.f) b[WF_MU][c] += amu;
@@ -493,7 +514,7 @@ __global__ void k_advance_uv_adj_col(Grid g, S s, S b, float dts) {
 int launch_advance_uv_adj(const Grid& g, const S& s, const S& b, float dts, cudaStream_t st) {
   const dim3 b3(32, 4), b2(32, 8);
   k_advance_uv_adj<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, dts);
-  k_advance_uv_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, dts);
+  k_advance_uv_adj_col<<<dim3((g.nx + 31) / 32, g.ny), dim3(32, kColLevels), 0, st>>>(g, s, b, dts);
   return 2;
 }
 
@@ -578,20 +599,33 @@ __global__ void k_calc_p_rho_adj(Grid g, S s, S b, int step) {
   if (aph != 0.f) b[WF_PH][p] += aph;
 }
 
-__global__ void k_calc_p_rho_adj_col(Grid g, S s, S b, int step) {
-  WRF_COLUMN_INDEX(g, j, i);
-  if (!prho_in(g, 0, j, i)) return;
+__global__ void __launch_bounds__(32 * kColLevels) k_calc_p_rho_adj_col(Grid g, S s, S b, int step) {
+  __shared__ float red[2][kColLevels][32];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.x * 32 + tx, j = blockIdx.y;
+  const bool on = i < g.nx && prho_in(g, 0, j, i);
   const size_t lev = (size_t)g.ny * g.nx;
-  const int c = g.i2(j, i);
-  const float mut = s[WF_MUTS][c];
+  const int c = g.i2(j, on ? i : 0);
+  const float mut = on ? s[WF_MUTS][c] : 1.f;
   float amu = 0.f, amut = 0.f;
-  for (int k = 0; k < g.nz - 1; ++k) {
+#pragma unroll 2
+  for (int k = ty; on && k < g.nz - 1; k += kColLevels) {
     const size_t p = k * lev + c;
     const PrhoTerm t = prho_term(g, s, b, step, k, j, i);
     const float alt = s[WF_ALT][p], t1 = s[WF_T_SAVE][p];
     const float Xb = s[WF_C2A][p] * t.p1b;
     amu += Xb * alt * (-t1) / t.Dn + t.Ab * (-alt / mut);
     amut += -Xb * t.X / mut + t.Ab * (-t.al / mut);
+  }
+  red[0][ty][tx] = amu;
+  red[1][ty][tx] = amut;
+  __syncthreads();
+  if (ty != 0 || !on) return;
+  amu = amut = 0.f;
+#pragma unroll
+  for (int y = 0; y < kColLevels; ++y) {
+    amu += red[0][y][tx];
+    amut += red[1][y][tx];
   }
   b[WF_MU][c] += amu;
   b[WF_MUTS][c] += amut;
@@ -620,7 +654,7 @@ int launch_calc_p_rho(const Grid& g, const S& s, int step, cudaStream_t st) {
 int launch_calc_p_rho_adj(const Grid& g, const S& s, const S& b, int step, cudaStream_t st) {
   const dim3 b3(32, 4), b2(32, 8);
   k_calc_p_rho_adj<<<point_grid(g, b3), b3, 0, st>>>(g, s, b, step);
-  k_calc_p_rho_adj_col<<<col_grid(g, b2), b2, 0, st>>>(g, s, b, step);
+  k_calc_p_rho_adj_col<<<dim3((g.nx + 31) / 32, g.ny), dim3(32, kColLevels), 0, st>>>(g, s, b, step);
   k_calc_p_rho_adj_out<<<point_grid(g, b3), b3, 0, st>>>(g, b, step);
   return 3;
 }
@@ -1589,9 +1623,14 @@ int launch_vsolve_w_adj(int ncol, int nz, const float* x, const float* a, const 
 }
 
 // one column of calc_coef_w's adjoint; the forward is k_coef_w (k_acoustic.cu)
-__global__ void k_coef_w_adj(Grid g, const float* mut_, const float* cqw, const float* c2a, const float* rdn,
-                             const float* rdnw, float dts, const float* abar, const float* alphabar,
-                             const float* gammabar, float* mutbar, float* cqwbar, float* c2abar) {
+// (the cotangent arrays are the caller's own buffers, distinct from the
+// operands: __restrict__ lets the level loops' loads run ahead of their
+// stores)
+__global__ void k_coef_w_adj(Grid g, const float* __restrict__ mut_, const float* __restrict__ cqw,
+                             const float* __restrict__ c2a, const float* __restrict__ rdn,
+                             const float* __restrict__ rdnw, float dts, const float* __restrict__ abar,
+                             const float* __restrict__ alphabar, const float* __restrict__ gammabar,
+                             float* __restrict__ mutbar, float* __restrict__ cqwbar, float* __restrict__ c2abar) {
   WRF_COLUMN_INDEX(g, j, i);
   if (j < g.jds || j >= g.jde - 1 || i < g.ids || i >= g.ide - 1) return;
   const int nz = g.nz;
@@ -1607,6 +1646,7 @@ __global__ void k_coef_w_adj(Grid g, const float* mut_, const float* cqw, const 
   const float c2t = c2a[(nz - 2) * lev + c], rwt = rdnw[nz - 2];
   const float atop = cofm2 * (rwt * rwt) * c2t * lid / mm;
   gm[0] = 0.f;
+#pragma unroll 4
   for (int k = 1; k < nz - 1; ++k) {
     const size_t p = k * lev + c;
     const float cw = cqw[p];
@@ -1631,6 +1671,7 @@ __global__ void k_coef_w_adj(Grid g, const float* mut_, const float* cqw, const 
     mmb += -bb * (btop - 1.0f) / mm - atb * atop / mm;
   }
   float c2b_next = 0.f;  // cotangent of c2a at level k (from the k+1 step's c2a(k) terms)
+#pragma unroll 4
   for (int k = nz - 2; k >= 1; --k) {
     const size_t p = k * lev + c;
     const float cw = cqw[p];

@@ -175,8 +175,13 @@ __global__ void k_hdiff_op(Grid g, S s, int var, const float* f, const float* ba
 // its reverse, over the same level ranges: the field's and the viscosity's
 // cotangents scattered with atomics, the column mass's summed over the
 // thread's levels first
-__global__ void k_hdiff_op_adj(Grid g, S s, int var, const float* f, const float* base, const float* mut,
-                               const float* K, const float* tbar, float* fbar, float* mutbar, float* Kbar) {
+// (the cotangent outputs are distinct from every operand and from each
+// other: __restrict__ lets a level's loads run ahead of the previous
+// level's atomic adds)
+__global__ void k_hdiff_op_adj(Grid g, S s, int var, const float* __restrict__ f, const float* __restrict__ base,
+                               const float* __restrict__ mut, const float* __restrict__ K,
+                               const float* __restrict__ tbar, float* __restrict__ fbar, float* __restrict__ mutbar,
+                               float* __restrict__ Kbar) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   const int z0 = blockIdx.z * kHdiffLevels;
   if (i >= g.nx || j >= g.ny || !diff_region(g, var, g.nz - 2, j, i)) return;
@@ -187,6 +192,7 @@ __global__ void k_hdiff_op_adj(Grid g, S s, int var, const float* f, const float
   diff_coefs(g, s, var, c, cf);
   float wm[4] = {0.f, 0.f, 0.f, 0.f};  // the mass averages' cotangents, per edge
   const float sgn[4] = {-1.f, 1.f, -1.f, 1.f};
+#pragma unroll 2
   for (int k = z0; k < z0 + kHdiffLevels && k < g.nz; ++k) {
     if (!diff_region(g, var, k, j, i)) continue;
     const size_t p = (size_t)k * lev + c;

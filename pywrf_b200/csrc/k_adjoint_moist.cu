@@ -105,11 +105,14 @@ __global__ void k_flowdep_adj(Grid g, S s, S b) {
   }
   if (!mode) return;
   const size_t p = base + (size_t)j * nx + i, q = base + (size_t)sj * nx + si;
+  float* fb = b[WF_MOIST];
+  float v[5];  // the five species' loads before the first store
+#pragma unroll
+  for (int m = 2; m < 7; ++m) v[m - 2] = fb[m * n3 + p];
+#pragma unroll
   for (int m = 2; m < 7; ++m) {
-    float* fb = b[WF_MOIST] + m * n3;
-    const float v = fb[p];
-    fb[p] = 0.f;
-    if (mode == 1 || cond) acc(fb, q, v);
+    fb[m * n3 + p] = 0.f;
+    if (mode == 1 || cond) acc(fb, m * n3 + q, v[m - 2]);
   }
 }
 
