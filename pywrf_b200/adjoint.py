@@ -237,6 +237,10 @@ class AdvanceUV(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        # outputs without a cotangent reach backward as None (its _bars / None
+        # checks hand out zeros from one shared buffer) instead of one
+        # zero-filled tensor each, which backward would then clone
+        ctx.set_materialize_grads(False)
         _cuda_only(*tensors)
         dts, emdiv, cf1, cf2, cf3, rdx, rdy = (float(x) for x in scal)
         named = dict(zip(UV_INPUTS + UV_DATA, tensors))
@@ -292,6 +296,10 @@ class Forces(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        # outputs without a cotangent reach backward as None (its _bars / None
+        # checks hand out zeros from one shared buffer) instead of one
+        # zero-filled tensor each, which backward would then clone
+        ctx.set_materialize_grads(False)
         _cuda_only(*tensors)
         terms = int(scal[0])
         rdx, rdy, cf1, cf2, cf3, cfn, cfn1 = (float(x) for x in scal[1:])
@@ -342,6 +350,10 @@ class Sumflux(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        # outputs without a cotangent reach backward as None (its _bars / None
+        # checks hand out zeros from one shared buffer) instead of one
+        # zero-filled tensor each, which backward would then clone
+        ctx.set_materialize_grads(False)
         _cuda_only(*tensors)
         iteration, nsub = int(scal[0]), int(scal[1])
         named = dict(zip(SF_INPUTS + SF_DATA, tensors))
@@ -459,6 +471,10 @@ class Prep(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        # outputs without a cotangent reach backward as None (its _bars / None
+        # checks hand out zeros from one shared buffer) instead of one
+        # zero-filled tensor each, which backward would then clone
+        ctx.set_materialize_grads(False)
         _cuda_only(*tensors)
         ops = int(scal[0])
         named = dict(zip(PREP_FIELDS + PREP_DATA, tensors))
@@ -573,6 +589,10 @@ class AdvanceW(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        # outputs without a cotangent reach backward as None (its _bars / None
+        # checks hand out zeros from one shared buffer) instead of one
+        # zero-filled tensor each, which backward would then clone
+        ctx.set_materialize_grads(False)
         _cuda_only(*tensors)
         dts, epssm, cf1, cf2, cf3, rdx, rdy = (float(x) for x in scal)
         named = dict(zip(AW_INPUTS + AW_DATA, tensors))
@@ -625,6 +645,10 @@ class AdvanceMuT(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        # outputs without a cotangent reach backward as None (its _bars / None
+        # checks hand out zeros from one shared buffer) instead of one
+        # zero-filled tensor each, which backward would then clone
+        ctx.set_materialize_grads(False)
         _cuda_only(*tensors)
         dts, epssm, rdx, rdy = (float(x) for x in scal[:4])
         named = dict(zip(MUT_INPUTS + MUT_DATA, tensors))
@@ -675,6 +699,10 @@ class CalcPRho(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, scal, *tensors):
+        # outputs without a cotangent reach backward as None (its _bars / None
+        # checks hand out zeros from one shared buffer) instead of one
+        # zero-filled tensor each, which backward would then clone
+        ctx.set_materialize_grads(False)
         _cuda_only(*tensors)
         smdiv, step, rdx, rdy = float(scal[0]), int(scal[1]), float(scal[2]), float(scal[3])
         named = dict(zip(PRHO_INPUTS + ("rdnw",), tensors))
@@ -797,6 +825,10 @@ class CoefW(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, mut, cqw, c2a, rdn, rdnw, dts: float, epssm: float, top_lid: bool, rdx: float, rdy: float):
+        # outputs without a cotangent reach backward as None (its _bars / None
+        # checks hand out zeros from one shared buffer) instead of one
+        # zero-filled tensor each, which backward would then clone
+        ctx.set_materialize_grads(False)
         _cuda_only(mut, cqw, c2a, rdn, rdnw)
         cg = scalar_grid(cqw.shape, rdx, rdy)
         cg.epssm = float(epssm)
@@ -949,6 +981,10 @@ class _TableOp(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, op, cg, *tensors):
+        # outputs without a cotangent reach backward as None (its _bars / None
+        # checks hand out zeros from one shared buffer) instead of one
+        # zero-filled tensor each, which backward would then clone
+        ctx.set_materialize_grads(False)
         _cuda_only(*tensors)
         named = dict(zip(op.fields + op.data, tensors))
         outs = {k: named[k].detach().clone() for k in op.outputs}
